@@ -1,0 +1,1893 @@
+// ORACLE — test infrastructure only.
+//
+// A CPU, FP64, scalar restatement of Synergia's space-charge + libFF tracking
+// step, written from the reference sources (paths relative to the synergia2
+// project root).  It exists to check the CUDA path: only tests/, the smoke
+// check of __graft_entry__.py and bench.py's cpu_baseline leg may load it.
+// Nothing in the product links or calls it.
+//
+// Parity pins: the libFF MAD-X golden tracks
+// (src/synergia/libFF/tests/lattices/madx_*.out), the zero-particle tests
+// (src/synergia/libFF/tests/test_zeroparticle_propagate.cc), the one-particle
+// deposit test (src/synergia/collective/tests/test_deposit.cc:42-97), the rod
+// bunch line-charge kick (src/synergia/collective/tests/
+// test_space_charge_3d_open_hockney_mpi.cc:8-107) and the Gaussian-sphere
+// potential of docs/devel/solvers/3d_open_hockney.py:10-22.  The FFT has no
+// golden vectors in the reference; it is pinned against a direct DFT and
+// numpy.fft by the tests.
+//
+// Build: oracle/Makefile (g++ -O2 -ffp-contract=off -fopenmp -shared).
+// -ffp-contract=off keeps every a*b+c as two IEEE roundings, as the reference
+// (no -ffast-math in effect, CMakeLists.txt:338) does.
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace orc {
+
+// ---------------------------------------------------------------------------
+// constants: src/synergia/foundation/physical_constants.h (PDG 2012)
+// ---------------------------------------------------------------------------
+namespace pc {
+constexpr double pi = 3.14159265358979323846;
+constexpr double mp = 0.938272046;
+constexpr double e = 1.602176565e-19;
+constexpr double c = 299792458.0;
+constexpr double mu0 = 4 * pi * 1.0e-7;
+constexpr double epsilon0 = 1.0 / (c * c * mu0);
+constexpr double rp = e / (4 * pi * epsilon0 * mp * 1.0e9);
+} // namespace pc
+
+thread_local std::string g_err;
+
+// ---------------------------------------------------------------------------
+// Four_momentum / Reference_particle (foundation/four_momentum.cc:8-16,
+// foundation/reference_particle.cc)
+// ---------------------------------------------------------------------------
+struct Refpart {
+    int charge = 1;
+    double mass = pc::mp;
+    double gamma = 1, beta = 0, p = 0, energy = 0;
+    std::array<double, 6> state{0, 0, 0, 0, 0, 0};
+    double s_n = 0;
+
+    void set_gamma(double g)
+    { // four_momentum.cc:8-16 update_from_gamma
+        if (g < 1.0) throw std::range_error("Four_momentum: gamma not >= 1.0");
+        gamma = g;
+        energy = gamma * mass;
+        beta = std::sqrt(1.0 - 1.0 / (gamma * gamma));
+        p = gamma * beta * mass;
+    }
+    void set_total_energy(double E) { set_gamma(E / mass); }
+    void set_kinetic_energy(double K) { set_gamma((mass + K) / mass); } // four_momentum.cc:84-88
+    // kind: 0 total energy, 1 momentum, 2 kinetic energy
+    void set_by(int kind, double v)
+    {
+        if (kind == 0)
+            set_total_energy(v);
+        else if (kind == 1)
+            set_momentum(v);
+        else
+            set_kinetic_energy(v);
+    }
+    void set_momentum(double mom)
+    { // four_momentum.cc:90-95 then set_beta
+        double r2 = mom * mom / (mass * mass);
+        double b = std::sqrt(r2 / (1 + r2));
+        if (b < 0.0 || b >= 1.0) throw std::range_error("beta out of range");
+        set_gamma(1.0 / std::sqrt(1.0 - b * b));
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Lattice_element / Lattice_element_slice (lattice/lattice_element*.cc)
+// ---------------------------------------------------------------------------
+struct Element {
+    std::string type, name;
+    std::map<std::string, double> d;
+    std::map<std::string, std::string> s;
+    std::map<std::string, std::vector<double>> v;
+
+    double get(const std::string& k, double def) const
+    {
+        auto it = d.find(k);
+        return it == d.end() ? def : it->second;
+    }
+    double get(const std::string& k) const
+    {
+        auto it = d.find(k);
+        if (it == d.end())
+            throw std::runtime_error("Lattice_element::get_double_attribute: element " +
+                                     name + " of type " + type +
+                                     " has no double attribute '" + k + "'");
+        return it->second;
+    }
+    bool has_s(const std::string& k) const { return s.count(k) > 0; }
+    std::string gets(const std::string& k, const std::string& def) const
+    {
+        auto it = s.find(k);
+        return it == s.end() ? def : it->second;
+    }
+    double length() const { return get("l", 0.0); }
+};
+
+struct Lattice {
+    std::vector<Element> elements;
+    Refpart ref;
+    double length() const
+    { // lattice.cc:195-201
+        double L = 0.0;
+        for (auto const& e : elements) L += e.length();
+        return L;
+    }
+};
+
+// lattice_element_slice.cc:9-47 (split_element_tolerance 1e-9)
+struct Slice {
+    const Element* e = nullptr;
+    double left = 0, right = 0;
+    bool ledge = true, redge = true;
+    Slice() = default;
+    explicit Slice(const Element& el) : e(&el), left(0), right(el.length()) {}
+    Slice(const Element& el, double l, double r) : e(&el), left(l), right(r)
+    {
+        const double tol = 1.0e-9;
+        if (left < 0.0) throw std::range_error("Lattice_element_slice: left must be >= 0.0");
+        if (left < tol) {
+            ledge = true;
+            left = 0.0;
+        } else
+            ledge = false;
+        double L = el.length();
+        if (right > L + tol)
+            throw std::range_error("Lattice_element_slice: right must be no greater than the length of the element");
+        bool eq;
+        if (std::abs(right) < tol)
+            eq = std::abs(right - L) < tol;
+        else
+            eq = std::abs((right - L) / right) < tol;
+        if (eq) {
+            redge = true;
+            right = L;
+        } else
+            redge = false;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Bunch (bunch/bunch.h, bunch_particles.h): N x 7 column-major FP64, masks.
+// ---------------------------------------------------------------------------
+struct Bunch {
+    int n_active = 0, n_valid = 0, n_total = 0;
+    int64_t cap = 0;
+    double real_num = 1.0;
+    std::vector<double> parts;
+    std::vector<uint8_t> masks, discards;
+    Refpart ref;    // bunch reference particle
+    Refpart design; // design reference particle
+    double& P(int64_t i, int j) { return parts[j * cap + i]; }
+
+    void update_total_num()
+    { // bunch.h:363-370
+        int old_total = n_total;
+        n_total = n_valid;
+        real_num = old_total ? n_total * real_num / old_total : 0.0;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// ff_algorithm.h units
+// ---------------------------------------------------------------------------
+inline bool close_to_zero(double v) { return std::fabs(v) < 1e-13; } // :18-22
+
+// drift_unit ff_algorithm.h:47-79
+inline void drift_unit(double& x, double xp, double& y, double yp, double& cdt, double dpop,
+                       double length, double reference_momentum, double m, double reference_cdt)
+{
+    double uni = 1.0;
+    double sig = (double)((0.0 < length) - (length < 0.0));
+    double vl = length, vm = m, vrm = reference_momentum, vrc = reference_cdt;
+    double dp = dpop + uni;
+    double inv_npz = uni / std::sqrt(dp * dp - xp * xp - yp * yp);
+    double lxpr = xp * vl * inv_npz;
+    double lypr = yp * vl * inv_npz;
+    double D2 = lxpr * lxpr + vl * vl + lypr * lypr;
+    double p = dp * vrm;
+    double E2 = p * p + vm * vm;
+    double ibeta2 = E2 / (p * p);
+    x = x + lxpr;
+    y = y + lypr;
+    cdt = cdt + sig * std::sqrt(D2 * ibeta2) - vrc;
+}
+
+// slot_unit ff_algorithm.h:83-129
+inline void slot_unit(double& x, double& xp, double& y, double& yp, double& cdt, double& dpop,
+                      double ct, double st, double pref, double m)
+{
+    const double uni = 1.0;
+    double r0 = x, r1 = y, r2 = 0.0;
+    double zp = std::sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
+    double p = (dpop + uni) * pref;
+    double e = std::sqrt(p * p + m * m);
+    double b0 = xp * pref / e;
+    double b1 = yp * pref / e;
+    double b2 = zp * pref / e;
+    double bp = st * b0 + ct * b2;
+    double tau = -x * st / bp;
+    r0 = x + tau * b0;
+    r1 = y + tau * b1;
+    r2 = tau * b2;
+    x = r0 * ct - r2 * st;
+    y = r1;
+    cdt = cdt + tau;
+    xp = xp * ct - zp * st;
+}
+
+// edge_unit (ref particle angle form) ff_algorithm.h:139-148
+inline void edge_unit(double y, double& xp, double& yp, double kx, double ky)
+{
+    yp = yp - kx * y;
+    xp = xp + ky * y;
+}
+
+// bend_complete ff_algorithm.h:191-251 (host, complex arithmetic)
+inline void bend_complete(double& x, double& xp, double& y, double& yp, double& cdt, double dpop,
+                          double dphi, double strength, double p_ref, double m, double cdt_ref,
+                          std::complex<double> phase, std::complex<double> term)
+{
+    typedef std::complex<double> CT;
+    const double uni = 1.0;
+    double p0 = p_ref;
+    double p = p_ref * (dpop + 1.0);
+    double E0 = std::sqrt(p0 * p0 + m * m);
+    double E = std::sqrt(p * p + m * m);
+    double igamma = m / E0;
+    double ibeta = uni / std::sqrt(uni - igamma * igamma);
+    double csq = pc::c * pc::c * 1e-9;
+    double psq = (dpop + 1.0) * (dpop + 1.0);
+    double Ef = uni / std::sqrt(psq + igamma * igamma * ibeta * ibeta);
+    double beta1 = Ef * xp;
+    double beta2 = Ef * yp;
+    double beta3 = Ef * std::sqrt((dpop + 1.0) * (dpop + 1.0) - xp * xp - yp * yp);
+    CT ui = CT(0.0, x);
+    CT vui = CT(pc::c * beta3, pc::c * beta1);
+    double iomega = E / (csq * strength);
+    CT bi = CT(0.0, 1.0) * vui * iomega - ui;
+    CT bf = bi * phase + term;
+    double rho = pc::c * std::sqrt(beta1 * beta1 + beta3 * beta3) * iomega;
+    double dthmphi = std::asin(bi.real() / rho) - std::asin(bf.real() / rho);
+    CT expf = std::exp(CT(0.0, dthmphi));
+    CT vuf = vui * expf;
+    CT uf = (ui + bi) * expf - bf;
+    double dtheta = dthmphi + dphi;
+    double ncdt = -pc::c * dtheta * iomega;
+    x = uf.imag();
+    y += beta2 * ncdt;
+    cdt += ncdt - cdt_ref;
+    xp = vuf.imag() / (Ef * pc::c);
+}
+
+// bend_unit ff_algorithm.h:255-343 (device form, real arithmetic)
+inline void bend_unit(double& x, double& xp, double& y, double& yp, double& cdt, double dpop,
+                      double theta, double strength, double p_ref, double m, double cdt_ref,
+                      std::complex<double> phase, std::complex<double> term)
+{
+    const double uni = 1.0;
+    const double tc = pc::c;
+    double p0 = p_ref;
+    double p = p_ref * (dpop + uni);
+    double E0 = std::sqrt(p0 * p0 + m * m);
+    double E = std::sqrt(p * p + m * m);
+    double igamma = m / E0;
+    double ibeta = uni / std::sqrt(uni - igamma * igamma);
+    double csq = pc::c * pc::c * 1e-9;
+    double psq = (dpop + uni) * (dpop + uni);
+    double Ef = uni / std::sqrt(psq + igamma * igamma * ibeta * ibeta);
+    double beta1 = Ef * xp;
+    double beta2 = Ef * yp;
+    double beta3 = Ef * std::sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
+    double ui_r = 0.0, ui_i = x;
+    double vui_r = tc * beta3, vui_i = tc * beta1;
+    double iomega = E / (csq * strength);
+    double bi_r = -vui_i * iomega - ui_r;
+    double bi_i = vui_r * iomega - ui_i;
+    double phase_r = phase.real(), phase_i = phase.imag();
+    double bf_r = bi_r * phase_r - bi_i * phase_i + term.real();
+    double bf_i = bi_r * phase_i + bi_i * phase_r + term.imag();
+    double rho = tc * std::sqrt(beta1 * beta1 + beta3 * beta3) * iomega;
+    double dthmphi = std::asin(bi_r / rho) - std::asin(bf_r / rho);
+    double expf_r = std::cos(dthmphi);
+    double expf_i = std::sin(dthmphi);
+    double vuf_i = vui_r * expf_i + vui_i * expf_r;
+    double uf_i = (ui_r + bi_r) * expf_i + (ui_i + bi_i) * expf_r - bf_i;
+    double dtheta = dthmphi + theta;
+    double ncdt = -tc * dtheta * iomega;
+    x = uf_i;
+    xp = vuf_i / (Ef * tc);
+    y = y + beta2 * ncdt;
+    cdt = cdt + ncdt - cdt_ref;
+}
+
+// thin kicks ff_algorithm.h:919-963
+inline void thin_dipole_unit(double, double& xp, double, double& yp, const double* kL)
+{
+    xp = xp - kL[0];
+    yp = yp + kL[1];
+}
+inline void thin_quadrupole_unit(double x, double& xp, double y, double& yp, const double* kL)
+{
+    double vk0 = kL[0], vk1 = kL[1];
+    xp = xp - vk0 * x + vk1 * y;
+    yp = yp + vk0 * y + vk1 * x;
+}
+inline void thin_sextupole_unit(double x, double& xp, double y, double& yp, const double* kL)
+{
+    double vk0 = kL[0], vk1 = kL[1];
+    xp = xp - 0.5 * vk0 * (x * x - y * y) + vk1 * x * y;
+    yp = yp + vk0 * x * y + 0.5 * vk1 * (x * x - y * y);
+}
+inline void thin_octupole_unit(double x, double& xp, double y, double& yp, const double* kL)
+{
+    double vk0 = kL[0], vk1 = kL[1];
+    double n1 = 0.5, n2 = 1.0 / 3.0;
+    xp = xp - n1 * vk0 * (x * x * x * n2 - x * y * y) + n1 * vk1 * (x * x * y - y * y * y * n2);
+    yp = yp - n1 * vk0 * (y * y * y * n2 - x * x * y) + n1 * vk1 * (x * x * x * n2 - x * y * y);
+}
+
+inline double factorial(int n)
+{ // ff_algorithm.h:1108-1117
+    if (n == 0) return 1.0;
+    double r = 1;
+    for (int i = 1; i <= n; ++i) r *= i;
+    return r;
+}
+inline double qpow(double x, int i)
+{ // utils/kokkos_types.h:89-95
+    double r = 1;
+    while (i--) r = r * x;
+    return r;
+}
+
+// thin_magnet_unit ff_algorithm.h:1122-1168
+inline void thin_magnet_unit(double x, double& xp, double y, double& yp, const double* kL, int n)
+{
+    for (int k = 0; k < n; k += 4)
+        xp = xp - (kL[0] * (n - k)) * qpow(x, n - k - 1) * qpow(y, k) / (factorial(n - k) * factorial(k));
+    for (int k = 2; k < n; k += 4)
+        xp = xp + (kL[0] * (n - k)) * qpow(x, n - k - 1) * qpow(y, k) / (factorial(n - k) * factorial(k));
+    for (int k = 1; k < n; k += 4)
+        xp = xp + (kL[1] * (n - k)) * qpow(x, n - k - 1) * qpow(y, k) / (factorial(n - k) * factorial(k));
+    for (int k = 3; k < n; k += 4)
+        xp = xp - (kL[1] * (n - k)) * qpow(x, n - k - 1) * qpow(y, k) / (factorial(n - k) * factorial(k));
+    for (int k = 4; k <= n; k += 4)
+        yp = yp - (kL[0] * k) * qpow(x, n - k) * qpow(y, k - 1) / (factorial(n - k) * factorial(k));
+    for (int k = 2; k <= n; k += 4)
+        yp = yp + (kL[0] * k) * qpow(x, n - k) * qpow(y, k - 1) / (factorial(n - k) * factorial(k));
+    for (int k = 1; k <= n; k += 4)
+        yp = yp + (kL[1] * k) * qpow(x, n - k) * qpow(y, k - 1) / (factorial(n - k) * factorial(k));
+    for (int k = 3; k <= n; k += 4)
+        yp = yp - (kL[1] * k) * qpow(x, n - k) * qpow(y, k - 1) / (factorial(n - k) * factorial(k));
+}
+
+// Kick functor forms used by the integrators.
+using kick_fn = void (*)(double, double&, double, double&, double, const double*);
+
+inline void quad_kick(double x, double& xp, double y, double& yp, double, const double* kL)
+{ // ff_quadrupole.h:16-19
+    thin_quadrupole_unit(x, xp, y, yp, kL);
+}
+inline void quad_cf_kick(double x, double& xp, double y, double& yp, double, const double* kL)
+{ // ff_quadrupole.h:22-35
+    thin_quadrupole_unit(x, xp, y, yp, kL);
+    if (kL[2] || kL[3]) thin_quadrupole_unit(x, xp, y, yp, kL + 2);
+    if (kL[4] || kL[5]) thin_sextupole_unit(x, xp, y, yp, kL + 4);
+    if (kL[6] || kL[7]) thin_octupole_unit(x, xp, y, yp, kL + 6);
+    if (kL[8] || kL[9]) thin_magnet_unit(x, xp, y, yp, kL + 8, 5);
+    if (kL[10] || kL[11]) thin_magnet_unit(x, xp, y, yp, kL + 10, 6);
+    if (kL[12] || kL[13]) thin_magnet_unit(x, xp, y, yp, kL + 12, 7);
+    if (kL[14] || kL[15]) thin_magnet_unit(x, xp, y, yp, kL + 14, 8);
+}
+inline void sext_kick(double x, double& xp, double y, double& yp, double, const double* kL)
+{ // ff_sextupole.h:11-13
+    thin_sextupole_unit(x, xp, y, yp, kL);
+}
+
+// yoshida6 ff_algorithm.h:1834-2008 (hardwired 6th order, 10 drifts/step)
+inline void yoshida6(double& x, double& xp, double& y, double& yp, double& cdt, double dpop,
+                     double reference_momentum, double m, double step_reference_cdt,
+                     double step_length, const double* step_strength, int steps, kick_fn kf,
+                     int components)
+{
+    const double c1 = 0.79361246386112147294625603763;
+    const double c2 = -0.206276584816439780698721319354;
+    const double c3 = -0.118008867881292655922412133144;
+    const double c4 = 0.236949573653050744373598734219;
+    const double d1 = 1.58722492772224294589251207526;
+    const double d2 = -1.99977809735512250728995471397;
+    const double d3 = -1.82324266348482825773733634154;
+    const double d4 = 2.29714181079092974648453380998;
+    double sub = step_reference_cdt * 0.1;
+    double k1[16], k2[16], k3[16], k4[16];
+    for (int i = 0; i < components; ++i)
+        for (int j = 0; j < 2; ++j) {
+            k1[i * 2 + j] = d1 * step_strength[i * 2 + j];
+            k2[i * 2 + j] = d2 * step_strength[i * 2 + j];
+            k3[i * 2 + j] = d3 * step_strength[i * 2 + j];
+            k4[i * 2 + j] = d4 * step_strength[i * 2 + j];
+        }
+    auto D = [&](double c) { drift_unit(x, xp, y, yp, cdt, dpop, c * step_length, reference_momentum, m, sub); };
+    for (int i = 0; i < steps; ++i) {
+        D(c1); kf(x, xp, y, yp, cdt, k1);
+        D(c2); kf(x, xp, y, yp, cdt, k2);
+        D(c2); kf(x, xp, y, yp, cdt, k1);
+        D(c3); kf(x, xp, y, yp, cdt, k3);
+        D(c4); kf(x, xp, y, yp, cdt, k4);
+        D(c4); kf(x, xp, y, yp, cdt, k3);
+        D(c3); kf(x, xp, y, yp, cdt, k1);
+        D(c2); kf(x, xp, y, yp, cdt, k2);
+        D(c2); kf(x, xp, y, yp, cdt, k1);
+        D(c1);
+    }
+}
+
+// general n-th order yoshida, ff_algorithm.h:1481-1646 (used only for the
+// design particle of thick sextupoles through FF_patterned_propagator)
+inline double yx1(int nn) { return 1.0 / (2.0 - std::pow(2.0, 1.0 / (2 * nn + 1))); }
+inline double yx0(int nn) { return 1.0 - 2.0 * yx1(nn); }
+inline void yoshida_element(int n, double& x, double& xp, double& y, double& yp, double& cdt,
+                            double dpop, double pref, double m, double step_ref_cdt,
+                            double step_length, const double* step_strength, double c,
+                            kick_fn kf, int components)
+{
+    if (n == 0) {
+        double sub = step_ref_cdt / 2.0;
+        double kl[16];
+        for (int i = 0; i < components * 2; ++i) kl[i] = step_strength[i] * c;
+        drift_unit(x, xp, y, yp, cdt, dpop, 0.5 * c * step_length, pref, m, sub);
+        kf(x, xp, y, yp, cdt, kl);
+        drift_unit(x, xp, y, yp, cdt, dpop, 0.5 * c * step_length, pref, m, sub);
+        return;
+    }
+    double sub = step_ref_cdt / 3.0;
+    yoshida_element(n - 1, x, xp, y, yp, cdt, dpop, pref, m, sub, step_length, step_strength, c * yx1(n), kf, components);
+    yoshida_element(n - 1, x, xp, y, yp, cdt, dpop, pref, m, sub, step_length, step_strength, c * yx0(n), kf, components);
+    yoshida_element(n - 1, x, xp, y, yp, cdt, dpop, pref, m, sub, step_length, step_strength, c * yx1(n), kf, components);
+}
+inline void yoshida_general(int order, double& x, double& xp, double& y, double& yp, double& cdt,
+                            double dpop, double pref, double m, double step_ref_cdt,
+                            double step_length, const double* step_strength, int steps,
+                            kick_fn kf, int components)
+{
+    const int n = (order - 2) / 2;
+    for (int i = 0; i < steps; ++i)
+        yoshida_element(n, x, xp, y, yp, cdt, dpop, pref, m, step_ref_cdt, step_length, step_strength, 1.0, kf, components);
+}
+
+// ---------------------------------------------------------------------------
+// Element maps (host part + particle loop), libFF/ff_*.h
+// ---------------------------------------------------------------------------
+static void drift_apply(const Slice& slice, Bunch& b)
+{ // ff_drift.h:95-152
+    const double length = slice.right - slice.left;
+    const double mass = b.ref.mass;
+    if (close_to_zero(length)) {
+        b.design.state[4] = 0.0;
+        return;
+    }
+    Refpart& ref_l = b.design;
+    const double ref_p = b.ref.p * (1.0 + b.ref.state[5]);
+    // get_reference_cdt ff_drift.h:69-88
+    double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3];
+    double cdt = 0.0, dpop = 0.0;
+    drift_unit(x, xp, y, yp, cdt, dpop, length, ref_l.p, ref_l.mass, 0.0);
+    ref_l.state = {x, xp, y, yp, cdt, dpop};
+    const double ref_cdt = cdt;
+    if (b.n_valid) {
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < b.n_active; ++i)
+            if (b.masks[i])
+                drift_unit(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), b.P(i, 4), b.P(i, 5), length, ref_p, mass, ref_cdt);
+    }
+    b.ref.s_n += length;
+}
+
+static void quad_apply(const Slice& slice, Bunch& b)
+{ // ff_quadrupole.h:310-565
+    const Element& ele = *slice.e;
+    double length = slice.right - slice.left;
+    const double xoff = ele.get("hoffset", 0.0);
+    const double yoff = ele.get("voffset", 0.0);
+    double tilt = ele.get("tilt", 0.0);
+    double kn[16] = {0};
+    kn[0] = ele.get("k1", 0.0);
+    kn[1] = ele.get("k1s", 0.0);
+    double quad_str = kn[0];
+    std::complex<double> ck1(kn[0], -kn[1]);
+    double rot = std::arg(ck1) / 2.0 + tilt;
+    if (tilt != 0.0) {
+        std::complex<double> ck2(kn[0], kn[1]);
+        ck2 = ck2 * std::exp(std::complex<double>(0.0, -2.0 * tilt));
+        kn[0] = ck2.real();
+        kn[1] = ck2.imag();
+    }
+    bool has_mp = false;
+    for (int i = 1; i < 8; ++i) {
+        std::string a = "a0", bb = "b0";
+        a[1] = '0' + i;
+        bb[1] = '0' + i;
+        kn[i * 2 + 0] = ele.get(bb, 0.0);
+        kn[i * 2 + 1] = ele.get(a, 0.0);
+        if (kn[i * 2 + 0] || kn[i * 2 + 1]) {
+            has_mp = true;
+            double coeff = factorial(i);
+            kn[i * 2 + 0] *= quad_str * coeff;
+            kn[i * 2 + 1] *= quad_str * coeff;
+            if (rot || tilt) {
+                auto ck = std::complex<double>(kn[i * 2 + 0], kn[i * 2 + 1]);
+                ck *= std::exp(std::complex<double>(0.0, -(i + 1) * tilt));
+                ck *= std::exp(std::complex<double>(0.0, -(i + 1) * rot));
+                kn[i * 2 + 0] = ck.real();
+                kn[i * 2 + 1] = ck.imag();
+            }
+        }
+    }
+    Refpart& ref_l = b.design;
+    const Refpart& ref_b = b.ref;
+    double brho_l = ref_l.p / ref_l.charge;
+    double brho_b = ref_b.p * (1.0 + ref_b.state[5]) / ref_l.charge;
+    double scale = brho_l / brho_b;
+    for (auto& k : kn) k *= scale;
+
+    auto ref_cdt_fn = [&](int steps) {
+        // get_reference_cdt ff_quadrupole.h:263-303
+        double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3];
+        double cdt = 0.0, dpop = 0.0;
+        x -= xoff;
+        y -= yoff;
+        if (close_to_zero(length))
+            thin_quadrupole_unit(x, xp, y, yp, kn);
+        else
+            yoshida6(x, xp, y, yp, cdt, dpop, ref_l.p, ref_l.mass, 0.0, length / steps, kn, steps, quad_cf_kick, 8);
+        x += xoff;
+        y += yoff;
+        ref_l.state = {x, xp, y, yp, cdt, dpop};
+        return cdt;
+    };
+
+    if (close_to_zero(length)) {
+        ref_cdt_fn(0);
+        double k2[2] = {kn[0], kn[1]};
+        if (b.n_valid) {
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < b.n_active; ++i)
+                if (b.masks[i]) {
+                    double x = b.P(i, 0) - xoff;
+                    double y = b.P(i, 2) - yoff;
+                    thin_quadrupole_unit(x, b.P(i, 1), y, b.P(i, 3), k2);
+                }
+        }
+    } else {
+        int steps = (int)ele.get("yoshida_steps", 4.0);
+        for (auto& k : kn) k *= length / steps;
+        double ref_p = ref_b.p, ref_m = ref_b.mass;
+        double ref_t = ref_cdt_fn(steps);
+        double step_ref_t = ref_t / steps, step_l = length / steps;
+        if (b.n_valid) {
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < b.n_active; ++i)
+                if (b.masks[i]) {
+                    double p0 = b.P(i, 0) - xoff, p2 = b.P(i, 2) - yoff;
+                    double p1 = b.P(i, 1), p3 = b.P(i, 3), p4 = b.P(i, 4), p5 = b.P(i, 5);
+                    if (has_mp)
+                        yoshida6(p0, p1, p2, p3, p4, p5, ref_p, ref_m, step_ref_t, step_l, kn, steps, quad_cf_kick, 8);
+                    else
+                        yoshida6(p0, p1, p2, p3, p4, p5, ref_p, ref_m, step_ref_t, step_l, kn, steps, quad_kick, 1);
+                    b.P(i, 0) = p0 + xoff;
+                    b.P(i, 1) = p1;
+                    b.P(i, 2) = p2 + yoff;
+                    b.P(i, 3) = p3;
+                    b.P(i, 4) = p4;
+                }
+        }
+        b.ref.s_n += length;
+    }
+}
+
+struct SbendParams { // ff_sbend.h:14-53
+    bool ledge, redge;
+    double length, angle, r0;
+    int steps;
+    double k_l[10];
+    double scale, strength, pref_b, m_b, ref_cdt;
+    double e1, e2, ce1, se1, ce2, se2;
+    double us_edge_k, ds_edge_k, us_edge_k_p, ds_edge_k_p;
+    double us_edge_k_x, us_edge_k_y, ds_edge_k_x, ds_edge_k_y;
+};
+
+static void sbend_apply(const Slice& slice, Bunch& b)
+{ // ff_sbend.h:741-969, pure dipole branch (cf == 0, no a/b multipoles)
+    const Element& ele = *slice.e;
+    SbendParams sp{};
+    double a = ele.get("angle");
+    double l = ele.get("l");
+    sp.length = slice.right - slice.left;
+    sp.angle = (sp.length / l) * a;
+    sp.r0 = l / a;
+    sp.steps = 6;
+    sp.ledge = slice.ledge;
+    sp.redge = slice.redge;
+    sp.e1 = ele.get("e1", 0.0);
+    sp.e2 = ele.get("e2", 0.0);
+    static const char* kn_names[10] = {"k1", "k1s", "k2", "k2s", "k3", "k3s", "k4", "k4s", "k5", "k5s"};
+    for (int i = 0; i < 10; ++i) sp.k_l[i] = ele.get(kn_names[i], 0.0);
+    for (int i = 0; i < 10; ++i)
+        if (sp.k_l[i] != 0.0)
+            throw std::runtime_error("oracle: combined-function sbend is not part of the restated path");
+    for (int i = 1; i < 5; ++i) {
+        std::string an = "a0", bn = "b0";
+        an[1] = '0' + i;
+        bn[1] = '0' + i;
+        if (ele.get(an, 0.0) != 0.0 || ele.get(bn, 0.0) != 0.0)
+            throw std::runtime_error("oracle: sbend multipole errors are not part of the restated path");
+    }
+    Refpart& ref_l = b.design;
+    const Refpart& ref_b = b.ref;
+    sp.scale = ref_l.p / (ref_b.p * (1.0 + ref_b.state[5]));
+    if (!sp.redge) sp.e2 = 0;
+    if (!sp.ledge) sp.e1 = 0;
+    const double brho_cnv = 1.0e-9 * pc::c;
+    double pref_l = ref_l.p;
+    double brho_l = pref_l / brho_cnv;
+    int charge_l = ref_l.charge;
+    double pref_b = ref_b.p;
+    double brho_b = pref_b / brho_cnv;
+    double m_b = b.ref.mass;
+    sp.strength = brho_l * a / l;
+    sp.pref_b = pref_b;
+    sp.m_b = m_b;
+    sp.ce1 = std::cos(-sp.e1);
+    sp.se1 = std::sin(-sp.e1);
+    sp.ce2 = std::cos(-sp.e2);
+    sp.se2 = std::sin(-sp.e2);
+    double sgn = (charge_l > 0) ? 1.0 : -1.0;
+    sp.us_edge_k = sgn * sp.strength * std::tan(sp.e1) / brho_b;
+    sp.ds_edge_k = -sgn * sp.strength * std::tan(-sp.e2) / brho_b;
+    sp.us_edge_k_p = sgn * sp.strength / brho_b;
+    sp.ds_edge_k_p = -sgn * sp.strength / brho_b;
+    sp.us_edge_k_x = sp.us_edge_k_y = sp.ds_edge_k_x = sp.ds_edge_k_y = 0.0;
+
+    // prop_reference ff_sbend.h:478-566
+    {
+        double m_l = ref_l.mass;
+        double x_l = ref_l.state[0], xp_l = ref_l.state[1], y_l = ref_l.state[2], yp_l = ref_l.state[3];
+        double cdt_l = 0.0, dpop_l = 0.0;
+        double dphi = -(sp.angle - (sp.e1 + sp.e2));
+        std::complex<double> phase = std::exp(std::complex<double>(0.0, -dphi));
+        std::complex<double> term = std::complex<double>(0.0, sp.length / sp.angle) *
+                                    std::complex<double>(1.0 - std::cos(sp.angle), -std::sin(sp.angle)) *
+                                    std::complex<double>(std::cos(sp.e2), -std::sin(sp.e2));
+        if (sp.ledge) {
+            slot_unit(x_l, xp_l, y_l, yp_l, cdt_l, dpop_l, sp.ce1, sp.se1, pref_l, m_l);
+            double p_l = 1.0 + dpop_l;
+            double zp_l = std::sqrt(p_l * p_l - xp_l * xp_l - yp_l * yp_l);
+            sp.us_edge_k_x = sp.us_edge_k_p * (xp_l / zp_l);
+            sp.us_edge_k_y = sp.us_edge_k_p * (yp_l / zp_l);
+            edge_unit(y_l, xp_l, yp_l, sp.us_edge_k_x / sp.scale, sp.us_edge_k_y / sp.scale);
+        }
+        bend_complete(x_l, xp_l, y_l, yp_l, cdt_l, dpop_l, dphi, sp.strength, pref_l, m_l, 0.0, phase, term);
+        if (sp.redge) {
+            double p_l = 1.0 + dpop_l;
+            double zp_l = std::sqrt(p_l * p_l - xp_l * xp_l - yp_l * yp_l);
+            sp.ds_edge_k_x = sp.ds_edge_k_p * (xp_l / zp_l);
+            sp.ds_edge_k_y = sp.ds_edge_k_p * (yp_l / zp_l);
+            edge_unit(y_l, xp_l, yp_l, sp.ds_edge_k_x / sp.scale, sp.ds_edge_k_y / sp.scale);
+            slot_unit(x_l, xp_l, y_l, yp_l, cdt_l, dpop_l, sp.ce2, sp.se2, pref_l, m_l);
+        }
+        ref_l.state = {x_l, xp_l, y_l, yp_l, cdt_l, dpop_l};
+        sp.ref_cdt = cdt_l;
+    }
+
+    // PropSbendSimd ff_sbend.h:127-215
+    const double dphi = -(sp.angle - (sp.e1 + sp.e2));
+    const std::complex<double> phase = std::exp(std::complex<double>(0.0, -dphi));
+    const std::complex<double> term = std::complex<double>(0.0, sp.length / sp.angle) *
+                                      std::complex<double>(1.0 - std::cos(sp.angle), -std::sin(sp.angle)) *
+                                      std::complex<double>(std::cos(sp.e2), -std::sin(sp.e2));
+    if (b.n_valid) {
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < b.n_active; ++i) {
+            if (!b.masks[i]) continue;
+            double p0 = b.P(i, 0), p1 = b.P(i, 1), p2 = b.P(i, 2), p3 = b.P(i, 3), p4 = b.P(i, 4), p5 = b.P(i, 5);
+            if (sp.ledge) {
+                slot_unit(p0, p1, p2, p3, p4, p5, sp.ce1, sp.se1, sp.pref_b, sp.m_b);
+                edge_unit(p2, p1, p3, sp.us_edge_k_x, sp.us_edge_k_y);
+            }
+            bend_unit(p0, p1, p2, p3, p4, p5, dphi, sp.strength, sp.pref_b, sp.m_b, sp.ref_cdt, phase, term);
+            if (sp.redge) {
+                edge_unit(p2, p1, p3, sp.ds_edge_k_x, sp.ds_edge_k_y);
+                slot_unit(p0, p1, p2, p3, p4, p5, sp.ce2, sp.se2, sp.pref_b, sp.m_b);
+            }
+            b.P(i, 0) = p0; b.P(i, 1) = p1; b.P(i, 2) = p2; b.P(i, 3) = p3; b.P(i, 4) = p4; b.P(i, 5) = p5;
+        }
+    }
+    b.ref.s_n += sp.length;
+}
+
+static void multipole_apply(const Slice& slice, Bunch& b)
+{ // ff_multipole.h:85-210
+    if (slice.right - slice.left > 0.0)
+        throw std::runtime_error("FF_multipole::apply() cannot deal with thick elements");
+    const int max_order = 8;
+    bool kn_on[8] = {false};
+    double kl[16] = {0};
+    std::vector<double> knl, ksl, tn;
+    const Element& element = *slice.e;
+    if (element.v.count("knl") || element.v.count("ksl")) {
+        std::vector<double> k0(1, 0.0);
+        knl = element.v.count("knl") ? element.v.at("knl") : k0;
+        ksl = element.v.count("ksl") ? element.v.at("ksl") : k0;
+        if (knl.size() > ksl.size())
+            ksl.resize(knl.size(), 0.0);
+        else if (knl.size() < ksl.size())
+            knl.resize(ksl.size(), 0.0);
+        double tilt = element.get("tilt", 0.0);
+        tn.resize(knl.size(), tilt);
+    } else {
+        for (int i = 0; i < 6; ++i) {
+            std::string skn = "k0l", stn = "t0";
+            skn[1] = '0' + i;
+            stn[1] = '0' + i;
+            knl.push_back(element.get(skn, 0.0));
+            tn.push_back(element.get(stn, 0.0));
+        }
+        int tail = (int)knl.size() - 1;
+        while (tail && knl[tail] == 0.0) --tail;
+        knl.resize(tail + 1);
+        ksl.resize(knl.size(), 0.0);
+        tn.resize(knl.size(), 0.0);
+    }
+    if ((int)knl.size() > max_order) throw std::runtime_error("oracle: multipole order above 8");
+    for (size_t i = 0; i < knl.size(); ++i) {
+        if (tn[i] != 0.0) {
+            std::complex<double> ck2(knl[i], ksl[i]);
+            ck2 = ck2 * std::exp(std::complex<double>(0.0, -(double)(i + 1) * tn[i]));
+            knl[i] = ck2.real();
+            ksl[i] = ck2.imag();
+        }
+    }
+    Refpart& ref_l = b.design;
+    const Refpart& ref_b = b.ref;
+    double brho_l = ref_l.p / ref_l.charge;
+    double brho_b = ref_b.p * (1.0 + ref_b.state[5]) / ref_l.charge;
+    double scale = brho_l / brho_b;
+    for (size_t i = 0; i < knl.size(); ++i) {
+        knl[i] *= scale;
+        ksl[i] *= scale;
+    }
+    for (size_t i = 0; i < knl.size(); ++i) {
+        if (knl[i] || ksl[i]) kn_on[i] = true;
+        kl[i * 2 + 0] = knl[i];
+        kl[i * 2 + 1] = ksl[i];
+    }
+    double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3], dpop = ref_l.state[5];
+    for (int n = 0; n < max_order; ++n)
+        if (kn_on[n]) thin_magnet_unit(x, xp, y, yp, &kl[n * 2], n + 1);
+    ref_l.state = {x, xp, y, yp, 0.0, dpop};
+    if (b.n_valid) {
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < b.n_active; ++i) {
+            if (!b.masks[i]) continue;
+            double p0 = b.P(i, 0), p1 = b.P(i, 1), p2 = b.P(i, 2), p3 = b.P(i, 3);
+            if (kn_on[0]) thin_dipole_unit(p0, p1, p2, p3, &kl[0]);
+            if (kn_on[1]) thin_quadrupole_unit(p0, p1, p2, p3, &kl[2]);
+            if (kn_on[2]) thin_sextupole_unit(p0, p1, p2, p3, &kl[4]);
+            if (kn_on[3]) thin_octupole_unit(p0, p1, p2, p3, &kl[6]);
+            for (int n = 4; n < max_order; ++n)
+                if (kn_on[n]) thin_magnet_unit(p0, p1, p2, p3, &kl[n * 2], n + 1);
+            b.P(i, 1) = p1;
+            b.P(i, 3) = p3;
+        }
+    }
+}
+
+static void sextupole_apply(const Slice& slice, Bunch& b)
+{ // ff_sextupole.h:18-92 with ff_patterned_propagator.h
+    const Element& element = *slice.e;
+    double length = slice.right - slice.left;
+    double k[2] = {element.get("k2", 0.0), element.get("k2s", 0.0)};
+    double tilt = element.get("tilt", 0.0);
+    if (tilt != 0.0) {
+        std::complex<double> ck2(k[0], k[1]);
+        ck2 = ck2 * std::exp(std::complex<double>(0.0, -3.0 * tilt));
+        k[0] = ck2.real();
+        k[1] = ck2.imag();
+    }
+    Refpart& ref_l = b.design;
+    const Refpart& ref_b = b.ref;
+    double brho_l = ref_l.p / ref_l.charge;
+    double brho_b = ref_b.p * (1.0 + ref_b.state[5]) / ref_l.charge;
+    double scale = brho_l / brho_b;
+    k[0] *= scale;
+    k[1] *= scale;
+    if (close_to_zero(length)) {
+        // get_reference_cdt_zero ff_patterned_propagator.h:227-244
+        double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3];
+        double dpop = 0.0;
+        sext_kick(x, xp, y, yp, dpop, k);
+        ref_l.state[1] = xp;
+        ref_l.state[3] = yp;
+        ref_l.state[4] = 0.0;
+        if (b.n_valid) {
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < b.n_active; ++i)
+                if (b.masks[i]) thin_sextupole_unit(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), k);
+        }
+    } else {
+        double pref = b.ref.p, mass = b.ref.mass;
+        int steps = (int)element.get("yoshida_steps", 4.0);
+        // get_reference_cdt_yoshida ff_patterned_propagator.h:275-316
+        double cdt = 0.0;
+        auto st = ref_l.state;
+        st[5] = 0.0;
+        double step_len = length / steps;
+        double step_str[2] = {k[0] * step_len, k[1] * step_len};
+        yoshida_general(6, st[0], st[1], st[2], st[3], cdt, st[5], ref_l.p, ref_l.mass, 0.0, step_len, step_str, steps, sext_kick, 1);
+        st[4] = cdt;
+        ref_l.state = st;
+        double ref_cdt = cdt;
+        // apply_yoshida_kick ff_patterned_propagator.h:199-225
+        double step_ref_cdt = ref_cdt / steps;
+        double ss[2] = {k[0] * step_len, k[1] * step_len};
+        if (b.n_valid) {
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < b.n_active; ++i) {
+                if (!b.masks[i]) continue;
+                double p0 = b.P(i, 0), p1 = b.P(i, 1), p2 = b.P(i, 2), p3 = b.P(i, 3), p4 = b.P(i, 4), p5 = b.P(i, 5);
+                yoshida6(p0, p1, p2, p3, p4, p5, pref, mass, step_ref_cdt, step_len, ss, steps, sext_kick, 1);
+                b.P(i, 0) = p0; b.P(i, 1) = p1; b.P(i, 2) = p2; b.P(i, 3) = p3; b.P(i, 4) = p4;
+            }
+        }
+        b.ref.s_n += length;
+    }
+}
+
+static void element_apply(const Slice& slice, Bunch& b)
+{ // ff_element.h:25-67
+    const std::string& t = slice.e->type;
+    if (t == "drift" || t == "monitor" || t == "hmonitor" || t == "vmonitor" || t == "marker" ||
+        t == "instrument" || t == "rcollimator")
+        drift_apply(slice, b);
+    else if (t == "sbend")
+        sbend_apply(slice, b);
+    else if (t == "quadrupole")
+        quad_apply(slice, b);
+    else if (t == "multipole")
+        multipole_apply(slice, b);
+    else if (t == "sextupole")
+        sextupole_apply(slice, b);
+    else
+        throw std::runtime_error("FF_element::apply() unknown element type = " + t + ", element name = " + slice.e->name);
+}
+
+// ---------------------------------------------------------------------------
+// Apertures: simulation/aperture_operation.h, bunch_particles.h:484-524
+// ---------------------------------------------------------------------------
+enum { AP_FINITE = 0, AP_CIRCULAR = 1, AP_ELLIPTICAL = 2, AP_RECTANGULAR = 3 };
+
+struct Aperture {
+    int kind = AP_FINITE;
+    double r2 = 1e6, xoff = 0, yoff = 0, h2 = 1, v2 = 1, width = 0, height = 0;
+    const Element* elem = nullptr;
+};
+
+static Aperture make_aperture(const std::string& type, const Slice& slice)
+{ // operation_extractor.cc:55-75
+    Aperture ap;
+    const Element& ele = *slice.e;
+    ap.elem = &ele;
+    if (type == "finite") {
+        ap.kind = AP_FINITE;
+    } else if (type == "circular") {
+        ap.kind = AP_CIRCULAR;
+        ap.xoff = ele.get("hoffset", 0.0);
+        ap.yoff = ele.get("voffset", 0.0);
+        double r = ele.get("circular_aperture_radius", 1000.0);
+        ap.r2 = r * r;
+    } else if (type == "elliptical") {
+        ap.kind = AP_ELLIPTICAL;
+        ap.xoff = ele.get("hoffset", 0.0);
+        ap.yoff = ele.get("voffset", 0.0);
+        double hr = ele.get("elliptical_aperture_horizontal_radius");
+        double vr = ele.get("elliptical_aperture_vertical_radius");
+        ap.h2 = hr * hr;
+        ap.v2 = vr * vr;
+    } else if (type == "rectangular") {
+        ap.kind = AP_RECTANGULAR;
+        ap.width = ele.get("rectangular_aperture_width");
+        ap.height = ele.get("rectangular_aperture_height");
+        ap.xoff = ele.get("hoffset", 0.0);
+        ap.yoff = ele.get("voffset", 0.0);
+    } else {
+        throw std::runtime_error("unknown aperture_type " + type);
+    }
+    return ap;
+}
+
+static int aperture_apply(const Aperture& ap, Bunch& b)
+{
+    int nd = 0;
+#pragma omp parallel for reduction(+ : nd) schedule(static)
+    for (int64_t i = 0; i < b.n_active; ++i) {
+        b.discards[i] = 0;
+        if (!b.masks[i]) continue;
+        bool discard = false;
+        switch (ap.kind) {
+        case AP_FINITE: {
+            bool fin = true;
+            for (int j = 0; j < 6; ++j)
+                if (!std::isfinite(b.P(i, j))) fin = false;
+            if (!fin)
+                discard = true;
+            else {
+                double pt = 1.0 + b.P(i, 5), px = b.P(i, 1), py = b.P(i, 3);
+                discard = pt * pt - px * px - py * py < 0.0;
+            }
+            break;
+        }
+        case AP_CIRCULAR: {
+            double xr = b.P(i, 0) - ap.xoff, yr = b.P(i, 2) - ap.yoff;
+            discard = (xr * xr + yr * yr) > ap.r2;
+            break;
+        }
+        case AP_ELLIPTICAL: {
+            double xr = b.P(i, 0) - ap.xoff, yr = b.P(i, 2) - ap.yoff;
+            discard = (xr * xr / ap.h2 + yr * yr / ap.v2) > 1.0;
+            break;
+        }
+        case AP_RECTANGULAR: {
+            double xr = b.P(i, 0) - ap.xoff, yr = b.P(i, 2) - ap.yoff;
+            discard = (std::fabs(xr) > 0.5 * ap.width) || (std::fabs(yr) > 0.5 * ap.height);
+            break;
+        }
+        }
+        if (discard) {
+            b.discards[i] = 1;
+            b.masks[i] = 0;
+            ++nd;
+        }
+    }
+    b.n_valid -= nd;
+    return nd;
+}
+
+// ---------------------------------------------------------------------------
+// FFT (project-written; radix-2 iterative, direct DFT for other lengths).
+// Pinned against a direct DFT and numpy.fft by the tests.
+// ---------------------------------------------------------------------------
+typedef std::complex<double> cplx;
+
+static void fft1d(cplx* a, int n, int sign, std::vector<cplx>& scratch)
+{
+    if (n <= 1) return;
+    if ((n & (n - 1)) == 0) {
+        for (int i = 1, j = 0; i < n; ++i) {
+            int bit = n >> 1;
+            for (; j & bit; bit >>= 1) j ^= bit;
+            j ^= bit;
+            if (i < j) std::swap(a[i], a[j]);
+        }
+        for (int len = 2; len <= n; len <<= 1) {
+            double ang = sign * 2.0 * pc::pi / len;
+            for (int k = 0; k < len / 2; ++k) {
+                cplx w(std::cos(ang * k), std::sin(ang * k));
+                for (int i = 0; i < n; i += len) {
+                    cplx u = a[i + k], v = a[i + k + len / 2] * w;
+                    a[i + k] = u + v;
+                    a[i + k + len / 2] = u - v;
+                }
+            }
+        }
+    } else {
+        scratch.assign(a, a + n);
+        for (int k = 0; k < n; ++k) {
+            cplx s(0, 0);
+            for (int j = 0; j < n; ++j) {
+                double ang = sign * 2.0 * pc::pi * (double)((int64_t)j * k % n) / n;
+                s += scratch[j] * cplx(std::cos(ang), std::sin(ang));
+            }
+            a[k] = s;
+        }
+    }
+}
+
+// In-place 3D complex FFT of a (nz, ny, nx) array, x fastest.  sign=-1 is
+// forward (FFTW/cuFFT convention), unnormalised.
+static void fft3d(cplx* a, int nx, int ny, int nz, int sign)
+{
+#pragma omp parallel
+    {
+        std::vector<cplx> buf, scr;
+        buf.resize(std::max(nx, std::max(ny, nz)));
+#pragma omp for schedule(static)
+        for (int64_t r = 0; r < (int64_t)ny * nz; ++r) fft1d(a + r * nx, nx, sign, scr);
+#pragma omp for schedule(static)
+        for (int64_t r = 0; r < (int64_t)nx * nz; ++r) {
+            int64_t z = r / nx, x = r % nx;
+            for (int y = 0; y < ny; ++y) buf[y] = a[(z * ny + y) * nx + x];
+            fft1d(buf.data(), ny, sign, scr);
+            for (int y = 0; y < ny; ++y) a[(z * ny + y) * nx + x] = buf[y];
+        }
+#pragma omp for schedule(static)
+        for (int64_t r = 0; r < (int64_t)nx * ny; ++r) {
+            for (int z = 0; z < nz; ++z) buf[z] = a[z * (int64_t)nx * ny + r];
+            fft1d(buf.data(), nz, sign, scr);
+            for (int z = 0; z < nz; ++z) a[z * (int64_t)nx * ny + r] = buf[z];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Space_charge_3d_open_hockney (collective/space_charge_3d_open_hockney.cc)
+// ---------------------------------------------------------------------------
+struct SCOptions { // simulation/implemented_collective_options.h:67-126
+    int shape[3] = {32, 32, 64};
+    int doubled_shape[3] = {64, 64, 128};
+    double size[3] = {0, 0, 0};
+    double offset[3] = {0, 0, 0};
+    int green_fn = 1; // 0 pointlike, 1 linear
+    int periodic_z = 0;
+    double z_period = 0.0;
+    int grid_entire_period = 0;
+    double n_sigma = 8.0;
+    double kick_scale = 1.0;
+    int domain_fixed = 0;
+};
+
+struct Domain { // rectangular_grid_domain.h:20-36
+    int g[3];
+    double size[3], offset[3], left[3], h[3];
+    void set(const int* shape, const double* sz, const double* off)
+    {
+        for (int i = 0; i < 3; ++i) {
+            g[i] = shape[i];
+            size[i] = sz[i];
+            offset[i] = off[i];
+            left[i] = off[i] - sz[i] / 2.0;
+            h[i] = sz[i] / (1.0 * shape[i]);
+        }
+    }
+};
+
+static double smallest_non_tiny(double val, double o1, double o2, double tiny)
+{ // space_charge_3d_open_hockney.cc:94-109
+    if (val > tiny) return val;
+    if (o1 > tiny && o2 > tiny) return std::min(o1, o2);
+    return std::max(o1, o2);
+}
+
+// collective/utils.h:9-18
+inline void leftmost_index_offset(double pos, double left, double inv_cell, int& idx, double& off)
+{
+    double s = (pos - left) * inv_cell - 0.5;
+    idx = (int)std::floor(s);
+    off = s - idx;
+}
+
+struct SC3D {
+    SCOptions o;
+    Domain dom, ddom;
+    int ng = 0; // doubled grid points
+    std::vector<cplx> rho, gr, phi; // full complex doubled grids (z, y, x)
+    std::vector<double> enx, eny, enz, rho_real, phi_real;
+    double fn_norm = 0, last_factor = 0;
+    std::array<double, 6> last_mean_std{};
+
+    explicit SC3D(const SCOptions& opt) : o(opt)
+    {
+        double one[3] = {1, 1, 1}, zero[3] = {0, 0, 0};
+        dom.set(o.shape, one, zero);
+        ddom.set(o.doubled_shape, one, zero);
+        if (o.domain_fixed) {
+            double ds[3] = {o.size[0] * 2.0, o.size[1] * 2.0, o.size[2] * 2.0};
+            dom.set(o.shape, o.size, o.offset);
+            ddom.set(o.doubled_shape, ds, o.offset);
+        }
+        ng = o.doubled_shape[0] * o.doubled_shape[1] * o.doubled_shape[2];
+    }
+
+    void update_domain(Bunch& b)
+    { // :494-540 with core_diagnostics.cc:422-460
+        if (o.domain_fixed) return;
+        double s[6] = {0, 0, 0, 0, 0, 0};
+        for (int64_t i = 0; i < b.n_active; ++i)
+            if (b.masks[i]) {
+                double x = b.P(i, 0), y = b.P(i, 2), z = b.P(i, 4);
+                s[0] += x; s[1] += y; s[2] += z;
+                s[3] += x * x; s[4] += y * y; s[5] += z * z;
+            }
+        double ms[6];
+        for (int j = 0; j < 3; ++j) {
+            ms[j] = s[j] / b.n_total;
+            ms[j + 3] = std::sqrt(s[j + 3] / b.n_total - std::pow(ms[j], 2));
+        }
+        for (int j = 0; j < 6; ++j) last_mean_std[j] = ms[j];
+        const double tiny = 1.0e-10;
+        if (ms[3] < tiny && ms[4] < tiny && ms[5] < tiny)
+            throw std::runtime_error("Space_charge_3d_open_hockney_eigen::update_domain: all three spatial dimensions have neglible extent");
+        double off[3] = {ms[0], ms[1], ms[2]};
+        double sz[3] = {o.n_sigma * smallest_non_tiny(ms[3], ms[4], ms[5], tiny),
+                        o.n_sigma * smallest_non_tiny(ms[4], ms[3], ms[5], tiny),
+                        o.n_sigma * smallest_non_tiny(ms[5], ms[3], ms[4], tiny)};
+        if (o.grid_entire_period) {
+            off[2] = 0.0;
+            sz[2] = o.z_period;
+        }
+        double ds[3] = {sz[0] * 2.0, sz[1] * 2.0, sz[2] * 2.0};
+        dom.set(o.shape, sz, off);
+        ddom.set(o.doubled_shape, ds, off);
+    }
+
+    // deposit_charge_rectangular_3d_omp_reduce deposit.cc:853-1031, into a
+    // dense (gz, gy, gx) grid; edges excluded (deposit.cc:23-30)
+    void deposit(Bunch& b)
+    {
+        int gx = dom.g[0], gy = dom.g[1], gz = dom.g[2];
+        double w0 = (b.real_num / b.n_total) * b.ref.charge * pc::e / (dom.h[0] * dom.h[1] * dom.h[2]);
+        double lx = dom.left[0], ly = dom.left[1], lz = dom.left[2];
+        double ihx = 1.0 / dom.h[0], ihy = 1.0 / dom.h[1], ihz = 1.0 / dom.h[2];
+        int64_t nc = (int64_t)gx * gy * gz;
+        rho_real.assign(nc, 0.0);
+        int nt = 1;
+#ifdef _OPENMP
+        nt = omp_get_max_threads();
+#endif
+        std::vector<double> rl((size_t)nt * nc, 0.0);
+        auto ingrid = [&](int ix, int iy, int iz) {
+            return ix > 0 && ix < gx - 1 && iy > 0 && iy < gy - 1 && iz > 0 && iz < gz - 1;
+        };
+#pragma omp parallel num_threads(nt)
+        {
+            int it = 0, ntt = 1;
+#ifdef _OPENMP
+            it = omp_get_thread_num();
+            ntt = omp_get_num_threads();
+#endif
+            int64_t le = b.n_active / ntt;
+            int64_t ps = it * le, pe = (it == ntt - 1) ? b.n_active : (it + 1) * le;
+            double* r = rl.data() + (size_t)it * nc;
+            for (int64_t n = ps; n < pe; ++n) {
+                if (!b.masks[n]) continue;
+                int ix, iy, iz;
+                double ox, oy, oz;
+                leftmost_index_offset(b.P(n, 0), lx, ihx, ix, ox);
+                leftmost_index_offset(b.P(n, 2), ly, ihy, iy, oy);
+                leftmost_index_offset(b.P(n, 4), lz, ihz, iz, oz);
+                int64_t base = (int64_t)iz * gx * gy;
+                if (ingrid(ix, iy, iz)) r[base + iy * gx + ix] += w0 * (1 - ox) * (1 - oy) * (1 - oz);
+                if (ingrid(ix + 1, iy, iz)) r[base + iy * gx + ix + 1] += w0 * (ox) * (1 - oy) * (1 - oz);
+                if (ingrid(ix, iy + 1, iz)) r[base + (iy + 1) * gx + ix] += w0 * (1 - ox) * (oy) * (1 - oz);
+                if (ingrid(ix + 1, iy + 1, iz)) r[base + (iy + 1) * gx + ix + 1] += w0 * (ox) * (oy) * (1 - oz);
+                base = (int64_t)(iz + 1) * gx * gy;
+                if (ingrid(ix, iy, iz + 1)) r[base + iy * gx + ix] += w0 * (1 - ox) * (1 - oy) * (oz);
+                if (ingrid(ix + 1, iy, iz + 1)) r[base + iy * gx + ix + 1] += w0 * (ox) * (1 - oy) * (oz);
+                if (ingrid(ix, iy + 1, iz + 1)) r[base + (iy + 1) * gx + ix] += w0 * (1 - ox) * (oy) * (oz);
+                if (ingrid(ix + 1, iy + 1, iz + 1)) r[base + (iy + 1) * gx + ix + 1] += w0 * (ox) * (oy) * (oz);
+            }
+        }
+#pragma omp parallel for schedule(static)
+        for (int64_t c = 0; c < nc; ++c) {
+            double w = 0.0;
+            for (int n = 0; n < nt; ++n) w += rl[(size_t)n * nc + c];
+            rho_real[c] = w;
+        }
+    }
+
+    // alg_g2_linear :230-348 / alg_g2_pointlike :136-228 into a full complex
+    // (dgz, dgy, dgx) grid
+    void green(std::vector<cplx>& g2)
+    {
+        if (o.periodic_z)
+            throw std::runtime_error("Space_charge_3d_open_hockney::get_green_fn2: periodic_z not yet implemented");
+        const int dgx = ddom.g[0], dgy = ddom.g[1], dgz = ddom.g[2];
+        const double hx = ddom.h[0], hy = ddom.h[1], hz = ddom.h[2];
+        g2.assign(ng, cplx(0, 0));
+        auto at = [&](int z, int y, int x) -> cplx& { return g2[((int64_t)z * dgy + y) * dgx + x]; };
+        if (o.green_fn == 0) {
+            const int gx = dom.g[0] + 1, gy = dom.g[1] + 1, gz = dom.g[2] + 1;
+            double G000 = 2.8 / std::min(hx, std::min(hy, hz));
+            for (int iz = 0; iz < gz; ++iz)
+                for (int iy = 0; iy < gy; ++iy)
+                    for (int ix = 0; ix < gx; ++ix) {
+                        double dx = ix * hx, dy = iy * hy, dz = iz * hz;
+                        double G = (ix == 0 && iy == 0 && iz == 0) ? G000 : 1.0 / std::sqrt(dx * dx + dy * dy + dz * dz);
+                        int mix = dgx - ix; if (mix == dgx) mix = 0;
+                        int miy = dgy - iy; if (miy == dgy) miy = 0;
+                        int miz = dgz - iz; if (miz == dgz) miz = 0;
+                        at(iz, iy, ix) = G; at(iz, miy, ix) = G; at(iz, iy, mix) = G; at(iz, miy, mix) = G;
+                        at(miz, iy, ix) = G; at(miz, miy, ix) = G; at(miz, iy, mix) = G; at(miz, miy, mix) = G;
+                    }
+            return;
+        }
+        const int gx0 = dom.g[0], gy0 = dom.g[1], gz0 = dom.g[2];
+        double rr0 = hx * hx + hy * hy;
+        double r10 = std::sqrt(hx * hx + hy * hy + hz * hz);
+        double G000 = (2.0 / rr0) * (hz * r10 + rr0 * std::log((hz + r10) / std::sqrt(rr0)) - hz * hz);
+        const double epsz = 1e-12 * hz;
+        for (int iz = 0; iz < dgz; ++iz)
+            for (int iy = 0; iy <= gy0; ++iy)
+                for (int ix = 0; ix <= gx0; ++ix) {
+                    double z = (iz > gz0) ? (dgz - iz) * hz : iz * hz;
+                    double y = iy * hy, x = ix * hx;
+                    double rr = x * x + y * y;
+                    double s0 = std::sqrt(rr + z * z);
+                    double sn = std::sqrt(rr + (z - hz) * (z - hz));
+                    double sp = std::sqrt(rr + (z + hz) * (z + hz));
+                    double G = 2.0 * s0 - sn - sp;
+                    double T1, T2, r1, r2;
+                    if (z < -hz) {
+                        r1 = (sn - z + hz) / (s0 - z);
+                        T1 = (hz - z) * std::log(r1);
+                        r2 = (s0 - z) / (sp - z - hz);
+                        T2 = (hz + z) * std::log(r2);
+                        G += T1 + T2;
+                    } else if (std::abs(z + hz) < epsz) {
+                        r1 = (sn - z + hz) / (s0 - z);
+                        T1 = (hz - z) * std::log(r1);
+                        G += T1;
+                    } else if (std::abs(z) < epsz) {
+                        if (std::abs(x) + std::abs(y) < 2. * epsz) {
+                            G += hz * G000;
+                        } else {
+                            r1 = (std::sqrt(hz * hz + rr) + hz) / std::sqrt(rr);
+                            G += 2.0 * hz * std::log(r1);
+                        }
+                    } else if (std::abs(z - hz) < epsz) {
+                        r1 = (sp + z + hz) / (s0 + z);
+                        T1 = (hz + z) * std::log(r1);
+                        G += T1;
+                    } else if (z > hz) {
+                        r1 = (s0 + z) / (sn + z - hz);
+                        T1 = (hz - z) * std::log(r1);
+                        r2 = (sp + z + hz) / (s0 + z);
+                        T2 = (hz + z) * std::log(r2);
+                        G += T1 + T2;
+                    }
+                    int miy = dgy - iy, mix = dgx - ix;
+                    if (mix == dgx) mix = 0;
+                    if (miy == dgy) miy = 0;
+                    at(iz, iy, ix) = G;
+                    if (iy != gy0) {
+                        at(iz, miy, ix) = G;
+                        if (ix != gx0) at(iz, miy, mix) = G;
+                    }
+                    if (ix != gx0) at(iz, iy, mix) = G;
+                }
+    }
+
+    // get_local_phi2 :642-676, get_normalization_force :708-735,
+    // alg_force_extractor_doubled_domain space_charge_3d_kernels.h:217-307
+    void solve()
+    {
+        const int dgx = ddom.g[0], dgy = ddom.g[1], dgz = ddom.g[2];
+        const int gx = dom.g[0], gy = dom.g[1], gz = dom.g[2];
+        rho.assign(ng, cplx(0, 0));
+        for (int z = 0; z < gz; ++z)
+            for (int y = 0; y < gy; ++y)
+                for (int x = 0; x < gx; ++x)
+                    rho[((int64_t)z * dgy + y) * dgx + x] = rho_real[((int64_t)z * gy + y) * gx + x];
+        green(gr);
+        fft3d(rho.data(), dgx, dgy, dgz, -1);
+        fft3d(gr.data(), dgx, dgy, dgz, -1);
+        phi.resize(ng);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < ng; ++i) {
+            double ar = rho[i].real(), ai = rho[i].imag(), br = gr[i].real(), bi = gr[i].imag();
+            phi[i] = cplx(ar * br - ai * bi, ar * bi + ai * br);
+        }
+        fft3d(phi.data(), dgx, dgy, dgz, +1);
+        double hx = dom.h[0], hy = dom.h[1], hz = dom.h[2];
+        double norm = hx * hy * hz;
+        norm *= 1.0 / (4.0 * pc::pi * pc::epsilon0);
+        norm *= 1.0;
+        if (o.green_fn == 1) norm *= 1.0 / (hz * hz);
+        norm *= 1.0 / (dgx * dgy * dgz);
+        fn_norm = norm;
+        phi_real.assign((int64_t)gx * gy * gz, 0.0);
+        for (int z = 0; z < gz; ++z)
+            for (int y = 0; y < gy; ++y)
+                for (int x = 0; x < gx; ++x)
+                    phi_real[((int64_t)z * gy + y) * gx + x] = phi[((int64_t)z * dgy + y) * dgx + x].real();
+        int64_t G = (int64_t)gx * gy * gz;
+        enx.assign(G, 0.0);
+        eny.assign(G, 0.0);
+        enz.assign(G, 0.0);
+        double ihx = 0.5 / ddom.h[0], ihy = 0.5 / ddom.h[1], ihz = 0.5 / ddom.h[2];
+        auto ph = [&](int z, int y, int x) { return phi[((int64_t)z * dgy + y) * dgx + x].real(); };
+#pragma omp parallel for schedule(static)
+        for (int iz = 1; iz < gz - 1; ++iz)
+            for (int iy = 1; iy < gy - 1; ++iy)
+                for (int ix = 1; ix < gx - 1; ++ix) {
+                    int64_t i = ((int64_t)iz * gy + iy) * gx + ix;
+                    enx[i] = -(ph(iz, iy, ix + 1) - ph(iz, iy, ix - 1)) * ihx;
+                    eny[i] = -(ph(iz, iy + 1, ix) - ph(iz, iy - 1, ix)) * ihy;
+                    enz[i] = -(ph(iz + 1, iy, ix) - ph(iz - 1, iy, ix)) * ihz;
+                }
+    }
+
+    // apply_kick :753-784 + zyx::alg_kicker space_charge_3d_kernels.h:91-215
+    void kick(Bunch& b, double time_step)
+    {
+        double q = b.ref.charge * pc::e;
+        double m = b.ref.mass;
+        double gamma = b.ref.gamma, beta = b.ref.beta, pref = b.ref.p;
+        double unit_conversion = pc::c / (1e9 * pc::e);
+        double factor = o.kick_scale * unit_conversion * q * time_step * fn_norm / (pref * gamma * gamma * beta);
+        last_factor = factor;
+        const int gx = dom.g[0], gy = dom.g[1], gz = dom.g[2];
+        double ihx = 1.0 / dom.h[0], ihy = 1.0 / dom.h[1], ihz = 1.0 / dom.h[2];
+        double lx = dom.left[0], ly = dom.left[1], lz = dom.left[2];
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < b.n_active; ++i) {
+            if (!b.masks[i]) continue;
+            int ix, iy, iz;
+            double ox, oy, oz;
+            leftmost_index_offset(b.P(i, 0), lx, ihx, ix, ox);
+            leftmost_index_offset(b.P(i, 2), ly, ihy, iy, oy);
+            leftmost_index_offset(b.P(i, 4), lz, ihz, iz, oz);
+            double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
+            if (!((ix >= 0 && ix < gx - 1) && (iy >= 0 && iy < gy - 1) && (iz >= 0 && iz < gz - 1))) continue;
+            auto interp = [&](const std::vector<double>& e) {
+                int64_t base = ((int64_t)iz * gy + iy) * gx + ix;
+                double val = aoz * aoy * aox * e[base];
+                val += aoz * aoy * ox * e[base + 1];
+                val += aoz * oy * aox * e[base + gx];
+                val += aoz * oy * ox * e[base + gx + 1];
+                base = ((int64_t)(iz + 1) * gy + iy) * gx + ix;
+                val += oz * aoy * aox * e[base];
+                val += oz * aoy * ox * e[base + 1];
+                val += oz * oy * aox * e[base + gx];
+                val += oz * oy * ox * e[base + gx + 1];
+                return val;
+            };
+            double val = interp(enz);
+            double p = pref + b.P(i, 5) * pref;
+            double Eoc_i = std::sqrt(p * p + m * m);
+            double Eoc_f = Eoc_i + factor * (-pref) * val;
+            double dpop = (std::sqrt(Eoc_f * Eoc_f - m * m) - std::sqrt(Eoc_i * Eoc_i - m * m)) / pref;
+            b.P(i, 5) += dpop;
+            val = interp(eny);
+            b.P(i, 3) += factor * val;
+            val = interp(enx);
+            b.P(i, 1) += factor * val;
+        }
+    }
+
+    void apply(Bunch& b, double time_step)
+    { // apply_bunch :423-453
+        if (!o.domain_fixed) update_domain(b);
+        deposit(b);
+        solve();
+        kick(b, time_step);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Steps and operators: split_operator_stepper.cc, independent_operator.cc,
+// independent_stepper_elements.cc, split_operator_stepper_elements.cc, step.cc
+// ---------------------------------------------------------------------------
+struct IndepOp {
+    std::vector<Slice> slices;
+    // operations: 'L' = libff group, 'A' = aperture
+    struct Opn {
+        char kind;
+        std::vector<Slice> group;
+        Aperture ap;
+    };
+    std::vector<Opn> ops;
+
+    void create_operations()
+    { // independent_operator.cc:25-91
+        ops.clear();
+        std::string aperture_type;
+        bool need_left = false, need_right = false;
+        std::string extractor_type, last_extractor_type;
+        std::vector<Slice> group;
+        for (auto const& slice : slices) {
+            const Element& el = *slice.e;
+            if (el.has_s("aperture_type")) {
+                aperture_type = el.gets("aperture_type", "");
+                need_left = slice.ledge;
+                need_right = slice.redge;
+            } else {
+                need_left = need_right = false;
+            }
+            extractor_type = el.gets("extractor_type", "default");
+            if (extractor_type != "default" && extractor_type != "libff")
+                throw std::runtime_error("unknown extractor_type: " + extractor_type);
+            if (((extractor_type != last_extractor_type) || need_left) && !group.empty()) {
+                ops.push_back({'L', group, {}});
+                group.clear();
+            }
+            if (need_left) ops.push_back({'A', {}, make_aperture(aperture_type, slice)});
+            group.push_back(slice);
+            last_extractor_type = extractor_type;
+            if (need_right) {
+                ops.push_back({'L', group, {}});
+                ops.push_back({'A', {}, make_aperture(aperture_type, slice)});
+                group.clear();
+            }
+        }
+        if (!group.empty()) ops.push_back({'L', group, {}});
+        ops.push_back({'A', {}, make_aperture("finite", slices.back())});
+        ops.push_back({'A', {}, make_aperture("circular", slices.back())});
+    }
+
+    void apply(Bunch& b, std::vector<int64_t>& lost_per_step)
+    {
+        for (auto& op : ops) {
+            if (op.kind == 'L') {
+                for (auto& s : op.group) element_apply(s, b);
+            } else {
+                int nd = aperture_apply(op.ap, b);
+                lost_per_step.push_back(nd);
+            }
+        }
+        b.update_total_num();
+    }
+};
+
+struct Step {
+    double length = 0;
+    // sequence of operators: 'I' independent, 'C' collective
+    std::vector<char> kinds;
+    std::vector<IndepOp> indeps;
+};
+
+template <typename IT>
+static std::vector<Slice> fixed_step_slices(IT& it, const IT& end, double& left, double step_length,
+                                            double& offset_fudge)
+{ // split_operator_stepper.cc:14-82 (force_diagnostics not supported)
+    const double tol = 1.0e-8;
+    std::vector<Slice> slices;
+    double length = offset_fudge;
+    bool complete = false;
+    while (!complete) {
+        double right = it->length();
+        if (length + (right - left) - tol <= step_length) {
+            Slice slice(*it, left, right);
+            slices.push_back(slice);
+            length += (right - left);
+            ++it;
+            left = 0.0;
+            if (std::abs(length - step_length) < tol) {
+                if ((it == end) || (it->length() != 0.0)) complete = true;
+            } else {
+                if (it == end) throw std::runtime_error("get_step stepped beyond end of lattice");
+            }
+        } else {
+            bool end_within_error = false;
+            double old_right = right;
+            right = step_length - length + left;
+            if (std::abs(old_right - right) < tol) {
+                right = old_right;
+                end_within_error = true;
+            }
+            Slice slice(*it, left, right);
+            slices.push_back(slice);
+            length += (right - left);
+            if (end_within_error) {
+                ++it;
+                left = 0.0;
+            } else {
+                left = right;
+            }
+            complete = true;
+        }
+    }
+    offset_fudge = length - step_length;
+    return slices;
+}
+
+enum { STEPPER_SPLIT = 0, STEPPER_SPLIT_ELEMENTS = 1, STEPPER_INDEP_ELEMENTS = 2 };
+
+static std::vector<Step> make_steps(const Lattice& lat, int kind, int num, bool has_collective)
+{
+    std::vector<Step> steps;
+    auto add_indep = [](Step& st, std::vector<Slice> sl) {
+        IndepOp op;
+        op.slices = std::move(sl);
+        op.create_operations();
+        st.kinds.push_back('I');
+        st.indeps.push_back(std::move(op));
+    };
+    if (kind == STEPPER_SPLIT) {
+        // split_operator_stepper.cc:132-261 (no force_diagnostics)
+        double step_length = lat.length() / num;
+        double half = 0.5 * step_length;
+        auto it = lat.elements.begin();
+        auto end = lat.elements.end();
+        if (it == end) return steps;
+        double left = 0.0, fudge = 0.0;
+        for (int i = 0; i < num; ++i) {
+            auto s1 = fixed_step_slices(it, end, left, half, fudge);
+            auto s2 = fixed_step_slices(it, end, left, half, fudge);
+            Step st;
+            st.length = step_length;
+            add_indep(st, s1);
+            if (has_collective) st.kinds.push_back('C');
+            add_indep(st, s2);
+            steps.push_back(std::move(st));
+        }
+        if (it != end)
+            throw std::runtime_error("internal error: split_operator_stepper did not make it to the end of the lattice\n");
+    } else {
+        if (num < 1) throw std::runtime_error("Split_operator_stepper_elements: steps_per_element must be >= 1");
+        for (auto const& ele : lat.elements) {
+            double length = ele.length();
+            if (length == 0.0) {
+                Step st;
+                st.length = 0.0;
+                add_indep(st, {Slice(ele)});
+                steps.push_back(std::move(st));
+                continue;
+            }
+            double sl = length / num;
+            for (int i = 0; i < num; ++i) {
+                double left = i * sl, right = (i + 1) * sl;
+                Step st;
+                st.length = sl;
+                if (kind == STEPPER_INDEP_ELEMENTS) {
+                    add_indep(st, {Slice(ele, left, right)});
+                } else {
+                    double middle = left + 0.5 * sl;
+                    add_indep(st, {Slice(ele, left, middle)});
+                    if (has_collective) st.kinds.push_back('C');
+                    add_indep(st, {Slice(ele, middle, right)});
+                }
+                steps.push_back(std::move(st));
+            }
+        }
+    }
+    return steps;
+}
+
+struct Sim {
+    Lattice lat;
+    Bunch b;
+    std::vector<Step> steps;
+    std::unique_ptr<SC3D> sc;
+    bool started = false;
+    std::vector<int64_t> losses;
+
+    void propagate(int turns)
+    { // propagator.cc:157-283 (single bunch, no diagnostics)
+        if (!started) {
+            b.design = lat.ref; // do_before_start: set_lattice_reference_particle
+            started = true;
+        }
+        for (int t = 0; t < turns; ++t) {
+            b.ref.s_n = 0.0;
+            for (auto& st : steps) {
+                if (b.n_active == 0) throw std::runtime_error("Step::apply() unable to proceed. no bunch in the simulator");
+                double time = st.length / (b.ref.beta * pc::c); // step.cc:44-53
+                size_t ii = 0;
+                for (char k : st.kinds) {
+                    if (k == 'I')
+                        st.indeps[ii++].apply(b, losses);
+                    else if (sc)
+                        sc->apply(b, time * 1.0);
+                }
+            }
+        }
+    }
+};
+
+} // namespace orc
+
+// ===========================================================================
+// C API used by the tests (ctypes)
+// ===========================================================================
+using namespace orc;
+
+#define ORC_TRY try {
+#define ORC_CATCH                                                                                  \
+    }                                                                                              \
+    catch (std::exception & ex)                                                                    \
+    {                                                                                              \
+        g_err = ex.what();                                                                         \
+        return 1;                                                                                  \
+    }                                                                                              \
+    return 0;
+
+extern "C" {
+
+const char* orc_last_error() { return g_err.c_str(); }
+
+int orc_set_threads(int n)
+{
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+// Reference particle given as (charge, mass, value, kind) with kind 0 =
+// total energy, 1 = momentum, 2 = kinetic energy [GeV].
+void* orc_lattice_new(int charge, double mass, double value, int kind)
+{
+    auto* L = new Lattice();
+    L->ref.charge = charge;
+    L->ref.mass = mass;
+    L->ref.set_by(kind, value);
+    return L;
+}
+void orc_lattice_free(void* l) { delete (Lattice*)l; }
+int orc_lattice_append(void* l, const char* type, const char* name)
+{
+    auto* L = (Lattice*)l;
+    Element e;
+    e.type = type;
+    e.name = name;
+    L->elements.push_back(e);
+    return (int)L->elements.size() - 1;
+}
+void orc_lattice_set_double(void* l, int idx, const char* k, double v) { ((Lattice*)l)->elements[idx].d[k] = v; }
+void orc_lattice_set_string(void* l, int idx, const char* k, const char* v) { ((Lattice*)l)->elements[idx].s[k] = v; }
+void orc_lattice_set_vector(void* l, int idx, const char* k, const double* v, int n)
+{
+    ((Lattice*)l)->elements[idx].v[k] = std::vector<double>(v, v + n);
+}
+double orc_lattice_length(void* l) { return ((Lattice*)l)->length(); }
+
+// Bunch reference particle given by (charge, mass, value, kind) as for
+// orc_lattice_new; sc_opts may be NULL (no collective operator).
+int orc_sim_new(void* lattice, int stepper_kind, int num, const SCOptions* sc_opts, int charge,
+                double mass, double value, int kind, int64_t n, double real_num, void** out)
+{
+    ORC_TRY
+    auto* s = new Sim();
+    s->lat = *(Lattice*)lattice;
+    s->b.ref.charge = charge;
+    s->b.ref.mass = mass;
+    s->b.ref.set_by(kind, value);
+    s->b.n_active = s->b.n_valid = s->b.n_total = (int)n;
+    s->b.cap = n;
+    s->b.real_num = real_num;
+    s->b.parts.assign(7 * n, 0.0);
+    for (int64_t i = 0; i < n; ++i) s->b.P(i, 6) = (double)i;
+    s->b.masks.assign(n, 1);
+    s->b.discards.assign(n, 0);
+    if (sc_opts) s->sc.reset(new SC3D(*sc_opts));
+    s->steps = make_steps(s->lat, stepper_kind, num, sc_opts != nullptr);
+    *out = s;
+    ORC_CATCH
+}
+void orc_sim_free(void* s) { delete (Sim*)s; }
+int orc_sim_num_steps(void* s) { return (int)((Sim*)s)->steps.size(); }
+
+// Step structure: returns per step the list of slices (element index, left,
+// right) so the tests can compare slicing with the product.
+int orc_sim_step_slices(void* sp, int step, int op, double* out, int cap)
+{
+    auto* s = (Sim*)sp;
+    auto& st = s->steps[step];
+    if (op >= (int)st.indeps.size()) return -1;
+    auto& sl = st.indeps[op].slices;
+    int n = 0;
+    for (auto& x : sl) {
+        if (n >= cap) break;
+        out[n * 3 + 0] = (double)(x.e - s->lat.elements.data());
+        out[n * 3 + 1] = x.left;
+        out[n * 3 + 2] = x.right;
+        ++n;
+    }
+    return n;
+}
+
+int orc_sim_set_particles(void* sp, const double* parts, const uint8_t* masks)
+{
+    auto* s = (Sim*)sp;
+    auto& b = s->b;
+    std::memcpy(b.parts.data(), parts, sizeof(double) * 7 * b.cap);
+    int nv = 0;
+    for (int64_t i = 0; i < b.n_active; ++i) {
+        b.masks[i] = masks ? masks[i] : 1;
+        nv += b.masks[i] ? 1 : 0;
+    }
+    b.n_valid = b.n_total = nv;
+    return 0;
+}
+int orc_sim_get_particles(void* sp, double* parts, uint8_t* masks, uint8_t* discards)
+{
+    auto* s = (Sim*)sp;
+    auto& b = s->b;
+    std::memcpy(parts, b.parts.data(), sizeof(double) * 7 * b.cap);
+    if (masks) std::memcpy(masks, b.masks.data(), b.n_active);
+    if (discards) std::memcpy(discards, b.discards.data(), b.n_active);
+    return 0;
+}
+int orc_sim_counts(void* sp, int* n_valid, int* n_total, double* real_num)
+{
+    auto* s = (Sim*)sp;
+    *n_valid = s->b.n_valid;
+    *n_total = s->b.n_total;
+    *real_num = s->b.real_num;
+    return 0;
+}
+int orc_sim_design_state(void* sp, double* state6, double* s_n)
+{
+    auto* s = (Sim*)sp;
+    for (int i = 0; i < 6; ++i) state6[i] = s->b.design.state[i];
+    *s_n = s->b.ref.s_n;
+    return 0;
+}
+int orc_sim_propagate(void* sp, int turns)
+{
+    ORC_TRY((Sim*)sp)->propagate(turns);
+    ORC_CATCH
+}
+int orc_sim_propagate_steps(void* sp, int first, int count)
+{ // partial turn (bench CPU sample): steps [first, first+count)
+    ORC_TRY
+    auto* s = (Sim*)sp;
+    if (!s->started) {
+        s->b.design = s->lat.ref;
+        s->started = true;
+    }
+    for (int k = first; k < first + count; ++k) {
+        auto& st = s->steps[k % s->steps.size()];
+        double time = st.length / (s->b.ref.beta * pc::c);
+        size_t ii = 0;
+        for (char kk : st.kinds) {
+            if (kk == 'I')
+                st.indeps[ii++].apply(s->b, s->losses);
+            else if (s->sc)
+                s->sc->apply(s->b, time);
+        }
+    }
+    ORC_CATCH
+}
+
+// Last space-charge solve of a Sim: domain (left[3], h[3]), rho, phi and E on
+// the original grid (gz, gy, gx), and fn_norm / kick factor.
+int orc_sim_sc_last(void* sp, double* left, double* h, double* rho, double* phi, double* ex, double* ey,
+                    double* ez, double* scalars)
+{
+    auto* s = (Sim*)sp;
+    if (!s->sc) return 1;
+    auto& sc = *s->sc;
+    for (int i = 0; i < 3; ++i) {
+        left[i] = sc.dom.left[i];
+        h[i] = sc.dom.h[i];
+    }
+    size_t G = sc.rho_real.size();
+    if (rho) std::memcpy(rho, sc.rho_real.data(), G * 8);
+    if (phi) std::memcpy(phi, sc.phi_real.data(), G * 8);
+    if (ex) std::memcpy(ex, sc.enx.data(), G * 8);
+    if (ey) std::memcpy(ey, sc.eny.data(), G * 8);
+    if (ez) std::memcpy(ez, sc.enz.data(), G * 8);
+    if (scalars) {
+        scalars[0] = sc.fn_norm;
+        scalars[1] = sc.last_factor;
+        for (int j = 0; j < 6; ++j) scalars[2 + j] = sc.last_mean_std[j];
+    }
+    return 0;
+}
+
+// One standalone space-charge kick on host particle arrays (the collective
+// operator alone, as the reference's own SC tests drive it).
+int orc_sc_apply(const SCOptions* opts, int charge, double mass, double value, int kind, int64_t n,
+                 double real_num, int n_total, double* parts, const uint8_t* masks, double time_step,
+                 double* left, double* h, double* rho, double* phi, double* ex, double* ey, double* ez,
+                 double* scalars)
+{
+    ORC_TRY
+    Bunch b;
+    b.ref.charge = charge;
+    b.ref.mass = mass;
+    b.ref.set_by(kind, value);
+    b.n_active = (int)n;
+    b.cap = n;
+    b.parts.assign(parts, parts + 7 * n);
+    b.masks.assign(n, 1);
+    int nv = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (masks) b.masks[i] = masks[i];
+        nv += b.masks[i] ? 1 : 0;
+    }
+    b.n_valid = nv;
+    b.n_total = n_total > 0 ? n_total : nv;
+    b.real_num = real_num;
+    SC3D sc(*opts);
+    sc.apply(b, time_step);
+    std::memcpy(parts, b.parts.data(), sizeof(double) * 7 * n);
+    for (int i = 0; i < 3; ++i) {
+        left[i] = sc.dom.left[i];
+        h[i] = sc.dom.h[i];
+    }
+    size_t G = sc.rho_real.size();
+    if (rho) std::memcpy(rho, sc.rho_real.data(), G * 8);
+    if (phi) std::memcpy(phi, sc.phi_real.data(), G * 8);
+    if (ex) std::memcpy(ex, sc.enx.data(), G * 8);
+    if (ey) std::memcpy(ey, sc.eny.data(), G * 8);
+    if (ez) std::memcpy(ez, sc.enz.data(), G * 8);
+    if (scalars) {
+        scalars[0] = sc.fn_norm;
+        scalars[1] = sc.last_factor;
+        for (int j = 0; j < 6; ++j) scalars[2 + j] = sc.last_mean_std[j];
+    }
+    ORC_CATCH
+}
+
+// Deposit alone into a dense (gz, gy, gx) grid for a given domain.
+int orc_deposit(const int* shape, const double* size, const double* offset, int charge, double real_num,
+                int n_total, int64_t n, const double* parts, const uint8_t* masks, double* rho_out)
+{
+    ORC_TRY
+    SCOptions o;
+    for (int i = 0; i < 3; ++i) {
+        o.shape[i] = shape[i];
+        o.doubled_shape[i] = 2 * shape[i];
+        o.size[i] = size[i];
+        o.offset[i] = offset[i];
+    }
+    o.domain_fixed = 1;
+    SC3D sc(o);
+    Bunch b;
+    b.ref.charge = charge;
+    b.n_active = (int)n;
+    b.cap = n;
+    b.parts.assign(parts, parts + 7 * n);
+    b.masks.assign(n, 1);
+    if (masks) std::memcpy(b.masks.data(), masks, n);
+    b.n_total = n_total;
+    b.real_num = real_num;
+    sc.deposit(b);
+    std::memcpy(rho_out, sc.rho_real.data(), sc.rho_real.size() * 8);
+    ORC_CATCH
+}
+
+// The oracle FFT on a (nz, ny, nx) complex array (interleaved re/im).
+int orc_fft3d(double* data, int nx, int ny, int nz, int sign)
+{
+    fft3d((cplx*)data, nx, ny, nz, sign);
+    return 0;
+}
+
+// Green function on the full doubled grid (real part), for a given domain.
+int orc_green(const int* shape, const int* dshape, const double* size, int green_fn, double* out)
+{
+    ORC_TRY
+    SCOptions o;
+    for (int i = 0; i < 3; ++i) {
+        o.shape[i] = shape[i];
+        o.doubled_shape[i] = dshape[i];
+        o.size[i] = size[i];
+        o.offset[i] = 0;
+    }
+    o.green_fn = green_fn;
+    o.domain_fixed = 1;
+    SC3D sc(o);
+    std::vector<cplx> g;
+    sc.green(g);
+    for (size_t i = 0; i < g.size(); ++i) out[i] = g[i].real();
+    ORC_CATCH
+}
+
+} // extern "C"
