@@ -1,0 +1,224 @@
+/*
+ * sb2.h — C ABI of the B200-native Synergia space-charge + tracking step.
+ *
+ * Every entry point takes plain pointers and sizes.  Particle storage follows
+ * the reference Bunch contract: an N x 7 FP64 column-major array (columns x,
+ * xp, y, yp, cdt, dpop, id; column stride = capacity) plus a uint8 mask per
+ * particle (1 = alive); lost particles are never compacted.
+ *
+ * Reference interfaces replaced (paths inside the synergia2 project):
+ *   Space_charge_3d_open_hockney_options  simulation/implemented_collective_options.h:67-126
+ *   Space_charge_3d_open_hockney::apply_impl / apply_bunch
+ *                                         collective/space_charge_3d_open_hockney.cc:400-453
+ *   FF_element::apply(slice, bunch)       libFF/ff_element.h:25-67
+ *   LibFF_operation::apply_impl           simulation/independent_operation.h:45-60
+ *   Aperture_operation<AP>::apply_impl    simulation/aperture_operation.h:14-24
+ *   Bunch::apply_aperture                 bunch/bunch.h:727-740
+ *   Split_operator_stepper::apply_impl    simulation/split_operator_stepper.cc:132-261
+ *   Split_operator_stepper_elements       simulation/split_operator_stepper_elements.cc:4-47
+ *   Independent_stepper_elements          simulation/independent_stepper_elements.cc:3-36
+ *   Propagator::propagate                 simulation/propagator.cc:157-283
+ *   Core_diagnostics::calculate_mom2      bunch/core_diagnostics.cc:351-365
+ *   calculate_emittances                  bunch/diagnostics_full2_host.cc
+ *
+ * Errors: every call returns an sb2_status; sb2_last_error() returns the
+ * message of the last failure on the calling thread (the text the reference
+ * throws as std::runtime_error where one exists).
+ */
+#ifndef SB2_H_
+#define SB2_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t sb2_status;
+enum {
+    SB2_OK = 0,
+    SB2_ERR_INVALID = 1,     /* bad argument / option */
+    SB2_ERR_CUDA = 2,        /* CUDA runtime failure */
+    SB2_ERR_RUNTIME = 3,     /* runtime_error raised by the physics (e.g. degenerate domain) */
+    SB2_ERR_UNSUPPORTED = 4, /* valid in the reference, not supported by this build */
+    SB2_ERR_NOMEM = 5        /* device allocation failed */
+};
+
+/* Message of the last failing call on this thread. */
+const char* sb2_last_error(void);
+/* Library version string. */
+const char* sb2_version(void);
+
+/* Per-category device timing of the library's own launches, measured with
+ * CUDA events recorded on the launching stream (the reference's
+ * scoped_simple_timer regions, utils/simple_timer.h:50-66).  Categories:
+ * 0 track (fused particle passes), 1 domain (bookkeeping + domain),
+ * 2 deposit, 3 green (Green-function transform), 4 solve (FFT
+ * convolution), 5 efield.  Off by default. */
+sb2_status sb2_profile_enable(int32_t on);
+sb2_status sb2_profile_read(int32_t category, const char** name, double* total_ms, int64_t* launches,
+                            int32_t reset);
+
+/* ---------------------------------------------------------------------
+ * Options of the 3D open-boundary Hockney solver.
+ * Replaces Space_charge_3d_open_hockney_options
+ * (simulation/implemented_collective_options.h:67-126).
+ * ------------------------------------------------------------------- */
+enum { SB2_GREEN_POINTLIKE = 0, SB2_GREEN_LINEAR = 1 };
+enum { SB2_PRECISION_FP64 = 0, SB2_PRECISION_MIXED = 1 };
+
+typedef struct sb2_sc3d_options {
+    int32_t shape[3];         /* grid (gx, gy, gz) */
+    int32_t doubled_shape[3]; /* doubled grid; must be 2*shape */
+    double size[3];           /* fixed-domain size [m, m, m(cdt)] */
+    double offset[3];         /* fixed-domain offset */
+    int32_t green_fn;         /* SB2_GREEN_* (default linear) */
+    int32_t periodic_z;       /* not implemented in the reference (throws) */
+    double z_period;
+    int32_t grid_entire_period;
+    double n_sigma;           /* adaptive domain size in sigmas (default 8) */
+    double kick_scale;        /* default 1 */
+    int32_t domain_fixed;     /* 1 after set_fixed_domain */
+    int32_t comm_group_size;  /* accepted for API parity; single GPU */
+    int32_t precision;        /* SB2_PRECISION_FP64 (drop-in) or _MIXED */
+} sb2_sc3d_options;
+
+/* Space_charge_3d_open_hockney_options(gridx, gridy, gridz) defaults. */
+sb2_status sb2_sc3d_options_init(sb2_sc3d_options* opts, int gx, int gy, int gz);
+/* Space_charge_3d_open_hockney_options::set_fixed_domain. */
+sb2_status sb2_sc3d_options_set_fixed_domain(sb2_sc3d_options* opts, const double offset[3],
+                                             const double size[3]);
+
+/* ---------------------------------------------------------------------
+ * Bunch: device-resident particles.  Replaces Bunch / bunch_particles_t
+ * (bunch/bunch.h, bunch/bunch_particles.h:24-205).
+ * ------------------------------------------------------------------- */
+typedef struct sb2_bunch sb2_bunch;
+
+/* Reference particle given as (charge [e], mass [GeV], value [GeV], kind):
+ * kind 0 = total energy, 1 = momentum, 2 = kinetic energy. */
+enum { SB2_REF_TOTAL_ENERGY = 0, SB2_REF_MOMENTUM = 1, SB2_REF_KINETIC_ENERGY = 2 };
+
+/* Bunch(ref, total_num, real_num): allocates capacity = n particles on the
+ * current device, ids 0..n-1, all masks 1, coordinates 0. */
+sb2_status sb2_bunch_create(int32_t charge, double mass, double value, int32_t kind, int64_t n,
+                            double real_num, sb2_bunch** out);
+/* Borrow caller-owned device memory (no copy, no ownership): parts is N x 7
+ * column-major with column stride `stride`, masks N bytes, discards N bytes
+ * (may be NULL). */
+sb2_status sb2_bunch_wrap(int32_t charge, double mass, double value, int32_t kind, double* parts,
+                          int64_t stride, uint8_t* masks, uint8_t* discards, int64_t n,
+                          double real_num, sb2_bunch** out);
+sb2_status sb2_bunch_destroy(sb2_bunch* b);
+/* checkin_particles: host N x 7 column-major (stride n) -> device; masks may
+ * be NULL (all alive).  Recounts valid particles. */
+sb2_status sb2_bunch_set_particles(sb2_bunch* b, const double* host_parts, const uint8_t* host_masks);
+/* checkout_particles: device -> host; any output may be NULL. */
+sb2_status sb2_bunch_get_particles(sb2_bunch* b, double* host_parts, uint8_t* host_masks,
+                                   uint8_t* host_discards);
+/* Device pointers of the bunch (for zero-copy callers). */
+sb2_status sb2_bunch_device_arrays(sb2_bunch* b, double** parts, int64_t* stride, uint8_t** masks,
+                                   uint8_t** discards);
+/* n_active (size), n_valid (local_num), n_total, real_num. */
+sb2_status sb2_bunch_counts(sb2_bunch* b, int64_t* n_active, int64_t* n_valid, int64_t* n_total,
+                            double* real_num);
+/* State [x, xp, y, yp, cdt, dpop] of the design reference particle and
+ * s_n of the bunch reference particle. */
+sb2_status sb2_bunch_design_state(sb2_bunch* b, double state[6], double* s_n);
+/* Synthetic seeded 6D uncorrelated Gaussian on the device (zero means;
+ * sigmas for x, xp, y, yp, cdt, dpop); counter-based generator, ids 0..n-1. */
+sb2_status sb2_bunch_populate_gaussian(sb2_bunch* b, const double sigma[6], uint64_t seed);
+/* Core_diagnostics::calculate_mean and calculate_mom2 (6 + 36 values,
+ * divided by n_total) and the rms emittances sqrt(det 2x2) of the x, y, z
+ * planes (diagnostics_full2_host.cc). */
+sb2_status sb2_bunch_moments(sb2_bunch* b, double mean[6], double mom2[36], double emit[3]);
+
+/* ---------------------------------------------------------------------
+ * Lattice: element list with attributes.  Replaces Lattice /
+ * Lattice_element (lattice/lattice.h, lattice/lattice_element.h) as the
+ * input of the steppers; no MAD-X parsing.
+ * ------------------------------------------------------------------- */
+typedef struct sb2_lattice sb2_lattice;
+sb2_status sb2_lattice_create(const char* name, sb2_lattice** out);
+sb2_status sb2_lattice_destroy(sb2_lattice* l);
+sb2_status sb2_lattice_set_reference_particle(sb2_lattice* l, int32_t charge, double mass,
+                                              double value, int32_t kind);
+/* Appends an element of MAD-X type name (drift, quadrupole, sbend,
+ * multipole, sextupole, marker, monitor, ...); returns its index. */
+sb2_status sb2_lattice_append(sb2_lattice* l, const char* type, const char* name, int32_t* index);
+sb2_status sb2_lattice_set_double(sb2_lattice* l, int32_t index, const char* attr, double value);
+sb2_status sb2_lattice_set_string(sb2_lattice* l, int32_t index, const char* attr, const char* value);
+sb2_status sb2_lattice_set_vector(sb2_lattice* l, int32_t index, const char* attr, const double* v,
+                                  int32_t n);
+sb2_status sb2_lattice_length(sb2_lattice* l, double* length);
+sb2_status sb2_lattice_num_elements(sb2_lattice* l, int32_t* n);
+
+/* ---------------------------------------------------------------------
+ * Propagator.  A stepper (split-operator by steps, split-operator per
+ * element, independent per element) with an optional space-charge operator.
+ * ------------------------------------------------------------------- */
+enum { SB2_STEPPER_SPLIT_OPERATOR = 0, SB2_STEPPER_SPLIT_OPERATOR_ELEMENTS = 1,
+       SB2_STEPPER_INDEPENDENT_ELEMENTS = 2 };
+
+typedef struct sb2_propagator sb2_propagator;
+/* sc may be NULL (Dummy_CO_options: no collective operator).  The lattice is
+ * copied; its element attributes are read at creation. */
+sb2_status sb2_propagator_create(const sb2_lattice* lattice, int32_t stepper, int32_t num_steps,
+                                 const sb2_sc3d_options* sc, sb2_propagator** out);
+sb2_status sb2_propagator_destroy(sb2_propagator* p);
+sb2_status sb2_propagator_num_steps(sb2_propagator* p, int32_t* n);
+/* Slices of independent operator `op` (0 = first half, 1 = second half) of
+ * step `step`: triples (element index, left, right); returns the count in
+ * *n (at most cap). */
+sb2_status sb2_propagator_step_slices(sb2_propagator* p, int32_t step, int32_t op, double* out,
+                                      int32_t cap, int32_t* n);
+/* Propagator::propagate(sim, logger, turns) for one bunch, on `stream`
+ * (cudaStream_t or NULL); returns after the device work is complete. */
+sb2_status sb2_propagator_propagate(sb2_propagator* p, sb2_bunch* b, int32_t turns, void* stream);
+/* Same over `count` consecutive steps starting at step `first` (steps wrap
+ * around the turn). */
+sb2_status sb2_propagator_propagate_steps(sb2_propagator* p, sb2_bunch* b, int32_t first,
+                                          int32_t count, void* stream);
+/* Charge lost on lattice element `index` through the aperture operations
+ * (Lattice_element::deposit_charge, aperture_operation.h:14-24), summed over
+ * all bunches this propagator has propagated. */
+sb2_status sb2_propagator_deposited_charge(sb2_propagator* p, int32_t index, double* charge);
+/* Last space-charge solve: domain (left, h), rho, phi and the three field
+ * components on the (gz, gy, gx) grid, scalars {fn_norm, factor, mean_std[6]}.
+ * Any output may be NULL. */
+sb2_status sb2_propagator_sc_last(sb2_propagator* p, double left[3], double h[3], double* rho,
+                                  double* phi, double* ex, double* ey, double* ez, double scalars[8]);
+
+/* ---------------------------------------------------------------------
+ * Collective operator alone: Space_charge_3d_open_hockney::apply_bunch
+ * (space_charge_3d_open_hockney.cc:423-453).
+ * ------------------------------------------------------------------- */
+typedef struct sb2_sc3d sb2_sc3d;
+sb2_status sb2_sc3d_create(const sb2_sc3d_options* opts, sb2_sc3d** out);
+sb2_status sb2_sc3d_destroy(sb2_sc3d* sc);
+/* One space-charge kick of the bunch over time_step [s]. */
+sb2_status sb2_sc3d_apply(sb2_sc3d* sc, sb2_bunch* b, double time_step, void* stream);
+/* Intermediate results of the last apply (as sb2_propagator_sc_last). */
+sb2_status sb2_sc3d_last(sb2_sc3d* sc, double left[3], double h[3], double* rho, double* phi,
+                         double* ex, double* ey, double* ez, double scalars[8]);
+
+/* ---------------------------------------------------------------------
+ * Independent operations on explicit slices of a lattice.
+ * ------------------------------------------------------------------- */
+/* LibFF_operation over the given slices, in order: triples (element index,
+ * left, right) of `lattice`; updates the bunch design reference particle
+ * (initialised from the lattice reference particle on first use). */
+sb2_status sb2_libff_apply(const sb2_lattice* lattice, const double* slices, int32_t nslices,
+                           sb2_bunch* b, void* stream);
+/* Aperture_operation<AP> for aperture type "finite", "circular",
+ * "elliptical" or "rectangular" with the attributes of element `index`;
+ * returns the number of discarded particles. */
+sb2_status sb2_aperture_apply(const sb2_lattice* lattice, int32_t index, const char* aperture_type,
+                              sb2_bunch* b, int32_t* ndiscarded, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SB2_H_ */

@@ -1,0 +1,435 @@
+"""synergia2_b200 — B200-native space-charge + tracking step of Synergia.
+
+Python mirror of the reference's own Python API for this path (class and
+method names as in synergia.foundation / lattice / collective / simulation /
+bunch), driving the sm_100a library libsb2.so through its C ABI
+(include/sb2.h).  Particles live on the GPU; host arrays cross only in
+get_particles / set_particles.
+
+    import synergia2_b200 as syn
+    ref = syn.Reference_particle(1, syn.Four_momentum(syn.pconstants.mp, syn.pconstants.mp + 2.5))
+    lat = syn.Lattice("fodo"); ...; lat.set_reference_particle(ref)
+    sc = syn.Space_charge_3d_open_hockney_options(64, 64, 128)
+    prop = syn.Propagator(lat, syn.Split_operator_stepper(sc, 8))
+    bunch = syn.Bunch(ref, 4194304, 1e11)
+    bunch.populate_gaussian([1e-3, 1e-4, 1e-3, 1e-4, 0.3, 1e-4], seed=1)
+    prop.propagate(bunch, 100)
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import SB2Error, check, lib
+
+__all__ = ["pconstants", "Four_momentum", "Reference_particle", "Lattice_element", "Lattice", "Bunch",
+           "Space_charge_3d_open_hockney_options", "Space_charge_3d_open_hockney", "Split_operator_stepper",
+           "Split_operator_stepper_elements", "Independent_stepper_elements", "Propagator", "SB2Error",
+           "green_fn_t", "precision_t"]
+
+
+class pconstants:
+    """foundation/physical_constants.h (PDG 2012)."""
+    mp = proton_mass = 0.938272046
+    me = electron_mass = 0.510998928e-3
+    e = 1.602176565e-19
+    c = 299792458.0
+    mu0 = 4 * math.pi * 1.0e-7
+    epsilon0 = 1.0 / (c * c * mu0)
+    rp = e / (4 * math.pi * epsilon0 * mp * 1.0e9)
+    proton_charge = 1
+
+
+class green_fn_t:
+    pointlike = _lib.SB2_GREEN_POINTLIKE
+    linear = _lib.SB2_GREEN_LINEAR
+
+
+class precision_t:
+    fp64 = _lib.SB2_PRECISION_FP64
+    mixed = _lib.SB2_PRECISION_MIXED
+
+
+def _pd(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if a is not None else None
+
+
+def _pu8(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)) if a is not None else None
+
+
+class Four_momentum:
+    """foundation/four_momentum.{h,cc}: kept as (mass, how, value) so the C
+    side rebuilds gamma, beta and p with the reference's own arithmetic."""
+
+    def __init__(self, mass, total_energy=None):
+        self.mass = mass
+        if total_energy is None:
+            self._kind, self._value = _lib.SB2_REF_TOTAL_ENERGY, mass
+        else:
+            self._kind, self._value = _lib.SB2_REF_TOTAL_ENERGY, total_energy
+
+    def set_momentum(self, p):
+        self._kind, self._value = _lib.SB2_REF_MOMENTUM, p
+
+    def set_kinetic_energy(self, k):
+        self._kind, self._value = _lib.SB2_REF_KINETIC_ENERGY, k
+
+    def set_total_energy(self, e):
+        self._kind, self._value = _lib.SB2_REF_TOTAL_ENERGY, e
+
+    def _gamma(self):
+        if self._kind == _lib.SB2_REF_TOTAL_ENERGY:
+            return self._value / self.mass
+        if self._kind == _lib.SB2_REF_KINETIC_ENERGY:
+            return (self.mass + self._value) / self.mass
+        r2 = self._value ** 2 / self.mass ** 2
+        b = math.sqrt(r2 / (1 + r2))
+        return 1.0 / math.sqrt(1.0 - b * b)
+
+    def get_gamma(self):
+        return self._gamma()
+
+    def get_beta(self):
+        g = self._gamma()
+        return math.sqrt(1.0 - 1.0 / (g * g))
+
+    def get_momentum(self):
+        g = self._gamma()
+        return g * self.get_beta() * self.mass
+
+    def get_total_energy(self):
+        return self._gamma() * self.mass
+
+
+class Reference_particle:
+    def __init__(self, charge, four_momentum):
+        self.charge = charge
+        self.four_momentum = four_momentum
+
+    def get_charge(self):
+        return self.charge
+
+    def get_mass(self):
+        return self.four_momentum.mass
+
+    def get_beta(self):
+        return self.four_momentum.get_beta()
+
+    def get_gamma(self):
+        return self.four_momentum.get_gamma()
+
+    def get_momentum(self):
+        return self.four_momentum.get_momentum()
+
+    def _spec(self):
+        fm = self.four_momentum
+        return self.charge, fm.mass, fm._value, fm._kind
+
+
+class Lattice_element:
+    """lattice/lattice_element.h: type name, element name, attributes."""
+
+    def __init__(self, type_name, name):
+        self.type = type_name
+        self.name = name
+        self.double = {}
+        self.string = {}
+        self.vector = {}
+
+    def set_double_attribute(self, k, v):
+        self.double[k] = float(v)
+
+    def set_string_attribute(self, k, v):
+        self.string[k] = str(v)
+
+    def set_vector_attribute(self, k, v):
+        self.vector[k] = [float(x) for x in v]
+
+    def get_double_attribute(self, k, default=None):
+        if k in self.double:
+            return self.double[k]
+        if default is None:
+            raise KeyError(k)
+        return default
+
+    def get_length(self):
+        return self.double.get("l", 0.0)
+
+    def get_type_name(self):
+        return self.type
+
+    def get_name(self):
+        return self.name
+
+
+class Lattice:
+    def __init__(self, name="lattice", elements=None, reference_particle=None):
+        self.name = name
+        self.elements = list(elements or [])
+        self.reference_particle = reference_particle
+
+    def append(self, element):
+        self.elements.append(element)
+
+    def set_reference_particle(self, ref):
+        self.reference_particle = ref
+
+    def get_reference_particle(self):
+        return self.reference_particle
+
+    def get_elements(self):
+        return self.elements
+
+    def get_length(self):
+        L = 0.0
+        for e in self.elements:
+            L += e.get_length()
+        return L
+
+    def _handle(self):
+        """Builds the C-side lattice (caller destroys)."""
+        h = ctypes.c_void_p()
+        check(lib().sb2_lattice_create(self.name.encode(), ctypes.byref(h)))
+        if self.reference_particle is not None:
+            check(lib().sb2_lattice_set_reference_particle(h, *self.reference_particle._spec()))
+        idx = ctypes.c_int32()
+        for e in self.elements:
+            check(lib().sb2_lattice_append(h, e.type.encode(), e.name.encode(), ctypes.byref(idx)))
+            for k, v in e.double.items():
+                check(lib().sb2_lattice_set_double(h, idx, k.encode(), v))
+            for k, v in e.string.items():
+                check(lib().sb2_lattice_set_string(h, idx, k.encode(), v.encode()))
+            for k, v in e.vector.items():
+                a = np.asarray(v, dtype=np.float64)
+                check(lib().sb2_lattice_set_vector(h, idx, k.encode(), _pd(a), len(a)))
+        return h
+
+
+class Bunch:
+    """bunch/bunch.h: N x 7 FP64 column-major particles + uint8 masks on the
+    GPU.  Columns x, xp, y, yp, cdt, dpop, id."""
+    x, xp, y, yp, cdt, dpop, id = range(7)
+
+    def __init__(self, reference_particle, total_num, real_num):
+        self.reference_particle = reference_particle
+        self.n = int(total_num)
+        h = ctypes.c_void_p()
+        check(lib().sb2_bunch_create(*reference_particle._spec(), self.n, float(real_num), ctypes.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            try:
+                lib().sb2_bunch_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+    def size(self):
+        return self.n
+
+    def set_particles(self, parts, masks=None):
+        """checkin: parts is (N, 7) (any order; copied as column-major)."""
+        p = np.asfortranarray(parts, dtype=np.float64)
+        assert p.shape == (self.n, 7)
+        m = None if masks is None else np.ascontiguousarray(masks, dtype=np.uint8)
+        check(lib().sb2_bunch_set_particles(self.h, _pd(p), _pu8(m)))
+
+    def get_particles(self):
+        """checkout: returns (parts (N,7) F-order, masks, discards)."""
+        p = np.zeros((self.n, 7), order="F")
+        m = np.zeros(self.n, np.uint8)
+        d = np.zeros(self.n, np.uint8)
+        check(lib().sb2_bunch_get_particles(self.h, _pd(p), _pu8(m), _pu8(d)))
+        return p, m, d
+
+    def get_local_particles(self):
+        return self.get_particles()[0]
+
+    def counts(self):
+        a, v, t, r = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_double()
+        check(lib().sb2_bunch_counts(self.h, ctypes.byref(a), ctypes.byref(v), ctypes.byref(t), ctypes.byref(r)))
+        return dict(size=a.value, local_num=v.value, total_num=t.value, real_num=r.value)
+
+    def get_local_num(self):
+        return self.counts()["local_num"]
+
+    def get_total_num(self):
+        return self.counts()["total_num"]
+
+    def get_real_num(self):
+        return self.counts()["real_num"]
+
+    def design_state(self):
+        st = np.zeros(6)
+        sn = ctypes.c_double()
+        check(lib().sb2_bunch_design_state(self.h, _pd(st), ctypes.byref(sn)))
+        return st, sn.value
+
+    def populate_gaussian(self, sigmas, seed):
+        s = np.asarray(sigmas, dtype=np.float64)
+        check(lib().sb2_bunch_populate_gaussian(self.h, _pd(s), int(seed)))
+
+    def moments(self):
+        mean, mom2, emit = np.zeros(6), np.zeros(36), np.zeros(3)
+        check(lib().sb2_bunch_moments(self.h, _pd(mean), _pd(mom2), _pd(emit)))
+        return mean, mom2.reshape(6, 6), emit
+
+    def device_arrays(self):
+        p, m, d = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        st = ctypes.c_int64()
+        check(lib().sb2_bunch_device_arrays(self.h, ctypes.byref(p), ctypes.byref(st), ctypes.byref(m),
+                                            ctypes.byref(d)))
+        return p.value, st.value, m.value, d.value
+
+
+class Space_charge_3d_open_hockney_options:
+    """simulation/implemented_collective_options.h:67-126."""
+
+    def __init__(self, gridx=32, gridy=32, gridz=64):
+        self._o = _lib.sb2_sc3d_options()
+        check(lib().sb2_sc3d_options_init(ctypes.byref(self._o), gridx, gridy, gridz))
+
+    def set_fixed_domain(self, offset, size):
+        o = np.asarray(offset, dtype=np.float64)
+        s = np.asarray(size, dtype=np.float64)
+        check(lib().sb2_sc3d_options_set_fixed_domain(ctypes.byref(self._o), _pd(o), _pd(s)))
+
+    def __getattr__(self, k):
+        if k == "_o":
+            raise AttributeError(k)
+        o = self.__dict__["_o"]
+        v = getattr(o, k)
+        return list(v) if hasattr(v, "__len__") else v
+
+    def __setattr__(self, k, v):
+        if k == "_o":
+            object.__setattr__(self, k, v)
+            return
+        o = self.__dict__["_o"]
+        cur = getattr(o, k)
+        if hasattr(cur, "__len__"):
+            for i, x in enumerate(v):
+                cur[i] = x
+        else:
+            setattr(o, k, v)
+
+
+class Space_charge_3d_open_hockney:
+    """The collective operator alone (space_charge_3d_open_hockney.cc:400-453)."""
+
+    def __init__(self, options):
+        self.options = options
+        h = ctypes.c_void_p()
+        check(lib().sb2_sc3d_create(ctypes.byref(options._o), ctypes.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            try:
+                lib().sb2_sc3d_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+    def apply(self, bunch, time_step):
+        check(lib().sb2_sc3d_apply(self.h, bunch.h, float(time_step), None))
+
+    def last(self):
+        gx, gy, gz = self.options.shape
+        return _sc_last(lambda *a: lib().sb2_sc3d_last(self.h, *a), gx, gy, gz)
+
+
+def _sc_last(fn, gx, gy, gz):
+    left, h, sc = np.zeros(3), np.zeros(3), np.zeros(8)
+    arrs = [np.zeros((gz, gy, gx)) for _ in range(5)]
+    check(fn(_pd(left), _pd(h), *[_pd(a) for a in arrs], _pd(sc)))
+    return dict(left=left, h=h, rho=arrs[0], phi=arrs[1], ex=arrs[2], ey=arrs[3], ez=arrs[4], fn_norm=sc[0],
+                factor=sc[1], mean_std=sc[2:8])
+
+
+class _Stepper:
+    kind = None
+
+    def __init__(self, collective_options, num):
+        self.collective_options = collective_options
+        self.num = num
+
+
+class Split_operator_stepper(_Stepper):
+    """simulation/split_operator_stepper.cc: num_steps split-operator steps."""
+    kind = _lib.SB2_STEPPER_SPLIT_OPERATOR
+
+    def __init__(self, collective_options, num_steps):
+        super().__init__(collective_options, num_steps)
+
+
+class Split_operator_stepper_elements(_Stepper):
+    kind = _lib.SB2_STEPPER_SPLIT_OPERATOR_ELEMENTS
+
+    def __init__(self, collective_options, steps_per_element):
+        super().__init__(collective_options, steps_per_element)
+
+
+class Independent_stepper_elements(_Stepper):
+    kind = _lib.SB2_STEPPER_INDEPENDENT_ELEMENTS
+
+    def __init__(self, steps_per_element):
+        super().__init__(None, steps_per_element)
+
+
+class Propagator:
+    """simulation/propagator.cc: Propagator(lattice, stepper).propagate."""
+
+    def __init__(self, lattice, stepper):
+        self.lattice = lattice
+        self.stepper = stepper
+        lh = lattice._handle()
+        try:
+            h = ctypes.c_void_p()
+            opts = stepper.collective_options
+            check(lib().sb2_propagator_create(lh, stepper.kind, stepper.num,
+                                              ctypes.byref(opts._o) if opts is not None else None,
+                                              ctypes.byref(h)))
+            self.h = h
+        finally:
+            lib().sb2_lattice_destroy(lh)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            try:
+                lib().sb2_propagator_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+    def num_steps(self):
+        n = ctypes.c_int32()
+        check(lib().sb2_propagator_num_steps(self.h, ctypes.byref(n)))
+        return n.value
+
+    def step_slices(self, step, op):
+        out = np.zeros((256, 3))
+        n = ctypes.c_int32()
+        check(lib().sb2_propagator_step_slices(self.h, step, op, _pd(out), 256, ctypes.byref(n)))
+        return None if n.value < 0 else out[: n.value]
+
+    def propagate(self, bunch, turns, stream=None):
+        check(lib().sb2_propagator_propagate(self.h, bunch.h, int(turns), stream))
+
+    def propagate_steps(self, bunch, first, count, stream=None):
+        check(lib().sb2_propagator_propagate_steps(self.h, bunch.h, int(first), int(count), stream))
+
+    def deposited_charge(self, index):
+        c = ctypes.c_double()
+        check(lib().sb2_propagator_deposited_charge(self.h, index, ctypes.byref(c)))
+        return c.value
+
+    def sc_last(self):
+        gx, gy, gz = self.stepper.collective_options.shape
+        return _sc_last(lambda *a: lib().sb2_propagator_sc_last(self.h, *a), gx, gy, gz)

@@ -1,0 +1,105 @@
+"""ctypes binding of libsb2.so (include/sb2.h).
+
+The library must have been built (python -m synergia2_b200.build); loading
+fails loudly otherwise — there is no CPU fallback.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsb2.so")
+_LIB = None
+
+SB2_OK, SB2_ERR_INVALID, SB2_ERR_CUDA, SB2_ERR_RUNTIME, SB2_ERR_UNSUPPORTED, SB2_ERR_NOMEM = range(6)
+SB2_GREEN_POINTLIKE, SB2_GREEN_LINEAR = 0, 1
+SB2_PRECISION_FP64, SB2_PRECISION_MIXED = 0, 1
+SB2_REF_TOTAL_ENERGY, SB2_REF_MOMENTUM, SB2_REF_KINETIC_ENERGY = 0, 1, 2
+SB2_STEPPER_SPLIT_OPERATOR, SB2_STEPPER_SPLIT_OPERATOR_ELEMENTS, SB2_STEPPER_INDEPENDENT_ELEMENTS = 0, 1, 2
+
+# Every function the header declares, with its ctypes signature.
+_c = ctypes
+_vp, _i32, _i64, _d, _u64, _cp = _c.c_void_p, _c.c_int32, _c.c_int64, _c.c_double, _c.c_uint64, _c.c_char_p
+_pd, _pu8, _pi32, _pi64 = _c.POINTER(_c.c_double), _c.POINTER(_c.c_uint8), _c.POINTER(_c.c_int32), _c.POINTER(_c.c_int64)
+
+
+class sb2_sc3d_options(ctypes.Structure):
+    _fields_ = [("shape", _c.c_int32 * 3), ("doubled_shape", _c.c_int32 * 3), ("size", _c.c_double * 3),
+                ("offset", _c.c_double * 3), ("green_fn", _c.c_int32), ("periodic_z", _c.c_int32),
+                ("z_period", _c.c_double), ("grid_entire_period", _c.c_int32), ("n_sigma", _c.c_double),
+                ("kick_scale", _c.c_double), ("domain_fixed", _c.c_int32), ("comm_group_size", _c.c_int32),
+                ("precision", _c.c_int32)]
+
+
+_popts = _c.POINTER(sb2_sc3d_options)
+_ppv = _c.POINTER(_c.c_void_p)
+
+SIGNATURES = {
+    "sb2_last_error": (_cp, []),
+    "sb2_version": (_cp, []),
+    "sb2_profile_enable": (_i32, [_i32]),
+    "sb2_profile_read": (_i32, [_i32, _c.POINTER(_cp), _pd, _pi64, _i32]),
+    "sb2_sc3d_options_init": (_i32, [_popts, _c.c_int, _c.c_int, _c.c_int]),
+    "sb2_sc3d_options_set_fixed_domain": (_i32, [_popts, _pd, _pd]),
+    "sb2_bunch_create": (_i32, [_i32, _d, _d, _i32, _i64, _d, _ppv]),
+    "sb2_bunch_wrap": (_i32, [_i32, _d, _d, _i32, _vp, _i64, _vp, _vp, _i64, _d, _ppv]),
+    "sb2_bunch_destroy": (_i32, [_vp]),
+    "sb2_bunch_set_particles": (_i32, [_vp, _pd, _pu8]),
+    "sb2_bunch_get_particles": (_i32, [_vp, _pd, _pu8, _pu8]),
+    "sb2_bunch_device_arrays": (_i32, [_vp, _ppv, _pi64, _ppv, _ppv]),
+    "sb2_bunch_counts": (_i32, [_vp, _pi64, _pi64, _pi64, _pd]),
+    "sb2_bunch_design_state": (_i32, [_vp, _pd, _pd]),
+    "sb2_bunch_populate_gaussian": (_i32, [_vp, _pd, _u64]),
+    "sb2_bunch_moments": (_i32, [_vp, _pd, _pd, _pd]),
+    "sb2_lattice_create": (_i32, [_cp, _ppv]),
+    "sb2_lattice_destroy": (_i32, [_vp]),
+    "sb2_lattice_set_reference_particle": (_i32, [_vp, _i32, _d, _d, _i32]),
+    "sb2_lattice_append": (_i32, [_vp, _cp, _cp, _pi32]),
+    "sb2_lattice_set_double": (_i32, [_vp, _i32, _cp, _d]),
+    "sb2_lattice_set_string": (_i32, [_vp, _i32, _cp, _cp]),
+    "sb2_lattice_set_vector": (_i32, [_vp, _i32, _cp, _pd, _i32]),
+    "sb2_lattice_length": (_i32, [_vp, _pd]),
+    "sb2_lattice_num_elements": (_i32, [_vp, _pi32]),
+    "sb2_propagator_create": (_i32, [_vp, _i32, _i32, _popts, _ppv]),
+    "sb2_propagator_destroy": (_i32, [_vp]),
+    "sb2_propagator_num_steps": (_i32, [_vp, _pi32]),
+    "sb2_propagator_step_slices": (_i32, [_vp, _i32, _i32, _pd, _i32, _pi32]),
+    "sb2_propagator_propagate": (_i32, [_vp, _vp, _i32, _vp]),
+    "sb2_propagator_propagate_steps": (_i32, [_vp, _vp, _i32, _i32, _vp]),
+    "sb2_propagator_deposited_charge": (_i32, [_vp, _i32, _pd]),
+    "sb2_propagator_sc_last": (_i32, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd]),
+    "sb2_sc3d_create": (_i32, [_popts, _ppv]),
+    "sb2_sc3d_destroy": (_i32, [_vp]),
+    "sb2_sc3d_apply": (_i32, [_vp, _vp, _d, _vp]),
+    "sb2_sc3d_last": (_i32, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd]),
+    "sb2_libff_apply": (_i32, [_vp, _pd, _i32, _vp, _vp]),
+    "sb2_aperture_apply": (_i32, [_vp, _i32, _cp, _vp, _pi32, _vp]),
+}
+
+
+class SB2Error(RuntimeError):
+    """Raised when a C-ABI call returns a non-zero sb2_status; carries the
+    library's message (the text the reference throws, where it throws)."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("synergia2_b200: %s is not built (run python -m synergia2_b200.build)" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def check(rc):
+    if rc != SB2_OK:
+        raise SB2Error(rc, lib().sb2_last_error().decode())
+    return rc

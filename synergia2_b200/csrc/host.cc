@@ -1,0 +1,2075 @@
+// Host runtime of the B200 space-charge + tracking step and its C ABI
+// (include/sb2.h).
+//
+// What lives here: reference-particle kinematics, the lattice and its
+// slicing by the three steppers, the host half of every libFF element map
+// (attribute lookup, strength scaling and design-reference-particle
+// propagation, done exactly as the reference does on the host), the fused
+// pass executor that turns one step into device launches, and the
+// space-charge operator's workspaces.
+//
+// Compiled with -ffp-contract=off: the host-side design-particle arithmetic
+// must round exactly as the reference's (no -ffast-math is in effect there,
+// CMakeLists.txt:338).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <complex>
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sb2.h"
+#include "sb2_kernels.h"
+
+namespace sb2 {
+
+// ---------------------------------------------------------------------------
+// constants: foundation/physical_constants.h (PDG 2012)
+// ---------------------------------------------------------------------------
+namespace pc {
+constexpr double pi = 3.14159265358979323846;
+constexpr double c = 299792458.0;
+constexpr double e = 1.602176565e-19;
+} // namespace pc
+
+struct Error : std::runtime_error {
+    sb2_status code;
+    Error(sb2_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+static void cuda_check(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess)
+        throw Error(e == cudaErrorMemoryAllocation ? SB2_ERR_NOMEM : SB2_ERR_CUDA,
+                    std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// Reference particle (foundation/four_momentum.cc, reference_particle.cc)
+// ---------------------------------------------------------------------------
+struct Refpart {
+    int charge = 1;
+    double mass = 0.938272046;
+    double gamma = 1, beta = 0, p = 0, energy = 0;
+    std::array<double, 6> state{0, 0, 0, 0, 0, 0};
+    double s = 0, s_n = 0;
+    int repetition = 0;
+
+    void set_gamma(double g)
+    { // four_momentum.cc:8-16
+        if (g < 1.0) throw Error(SB2_ERR_INVALID, "Four_momentum: gamma not >= 1.0");
+        gamma = g;
+        energy = gamma * mass;
+        beta = std::sqrt(1.0 - 1.0 / (gamma * gamma));
+        p = gamma * beta * mass;
+    }
+    void set(int chg, double m, double value, int kind)
+    {
+        charge = chg;
+        mass = m;
+        if (kind == SB2_REF_TOTAL_ENERGY)
+            set_gamma(value / mass);
+        else if (kind == SB2_REF_KINETIC_ENERGY)
+            set_gamma((mass + value) / mass);
+        else if (kind == SB2_REF_MOMENTUM) { // four_momentum.cc:90-110
+            double r2 = value * value / (mass * mass);
+            double b = std::sqrt(r2 / (1 + r2));
+            if ((b < 0.0) || (b >= 1.0))
+                throw Error(SB2_ERR_INVALID, "Four_momentum: beta not in range 0.0 <= beta < 1.0");
+            set_gamma(1.0 / std::sqrt(1.0 - b * b));
+        } else
+            throw Error(SB2_ERR_INVALID, "unknown reference particle kind");
+    }
+    void start_repetition()
+    { // reference_particle.cc:231-237
+        if (s == 0.0) s = s_n;
+        if (s_n > 0.0) repetition += 1;
+        s_n = 0.0;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Lattice (lattice/lattice_element.h, lattice.cc)
+// ---------------------------------------------------------------------------
+struct Element {
+    std::string type, name;
+    std::map<std::string, double> d;
+    std::map<std::string, std::string> s;
+    std::map<std::string, std::vector<double>> v;
+
+    double get(const std::string& k, double def) const
+    {
+        auto it = d.find(k);
+        return it == d.end() ? def : it->second;
+    }
+    double get(const std::string& k) const
+    {
+        auto it = d.find(k);
+        if (it == d.end())
+            throw Error(SB2_ERR_RUNTIME, "Lattice_element::get_double_attribute: element " + name +
+                                             " of type " + type + " has no double attribute '" + k + "'");
+        return it->second;
+    }
+    bool has_string(const std::string& k) const { return s.count(k) > 0; }
+    std::string get_string(const std::string& k, const std::string& def) const
+    {
+        auto it = s.find(k);
+        return it == s.end() ? def : it->second;
+    }
+    double length() const { return get("l", 0.0); }
+};
+
+struct Lattice {
+    std::string name;
+    std::vector<Element> elements;
+    Refpart ref;
+    bool has_ref = false;
+
+    double length() const
+    { // lattice.cc:195-201
+        double L = 0.0;
+        for (auto const& e : elements) L += e.length();
+        return L;
+    }
+};
+
+// lattice_element_slice.cc:9-47
+struct Slice {
+    int elem = -1;
+    double left = 0, right = 0;
+    bool ledge = true, redge = true;
+};
+
+static Slice make_slice(const Lattice& lat, int ei, double l, double r)
+{
+    const double tol = 1.0e-9;
+    Slice s;
+    s.elem = ei;
+    s.left = l;
+    s.right = r;
+    if (l < 0.0) throw Error(SB2_ERR_RUNTIME, "Lattice_element_slice: left must be >= 0.0");
+    if (l < tol) {
+        s.ledge = true;
+        s.left = 0.0;
+    } else
+        s.ledge = false;
+    double L = lat.elements[ei].length();
+    if (r > L + tol)
+        throw Error(SB2_ERR_RUNTIME,
+                    "Lattice_element_slice: right must be no greater than the length of the element");
+    bool eq = (std::abs(r) < tol) ? (std::abs(r - L) < tol) : (std::abs((r - L) / r) < tol); // floating_point_equal
+    if (eq) {
+        s.redge = true;
+        s.right = L;
+    } else
+        s.redge = false;
+    return s;
+}
+
+static Slice whole_slice(const Lattice& lat, int ei)
+{
+    Slice s;
+    s.elem = ei;
+    s.left = 0;
+    s.right = lat.elements[ei].length();
+    s.ledge = s.redge = true;
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// Host copies of the libFF units used for the design reference particle
+// (ff_algorithm.h; same operation order)
+// ---------------------------------------------------------------------------
+namespace hostff {
+inline bool close_to_zero(double v) { return std::fabs(v) < 1e-13; }
+
+inline void drift_unit(double& x, double xp, double& y, double yp, double& cdt, double dpop, double length,
+                       double ref_p, double m, double ref_cdt)
+{
+    const double uni = 1.0;
+    const double sig = (double)((0.0 < length) - (length < 0.0));
+    double dp = dpop + uni;
+    double inv_npz = uni / std::sqrt(dp * dp - xp * xp - yp * yp);
+    double lxpr = xp * length * inv_npz;
+    double lypr = yp * length * inv_npz;
+    double D2 = lxpr * lxpr + length * length + lypr * lypr;
+    double p = dp * ref_p;
+    double E2 = p * p + m * m;
+    double ibeta2 = E2 / (p * p);
+    x = x + lxpr;
+    y = y + lypr;
+    cdt = cdt + sig * std::sqrt(D2 * ibeta2) - ref_cdt;
+}
+inline void thin_quad(double x, double& xp, double y, double& yp, const double* k)
+{
+    xp = xp - k[0] * x + k[1] * y;
+    yp = yp + k[0] * y + k[1] * x;
+}
+inline void thin_sext(double x, double& xp, double y, double& yp, const double* k)
+{
+    xp = xp - 0.5 * k[0] * (x * x - y * y) + k[1] * x * y;
+    yp = yp + k[0] * x * y + 0.5 * k[1] * (x * x - y * y);
+}
+inline void thin_oct(double x, double& xp, double y, double& yp, const double* k)
+{
+    const double n1 = 0.5, n2 = 1.0 / 3.0;
+    xp = xp - n1 * k[0] * (x * x * x * n2 - x * y * y) + n1 * k[1] * (x * x * y - y * y * y * n2);
+    yp = yp - n1 * k[0] * (y * y * y * n2 - x * x * y) + n1 * k[1] * (x * x * x * n2 - x * y * y);
+}
+inline double factorial(int n)
+{
+    if (n == 0) return 1.0;
+    double r = 1;
+    for (int i = 1; i <= n; ++i) r *= i;
+    return r;
+}
+inline double qpow(double x, int i)
+{
+    double r = 1;
+    while (i--) r = r * x;
+    return r;
+}
+inline void thin_magnet(double x, double& xp, double y, double& yp, const double* kL, int n)
+{
+    for (int k = 0; k < n; k += 4)
+        xp = xp - (kL[0] * (n - k)) * qpow(x, n - k - 1) * qpow(y, k) / (factorial(n - k) * factorial(k));
+    for (int k = 2; k < n; k += 4)
+        xp = xp + (kL[0] * (n - k)) * qpow(x, n - k - 1) * qpow(y, k) / (factorial(n - k) * factorial(k));
+    for (int k = 1; k < n; k += 4)
+        xp = xp + (kL[1] * (n - k)) * qpow(x, n - k - 1) * qpow(y, k) / (factorial(n - k) * factorial(k));
+    for (int k = 3; k < n; k += 4)
+        xp = xp - (kL[1] * (n - k)) * qpow(x, n - k - 1) * qpow(y, k) / (factorial(n - k) * factorial(k));
+    for (int k = 4; k <= n; k += 4)
+        yp = yp - (kL[0] * k) * qpow(x, n - k) * qpow(y, k - 1) / (factorial(n - k) * factorial(k));
+    for (int k = 2; k <= n; k += 4)
+        yp = yp + (kL[0] * k) * qpow(x, n - k) * qpow(y, k - 1) / (factorial(n - k) * factorial(k));
+    for (int k = 1; k <= n; k += 4)
+        yp = yp + (kL[1] * k) * qpow(x, n - k) * qpow(y, k - 1) / (factorial(n - k) * factorial(k));
+    for (int k = 3; k <= n; k += 4)
+        yp = yp - (kL[1] * k) * qpow(x, n - k) * qpow(y, k - 1) / (factorial(n - k) * factorial(k));
+}
+inline void cf_kick(double x, double& xp, double y, double& yp, const double* kL)
+{ // ff_quadrupole.h:22-35
+    thin_quad(x, xp, y, yp, kL);
+    if (kL[2] || kL[3]) thin_quad(x, xp, y, yp, kL + 2);
+    if (kL[4] || kL[5]) thin_sext(x, xp, y, yp, kL + 4);
+    if (kL[6] || kL[7]) thin_oct(x, xp, y, yp, kL + 6);
+    if (kL[8] || kL[9]) thin_magnet(x, xp, y, yp, kL + 8, 5);
+    if (kL[10] || kL[11]) thin_magnet(x, xp, y, yp, kL + 10, 6);
+    if (kL[12] || kL[13]) thin_magnet(x, xp, y, yp, kL + 12, 7);
+    if (kL[14] || kL[15]) thin_magnet(x, xp, y, yp, kL + 14, 8);
+}
+
+constexpr double Y_C1 = 0.79361246386112147294625603763;
+constexpr double Y_C2 = -0.206276584816439780698721319354;
+constexpr double Y_C3 = -0.118008867881292655922412133144;
+constexpr double Y_C4 = 0.236949573653050744373598734219;
+constexpr double Y_D1 = 1.58722492772224294589251207526;
+constexpr double Y_D2 = -1.99977809735512250728995471397;
+constexpr double Y_D3 = -1.82324266348482825773733634154;
+constexpr double Y_D4 = 2.29714181079092974648453380998;
+
+using kick_fn = void (*)(double, double&, double, double&, const double*);
+
+// yoshida6 ff_algorithm.h:1834-2008
+inline void yoshida6(double& x, double& xp, double& y, double& yp, double& cdt, double dpop, double pref,
+                     double m, double step_ref_cdt, double step_length, const double* step_strength, int steps,
+                     kick_fn kf, int components)
+{
+    double sub = step_ref_cdt * 0.1;
+    double k1[16], k2[16], k3[16], k4[16];
+    for (int i = 0; i < components * 2; ++i) {
+        k1[i] = Y_D1 * step_strength[i];
+        k2[i] = Y_D2 * step_strength[i];
+        k3[i] = Y_D3 * step_strength[i];
+        k4[i] = Y_D4 * step_strength[i];
+    }
+    auto D = [&](double cc) { drift_unit(x, xp, y, yp, cdt, dpop, cc * step_length, pref, m, sub); };
+    for (int i = 0; i < steps; ++i) {
+        D(Y_C1); kf(x, xp, y, yp, k1);
+        D(Y_C2); kf(x, xp, y, yp, k2);
+        D(Y_C2); kf(x, xp, y, yp, k1);
+        D(Y_C3); kf(x, xp, y, yp, k3);
+        D(Y_C4); kf(x, xp, y, yp, k4);
+        D(Y_C4); kf(x, xp, y, yp, k3);
+        D(Y_C3); kf(x, xp, y, yp, k1);
+        D(Y_C2); kf(x, xp, y, yp, k2);
+        D(Y_C2); kf(x, xp, y, yp, k1);
+        D(Y_C1);
+    }
+}
+
+// general 6th-order yoshida, ff_algorithm.h:1481-1646
+inline double yx1(int nn) { return 1.0 / (2.0 - std::pow(2.0, 1.0 / (2 * nn + 1))); }
+inline double yx0(int nn) { return 1.0 - 2.0 * yx1(nn); }
+inline void yoshida_element(int n, double& x, double& xp, double& y, double& yp, double& cdt, double dpop,
+                            double pref, double m, double step_ref_cdt, double step_length, const double* ss,
+                            double c, kick_fn kf, int comps)
+{
+    if (n == 0) {
+        double sub = step_ref_cdt / 2.0;
+        double kl[16];
+        for (int i = 0; i < comps * 2; ++i) kl[i] = ss[i] * c;
+        drift_unit(x, xp, y, yp, cdt, dpop, 0.5 * c * step_length, pref, m, sub);
+        kf(x, xp, y, yp, kl);
+        drift_unit(x, xp, y, yp, cdt, dpop, 0.5 * c * step_length, pref, m, sub);
+        return;
+    }
+    double sub = step_ref_cdt / 3.0;
+    yoshida_element(n - 1, x, xp, y, yp, cdt, dpop, pref, m, sub, step_length, ss, c * yx1(n), kf, comps);
+    yoshida_element(n - 1, x, xp, y, yp, cdt, dpop, pref, m, sub, step_length, ss, c * yx0(n), kf, comps);
+    yoshida_element(n - 1, x, xp, y, yp, cdt, dpop, pref, m, sub, step_length, ss, c * yx1(n), kf, comps);
+}
+
+// slot_unit ff_algorithm.h:83-129
+inline void slot_unit(double& x, double& xp, double& y, double& yp, double& cdt, double& dpop, double ct,
+                      double st, double pref, double m)
+{
+    const double uni = 1.0;
+    double zp = std::sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
+    double p = (dpop + uni) * pref;
+    double e = std::sqrt(p * p + m * m);
+    double b0 = xp * pref / e;
+    double b1 = yp * pref / e;
+    double b2 = zp * pref / e;
+    double bp = st * b0 + ct * b2;
+    double tau = -x * st / bp;
+    double r0 = x + tau * b0;
+    double r1 = y + tau * b1;
+    double r2 = tau * b2;
+    x = r0 * ct - r2 * st;
+    y = r1;
+    cdt = cdt + tau;
+    xp = xp * ct - zp * st;
+}
+
+// bend_complete ff_algorithm.h:191-251 (complex arithmetic form)
+inline void bend_complete(double& x, double& xp, double& y, double& yp, double& cdt, double dpop, double dphi,
+                          double strength, double p_ref, double m, double cdt_ref, std::complex<double> phase,
+                          std::complex<double> term)
+{
+    typedef std::complex<double> CT;
+    const double uni = 1.0;
+    double p0 = p_ref;
+    double p = p_ref * (dpop + 1.0);
+    double E0 = std::sqrt(p0 * p0 + m * m);
+    double E = std::sqrt(p * p + m * m);
+    double igamma = m / E0;
+    double ibeta = uni / std::sqrt(uni - igamma * igamma);
+    double csq = pc::c * pc::c * 1e-9;
+    double psq = (dpop + 1.0) * (dpop + 1.0);
+    double Ef = uni / std::sqrt(psq + igamma * igamma * ibeta * ibeta);
+    double beta1 = Ef * xp;
+    double beta2 = Ef * yp;
+    double beta3 = Ef * std::sqrt((dpop + 1.0) * (dpop + 1.0) - xp * xp - yp * yp);
+    CT ui = CT(0.0, x);
+    CT vui = CT(pc::c * beta3, pc::c * beta1);
+    double iomega = E / (csq * strength);
+    CT bi = CT(0.0, 1.0) * vui * iomega - ui;
+    CT bf = bi * phase + term;
+    double rho = pc::c * std::sqrt(beta1 * beta1 + beta3 * beta3) * iomega;
+    double dthmphi = std::asin(bi.real() / rho) - std::asin(bf.real() / rho);
+    CT expf = std::exp(CT(0.0, dthmphi));
+    CT vuf = vui * expf;
+    CT uf = (ui + bi) * expf - bf;
+    double dtheta = dthmphi + dphi;
+    double ncdt = -pc::c * dtheta * iomega;
+    x = uf.imag();
+    y += beta2 * ncdt;
+    cdt += ncdt - cdt_ref;
+    xp = vuf.imag() / (Ef * pc::c);
+}
+
+void quad_kick_cb(double x, double& xp, double y, double& yp, const double* k) { cf_kick(x, xp, y, yp, k); }
+void sext_kick_cb(double x, double& xp, double y, double& yp, const double* k) { thin_sext(x, xp, y, yp, k); }
+} // namespace hostff
+
+// ---------------------------------------------------------------------------
+// Bunch
+// ---------------------------------------------------------------------------
+struct Bunch {
+    int device = 0;
+    double* parts = nullptr;
+    int64_t stride = 0;
+    uint8_t* masks = nullptr;
+    uint8_t* discards = nullptr;
+    int64_t n = 0;
+    bool owns = false;
+    BunchCounters* counters = nullptr; // device
+    BunchCounters host_counters{};     // last value read back
+    Refpart ref;
+    Refpart design;
+    bool design_set = false;
+    int turns_done = 0;
+
+    ~Bunch()
+    {
+        if (owns) {
+            cudaFree(parts);
+            cudaFree(masks);
+            cudaFree(discards);
+        }
+        cudaFree(counters);
+    }
+    void sync_counters(cudaStream_t s)
+    {
+        cuda_check(cudaMemcpyAsync(&host_counters, counters, sizeof(BunchCounters), cudaMemcpyDeviceToHost, s),
+                   "counters");
+        cuda_check(cudaStreamSynchronize(s), "sync");
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Operations of one independent operator (independent_operator.cc:25-91)
+// ---------------------------------------------------------------------------
+struct Operation {
+    bool aperture = false;
+    std::vector<Slice> group; // libFF group
+    std::string ap_type;
+    Slice ap_slice;
+};
+
+static std::vector<Operation> create_operations(const Lattice& lat, const std::vector<Slice>& slices)
+{
+    std::vector<Operation> ops;
+    std::string aperture_type;
+    bool need_left = false, need_right = false;
+    std::string extractor_type, last_extractor_type;
+    std::vector<Slice> group;
+    auto push_group = [&]() {
+        Operation o;
+        o.group = group;
+        ops.push_back(o);
+    };
+    auto push_ap = [&](const std::string& t, const Slice& s) {
+        if (t != "finite" && t != "circular" && t != "elliptical" && t != "rectangular")
+            throw Error(t == "polygon" ? SB2_ERR_UNSUPPORTED : SB2_ERR_RUNTIME, "unknown aperture_type " + t);
+        Operation o;
+        o.aperture = true;
+        o.ap_type = t;
+        o.ap_slice = s;
+        ops.push_back(o);
+    };
+    for (auto const& slice : slices) {
+        const Element& el = lat.elements[slice.elem];
+        if (el.has_string("aperture_type")) {
+            aperture_type = el.get_string("aperture_type", "");
+            need_left = slice.ledge;
+            need_right = slice.redge;
+        } else {
+            need_left = need_right = false;
+        }
+        extractor_type = el.get_string("extractor_type", "default");
+        if (extractor_type != "default" && extractor_type != "libff")
+            throw Error(SB2_ERR_UNSUPPORTED, "unknown extractor_type: " + extractor_type);
+        if (((extractor_type != last_extractor_type) || need_left) && !group.empty()) {
+            push_group();
+            group.clear();
+        }
+        if (need_left) push_ap(aperture_type, slice);
+        group.push_back(slice);
+        last_extractor_type = extractor_type;
+        if (need_right) {
+            push_group();
+            push_ap(aperture_type, slice);
+            group.clear();
+        }
+    }
+    if (!group.empty()) push_group();
+    push_ap("finite", slices.back());
+    push_ap("circular", slices.back());
+    return ops;
+}
+
+struct IndepOperator {
+    std::vector<Slice> slices;
+    std::vector<Operation> ops;
+};
+
+struct Step {
+    double length = 0;
+    std::vector<char> items; // 'I' independent, 'C' collective
+    std::vector<IndepOperator> indeps;
+};
+
+// get_fixed_step_slices split_operator_stepper.cc:14-82 (no force_diagnostics)
+static std::vector<Slice> fixed_step_slices(const Lattice& lat, size_t& it, double& left, double step_length,
+                                            double& offset_fudge)
+{
+    const double tol = 1.0e-8;
+    std::vector<Slice> slices;
+    double length = offset_fudge;
+    bool complete = false;
+    const size_t end = lat.elements.size();
+    while (!complete) {
+        double right = lat.elements[it].length();
+        if (length + (right - left) - tol <= step_length) {
+            slices.push_back(make_slice(lat, (int)it, left, right));
+            length += (right - left);
+            ++it;
+            left = 0.0;
+            if (std::abs(length - step_length) < tol) {
+                if ((it == end) || (lat.elements[it].length() != 0.0)) complete = true;
+            } else {
+                if (it == end) throw Error(SB2_ERR_RUNTIME, "get_step stepped beyond end of lattice");
+            }
+        } else {
+            bool end_within_error = false;
+            double old_right = right;
+            right = step_length - length + left;
+            if (std::abs(old_right - right) < tol) {
+                right = old_right;
+                end_within_error = true;
+            }
+            slices.push_back(make_slice(lat, (int)it, left, right));
+            length += (right - left);
+            if (end_within_error) {
+                ++it;
+                left = 0.0;
+            } else {
+                left = right;
+            }
+            complete = true;
+        }
+    }
+    offset_fudge = length - step_length;
+    return slices;
+}
+
+static std::vector<Step> make_steps(const Lattice& lat, int kind, int num, bool collective)
+{
+    std::vector<Step> steps;
+    auto add_indep = [&](Step& st, std::vector<Slice> sl) {
+        IndepOperator op;
+        op.slices = std::move(sl);
+        op.ops = create_operations(lat, op.slices);
+        st.items.push_back('I');
+        st.indeps.push_back(std::move(op));
+    };
+    if (kind == SB2_STEPPER_SPLIT_OPERATOR) {
+        // Split_operator_stepper::apply_impl split_operator_stepper.cc:132-261
+        if (num < 1) throw Error(SB2_ERR_INVALID, "Split_operator_stepper: num_steps must be >= 1");
+        double step_length = lat.length() / num;
+        double half = 0.5 * step_length;
+        if (lat.elements.empty()) return steps;
+        size_t it = 0;
+        double left = 0.0, fudge = 0.0;
+        for (int i = 0; i < num; ++i) {
+            for (auto const& el : lat.elements)
+                if (el.has_string("force_diagnostics"))
+                    throw Error(SB2_ERR_UNSUPPORTED, "force_diagnostics substeps are not supported");
+            auto s1 = fixed_step_slices(lat, it, left, half, fudge);
+            auto s2 = fixed_step_slices(lat, it, left, half, fudge);
+            Step st;
+            st.length = step_length;
+            add_indep(st, s1);
+            if (collective) st.items.push_back('C');
+            add_indep(st, s2);
+            steps.push_back(std::move(st));
+        }
+        if (it != lat.elements.size())
+            throw Error(SB2_ERR_RUNTIME,
+                        "internal error: split_operator_stepper did not make it to the end of the lattice\n");
+    } else if (kind == SB2_STEPPER_SPLIT_OPERATOR_ELEMENTS || kind == SB2_STEPPER_INDEPENDENT_ELEMENTS) {
+        // split_operator_stepper_elements.cc:4-47, independent_stepper_elements.cc:3-36
+        if (num < 1) throw Error(SB2_ERR_INVALID, "Split_operator_stepper_elements: steps_per_element must be >= 1");
+        for (size_t ei = 0; ei < lat.elements.size(); ++ei) {
+            double length = lat.elements[ei].length();
+            if (length == 0.0) {
+                Step st;
+                st.length = 0.0;
+                add_indep(st, {whole_slice(lat, (int)ei)});
+                steps.push_back(std::move(st));
+                continue;
+            }
+            double sl = length / num;
+            for (int i = 0; i < num; ++i) {
+                double left = i * sl, right = (i + 1) * sl;
+                Step st;
+                st.length = sl;
+                if (kind == SB2_STEPPER_INDEPENDENT_ELEMENTS) {
+                    add_indep(st, {make_slice(lat, (int)ei, left, right)});
+                } else {
+                    double middle = left + 0.5 * sl;
+                    add_indep(st, {make_slice(lat, (int)ei, left, middle)});
+                    if (collective) st.items.push_back('C');
+                    add_indep(st, {make_slice(lat, (int)ei, middle, right)});
+                }
+                steps.push_back(std::move(st));
+            }
+        }
+    } else {
+        throw Error(SB2_ERR_INVALID, "unknown stepper kind");
+    }
+    return steps;
+}
+
+// ---------------------------------------------------------------------------
+// Host half of the element maps -> MapOps
+// ---------------------------------------------------------------------------
+static MapOp new_op(int kind)
+{
+    MapOp o;
+    std::memset(&o, 0, sizeof(o));
+    o.kind = kind;
+    return o;
+}
+
+static double brho_scale(const Bunch& b)
+{
+    const Refpart& ref_l = b.design;
+    const Refpart& ref_b = b.ref;
+    double brho_l = ref_l.p / ref_l.charge;
+    double brho_b = ref_b.p * (1.0 + ref_b.state[5]) / ref_l.charge;
+    return brho_l / brho_b;
+}
+
+// FF_drift::apply ff_drift.h:95-152
+static void ops_drift(const Slice& sl, Bunch& b, std::vector<MapOp>& out)
+{
+    const double length = sl.right - sl.left;
+    if (hostff::close_to_zero(length)) {
+        b.design.state[4] = 0.0;
+        return;
+    }
+    Refpart& ref_l = b.design;
+    const double ref_p = b.ref.p * (1.0 + b.ref.state[5]);
+    double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3];
+    double cdt = 0.0, dpop = 0.0;
+    hostff::drift_unit(x, xp, y, yp, cdt, dpop, length, ref_l.p, ref_l.mass, 0.0);
+    ref_l.state = {x, xp, y, yp, cdt, dpop};
+    MapOp o = new_op(OP_DRIFT);
+    o.d[0] = length;
+    o.d[1] = ref_p;
+    o.d[2] = b.ref.mass;
+    o.d[3] = cdt;
+    out.push_back(o);
+    b.ref.s_n += length;
+}
+
+// FF_quadrupole::apply ff_quadrupole.h:310-565
+static void ops_quad(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
+{
+    const Element& ele = lat.elements[sl.elem];
+    double length = sl.right - sl.left;
+    const double xoff = ele.get("hoffset", 0.0);
+    const double yoff = ele.get("voffset", 0.0);
+    double tilt = ele.get("tilt", 0.0);
+    double kn[16] = {0};
+    kn[0] = ele.get("k1", 0.0);
+    kn[1] = ele.get("k1s", 0.0);
+    double quad_str = kn[0];
+    std::complex<double> ck1(kn[0], -kn[1]);
+    double rot = std::arg(ck1) / 2.0 + tilt;
+    if (tilt != 0.0) {
+        std::complex<double> ck2(kn[0], kn[1]);
+        ck2 = ck2 * std::exp(std::complex<double>(0.0, -2.0 * tilt));
+        kn[0] = ck2.real();
+        kn[1] = ck2.imag();
+    }
+    bool has_mp = false;
+    for (int i = 1; i < 8; ++i) {
+        std::string a = "a0", bb = "b0";
+        a[1] = (char)('0' + i);
+        bb[1] = (char)('0' + i);
+        kn[i * 2 + 0] = ele.get(bb, 0.0);
+        kn[i * 2 + 1] = ele.get(a, 0.0);
+        if (kn[i * 2 + 0] || kn[i * 2 + 1]) {
+            has_mp = true;
+            double coeff = hostff::factorial(i);
+            kn[i * 2 + 0] *= quad_str * coeff;
+            kn[i * 2 + 1] *= quad_str * coeff;
+            if (rot || tilt) {
+                auto ck = std::complex<double>(kn[i * 2 + 0], kn[i * 2 + 1]);
+                ck *= std::exp(std::complex<double>(0.0, -(i + 1) * tilt));
+                ck *= std::exp(std::complex<double>(0.0, -(i + 1) * rot));
+                kn[i * 2 + 0] = ck.real();
+                kn[i * 2 + 1] = ck.imag();
+            }
+        }
+    }
+    Refpart& ref_l = b.design;
+    double scale = brho_scale(b);
+    for (auto& k : kn) k *= scale;
+
+    auto ref_cdt = [&](int steps) { // get_reference_cdt ff_quadrupole.h:263-303
+        double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3];
+        double cdt = 0.0, dpop = 0.0;
+        x -= xoff;
+        y -= yoff;
+        if (hostff::close_to_zero(length))
+            hostff::thin_quad(x, xp, y, yp, kn);
+        else
+            hostff::yoshida6(x, xp, y, yp, cdt, dpop, ref_l.p, ref_l.mass, 0.0, length / steps, kn, steps,
+                             hostff::quad_kick_cb, 8);
+        x += xoff;
+        y += yoff;
+        ref_l.state = {x, xp, y, yp, cdt, dpop};
+        return cdt;
+    };
+
+    if (hostff::close_to_zero(length)) {
+        ref_cdt(0);
+        MapOp o = new_op(OP_THIN_QUAD);
+        o.d[0] = xoff;
+        o.d[1] = yoff;
+        o.d[2] = kn[0];
+        o.d[3] = kn[1];
+        out.push_back(o);
+        return;
+    }
+    int steps = (int)ele.get("yoshida_steps", 4.0);
+    for (auto& k : kn) k *= length / steps;
+    double ref_p = b.ref.p, ref_m = b.ref.mass;
+    double ref_t = ref_cdt(steps);
+    double step_ref_t = ref_t / steps, step_l = length / steps;
+    MapOp o = new_op(has_mp ? OP_QUAD_CF : OP_QUAD);
+    o.steps = steps;
+    o.d[0] = xoff;
+    o.d[1] = yoff;
+    o.d[2] = ref_p;
+    o.d[3] = ref_m;
+    o.d[4] = step_ref_t * 0.1;
+    o.d[5] = hostff::Y_C1 * step_l;
+    o.d[6] = hostff::Y_C2 * step_l;
+    o.d[7] = hostff::Y_C3 * step_l;
+    o.d[8] = hostff::Y_C4 * step_l;
+    const int comps = has_mp ? 8 : 1;
+    const int KS = has_mp ? 16 : 2;
+    for (int i = 0; i < comps * 2; ++i) {
+        o.d[9 + i] = hostff::Y_D1 * kn[i];
+        o.d[9 + KS + i] = hostff::Y_D2 * kn[i];
+        o.d[9 + 2 * KS + i] = hostff::Y_D3 * kn[i];
+        o.d[9 + 3 * KS + i] = hostff::Y_D4 * kn[i];
+    }
+    out.push_back(o);
+    b.ref.s_n += length;
+}
+
+// FF_sbend::apply ff_sbend.h:741-969 (pure dipole: no k1..k5 / a_n b_n)
+static void ops_sbend(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
+{
+    const Element& ele = lat.elements[sl.elem];
+    double a = ele.get("angle");
+    double l = ele.get("l");
+    double length = sl.right - sl.left;
+    double angle = (length / l) * a;
+    bool ledge = sl.ledge, redge = sl.redge;
+    double e1 = ele.get("e1", 0.0), e2 = ele.get("e2", 0.0);
+    static const char* kn_names[10] = {"k1", "k1s", "k2", "k2s", "k3", "k3s", "k4", "k4s", "k5", "k5s"};
+    for (auto nm : kn_names)
+        if (ele.get(nm, 0.0) != 0.0)
+            throw Error(SB2_ERR_UNSUPPORTED, "combined-function sbend (bend_yoshida6) is not supported by this build");
+    for (int i = 1; i < 5; ++i) {
+        std::string an = "a0", bn = "b0";
+        an[1] = (char)('0' + i);
+        bn[1] = (char)('0' + i);
+        if (ele.get(an, 0.0) != 0.0 || ele.get(bn, 0.0) != 0.0)
+            throw Error(SB2_ERR_UNSUPPORTED, "sbend multipole errors are not supported by this build");
+    }
+    Refpart& ref_l = b.design;
+    const Refpart& ref_b = b.ref;
+    double scale = ref_l.p / (ref_b.p * (1.0 + ref_b.state[5]));
+    if (!redge) e2 = 0;
+    if (!ledge) e1 = 0;
+    const double cnv = 1.0e-9 * pc::c;
+    double pref_l = ref_l.p;
+    double brho_l = pref_l / cnv;
+    int charge_l = ref_l.charge;
+    double pref_b = ref_b.p;
+    double brho_b = pref_b / cnv;
+    double m_b = b.ref.mass;
+    double strength = brho_l * a / l;
+    double ce1 = std::cos(-e1), se1 = std::sin(-e1), ce2 = std::cos(-e2), se2 = std::sin(-e2);
+    double sgn = (charge_l > 0) ? 1.0 : -1.0;
+    double us_edge_k_p = sgn * strength / brho_b;
+    double ds_edge_k_p = -sgn * strength / brho_b;
+    double us_kx = 0, us_ky = 0, ds_kx = 0, ds_ky = 0;
+    double dphi = -(angle - (e1 + e2));
+    std::complex<double> phase = std::exp(std::complex<double>(0.0, -dphi));
+    std::complex<double> term = std::complex<double>(0.0, length / angle) *
+                                std::complex<double>(1.0 - std::cos(angle), -std::sin(angle)) *
+                                std::complex<double>(std::cos(e2), -std::sin(e2));
+    { // prop_reference ff_sbend.h:478-566
+        double m_l = ref_l.mass;
+        double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3];
+        double cdt = 0.0, dpop = 0.0;
+        if (ledge) {
+            hostff::slot_unit(x, xp, y, yp, cdt, dpop, ce1, se1, pref_l, m_l);
+            double p_l = 1.0 + dpop;
+            double zp = std::sqrt(p_l * p_l - xp * xp - yp * yp);
+            us_kx = us_edge_k_p * (xp / zp);
+            us_ky = us_edge_k_p * (yp / zp);
+            double kx = us_kx / scale, ky = us_ky / scale;
+            yp = yp - kx * y;
+            xp = xp + ky * y;
+        }
+        hostff::bend_complete(x, xp, y, yp, cdt, dpop, dphi, strength, pref_l, m_l, 0.0, phase, term);
+        if (redge) {
+            double p_l = 1.0 + dpop;
+            double zp = std::sqrt(p_l * p_l - xp * xp - yp * yp);
+            ds_kx = ds_edge_k_p * (xp / zp);
+            ds_ky = ds_edge_k_p * (yp / zp);
+            double kx = ds_kx / scale, ky = ds_ky / scale;
+            yp = yp - kx * y;
+            xp = xp + ky * y;
+            hostff::slot_unit(x, xp, y, yp, cdt, dpop, ce2, se2, pref_l, m_l);
+        }
+        ref_l.state = {x, xp, y, yp, cdt, dpop};
+        MapOp o = new_op(OP_SBEND);
+        o.flags = (ledge ? 1 : 0) | (redge ? 2 : 0);
+        o.d[0] = ce1; o.d[1] = se1; o.d[2] = ce2; o.d[3] = se2;
+        o.d[4] = us_kx; o.d[5] = us_ky; o.d[6] = ds_kx; o.d[7] = ds_ky;
+        o.d[8] = dphi; o.d[9] = phase.real(); o.d[10] = phase.imag();
+        o.d[11] = term.real(); o.d[12] = term.imag();
+        o.d[13] = strength; o.d[14] = pref_b; o.d[15] = m_b; o.d[16] = cdt;
+        out.push_back(o);
+    }
+    b.ref.s_n += length;
+}
+
+// FF_multipole::apply ff_multipole.h:85-210
+static void ops_multipole(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
+{
+    if (sl.right - sl.left > 0.0) throw Error(SB2_ERR_RUNTIME, "FF_multipole::apply() cannot deal with thick elements");
+    const Element& el = lat.elements[sl.elem];
+    const int max_order = 8;
+    std::vector<double> knl, ksl, tn;
+    if (el.v.count("knl") || el.v.count("ksl")) {
+        std::vector<double> k0(1, 0.0);
+        knl = el.v.count("knl") ? el.v.at("knl") : k0;
+        ksl = el.v.count("ksl") ? el.v.at("ksl") : k0;
+        if (knl.size() > ksl.size())
+            ksl.resize(knl.size(), 0.0);
+        else if (knl.size() < ksl.size())
+            knl.resize(ksl.size(), 0.0);
+        tn.resize(knl.size(), el.get("tilt", 0.0));
+    } else {
+        for (int i = 0; i < 6; ++i) {
+            std::string skn = "k0l", stn = "t0";
+            skn[1] = (char)('0' + i);
+            stn[1] = (char)('0' + i);
+            knl.push_back(el.get(skn, 0.0));
+            tn.push_back(el.get(stn, 0.0));
+        }
+        int tail = (int)knl.size() - 1;
+        while (tail && knl[tail] == 0.0) --tail;
+        knl.resize(tail + 1);
+        ksl.resize(knl.size(), 0.0);
+        tn.resize(knl.size(), 0.0);
+    }
+    if ((int)knl.size() > max_order) throw Error(SB2_ERR_UNSUPPORTED, "multipole order above 8");
+    for (size_t i = 0; i < knl.size(); ++i)
+        if (tn[i] != 0.0) {
+            std::complex<double> ck2(knl[i], ksl[i]);
+            ck2 = ck2 * std::exp(std::complex<double>(0.0, -(double)(i + 1) * tn[i]));
+            knl[i] = ck2.real();
+            ksl[i] = ck2.imag();
+        }
+    double scale = brho_scale(b);
+    for (size_t i = 0; i < knl.size(); ++i) {
+        knl[i] *= scale;
+        ksl[i] *= scale;
+    }
+    MapOp o = new_op(OP_MPOLE);
+    for (size_t i = 0; i < knl.size(); ++i) {
+        if (knl[i] || ksl[i]) o.flags |= (1 << i);
+        o.d[i * 2 + 0] = knl[i];
+        o.d[i * 2 + 1] = ksl[i];
+    }
+    Refpart& ref_l = b.design;
+    double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3], dpop = ref_l.state[5];
+    for (int n = 0; n < max_order; ++n)
+        if (o.flags & (1 << n)) hostff::thin_magnet(x, xp, y, yp, &o.d[n * 2], n + 1);
+    ref_l.state = {x, xp, y, yp, 0.0, dpop};
+    out.push_back(o);
+}
+
+// FF_sextupole::apply ff_sextupole.h:18-92 + ff_patterned_propagator.h
+static void ops_sextupole(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
+{
+    const Element& el = lat.elements[sl.elem];
+    double length = sl.right - sl.left;
+    double k[2] = {el.get("k2", 0.0), el.get("k2s", 0.0)};
+    double tilt = el.get("tilt", 0.0);
+    if (tilt != 0.0) {
+        std::complex<double> ck2(k[0], k[1]);
+        ck2 = ck2 * std::exp(std::complex<double>(0.0, -3.0 * tilt));
+        k[0] = ck2.real();
+        k[1] = ck2.imag();
+    }
+    double scale = brho_scale(b);
+    k[0] *= scale;
+    k[1] *= scale;
+    Refpart& ref_l = b.design;
+    if (hostff::close_to_zero(length)) {
+        double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3];
+        hostff::thin_sext(x, xp, y, yp, k);
+        ref_l.state[1] = xp;
+        ref_l.state[3] = yp;
+        ref_l.state[4] = 0.0;
+        MapOp o = new_op(OP_THIN_SEXT);
+        o.d[2] = k[0];
+        o.d[3] = k[1];
+        out.push_back(o);
+        return;
+    }
+    int steps = (int)el.get("yoshida_steps", 4.0);
+    double cdt = 0.0;
+    auto st = ref_l.state;
+    st[5] = 0.0;
+    double step_len = length / steps;
+    double step_str[2] = {k[0] * step_len, k[1] * step_len};
+    // yoshida<double, kf, 6, 1> ff_algorithm.h:1622-1646: n = (6 - 2) / 2
+    for (int i = 0; i < steps; ++i)
+        hostff::yoshida_element(2, st[0], st[1], st[2], st[3], cdt, st[5], ref_l.p, ref_l.mass, 0.0, step_len,
+                                step_str, 1.0, hostff::sext_kick_cb, 1);
+    st[4] = cdt;
+    ref_l.state = st;
+    double step_ref_cdt = cdt / steps;
+    MapOp o = new_op(OP_SEXT_YOSHIDA);
+    o.steps = steps;
+    o.d[2] = b.ref.p;
+    o.d[3] = b.ref.mass;
+    o.d[4] = step_ref_cdt * 0.1;
+    o.d[5] = hostff::Y_C1 * step_len;
+    o.d[6] = hostff::Y_C2 * step_len;
+    o.d[7] = hostff::Y_C3 * step_len;
+    o.d[8] = hostff::Y_C4 * step_len;
+    for (int i = 0; i < 2; ++i) {
+        o.d[9 + i] = hostff::Y_D1 * step_str[i];
+        o.d[11 + i] = hostff::Y_D2 * step_str[i];
+        o.d[13 + i] = hostff::Y_D3 * step_str[i];
+        o.d[15 + i] = hostff::Y_D4 * step_str[i];
+    }
+    out.push_back(o);
+    b.ref.s_n += length;
+}
+
+// FF_element::apply ff_element.h:25-67
+static void ops_slice(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
+{
+    const std::string& t = lat.elements[sl.elem].type;
+    if (t == "drift" || t == "monitor" || t == "hmonitor" || t == "vmonitor" || t == "marker" || t == "instrument" ||
+        t == "rcollimator")
+        ops_drift(sl, b, out);
+    else if (t == "sbend")
+        ops_sbend(lat, sl, b, out);
+    else if (t == "quadrupole")
+        ops_quad(lat, sl, b, out);
+    else if (t == "multipole")
+        ops_multipole(lat, sl, b, out);
+    else if (t == "sextupole")
+        ops_sextupole(lat, sl, b, out);
+    else if (t == "octupole" || t == "hkicker" || t == "vkicker" || t == "kicker" || t == "solenoid" ||
+             t == "rfcavity" || t == "elens" || t == "nllens" || t == "foil" || t == "dipedge" || t == "matrix")
+        throw Error(SB2_ERR_UNSUPPORTED, "element type " + t + " is not on the GPU path of this build (element " +
+                                             lat.elements[sl.elem].name + ")");
+    else
+        throw Error(SB2_ERR_RUNTIME, "FF_element::apply() unknown element type = " + t + ", element name = " +
+                                         lat.elements[sl.elem].name);
+}
+
+// Aperture_operation constructors (aperture_operation.h)
+static MapOp op_aperture(const Lattice& lat, const std::string& type, const Slice& sl)
+{
+    const Element& el = lat.elements[sl.elem];
+    if (type == "finite") return new_op(OP_AP_FINITE);
+    if (type == "circular") {
+        MapOp o = new_op(OP_AP_CIRCULAR);
+        double r = el.get("circular_aperture_radius", 1000.0);
+        o.d[0] = r * r;
+        o.d[1] = el.get("hoffset", 0.0);
+        o.d[2] = el.get("voffset", 0.0);
+        return o;
+    }
+    if (type == "elliptical") {
+        MapOp o = new_op(OP_AP_ELLIPTICAL);
+        double hr = el.get("elliptical_aperture_horizontal_radius");
+        double vr = el.get("elliptical_aperture_vertical_radius");
+        o.d[0] = hr * hr;
+        o.d[1] = vr * vr;
+        o.d[2] = el.get("hoffset", 0.0);
+        o.d[3] = el.get("voffset", 0.0);
+        return o;
+    }
+    if (type == "rectangular") {
+        MapOp o = new_op(OP_AP_RECTANGULAR);
+        o.d[0] = el.get("rectangular_aperture_width");
+        o.d[1] = el.get("rectangular_aperture_height");
+        o.d[2] = el.get("hoffset", 0.0);
+        o.d[3] = el.get("voffset", 0.0);
+        return o;
+    }
+    throw Error(SB2_ERR_RUNTIME, "unknown aperture_type " + type);
+}
+
+
+// ---------------------------------------------------------------------------
+// Kernel-category timing with CUDA events on the launching stream (the
+// reference's scoped_simple_timer labels, utils/simple_timer.h:50-66).
+// Off unless sb2_profile_enable(1) is called.
+// ---------------------------------------------------------------------------
+enum ProfCat { PROF_TRACK = 0, PROF_DOMAIN, PROF_DEPOSIT, PROF_GREEN, PROF_SOLVE, PROF_EFIELD, PROF_NCAT };
+static const char* kProfNames[PROF_NCAT] = {"track", "domain", "deposit", "green", "solve", "efield"};
+
+struct Profiler {
+    bool on = false;
+    struct Rec {
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs[PROF_NCAT];
+    std::vector<cudaEvent_t> pool;
+    double total_ms[PROF_NCAT] = {0};
+    int64_t count[PROF_NCAT] = {0};
+
+    cudaEvent_t ev()
+    {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        cuda_check(cudaEventCreate(&e), "event");
+        return e;
+    }
+    Rec begin(int cat, cudaStream_t s)
+    {
+        (void)cat;
+        Rec r{ev(), nullptr};
+        cuda_check(cudaEventRecord(r.a, s), "event");
+        return r;
+    }
+    void end(int cat, Rec r, cudaStream_t s)
+    {
+        r.b = ev();
+        cuda_check(cudaEventRecord(r.b, s), "event");
+        recs[cat].push_back(r);
+    }
+    void collect()
+    {
+        for (int c = 0; c < PROF_NCAT; ++c) {
+            for (auto& r : recs[c]) {
+                cuda_check(cudaEventSynchronize(r.b), "event");
+                float ms = 0;
+                cuda_check(cudaEventElapsedTime(&ms, r.a, r.b), "event");
+                total_ms[c] += ms;
+                count[c] += 1;
+                pool.push_back(r.a);
+                pool.push_back(r.b);
+            }
+            recs[c].clear();
+        }
+    }
+    void reset()
+    {
+        collect();
+        for (int c = 0; c < PROF_NCAT; ++c) {
+            total_ms[c] = 0;
+            count[c] = 0;
+        }
+    }
+};
+static Profiler g_prof;
+
+struct ProfScope {
+    int cat;
+    cudaStream_t s;
+    Profiler::Rec r{};
+    ProfScope(int c, cudaStream_t st) : cat(c), s(st)
+    {
+        if (g_prof.on) r = g_prof.begin(cat, s);
+    }
+    ~ProfScope()
+    {
+        if (g_prof.on && r.a) g_prof.end(cat, r, s);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Space-charge operator: options, workspaces, solve
+// ---------------------------------------------------------------------------
+static bool is_pow2(int v) { return v > 1 && (v & (v - 1)) == 0; }
+static int ilog2(int v)
+{
+    int l = 0;
+    while ((1 << l) < v) ++l;
+    return l;
+}
+
+template <typename T>
+static T* dalloc(size_t count, const char* what)
+{
+    void* p = nullptr;
+    cuda_check(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)), what);
+    return (T*)p;
+}
+
+struct SpaceCharge {
+    sb2_sc3d_options o;
+    Dims d{};
+    int64_t G = 0;
+    double* rho = nullptr;
+    double2* S = nullptr;
+    double* ghat = nullptr;
+    double* phi = nullptr;
+    double2* E = nullptr;
+    double2 *tw_x = nullptr, *tw_y = nullptr, *tw_z = nullptr;
+    ScState* state = nullptr;
+    double* mom_partials = nullptr;
+    int n_partials = 0;
+    bool ghat_valid = false;
+
+    // Option checks done at construction, before any device allocation.
+    static void validate(const sb2_sc3d_options& o)
+    {
+        for (int i = 0; i < 3; ++i) {
+            if (o.shape[i] < 3) throw Error(SB2_ERR_INVALID, "space-charge grid shape must be >= 3 in each dimension");
+            if (o.doubled_shape[i] != 2 * o.shape[i])
+                throw Error(SB2_ERR_UNSUPPORTED, "doubled_shape must be 2 * shape on the GPU path");
+            if (!is_pow2(o.doubled_shape[i]) || o.doubled_shape[i] < 8 || o.doubled_shape[i] > 4096)
+                throw Error(SB2_ERR_UNSUPPORTED, "doubled grid sizes must be powers of two in [8, 4096] on the GPU path");
+        }
+        if (o.periodic_z)
+            throw Error(SB2_ERR_RUNTIME, "Space_charge_3d_open_hockney::get_green_fn2_linear: periodic_z not yet implemented");
+        if (o.precision != SB2_PRECISION_FP64 && o.precision != SB2_PRECISION_MIXED)
+            throw Error(SB2_ERR_INVALID, "unknown precision");
+        if (o.domain_fixed)
+            for (int i = 0; i < 3; ++i)
+                if (!(o.size[i] > 0.0)) throw Error(SB2_ERR_INVALID, "fixed domain size must be > 0");
+    }
+
+    explicit SpaceCharge(const sb2_sc3d_options& opts) : o(opts)
+    {
+        validate(o);
+        d.gx = o.shape[0];
+        d.gy = o.shape[1];
+        d.gz = o.shape[2];
+        d.nx = o.doubled_shape[0];
+        d.ny = o.doubled_shape[1];
+        d.nz = o.doubled_shape[2];
+        d.nkx = d.nx / 2 + 1;
+        d.nkxp = (d.nkx + 1) & ~1;
+        d.lx = ilog2(d.nx);
+        d.ly = ilog2(d.ny);
+        d.lz = ilog2(d.nz);
+        G = (int64_t)d.gx * d.gy * d.gz;
+        rho = dalloc<double>(G, "rho");
+        phi = dalloc<double>(G, "phi");
+        E = dalloc<double2>(2 * G, "E");
+        S = dalloc<double2>((size_t)d.nz * d.ny * d.nkxp, "spectrum");
+        ghat = dalloc<double>((size_t)(d.nx / 2 + 1) * (d.ny / 2 + 1) * (d.nz / 2 + 1), "ghat");
+        state = dalloc<ScState>(1, "sc state");
+        n_partials = track_grid_blocks();
+        mom_partials = dalloc<double>((size_t)n_partials * 6, "moments");
+        cuda_check(cudaMemset(state, 0, sizeof(ScState)), "memset");
+        cuda_check(cudaMemset(E, 0, sizeof(double2) * 2 * G), "memset");
+        tw_x = twiddles(d.nx);
+        tw_y = twiddles(d.ny);
+        tw_z = twiddles(d.nz);
+    }
+    ~SpaceCharge()
+    {
+        cudaFree(rho);
+        cudaFree(phi);
+        cudaFree(E);
+        cudaFree(S);
+        cudaFree(ghat);
+        cudaFree(state);
+        cudaFree(mom_partials);
+        cudaFree(tw_x);
+        cudaFree(tw_y);
+        cudaFree(tw_z);
+    }
+    static double2* twiddles(int L)
+    {
+        std::vector<double2> h(L / 2);
+        for (int k = 0; k < L / 2; ++k) {
+            long double a = -2.0L * 3.14159265358979323846264338327950288L * k / L;
+            h[k] = make_double2((double)std::cos(a), (double)std::sin(a));
+        }
+        double2* dp = dalloc<double2>(L / 2, "twiddles");
+        cuda_check(cudaMemcpy(dp, h.data(), sizeof(double2) * (L / 2), cudaMemcpyHostToDevice), "twiddles");
+        return dp;
+    }
+
+    DomainParams domain_params(const Bunch& b, double time_step) const
+    {
+        DomainParams p;
+        std::memset(&p, 0, sizeof(p));
+        p.counters = b.counters;
+        p.moment_partials = mom_partials;
+        p.n_partials = n_partials;
+        p.compute_domain = 1;
+        p.sc = state;
+        for (int i = 0; i < 3; ++i) {
+            p.g[i] = o.shape[i];
+            p.dg[i] = o.doubled_shape[i];
+            p.fixed_size[i] = o.size[i];
+            p.fixed_offset[i] = o.offset[i];
+        }
+        p.domain_fixed = o.domain_fixed;
+        p.grid_entire_period = o.grid_entire_period;
+        p.green_linear = o.green_fn == SB2_GREEN_LINEAR;
+        p.n_sigma = o.n_sigma;
+        p.z_period = o.z_period;
+        p.kick_scale = o.kick_scale;
+        p.charge = b.ref.charge;
+        p.pref = b.ref.p;
+        p.gamma = b.ref.gamma;
+        p.beta = b.ref.beta;
+        p.time_step = time_step;
+        return p;
+    }
+
+    // deposit -> Ghat (if needed) -> convolution -> E; the domain is already
+    // in `state`.
+    void solve(const Bunch& b, cudaStream_t s)
+    {
+        {
+            ProfScope ps(PROF_DEPOSIT, s);
+            cuda_check(cudaMemsetAsync(rho, 0, sizeof(double) * G, s), "memset rho");
+            cuda_check(launch_deposit(b.parts, b.stride, b.masks, b.n, state, rho, d.gx, d.gy, d.gz, s), "deposit");
+        }
+        if (!o.domain_fixed || !ghat_valid) {
+            ProfScope ps(PROF_GREEN, s);
+            cuda_check(launch_green(state, ghat, d, o.green_fn == SB2_GREEN_LINEAR, tw_x, tw_y, tw_z, s), "green");
+            ghat_valid = true;
+        }
+        {
+            ProfScope ps(PROF_SOLVE, s);
+            cuda_check(launch_convolve(rho, S, ghat, phi, d, tw_x, tw_y, tw_z, state, s), "convolve");
+        }
+        {
+            ProfScope ps(PROF_EFIELD, s);
+            cuda_check(launch_efield(phi, E, d.gx, d.gy, d.gz, state, s), "efield");
+        }
+    }
+
+    void copy_last(double* left, double* h, double* rho_o, double* phi_o, double* ex, double* ey, double* ez,
+                   double* scalars)
+    {
+        ScState st;
+        cuda_check(cudaMemcpy(&st, state, sizeof(st), cudaMemcpyDeviceToHost), "state");
+        if (left)
+            for (int i = 0; i < 3; ++i) left[i] = st.left[i];
+        if (h)
+            for (int i = 0; i < 3; ++i) h[i] = st.h[i];
+        if (rho_o) cuda_check(cudaMemcpy(rho_o, rho, sizeof(double) * G, cudaMemcpyDeviceToHost), "rho");
+        if (phi_o) cuda_check(cudaMemcpy(phi_o, phi, sizeof(double) * G, cudaMemcpyDeviceToHost), "phi");
+        if (ex || ey || ez) {
+            std::vector<double2> e(2 * G);
+            cuda_check(cudaMemcpy(e.data(), E, sizeof(double2) * 2 * G, cudaMemcpyDeviceToHost), "E");
+            for (int64_t i = 0; i < G; ++i) {
+                if (ex) ex[i] = e[2 * i].x;
+                if (ey) ey[i] = e[2 * i].y;
+                if (ez) ez[i] = e[2 * i + 1].x;
+            }
+        }
+        if (scalars) {
+            scalars[0] = st.fn_norm;
+            scalars[1] = st.factor;
+            for (int j = 0; j < 6; ++j) scalars[2 + j] = st.mean_std[j];
+        }
+    }
+
+    void check_error()
+    {
+        ScState st;
+        cuda_check(cudaMemcpy(&st, state, sizeof(st), cudaMemcpyDeviceToHost), "state");
+        if (st.error == 1)
+            throw Error(SB2_ERR_RUNTIME, "Space_charge_3d_open_hockney_eigen::update_domain: all three spatial "
+                                         "dimensions have neglible extent");
+    }
+};
+
+
+// ---------------------------------------------------------------------------
+// Engine: accumulates the particle-local ops of consecutive operators and
+// launches them as fused particle passes (one read + one write of the
+// particle array per pass), followed by the bookkeeping/domain kernel.
+// ---------------------------------------------------------------------------
+struct Engine {
+    int32_t* ap_counts = nullptr;
+    std::vector<MapOp> ops;
+    PassBook book{};
+    int nslots = 0;
+
+    Engine()
+    {
+        ap_counts = dalloc<int32_t>(kMaxSlotsPerPass, "aperture counters");
+        cuda_check(cudaMemset(ap_counts, 0, sizeof(int32_t) * kMaxSlotsPerPass), "memset");
+        reset();
+    }
+    ~Engine() { cudaFree(ap_counts); }
+    void reset()
+    {
+        ops.clear();
+        std::memset(&book, 0, sizeof(book));
+        nslots = 0;
+    }
+
+    // One independent operator: its libFF groups and apertures, then
+    // update_total_num (independent_operator.cc:94-133).
+    void add_operator(const Lattice& lat, const IndepOperator& op, Bunch& b, SpaceCharge* sc, double* elem_charge,
+                      cudaStream_t s)
+    {
+        int naps = 0;
+        for (auto const& o : op.ops) naps += o.aperture ? 1 : 0;
+        if (naps > kMaxSlotsPerPass) throw Error(SB2_ERR_UNSUPPORTED, "too many apertures in one operator");
+        if (book.n_operators == kMaxOperatorsPerPass || nslots + naps > kMaxSlotsPerPass)
+            flush(b, sc, elem_charge, false, 0.0, s);
+        int first = nslots;
+        for (auto const& o : op.ops) {
+            if (o.aperture) {
+                MapOp m = op_aperture(lat, o.ap_type, o.ap_slice);
+                m.slot = nslots;
+                book.slot_elem[nslots] = o.ap_slice.elem;
+                ++nslots;
+                ops.push_back(m);
+            } else {
+                for (auto const& sl : o.group) ops_slice(lat, sl, b, ops);
+            }
+        }
+        book.slot_begin[book.n_operators] = first;
+        book.slot_end[book.n_operators] = nslots;
+        ++book.n_operators;
+    }
+
+    void add_kick() { ops.push_back(new_op(OP_SC_KICK)); }
+
+    // Launch the pending ops.  with_domain: append the moment sums and run
+    // the domain computation for a space-charge kick of `time_step`.
+    void flush(Bunch& b, SpaceCharge* sc, double* elem_charge, bool with_domain, double time_step, cudaStream_t s)
+    {
+        if (with_domain && !sc->o.domain_fixed) ops.push_back(new_op(OP_MOMENTS));
+        size_t i = 0;
+        while (i < ops.size()) {
+            size_t n = std::min<size_t>(kMaxOpsPerPass, ops.size() - i);
+            TrackParams tp;
+            std::memset(&tp, 0, offsetof(TrackParams, ops));
+            tp.parts = b.parts;
+            tp.stride = b.stride;
+            tp.masks = b.masks;
+            tp.discards = b.discards;
+            tp.n = b.n;
+            tp.ap_counts = ap_counts;
+            tp.nops = (int32_t)n;
+            tp.slot_base = -1;
+            bool has_mom = false;
+            for (size_t k = 0; k < n; ++k) {
+                const MapOp& m = ops[i + k];
+                tp.ops[k] = m;
+                if (m.kind >= OP_AP_FINITE && m.kind <= OP_AP_RECTANGULAR) {
+                    tp.write_discards = 1;
+                    if (tp.slot_base < 0) tp.slot_base = m.slot;
+                }
+                if (m.kind == OP_MOMENTS) has_mom = true;
+            }
+            if (tp.slot_base < 0) tp.slot_base = 0;
+            if (sc) {
+                tp.sc = sc->state;
+                tp.efield = sc->E;
+                tp.gx = sc->d.gx;
+                tp.gy = sc->d.gy;
+                tp.gz = sc->d.gz;
+                tp.kick_pref = b.ref.p;
+                tp.kick_m = b.ref.mass;
+                if (has_mom) tp.moment_partials = sc->mom_partials;
+            }
+            {
+                ProfScope ps(PROF_TRACK, s);
+                cuda_check(launch_track(tp, s), "track kernel");
+            }
+            i += n;
+        }
+        if (book.n_operators > 0 || with_domain) {
+            DomainParams dp;
+            if (with_domain)
+                dp = sc->domain_params(b, time_step);
+            else {
+                std::memset(&dp, 0, sizeof(dp));
+                dp.counters = b.counters;
+            }
+            dp.ap_counts = ap_counts;
+            dp.elem_charge = elem_charge;
+            dp.book = book;
+            ProfScope ps(PROF_DOMAIN, s);
+            cuda_check(launch_book_domain(dp, s), "domain kernel");
+        }
+        reset();
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Propagator
+// ---------------------------------------------------------------------------
+struct Propagator {
+    Lattice lat;
+    int stepper = 0, num = 1;
+    std::vector<Step> steps;
+    bool has_sc = false;
+    sb2_sc3d_options sc_opts{};
+    // device resources, allocated on first propagate
+    std::unique_ptr<SpaceCharge> sc;
+    std::unique_ptr<Engine> engine_;
+    double* elem_charge = nullptr;
+
+    Propagator(const Lattice& l, int stepper_kind, int n, const sb2_sc3d_options* opts)
+        : lat(l), stepper(stepper_kind), num(n)
+    {
+        if (!lat.has_ref) throw Error(SB2_ERR_INVALID, "lattice has no reference particle");
+        if (opts) {
+            SpaceCharge::validate(*opts);
+            sc_opts = *opts;
+            has_sc = true;
+        }
+        steps = make_steps(lat, stepper, num, has_sc);
+    }
+    ~Propagator() { cudaFree(elem_charge); }
+
+    void ensure_device()
+    {
+        if (!engine_) engine_.reset(new Engine());
+        if (has_sc && !sc) sc.reset(new SpaceCharge(sc_opts));
+        if (!elem_charge) {
+            elem_charge = dalloc<double>(lat.elements.size(), "element charge");
+            cuda_check(cudaMemset(elem_charge, 0, sizeof(double) * std::max<size_t>(1, lat.elements.size())), "memset");
+        }
+    }
+
+    void begin(Bunch& b)
+    { // do_before_start propagator.cc:8-23
+        ensure_device();
+        if (b.turns_done == 0 && !b.design_set) {
+            b.design = lat.ref;
+            b.design_set = true;
+        }
+    }
+
+    void run_step(Bunch& b, const Step& st, cudaStream_t s)
+    { // Step::apply step.cc:44-79
+        double time = st.length / (b.ref.beta * pc::c);
+        size_t ii = 0;
+        for (char item : st.items) {
+            if (item == 'I') {
+                engine_->add_operator(lat, st.indeps[ii++], b, sc.get(), elem_charge, s);
+            } else if (sc) {
+                engine_->flush(b, sc.get(), elem_charge, true, time * 1.0, s);
+                sc->solve(b, s);
+                engine_->add_kick();
+            }
+        }
+    }
+
+    void finish(Bunch& b, cudaStream_t s)
+    {
+        engine_->flush(b, sc.get(), elem_charge, false, 0.0, s);
+        b.sync_counters(s);
+        if (sc) sc->check_error();
+    }
+
+    void propagate(Bunch& b, int turns, cudaStream_t s)
+    { // Propagator::propagate propagator.cc:157-283 (one bunch, no diagnostics)
+        begin(b);
+        for (int t = 0; t < turns; ++t) {
+            b.ref.start_repetition(); // do_start_repetition propagator.cc:25-34
+            for (auto const& st : steps) run_step(b, st, s);
+            b.turns_done += 1;
+        }
+        finish(b, s);
+    }
+
+    void propagate_steps(Bunch& b, int first, int count, cudaStream_t s)
+    {
+        begin(b);
+        const int ns = (int)steps.size();
+        for (int k = first; k < first + count; ++k) {
+            int si = ((k % ns) + ns) % ns;
+            if (si == 0) b.ref.start_repetition();
+            run_step(b, steps[si], s);
+            if (si == ns - 1) b.turns_done += 1;
+        }
+        finish(b, s);
+    }
+};
+
+// Standalone collective operator (space_charge_3d_open_hockney.cc:400-453)
+struct ScOperator {
+    SpaceCharge sc;
+    Engine engine;
+    explicit ScOperator(const sb2_sc3d_options& o) : sc(o) {}
+    void apply(Bunch& b, double time_step, cudaStream_t s)
+    {
+        engine.flush(b, &sc, nullptr, true, time_step, s);
+        sc.solve(b, s);
+        engine.add_kick();
+        engine.flush(b, &sc, nullptr, false, 0.0, s);
+        cuda_check(cudaStreamSynchronize(s), "sync");
+        sc.check_error();
+    }
+};
+
+} // namespace sb2
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace sb2;
+
+struct sb2_bunch {
+    Bunch b;
+};
+struct sb2_lattice {
+    Lattice l;
+};
+struct sb2_propagator {
+    std::unique_ptr<Propagator> p;
+};
+struct sb2_sc3d {
+    std::unique_ptr<ScOperator> op;
+};
+
+static thread_local std::string g_last_error;
+
+#define SB2_TRY try {
+#define SB2_CATCH                                                                                                  \
+    }                                                                                                              \
+    catch (const Error& ex)                                                                                        \
+    {                                                                                                              \
+        g_last_error = ex.what();                                                                                  \
+        return ex.code;                                                                                            \
+    }                                                                                                              \
+    catch (const std::bad_alloc&)                                                                                  \
+    {                                                                                                              \
+        g_last_error = "host allocation failed";                                                                   \
+        return SB2_ERR_NOMEM;                                                                                      \
+    }                                                                                                              \
+    catch (const std::exception& ex)                                                                               \
+    {                                                                                                              \
+        g_last_error = ex.what();                                                                                  \
+        return SB2_ERR_RUNTIME;                                                                                    \
+    }                                                                                                              \
+    return SB2_OK;
+
+#define SB2_REQUIRE(cond, msg)                                                                                     \
+    if (!(cond)) throw Error(SB2_ERR_INVALID, msg)
+
+static cudaStream_t as_stream(void* s) { return (cudaStream_t)s; }
+
+extern "C" {
+
+const char* sb2_last_error(void) { return g_last_error.c_str(); }
+const char* sb2_version(void) { return "synergia2_b200 0.1 (sm_100a)"; }
+
+sb2_status sb2_profile_enable(int32_t on)
+{
+    SB2_TRY
+    g_prof.on = on != 0;
+    SB2_CATCH
+}
+
+sb2_status sb2_profile_read(int32_t category, const char** name, double* total_ms, int64_t* launches, int32_t reset)
+{
+    SB2_TRY
+    SB2_REQUIRE(category >= 0 && category < PROF_NCAT, "bad profile category");
+    g_prof.collect();
+    if (name) *name = kProfNames[category];
+    if (total_ms) *total_ms = g_prof.total_ms[category];
+    if (launches) *launches = g_prof.count[category];
+    if (reset) {
+        g_prof.total_ms[category] = 0;
+        g_prof.count[category] = 0;
+    }
+    SB2_CATCH
+}
+
+sb2_status sb2_sc3d_options_init(sb2_sc3d_options* o, int gx, int gy, int gz)
+{
+    SB2_TRY
+    SB2_REQUIRE(o, "null options");
+    std::memset(o, 0, sizeof(*o));
+    o->shape[0] = gx;
+    o->shape[1] = gy;
+    o->shape[2] = gz;
+    o->doubled_shape[0] = gx * 2;
+    o->doubled_shape[1] = gy * 2;
+    o->doubled_shape[2] = gz * 2;
+    o->green_fn = SB2_GREEN_LINEAR;
+    o->n_sigma = 8.0;
+    o->kick_scale = 1.0;
+    o->comm_group_size = 4;
+    o->precision = SB2_PRECISION_FP64;
+    SB2_CATCH
+}
+
+sb2_status sb2_sc3d_options_set_fixed_domain(sb2_sc3d_options* o, const double offset[3], const double size[3])
+{ // implemented_collective_options.h:97-108
+    SB2_TRY
+    SB2_REQUIRE(o && offset && size, "null argument");
+    for (int i = 0; i < 3; ++i) {
+        o->offset[i] = offset[i];
+        o->size[i] = size[i];
+    }
+    o->domain_fixed = 1;
+    SB2_CATCH
+}
+
+static void bunch_alloc_counters(Bunch& b, double real_num)
+{
+    b.counters = dalloc<BunchCounters>(1, "counters");
+    b.host_counters.n_valid = (int32_t)b.n;
+    b.host_counters.n_total = (int32_t)b.n;
+    b.host_counters.real_num = real_num;
+    cuda_check(cudaMemcpy(b.counters, &b.host_counters, sizeof(BunchCounters), cudaMemcpyHostToDevice), "counters");
+}
+
+sb2_status sb2_bunch_create(int32_t charge, double mass, double value, int32_t kind, int64_t n, double real_num,
+                            sb2_bunch** out)
+{
+    SB2_TRY
+    SB2_REQUIRE(out && n >= 0 && n < (int64_t)INT32_MAX, "bad bunch size");
+    auto* h = new sb2_bunch();
+    std::unique_ptr<sb2_bunch> guard(h);
+    Bunch& b = h->b;
+    cuda_check(cudaGetDevice(&b.device), "device");
+    b.ref.set(charge, mass, value, kind);
+    b.n = n;
+    b.stride = n;
+    b.owns = true;
+    b.parts = dalloc<double>((size_t)7 * n, "particles");
+    b.masks = dalloc<uint8_t>(n, "masks");
+    b.discards = dalloc<uint8_t>(n, "discards");
+    cuda_check(cudaMemset(b.parts, 0, sizeof(double) * 7 * std::max<int64_t>(n, 1)), "memset");
+    cuda_check(cudaMemset(b.masks, 1, std::max<int64_t>(n, 1)), "memset");
+    cuda_check(cudaMemset(b.discards, 0, std::max<int64_t>(n, 1)), "memset");
+    if (n) { // ids 0..n-1 (bunch_particles.cc:283-300)
+        std::vector<double> ids(n);
+        for (int64_t i = 0; i < n; ++i) ids[i] = (double)i;
+        cuda_check(cudaMemcpy(b.parts + 6 * n, ids.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "ids");
+    }
+    bunch_alloc_counters(b, real_num);
+    *out = guard.release();
+    SB2_CATCH
+}
+
+sb2_status sb2_bunch_wrap(int32_t charge, double mass, double value, int32_t kind, double* parts, int64_t stride,
+                          uint8_t* masks, uint8_t* discards, int64_t n, double real_num, sb2_bunch** out)
+{
+    SB2_TRY
+    SB2_REQUIRE(out && parts && masks && stride >= n && n >= 0, "bad wrapped bunch");
+    auto* h = new sb2_bunch();
+    std::unique_ptr<sb2_bunch> guard(h);
+    Bunch& b = h->b;
+    cuda_check(cudaGetDevice(&b.device), "device");
+    b.ref.set(charge, mass, value, kind);
+    b.n = n;
+    b.stride = stride;
+    b.parts = parts;
+    b.masks = masks;
+    b.discards = discards;
+    b.owns = false;
+    bunch_alloc_counters(b, real_num);
+    // count valid particles
+    std::vector<uint8_t> m(n);
+    if (n) cuda_check(cudaMemcpy(m.data(), masks, n, cudaMemcpyDeviceToHost), "masks");
+    int64_t nv = 0;
+    for (auto v : m) nv += v ? 1 : 0;
+    b.host_counters.n_valid = b.host_counters.n_total = (int32_t)nv;
+    cuda_check(cudaMemcpy(b.counters, &b.host_counters, sizeof(BunchCounters), cudaMemcpyHostToDevice), "counters");
+    *out = guard.release();
+    SB2_CATCH
+}
+
+sb2_status sb2_bunch_destroy(sb2_bunch* b)
+{
+    SB2_TRY
+    delete b;
+    SB2_CATCH
+}
+
+sb2_status sb2_bunch_set_particles(sb2_bunch* h, const double* host_parts, const uint8_t* host_masks)
+{
+    SB2_TRY
+    SB2_REQUIRE(h && host_parts, "null argument");
+    Bunch& b = h->b;
+    if (b.n == 0) return SB2_OK;
+    cuda_check(cudaMemcpy2D(b.parts, sizeof(double) * b.stride, host_parts, sizeof(double) * b.n,
+                            sizeof(double) * b.n, 7, cudaMemcpyHostToDevice),
+               "checkin");
+    int64_t nv = b.n;
+    if (host_masks) {
+        cuda_check(cudaMemcpy(b.masks, host_masks, b.n, cudaMemcpyHostToDevice), "masks");
+        nv = 0;
+        for (int64_t i = 0; i < b.n; ++i) nv += host_masks[i] ? 1 : 0;
+    } else {
+        cuda_check(cudaMemset(b.masks, 1, b.n), "masks");
+    }
+    cuda_check(cudaMemcpy(&b.host_counters, b.counters, sizeof(BunchCounters), cudaMemcpyDeviceToHost), "counters");
+    b.host_counters.n_valid = b.host_counters.n_total = (int32_t)nv;
+    cuda_check(cudaMemcpy(b.counters, &b.host_counters, sizeof(BunchCounters), cudaMemcpyHostToDevice), "counters");
+    SB2_CATCH
+}
+
+sb2_status sb2_bunch_get_particles(sb2_bunch* h, double* host_parts, uint8_t* host_masks, uint8_t* host_discards)
+{
+    SB2_TRY
+    SB2_REQUIRE(h, "null bunch");
+    Bunch& b = h->b;
+    if (b.n == 0) return SB2_OK;
+    if (host_parts)
+        cuda_check(cudaMemcpy2D(host_parts, sizeof(double) * b.n, b.parts, sizeof(double) * b.stride,
+                                sizeof(double) * b.n, 7, cudaMemcpyDeviceToHost),
+                   "checkout");
+    if (host_masks) cuda_check(cudaMemcpy(host_masks, b.masks, b.n, cudaMemcpyDeviceToHost), "masks");
+    if (host_discards) {
+        if (b.discards)
+            cuda_check(cudaMemcpy(host_discards, b.discards, b.n, cudaMemcpyDeviceToHost), "discards");
+        else
+            std::memset(host_discards, 0, b.n);
+    }
+    SB2_CATCH
+}
+
+sb2_status sb2_bunch_device_arrays(sb2_bunch* h, double** parts, int64_t* stride, uint8_t** masks, uint8_t** discards)
+{
+    SB2_TRY
+    SB2_REQUIRE(h, "null bunch");
+    if (parts) *parts = h->b.parts;
+    if (stride) *stride = h->b.stride;
+    if (masks) *masks = h->b.masks;
+    if (discards) *discards = h->b.discards;
+    SB2_CATCH
+}
+
+sb2_status sb2_bunch_counts(sb2_bunch* h, int64_t* n_active, int64_t* n_valid, int64_t* n_total, double* real_num)
+{
+    SB2_TRY
+    SB2_REQUIRE(h, "null bunch");
+    Bunch& b = h->b;
+    cuda_check(cudaMemcpy(&b.host_counters, b.counters, sizeof(BunchCounters), cudaMemcpyDeviceToHost), "counters");
+    if (n_active) *n_active = b.n;
+    if (n_valid) *n_valid = b.host_counters.n_valid;
+    if (n_total) *n_total = b.host_counters.n_total;
+    if (real_num) *real_num = b.host_counters.real_num;
+    SB2_CATCH
+}
+
+sb2_status sb2_bunch_design_state(sb2_bunch* h, double state[6], double* s_n)
+{
+    SB2_TRY
+    SB2_REQUIRE(h, "null bunch");
+    if (state)
+        for (int i = 0; i < 6; ++i) state[i] = h->b.design.state[i];
+    if (s_n) *s_n = h->b.ref.s_n;
+    SB2_CATCH
+}
+
+sb2_status sb2_bunch_populate_gaussian(sb2_bunch* h, const double sigma[6], uint64_t seed)
+{
+    SB2_TRY
+    SB2_REQUIRE(h && sigma, "null argument");
+    Bunch& b = h->b;
+    if (b.n) cuda_check(launch_populate(b.parts, b.stride, b.masks, b.n, sigma, seed, 0), "populate");
+    cuda_check(cudaDeviceSynchronize(), "populate");
+    b.host_counters.n_valid = b.host_counters.n_total = (int32_t)b.n;
+    cuda_check(cudaMemcpy(&b.host_counters.real_num, &b.counters->real_num, sizeof(double), cudaMemcpyDeviceToHost),
+               "counters");
+    cuda_check(cudaMemcpy(b.counters, &b.host_counters, sizeof(BunchCounters), cudaMemcpyHostToDevice), "counters");
+    SB2_CATCH
+}
+
+sb2_status sb2_bunch_moments(sb2_bunch* h, double mean[6], double mom2[36], double emit[3])
+{ // Core_diagnostics::calculate_mean / calculate_mom2, calculate_emittances
+    SB2_TRY
+    SB2_REQUIRE(h, "null bunch");
+    Bunch& b = h->b;
+    const int nb = track_grid_blocks();
+    double* part = dalloc<double>((size_t)nb * 27, "moment partials");
+    double* dmean = dalloc<double>(6, "mean");
+    std::vector<double> hp((size_t)nb * 27);
+    cuda_check(cudaMemcpy(&b.host_counters, b.counters, sizeof(BunchCounters), cudaMemcpyDeviceToHost), "counters");
+    double nt = b.host_counters.n_total;
+    double mu[6] = {0, 0, 0, 0, 0, 0};
+    cuda_check(launch_moments(b.parts, b.stride, b.masks, b.n, nullptr, part, nb, 0), "moments");
+    cuda_check(cudaMemcpy(hp.data(), part, sizeof(double) * nb * 27, cudaMemcpyDeviceToHost), "moments");
+    for (int k = 0; k < nb; ++k)
+        for (int j = 0; j < 6; ++j) mu[j] += hp[(size_t)k * 27 + j];
+    for (int j = 0; j < 6; ++j) mu[j] /= nt;
+    cuda_check(cudaMemcpy(dmean, mu, sizeof(mu), cudaMemcpyHostToDevice), "mean");
+    cuda_check(launch_moments(b.parts, b.stride, b.masks, b.n, dmean, part, nb, 0), "moments");
+    cuda_check(cudaMemcpy(hp.data(), part, sizeof(double) * nb * 27, cudaMemcpyDeviceToHost), "moments");
+    cudaFree(part);
+    cudaFree(dmean);
+    double m2[6][6];
+    int t = 6;
+    double acc[21] = {0};
+    for (int k = 0; k < nb; ++k)
+        for (int j = 0; j < 21; ++j) acc[j] += hp[(size_t)k * 27 + 6 + j];
+    for (int j = 0; j < 6; ++j)
+        for (int k = 0; k <= j; ++k) {
+            m2[j][k] = m2[k][j] = acc[t - 6] / nt;
+            ++t;
+        }
+    if (mean)
+        for (int j = 0; j < 6; ++j) mean[j] = mu[j];
+    if (mom2)
+        for (int j = 0; j < 6; ++j)
+            for (int k = 0; k < 6; ++k) mom2[j * 6 + k] = m2[j][k];
+    if (emit)
+        for (int pl = 0; pl < 3; ++pl) {
+            double det = m2[2 * pl][2 * pl] * m2[2 * pl + 1][2 * pl + 1] - m2[2 * pl][2 * pl + 1] * m2[2 * pl + 1][2 * pl];
+            if (det < 0 && det > -1.0e-15) det = 0; // eliminate_small_negative
+            emit[pl] = std::sqrt(det);
+        }
+    SB2_CATCH
+}
+
+sb2_status sb2_lattice_create(const char* name, sb2_lattice** out)
+{
+    SB2_TRY
+    SB2_REQUIRE(out, "null out");
+    auto* l = new sb2_lattice();
+    l->l.name = name ? name : "";
+    *out = l;
+    SB2_CATCH
+}
+sb2_status sb2_lattice_destroy(sb2_lattice* l)
+{
+    SB2_TRY
+    delete l;
+    SB2_CATCH
+}
+sb2_status sb2_lattice_set_reference_particle(sb2_lattice* l, int32_t charge, double mass, double value, int32_t kind)
+{
+    SB2_TRY
+    SB2_REQUIRE(l, "null lattice");
+    l->l.ref.set(charge, mass, value, kind);
+    l->l.has_ref = true;
+    SB2_CATCH
+}
+sb2_status sb2_lattice_append(sb2_lattice* l, const char* type, const char* name, int32_t* index)
+{
+    SB2_TRY
+    SB2_REQUIRE(l && type, "null argument");
+    Element e;
+    e.type = type;
+    e.name = name ? name : "";
+    l->l.elements.push_back(e);
+    if (index) *index = (int32_t)l->l.elements.size() - 1;
+    SB2_CATCH
+}
+static Element& elem_at(sb2_lattice* l, int32_t i)
+{
+    if (!l || i < 0 || i >= (int32_t)l->l.elements.size()) throw Error(SB2_ERR_INVALID, "element index out of range");
+    return l->l.elements[i];
+}
+sb2_status sb2_lattice_set_double(sb2_lattice* l, int32_t i, const char* attr, double v)
+{
+    SB2_TRY
+    SB2_REQUIRE(attr, "null attribute");
+    elem_at(l, i).d[attr] = v;
+    SB2_CATCH
+}
+sb2_status sb2_lattice_set_string(sb2_lattice* l, int32_t i, const char* attr, const char* v)
+{
+    SB2_TRY
+    SB2_REQUIRE(attr && v, "null attribute");
+    elem_at(l, i).s[attr] = v;
+    SB2_CATCH
+}
+sb2_status sb2_lattice_set_vector(sb2_lattice* l, int32_t i, const char* attr, const double* v, int32_t n)
+{
+    SB2_TRY
+    SB2_REQUIRE(attr && (v || n == 0) && n >= 0, "bad vector attribute");
+    elem_at(l, i).v[attr] = std::vector<double>(v, v + n);
+    SB2_CATCH
+}
+sb2_status sb2_lattice_length(sb2_lattice* l, double* length)
+{
+    SB2_TRY
+    SB2_REQUIRE(l && length, "null argument");
+    *length = l->l.length();
+    SB2_CATCH
+}
+sb2_status sb2_lattice_num_elements(sb2_lattice* l, int32_t* n)
+{
+    SB2_TRY
+    SB2_REQUIRE(l && n, "null argument");
+    *n = (int32_t)l->l.elements.size();
+    SB2_CATCH
+}
+
+
+sb2_status sb2_propagator_create(const sb2_lattice* lattice, int32_t stepper, int32_t num_steps,
+                                 const sb2_sc3d_options* sc, sb2_propagator** out)
+{
+    SB2_TRY
+    SB2_REQUIRE(lattice && out, "null argument");
+    auto* p = new sb2_propagator();
+    std::unique_ptr<sb2_propagator> guard(p);
+    p->p.reset(new Propagator(lattice->l, stepper, num_steps, sc));
+    *out = guard.release();
+    SB2_CATCH
+}
+sb2_status sb2_propagator_destroy(sb2_propagator* p)
+{
+    SB2_TRY
+    delete p;
+    SB2_CATCH
+}
+sb2_status sb2_propagator_num_steps(sb2_propagator* p, int32_t* n)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && n, "null argument");
+    *n = (int32_t)p->p->steps.size();
+    SB2_CATCH
+}
+sb2_status sb2_propagator_step_slices(sb2_propagator* p, int32_t step, int32_t op, double* out, int32_t cap, int32_t* n)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && n && step >= 0 && step < (int32_t)p->p->steps.size(), "bad step");
+    auto& st = p->p->steps[step];
+    if (op < 0 || op >= (int32_t)st.indeps.size()) {
+        *n = -1;
+        return SB2_OK;
+    }
+    auto& sl = st.indeps[op].slices;
+    int32_t k = 0;
+    for (auto& s : sl) {
+        if (k >= cap) break;
+        out[k * 3 + 0] = s.elem;
+        out[k * 3 + 1] = s.left;
+        out[k * 3 + 2] = s.right;
+        ++k;
+    }
+    *n = k;
+    SB2_CATCH
+}
+
+sb2_status sb2_propagator_propagate(sb2_propagator* p, sb2_bunch* b, int32_t turns, void* stream)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && b && turns >= 0, "bad argument");
+    p->p->propagate(b->b, turns, as_stream(stream));
+    SB2_CATCH
+}
+sb2_status sb2_propagator_propagate_steps(sb2_propagator* p, sb2_bunch* b, int32_t first, int32_t count, void* stream)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && b && count >= 0, "bad argument");
+    p->p->propagate_steps(b->b, first, count, as_stream(stream));
+    SB2_CATCH
+}
+sb2_status sb2_propagator_deposited_charge(sb2_propagator* p, int32_t index, double* charge)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && charge && index >= 0 && index < (int32_t)p->p->lat.elements.size(), "bad element index");
+    *charge = 0.0;
+    if (!p->p->elem_charge) return SB2_OK;
+    cuda_check(cudaMemcpy(charge, p->p->elem_charge + index, sizeof(double), cudaMemcpyDeviceToHost), "charge");
+    SB2_CATCH
+}
+
+sb2_status sb2_propagator_sc_last(sb2_propagator* p, double left[3], double h[3], double* rho, double* phi, double* ex,
+                                  double* ey, double* ez, double scalars[8])
+{
+    SB2_TRY
+    SB2_REQUIRE(p, "null propagator");
+    if (!p->p->has_sc) throw Error(SB2_ERR_INVALID, "propagator has no space-charge operator");
+    if (!p->p->sc) throw Error(SB2_ERR_INVALID, "propagator has not run a space-charge kick yet");
+    p->p->sc->copy_last(left, h, rho, phi, ex, ey, ez, scalars);
+    SB2_CATCH
+}
+
+sb2_status sb2_sc3d_create(const sb2_sc3d_options* opts, sb2_sc3d** out)
+{
+    SB2_TRY
+    SB2_REQUIRE(opts && out, "null argument");
+    auto* s = new sb2_sc3d();
+    std::unique_ptr<sb2_sc3d> guard(s);
+    s->op.reset(new ScOperator(*opts));
+    *out = guard.release();
+    SB2_CATCH
+}
+sb2_status sb2_sc3d_destroy(sb2_sc3d* sc)
+{
+    SB2_TRY
+    delete sc;
+    SB2_CATCH
+}
+sb2_status sb2_sc3d_apply(sb2_sc3d* sc, sb2_bunch* b, double time_step, void* stream)
+{
+    SB2_TRY
+    SB2_REQUIRE(sc && b, "null argument");
+    sc->op->apply(b->b, time_step, as_stream(stream));
+    b->b.sync_counters(as_stream(stream));
+    SB2_CATCH
+}
+sb2_status sb2_sc3d_last(sb2_sc3d* sc, double left[3], double h[3], double* rho, double* phi, double* ex, double* ey,
+                         double* ez, double scalars[8])
+{
+    SB2_TRY
+    SB2_REQUIRE(sc, "null argument");
+    sc->op->sc.copy_last(left, h, rho, phi, ex, ey, ez, scalars);
+    SB2_CATCH
+}
+
+sb2_status sb2_libff_apply(const sb2_lattice* lattice, const double* slices, int32_t nslices, sb2_bunch* hb, void* stream)
+{
+    SB2_TRY
+    SB2_REQUIRE(lattice && hb && (slices || nslices == 0), "null argument");
+    Bunch& b = hb->b;
+    const Lattice& lat = lattice->l;
+    if (!b.design_set) {
+        b.design = lat.ref;
+        b.design_set = true;
+    }
+    Engine eng;
+    std::vector<MapOp> ops;
+    for (int32_t i = 0; i < nslices; ++i) {
+        int ei = (int)slices[3 * i];
+        SB2_REQUIRE(ei >= 0 && ei < (int)lat.elements.size(), "slice element out of range");
+        Slice sl = make_slice(lat, ei, slices[3 * i + 1], slices[3 * i + 2]);
+        ops_slice(lat, sl, b, eng.ops);
+    }
+    eng.flush(b, nullptr, nullptr, false, 0.0, as_stream(stream));
+    cuda_check(cudaStreamSynchronize(as_stream(stream)), "sync");
+    SB2_CATCH
+}
+
+sb2_status sb2_aperture_apply(const sb2_lattice* lattice, int32_t index, const char* aperture_type, sb2_bunch* hb,
+                              int32_t* ndiscarded, void* stream)
+{
+    SB2_TRY
+    SB2_REQUIRE(lattice && hb && aperture_type, "null argument");
+    SB2_REQUIRE(index >= 0 && index < (int32_t)lattice->l.elements.size(), "element index out of range");
+    Bunch& b = hb->b;
+    Engine eng;
+    Slice sl = whole_slice(lattice->l, index);
+    MapOp m = op_aperture(lattice->l, aperture_type, sl);
+    m.slot = 0;
+    eng.ops.push_back(m);
+    eng.nslots = 1;
+    // a lone aperture does not run update_total_num: only n_valid changes
+    eng.flush(b, nullptr, nullptr, false, 0.0, as_stream(stream));
+    int32_t nd = 0;
+    cuda_check(cudaMemcpyAsync(&nd, eng.ap_counts, sizeof(int32_t), cudaMemcpyDeviceToHost, as_stream(stream)), "count");
+    cuda_check(cudaMemsetAsync(eng.ap_counts, 0, sizeof(int32_t), as_stream(stream)), "count");
+    b.sync_counters(as_stream(stream));
+    b.host_counters.n_valid -= nd;
+    cuda_check(cudaMemcpy(b.counters, &b.host_counters, sizeof(BunchCounters), cudaMemcpyHostToDevice), "counters");
+    if (ndiscarded) *ndiscarded = nd;
+    SB2_CATCH
+}
+
+} // extern "C"

@@ -1,0 +1,74 @@
+// Kernel parameter blocks and launchers shared by the host runtime and the
+// .cu translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "sb2_ops.h"
+
+namespace sb2 {
+
+struct TrackParams {
+    double* parts;
+    int64_t stride;
+    uint8_t* masks;
+    uint8_t* discards;
+    int64_t n;
+    int32_t* ap_counts;         // discard counter per aperture slot
+    double* moment_partials;    // [gridDim.x][6]
+    const ScState* sc;          // space-charge state (kick)
+    const double2* efield;      // (gz,gy,gx) cells x {ex,ey | ez,0}
+    int32_t gx, gy, gz;
+    double kick_pref, kick_m;
+    int32_t nops;
+    int32_t write_discards;
+    int32_t slot_base;          // aperture slots of this launch: slot_base + [0, kMaxOpsPerPass)
+    MapOp ops[kMaxOpsPerPass];
+};
+
+struct DomainParams {
+    BunchCounters* counters;
+    int32_t* ap_counts;
+    double* elem_charge; // per lattice element, may be null
+    PassBook book;
+    const double* moment_partials;
+    int32_t n_partials;
+    int32_t compute_domain; // 0: bookkeeping only
+    ScState* sc;
+    // options
+    int32_t g[3], dg[3];
+    int32_t domain_fixed, grid_entire_period, green_linear;
+    double n_sigma, z_period, kick_scale;
+    double fixed_size[3], fixed_offset[3];
+    // bunch
+    int32_t charge;
+    double pref, gamma, beta;
+    double time_step;
+};
+
+struct Dims {
+    int gx, gy, gz;    // original grid
+    int nx, ny, nz;    // doubled grid
+    int nkx, nkxp;     // nx/2+1, padded row pitch of S
+    int lx, ly, lz;    // log2 of nx, ny, nz
+};
+
+// track.cu
+int track_grid_blocks();
+cudaError_t launch_track(const TrackParams& p, cudaStream_t s);
+cudaError_t launch_moments(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
+                           const double* mean, double* partials, int nblocks, cudaStream_t s);
+cudaError_t launch_populate(double* parts, int64_t stride, uint8_t* masks, int64_t n, const double* sig,
+                            uint64_t seed, cudaStream_t s);
+// sc3d.cu
+cudaError_t launch_book_domain(const DomainParams& p, cudaStream_t s);
+cudaError_t launch_deposit(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
+                           const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s);
+cudaError_t launch_green(const ScState* sc, double* G, const Dims& d, int linear, const double2* tw_x,
+                         const double2* tw_y, const double2* tw_z, cudaStream_t s);
+cudaError_t launch_convolve(const double* rho, double2* S, const double* Ghat, double* phi, const Dims& d,
+                            const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
+                            cudaStream_t s);
+cudaError_t launch_efield(const double* phi, double2* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s);
+
+} // namespace sb2

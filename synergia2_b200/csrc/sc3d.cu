@@ -1,0 +1,655 @@
+// 3D open-boundary Hockney solver kernels for sm_100a (FP64 path).
+//
+// Layouts in HBM (x fastest everywhere):
+//   rho, phi   dense real (gz, gy, gx) on the original grid
+//   S          complex spectrum [nz][ny][nkxp], nkx = nx/2+1 (padded even)
+//   Ghat       real octant [nz/2+1][ny/2+1][nx/2+1]: the transform of the
+//              mirrored Green function is real and even in every axis, so
+//              only this octant is built and read
+//   E          (gz, gy, gx) cells x {ex, ey, ez, 0} FP64 (32 B per cell)
+//
+// The convolution phi = IFFT(FFT(rho_padded) * FFT(G2)) of
+// space_charge_3d_open_hockney.cc:642-676 is computed in five line passes
+// that skip the zero padding: x (pairs of real rows packed as one complex
+// FFT), y (first gy inputs), z forward + Ghat multiply + z inverse in one
+// kernel (first gz inputs, first gz outputs), y inverse (first gy outputs),
+// x inverse (Hermitian pairs, first gx outputs).  Each pass stages a tile of
+// lines in shared memory and runs a radix-2 Stockham-free in-place
+// Cooley-Tukey transform there.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdint>
+
+#include "sb2_kernels.h"
+
+namespace sb2 {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kE = 1.602176565e-19;
+constexpr double kCl = 299792458.0;
+constexpr double kMu0 = 4 * kPi * 1.0e-7;
+constexpr double kEps0 = 1.0 / (kCl * kCl * kMu0);
+
+// ---------------------------------------------------------------------------
+// bookkeeping + domain (one block)
+// ---------------------------------------------------------------------------
+
+__device__ double smallest_non_tiny(double val, double o1, double o2, double tiny)
+{ // space_charge_3d_open_hockney.cc:94-109
+    if (val > tiny) return val;
+    if ((o1 > tiny) && (o2 > tiny)) return fmin(o1, o2);
+    return fmax(o1, o2);
+}
+
+__global__ void __launch_bounds__(256) book_domain_kernel(const __grid_constant__ DomainParams p)
+{
+    __shared__ double s_sum[256][6];
+    // fixed-order reduction of the per-block moment partials
+    if (p.compute_domain && !p.domain_fixed) {
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        for (int b = threadIdx.x; b < p.n_partials; b += blockDim.x)
+            for (int j = 0; j < 6; ++j) acc[j] += p.moment_partials[b * 6 + j];
+        for (int j = 0; j < 6; ++j) s_sum[threadIdx.x][j] = acc[j];
+        __syncthreads();
+        for (int w = 128; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w)
+                for (int j = 0; j < 6; ++j) s_sum[threadIdx.x][j] += s_sum[threadIdx.x + w][j];
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x != 0) return;
+
+    // bookkeeping: aperture operations then update_total_num per operator
+    // (independent_operator.cc:94-133, aperture_operation.h:14-24,
+    // bunch.h:363-370)
+    BunchCounters c = *p.counters;
+    for (int o = 0; o < p.book.n_operators; ++o) {
+        int nd_op = 0;
+        for (int s = p.book.slot_begin[o]; s < p.book.slot_end[o]; ++s) {
+            int nd = p.ap_counts[s];
+            p.ap_counts[s] = 0;
+            int el = p.book.slot_elem[s];
+            if (p.elem_charge && el >= 0 && nd) p.elem_charge[el] += nd * c.real_num / c.n_total;
+            nd_op += nd;
+            c.n_valid -= nd;
+        }
+        int old_total = c.n_total;
+        c.n_total = c.n_valid;
+        c.real_num = old_total ? c.n_total * c.real_num / old_total : 0.0;
+    }
+    *p.counters = c;
+    if (!p.compute_domain) return;
+
+    ScState st = *p.sc;
+    st.error = 0;
+    double size[3], offset[3];
+    if (p.domain_fixed) {
+        for (int i = 0; i < 3; ++i) {
+            size[i] = p.fixed_size[i];
+            offset[i] = p.fixed_offset[i];
+        }
+    } else {
+        // update_domain :494-540; calculate_spatial_mean_stddev
+        // core_diagnostics.cc:422-460 (divides by n_total)
+        double ms[6];
+        for (int j = 0; j < 3; ++j) {
+            ms[j] = s_sum[0][j] / c.n_total;
+            ms[j + 3] = sqrt((s_sum[0][j + 3]) / c.n_total - ms[j] * ms[j]);
+        }
+        for (int j = 0; j < 6; ++j) st.mean_std[j] = ms[j];
+        const double tiny = 1.0e-10;
+        if ((ms[3] < tiny) && (ms[4] < tiny) && (ms[5] < tiny)) {
+            st.error = 1;
+            st.valid = 0;
+            *p.sc = st;
+            return;
+        }
+        offset[0] = ms[0];
+        offset[1] = ms[1];
+        offset[2] = ms[2];
+        size[0] = p.n_sigma * smallest_non_tiny(ms[3], ms[4], ms[5], tiny);
+        size[1] = p.n_sigma * smallest_non_tiny(ms[4], ms[3], ms[5], tiny);
+        size[2] = p.n_sigma * smallest_non_tiny(ms[5], ms[3], ms[4], tiny);
+        if (p.grid_entire_period) {
+            offset[2] = 0.0;
+            size[2] = p.z_period;
+        }
+    }
+    // Rectangular_grid_domain rectangular_grid_domain.h:20-36 (original and
+    // doubled domains)
+    for (int i = 0; i < 3; ++i) {
+        st.left[i] = offset[i] - size[i] / 2.0;
+        st.h[i] = size[i] / (1.0 * p.g[i]);
+        st.ih[i] = 1.0 / st.h[i];
+        st.dh[i] = (size[i] * 2.0) / (1.0 * p.dg[i]);
+    }
+    // deposit weight deposit.cc:608-610
+    st.w0 = (c.real_num / c.n_total) * p.charge * kE / (st.h[0] * st.h[1] * st.h[2]);
+    // get_normalization_force :708-735
+    double norm = st.h[0] * st.h[1] * st.h[2];
+    norm *= 1.0 / (4.0 * kPi * kEps0);
+    norm *= 1.0;
+    if (p.green_linear) norm *= 1.0 / (st.h[2] * st.h[2]);
+    norm *= 1.0 / (p.dg[0] * p.dg[1] * p.dg[2]);
+    st.fn_norm = norm;
+    // apply_kick :753-770
+    double q = p.charge * kE;
+    double unit_conversion = kCl / (1e9 * kE);
+    st.factor = p.kick_scale * unit_conversion * q * p.time_step * st.fn_norm /
+                (p.pref * p.gamma * p.gamma * p.beta);
+    st.valid = 1;
+    *p.sc = st;
+}
+
+// ---------------------------------------------------------------------------
+// deposit (FP64, global atomics): sv_zyx_rho_reducer_non_periodic
+// deposit.cc:309-394; edges excluded deposit.cc:23-30
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void leftmost_d(double pos, double left, double inv, int& idx, double& off)
+{
+    double s = (pos - left) * inv - 0.5;
+    idx = (int)floor(s);
+    off = s - idx;
+}
+
+__global__ void __launch_bounds__(256) deposit_kernel(const double* __restrict__ parts, int64_t stride,
+                                                      const uint8_t* __restrict__ masks, int64_t n,
+                                                      const ScState* __restrict__ scp, double* rho,
+                                                      int gx, int gy, int gz)
+{
+    const ScState& sc = *scp;
+    if (!sc.valid) return;
+    const double lx = sc.left[0], ly = sc.left[1], lz = sc.left[2];
+    const double ihx = sc.ih[0], ihy = sc.ih[1], ihz = sc.ih[2];
+    const double w0 = sc.w0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (!masks[i]) continue;
+        int ix, iy, iz;
+        double ox, oy, oz;
+        leftmost_d(parts[i], lx, ihx, ix, ox);
+        leftmost_d(parts[i + 2 * stride], ly, ihy, iy, oy);
+        leftmost_d(parts[i + 4 * stride], lz, ihz, iz, oz);
+        double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
+        bool x0 = ix > 0 && ix < gx - 1, x1 = ix + 1 > 0 && ix + 1 < gx - 1;
+        bool y0 = iy > 0 && iy < gy - 1, y1 = iy + 1 > 0 && iy + 1 < gy - 1;
+        bool z0 = iz > 0 && iz < gz - 1, z1 = iz + 1 > 0 && iz + 1 < gz - 1;
+        int64_t base = (int64_t)iz * gx * gy;
+        if (z0) {
+            if (y0 && x0) atomicAdd(&rho[base + iy * gx + ix], w0 * aox * aoy * aoz);
+            if (y0 && x1) atomicAdd(&rho[base + iy * gx + ix + 1], w0 * ox * aoy * aoz);
+            if (y1 && x0) atomicAdd(&rho[base + (iy + 1) * gx + ix], w0 * aox * oy * aoz);
+            if (y1 && x1) atomicAdd(&rho[base + (iy + 1) * gx + ix + 1], w0 * ox * oy * aoz);
+        }
+        base = (int64_t)(iz + 1) * gx * gy;
+        if (z1) {
+            if (y0 && x0) atomicAdd(&rho[base + iy * gx + ix], w0 * aox * aoy * oz);
+            if (y0 && x1) atomicAdd(&rho[base + iy * gx + ix + 1], w0 * ox * aoy * oz);
+            if (y1 && x0) atomicAdd(&rho[base + (iy + 1) * gx + ix], w0 * aox * oy * oz);
+            if (y1 && x1) atomicAdd(&rho[base + (iy + 1) * gx + ix + 1], w0 * ox * oy * oz);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Green function octant: alg_g2_linear :230-348 / alg_g2_pointlike :136-228
+// evaluated for ix <= gx, iy <= gy, iz <= gz (doubled shape = 2 * shape,
+// so this octant plus mirroring is the whole doubled-grid G2)
+// ---------------------------------------------------------------------------
+__global__ void green_octant_kernel(const ScState* __restrict__ scp, double* G, int gx0, int gy0, int gz0,
+                                    int linear)
+{
+    const ScState& sc = *scp;
+    if (!sc.valid) return;
+    const int ox = gx0 + 1, oy = gy0 + 1, oz = gz0 + 1;
+    const int64_t total = (int64_t)ox * oy * oz;
+    const double hx = sc.dh[0], hy = sc.dh[1], hz = sc.dh[2];
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        int ix = (int)(t % ox);
+        int iy = (int)((t / ox) % oy);
+        int iz = (int)(t / ((int64_t)ox * oy));
+        double Gv;
+        if (!linear) {
+            double G000 = 2.8 / fmin(hx, fmin(hy, hz));
+            double dx = ix * hx, dy = iy * hy, dz = iz * hz;
+            Gv = (ix == 0 && iy == 0 && iz == 0) ? G000 : 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
+        } else {
+            double rr0 = hx * hx + hy * hy;
+            double r10 = sqrt(hx * hx + hy * hy + hz * hz);
+            double G000 = (2.0 / rr0) * (hz * r10 + rr0 * log((hz + r10) / sqrt(rr0)) - hz * hz);
+            double z = iz * hz; // iz <= gz0
+            double y = iy * hy, x = ix * hx;
+            double rr = x * x + y * y;
+            double s0 = sqrt(rr + z * z);
+            double sn = sqrt(rr + (z - hz) * (z - hz));
+            double sp = sqrt(rr + (z + hz) * (z + hz));
+            Gv = 2.0 * s0 - sn - sp;
+            const double epsz = 1e-12 * hz;
+            double T1, T2, r1, r2;
+            if (z < -hz) {
+                r1 = (sn - z + hz) / (s0 - z);
+                T1 = (hz - z) * log(r1);
+                r2 = (s0 - z) / (sp - z - hz);
+                T2 = (hz + z) * log(r2);
+                Gv += T1 + T2;
+            } else if (fabs(z + hz) < epsz) {
+                r1 = (sn - z + hz) / (s0 - z);
+                T1 = (hz - z) * log(r1);
+                Gv += T1;
+            } else if (fabs(z) < epsz) {
+                if (fabs(x) + fabs(y) < 2. * epsz) {
+                    Gv += hz * G000;
+                } else {
+                    r1 = (sqrt(hz * hz + rr) + hz) / sqrt(rr);
+                    Gv += 2.0 * hz * log(r1);
+                }
+            } else if (fabs(z - hz) < epsz) {
+                r1 = (sp + z + hz) / (s0 + z);
+                T1 = (hz + z) * log(r1);
+                Gv += T1;
+            } else if (z > hz) {
+                r1 = (s0 + z) / (sn + z - hz);
+                T1 = (hz - z) * log(r1);
+                r2 = (sp + z + hz) / (s0 + z);
+                T2 = (hz + z) * log(r2);
+                Gv += T1 + T2;
+            }
+        }
+        G[t] = Gv;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory radix-2 FFT core.  A tile holds `nl` lines of length L
+// (L a power of two) as s[line * L + j].  DIT expects bit-reversed input and
+// leaves natural order; DIF takes natural order and leaves bit-reversed.
+// tw[k] = exp(-2 pi i k / L), k < L/2; `inv` conjugates.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ unsigned brev_n(unsigned j, int logL) { return logL ? (__brev(j) >> (32 - logL)) : 0u; }
+
+// Lines sit at pitch L + 1 in shared memory so that threads walking
+// consecutive lines hit different banks.
+__device__ void smem_dit(double2* s, int nl, int L, int logL, const double2* __restrict__ tw, bool inv)
+{
+    const int P = L + 1;
+    const int halfL = L >> 1;
+    const int nb = nl * halfL;
+    for (int st = 0; st < logL; ++st) {
+        const int half = 1 << st;
+        const int tstride = halfL >> st; // L / (2*half)
+        for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+            int line = t / halfL, bf = t - line * halfL;
+            int pos = bf & (half - 1), grp = bf >> st;
+            int i0 = line * P + grp * 2 * half + pos, i1 = i0 + half;
+            double2 w = tw[pos * tstride];
+            if (inv) w.y = -w.y;
+            double2 a = s[i0], b = cmul(s[i1], w);
+            s[i0] = cadd(a, b);
+            s[i1] = csub(a, b);
+        }
+        __syncthreads();
+    }
+}
+
+__device__ void smem_dif(double2* s, int nl, int L, int logL, const double2* __restrict__ tw, bool inv)
+{
+    const int P = L + 1;
+    const int halfL = L >> 1;
+    const int nb = nl * halfL;
+    for (int st = logL - 1; st >= 0; --st) {
+        const int half = 1 << st;
+        const int tstride = halfL >> st;
+        for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+            int line = t / halfL, bf = t - line * halfL;
+            int pos = bf & (half - 1), grp = bf >> st;
+            int i0 = line * P + grp * 2 * half + pos, i1 = i0 + half;
+            double2 w = tw[pos * tstride];
+            if (inv) w.y = -w.y;
+            double2 a = s[i0], b = s[i1];
+            s[i0] = cadd(a, b);
+            s[i1] = cmul(csub(a, b), w);
+        }
+        __syncthreads();
+    }
+}
+
+constexpr int kFftTile = 4096; // complex elements per CTA tile (64 KB + line padding)
+// nl = kFftTile / L lines at pitch L + 1 take kFftTile + nl elements; the
+// smallest transform length is 8 (grid shape >= 3 doubled to a power of 2).
+constexpr int kFftMinLen = 8;
+constexpr int kFftSmemBytes = (kFftTile + kFftTile / kFftMinLen) * 16;
+constexpr int kFftThreads = 256;
+
+
+// XF: pairs of real rows (y, y+1) of rho -> S rows (r2c, first gx inputs)
+__global__ void __launch_bounds__(kFftThreads) fft_xf_kernel(const double* __restrict__ rho, double2* S,
+                                                             const double2* __restrict__ tw, Dims d,
+                                                             const ScState* __restrict__ scp)
+{
+    extern __shared__ double2 sm[];
+    if (!scp->valid) return;
+    const int L = d.nx, nl = kFftTile / L;
+    const int npy = (d.gy + 1) / 2;
+    const int64_t nlines = (int64_t)npy * d.gz;
+    const int64_t l0 = (int64_t)blockIdx.x * nl;
+    const int nlt = (int)min((int64_t)nl, nlines - l0);
+    if (nlt <= 0) return;
+    for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
+        int li = idx / L, j = idx - li * L;
+        int64_t l = l0 + li;
+        int pr = (int)(l % npy), z = (int)(l / npy);
+        int ya = 2 * pr, yb = ya + 1;
+        double2 v = make_double2(0.0, 0.0);
+        if (j < d.gx) {
+            v.x = rho[((int64_t)z * d.gy + ya) * d.gx + j];
+            if (yb < d.gy) v.y = rho[((int64_t)z * d.gy + yb) * d.gx + j];
+        }
+        sm[li * (L + 1) + brev_n(j, d.lx)] = v;
+    }
+    __syncthreads();
+    smem_dit(sm, nlt, L, d.lx, tw, false);
+    const int nk = d.nkx;
+    for (int idx = threadIdx.x; idx < nlt * nk; idx += blockDim.x) {
+        int li = idx / nk, k = idx - li * nk;
+        int64_t l = l0 + li;
+        int pr = (int)(l % npy), z = (int)(l / npy);
+        int ya = 2 * pr, yb = ya + 1;
+        double2 Z = sm[li * (L + 1) + k], Zn = sm[li * (L + 1) + ((L - k) & (L - 1))];
+        double2 A = make_double2((Z.x + Zn.x) * 0.5, (Z.y - Zn.y) * 0.5);
+        double2 B = make_double2((Z.y + Zn.y) * 0.5, -(Z.x - Zn.x) * 0.5);
+        S[((int64_t)z * d.ny + ya) * d.nkxp + k] = A;
+        if (yb < d.gy) S[((int64_t)z * d.ny + yb) * d.nkxp + k] = B;
+    }
+}
+
+// Y passes: lines (kx, z<gz) along y.  forward: first gy inputs, all ny
+// outputs; inverse: all inputs, first gy outputs.
+__global__ void __launch_bounds__(kFftThreads) fft_y_kernel(double2* S, const double2* __restrict__ tw, Dims d,
+                                                            int inverse, const ScState* __restrict__ scp)
+{
+    extern __shared__ double2 sm[];
+    if (!scp->valid) return;
+    const int L = d.ny, nl = kFftTile / L;
+    const int64_t nlines = (int64_t)d.nkx * d.gz;
+    const int64_t l0 = (int64_t)blockIdx.x * nl;
+    const int nlt = (int)min((int64_t)nl, nlines - l0);
+    if (nlt <= 0) return;
+    const int nin = inverse ? L : d.gy;
+    for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
+        int j = idx / nlt, li = idx - j * nlt; // consecutive threads: consecutive kx
+        int64_t l = l0 + li;
+        int kx = (int)(l % d.nkx), z = (int)(l / d.nkx);
+        double2 v = make_double2(0.0, 0.0);
+        if (j < nin) v = S[((int64_t)z * d.ny + j) * d.nkxp + kx];
+        sm[li * (L + 1) + (inverse ? j : (int)brev_n(j, d.ly))] = v;
+    }
+    __syncthreads();
+    if (!inverse)
+        smem_dit(sm, nlt, L, d.ly, tw, false);
+    else
+        smem_dif(sm, nlt, L, d.ly, tw, true);
+    const int nout = inverse ? d.gy : L;
+    for (int idx = threadIdx.x; idx < nlt * nout; idx += blockDim.x) {
+        int j = idx / nlt, li = idx - j * nlt;
+        int64_t l = l0 + li;
+        int kx = (int)(l % d.nkx), z = (int)(l / d.nkx);
+        double2 v = sm[li * (L + 1) + (inverse ? (int)brev_n(j, d.ly) : j)];
+        S[((int64_t)z * d.ny + j) * d.nkxp + kx] = v;
+    }
+}
+
+// Z pass: lines (kx, ky) along z: forward (first gz inputs), multiply by
+// the real octant Ghat(kx, min(ky, ny-ky), min(kz, nz-kz)), inverse, first gz
+// outputs.  (alg_cplx_multiplier :350-372 fused between the transforms.)
+__global__ void __launch_bounds__(kFftThreads) fft_z_conv_kernel(double2* S, const double* __restrict__ Ghat,
+                                                                 const double2* __restrict__ tw, Dims d,
+                                                                 const ScState* __restrict__ scp)
+{
+    extern __shared__ double2 sm[];
+    if (!scp->valid) return;
+    const int L = d.nz, nl = kFftTile / L;
+    const int64_t nlines = (int64_t)d.nkx * d.ny;
+    const int64_t l0 = (int64_t)blockIdx.x * nl;
+    const int nlt = (int)min((int64_t)nl, nlines - l0);
+    if (nlt <= 0) return;
+    for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
+        int j = idx / nlt, li = idx - j * nlt;
+        int64_t l = l0 + li;
+        int kx = (int)(l % d.nkx), ky = (int)(l / d.nkx);
+        double2 v = make_double2(0.0, 0.0);
+        if (j < d.gz) v = S[((int64_t)j * d.ny + ky) * d.nkxp + kx];
+        sm[li * (L + 1) + brev_n(j, d.lz)] = v;
+    }
+    __syncthreads();
+    smem_dit(sm, nlt, L, d.lz, tw, false);
+    const int ogx = d.nx / 2 + 1, ogy = d.ny / 2 + 1;
+    for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
+        int li = idx / L, kz = idx - li * L;
+        int64_t l = l0 + li;
+        int kx = (int)(l % d.nkx), ky = (int)(l / d.nkx);
+        int my = ky <= d.ny / 2 ? ky : d.ny - ky;
+        int mz = kz <= d.nz / 2 ? kz : d.nz - kz;
+        double g = Ghat[((int64_t)mz * ogy + my) * ogx + kx];
+        double2 v = sm[li * (L + 1) + kz];
+        sm[li * (L + 1) + kz] = make_double2(v.x * g, v.y * g);
+    }
+    __syncthreads();
+    smem_dif(sm, nlt, L, d.lz, tw, true);
+    for (int idx = threadIdx.x; idx < nlt * d.gz; idx += blockDim.x) {
+        int j = idx / nlt, li = idx - j * nlt;
+        int64_t l = l0 + li;
+        int kx = (int)(l % d.nkx), ky = (int)(l / d.nkx);
+        S[((int64_t)j * d.ny + ky) * d.nkxp + kx] = sm[li * (L + 1) + brev_n(j, d.lz)];
+    }
+}
+
+// XI: Hermitian pairs of spectrum rows -> real rows (y, y+1) of phi (c2r,
+// first gx outputs); imaginary parts of the k = 0 and k = nx/2 terms are
+// ignored as a c2r transform does.
+__global__ void __launch_bounds__(kFftThreads) fft_xi_kernel(const double2* __restrict__ S, double* phi,
+                                                             const double2* __restrict__ tw, Dims d,
+                                                             const ScState* __restrict__ scp)
+{
+    extern __shared__ double2 sm[];
+    if (!scp->valid) return;
+    const int L = d.nx, nl = kFftTile / L;
+    const int npy = (d.gy + 1) / 2;
+    const int64_t nlines = (int64_t)npy * d.gz;
+    const int64_t l0 = (int64_t)blockIdx.x * nl;
+    const int nlt = (int)min((int64_t)nl, nlines - l0);
+    if (nlt <= 0) return;
+    const int half = L / 2;
+    for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
+        int li = idx / L, j = idx - li * L;
+        int64_t l = l0 + li;
+        int pr = (int)(l % npy), z = (int)(l / npy);
+        int ya = 2 * pr, yb = ya + 1;
+        int k = j <= half ? j : L - j;
+        double2 A = S[((int64_t)z * d.ny + ya) * d.nkxp + k];
+        double2 B = (yb < d.gy) ? S[((int64_t)z * d.ny + yb) * d.nkxp + k] : make_double2(0.0, 0.0);
+        if (k == 0 || k == half) {
+            A.y = 0.0;
+            B.y = 0.0;
+        }
+        if (j > half) {
+            A.y = -A.y;
+            B.y = -B.y;
+        }
+        sm[li * (L + 1) + j] = make_double2(A.x - B.y, A.y + B.x);
+    }
+    __syncthreads();
+    smem_dif(sm, nlt, L, d.lx, tw, true);
+    for (int idx = threadIdx.x; idx < nlt * d.gx; idx += blockDim.x) {
+        int li = idx / d.gx, j = idx - li * d.gx;
+        int64_t l = l0 + li;
+        int pr = (int)(l % npy), z = (int)(l / npy);
+        int ya = 2 * pr, yb = ya + 1;
+        double2 v = sm[li * (L + 1) + brev_n(j, d.lx)];
+        phi[((int64_t)z * d.gy + ya) * d.gx + j] = v.x;
+        if (yb < d.gy) phi[((int64_t)z * d.gy + yb) * d.gx + j] = v.y;
+    }
+}
+
+// Ghat passes on the real octant (ox, oy, oz) = (nx/2+1, ny/2+1, nz/2+1):
+// axis 0/1/2 transforms even real lines rebuilt by mirroring; real part of
+// the first L/2+1 outputs stored back in place.
+__global__ void __launch_bounds__(kFftThreads) fft_green_kernel(double* G, const double2* __restrict__ tw,
+                                                                int axis, int L, int logL, int ox, int oy, int oz,
+                                                                const ScState* __restrict__ scp)
+{
+    extern __shared__ double2 sm[];
+    if (!scp->valid) return;
+    const int nl = kFftTile / L;
+    const int half = L / 2;
+    int64_t nlines, sa, sj;
+    int na;
+    if (axis == 0) { nlines = (int64_t)oy * oz; na = 1; sa = ox; sj = 1; }
+    else if (axis == 1) { nlines = (int64_t)ox * oz; na = ox; sa = 1; sj = ox; }
+    else { nlines = (int64_t)ox * oy; na = ox * oy; sa = 1; sj = (int64_t)ox * oy; }
+    const int64_t l0 = (int64_t)blockIdx.x * nl;
+    const int nlt = (int)min((int64_t)nl, nlines - l0);
+    if (nlt <= 0) return;
+    auto line_base = [&](int64_t l) -> int64_t {
+        if (axis == 0) return l * ox;                                  // (y, z) rows
+        if (axis == 1) return (l % ox) + (l / ox) * (int64_t)ox * oy;  // (kx, z)
+        return l;                                                      // (kx, ky)
+    };
+    (void)na;
+    (void)sa;
+    for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
+        int li, j;
+        if (axis == 0) { li = idx / L; j = idx - li * L; }
+        else { j = idx / nlt; li = idx - j * nlt; }
+        int m = j <= half ? j : L - j;
+        double v = G[line_base(l0 + li) + m * sj];
+        sm[li * (L + 1) + brev_n(j, logL)] = make_double2(v, 0.0);
+    }
+    __syncthreads();
+    smem_dit(sm, nlt, L, logL, tw, false);
+    for (int idx = threadIdx.x; idx < nlt * (half + 1); idx += blockDim.x) {
+        int li, k;
+        if (axis == 0) { li = idx / (half + 1); k = idx - li * (half + 1); }
+        else { k = idx / nlt; li = idx - k * nlt; }
+        G[line_base(l0 + li) + k * sj] = sm[li * (L + 1) + k].x;
+    }
+}
+
+// E = -grad phi by central differences on interior cells of the original
+// grid, zero on the boundary: alg_force_extractor_doubled_domain
+// space_charge_3d_kernels.h:217-307 (h of the doubled domain).
+__global__ void efield_kernel(const double* __restrict__ phi, double2* E, int gx, int gy, int gz,
+                              const ScState* __restrict__ scp)
+{
+    const ScState& sc = *scp;
+    if (!sc.valid) return;
+    const double ihx = 0.5 / sc.dh[0], ihy = 0.5 / sc.dh[1], ihz = 0.5 / sc.dh[2];
+    const int64_t total = (int64_t)gx * gy * gz;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int ix = (int)(i % gx);
+        int iy = (int)((i / gx) % gy);
+        int iz = (int)(i / ((int64_t)gx * gy));
+        double ex = 0, ey = 0, ez = 0;
+        if (!(ix == 0 || ix == gx - 1 || iy == 0 || iy == gy - 1 || iz == 0 || iz == gz - 1)) {
+            ex = -(phi[i + 1] - phi[i - 1]) * ihx;
+            ey = -(phi[i + gx] - phi[i - gx]) * ihy;
+            ez = -(phi[i + (int64_t)gx * gy] - phi[i - (int64_t)gx * gy]) * ihz;
+        }
+        E[2 * i] = make_double2(ex, ey);
+        E[2 * i + 1] = make_double2(ez, 0.0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static int sm_count()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+cudaError_t launch_book_domain(const DomainParams& p, cudaStream_t s)
+{
+    book_domain_kernel<<<1, 256, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_deposit(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
+                           const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s)
+{
+    deposit_kernel<<<sm_count() * 8, 256, 0, s>>>(parts, stride, masks, n, sc, rho, gx, gy, gz);
+    return cudaGetLastError();
+}
+
+static cudaError_t set_fft_smem()
+{
+    static bool done = false;
+    if (done) return cudaSuccess;
+    const int bytes = kFftSmemBytes;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(fft_xf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+    if ((e = cudaFuncSetAttribute(fft_y_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+    if ((e = cudaFuncSetAttribute(fft_z_conv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+    if ((e = cudaFuncSetAttribute(fft_xi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+    if ((e = cudaFuncSetAttribute(fft_green_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+    done = true;
+    return cudaSuccess;
+}
+
+static inline int ceil_div64(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// Ghat from the current domain: octant G, then the three even-line passes.
+cudaError_t launch_green(const ScState* sc, double* G, const Dims& d, int linear, const double2* tw_x,
+                         const double2* tw_y, const double2* tw_z, cudaStream_t s)
+{
+    cudaError_t e = set_fft_smem();
+    if (e) return e;
+    const int ox = d.nx / 2 + 1, oy = d.ny / 2 + 1, oz = d.nz / 2 + 1;
+    green_octant_kernel<<<sm_count() * 4, 256, 0, s>>>(sc, G, d.gx, d.gy, d.gz, linear);
+    const size_t sh = kFftSmemBytes;
+    fft_green_kernel<<<ceil_div64((int64_t)oy * oz, kFftTile / d.nx), kFftThreads, sh, s>>>(G, tw_x, 0, d.nx, d.lx, ox, oy, oz, sc);
+    fft_green_kernel<<<ceil_div64((int64_t)ox * oz, kFftTile / d.ny), kFftThreads, sh, s>>>(G, tw_y, 1, d.ny, d.ly, ox, oy, oz, sc);
+    fft_green_kernel<<<ceil_div64((int64_t)ox * oy, kFftTile / d.nz), kFftThreads, sh, s>>>(G, tw_z, 2, d.nz, d.lz, ox, oy, oz, sc);
+    return cudaGetLastError();
+}
+
+// rho -> phi through the five line passes.
+cudaError_t launch_convolve(const double* rho, double2* S, const double* Ghat, double* phi, const Dims& d,
+                            const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
+                            cudaStream_t s)
+{
+    cudaError_t e = set_fft_smem();
+    if (e) return e;
+    const size_t sh = kFftSmemBytes;
+    const int npy = (d.gy + 1) / 2;
+    fft_xf_kernel<<<ceil_div64((int64_t)npy * d.gz, kFftTile / d.nx), kFftThreads, sh, s>>>(rho, S, tw_x, d, sc);
+    fft_y_kernel<<<ceil_div64((int64_t)d.nkx * d.gz, kFftTile / d.ny), kFftThreads, sh, s>>>(S, tw_y, d, 0, sc);
+    fft_z_conv_kernel<<<ceil_div64((int64_t)d.nkx * d.ny, kFftTile / d.nz), kFftThreads, sh, s>>>(S, Ghat, tw_z, d, sc);
+    fft_y_kernel<<<ceil_div64((int64_t)d.nkx * d.gz, kFftTile / d.ny), kFftThreads, sh, s>>>(S, tw_y, d, 1, sc);
+    fft_xi_kernel<<<ceil_div64((int64_t)npy * d.gz, kFftTile / d.nx), kFftThreads, sh, s>>>(S, phi, tw_x, d, sc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_efield(const double* phi, double2* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s)
+{
+    int64_t total = (int64_t)gx * gy * gz;
+    int nb = (int)std::min<int64_t>((total + 255) / 256, (int64_t)sm_count() * 16);
+    efield_kernel<<<nb, 256, 0, s>>>(phi, E, gx, gy, gz, sc);
+    return cudaGetLastError();
+}
+
+} // namespace sb2

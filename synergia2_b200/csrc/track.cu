@@ -1,0 +1,562 @@
+// Particle-pass kernels for sm_100a.
+//
+// One launch runs a whole sequence of particle-local operations (element
+// slice maps, apertures, the space-charge kick, the spatial-moment sums) on
+// each particle while its six coordinates stay in registers: the column-major
+// N x 7 FP64 array is read once and written once per pass, coalesced (one
+// particle per thread, 32 consecutive particles per warp per column).
+//
+// Built with --fmad=false: every a*b+c keeps two IEEE roundings and sqrt/div
+// are IEEE-correct, so the maps reproduce the reference's FP64 arithmetic
+// (libFF/ff_algorithm.h) operation for operation.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "sb2_kernels.h"
+
+namespace sb2 {
+
+constexpr double kC = 299792458.0;
+
+// ---------------------------------------------------------------------------
+// ff_algorithm.h units, same operation order as the reference
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void drift_unit(double& x, double xp, double& y, double yp, double& cdt,
+                                           double dpop, double length, double reference_momentum,
+                                           double m, double reference_cdt)
+{ // ff_algorithm.h:47-79
+    const double uni = 1.0;
+    const double sig = (double)((0.0 < length) - (length < 0.0));
+    double dp = dpop + uni;
+    double inv_npz = uni / sqrt(dp * dp - xp * xp - yp * yp);
+    double lxpr = xp * length * inv_npz;
+    double lypr = yp * length * inv_npz;
+    double D2 = lxpr * lxpr + length * length + lypr * lypr;
+    double p = dp * reference_momentum;
+    double E2 = p * p + m * m;
+    double ibeta2 = E2 / (p * p);
+    x = x + lxpr;
+    y = y + lypr;
+    cdt = cdt + sig * sqrt(D2 * ibeta2) - reference_cdt;
+}
+
+__device__ __forceinline__ void thin_quadrupole_unit(double x, double& xp, double y, double& yp,
+                                                     double k0, double k1)
+{ // ff_algorithm.h:929-936
+    xp = xp - k0 * x + k1 * y;
+    yp = yp + k0 * y + k1 * x;
+}
+
+__device__ __forceinline__ void thin_sextupole_unit(double x, double& xp, double y, double& yp,
+                                                    double k0, double k1)
+{ // ff_algorithm.h:940-947
+    xp = xp - 0.5 * k0 * (x * x - y * y) + k1 * x * y;
+    yp = yp + k0 * x * y + 0.5 * k1 * (x * x - y * y);
+}
+
+__device__ __forceinline__ void thin_octupole_unit(double x, double& xp, double y, double& yp,
+                                                   double k0, double k1)
+{ // ff_algorithm.h:951-963
+    const double n1 = 0.5, n2 = 1.0 / 3.0;
+    xp = xp - n1 * k0 * (x * x * x * n2 - x * y * y) + n1 * k1 * (x * x * y - y * y * y * n2);
+    yp = yp - n1 * k0 * (y * y * y * n2 - x * x * y) + n1 * k1 * (x * x * x * n2 - x * y * y);
+}
+
+__device__ __forceinline__ double factorial_d(int n)
+{ // ff_algorithm.h:1108-1117
+    if (n == 0) return 1.0;
+    double r = 1;
+    for (int i = 1; i <= n; ++i) r *= i;
+    return r;
+}
+
+__device__ __forceinline__ double qpow_d(double x, int i)
+{ // utils/kokkos_types.h:89-95
+    double r = 1;
+    while (i--) r = r * x;
+    return r;
+}
+
+__device__ void thin_magnet_unit(double x, double& xp, double y, double& yp, double kl0, double kl1,
+                                 int n)
+{ // ff_algorithm.h:1122-1168
+    for (int k = 0; k < n; k += 4)
+        xp = xp - (kl0 * (n - k)) * qpow_d(x, n - k - 1) * qpow_d(y, k) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 2; k < n; k += 4)
+        xp = xp + (kl0 * (n - k)) * qpow_d(x, n - k - 1) * qpow_d(y, k) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 1; k < n; k += 4)
+        xp = xp + (kl1 * (n - k)) * qpow_d(x, n - k - 1) * qpow_d(y, k) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 3; k < n; k += 4)
+        xp = xp - (kl1 * (n - k)) * qpow_d(x, n - k - 1) * qpow_d(y, k) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 4; k <= n; k += 4)
+        yp = yp - (kl0 * k) * qpow_d(x, n - k) * qpow_d(y, k - 1) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 2; k <= n; k += 4)
+        yp = yp + (kl0 * k) * qpow_d(x, n - k) * qpow_d(y, k - 1) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 1; k <= n; k += 4)
+        yp = yp + (kl1 * k) * qpow_d(x, n - k) * qpow_d(y, k - 1) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 3; k <= n; k += 4)
+        yp = yp - (kl1 * k) * qpow_d(x, n - k) * qpow_d(y, k - 1) / (factorial_d(n - k) * factorial_d(k));
+}
+
+// cf_kick ff_quadrupole.h:22-35
+__device__ __forceinline__ void quad_cf_kick(double x, double& xp, double y, double& yp, const double* kL)
+{
+    thin_quadrupole_unit(x, xp, y, yp, kL[0], kL[1]);
+    if (kL[2] || kL[3]) thin_quadrupole_unit(x, xp, y, yp, kL[2], kL[3]);
+    if (kL[4] || kL[5]) thin_sextupole_unit(x, xp, y, yp, kL[4], kL[5]);
+    if (kL[6] || kL[7]) thin_octupole_unit(x, xp, y, yp, kL[6], kL[7]);
+    if (kL[8] || kL[9]) thin_magnet_unit(x, xp, y, yp, kL[8], kL[9], 5);
+    if (kL[10] || kL[11]) thin_magnet_unit(x, xp, y, yp, kL[10], kL[11], 6);
+    if (kL[12] || kL[13]) thin_magnet_unit(x, xp, y, yp, kL[12], kL[13], 7);
+    if (kL[14] || kL[15]) thin_magnet_unit(x, xp, y, yp, kL[14], kL[15], 8);
+}
+
+// slot_unit ff_algorithm.h:83-129
+__device__ __forceinline__ void slot_unit(double& x, double& xp, double& y, double& yp, double& cdt,
+                                          double& dpop, double ct, double st, double pref, double m)
+{
+    const double uni = 1.0;
+    double zp = sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
+    double p = (dpop + uni) * pref;
+    double e = sqrt(p * p + m * m);
+    double b0 = xp * pref / e;
+    double b1 = yp * pref / e;
+    double b2 = zp * pref / e;
+    double bp = st * b0 + ct * b2;
+    double tau = -x * st / bp;
+    double r0 = x + tau * b0;
+    double r1 = y + tau * b1;
+    double r2 = tau * b2;
+    x = r0 * ct - r2 * st;
+    y = r1;
+    cdt = cdt + tau;
+    xp = xp * ct - zp * st;
+}
+
+// bend_unit ff_algorithm.h:255-343
+__device__ __forceinline__ void bend_unit(double& x, double& xp, double& y, double& yp, double& cdt,
+                                          double dpop, double theta, double strength, double p_ref,
+                                          double m, double cdt_ref, double phase_r, double phase_i,
+                                          double term_r, double term_i)
+{
+    const double uni = 1.0;
+    const double tc = kC;
+    double p0 = p_ref;
+    double p = p_ref * (dpop + uni);
+    double E0 = sqrt(p0 * p0 + m * m);
+    double E = sqrt(p * p + m * m);
+    double igamma = m / E0;
+    double ibeta = uni / sqrt(uni - igamma * igamma);
+    double csq = kC * kC * 1e-9;
+    double psq = (dpop + uni) * (dpop + uni);
+    double Ef = uni / sqrt(psq + igamma * igamma * ibeta * ibeta);
+    double beta1 = Ef * xp;
+    double beta2 = Ef * yp;
+    double beta3 = Ef * sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
+    double ui_r = 0.0, ui_i = x;
+    double vui_r = tc * beta3, vui_i = tc * beta1;
+    double iomega = E / (csq * strength);
+    double bi_r = -vui_i * iomega - ui_r;
+    double bi_i = vui_r * iomega - ui_i;
+    double bf_r = bi_r * phase_r - bi_i * phase_i + term_r;
+    double bf_i = bi_r * phase_i + bi_i * phase_r + term_i;
+    double rho = tc * sqrt(beta1 * beta1 + beta3 * beta3) * iomega;
+    double dthmphi = asin(bi_r / rho) - asin(bf_r / rho);
+    double expf_r = cos(dthmphi);
+    double expf_i = sin(dthmphi);
+    double vuf_i = vui_r * expf_i + vui_i * expf_r;
+    double uf_i = (ui_r + bi_r) * expf_i + (ui_i + bi_i) * expf_r - bf_i;
+    double dtheta = dthmphi + theta;
+    double ncdt = -tc * dtheta * iomega;
+    x = uf_i;
+    xp = vuf_i / (Ef * tc);
+    y = y + beta2 * ncdt;
+    cdt = cdt + ncdt - cdt_ref;
+}
+
+// yoshida6 ff_algorithm.h:1834-2008 with the drift lengths c_i*step_length,
+// the 0.1*step_ref_cdt substep and the d_i-scaled strengths precomputed on
+// the host (identical doubles).  kind selects the kick function.
+template <int KIND>
+__device__ __forceinline__ void yoshida6_op(double& x, double& xp, double& y, double& yp, double& cdt,
+                                            double dpop, const MapOp& op)
+{
+    const double pref = op.d[2], m = op.d[3], sub = op.d[4];
+    const double l1 = op.d[5], l2 = op.d[6], l3 = op.d[7], l4 = op.d[8];
+    const double* k = op.d + 9;
+    constexpr int KS = (KIND == OP_QUAD_CF) ? 16 : 2; // stride between k1..k4
+    auto kick = [&](const double* kk) {
+        if (KIND == OP_QUAD)
+            thin_quadrupole_unit(x, xp, y, yp, kk[0], kk[1]);
+        else if (KIND == OP_SEXT_YOSHIDA)
+            thin_sextupole_unit(x, xp, y, yp, kk[0], kk[1]);
+        else
+            quad_cf_kick(x, xp, y, yp, kk);
+    };
+    const double* k1 = k;
+    const double* k2 = k + KS;
+    const double* k3 = k + 2 * KS;
+    const double* k4 = k + 3 * KS;
+    for (int i = 0; i < op.steps; ++i) {
+        drift_unit(x, xp, y, yp, cdt, dpop, l1, pref, m, sub); kick(k1);
+        drift_unit(x, xp, y, yp, cdt, dpop, l2, pref, m, sub); kick(k2);
+        drift_unit(x, xp, y, yp, cdt, dpop, l2, pref, m, sub); kick(k1);
+        drift_unit(x, xp, y, yp, cdt, dpop, l3, pref, m, sub); kick(k3);
+        drift_unit(x, xp, y, yp, cdt, dpop, l4, pref, m, sub); kick(k4);
+        drift_unit(x, xp, y, yp, cdt, dpop, l4, pref, m, sub); kick(k3);
+        drift_unit(x, xp, y, yp, cdt, dpop, l3, pref, m, sub); kick(k1);
+        drift_unit(x, xp, y, yp, cdt, dpop, l2, pref, m, sub); kick(k2);
+        drift_unit(x, xp, y, yp, cdt, dpop, l2, pref, m, sub); kick(k1);
+        drift_unit(x, xp, y, yp, cdt, dpop, l1, pref, m, sub);
+    }
+}
+
+// collective/utils.h:9-18
+__device__ __forceinline__ void leftmost(double pos, double left, double inv, int& idx, double& off)
+{
+    double s = (pos - left) * inv - 0.5;
+    idx = (int)floor(s);
+    off = s - idx;
+}
+
+
+constexpr int kTrackThreads = 256;
+
+__global__ void __launch_bounds__(kTrackThreads) track_kernel(const __grid_constant__ TrackParams p)
+{
+    __shared__ int s_counts[kMaxOpsPerPass];
+    __shared__ double s_red[kTrackThreads / 32][6];
+    for (int i = threadIdx.x; i < kMaxOpsPerPass; i += blockDim.x) s_counts[i] = 0;
+    __syncthreads();
+
+    double ms[6] = {0, 0, 0, 0, 0, 0};
+    bool want_moments = false;
+
+    const int64_t n = p.n;
+    const int64_t S = p.stride;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        bool alive = p.masks[i] != 0;
+        bool alive_in = alive;
+        int disc = 0;
+        double x = 0, xp = 0, y = 0, yp = 0, cdt = 0, dpop = 0;
+        if (alive) {
+            x = p.parts[i];
+            xp = p.parts[i + S];
+            y = p.parts[i + 2 * S];
+            yp = p.parts[i + 3 * S];
+            cdt = p.parts[i + 4 * S];
+            dpop = p.parts[i + 5 * S];
+        }
+        for (int o = 0; o < p.nops; ++o) {
+            const MapOp& op = p.ops[o];
+            const int kind = op.kind;
+            if (kind >= OP_AP_FINITE && kind <= OP_AP_RECTANGULAR) {
+                // discard_applier bunch_particles.h:484-503: discards(i) is
+                // reset by every aperture, then set if this one discards.
+                disc = 0;
+                if (alive) {
+                    bool d;
+                    if (kind == OP_AP_FINITE) {
+                        if (!isfinite(x) || !isfinite(xp) || !isfinite(y) || !isfinite(yp) ||
+                            !isfinite(cdt) || !isfinite(dpop))
+                            d = true;
+                        else {
+                            double pt = 1.0 + dpop;
+                            d = pt * pt - xp * xp - yp * yp < 0.0;
+                        }
+                    } else if (kind == OP_AP_CIRCULAR) {
+                        double xr = x - op.d[1], yr = y - op.d[2];
+                        d = (xr * xr + yr * yr) > op.d[0];
+                    } else if (kind == OP_AP_ELLIPTICAL) {
+                        double xr = x - op.d[2], yr = y - op.d[3];
+                        d = (xr * xr / op.d[0] + yr * yr / op.d[1]) > 1.0;
+                    } else {
+                        double xr = x - op.d[2], yr = y - op.d[3];
+                        d = (fabs(xr) > 0.5 * op.d[0]) || (fabs(yr) > 0.5 * op.d[1]);
+                    }
+                    if (d) {
+                        disc = 1;
+                        alive = false;
+                        atomicAdd(&s_counts[op.slot - p.slot_base], 1);
+                    }
+                }
+                continue;
+            }
+            if (kind == OP_MOMENTS) {
+                want_moments = true;
+                if (alive) {
+                    ms[0] += x; ms[1] += y; ms[2] += cdt;
+                    ms[3] += x * x; ms[4] += y * y; ms[5] += cdt * cdt;
+                }
+                continue;
+            }
+            if (!alive) continue;
+            switch (kind) {
+            case OP_DRIFT:
+                drift_unit(x, xp, y, yp, cdt, dpop, op.d[0], op.d[1], op.d[2], op.d[3]);
+                break;
+            case OP_QUAD: {
+                double xx = x - op.d[0], yy = y - op.d[1];
+                yoshida6_op<OP_QUAD>(xx, xp, yy, yp, cdt, dpop, op);
+                x = xx + op.d[0];
+                y = yy + op.d[1];
+                break;
+            }
+            case OP_QUAD_CF: {
+                double xx = x - op.d[0], yy = y - op.d[1];
+                yoshida6_op<OP_QUAD_CF>(xx, xp, yy, yp, cdt, dpop, op);
+                x = xx + op.d[0];
+                y = yy + op.d[1];
+                break;
+            }
+            case OP_SEXT_YOSHIDA:
+                yoshida6_op<OP_SEXT_YOSHIDA>(x, xp, y, yp, cdt, dpop, op);
+                break;
+            case OP_THIN_QUAD: {
+                double xx = x - op.d[0], yy = y - op.d[1];
+                thin_quadrupole_unit(xx, xp, yy, yp, op.d[2], op.d[3]);
+                break;
+            }
+            case OP_THIN_SEXT:
+                thin_sextupole_unit(x, xp, y, yp, op.d[2], op.d[3]);
+                break;
+            case OP_MPOLE: {
+                const double* kl = op.d;
+                const int on = op.flags;
+                if (on & 1) { xp = xp - kl[0]; yp = yp + kl[1]; }
+                if (on & 2) thin_quadrupole_unit(x, xp, y, yp, kl[2], kl[3]);
+                if (on & 4) thin_sextupole_unit(x, xp, y, yp, kl[4], kl[5]);
+                if (on & 8) thin_octupole_unit(x, xp, y, yp, kl[6], kl[7]);
+                for (int nn = 4; nn < 8; ++nn)
+                    if (on & (1 << nn)) thin_magnet_unit(x, xp, y, yp, kl[nn * 2], kl[nn * 2 + 1], nn + 1);
+                break;
+            }
+            case OP_SBEND: {
+                const double* d = op.d;
+                if (op.flags & 1) {
+                    slot_unit(x, xp, y, yp, cdt, dpop, d[0], d[1], d[14], d[15]);
+                    yp = yp - d[4] * y; // edge_unit ff_algorithm.h:139-148
+                    xp = xp + d[5] * y;
+                }
+                bend_unit(x, xp, y, yp, cdt, dpop, d[8], d[13], d[14], d[15], d[16], d[9], d[10], d[11], d[12]);
+                if (op.flags & 2) {
+                    yp = yp - d[6] * y;
+                    xp = xp + d[7] * y;
+                    slot_unit(x, xp, y, yp, cdt, dpop, d[2], d[3], d[14], d[15]);
+                }
+                break;
+            }
+            case OP_SC_KICK: {
+                // zyx::alg_kicker space_charge_3d_kernels.h:91-215
+                const ScState& sc = *p.sc;
+                if (!sc.valid) break;
+                int ix, iy, iz;
+                double ox, oy, oz;
+                leftmost(x, sc.left[0], sc.ih[0], ix, ox);
+                leftmost(y, sc.left[1], sc.ih[1], iy, oy);
+                leftmost(cdt, sc.left[2], sc.ih[2], iz, oz);
+                const int gx = p.gx, gy = p.gy, gz = p.gz;
+                if (!((ix >= 0 && ix < gx - 1) && (iy >= 0 && iy < gy - 1) && (iz >= 0 && iz < gz - 1)))
+                    break;
+                double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
+                const int64_t b0 = ((int64_t)iz * gy + iy) * gx + ix;
+                const int64_t b1 = ((int64_t)(iz + 1) * gy + iy) * gx + ix;
+                const double2* E = p.efield;
+                // corner fields: .x/.y of [2c] = ex, ey; .x of [2c+1] = ez
+                double2 a00 = E[2 * b0], a01 = E[2 * (b0 + 1)], a10 = E[2 * (b0 + gx)], a11 = E[2 * (b0 + gx + 1)];
+                double2 c00 = E[2 * b1], c01 = E[2 * (b1 + 1)], c10 = E[2 * (b1 + gx)], c11 = E[2 * (b1 + gx + 1)];
+                double z00 = E[2 * b0 + 1].x, z01 = E[2 * (b0 + 1) + 1].x, z10 = E[2 * (b0 + gx) + 1].x,
+                       z11 = E[2 * (b0 + gx + 1) + 1].x;
+                double w00 = E[2 * b1 + 1].x, w01 = E[2 * (b1 + 1) + 1].x, w10 = E[2 * (b1 + gx) + 1].x,
+                       w11 = E[2 * (b1 + gx + 1) + 1].x;
+                const double factor = sc.factor, pref = p.kick_pref, m = p.kick_m;
+                double val = aoz * aoy * aox * z00;
+                val += aoz * aoy * ox * z01;
+                val += aoz * oy * aox * z10;
+                val += aoz * oy * ox * z11;
+                val += oz * aoy * aox * w00;
+                val += oz * aoy * ox * w01;
+                val += oz * oy * aox * w10;
+                val += oz * oy * ox * w11;
+                double pp = pref + dpop * pref;
+                double Eoc_i = sqrt(pp * pp + m * m);
+                double Eoc_f = Eoc_i + factor * (-pref) * val;
+                double ddp = (sqrt(Eoc_f * Eoc_f - m * m) - sqrt(Eoc_i * Eoc_i - m * m)) / pref;
+                dpop += ddp;
+                val = aoz * aoy * aox * a00.y;
+                val += aoz * aoy * ox * a01.y;
+                val += aoz * oy * aox * a10.y;
+                val += aoz * oy * ox * a11.y;
+                val += oz * aoy * aox * c00.y;
+                val += oz * aoy * ox * c01.y;
+                val += oz * oy * aox * c10.y;
+                val += oz * oy * ox * c11.y;
+                yp += factor * val;
+                val = aoz * aoy * aox * a00.x;
+                val += aoz * aoy * ox * a01.x;
+                val += aoz * oy * aox * a10.x;
+                val += aoz * oy * ox * a11.x;
+                val += oz * aoy * aox * c00.x;
+                val += oz * aoy * ox * c01.x;
+                val += oz * oy * aox * c10.x;
+                val += oz * oy * ox * c11.x;
+                xp += factor * val;
+                break;
+            }
+            default:
+                break;
+            }
+        }
+        if (alive_in) {
+            p.parts[i] = x;
+            p.parts[i + S] = xp;
+            p.parts[i + 2 * S] = y;
+            p.parts[i + 3 * S] = yp;
+            p.parts[i + 4 * S] = cdt;
+            p.parts[i + 5 * S] = dpop;
+            if (!alive) p.masks[i] = 0;
+        }
+        if (p.write_discards && p.discards) p.discards[i] = (uint8_t)disc;
+    }
+
+    // per-aperture discard counts
+    __syncthreads();
+    for (int s = threadIdx.x; s < kMaxOpsPerPass; s += blockDim.x)
+        if (s_counts[s]) atomicAdd(&p.ap_counts[p.slot_base + s], s_counts[s]);
+
+    // moments: fixed-order block reduction -> one partial per block
+    bool any_mom = false;
+    for (int o = 0; o < p.nops; ++o) any_mom |= (p.ops[o].kind == OP_MOMENTS);
+    (void)want_moments;
+    if (any_mom && p.moment_partials) {
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        for (int j = 0; j < 6; ++j) {
+            double v = ms[j];
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0) s_red[w][j] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < 6) {
+            double v = 0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) v += s_red[k][threadIdx.x];
+            p.moment_partials[blockIdx.x * 6 + threadIdx.x] = v;
+        }
+    }
+}
+
+// Masked sums for diagnostics: mean (6) or central second moments (21 lower
+// triangle) per block, core_diagnostics.cc:105-111,174-186.
+__global__ void __launch_bounds__(256) moments_kernel(const double* parts, int64_t stride,
+                                                      const uint8_t* masks, int64_t n,
+                                                      const double* mean, double* partials)
+{
+    __shared__ double s_red[8][28];
+    double acc[27];
+    for (int j = 0; j < 27; ++j) acc[j] = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (!masks[i]) continue;
+        double v[6];
+        for (int j = 0; j < 6; ++j) v[j] = parts[i + j * stride];
+        for (int j = 0; j < 6; ++j) acc[j] += v[j];
+        if (mean) {
+            int t = 6;
+            for (int j = 0; j < 6; ++j) {
+                double dj = v[j] - mean[j];
+                for (int k = 0; k <= j; ++k) acc[t++] += dj * (v[k] - mean[k]);
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int j = 0; j < 27; ++j) {
+        double v = acc[j];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) s_red[w][j] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 27) {
+        double v = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) v += s_red[k][threadIdx.x];
+        partials[blockIdx.x * 27 + threadIdx.x] = v;
+    }
+}
+
+// Counter-based normal generator: Philox-4x32-10 (Salmon et al., SC'11)
+// keyed by the seed, counter = (particle, column pair); Box-Muller.
+__device__ __forceinline__ void philox4x32(uint32_t c[4], uint32_t k0, uint32_t k1)
+{
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
+        uint32_t n0 = hi1 ^ c[1] ^ k0, n1 = lo1, n2 = hi0 ^ c[3] ^ k1, n3 = lo0;
+        c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+__global__ void populate_kernel(double* parts, int64_t stride, uint8_t* masks, int64_t n,
+                                double s0, double s1, double s2, double s3, double s4, double s5,
+                                uint64_t seed)
+{
+    const double sig[6] = {s0, s1, s2, s3, s4, s5};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        for (int pr = 0; pr < 3; ++pr) {
+            uint32_t c[4] = {(uint32_t)i, (uint32_t)(i >> 32), (uint32_t)pr, 0x5b200u};
+            philox4x32(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+            uint64_t a = ((uint64_t)c[0] << 32) | c[1];
+            uint64_t b = ((uint64_t)c[2] << 32) | c[3];
+            double u1 = ((a >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+            double u2 = ((b >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+            double r = sqrt(-2.0 * log(u1));
+            double sn, cs;
+            sincospi(2.0 * u2, &sn, &cs);
+            parts[i + (2 * pr) * stride] = sig[2 * pr] * r * cs;
+            parts[i + (2 * pr + 1) * stride] = sig[2 * pr + 1] * r * sn;
+        }
+        parts[i + 6 * stride] = (double)i;
+        masks[i] = 1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers (called from host.cc)
+// ---------------------------------------------------------------------------
+int track_grid_blocks()
+{
+    static int nb = 0;
+    if (!nb) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        nb = sms * 8;
+    }
+    return nb;
+}
+
+cudaError_t launch_track(const TrackParams& p, cudaStream_t s)
+{
+    int nb = track_grid_blocks();
+    track_kernel<<<nb, kTrackThreads, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_moments(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
+                           const double* mean, double* partials, int nblocks, cudaStream_t s)
+{
+    moments_kernel<<<nblocks, 256, 0, s>>>(parts, stride, masks, n, mean, partials);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_populate(double* parts, int64_t stride, uint8_t* masks, int64_t n, const double* sig,
+                            uint64_t seed, cudaStream_t s)
+{
+    int nb = track_grid_blocks();
+    populate_kernel<<<nb, 256, 0, s>>>(parts, stride, masks, n, sig[0], sig[1], sig[2], sig[3], sig[4],
+                                       sig[5], seed);
+    return cudaGetLastError();
+}
+
+} // namespace sb2

@@ -1,0 +1,200 @@
+"""GPU parity of the element maps and apertures against the oracle.
+
+The FP64 map kernels run without FMA contraction and with IEEE sqrt/div, so
+drift, quadrupole (Yoshida), thin multipole and sextupole maps are compared
+bit for bit with the oracle; the sector bend calls asin/sin/cos, whose CUDA
+and libm results may differ in the last bit, so it is held to 1e-12
+relative.  Particle ids and lost-particle sets must match exactly.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from helpers import (MP, ROOT, SIG_C0, elem, fodo_cell, gaussian_bunch, oracle_lattice, product_lattice,
+                     ring_cell)
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.load(open(os.path.join(ROOT, "tests", "golden", "madx_tracks.json")))["cases"]
+
+
+def run_both(syn, orc, spec, parts, stepper, num, turns, value=2.5 + MP, kind=0, masks=None, real_num=1e11):
+    n = parts.shape[0]
+    lat, ref = product_lattice(spec, value=value, kind=kind)
+    if stepper == "indep":
+        st, ok = syn.Independent_stepper_elements(num), orc.STEPPER_INDEP_ELEMENTS
+    elif stepper == "split":
+        st, ok = syn.Split_operator_stepper(None, num), orc.STEPPER_SPLIT
+    else:
+        st, ok = syn.Split_operator_stepper_elements(None, num), orc.STEPPER_SPLIT_ELEMENTS
+    prop = syn.Propagator(lat, st)
+    b = syn.Bunch(ref, n, real_num)
+    b.set_particles(parts, masks)
+    prop.propagate(b, turns)
+    gp, gm, gd = b.get_particles()
+    sim = orc.Sim(oracle_lattice(spec, value=value, kind=kind), n, real_num, stepper=ok, num=num,
+                  value=value, kind=kind)
+    sim.set_particles(parts, masks)
+    sim.propagate(turns)
+    op, om, od = sim.get_particles()
+    return (gp, gm, gd, b, prop), (op, om, od, sim)
+
+
+@pytest.mark.parametrize("case", GOLDEN, ids=[c["name"] for c in GOLDEN])
+def test_gpu_madx_golden(syn, orc, case):
+    """The reference's MAD-X element tests through the GPU path: within the
+    reference's tolerances of MAD-X and bit-identical to the oracle."""
+    p = np.zeros((16, 7), order="F")
+    p[:, :6] = np.array(case["initial"])
+    p[:, 6] = np.arange(16)
+    (gp, gm, _, _, _), (op, _, _, _) = run_both(syn, orc, case["lattice"], p, "indep", 1, 1,
+                                                value=case["p0"], kind=1, real_num=1e10)
+    exp = np.array(case["expected"])
+    tol = np.array(case["tol"])
+    assert np.all(np.abs(gp[:, :6] - exp) <= tol)
+    assert np.array_equal(gp, op)
+    assert gm.all()
+
+
+def test_gpu_fodo_no_space_charge_bit_exact(syn, orc):
+    """FODO cell, split-operator stepper with 8 steps and no collective
+    operator, 3 turns: every coordinate bit-identical to the oracle."""
+    n = 20000
+    p = gaussian_bunch(n, SIG_C0, 11)
+    (gp, gm, gd, b, _), (op, om, od, sim) = run_both(syn, orc, fodo_cell(), p, "split", 8, 3)
+    assert np.array_equal(gp, op)
+    assert np.array_equal(gm, om) and gm.all()
+    st_g, sn_g = b.design_state()
+    st_o, sn_o = sim.design_state()
+    assert np.array_equal(st_g, st_o) and sn_g == sn_o
+
+
+def test_gpu_ring_losses_exact(syn, orc):
+    """Ring cell (sector bends, thin sextupoles, r = 4 mm circular aperture
+    on every element) with a bunch wide enough to lose particles: lost sets,
+    ids, discards and the n_valid / n_total / real_num bookkeeping match the
+    oracle exactly; surviving coordinates within 1e-12 relative."""
+    n = 30000
+    p = gaussian_bunch(n, [2e-3, 1e-4, 2e-3, 1e-4, 0.3, 1e-4], 5)
+    (gp, gm, gd, b, _), (op, om, od, sim) = run_both(syn, orc, ring_cell(radius=0.004), p, "split", 16, 2)
+    assert np.array_equal(gm, om)
+    assert np.array_equal(gd, od)
+    assert 0 < int(gm.sum()) < n
+    assert np.array_equal(gp[:, 6], op[:, 6])
+    scale = np.max(np.abs(op[:, :6]), axis=0)
+    alive = om.astype(bool)
+    err = np.max(np.abs(gp[alive, :6] - op[alive, :6]), axis=0) / scale
+    assert np.all(err <= 1e-12), err
+    c = b.counts()
+    nv, nt, rn = sim.counts()
+    assert c["local_num"] == nv and c["total_num"] == nt
+    assert c["real_num"] == rn
+
+
+def test_gpu_finite_aperture_discards_nan(syn, orc):
+    """Finite_aperture (aperture_operation.h:54-86) drops NaN/Inf particles
+    and particles with (1+dpop)^2 < xp^2 + yp^2."""
+    n = 1000
+    p = gaussian_bunch(n, SIG_C0, 2)
+    p[3, 0] = np.nan
+    p[7, 1] = np.inf
+    p[11, 1] = 2.0  # xp > 1 + dpop
+    (gp, gm, gd, b, _), (op, om, od, _) = run_both(syn, orc, fodo_cell(), p, "split", 4, 1)
+    assert not gm[3] and not gm[7] and not gm[11]
+    assert np.array_equal(gm, om)
+    assert b.get_total_num() == n - 3
+
+
+def test_gpu_masked_particles_frozen(syn, orc):
+    """Masked-out particles are not propagated (masks checked per particle,
+    gsv size 1 on the GPU build)."""
+    n = 512
+    p = gaussian_bunch(n, SIG_C0, 9)
+    m = np.ones(n, np.uint8)
+    m[::7] = 0
+    (gp, gm, _, b, _), (op, om, _, _) = run_both(syn, orc, fodo_cell(), p, "split", 8, 1, masks=m)
+    assert np.array_equal(gp[~m.astype(bool)], p[~m.astype(bool)])
+    assert np.array_equal(gp, op) and np.array_equal(gm, om)
+
+
+@pytest.mark.parametrize("elem_def,tol", [
+    (elem("sbend", "b", l=2.0, angle=math.pi / 24), 2.0e-17),
+    (elem("drift", "d", l=10.0), 2.0e-17),
+    (elem("quadrupole", "q", l=4.0, k1=1 / 10), 2.0e-17),
+    (elem("sextupole", "s", l=0.5, k2=0.25), 2.0e-17),
+    (elem("quadrupole", "q", l=4.0, k1=1 / 10, tilt=math.pi / 4), 2.0e-17),
+])
+def test_gpu_zero_particle(syn, orc, elem_def, tol):
+    """libFF/tests/test_zeroparticle_propagate.cc: a particle at 0 stays at 0
+    and the design particle's cdt * beta equals the element length."""
+    n = 8
+    p = np.zeros((n, 7), order="F")
+    p[:, 6] = np.arange(n)
+    value = 0.8 + MP
+    (gp, _, _, b, _), (op, _, _, sim) = run_both(syn, orc, [elem_def], p, "indep", 1, 1, value=value, real_num=1e9)
+    assert np.all(np.abs(gp[0, :4]) < tol)
+    st, _ = b.design_state()
+    gamma = value / MP
+    beta = math.sqrt(1 - 1 / gamma ** 2)
+    L = elem_def["double"]["l"]
+    assert abs(1 - st[4] * beta / L) < 1.0e-7
+    assert np.allclose(gp, op, rtol=0, atol=1e-15)
+
+
+def test_gpu_thin_elements_and_edge_apertures(syn, orc):
+    """Thin multipole (MAD-X knl/ksl and MAD8 kNl forms, tilt), thin
+    sextupole, element apertures from aperture_type (independent_operator.cc:
+    41-72), elliptical and rectangular apertures."""
+    spec = [elem("drift", "d0", l=0.3),
+            elem("multipole", "m1", knl=[0.0, 0.02, 1.5], ksl=[0.0, 0.0, 0.3], tilt=0.1),
+            elem("multipole", "m2", k1l=0.01, k2l=-0.5, t2=0.05),
+            elem("quadrupole", "q", l=0.4, k1=0.7, aperture_type="elliptical",
+                 elliptical_aperture_horizontal_radius=0.004, elliptical_aperture_vertical_radius=0.003),
+            elem("sextupole", "s", l=0.0, k2=3.0, k2s=0.5),
+            elem("drift", "d1", l=0.6, aperture_type="rectangular", rectangular_aperture_width=0.008,
+                 rectangular_aperture_height=0.006)]
+    n = 20000
+    p = gaussian_bunch(n, [2e-3, 2e-4, 2e-3, 2e-4, 0.3, 1e-3], 4)
+    (gp, gm, gd, b, _), (op, om, od, sim) = run_both(syn, orc, spec, p, "split", 3, 2)
+    assert np.array_equal(gm, om) and np.array_equal(gd, od)
+    assert 0 < int(gm.sum()) < n
+    assert np.array_equal(gp, op)
+
+
+def test_gpu_quad_multipole_errors(syn, orc):
+    """Quadrupole with a_n / b_n multipole errors (cf_kick, ff_quadrupole.h:
+    22-35, 362-391) and offsets."""
+    spec = [elem("quadrupole", "q", l=0.8, k1=0.5, b2=0.3, a3=0.1, hoffset=1e-4, voffset=-2e-4, tilt=0.02,
+                 yoshida_steps=3), elem("drift", "d", l=1.0)]
+    n = 5000
+    p = gaussian_bunch(n, SIG_C0, 8)
+    (gp, gm, _, _, _), (op, om, _, _) = run_both(syn, orc, spec, p, "indep", 2, 1)
+    assert np.array_equal(gp, op)
+
+
+def test_gpu_yoshida_sextupole_thick(syn, orc):
+    n = 5000
+    p = gaussian_bunch(n, SIG_C0, 6)
+    spec = [elem("sextupole", "s", l=0.7, k2=2.0, k2s=0.3, tilt=0.1), elem("drift", "d", l=0.5)]
+    (gp, _, _, b, _), (op, _, _, sim) = run_both(syn, orc, spec, p, "indep", 3, 2)
+    assert np.array_equal(gp, op)
+    assert np.array_equal(b.design_state()[0], sim.design_state()[0])
+
+
+def test_gpu_empty_bunch(syn):
+    lat, ref = product_lattice(fodo_cell())
+    prop = syn.Propagator(lat, syn.Split_operator_stepper(None, 8))
+    b = syn.Bunch(ref, 0, 1e11)
+    prop.propagate(b, 2)
+    assert b.get_total_num() == 0
+
+
+def test_gpu_unsupported_element_is_reported(syn):
+    lat, ref = product_lattice([elem("rfcavity", "rf", l=1.0, volt=0.1)])
+    prop = syn.Propagator(lat, syn.Independent_stepper_elements(1))
+    b = syn.Bunch(ref, 16, 1e10)
+    with pytest.raises(syn.SB2Error, match="rfcavity"):
+        prop.propagate(b, 1)

@@ -1,0 +1,166 @@
+"""GPU parity of the 3D open-boundary Hockney space-charge solver.
+
+FP64 tolerances (written in each test):
+  * charge density, potential and fields: 1e-10 relative L2 against the
+    oracle on the same particles (the deposit's summation order and the FFT
+    algorithm are the only differences);
+  * kicked coordinates: the kick itself (xp, yp, dpop change) within 1e-9
+    relative of the oracle's kick, positions bit-identical;
+  * known answers of the reference's own tests: rod-bunch line-charge kick
+    and Gaussian-sphere field.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import MP, SIG_C0, fodo_cell, gaussian_bunch, oracle_lattice, product_lattice, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-10
+
+
+def sc_both(syn, orc, parts, shape, time_step, real_num=1e11, green_fn=1, fixed=None, value=2.5 + MP, masks=None):
+    gx, gy, gz = shape
+    opts = syn.Space_charge_3d_open_hockney_options(gx, gy, gz)
+    opts.green_fn = green_fn
+    if fixed is not None:
+        opts.set_fixed_domain(*fixed)
+    fm = syn.Four_momentum(MP, value)
+    ref = syn.Reference_particle(1, fm)
+    b = syn.Bunch(ref, parts.shape[0], real_num)
+    b.set_particles(parts, masks)
+    sc = syn.Space_charge_3d_open_hockney(opts)
+    sc.apply(b, time_step)
+    gp, gm, _ = b.get_particles()
+    g = sc.last()
+    oopts = orc.SCOptions.make(gx, gy, gz, green_fn=green_fn, fixed=fixed)
+    op, o = orc.sc_apply(oopts, parts, time_step, real_num, masks=masks, value=value, kind=orc.REF_TOTAL_ENERGY)
+    return gp, g, op, o
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 32), (32, 16, 64), (8, 32, 16)])
+@pytest.mark.parametrize("green_fn", [1, 0])
+def test_sc_fields_match_oracle(syn, orc, shape, green_fn):
+    n = 200000
+    p = gaussian_bunch(n, SIG_C0, 21)
+    ts = 1.25 / (0.96 * 299792458.0)
+    gp, g, op, o = sc_both(syn, orc, p, shape, ts, green_fn=green_fn)
+    assert np.allclose(g["left"], o["left"], rtol=1e-13, atol=0)
+    assert np.allclose(g["h"], o["h"], rtol=1e-13, atol=0)
+    assert rel_l2(g["rho"], o["rho"]) <= FIELD_TOL
+    assert rel_l2(g["phi"], o["phi"]) <= FIELD_TOL
+    for c in ("ex", "ey", "ez"):
+        assert rel_l2(g[c], o[c]) <= FIELD_TOL, c
+    assert abs(g["fn_norm"] / o["fn_norm"] - 1) <= 1e-13
+    assert abs(g["factor"] / o["factor"] - 1) <= 1e-13
+    # positions untouched, kicks agree
+    for j in (0, 2, 4, 6):
+        assert np.array_equal(gp[:, j], op[:, j])
+    for j in (1, 3, 5):
+        kick_g = gp[:, j] - p[:, j]
+        kick_o = op[:, j] - p[:, j]
+        assert rel_l2(kick_g, kick_o) <= 1e-9, j
+
+
+def test_sc_fixed_domain_and_masks(syn, orc):
+    n = 100000
+    p = gaussian_bunch(n, SIG_C0, 22)
+    m = np.ones(n, np.uint8)
+    m[::5] = 0
+    fixed = ((0.0, 0.0, 0.0), (8e-3, 8e-3, 2.4))
+    gp, g, op, o = sc_both(syn, orc, p, (16, 16, 16), 1e-8, fixed=fixed, masks=m)
+    assert rel_l2(g["rho"], o["rho"]) <= FIELD_TOL
+    for c in ("ex", "ey", "ez"):
+        assert rel_l2(g[c], o[c]) <= FIELD_TOL
+    dead = ~m.astype(bool)
+    assert np.array_equal(gp[dead], p[dead])
+
+
+def test_sc_rod_bunch_line_charge(syn):
+    """collective/tests/test_space_charge_3d_open_hockney_mpi.cc:8-107 at the
+    reference's size (2,000,009 particles, 256 x 256 x 64, fixed domain):
+    probe kick vs 2 N r_p / (L beta^2 gamma^3) * D / r to 1e-3 relative
+    (the reference allows 0.01 absolute)."""
+    from test_oracle import rod_bunch
+    for gamma in (61.0 / 60.0, 61.0 / 11.0):
+        p, beta = rod_bunch(250001, gamma)
+        probe = 80e-6
+        opts = syn.Space_charge_3d_open_hockney_options(256, 256, 64)
+        opts.set_fixed_domain([0, 0, 0], [probe * 4, probe * 4, 0.1 / beta])
+        ref = syn.Reference_particle(1, syn.Four_momentum(MP, MP * gamma))
+        b = syn.Bunch(ref, p.shape[0], 5.0e9)
+        b.set_particles(p)
+        syn.Space_charge_3d_open_hockney(opts).apply(b, 0.1 / (beta * 299792458.0))
+        out = b.get_particles()[0]
+        bg = beta * gamma
+        rp = syn.pconstants.rp
+        expected = ((2.0 * 5.0e9 * rp) / (0.1 * bg * bg * gamma)) * (0.1 / probe)
+        assert abs(out[0, 1] - expected) < 0.01
+        assert abs(out[0, 1] / expected - 1) < 1e-3
+
+
+def test_sc_degenerate_domain_error(syn):
+    """space_charge_3d_open_hockney.cc:512-516: all sigmas below 1e-10."""
+    ref = syn.Reference_particle(1, syn.Four_momentum(MP, MP + 2.5))
+    b = syn.Bunch(ref, 1000, 1e10)
+    sc = syn.Space_charge_3d_open_hockney(syn.Space_charge_3d_open_hockney_options(8, 8, 8))
+    with pytest.raises(syn.SB2Error, match="neglible extent"):
+        sc.apply(b, 1e-9)
+
+
+def test_propagate_with_space_charge_matches_oracle(syn, orc):
+    """FODO cell, split operator with 8 kicks per cell, adaptive domain,
+    linear Green function, 2 turns (16 kicks): last solve's fields within
+    1e-10 of the oracle's, coordinates within 1e-10 relative, ids and masks
+    exact."""
+    n, shape, turns = 100000, (16, 16, 32), 2
+    p = gaussian_bunch(n, SIG_C0, 31)
+    lat, ref = product_lattice(fodo_cell())
+    opts = syn.Space_charge_3d_open_hockney_options(*shape)
+    prop = syn.Propagator(lat, syn.Split_operator_stepper(opts, 8))
+    b = syn.Bunch(ref, n, 1e11)
+    b.set_particles(p)
+    prop.propagate(b, turns)
+    gp, gm, _ = b.get_particles()
+    g = prop.sc_last()
+    sim = orc.Sim(oracle_lattice(fodo_cell()), n, 1e11, stepper=orc.STEPPER_SPLIT, num=8,
+                  sc=orc.SCOptions.make(*shape), value=2.5 + MP)
+    sim.set_particles(p)
+    sim.propagate(turns)
+    op, om, _ = sim.get_particles()
+    o = sim.sc_last(shape)
+    assert np.array_equal(gm, om) and np.array_equal(gp[:, 6], op[:, 6])
+    for c in ("rho", "ex", "ey", "ez"):
+        assert rel_l2(g[c], o[c]) <= FIELD_TOL, c
+    for j in range(6):
+        assert rel_l2(gp[:, j], op[:, j]) <= 1e-10, j
+
+
+def test_bunch_moments_and_emittance(syn):
+    n = 100000
+    p = gaussian_bunch(n, SIG_C0, 41)
+    ref = syn.Reference_particle(1, syn.Four_momentum(MP, MP + 2.5))
+    b = syn.Bunch(ref, n, 1e11)
+    b.set_particles(p)
+    mean, mom2, emit = b.moments()
+    assert np.allclose(mean, p[:, :6].mean(0), rtol=0, atol=1e-12)
+    c = np.cov(p[:, :6].T, bias=True)
+    assert np.allclose(mom2, c, rtol=1e-9, atol=1e-30)
+    ex = math.sqrt(c[0, 0] * c[1, 1] - c[0, 1] ** 2)
+    assert abs(emit[0] / ex - 1) < 1e-9
+
+
+def test_populate_gaussian_statistics(syn):
+    n = 1 << 20
+    ref = syn.Reference_particle(1, syn.Four_momentum(MP, MP + 2.5))
+    b = syn.Bunch(ref, n, 1e11)
+    b.populate_gaussian(SIG_C0, seed=3)
+    p, m, _ = b.get_particles()
+    assert m.all() and np.array_equal(p[:, 6], np.arange(n))
+    sd = p[:, :6].std(0)
+    assert np.allclose(sd, SIG_C0, rtol=5e-3)
+    b2 = syn.Bunch(ref, n, 1e11)
+    b2.populate_gaussian(SIG_C0, seed=3)
+    assert np.array_equal(b2.get_particles()[0], p)
