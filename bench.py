@@ -160,6 +160,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=8)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--particles", type=int, default=N_PART, help="bunch size (profiling cases only)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -189,7 +191,8 @@ def main():
     lat, ref = fodo_lattice(syn)
     opts = syn.Space_charge_3d_open_hockney_options(*GRID)
     prop = syn.Propagator(lat, syn.Split_operator_stepper(opts, KICKS_PER_CELL))
-    bunch = syn.Bunch(ref, N_PART, REAL_NUM)
+    npart = args.particles
+    bunch = syn.Bunch(ref, npart, REAL_NUM)
     bunch.populate_gaussian(SIGMAS, seed=1 + rank)
 
     def barrier():
@@ -237,26 +240,27 @@ def main():
     # end to end through the public API with host buffers: checkin from pinned
     # host memory, K steps (each returning the bunch counts to the host),
     # checkout to pinned host memory.
-    host = torch.empty((7, N_PART), dtype=torch.float64, pin_memory=True)
-    hmask = torch.empty(N_PART, dtype=torch.uint8, pin_memory=True)
+    host = torch.empty((7, npart), dtype=torch.float64, pin_memory=True)
+    hmask = torch.empty(npart, dtype=torch.uint8, pin_memory=True)
     pd = ctypes.cast(host.data_ptr(), ctypes.POINTER(ctypes.c_double))
     pm = ctypes.cast(hmask.data_ptr(), ctypes.POINTER(ctypes.c_uint8))
     syn.check(L.sb2_bunch_get_particles(bunch.h, pd, pm, None))
     barrier()
+    e2e_steps = 0 if args.no_e2e else args.steps
     t0 = time.perf_counter()
     syn.check(L.sb2_bunch_set_particles(bunch.h, pd, pm))
-    for k in range(args.steps):
+    for k in range(e2e_steps):
         syn.check(L.sb2_propagator_propagate_steps(prop.h, bunch.h, args.warmup + k, 1, sp))
     syn.check(L.sb2_bunch_get_particles(bunch.h, pd, pm, None))
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    e2e_total = bunch.get_total_num() * args.steps
+    e2e_total = bunch.get_total_num() * max(e2e_steps, 1)
     if dist is not None:
         t = torch.tensor([e2e_s, float(e2e_total)], device="cuda", dtype=torch.float64)
         dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
         dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
         e2e_s, e2e_total = t[0].item(), t[1].item()
-    bunch_bytes = N_PART * (7 * 8 + 1)
+    bunch_bytes = npart * (7 * 8 + 1)
 
     if rank == 0:
         pk, src = peaks()
@@ -281,7 +285,8 @@ def main():
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "global_batch": N_PART * world, "grid": list(GRID),
+            "config": {"workload": WORKLOAD if npart == N_PART else WORKLOAD.replace("4,194,304", str(npart)),
+                       "global_batch": npart * world, "grid": list(GRID),
                        "precision": "fp64 (drop-in)", "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (bunch 235 MB per GPU)",
                        "step_breakdown_ms": {k: round(v[0] / args.steps, 4) for k, v in prof.items()}},
@@ -297,7 +302,7 @@ def main():
             "gpu_launches": gpu_launches,
             "clocks": clk,
         }
-        if not args.no_cpu_baseline and world == 1:
+        if not args.no_cpu_baseline and world == 1 and npart == N_PART:
             out["cpu_baseline"] = cpu_baseline()
         print(json.dumps(out))
     if dist is not None:

@@ -47,9 +47,11 @@ struct Error : std::runtime_error {
 
 static void cuda_check(cudaError_t e, const char* what)
 {
-    if (e != cudaSuccess)
+    if (e != cudaSuccess) {
+        cudaGetLastError(); // clear a non-sticky error so later launch checks do not see it
         throw Error(e == cudaErrorMemoryAllocation ? SB2_ERR_NOMEM : SB2_ERR_CUDA,
                     std::string(what) + ": " + cudaGetErrorString(e));
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1136,8 +1138,8 @@ struct SpaceCharge {
             if (o.shape[i] < 3) throw Error(SB2_ERR_INVALID, "space-charge grid shape must be >= 3 in each dimension");
             if (o.doubled_shape[i] != 2 * o.shape[i])
                 throw Error(SB2_ERR_UNSUPPORTED, "doubled_shape must be 2 * shape on the GPU path");
-            if (!is_pow2(o.doubled_shape[i]) || o.doubled_shape[i] < 8 || o.doubled_shape[i] > 4096)
-                throw Error(SB2_ERR_UNSUPPORTED, "doubled grid sizes must be powers of two in [8, 4096] on the GPU path");
+            if (!is_pow2(o.doubled_shape[i]) || o.doubled_shape[i] < 8 || o.doubled_shape[i] > 2048)
+                throw Error(SB2_ERR_UNSUPPORTED, "doubled grid sizes must be powers of two in [8, 2048] on the GPU path");
         }
         if (o.periodic_z)
             throw Error(SB2_ERR_RUNTIME, "Space_charge_3d_open_hockney::get_green_fn2_linear: periodic_z not yet implemented");
@@ -1190,15 +1192,16 @@ struct SpaceCharge {
         cudaFree(tw_y);
         cudaFree(tw_z);
     }
+    // exp(-2 pi i k / L), k < L, from long-double sin/cos
     static double2* twiddles(int L)
     {
-        std::vector<double2> h(L / 2);
-        for (int k = 0; k < L / 2; ++k) {
+        std::vector<double2> h(L);
+        for (int k = 0; k < L; ++k) {
             long double a = -2.0L * 3.14159265358979323846264338327950288L * k / L;
             h[k] = make_double2((double)std::cos(a), (double)std::sin(a));
         }
-        double2* dp = dalloc<double2>(L / 2, "twiddles");
-        cuda_check(cudaMemcpy(dp, h.data(), sizeof(double2) * (L / 2), cudaMemcpyHostToDevice), "twiddles");
+        double2* dp = dalloc<double2>(L, "twiddles");
+        cuda_check(cudaMemcpy(dp, h.data(), sizeof(double2) * L, cudaMemcpyHostToDevice), "twiddles");
         return dp;
     }
 
@@ -1646,12 +1649,13 @@ sb2_status sb2_bunch_create(int32_t charge, double mass, double value, int32_t k
     b.n = n;
     b.stride = n;
     b.owns = true;
-    b.parts = dalloc<double>((size_t)7 * n, "particles");
-    b.masks = dalloc<uint8_t>(n, "masks");
-    b.discards = dalloc<uint8_t>(n, "discards");
-    cuda_check(cudaMemset(b.parts, 0, sizeof(double) * 7 * std::max<int64_t>(n, 1)), "memset");
-    cuda_check(cudaMemset(b.masks, 1, std::max<int64_t>(n, 1)), "memset");
-    cuda_check(cudaMemset(b.discards, 0, std::max<int64_t>(n, 1)), "memset");
+    const int64_t cap = std::max<int64_t>(n, 1);
+    b.parts = dalloc<double>((size_t)7 * cap, "particles");
+    b.masks = dalloc<uint8_t>(cap, "masks");
+    b.discards = dalloc<uint8_t>(cap, "discards");
+    cuda_check(cudaMemset(b.parts, 0, sizeof(double) * 7 * cap), "memset");
+    cuda_check(cudaMemset(b.masks, 1, cap), "memset");
+    cuda_check(cudaMemset(b.discards, 0, cap), "memset");
     if (n) { // ids 0..n-1 (bunch_particles.cc:283-300)
         std::vector<double> ids(n);
         for (int64_t i = 0; i < n; ++i) ids[i] = (double)i;

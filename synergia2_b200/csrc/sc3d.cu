@@ -14,8 +14,8 @@
 // FFT), y (first gy inputs), z forward + Ghat multiply + z inverse in one
 // kernel (first gz inputs, first gz outputs), y inverse (first gy outputs),
 // x inverse (Hermitian pairs, first gx outputs).  Each pass stages a tile of
-// lines in shared memory and runs a radix-2 Stockham-free in-place
-// Cooley-Tukey transform there.
+// lines in shared memory and runs a Stockham transform there with radix-8/4/2
+// butterflies in registers.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cstdint>
@@ -261,10 +261,12 @@ __global__ void green_octant_kernel(const ScState* __restrict__ scp, double* G, 
 }
 
 // ---------------------------------------------------------------------------
-// Shared-memory radix-2 FFT core.  A tile holds `nl` lines of length L
-// (L a power of two) as s[line * L + j].  DIT expects bit-reversed input and
-// leaves natural order; DIF takes natural order and leaves bit-reversed.
-// tw[k] = exp(-2 pi i k / L), k < L/2; `inv` conjugates.
+// Shared-memory Stockham FFT with radix-8/4/2 butterflies in registers.
+// A tile holds `nl` lines of length L (power of two, 8..4096) at pitch L in
+// shared memory; each pass reads every element once, does one radix-R
+// butterfly per (line, j) in registers and writes the Stockham-ordered
+// result to the other buffer.  Input and output are in natural order.
+// tw[k] = exp(-2 pi i k / L) for k < L; `sign` > 0 selects the inverse.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double2 cmul(double2 a, double2 b)
 {
@@ -272,61 +274,121 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b)
 }
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ unsigned brev_n(unsigned j, int logL) { return logL ? (__brev(j) >> (32 - logL)) : 0u; }
 
-// Lines sit at pitch L + 1 in shared memory so that threads walking
-// consecutive lines hit different banks.
-__device__ void smem_dit(double2* s, int nl, int L, int logL, const double2* __restrict__ tw, bool inv)
+// In-register DFT of size R (2, 4, 8) in natural order: X[k] = sum_r v[r] w^(rk),
+// w = exp(-/+ 2 pi i / R).
+template <int R>
+__device__ __forceinline__ void dft_reg(double2* v, bool inv);
+
+template <>
+__device__ __forceinline__ void dft_reg<2>(double2* v, bool)
 {
-    const int P = L + 1;
-    const int halfL = L >> 1;
-    const int nb = nl * halfL;
-    for (int st = 0; st < logL; ++st) {
-        const int half = 1 << st;
-        const int tstride = halfL >> st; // L / (2*half)
-        for (int t = threadIdx.x; t < nb; t += blockDim.x) {
-            int line = t / halfL, bf = t - line * halfL;
-            int pos = bf & (half - 1), grp = bf >> st;
-            int i0 = line * P + grp * 2 * half + pos, i1 = i0 + half;
-            double2 w = tw[pos * tstride];
-            if (inv) w.y = -w.y;
-            double2 a = s[i0], b = cmul(s[i1], w);
-            s[i0] = cadd(a, b);
-            s[i1] = csub(a, b);
-        }
-        __syncthreads();
+    double2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+}
+
+// multiply by -i (forward) or +i (inverse)
+__device__ __forceinline__ double2 rot90(double2 a, bool inv)
+{
+    return inv ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+template <>
+__device__ __forceinline__ void dft_reg<4>(double2* v, bool inv)
+{
+    double2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+    double2 s13 = cadd(v[1], v[3]), d13 = rot90(csub(v[1], v[3]), inv);
+    v[0] = cadd(s02, s13);
+    v[2] = csub(s02, s13);
+    v[1] = cadd(d02, d13);
+    v[3] = csub(d02, d13);
+}
+
+template <>
+__device__ __forceinline__ void dft_reg<8>(double2* v, bool inv)
+{
+    const double h = 0.70710678118654752440;
+    // radix-2 first stage (decimation in frequency)
+    double2 a[4], b[4];
+    for (int r = 0; r < 4; ++r) {
+        a[r] = cadd(v[r], v[r + 4]);
+        b[r] = csub(v[r], v[r + 4]);
+    }
+    // twiddles w8^r on the difference branch
+    b[1] = inv ? make_double2(h * (b[1].x - b[1].y), h * (b[1].x + b[1].y))
+               : make_double2(h * (b[1].x + b[1].y), h * (b[1].y - b[1].x));
+    b[2] = rot90(b[2], inv);
+    b[3] = inv ? make_double2(-h * (b[3].x + b[3].y), h * (b[3].x - b[3].y))
+               : make_double2(h * (b[3].y - b[3].x), -h * (b[3].x + b[3].y));
+    dft_reg<4>(a, inv); // even outputs
+    dft_reg<4>(b, inv); // odd outputs
+    for (int k = 0; k < 4; ++k) {
+        v[2 * k] = a[k];
+        v[2 * k + 1] = b[k];
     }
 }
 
-__device__ void smem_dif(double2* s, int nl, int L, int logL, const double2* __restrict__ tw, bool inv)
+template <int R>
+__device__ __forceinline__ void stockham_pass(const double2* __restrict__ src, double2* __restrict__ dst, int nl,
+                                              int L, int Ns, const double2* __restrict__ tw, bool inv)
 {
-    const int P = L + 1;
-    const int halfL = L >> 1;
-    const int nb = nl * halfL;
-    for (int st = logL - 1; st >= 0; --st) {
-        const int half = 1 << st;
-        const int tstride = halfL >> st;
-        for (int t = threadIdx.x; t < nb; t += blockDim.x) {
-            int line = t / halfL, bf = t - line * halfL;
-            int pos = bf & (half - 1), grp = bf >> st;
-            int i0 = line * P + grp * 2 * half + pos, i1 = i0 + half;
-            double2 w = tw[pos * tstride];
-            if (inv) w.y = -w.y;
-            double2 a = s[i0], b = s[i1];
-            s[i0] = cadd(a, b);
-            s[i1] = cmul(csub(a, b), w);
+    // element j of line li sits at j * nl + li: consecutive threads take
+    // consecutive lines, so every read and write below is contiguous
+    const int T = L / R;
+    const int total = nl * T;
+    const int tstep = L / (Ns * R);
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        const int j = t / nl, li = t - j * nl;
+        const int k = j & (Ns - 1);
+        double2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = src[(j + r * T) * nl + li];
+        if (Ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                double2 w = tw[(k * r * tstep) & (L - 1)];
+                if (inv) w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
         }
-        __syncthreads();
+        dft_reg<R>(v, inv);
+        const int idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst[(idxD + r * Ns) * nl + li] = v[r];
     }
 }
 
-constexpr int kFftTile = 4096; // complex elements per CTA tile (64 KB + line padding)
-// nl = kFftTile / L lines at pitch L + 1 take kFftTile + nl elements; the
-// smallest transform length is 8 (grid shape >= 3 doubled to a power of 2).
-constexpr int kFftMinLen = 8;
-constexpr int kFftSmemBytes = (kFftTile + kFftTile / kFftMinLen) * 16;
+// FFT of the nl lines in b0 (layout j * nl + li); returns the buffer
+// holding the result.
+__device__ double2* smem_fft(double2* b0, double2* b1, int nl, int L, const double2* __restrict__ tw, bool inv)
+{
+    double2* src = b0;
+    double2* dst = b1;
+    int Ns = 1;
+    while (Ns < L) {
+        const int rem = L / Ns;
+        if (rem >= 8 && rem != 16) {
+            stockham_pass<8>(src, dst, nl, L, Ns, tw, inv);
+            Ns *= 8;
+        } else if (rem >= 4) {
+            stockham_pass<4>(src, dst, nl, L, Ns, tw, inv);
+            Ns *= 4;
+        } else {
+            stockham_pass<2>(src, dst, nl, L, Ns, tw, inv);
+            Ns *= 2;
+        }
+        __syncthreads();
+        double2* t = src;
+        src = dst;
+        dst = t;
+    }
+    return src;
+}
+
+constexpr int kFftTile = 2048; // complex elements per line tile (32 KB; two tiles per CTA)
+constexpr int kFftSmemBytes = 2 * kFftTile * 16;
 constexpr int kFftThreads = 256;
-
 
 // XF: pairs of real rows (y, y+1) of rho -> S rows (r2c, first gx inputs)
 __global__ void __launch_bounds__(kFftThreads) fft_xf_kernel(const double* __restrict__ rho, double2* S,
@@ -341,6 +403,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_xf_kernel(const double* __res
     const int64_t l0 = (int64_t)blockIdx.x * nl;
     const int nlt = (int)min((int64_t)nl, nlines - l0);
     if (nlt <= 0) return;
+    double2* b0 = sm;
+    double2* b1 = sm + kFftTile;
     for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
         int li = idx / L, j = idx - li * L;
         int64_t l = l0 + li;
@@ -351,17 +415,17 @@ __global__ void __launch_bounds__(kFftThreads) fft_xf_kernel(const double* __res
             v.x = rho[((int64_t)z * d.gy + ya) * d.gx + j];
             if (yb < d.gy) v.y = rho[((int64_t)z * d.gy + yb) * d.gx + j];
         }
-        sm[li * (L + 1) + brev_n(j, d.lx)] = v;
+        b0[(j) * nlt + li] = v;
     }
     __syncthreads();
-    smem_dit(sm, nlt, L, d.lx, tw, false);
+    double2* r = smem_fft(b0, b1, nlt, L, tw, false);
     const int nk = d.nkx;
     for (int idx = threadIdx.x; idx < nlt * nk; idx += blockDim.x) {
         int li = idx / nk, k = idx - li * nk;
         int64_t l = l0 + li;
         int pr = (int)(l % npy), z = (int)(l / npy);
         int ya = 2 * pr, yb = ya + 1;
-        double2 Z = sm[li * (L + 1) + k], Zn = sm[li * (L + 1) + ((L - k) & (L - 1))];
+        double2 Z = r[(k) * nlt + li], Zn = r[(((L - k) & (L - 1))) * nlt + li];
         double2 A = make_double2((Z.x + Zn.x) * 0.5, (Z.y - Zn.y) * 0.5);
         double2 B = make_double2((Z.y + Zn.y) * 0.5, -(Z.x - Zn.x) * 0.5);
         S[((int64_t)z * d.ny + ya) * d.nkxp + k] = A;
@@ -381,6 +445,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_y_kernel(double2* S, const do
     const int64_t l0 = (int64_t)blockIdx.x * nl;
     const int nlt = (int)min((int64_t)nl, nlines - l0);
     if (nlt <= 0) return;
+    double2* b0 = sm;
+    double2* b1 = sm + kFftTile;
     const int nin = inverse ? L : d.gy;
     for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
         int j = idx / nlt, li = idx - j * nlt; // consecutive threads: consecutive kx
@@ -388,20 +454,16 @@ __global__ void __launch_bounds__(kFftThreads) fft_y_kernel(double2* S, const do
         int kx = (int)(l % d.nkx), z = (int)(l / d.nkx);
         double2 v = make_double2(0.0, 0.0);
         if (j < nin) v = S[((int64_t)z * d.ny + j) * d.nkxp + kx];
-        sm[li * (L + 1) + (inverse ? j : (int)brev_n(j, d.ly))] = v;
+        b0[(j) * nlt + li] = v;
     }
     __syncthreads();
-    if (!inverse)
-        smem_dit(sm, nlt, L, d.ly, tw, false);
-    else
-        smem_dif(sm, nlt, L, d.ly, tw, true);
+    double2* r = smem_fft(b0, b1, nlt, L, tw, inverse != 0);
     const int nout = inverse ? d.gy : L;
     for (int idx = threadIdx.x; idx < nlt * nout; idx += blockDim.x) {
         int j = idx / nlt, li = idx - j * nlt;
         int64_t l = l0 + li;
         int kx = (int)(l % d.nkx), z = (int)(l / d.nkx);
-        double2 v = sm[li * (L + 1) + (inverse ? (int)brev_n(j, d.ly) : j)];
-        S[((int64_t)z * d.ny + j) * d.nkxp + kx] = v;
+        S[((int64_t)z * d.ny + j) * d.nkxp + kx] = r[(j) * nlt + li];
     }
 }
 
@@ -419,34 +481,37 @@ __global__ void __launch_bounds__(kFftThreads) fft_z_conv_kernel(double2* S, con
     const int64_t l0 = (int64_t)blockIdx.x * nl;
     const int nlt = (int)min((int64_t)nl, nlines - l0);
     if (nlt <= 0) return;
+    double2* b0 = sm;
+    double2* b1 = sm + kFftTile;
     for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
         int j = idx / nlt, li = idx - j * nlt;
         int64_t l = l0 + li;
         int kx = (int)(l % d.nkx), ky = (int)(l / d.nkx);
         double2 v = make_double2(0.0, 0.0);
         if (j < d.gz) v = S[((int64_t)j * d.ny + ky) * d.nkxp + kx];
-        sm[li * (L + 1) + brev_n(j, d.lz)] = v;
+        b0[(j) * nlt + li] = v;
     }
     __syncthreads();
-    smem_dit(sm, nlt, L, d.lz, tw, false);
+    double2* r = smem_fft(b0, b1, nlt, L, tw, false);
+    double2* o = (r == b0) ? b1 : b0;
     const int ogx = d.nx / 2 + 1, ogy = d.ny / 2 + 1;
     for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
-        int li = idx / L, kz = idx - li * L;
+        int kz = idx / nlt, li = idx - kz * nlt;
         int64_t l = l0 + li;
         int kx = (int)(l % d.nkx), ky = (int)(l / d.nkx);
         int my = ky <= d.ny / 2 ? ky : d.ny - ky;
         int mz = kz <= d.nz / 2 ? kz : d.nz - kz;
         double g = Ghat[((int64_t)mz * ogy + my) * ogx + kx];
-        double2 v = sm[li * (L + 1) + kz];
-        sm[li * (L + 1) + kz] = make_double2(v.x * g, v.y * g);
+        double2 v = r[(kz) * nlt + li];
+        r[(kz) * nlt + li] = make_double2(v.x * g, v.y * g);
     }
     __syncthreads();
-    smem_dif(sm, nlt, L, d.lz, tw, true);
+    double2* q = smem_fft(r, o, nlt, L, tw, true);
     for (int idx = threadIdx.x; idx < nlt * d.gz; idx += blockDim.x) {
         int j = idx / nlt, li = idx - j * nlt;
         int64_t l = l0 + li;
         int kx = (int)(l % d.nkx), ky = (int)(l / d.nkx);
-        S[((int64_t)j * d.ny + ky) * d.nkxp + kx] = sm[li * (L + 1) + brev_n(j, d.lz)];
+        S[((int64_t)j * d.ny + ky) * d.nkxp + kx] = q[(j) * nlt + li];
     }
 }
 
@@ -465,6 +530,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_xi_kernel(const double2* __re
     const int64_t l0 = (int64_t)blockIdx.x * nl;
     const int nlt = (int)min((int64_t)nl, nlines - l0);
     if (nlt <= 0) return;
+    double2* b0 = sm;
+    double2* b1 = sm + kFftTile;
     const int half = L / 2;
     for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
         int li = idx / L, j = idx - li * L;
@@ -482,16 +549,16 @@ __global__ void __launch_bounds__(kFftThreads) fft_xi_kernel(const double2* __re
             A.y = -A.y;
             B.y = -B.y;
         }
-        sm[li * (L + 1) + j] = make_double2(A.x - B.y, A.y + B.x);
+        b0[(j) * nlt + li] = make_double2(A.x - B.y, A.y + B.x);
     }
     __syncthreads();
-    smem_dif(sm, nlt, L, d.lx, tw, true);
+    double2* r = smem_fft(b0, b1, nlt, L, tw, true);
     for (int idx = threadIdx.x; idx < nlt * d.gx; idx += blockDim.x) {
         int li = idx / d.gx, j = idx - li * d.gx;
         int64_t l = l0 + li;
         int pr = (int)(l % npy), z = (int)(l / npy);
         int ya = 2 * pr, yb = ya + 1;
-        double2 v = sm[li * (L + 1) + brev_n(j, d.lx)];
+        double2 v = r[(j) * nlt + li];
         phi[((int64_t)z * d.gy + ya) * d.gx + j] = v.x;
         if (yb < d.gy) phi[((int64_t)z * d.gy + yb) * d.gx + j] = v.y;
     }
@@ -501,43 +568,41 @@ __global__ void __launch_bounds__(kFftThreads) fft_xi_kernel(const double2* __re
 // axis 0/1/2 transforms even real lines rebuilt by mirroring; real part of
 // the first L/2+1 outputs stored back in place.
 __global__ void __launch_bounds__(kFftThreads) fft_green_kernel(double* G, const double2* __restrict__ tw,
-                                                                int axis, int L, int logL, int ox, int oy, int oz,
+                                                                int axis, int L, int ox, int oy, int oz,
                                                                 const ScState* __restrict__ scp)
 {
     extern __shared__ double2 sm[];
     if (!scp->valid) return;
     const int nl = kFftTile / L;
     const int half = L / 2;
-    int64_t nlines, sa, sj;
-    int na;
-    if (axis == 0) { nlines = (int64_t)oy * oz; na = 1; sa = ox; sj = 1; }
-    else if (axis == 1) { nlines = (int64_t)ox * oz; na = ox; sa = 1; sj = ox; }
-    else { nlines = (int64_t)ox * oy; na = ox * oy; sa = 1; sj = (int64_t)ox * oy; }
+    int64_t nlines, sj;
+    if (axis == 0) { nlines = (int64_t)oy * oz; sj = 1; }
+    else if (axis == 1) { nlines = (int64_t)ox * oz; sj = ox; }
+    else { nlines = (int64_t)ox * oy; sj = (int64_t)ox * oy; }
     const int64_t l0 = (int64_t)blockIdx.x * nl;
     const int nlt = (int)min((int64_t)nl, nlines - l0);
     if (nlt <= 0) return;
+    double2* b0 = sm;
+    double2* b1 = sm + kFftTile;
     auto line_base = [&](int64_t l) -> int64_t {
         if (axis == 0) return l * ox;                                  // (y, z) rows
         if (axis == 1) return (l % ox) + (l / ox) * (int64_t)ox * oy;  // (kx, z)
         return l;                                                      // (kx, ky)
     };
-    (void)na;
-    (void)sa;
     for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
         int li, j;
         if (axis == 0) { li = idx / L; j = idx - li * L; }
         else { j = idx / nlt; li = idx - j * nlt; }
         int m = j <= half ? j : L - j;
-        double v = G[line_base(l0 + li) + m * sj];
-        sm[li * (L + 1) + brev_n(j, logL)] = make_double2(v, 0.0);
+        b0[(j) * nlt + li] = make_double2(G[line_base(l0 + li) + m * sj], 0.0);
     }
     __syncthreads();
-    smem_dit(sm, nlt, L, logL, tw, false);
+    double2* r = smem_fft(b0, b1, nlt, L, tw, false);
     for (int idx = threadIdx.x; idx < nlt * (half + 1); idx += blockDim.x) {
         int li, k;
         if (axis == 0) { li = idx / (half + 1); k = idx - li * (half + 1); }
         else { k = idx / nlt; li = idx - k * nlt; }
-        G[line_base(l0 + li) + k * sj] = sm[li * (L + 1) + k].x;
+        G[line_base(l0 + li) + k * sj] = r[(k) * nlt + li].x;
     }
 }
 
@@ -621,9 +686,9 @@ cudaError_t launch_green(const ScState* sc, double* G, const Dims& d, int linear
     const int ox = d.nx / 2 + 1, oy = d.ny / 2 + 1, oz = d.nz / 2 + 1;
     green_octant_kernel<<<sm_count() * 4, 256, 0, s>>>(sc, G, d.gx, d.gy, d.gz, linear);
     const size_t sh = kFftSmemBytes;
-    fft_green_kernel<<<ceil_div64((int64_t)oy * oz, kFftTile / d.nx), kFftThreads, sh, s>>>(G, tw_x, 0, d.nx, d.lx, ox, oy, oz, sc);
-    fft_green_kernel<<<ceil_div64((int64_t)ox * oz, kFftTile / d.ny), kFftThreads, sh, s>>>(G, tw_y, 1, d.ny, d.ly, ox, oy, oz, sc);
-    fft_green_kernel<<<ceil_div64((int64_t)ox * oy, kFftTile / d.nz), kFftThreads, sh, s>>>(G, tw_z, 2, d.nz, d.lz, ox, oy, oz, sc);
+    fft_green_kernel<<<ceil_div64((int64_t)oy * oz, kFftTile / d.nx), kFftThreads, sh, s>>>(G, tw_x, 0, d.nx, ox, oy, oz, sc);
+    fft_green_kernel<<<ceil_div64((int64_t)ox * oz, kFftTile / d.ny), kFftThreads, sh, s>>>(G, tw_y, 1, d.ny, ox, oy, oz, sc);
+    fft_green_kernel<<<ceil_div64((int64_t)ox * oy, kFftTile / d.nz), kFftThreads, sh, s>>>(G, tw_z, 2, d.nz, ox, oy, oz, sc);
     return cudaGetLastError();
 }
 

@@ -11,6 +11,7 @@
 // (libFF/ff_algorithm.h) operation for operation.
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <cstdlib>
 
 #include "sb2_kernels.h"
 
@@ -77,8 +78,8 @@ __device__ __forceinline__ double qpow_d(double x, int i)
     return r;
 }
 
-__device__ void thin_magnet_unit(double x, double& xp, double y, double& yp, double kl0, double kl1,
-                                 int n)
+__device__ __noinline__ void thin_magnet_unit(double x, double& xp, double y, double& yp, double kl0, double kl1,
+                                              int n)
 { // ff_algorithm.h:1122-1168
     for (int k = 0; k < n; k += 4)
         xp = xp - (kl0 * (n - k)) * qpow_d(x, n - k - 1) * qpow_d(y, k) / (factorial_d(n - k) * factorial_d(k));
@@ -99,7 +100,7 @@ __device__ void thin_magnet_unit(double x, double& xp, double y, double& yp, dou
 }
 
 // cf_kick ff_quadrupole.h:22-35
-__device__ __forceinline__ void quad_cf_kick(double x, double& xp, double y, double& yp, const double* kL)
+__device__ __noinline__ void quad_cf_kick(double x, double& xp, double y, double& yp, const double* kL)
 {
     thin_quadrupole_unit(x, xp, y, yp, kL[0], kL[1]);
     if (kL[2] || kL[3]) thin_quadrupole_unit(x, xp, y, yp, kL[2], kL[3]);
@@ -174,6 +175,23 @@ __device__ __forceinline__ void bend_unit(double& x, double& xp, double& y, doub
     cdt = cdt + ncdt - cdt_ref;
 }
 
+// PropSbendSimd ff_sbend.h:127-215 for one particle (out of line: rare op)
+__device__ __noinline__ void sbend_op(double& x, double& xp, double& y, double& yp, double& cdt, double& dpop,
+                                      const double* d, int flags)
+{
+    if (flags & 1) {
+        slot_unit(x, xp, y, yp, cdt, dpop, d[0], d[1], d[14], d[15]);
+        yp = yp - d[4] * y; // edge_unit ff_algorithm.h:139-148
+        xp = xp + d[5] * y;
+    }
+    bend_unit(x, xp, y, yp, cdt, dpop, d[8], d[13], d[14], d[15], d[16], d[9], d[10], d[11], d[12]);
+    if (flags & 2) {
+        yp = yp - d[6] * y;
+        xp = xp + d[7] * y;
+        slot_unit(x, xp, y, yp, cdt, dpop, d[2], d[3], d[14], d[15]);
+    }
+}
+
 // yoshida6 ff_algorithm.h:1834-2008 with the drift lengths c_i*step_length,
 // the 0.1*step_ref_cdt substep and the d_i-scaled strengths precomputed on
 // the host (identical doubles).  kind selects the kick function.
@@ -222,15 +240,28 @@ __device__ __forceinline__ void leftmost(double pos, double left, double inv, in
 
 constexpr int kTrackThreads = 256;
 
-__global__ void __launch_bounds__(kTrackThreads) track_kernel(const __grid_constant__ TrackParams p)
-{
-    __shared__ int s_counts[kMaxOpsPerPass];
-    __shared__ double s_red[kTrackThreads / 32][6];
-    for (int i = threadIdx.x; i < kMaxOpsPerPass; i += blockDim.x) s_counts[i] = 0;
-    __syncthreads();
+// Two compiled variants: FULL runs every op kind; LIGHT omits the Yoshida
+// integrators and the sector bend so that passes made only of drifts, thin
+// kicks, apertures, the space-charge kick and the moment sums fit in fewer
+// registers and run at higher occupancy.
+enum TrackVariant { TRACK_LIGHT = 0, TRACK_FULL = 1, TRACK_FULL_WIDE = 2 };
 
-    double ms[6] = {0, 0, 0, 0, 0, 0};
-    bool want_moments = false;
+// Minimum resident CTAs per SM for each variant (register budget).
+template <int V>
+struct TrackOcc {
+    static constexpr int value = V == TRACK_LIGHT ? 3 : (V == TRACK_FULL ? 3 : 2);
+};
+
+template <int VARIANT>
+__global__ void __launch_bounds__(kTrackThreads, TrackOcc<VARIANT>::value)
+    track_kernel(const __grid_constant__ TrackParams p)
+{
+    constexpr bool kFull = VARIANT != TRACK_LIGHT;
+    __shared__ int s_counts[kMaxOpsPerPass];
+    __shared__ double s_mom[6][kTrackThreads]; // per-thread moment sums
+    for (int i = threadIdx.x; i < kMaxOpsPerPass; i += blockDim.x) s_counts[i] = 0;
+    for (int j = 0; j < 6; ++j) s_mom[j][threadIdx.x] = 0.0;
+    __syncthreads();
 
     const int64_t n = p.n;
     const int64_t S = p.stride;
@@ -284,10 +315,14 @@ __global__ void __launch_bounds__(kTrackThreads) track_kernel(const __grid_const
                 continue;
             }
             if (kind == OP_MOMENTS) {
-                want_moments = true;
                 if (alive) {
-                    ms[0] += x; ms[1] += y; ms[2] += cdt;
-                    ms[3] += x * x; ms[4] += y * y; ms[5] += cdt * cdt;
+                    double* m = &s_mom[0][threadIdx.x];
+                    m[0 * kTrackThreads] += x;
+                    m[1 * kTrackThreads] += y;
+                    m[2 * kTrackThreads] += cdt;
+                    m[3 * kTrackThreads] += x * x;
+                    m[4 * kTrackThreads] += y * y;
+                    m[5 * kTrackThreads] += cdt * cdt;
                 }
                 continue;
             }
@@ -297,21 +332,25 @@ __global__ void __launch_bounds__(kTrackThreads) track_kernel(const __grid_const
                 drift_unit(x, xp, y, yp, cdt, dpop, op.d[0], op.d[1], op.d[2], op.d[3]);
                 break;
             case OP_QUAD: {
-                double xx = x - op.d[0], yy = y - op.d[1];
-                yoshida6_op<OP_QUAD>(xx, xp, yy, yp, cdt, dpop, op);
-                x = xx + op.d[0];
-                y = yy + op.d[1];
+                if constexpr (kFull) {
+                    double xx = x - op.d[0], yy = y - op.d[1];
+                    yoshida6_op<OP_QUAD>(xx, xp, yy, yp, cdt, dpop, op);
+                    x = xx + op.d[0];
+                    y = yy + op.d[1];
+                }
                 break;
             }
             case OP_QUAD_CF: {
-                double xx = x - op.d[0], yy = y - op.d[1];
-                yoshida6_op<OP_QUAD_CF>(xx, xp, yy, yp, cdt, dpop, op);
-                x = xx + op.d[0];
-                y = yy + op.d[1];
+                if constexpr (kFull) {
+                    double xx = x - op.d[0], yy = y - op.d[1];
+                    yoshida6_op<OP_QUAD_CF>(xx, xp, yy, yp, cdt, dpop, op);
+                    x = xx + op.d[0];
+                    y = yy + op.d[1];
+                }
                 break;
             }
             case OP_SEXT_YOSHIDA:
-                yoshida6_op<OP_SEXT_YOSHIDA>(x, xp, y, yp, cdt, dpop, op);
+                if constexpr (kFull) yoshida6_op<OP_SEXT_YOSHIDA>(x, xp, y, yp, cdt, dpop, op);
                 break;
             case OP_THIN_QUAD: {
                 double xx = x - op.d[0], yy = y - op.d[1];
@@ -333,18 +372,7 @@ __global__ void __launch_bounds__(kTrackThreads) track_kernel(const __grid_const
                 break;
             }
             case OP_SBEND: {
-                const double* d = op.d;
-                if (op.flags & 1) {
-                    slot_unit(x, xp, y, yp, cdt, dpop, d[0], d[1], d[14], d[15]);
-                    yp = yp - d[4] * y; // edge_unit ff_algorithm.h:139-148
-                    xp = xp + d[5] * y;
-                }
-                bend_unit(x, xp, y, yp, cdt, dpop, d[8], d[13], d[14], d[15], d[16], d[9], d[10], d[11], d[12]);
-                if (op.flags & 2) {
-                    yp = yp - d[6] * y;
-                    xp = xp + d[7] * y;
-                    slot_unit(x, xp, y, yp, cdt, dpop, d[2], d[3], d[14], d[15]);
-                }
+                if constexpr (kFull) sbend_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
                 break;
             }
             case OP_SC_KICK: {
@@ -428,20 +456,13 @@ __global__ void __launch_bounds__(kTrackThreads) track_kernel(const __grid_const
     // moments: fixed-order block reduction -> one partial per block
     bool any_mom = false;
     for (int o = 0; o < p.nops; ++o) any_mom |= (p.ops[o].kind == OP_MOMENTS);
-    (void)want_moments;
     if (any_mom && p.moment_partials) {
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        for (int j = 0; j < 6; ++j) {
-            double v = ms[j];
-            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-            if (lane == 0) s_red[w][j] = v;
+        for (int w = kTrackThreads / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w)
+                for (int j = 0; j < 6; ++j) s_mom[j][threadIdx.x] += s_mom[j][threadIdx.x + w];
+            __syncthreads();
         }
-        __syncthreads();
-        if (threadIdx.x < 6) {
-            double v = 0;
-            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) v += s_red[k][threadIdx.x];
-            p.moment_partials[blockIdx.x * 6 + threadIdx.x] = v;
-        }
+        if (threadIdx.x < 6) p.moment_partials[blockIdx.x * 6 + threadIdx.x] = s_mom[threadIdx.x][0];
     }
 }
 
@@ -536,10 +557,37 @@ int track_grid_blocks()
     return nb;
 }
 
+bool track_needs_full(const MapOp* ops, int n)
+{
+    for (int i = 0; i < n; ++i) {
+        int k = ops[i].kind;
+        if (k == OP_QUAD || k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_SBEND) return true;
+    }
+    return false;
+}
+
+// Register budget of the full variant: 2 CTAs/SM (128 registers; measured
+// faster for the Yoshida passes) unless SB2_TRACK_FULL_OCC=3 selects
+// 3 CTAs/SM (80 registers).
+static int full_variant()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("SB2_TRACK_FULL_OCC");
+        v = (e && atoi(e) == 3) ? TRACK_FULL : TRACK_FULL_WIDE;
+    }
+    return v;
+}
+
 cudaError_t launch_track(const TrackParams& p, cudaStream_t s)
 {
     int nb = track_grid_blocks();
-    track_kernel<<<nb, kTrackThreads, 0, s>>>(p);
+    if (!track_needs_full(p.ops, p.nops))
+        track_kernel<TRACK_LIGHT><<<nb, kTrackThreads, 0, s>>>(p);
+    else if (full_variant() == TRACK_FULL_WIDE)
+        track_kernel<TRACK_FULL_WIDE><<<nb, kTrackThreads, 0, s>>>(p);
+    else
+        track_kernel<TRACK_FULL><<<nb, kTrackThreads, 0, s>>>(p);
     return cudaGetLastError();
 }
 
