@@ -203,6 +203,22 @@ sb2_status sb2_sc3d_apply(sb2_sc3d* sc, sb2_bunch* b, double time_step, void* st
 sb2_status sb2_sc3d_last(sb2_sc3d* sc, double left[3], double h[3], double* rho, double* phi,
                          double* ex, double* ey, double* ez, double scalars[8]);
 
+/* Space-charge kick that allocates nothing (no counterpart in the
+ * reference): the same kick as sb2_sc3d_apply on caller-owned device arrays
+ * (parts N x 7 column-major with column stride `stride`, masks N bytes;
+ * parts updated in place), for callers that manage all device memory
+ * themselves and cannot have the library call cudaMalloc/cudaFree.  All
+ * workspaces live in one fixed 12 MiB device array that every GPU loading
+ * the library holds until exit, so grids are limited to 65,536 cells with
+ * doubled dimensions <= 128 (larger grids return SB2_ERR_INVALID).  The
+ * first call on a device looks up that array's address and should come
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race.  Returns after the stream is synchronised. */
+sb2_status sb2_sc3d_apply_noalloc(const sb2_sc3d_options* opts, double* parts, int64_t stride,
+                                  const uint8_t* masks, int64_t n, int32_t n_total, double real_num,
+                                  int32_t charge, double mass, double value, int32_t kind, double time_step,
+                                  void* stream);
+
 /* ---------------------------------------------------------------------
  * Independent operations on explicit slices of a lattice.
  * ------------------------------------------------------------------- */

@@ -1522,6 +1522,37 @@ struct ScOperator {
     }
 };
 
+// Helpers for the other translation units: option checks and reference
+// kinematics without exceptions crossing the boundary.
+int check_sc_options(const sb2_sc3d_options& o, std::string* msg)
+{
+    try {
+        SpaceCharge::validate(o);
+    } catch (const Error& e) {
+        if (msg) *msg = e.what();
+        return e.code;
+    }
+    return SB2_OK;
+}
+
+int ref_kinematics(int charge, double mass, double value, int kind, double* gamma, double* beta, double* p,
+                   std::string* msg)
+{
+    try {
+        Refpart r;
+        r.set(charge, mass, value, kind);
+        *gamma = r.gamma;
+        *beta = r.beta;
+        *p = r.p;
+    } catch (const Error& e) {
+        if (msg) *msg = e.what();
+        return e.code;
+    }
+    return SB2_OK;
+}
+
+void set_last_error(const std::string& m);
+
 } // namespace sb2
 
 // ===========================================================================
@@ -1543,6 +1574,7 @@ struct sb2_sc3d {
 };
 
 static thread_local std::string g_last_error;
+void sb2::set_last_error(const std::string& m) { g_last_error = m; }
 
 #define SB2_TRY try {
 #define SB2_CATCH                                                                                                  \

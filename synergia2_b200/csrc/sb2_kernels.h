@@ -3,6 +3,9 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <string>
+
+#include "../../include/sb2.h"
 
 #include "sb2_ops.h"
 
@@ -70,5 +73,10 @@ cudaError_t launch_convolve(const double* rho, double2* S, const double* Ghat, d
                             const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
                             cudaStream_t s);
 cudaError_t launch_efield(const double* phi, double2* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s);
+// host.cc
+int check_sc_options(const sb2_sc3d_options& o, std::string* msg);
+int ref_kinematics(int charge, double mass, double value, int kind, double* gamma, double* beta, double* p,
+                   std::string* msg);
+void set_last_error(const std::string& m);
 
 } // namespace sb2
