@@ -208,7 +208,7 @@ def main():
     # timed region: device time with CUDA events on the launching stream
     clocks = Clocks(local)
     L.sb2_profile_enable(1)
-    for c in range(6):
+    for c in range(7):
         L.sb2_profile_read(c, None, None, None, 1)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -221,7 +221,7 @@ def main():
     L.sb2_profile_enable(0)
     ms = e0.elapsed_time(e1)
     prof = {}
-    for c in range(6):
+    for c in range(7):
         nm, tot, cnt = ctypes.c_char_p(), ctypes.c_double(), ctypes.c_int64()
         syn.check(L.sb2_profile_read(c, ctypes.byref(nm), ctypes.byref(tot), ctypes.byref(cnt), 1))
         prof[nm.value.decode()] = (tot.value, cnt.value)
@@ -279,7 +279,8 @@ def main():
                 traffic = None
         gpu_launches = int(prof.get("track", (0, 0))[1] + prof.get("domain", (0, 0))[1] +
                            prof.get("deposit", (0, 0))[1] + 4 * prof.get("green", (0, 0))[1] +
-                           5 * prof.get("solve", (0, 0))[1] + prof.get("efield", (0, 0))[1])
+                           5 * prof.get("solve", (0, 0))[1] + prof.get("efield", (0, 0))[1] +
+                           5 * prof.get("sort", (0, 0))[1])
         out = {
             "metric": "macroparticle-steps/s", "value": value, "unit": "macroparticle-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,

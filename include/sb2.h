@@ -55,7 +55,8 @@ const char* sb2_version(void);
  * scoped_simple_timer regions, utils/simple_timer.h:50-66).  Categories:
  * 0 track (fused particle passes), 1 domain (bookkeeping + domain),
  * 2 deposit, 3 green (Green-function transform), 4 solve (FFT
- * convolution), 5 efield.  Off by default. */
+ * convolution), 5 efield, 6 sort (cell-ordered working copy).  Off by
+ * default. */
 sb2_status sb2_profile_enable(int32_t on);
 sb2_status sb2_profile_read(int32_t category, const char** name, double* total_ms, int64_t* launches,
                             int32_t reset);

@@ -20,7 +20,7 @@ OUT = os.path.join(HERE, "libsb2.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["track.cu", "sc3d.cu", "noalloc.cu"]
+CU_SOURCES = ["track.cu", "sc3d.cu", "sort.cu", "noalloc.cu"]
 CXX_SOURCES = ["host.cc"]
 
 

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <array>
 #include <cmath>
 #include <complex>
@@ -1020,8 +1021,8 @@ static MapOp op_aperture(const Lattice& lat, const std::string& type, const Slic
 // reference's scoped_simple_timer labels, utils/simple_timer.h:50-66).
 // Off unless sb2_profile_enable(1) is called.
 // ---------------------------------------------------------------------------
-enum ProfCat { PROF_TRACK = 0, PROF_DOMAIN, PROF_DEPOSIT, PROF_GREEN, PROF_SOLVE, PROF_EFIELD, PROF_NCAT };
-static const char* kProfNames[PROF_NCAT] = {"track", "domain", "deposit", "green", "solve", "efield"};
+enum ProfCat { PROF_TRACK = 0, PROF_DOMAIN, PROF_DEPOSIT, PROF_GREEN, PROF_SOLVE, PROF_EFIELD, PROF_SORT, PROF_NCAT };
+static const char* kProfNames[PROF_NCAT] = {"track", "domain", "deposit", "green", "solve", "efield", "sort"};
 
 struct Profiler {
     bool on = false;
@@ -1426,6 +1427,12 @@ struct Propagator {
     std::unique_ptr<SpaceCharge> sc;
     std::unique_ptr<Engine> engine_;
     double* elem_charge = nullptr;
+    // cell-ordered working copy of the bunch (space-charge runs only)
+    bool cell_sort = true;
+    int sort_interval = 4; // re-sort before every k-th space-charge kick (measured best of 1, 2, 4, 8 at 4M particles)
+    int kicks_since_sort = 0;
+    SortBuffers sb{};
+    int64_t sb_cap = -1;
 
     Propagator(const Lattice& l, int stepper_kind, int n, const sb2_sc3d_options* opts)
         : lat(l), stepper(stepper_kind), num(n)
@@ -1437,8 +1444,112 @@ struct Propagator {
             has_sc = true;
         }
         steps = make_steps(lat, stepper, num, has_sc);
+        const char* e = getenv("SB2_CELL_SORT");
+        if (e && atoi(e) == 0) cell_sort = false;
+        const char* k = getenv("SB2_SORT_INTERVAL");
+        if (k && atoi(k) > 0) sort_interval = atoi(k);
     }
-    ~Propagator() { cudaFree(elem_charge); }
+    ~Propagator()
+    {
+        cudaFree(elem_charge);
+        free_sort();
+    }
+
+    void free_sort()
+    {
+        cudaFree(sb.parts);
+        cudaFree(sb.masks);
+        cudaFree(sb.discards);
+        cudaFree(sb.perm);
+        cudaFree(sb.parts2);
+        cudaFree(sb.masks2);
+        cudaFree(sb.discards2);
+        cudaFree(sb.perm2);
+        cudaFree(sb.scratch);
+        sb = SortBuffers{};
+        sb_cap = -1;
+    }
+
+    bool sorting(const Bunch& b) const { return has_sc && cell_sort && b.n >= 64; }
+
+    // Points the bunch at a cell-ordered working copy for the duration of
+    // a propagate call and restores (scatters back) at the end.
+    struct SortScope {
+        Propagator& P;
+        Bunch& b;
+        cudaStream_t s;
+        bool active = false;
+        double* u_parts;
+        int64_t u_stride;
+        uint8_t *u_masks, *u_discards;
+        SortScope(Propagator& p, Bunch& bb, cudaStream_t st) : P(p), b(bb), s(st)
+        {
+            u_parts = b.parts;
+            u_stride = b.stride;
+            u_masks = b.masks;
+            u_discards = b.discards;
+            if (!P.sorting(b)) return;
+            P.alloc_sort(b.n);
+            ProfScope ps(PROF_SORT, s);
+            cuda_check(launch_sort_gather_in(b.parts, b.stride, b.masks, b.discards, P.sb, s), "sort gather");
+            b.parts = P.sb.parts;
+            b.stride = P.sb.stride;
+            b.masks = P.sb.masks;
+            b.discards = P.sb.discards;
+            active = true;
+        }
+        void restore()
+        {
+            if (!active) return;
+            active = false;
+            b.parts = u_parts;
+            b.stride = u_stride;
+            b.masks = u_masks;
+            b.discards = u_discards;
+            ProfScope ps(PROF_SORT, s);
+            cuda_check(launch_sort_scatter_out(P.sb, u_parts, u_stride, u_masks, u_discards, s), "sort scatter");
+        }
+        ~SortScope()
+        {
+            try {
+                restore();
+            } catch (...) {
+            }
+        }
+    };
+
+    void alloc_sort(int64_t n)
+    {
+        const int64_t G = (int64_t)sc_opts.shape[0] * sc_opts.shape[1] * sc_opts.shape[2];
+        if (sb_cap == n && sb.scratch) return;
+        free_sort();
+        sb.n = n;
+        sb.stride = n;
+        sb.parts = dalloc<double>((size_t)7 * n, "sort copy");
+        sb.parts2 = dalloc<double>((size_t)7 * n, "sort copy");
+        sb.masks = dalloc<uint8_t>(n, "sort copy");
+        sb.masks2 = dalloc<uint8_t>(n, "sort copy");
+        sb.discards = dalloc<uint8_t>(n, "sort copy");
+        sb.discards2 = dalloc<uint8_t>(n, "sort copy");
+        sb.perm = dalloc<int32_t>(n, "sort copy");
+        sb.perm2 = dalloc<int32_t>(n, "sort copy");
+        sb.scratch = dalloc<int32_t>(sort_scratch_ints(G), "sort scratch");
+        sb_cap = n;
+    }
+
+    // Re-sort the working copy by the cells of the current domain.
+    void resort(Bunch& b, cudaStream_t s)
+    {
+        ProfScope ps(PROF_SORT, s);
+        cuda_check(launch_cell_sort(sb, sc->state, sc->d.gx, sc->d.gy, sc->d.gz, s), "cell sort");
+        std::swap(sb.parts, sb.parts2);
+        std::swap(sb.masks, sb.masks2);
+        std::swap(sb.discards, sb.discards2);
+        std::swap(sb.perm, sb.perm2);
+        b.parts = sb.parts;
+        b.masks = sb.masks;
+        b.discards = sb.discards;
+    }
 
     void ensure_device()
     {
@@ -1468,6 +1579,7 @@ struct Propagator {
                 engine_->add_operator(lat, st.indeps[ii++], b, sc.get(), elem_charge, s);
             } else if (sc) {
                 engine_->flush(b, sc.get(), elem_charge, true, time * 1.0, s);
+                if (sort_active && (kicks_since_sort++ % sort_interval) == 0) resort(b, s);
                 sc->solve(b, s);
                 engine_->add_kick();
             }
@@ -1481,20 +1593,31 @@ struct Propagator {
         if (sc) sc->check_error();
     }
 
+    bool sort_active = false;
+
     void propagate(Bunch& b, int turns, cudaStream_t s)
     { // Propagator::propagate propagator.cc:157-283 (one bunch, no diagnostics)
         begin(b);
+        SortScope scope(*this, b, s);
+        sort_active = scope.active;
+        kicks_since_sort = 0;
         for (int t = 0; t < turns; ++t) {
             b.ref.start_repetition(); // do_start_repetition propagator.cc:25-34
             for (auto const& st : steps) run_step(b, st, s);
             b.turns_done += 1;
         }
+        engine_->flush(b, sc.get(), elem_charge, false, 0.0, s);
+        scope.restore();
+        sort_active = false;
         finish(b, s);
     }
 
     void propagate_steps(Bunch& b, int first, int count, cudaStream_t s)
     {
         begin(b);
+        SortScope scope(*this, b, s);
+        sort_active = scope.active;
+        kicks_since_sort = 0;
         const int ns = (int)steps.size();
         for (int k = first; k < first + count; ++k) {
             int si = ((k % ns) + ns) % ns;
@@ -1502,6 +1625,9 @@ struct Propagator {
             run_step(b, steps[si], s);
             if (si == ns - 1) b.turns_done += 1;
         }
+        engine_->flush(b, sc.get(), elem_charge, false, 0.0, s);
+        scope.restore();
+        sort_active = false;
         finish(b, s);
     }
 };

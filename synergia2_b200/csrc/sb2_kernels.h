@@ -56,6 +56,20 @@ struct Dims {
     int lx, ly, lz;    // log2 of nx, ny, nz
 };
 
+// Working copy of a bunch ordered by deposit cell (sort.cu), double-buffered.
+struct SortBuffers {
+    double* parts;
+    uint8_t* masks;
+    uint8_t* discards;
+    int32_t* perm;   // original index of each working-copy particle
+    double* parts2;
+    uint8_t* masks2;
+    uint8_t* discards2;
+    int32_t* perm2;
+    int64_t n, stride;
+    int32_t* scratch; // sort_scratch_ints(G) ints
+};
+
 // track.cu
 int track_grid_blocks();
 cudaError_t launch_track(const TrackParams& p, cudaStream_t s);
@@ -73,6 +87,13 @@ cudaError_t launch_convolve(const double* rho, double2* S, const double* Ghat, d
                             const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
                             cudaStream_t s);
 cudaError_t launch_efield(const double* phi, double2* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s);
+// sort.cu
+size_t sort_scratch_ints(int64_t G);
+cudaError_t launch_cell_sort(const SortBuffers& sb, const ScState* sc, int gx, int gy, int gz, cudaStream_t s);
+cudaError_t launch_sort_gather_in(const double* ups, int64_t ustride, const uint8_t* um, const uint8_t* ud,
+                                  const SortBuffers& sb, cudaStream_t s);
+cudaError_t launch_sort_scatter_out(const SortBuffers& sb, double* ups, int64_t ustride, uint8_t* um, uint8_t* ud,
+                                    cudaStream_t s);
 // host.cc
 int check_sc_options(const sb2_sc3d_options& o, std::string* msg);
 int ref_kinematics(int charge, double mass, double value, int kind, double* gamma, double* beta, double* p,

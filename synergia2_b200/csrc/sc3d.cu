@@ -152,6 +152,10 @@ __device__ __forceinline__ void leftmost_d(double pos, double left, double inv, 
     off = s - idx;
 }
 
+// Particles whose stencils start in the same cell are summed inside the
+// warp first (a segmented shuffle scan over runs of equal cell keys), so a
+// cell-ordered bunch issues one set of 8 atomics per run instead of per
+// particle; with no equal neighbours the scan is skipped.
 __global__ void __launch_bounds__(256) deposit_kernel(const double* __restrict__ parts, int64_t stride,
                                                       const uint8_t* __restrict__ masks, int64_t n,
                                                       const ScState* __restrict__ scp, double* rho,
@@ -162,31 +166,67 @@ __global__ void __launch_bounds__(256) deposit_kernel(const double* __restrict__
     const double lx = sc.left[0], ly = sc.left[1], lz = sc.left[2];
     const double ihx = sc.ih[0], ihy = sc.ih[1], ihz = sc.ih[2];
     const double w0 = sc.w0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        if (!masks[i]) continue;
-        int ix, iy, iz;
-        double ox, oy, oz;
-        leftmost_d(parts[i], lx, ihx, ix, ox);
-        leftmost_d(parts[i + 2 * stride], ly, ihy, iy, oy);
-        leftmost_d(parts[i + 4 * stride], lz, ihz, iz, oz);
-        double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
+    const int lane = threadIdx.x & 31;
+    const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t wb = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane; wb < n; wb += wstride) {
+        const int64_t i = wb + lane;
+        int ix = 0, iy = 0, iz = 0;
+        int64_t key = -1;
+        double w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (i < n && masks[i]) {
+            double ox, oy, oz;
+            leftmost_d(parts[i], lx, ihx, ix, ox);
+            leftmost_d(parts[i + 2 * stride], ly, ihy, iy, oy);
+            leftmost_d(parts[i + 4 * stride], lz, ihz, iz, oz);
+            if (ix >= -1 && ix < gx && iy >= -1 && iy < gy && iz >= -1 && iz < gz) {
+                key = ((int64_t)(iz + 1) * (gy + 1) + (iy + 1)) * (gx + 1) + (ix + 1);
+                double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
+                w[0] = w0 * aox * aoy * aoz;
+                w[1] = w0 * ox * aoy * aoz;
+                w[2] = w0 * aox * oy * aoz;
+                w[3] = w0 * ox * oy * aoz;
+                w[4] = w0 * aox * aoy * oz;
+                w[5] = w0 * ox * aoy * oz;
+                w[6] = w0 * aox * oy * oz;
+                w[7] = w0 * ox * oy * oz;
+            }
+        }
+        const int64_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+        const int64_t next = __shfl_down_sync(0xffffffffu, key, 1);
+        const bool head = lane == 0 || prev != key;
+        const bool tail = lane == 31 || next != key;
+        const unsigned heads = __ballot_sync(0xffffffffu, head);
+        if (heads != 0xffffffffu) { // some run longer than one particle
+            unsigned le;
+            asm("mov.u32 %0, %%lanemask_le;" : "=r"(le));
+            const int seg = 31 - __clz(heads & le);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                double v = w[c];
+                for (int o = 1; o < 32; o <<= 1) {
+                    double u = __shfl_up_sync(0xffffffffu, v, o);
+                    if (lane - o >= seg) v += u;
+                }
+                w[c] = v;
+            }
+        }
+        if (!tail || key < 0) continue;
         bool x0 = ix > 0 && ix < gx - 1, x1 = ix + 1 > 0 && ix + 1 < gx - 1;
         bool y0 = iy > 0 && iy < gy - 1, y1 = iy + 1 > 0 && iy + 1 < gy - 1;
         bool z0 = iz > 0 && iz < gz - 1, z1 = iz + 1 > 0 && iz + 1 < gz - 1;
         int64_t base = (int64_t)iz * gx * gy;
         if (z0) {
-            if (y0 && x0) atomicAdd(&rho[base + iy * gx + ix], w0 * aox * aoy * aoz);
-            if (y0 && x1) atomicAdd(&rho[base + iy * gx + ix + 1], w0 * ox * aoy * aoz);
-            if (y1 && x0) atomicAdd(&rho[base + (iy + 1) * gx + ix], w0 * aox * oy * aoz);
-            if (y1 && x1) atomicAdd(&rho[base + (iy + 1) * gx + ix + 1], w0 * ox * oy * aoz);
+            if (y0 && x0) atomicAdd(&rho[base + iy * gx + ix], w[0]);
+            if (y0 && x1) atomicAdd(&rho[base + iy * gx + ix + 1], w[1]);
+            if (y1 && x0) atomicAdd(&rho[base + (iy + 1) * gx + ix], w[2]);
+            if (y1 && x1) atomicAdd(&rho[base + (iy + 1) * gx + ix + 1], w[3]);
         }
         base = (int64_t)(iz + 1) * gx * gy;
         if (z1) {
-            if (y0 && x0) atomicAdd(&rho[base + iy * gx + ix], w0 * aox * aoy * oz);
-            if (y0 && x1) atomicAdd(&rho[base + iy * gx + ix + 1], w0 * ox * aoy * oz);
-            if (y1 && x0) atomicAdd(&rho[base + (iy + 1) * gx + ix], w0 * aox * oy * oz);
-            if (y1 && x1) atomicAdd(&rho[base + (iy + 1) * gx + ix + 1], w0 * ox * oy * oz);
+            if (y0 && x0) atomicAdd(&rho[base + iy * gx + ix], w[4]);
+            if (y0 && x1) atomicAdd(&rho[base + iy * gx + ix + 1], w[5]);
+            if (y1 && x0) atomicAdd(&rho[base + (iy + 1) * gx + ix], w[6]);
+            if (y1 && x1) atomicAdd(&rho[base + (iy + 1) * gx + ix + 1], w[7]);
         }
     }
 }

@@ -1,0 +1,266 @@
+// Cell-ordered working copy of a bunch for the space-charge step.
+//
+// Unsorted particles make the CIC deposit one FP64 atomic per particle and
+// corner (L2 atomic bound) and make the kick's field gathers touch a
+// different cache line per thread (L1 wavefront bound).  During a propagate
+// call the particles therefore live in a working copy ordered by the cell of
+// their deposit stencil, rebuilt before each deposit by a counting sort:
+//   key       cell (iz*gy + iy)*gx + ix of the stencil's lower corner;
+//             G for live particles outside the grid, G+1 for lost ones
+//   histogram warp-aggregated atomics on key counts
+//   scan      exclusive prefix sum of the counts (three small kernels)
+//   scatter   every column, the mask, the discard flag and the original
+//             index move to offset[key] + rank
+// The caller's arrays are untouched until the call ends, when the working
+// copy is scattered back to the original order.  The order within a cell
+// depends on atomic arrival order; every per-particle result is independent
+// of it.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "sb2_kernels.h"
+
+namespace sb2 {
+
+__device__ __forceinline__ int cell_key(double x, double y, double z, const ScState& sc, int gx, int gy, int gz)
+{ // collective/utils.h:9-18
+    double sx = (x - sc.left[0]) * sc.ih[0] - 0.5;
+    double sy = (y - sc.left[1]) * sc.ih[1] - 0.5;
+    double sz = (z - sc.left[2]) * sc.ih[2] - 0.5;
+    int ix = (int)floor(sx), iy = (int)floor(sy), iz = (int)floor(sz);
+    const int G = gx * gy * gz;
+    if (ix < 0 || ix >= gx || iy < 0 || iy >= gy || iz < 0 || iz >= gz) return G;
+    return (iz * gy + iy) * gx + ix;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__global__ void __launch_bounds__(256) sort_hist_kernel(const double* __restrict__ parts, int64_t stride,
+                                                        const uint8_t* __restrict__ masks, int64_t n,
+                                                        const ScState* __restrict__ scp, int gx, int gy, int gz,
+                                                        int32_t* counts)
+{
+    const ScState& sc = *scp;
+    const int G = gx * gy * gz;
+    const int lane = threadIdx.x & 31;
+    const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t wb = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane; wb < n; wb += wstride) {
+        const int64_t i = wb + lane;
+        int key = -1;
+        if (i < n) {
+            if (!masks[i] || !sc.valid)
+                key = G + 1;
+            else
+                key = cell_key(parts[i], parts[i + 2 * stride], parts[i + 4 * stride], sc, gx, gy, gz);
+        }
+        const unsigned grp = __match_any_sync(0xffffffffu, key);
+        if (key >= 0 && lane == __ffs(grp) - 1) atomicAdd(&counts[key], __popc(grp));
+    }
+}
+
+// exclusive scan: per-block (1024 values), then block sums, then add
+constexpr int kScanBlock = 1024;
+
+__global__ void __launch_bounds__(256) scan_block_kernel(const int32_t* __restrict__ in, int32_t* out, int n,
+                                                         int32_t* block_sums)
+{
+    __shared__ int32_t s[kScanBlock];
+    __shared__ int32_t warp_tot[8];
+    const int base = blockIdx.x * kScanBlock;
+    for (int k = threadIdx.x; k < kScanBlock; k += blockDim.x) s[k] = (base + k < n) ? in[base + k] : 0;
+    __syncthreads();
+    // each thread owns 4 consecutive values
+    const int t = threadIdx.x;
+    int32_t v0 = s[4 * t], v1 = s[4 * t + 1], v2 = s[4 * t + 2], v3 = s[4 * t + 3];
+    int32_t tot = v0 + v1 + v2 + v3;
+    const int lane = t & 31, w = t >> 5;
+    int32_t inc = tot;
+    for (int o = 1; o < 32; o <<= 1) {
+        int32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    if (lane == 31) warp_tot[w] = inc;
+    __syncthreads();
+    int32_t woff = 0;
+    for (int k = 0; k < w; ++k) woff += warp_tot[k];
+    int32_t ex = woff + inc - tot;
+    s[4 * t] = ex;
+    s[4 * t + 1] = ex + v0;
+    s[4 * t + 2] = ex + v0 + v1;
+    s[4 * t + 3] = ex + v0 + v1 + v2;
+    __syncthreads();
+    for (int k = threadIdx.x; k < kScanBlock; k += blockDim.x)
+        if (base + k < n) out[base + k] = s[k];
+    if (threadIdx.x == blockDim.x - 1) {
+        int32_t all = 0;
+        for (int k = 0; k < 8; ++k) all += warp_tot[k];
+        block_sums[blockIdx.x] = all;
+    }
+}
+
+__global__ void __launch_bounds__(1024) scan_sums_kernel(int32_t* sums, int nb)
+{
+    // single block: sequential per-thread chunks, then a block scan of the
+    // chunk totals
+    __shared__ int32_t tot[1024];
+    const int per = (nb + 1023) / 1024;
+    const int b = threadIdx.x * per;
+    int32_t acc = 0;
+    for (int k = 0; k < per && b + k < nb; ++k) acc += sums[b + k];
+    tot[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        int32_t u = (threadIdx.x >= (unsigned)o) ? tot[threadIdx.x - o] : 0;
+        __syncthreads();
+        tot[threadIdx.x] += u;
+        __syncthreads();
+    }
+    int32_t run = tot[threadIdx.x] - acc; // exclusive
+    for (int k = 0; k < per && b + k < nb; ++k) {
+        int32_t v = sums[b + k];
+        sums[b + k] = run;
+        run += v;
+    }
+}
+
+__global__ void scan_add_kernel(int32_t* out, int n, const int32_t* __restrict__ sums)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += sums[i / kScanBlock];
+}
+
+__global__ void __launch_bounds__(256) sort_scatter_kernel(const double* __restrict__ src, const uint8_t* __restrict__ m_src,
+                                                           const uint8_t* __restrict__ d_src,
+                                                           const int32_t* __restrict__ p_src, double* dst,
+                                                           uint8_t* m_dst, uint8_t* d_dst, int32_t* p_dst, int64_t n,
+                                                           int64_t stride, const ScState* __restrict__ scp, int gx,
+                                                           int gy, int gz, const int32_t* __restrict__ offsets,
+                                                           int32_t* cursor)
+{
+    const ScState& sc = *scp;
+    const int G = gx * gy * gz;
+    const int lane = threadIdx.x & 31;
+    const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t wb = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane; wb < n; wb += wstride) {
+        const int64_t i = wb + lane;
+        int key = -1;
+        double v[7];
+        uint8_t mk = 0;
+        if (i < n) {
+            for (int j = 0; j < 7; ++j) v[j] = src[i + j * stride];
+            mk = m_src[i];
+            key = (!mk || !sc.valid) ? G + 1 : cell_key(v[0], v[2], v[4], sc, gx, gy, gz);
+        }
+        const unsigned grp = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(grp) - 1;
+        int32_t b = 0;
+        if (key >= 0 && lane == leader) b = atomicAdd(&cursor[key], __popc(grp));
+        b = __shfl_sync(0xffffffffu, b, leader);
+        if (key < 0) continue;
+        const int64_t pos = (int64_t)offsets[key] + b + __popc(grp & lanemask_lt());
+        for (int j = 0; j < 7; ++j) dst[pos + j * stride] = v[j];
+        m_dst[pos] = mk;
+        d_dst[pos] = d_src[i];
+        p_dst[pos] = p_src[i];
+    }
+}
+
+// working copy <- caller arrays (identity order)
+__global__ void sort_gather_in_kernel(const double* __restrict__ ups, int64_t ustride, const uint8_t* __restrict__ um,
+                                      const uint8_t* __restrict__ ud, double* w, uint8_t* wm, uint8_t* wd, int32_t* wp,
+                                      int64_t n, int64_t wstride)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        for (int j = 0; j < 7; ++j) w[i + j * wstride] = ups[i + j * ustride];
+        wm[i] = um[i];
+        wd[i] = ud ? ud[i] : 0;
+        wp[i] = (int32_t)i;
+    }
+}
+
+// caller arrays <- working copy, back in the original order: invert the
+// permutation (4-byte scattered writes), then gather so that the wide
+// writes to the caller's columns are coalesced
+__global__ void sort_invert_kernel(const int32_t* __restrict__ wp, int32_t* inv, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        inv[wp[i]] = (int32_t)i;
+}
+
+__global__ void sort_scatter_out_kernel(const double* __restrict__ w, const uint8_t* __restrict__ wm,
+                                        const uint8_t* __restrict__ wd, const int32_t* __restrict__ inv, double* ups,
+                                        int64_t ustride, uint8_t* um, uint8_t* ud, int64_t n, int64_t wstride)
+{
+    for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < n; o += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = inv[o];
+        for (int j = 0; j < 7; ++j) ups[o + j * ustride] = w[i + j * wstride];
+        um[o] = wm[i];
+        if (ud) ud[o] = wd[i];
+    }
+}
+
+static int sm_count_s()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+size_t sort_scratch_ints(int64_t G)
+{ // counts, offsets (=cursor base), cursor, block sums
+    const int64_t m = G + 2;
+    return (size_t)(3 * m + (m + kScanBlock - 1) / kScanBlock + 8);
+}
+
+cudaError_t launch_cell_sort(const SortBuffers& sb, const ScState* sc, int gx, int gy, int gz, cudaStream_t s)
+{
+    const int64_t G = (int64_t)gx * gy * gz;
+    const int m = (int)(G + 2);
+    int32_t* counts = sb.scratch;
+    int32_t* offsets = counts + m;
+    int32_t* cursor = offsets + m;
+    int32_t* bsums = cursor + m;
+    const int nb = (m + kScanBlock - 1) / kScanBlock;
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(counts, 0, sizeof(int32_t) * m, s))) return e;
+    if ((e = cudaMemsetAsync(cursor, 0, sizeof(int32_t) * m, s))) return e;
+    const int grid = sm_count_s() * 8;
+    sort_hist_kernel<<<grid, 256, 0, s>>>(sb.parts, sb.stride, sb.masks, sb.n, sc, gx, gy, gz, counts);
+    scan_block_kernel<<<nb, 256, 0, s>>>(counts, offsets, m, bsums);
+    scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nb);
+    scan_add_kernel<<<(m + 255) / 256, 256, 0, s>>>(offsets, m, bsums);
+    sort_scatter_kernel<<<grid, 256, 0, s>>>(sb.parts, sb.masks, sb.discards, sb.perm, sb.parts2, sb.masks2,
+                                             sb.discards2, sb.perm2, sb.n, sb.stride, sc, gx, gy, gz, offsets, cursor);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort_gather_in(const double* ups, int64_t ustride, const uint8_t* um, const uint8_t* ud,
+                                  const SortBuffers& sb, cudaStream_t s)
+{
+    sort_gather_in_kernel<<<sm_count_s() * 8, 256, 0, s>>>(ups, ustride, um, ud, sb.parts, sb.masks, sb.discards,
+                                                             sb.perm, sb.n, sb.stride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort_scatter_out(const SortBuffers& sb, double* ups, int64_t ustride, uint8_t* um, uint8_t* ud,
+                                    cudaStream_t s)
+{
+    // perm2 is free outside a sort: it holds the inverse permutation here
+    sort_invert_kernel<<<sm_count_s() * 8, 256, 0, s>>>(sb.perm, sb.perm2, sb.n);
+    sort_scatter_out_kernel<<<sm_count_s() * 8, 256, 0, s>>>(sb.parts, sb.masks, sb.discards, sb.perm2, ups, ustride,
+                                                               um, ud, sb.n, sb.stride);
+    return cudaGetLastError();
+}
+
+} // namespace sb2

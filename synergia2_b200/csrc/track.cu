@@ -252,200 +252,236 @@ struct TrackOcc {
     static constexpr int value = V == TRACK_LIGHT ? 3 : (V == TRACK_FULL ? 3 : 2);
 };
 
+// One particle in registers during a pass.
+struct Part {
+    double x, xp, y, yp, cdt, dpop;
+    bool alive;
+    int disc;
+};
+
+// Applies one op to one particle (apertures, moments and maps).
 template <int VARIANT>
+__device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, Part& P, int* s_counts,
+                                         double* s_mom_col)
+{
+    constexpr bool kFull = VARIANT != TRACK_LIGHT;
+    const int kind = op.kind;
+    double& x = P.x;
+    double& xp = P.xp;
+    double& y = P.y;
+    double& yp = P.yp;
+    double& cdt = P.cdt;
+    double& dpop = P.dpop;
+    if (kind >= OP_AP_FINITE && kind <= OP_AP_RECTANGULAR) {
+        // discard_applier bunch_particles.h:484-503: discards(i) is reset by
+        // every aperture, then set if this one discards.
+        P.disc = 0;
+        if (P.alive) {
+            bool d;
+            if (kind == OP_AP_FINITE) {
+                if (!isfinite(x) || !isfinite(xp) || !isfinite(y) || !isfinite(yp) || !isfinite(cdt) ||
+                    !isfinite(dpop))
+                    d = true;
+                else {
+                    double pt = 1.0 + dpop;
+                    d = pt * pt - xp * xp - yp * yp < 0.0;
+                }
+            } else if (kind == OP_AP_CIRCULAR) {
+                double xr = x - op.d[1], yr = y - op.d[2];
+                d = (xr * xr + yr * yr) > op.d[0];
+            } else if (kind == OP_AP_ELLIPTICAL) {
+                double xr = x - op.d[2], yr = y - op.d[3];
+                d = (xr * xr / op.d[0] + yr * yr / op.d[1]) > 1.0;
+            } else {
+                double xr = x - op.d[2], yr = y - op.d[3];
+                d = (fabs(xr) > 0.5 * op.d[0]) || (fabs(yr) > 0.5 * op.d[1]);
+            }
+            if (d) {
+                P.disc = 1;
+                P.alive = false;
+                atomicAdd(&s_counts[op.slot - p.slot_base], 1);
+            }
+        }
+        return;
+    }
+    if (kind == OP_MOMENTS) {
+        if (P.alive) {
+            s_mom_col[0 * kTrackThreads] += x;
+            s_mom_col[1 * kTrackThreads] += y;
+            s_mom_col[2 * kTrackThreads] += cdt;
+            s_mom_col[3 * kTrackThreads] += x * x;
+            s_mom_col[4 * kTrackThreads] += y * y;
+            s_mom_col[5 * kTrackThreads] += cdt * cdt;
+        }
+        return;
+    }
+    if (!P.alive) return;
+        switch (kind) {
+        case OP_DRIFT:
+            drift_unit(x, xp, y, yp, cdt, dpop, op.d[0], op.d[1], op.d[2], op.d[3]);
+            break;
+        case OP_QUAD: {
+            if constexpr (kFull) {
+                double xx = x - op.d[0], yy = y - op.d[1];
+                yoshida6_op<OP_QUAD>(xx, xp, yy, yp, cdt, dpop, op);
+                x = xx + op.d[0];
+                y = yy + op.d[1];
+            }
+            break;
+        }
+        case OP_QUAD_CF: {
+            if constexpr (kFull) {
+                double xx = x - op.d[0], yy = y - op.d[1];
+                yoshida6_op<OP_QUAD_CF>(xx, xp, yy, yp, cdt, dpop, op);
+                x = xx + op.d[0];
+                y = yy + op.d[1];
+            }
+            break;
+        }
+        case OP_SEXT_YOSHIDA:
+            if constexpr (kFull) yoshida6_op<OP_SEXT_YOSHIDA>(x, xp, y, yp, cdt, dpop, op);
+            break;
+        case OP_THIN_QUAD: {
+            double xx = x - op.d[0], yy = y - op.d[1];
+            thin_quadrupole_unit(xx, xp, yy, yp, op.d[2], op.d[3]);
+            break;
+        }
+        case OP_THIN_SEXT:
+            thin_sextupole_unit(x, xp, y, yp, op.d[2], op.d[3]);
+            break;
+        case OP_MPOLE: {
+            const double* kl = op.d;
+            const int on = op.flags;
+            if (on & 1) { xp = xp - kl[0]; yp = yp + kl[1]; }
+            if (on & 2) thin_quadrupole_unit(x, xp, y, yp, kl[2], kl[3]);
+            if (on & 4) thin_sextupole_unit(x, xp, y, yp, kl[4], kl[5]);
+            if (on & 8) thin_octupole_unit(x, xp, y, yp, kl[6], kl[7]);
+            for (int nn = 4; nn < 8; ++nn)
+                if (on & (1 << nn)) thin_magnet_unit(x, xp, y, yp, kl[nn * 2], kl[nn * 2 + 1], nn + 1);
+            break;
+        }
+        case OP_SBEND: {
+            if constexpr (kFull) sbend_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
+            break;
+        }
+        case OP_SC_KICK: {
+            // zyx::alg_kicker space_charge_3d_kernels.h:91-215
+            const ScState& sc = *p.sc;
+            if (!sc.valid) break;
+            int ix, iy, iz;
+            double ox, oy, oz;
+            leftmost(x, sc.left[0], sc.ih[0], ix, ox);
+            leftmost(y, sc.left[1], sc.ih[1], iy, oy);
+            leftmost(cdt, sc.left[2], sc.ih[2], iz, oz);
+            const int gx = p.gx, gy = p.gy, gz = p.gz;
+            if (!((ix >= 0 && ix < gx - 1) && (iy >= 0 && iy < gy - 1) && (iz >= 0 && iz < gz - 1)))
+                break;
+            double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
+            const int64_t b0 = ((int64_t)iz * gy + iy) * gx + ix;
+            const int64_t b1 = ((int64_t)(iz + 1) * gy + iy) * gx + ix;
+            const double2* E = p.efield;
+            // corner fields: .x/.y of [2c] = ex, ey; .x of [2c+1] = ez
+            double2 a00 = E[2 * b0], a01 = E[2 * (b0 + 1)], a10 = E[2 * (b0 + gx)], a11 = E[2 * (b0 + gx + 1)];
+            double2 c00 = E[2 * b1], c01 = E[2 * (b1 + 1)], c10 = E[2 * (b1 + gx)], c11 = E[2 * (b1 + gx + 1)];
+            double z00 = E[2 * b0 + 1].x, z01 = E[2 * (b0 + 1) + 1].x, z10 = E[2 * (b0 + gx) + 1].x,
+                   z11 = E[2 * (b0 + gx + 1) + 1].x;
+            double w00 = E[2 * b1 + 1].x, w01 = E[2 * (b1 + 1) + 1].x, w10 = E[2 * (b1 + gx) + 1].x,
+                   w11 = E[2 * (b1 + gx + 1) + 1].x;
+            const double factor = sc.factor, pref = p.kick_pref, m = p.kick_m;
+            double val = aoz * aoy * aox * z00;
+            val += aoz * aoy * ox * z01;
+            val += aoz * oy * aox * z10;
+            val += aoz * oy * ox * z11;
+            val += oz * aoy * aox * w00;
+            val += oz * aoy * ox * w01;
+            val += oz * oy * aox * w10;
+            val += oz * oy * ox * w11;
+            double pp = pref + dpop * pref;
+            double Eoc_i = sqrt(pp * pp + m * m);
+            double Eoc_f = Eoc_i + factor * (-pref) * val;
+            double ddp = (sqrt(Eoc_f * Eoc_f - m * m) - sqrt(Eoc_i * Eoc_i - m * m)) / pref;
+            dpop += ddp;
+            val = aoz * aoy * aox * a00.y;
+            val += aoz * aoy * ox * a01.y;
+            val += aoz * oy * aox * a10.y;
+            val += aoz * oy * ox * a11.y;
+            val += oz * aoy * aox * c00.y;
+            val += oz * aoy * ox * c01.y;
+            val += oz * oy * aox * c10.y;
+            val += oz * oy * ox * c11.y;
+            yp += factor * val;
+            val = aoz * aoy * aox * a00.x;
+            val += aoz * aoy * ox * a01.x;
+            val += aoz * oy * aox * a10.x;
+            val += aoz * oy * ox * a11.x;
+            val += oz * aoy * aox * c00.x;
+            val += oz * aoy * ox * c01.x;
+            val += oz * oy * aox * c10.x;
+            val += oz * oy * ox * c11.x;
+            xp += factor * val;
+            break;
+        }
+        default:
+            break;
+        }
+}
+
+// PPT particles per thread travel through the op list together, so their
+// independent load and arithmetic chains overlap (more bytes in flight per
+// thread for the memory-bound passes).
+template <int VARIANT, int PPT>
 __global__ void __launch_bounds__(kTrackThreads, TrackOcc<VARIANT>::value)
     track_kernel(const __grid_constant__ TrackParams p)
 {
-    constexpr bool kFull = VARIANT != TRACK_LIGHT;
     __shared__ int s_counts[kMaxOpsPerPass];
     __shared__ double s_mom[6][kTrackThreads]; // per-thread moment sums
     for (int i = threadIdx.x; i < kMaxOpsPerPass; i += blockDim.x) s_counts[i] = 0;
     for (int j = 0; j < 6; ++j) s_mom[j][threadIdx.x] = 0.0;
     __syncthreads();
+    double* s_mom_col = &s_mom[0][threadIdx.x];
 
     const int64_t n = p.n;
     const int64_t S = p.stride;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        bool alive = p.masks[i] != 0;
-        bool alive_in = alive;
-        int disc = 0;
-        double x = 0, xp = 0, y = 0, yp = 0, cdt = 0, dpop = 0;
-        if (alive) {
-            x = p.parts[i];
-            xp = p.parts[i + S];
-            y = p.parts[i + 2 * S];
-            yp = p.parts[i + 3 * S];
-            cdt = p.parts[i + 4 * S];
-            dpop = p.parts[i + 5 * S];
+    const int64_t tile = (int64_t)blockDim.x * PPT;
+    for (int64_t base = blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
+        Part P[PPT];
+        bool in[PPT];
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+            const int64_t i = base + q * blockDim.x + threadIdx.x;
+            P[q].alive = (i < n) && p.masks[i] != 0;
+            in[q] = P[q].alive;
+            P[q].disc = 0;
+            P[q].x = P[q].xp = P[q].y = P[q].yp = P[q].cdt = P[q].dpop = 0.0;
+            if (P[q].alive) {
+                P[q].x = p.parts[i];
+                P[q].xp = p.parts[i + S];
+                P[q].y = p.parts[i + 2 * S];
+                P[q].yp = p.parts[i + 3 * S];
+                P[q].cdt = p.parts[i + 4 * S];
+                P[q].dpop = p.parts[i + 5 * S];
+            }
         }
         for (int o = 0; o < p.nops; ++o) {
             const MapOp& op = p.ops[o];
-            const int kind = op.kind;
-            if (kind >= OP_AP_FINITE && kind <= OP_AP_RECTANGULAR) {
-                // discard_applier bunch_particles.h:484-503: discards(i) is
-                // reset by every aperture, then set if this one discards.
-                disc = 0;
-                if (alive) {
-                    bool d;
-                    if (kind == OP_AP_FINITE) {
-                        if (!isfinite(x) || !isfinite(xp) || !isfinite(y) || !isfinite(yp) ||
-                            !isfinite(cdt) || !isfinite(dpop))
-                            d = true;
-                        else {
-                            double pt = 1.0 + dpop;
-                            d = pt * pt - xp * xp - yp * yp < 0.0;
-                        }
-                    } else if (kind == OP_AP_CIRCULAR) {
-                        double xr = x - op.d[1], yr = y - op.d[2];
-                        d = (xr * xr + yr * yr) > op.d[0];
-                    } else if (kind == OP_AP_ELLIPTICAL) {
-                        double xr = x - op.d[2], yr = y - op.d[3];
-                        d = (xr * xr / op.d[0] + yr * yr / op.d[1]) > 1.0;
-                    } else {
-                        double xr = x - op.d[2], yr = y - op.d[3];
-                        d = (fabs(xr) > 0.5 * op.d[0]) || (fabs(yr) > 0.5 * op.d[1]);
-                    }
-                    if (d) {
-                        disc = 1;
-                        alive = false;
-                        atomicAdd(&s_counts[op.slot - p.slot_base], 1);
-                    }
-                }
-                continue;
-            }
-            if (kind == OP_MOMENTS) {
-                if (alive) {
-                    double* m = &s_mom[0][threadIdx.x];
-                    m[0 * kTrackThreads] += x;
-                    m[1 * kTrackThreads] += y;
-                    m[2 * kTrackThreads] += cdt;
-                    m[3 * kTrackThreads] += x * x;
-                    m[4 * kTrackThreads] += y * y;
-                    m[5 * kTrackThreads] += cdt * cdt;
-                }
-                continue;
-            }
-            if (!alive) continue;
-            switch (kind) {
-            case OP_DRIFT:
-                drift_unit(x, xp, y, yp, cdt, dpop, op.d[0], op.d[1], op.d[2], op.d[3]);
-                break;
-            case OP_QUAD: {
-                if constexpr (kFull) {
-                    double xx = x - op.d[0], yy = y - op.d[1];
-                    yoshida6_op<OP_QUAD>(xx, xp, yy, yp, cdt, dpop, op);
-                    x = xx + op.d[0];
-                    y = yy + op.d[1];
-                }
-                break;
-            }
-            case OP_QUAD_CF: {
-                if constexpr (kFull) {
-                    double xx = x - op.d[0], yy = y - op.d[1];
-                    yoshida6_op<OP_QUAD_CF>(xx, xp, yy, yp, cdt, dpop, op);
-                    x = xx + op.d[0];
-                    y = yy + op.d[1];
-                }
-                break;
-            }
-            case OP_SEXT_YOSHIDA:
-                if constexpr (kFull) yoshida6_op<OP_SEXT_YOSHIDA>(x, xp, y, yp, cdt, dpop, op);
-                break;
-            case OP_THIN_QUAD: {
-                double xx = x - op.d[0], yy = y - op.d[1];
-                thin_quadrupole_unit(xx, xp, yy, yp, op.d[2], op.d[3]);
-                break;
-            }
-            case OP_THIN_SEXT:
-                thin_sextupole_unit(x, xp, y, yp, op.d[2], op.d[3]);
-                break;
-            case OP_MPOLE: {
-                const double* kl = op.d;
-                const int on = op.flags;
-                if (on & 1) { xp = xp - kl[0]; yp = yp + kl[1]; }
-                if (on & 2) thin_quadrupole_unit(x, xp, y, yp, kl[2], kl[3]);
-                if (on & 4) thin_sextupole_unit(x, xp, y, yp, kl[4], kl[5]);
-                if (on & 8) thin_octupole_unit(x, xp, y, yp, kl[6], kl[7]);
-                for (int nn = 4; nn < 8; ++nn)
-                    if (on & (1 << nn)) thin_magnet_unit(x, xp, y, yp, kl[nn * 2], kl[nn * 2 + 1], nn + 1);
-                break;
-            }
-            case OP_SBEND: {
-                if constexpr (kFull) sbend_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
-                break;
-            }
-            case OP_SC_KICK: {
-                // zyx::alg_kicker space_charge_3d_kernels.h:91-215
-                const ScState& sc = *p.sc;
-                if (!sc.valid) break;
-                int ix, iy, iz;
-                double ox, oy, oz;
-                leftmost(x, sc.left[0], sc.ih[0], ix, ox);
-                leftmost(y, sc.left[1], sc.ih[1], iy, oy);
-                leftmost(cdt, sc.left[2], sc.ih[2], iz, oz);
-                const int gx = p.gx, gy = p.gy, gz = p.gz;
-                if (!((ix >= 0 && ix < gx - 1) && (iy >= 0 && iy < gy - 1) && (iz >= 0 && iz < gz - 1)))
-                    break;
-                double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
-                const int64_t b0 = ((int64_t)iz * gy + iy) * gx + ix;
-                const int64_t b1 = ((int64_t)(iz + 1) * gy + iy) * gx + ix;
-                const double2* E = p.efield;
-                // corner fields: .x/.y of [2c] = ex, ey; .x of [2c+1] = ez
-                double2 a00 = E[2 * b0], a01 = E[2 * (b0 + 1)], a10 = E[2 * (b0 + gx)], a11 = E[2 * (b0 + gx + 1)];
-                double2 c00 = E[2 * b1], c01 = E[2 * (b1 + 1)], c10 = E[2 * (b1 + gx)], c11 = E[2 * (b1 + gx + 1)];
-                double z00 = E[2 * b0 + 1].x, z01 = E[2 * (b0 + 1) + 1].x, z10 = E[2 * (b0 + gx) + 1].x,
-                       z11 = E[2 * (b0 + gx + 1) + 1].x;
-                double w00 = E[2 * b1 + 1].x, w01 = E[2 * (b1 + 1) + 1].x, w10 = E[2 * (b1 + gx) + 1].x,
-                       w11 = E[2 * (b1 + gx + 1) + 1].x;
-                const double factor = sc.factor, pref = p.kick_pref, m = p.kick_m;
-                double val = aoz * aoy * aox * z00;
-                val += aoz * aoy * ox * z01;
-                val += aoz * oy * aox * z10;
-                val += aoz * oy * ox * z11;
-                val += oz * aoy * aox * w00;
-                val += oz * aoy * ox * w01;
-                val += oz * oy * aox * w10;
-                val += oz * oy * ox * w11;
-                double pp = pref + dpop * pref;
-                double Eoc_i = sqrt(pp * pp + m * m);
-                double Eoc_f = Eoc_i + factor * (-pref) * val;
-                double ddp = (sqrt(Eoc_f * Eoc_f - m * m) - sqrt(Eoc_i * Eoc_i - m * m)) / pref;
-                dpop += ddp;
-                val = aoz * aoy * aox * a00.y;
-                val += aoz * aoy * ox * a01.y;
-                val += aoz * oy * aox * a10.y;
-                val += aoz * oy * ox * a11.y;
-                val += oz * aoy * aox * c00.y;
-                val += oz * aoy * ox * c01.y;
-                val += oz * oy * aox * c10.y;
-                val += oz * oy * ox * c11.y;
-                yp += factor * val;
-                val = aoz * aoy * aox * a00.x;
-                val += aoz * aoy * ox * a01.x;
-                val += aoz * oy * aox * a10.x;
-                val += aoz * oy * ox * a11.x;
-                val += oz * aoy * aox * c00.x;
-                val += oz * aoy * ox * c01.x;
-                val += oz * oy * aox * c10.x;
-                val += oz * oy * ox * c11.x;
-                xp += factor * val;
-                break;
-            }
-            default:
-                break;
-            }
+#pragma unroll
+            for (int q = 0; q < PPT; ++q) apply_op<VARIANT>(p, op, P[q], s_counts, s_mom_col);
         }
-        if (alive_in) {
-            p.parts[i] = x;
-            p.parts[i + S] = xp;
-            p.parts[i + 2 * S] = y;
-            p.parts[i + 3 * S] = yp;
-            p.parts[i + 4 * S] = cdt;
-            p.parts[i + 5 * S] = dpop;
-            if (!alive) p.masks[i] = 0;
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+            const int64_t i = base + q * blockDim.x + threadIdx.x;
+            if (i >= n) continue;
+            if (in[q]) {
+                p.parts[i] = P[q].x;
+                p.parts[i + S] = P[q].xp;
+                p.parts[i + 2 * S] = P[q].y;
+                p.parts[i + 3 * S] = P[q].yp;
+                p.parts[i + 4 * S] = P[q].cdt;
+                p.parts[i + 5 * S] = P[q].dpop;
+                if (!P[q].alive) p.masks[i] = 0;
+            }
+            if (p.write_discards && p.discards) p.discards[i] = (uint8_t)P[q].disc;
         }
-        if (p.write_discards && p.discards) p.discards[i] = (uint8_t)disc;
     }
 
     // per-aperture discard counts
@@ -583,11 +619,11 @@ cudaError_t launch_track(const TrackParams& p, cudaStream_t s)
 {
     int nb = track_grid_blocks();
     if (!track_needs_full(p.ops, p.nops))
-        track_kernel<TRACK_LIGHT><<<nb, kTrackThreads, 0, s>>>(p);
+        track_kernel<TRACK_LIGHT, 2><<<nb, kTrackThreads, 0, s>>>(p);
     else if (full_variant() == TRACK_FULL_WIDE)
-        track_kernel<TRACK_FULL_WIDE><<<nb, kTrackThreads, 0, s>>>(p);
+        track_kernel<TRACK_FULL_WIDE, 1><<<nb, kTrackThreads, 0, s>>>(p);
     else
-        track_kernel<TRACK_FULL><<<nb, kTrackThreads, 0, s>>>(p);
+        track_kernel<TRACK_FULL, 1><<<nb, kTrackThreads, 0, s>>>(p);
     return cudaGetLastError();
 }
 

@@ -164,3 +164,25 @@ def test_populate_gaussian_statistics(syn):
     b2 = syn.Bunch(ref, n, 1e11)
     b2.populate_gaussian(SIG_C0, seed=3)
     assert np.array_equal(b2.get_particles()[0], p)
+
+
+def test_cell_sorted_working_copy_matches_unsorted(syn, monkeypatch):
+    """The propagator's cell-ordered working copy is invisible to callers:
+    particles come back in their original order (ids, masks) and agree with
+    a run without it to the FP64 tolerance of the deposit order."""
+    n, shape = 50000, (16, 16, 32)
+    p = gaussian_bunch(n, SIG_C0, 61)
+    p[::97, 0] += 0.05  # a few particles outside the domain
+    out = []
+    for sort in ("1", "0"):
+        monkeypatch.setenv("SB2_CELL_SORT", sort)
+        lat, ref = product_lattice(fodo_cell())
+        prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(*shape), 8))
+        b = syn.Bunch(ref, n, 1e11)
+        b.set_particles(p)
+        prop.propagate(b, 1)
+        out.append(b.get_particles())
+    (a, am, ad), (u, um, ud) = out
+    assert np.array_equal(a[:, 6], np.arange(n)) and np.array_equal(am, um) and np.array_equal(ad, ud)
+    for j in range(6):
+        assert rel_l2(a[:, j], u[:, j]) <= 1e-10, j
