@@ -1121,12 +1121,17 @@ struct SpaceCharge {
     sb2_sc3d_options o;
     Dims d{};
     int64_t G = 0;
+    bool mixed = false;
     double* rho = nullptr;
     double2* S = nullptr;
     double* ghat = nullptr;
     double* phi = nullptr;
     double2* E = nullptr;
     double2 *tw_x = nullptr, *tw_y = nullptr, *tw_z = nullptr;
+    // mixed precision: FP32 spectrum, potential and field
+    float2* S32 = nullptr;
+    float* phi32 = nullptr;
+    float4* E32 = nullptr;
     ScState* state = nullptr;
     double* mom_partials = nullptr;
     int n_partials = 0;
@@ -1166,16 +1171,24 @@ struct SpaceCharge {
         d.ly = ilog2(d.ny);
         d.lz = ilog2(d.nz);
         G = (int64_t)d.gx * d.gy * d.gz;
+        mixed = o.precision == SB2_PRECISION_MIXED;
         rho = dalloc<double>(G, "rho");
-        phi = dalloc<double>(G, "phi");
-        E = dalloc<double2>(2 * G, "E");
-        S = dalloc<double2>((size_t)d.nz * d.ny * d.nkxp, "spectrum");
+        if (mixed) {
+            phi32 = dalloc<float>(G, "phi");
+            E32 = dalloc<float4>(G, "E");
+            S32 = dalloc<float2>((size_t)d.nz * d.ny * d.nkxp, "spectrum");
+            cuda_check(cudaMemset(E32, 0, sizeof(float4) * G), "memset");
+        } else {
+            phi = dalloc<double>(G, "phi");
+            E = dalloc<double2>(2 * G, "E");
+            S = dalloc<double2>((size_t)d.nz * d.ny * d.nkxp, "spectrum");
+            cuda_check(cudaMemset(E, 0, sizeof(double2) * 2 * G), "memset");
+        }
         ghat = dalloc<double>((size_t)(d.nx / 2 + 1) * (d.ny / 2 + 1) * (d.nz / 2 + 1), "ghat");
         state = dalloc<ScState>(1, "sc state");
         n_partials = track_grid_blocks();
         mom_partials = dalloc<double>((size_t)n_partials * 6, "moments");
         cuda_check(cudaMemset(state, 0, sizeof(ScState)), "memset");
-        cuda_check(cudaMemset(E, 0, sizeof(double2) * 2 * G), "memset");
         tw_x = twiddles(d.nx);
         tw_y = twiddles(d.ny);
         tw_z = twiddles(d.nz);
@@ -1192,6 +1205,9 @@ struct SpaceCharge {
         cudaFree(tw_x);
         cudaFree(tw_y);
         cudaFree(tw_z);
+        cudaFree(S32);
+        cudaFree(phi32);
+        cudaFree(E32);
     }
     // exp(-2 pi i k / L), k < L, from long-double sin/cos
     static double2* twiddles(int L)
@@ -1251,11 +1267,17 @@ struct SpaceCharge {
         }
         {
             ProfScope ps(PROF_SOLVE, s);
-            cuda_check(launch_convolve(rho, S, ghat, phi, d, tw_x, tw_y, tw_z, state, s), "convolve");
+            if (mixed)
+                cuda_check(launch_convolve_f32(rho, S32, ghat, phi32, d, tw_x, tw_y, tw_z, state, s), "convolve");
+            else
+                cuda_check(launch_convolve(rho, S, ghat, phi, d, tw_x, tw_y, tw_z, state, s), "convolve");
         }
         {
             ProfScope ps(PROF_EFIELD, s);
-            cuda_check(launch_efield(phi, E, d.gx, d.gy, d.gz, state, s), "efield");
+            if (mixed)
+                cuda_check(launch_efield_f32(phi32, E32, d.gx, d.gy, d.gz, state, s), "efield");
+            else
+                cuda_check(launch_efield(phi, E, d.gx, d.gy, d.gz, state, s), "efield");
         }
     }
 
@@ -1269,14 +1291,31 @@ struct SpaceCharge {
         if (h)
             for (int i = 0; i < 3; ++i) h[i] = st.h[i];
         if (rho_o) cuda_check(cudaMemcpy(rho_o, rho, sizeof(double) * G, cudaMemcpyDeviceToHost), "rho");
-        if (phi_o) cuda_check(cudaMemcpy(phi_o, phi, sizeof(double) * G, cudaMemcpyDeviceToHost), "phi");
+        if (phi_o) {
+            if (mixed) {
+                std::vector<float> f(G);
+                cuda_check(cudaMemcpy(f.data(), phi32, sizeof(float) * G, cudaMemcpyDeviceToHost), "phi");
+                for (int64_t i = 0; i < G; ++i) phi_o[i] = f[i];
+            } else
+                cuda_check(cudaMemcpy(phi_o, phi, sizeof(double) * G, cudaMemcpyDeviceToHost), "phi");
+        }
         if (ex || ey || ez) {
-            std::vector<double2> e(2 * G);
-            cuda_check(cudaMemcpy(e.data(), E, sizeof(double2) * 2 * G, cudaMemcpyDeviceToHost), "E");
-            for (int64_t i = 0; i < G; ++i) {
-                if (ex) ex[i] = e[2 * i].x;
-                if (ey) ey[i] = e[2 * i].y;
-                if (ez) ez[i] = e[2 * i + 1].x;
+            if (mixed) {
+                std::vector<float4> e(G);
+                cuda_check(cudaMemcpy(e.data(), E32, sizeof(float4) * G, cudaMemcpyDeviceToHost), "E");
+                for (int64_t i = 0; i < G; ++i) {
+                    if (ex) ex[i] = e[i].x;
+                    if (ey) ey[i] = e[i].y;
+                    if (ez) ez[i] = e[i].z;
+                }
+            } else {
+                std::vector<double2> e(2 * G);
+                cuda_check(cudaMemcpy(e.data(), E, sizeof(double2) * 2 * G, cudaMemcpyDeviceToHost), "E");
+                for (int64_t i = 0; i < G; ++i) {
+                    if (ex) ex[i] = e[2 * i].x;
+                    if (ey) ey[i] = e[2 * i].y;
+                    if (ez) ez[i] = e[2 * i + 1].x;
+                }
             }
         }
         if (scalars) {
@@ -1383,6 +1422,7 @@ struct Engine {
             if (sc) {
                 tp.sc = sc->state;
                 tp.efield = sc->E;
+                tp.efield32 = sc->E32;
                 tp.gx = sc->d.gx;
                 tp.gy = sc->d.gy;
                 tp.gz = sc->d.gz;

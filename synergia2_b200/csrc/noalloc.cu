@@ -119,6 +119,8 @@ extern "C" sb2_status sb2_sc3d_apply_noalloc(const sb2_sc3d_options* opts, doubl
     int rc = check_sc_options(*opts, &msg);
     if (rc != SB2_OK) return fail(rc, msg);
     const sb2_sc3d_options& o = *opts;
+    if (o.precision != SB2_PRECISION_FP64)
+        return fail(SB2_ERR_UNSUPPORTED, "sb2_sc3d_apply_noalloc: only the FP64 path runs without allocation");
     Dims d{};
     d.gx = o.shape[0];
     d.gy = o.shape[1];

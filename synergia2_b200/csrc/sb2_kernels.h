@@ -20,7 +20,8 @@ struct TrackParams {
     int32_t* ap_counts;         // discard counter per aperture slot
     double* moment_partials;    // [gridDim.x][6]
     const ScState* sc;          // space-charge state (kick)
-    const double2* efield;      // (gz,gy,gx) cells x {ex,ey | ez,0}
+    const double2* efield;      // (gz,gy,gx) cells x {ex,ey | ez,0}, FP64 path
+    const float4* efield32;     // (gz,gy,gx) cells x {ex,ey,ez,0}, mixed path (used when set)
     int32_t gx, gy, gz;
     double kick_pref, kick_m;
     int32_t nops;
@@ -87,6 +88,10 @@ cudaError_t launch_convolve(const double* rho, double2* S, const double* Ghat, d
                             const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
                             cudaStream_t s);
 cudaError_t launch_efield(const double* phi, double2* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s);
+cudaError_t launch_convolve_f32(const double* rho, float2* S, const double* Ghat, float* phi, const Dims& d,
+                                const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
+                                cudaStream_t s);
+cudaError_t launch_efield_f32(const float* phi, float4* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s);
 // sort.cu
 size_t sort_scratch_ints(int64_t G);
 cudaError_t launch_cell_sort(const SortBuffers& sb, const ScState* sc, int gx, int gy, int gz, cudaStream_t s);

@@ -308,103 +308,116 @@ __global__ void green_octant_kernel(const ScState* __restrict__ scp, double* G, 
 // result to the other buffer.  Input and output are in natural order.
 // tw[k] = exp(-2 pi i k / L) for k < L; `sign` > 0 selects the inverse.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double2 cmul(double2 a, double2 b)
-{
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// Complex helpers for double2 (FP64 path) and float2 (mixed path).
+template <typename C> struct CxT;
+template <> struct CxT<double2> { typedef double R; };
+template <> struct CxT<float2> { typedef float R; };
+__device__ __forceinline__ double2 mkc(double x, double y, double2*) { return make_double2(x, y); }
+__device__ __forceinline__ float2 mkc(float x, float y, float2*) { return make_float2(x, y); }
+template <typename C>
+__device__ __forceinline__ C cplx(typename CxT<C>::R x, typename CxT<C>::R y) { return mkc(x, y, (C*)nullptr); }
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) { return cplx<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+template <typename C>
+__device__ __forceinline__ C cadd(C a, C b) { return cplx<C>(a.x + b.x, a.y + b.y); }
+template <typename C>
+__device__ __forceinline__ C csub(C a, C b) { return cplx<C>(a.x - b.x, a.y - b.y); }
+// multiply by -i (forward) or +i (inverse)
+template <typename C>
+__device__ __forceinline__ C rot90(C a, bool inv) { return inv ? cplx<C>(-a.y, a.x) : cplx<C>(a.y, -a.x); }
 
 // In-register DFT of size R (2, 4, 8) in natural order: X[k] = sum_r v[r] w^(rk),
 // w = exp(-/+ 2 pi i / R).
-template <int R>
-__device__ __forceinline__ void dft_reg(double2* v, bool inv);
+template <int RAD, typename C>
+struct DftReg;
 
-template <>
-__device__ __forceinline__ void dft_reg<2>(double2* v, bool)
-{
-    double2 a = v[0], b = v[1];
-    v[0] = cadd(a, b);
-    v[1] = csub(a, b);
-}
-
-// multiply by -i (forward) or +i (inverse)
-__device__ __forceinline__ double2 rot90(double2 a, bool inv)
-{
-    return inv ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
-}
-
-template <>
-__device__ __forceinline__ void dft_reg<4>(double2* v, bool inv)
-{
-    double2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
-    double2 s13 = cadd(v[1], v[3]), d13 = rot90(csub(v[1], v[3]), inv);
-    v[0] = cadd(s02, s13);
-    v[2] = csub(s02, s13);
-    v[1] = cadd(d02, d13);
-    v[3] = csub(d02, d13);
-}
-
-template <>
-__device__ __forceinline__ void dft_reg<8>(double2* v, bool inv)
-{
-    const double h = 0.70710678118654752440;
-    // radix-2 first stage (decimation in frequency)
-    double2 a[4], b[4];
-    for (int r = 0; r < 4; ++r) {
-        a[r] = cadd(v[r], v[r + 4]);
-        b[r] = csub(v[r], v[r + 4]);
+template <typename C>
+struct DftReg<2, C> {
+    static __device__ __forceinline__ void run(C* v, bool)
+    {
+        C a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
     }
-    // twiddles w8^r on the difference branch
-    b[1] = inv ? make_double2(h * (b[1].x - b[1].y), h * (b[1].x + b[1].y))
-               : make_double2(h * (b[1].x + b[1].y), h * (b[1].y - b[1].x));
-    b[2] = rot90(b[2], inv);
-    b[3] = inv ? make_double2(-h * (b[3].x + b[3].y), h * (b[3].x - b[3].y))
-               : make_double2(h * (b[3].y - b[3].x), -h * (b[3].x + b[3].y));
-    dft_reg<4>(a, inv); // even outputs
-    dft_reg<4>(b, inv); // odd outputs
-    for (int k = 0; k < 4; ++k) {
-        v[2 * k] = a[k];
-        v[2 * k + 1] = b[k];
-    }
-}
+};
 
-template <int R>
-__device__ __forceinline__ void stockham_pass(const double2* __restrict__ src, double2* __restrict__ dst, int nl,
-                                              int L, int Ns, const double2* __restrict__ tw, bool inv)
+template <typename C>
+struct DftReg<4, C> {
+    static __device__ __forceinline__ void run(C* v, bool inv)
+    {
+        C s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+        C s13 = cadd(v[1], v[3]), d13 = rot90(csub(v[1], v[3]), inv);
+        v[0] = cadd(s02, s13);
+        v[2] = csub(s02, s13);
+        v[1] = cadd(d02, d13);
+        v[3] = csub(d02, d13);
+    }
+};
+
+template <typename C>
+struct DftReg<8, C> {
+    static __device__ __forceinline__ void run(C* v, bool inv)
+    {
+        typedef typename CxT<C>::R R;
+        const R h = (R)0.70710678118654752440;
+        // radix-2 first stage (decimation in frequency)
+        C a[4], b[4];
+        for (int r = 0; r < 4; ++r) {
+            a[r] = cadd(v[r], v[r + 4]);
+            b[r] = csub(v[r], v[r + 4]);
+        }
+        // twiddles w8^r on the difference branch
+        b[1] = inv ? cplx<C>(h * (b[1].x - b[1].y), h * (b[1].x + b[1].y))
+                   : cplx<C>(h * (b[1].x + b[1].y), h * (b[1].y - b[1].x));
+        b[2] = rot90(b[2], inv);
+        b[3] = inv ? cplx<C>(-h * (b[3].x + b[3].y), h * (b[3].x - b[3].y))
+                   : cplx<C>(h * (b[3].y - b[3].x), -h * (b[3].x + b[3].y));
+        DftReg<4, C>::run(a, inv); // even outputs
+        DftReg<4, C>::run(b, inv); // odd outputs
+        for (int k = 0; k < 4; ++k) {
+            v[2 * k] = a[k];
+            v[2 * k + 1] = b[k];
+        }
+    }
+};
+
+template <int RAD, typename C>
+__device__ __forceinline__ void stockham_pass(const C* __restrict__ src, C* __restrict__ dst, int nl, int L, int Ns,
+                                              const C* __restrict__ tw, bool inv)
 {
     // element j of line li sits at j * nl + li: consecutive threads take
     // consecutive lines, so every read and write below is contiguous
-    const int T = L / R;
+    const int T = L / RAD;
     const int total = nl * T;
-    const int tstep = L / (Ns * R);
+    const int tstep = L / (Ns * RAD);
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
         const int j = t / nl, li = t - j * nl;
         const int k = j & (Ns - 1);
-        double2 v[R];
+        C v[RAD];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = src[(j + r * T) * nl + li];
+        for (int r = 0; r < RAD; ++r) v[r] = src[(j + r * T) * nl + li];
         if (Ns > 1) {
 #pragma unroll
-            for (int r = 1; r < R; ++r) {
-                double2 w = tw[(k * r * tstep) & (L - 1)];
+            for (int r = 1; r < RAD; ++r) {
+                C w = tw[(k * r * tstep) & (L - 1)];
                 if (inv) w.y = -w.y;
                 v[r] = cmul(v[r], w);
             }
         }
-        dft_reg<R>(v, inv);
-        const int idxD = (j / Ns) * Ns * R + k;
+        DftReg<RAD, C>::run(v, inv);
+        const int idxD = (j / Ns) * Ns * RAD + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) dst[(idxD + r * Ns) * nl + li] = v[r];
+        for (int r = 0; r < RAD; ++r) dst[(idxD + r * Ns) * nl + li] = v[r];
     }
 }
 
 // FFT of the nl lines in b0 (layout j * nl + li); returns the buffer
 // holding the result.
-__device__ double2* smem_fft(double2* b0, double2* b1, int nl, int L, const double2* __restrict__ tw, bool inv)
+template <typename C>
+__device__ C* smem_fft(C* b0, C* b1, int nl, int L, const C* __restrict__ tw, bool inv)
 {
-    double2* src = b0;
-    double2* dst = b1;
+    C* src = b0;
+    C* dst = b1;
     int Ns = 1;
     while (Ns < L) {
         const int rem = L / Ns;
@@ -419,7 +432,7 @@ __device__ double2* smem_fft(double2* b0, double2* b1, int nl, int L, const doub
             Ns *= 2;
         }
         __syncthreads();
-        double2* t = src;
+        C* t = src;
         src = dst;
         dst = t;
     }
@@ -431,11 +444,24 @@ constexpr int kFftSmemBytes = 2 * kFftTile * 16;
 constexpr int kFftThreads = 256;
 
 // XF: pairs of real rows (y, y+1) of rho -> S rows (r2c, first gx inputs)
-__global__ void __launch_bounds__(kFftThreads) fft_xf_kernel(const double* __restrict__ rho, double2* S,
+// Global storage of the spectrum is C (double2, or float2 for the mixed
+// path); every pass converts to double2 on load and computes in FP64 in
+// shared memory and registers, so the mixed path only rounds at the five
+// pass boundaries.
+__device__ __forceinline__ double2 to_d(double2 v) { return v; }
+__device__ __forceinline__ double2 to_d(float2 v) { return make_double2(v.x, v.y); }
+template <typename C> __device__ __forceinline__ C from_d(double2 v);
+template <> __device__ __forceinline__ double2 from_d<double2>(double2 v) { return v; }
+template <> __device__ __forceinline__ float2 from_d<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+
+// XF: pairs of real rows (y, y+1) of rho -> S rows (r2c, first gx inputs)
+template <typename C>
+__global__ void __launch_bounds__(kFftThreads) fft_xf_kernel(const double* __restrict__ rho, C* S,
                                                              const double2* __restrict__ tw, Dims d,
                                                              const ScState* __restrict__ scp)
 {
-    extern __shared__ double2 sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    double2* sm = (double2*)sm_raw;
     if (!scp->valid) return;
     const int L = d.nx, nl = kFftTile / L;
     const int npy = (d.gy + 1) / 2;
@@ -455,7 +481,7 @@ __global__ void __launch_bounds__(kFftThreads) fft_xf_kernel(const double* __res
             v.x = rho[((int64_t)z * d.gy + ya) * d.gx + j];
             if (yb < d.gy) v.y = rho[((int64_t)z * d.gy + yb) * d.gx + j];
         }
-        b0[(j) * nlt + li] = v;
+        b0[j * nlt + li] = v;
     }
     __syncthreads();
     double2* r = smem_fft(b0, b1, nlt, L, tw, false);
@@ -465,20 +491,22 @@ __global__ void __launch_bounds__(kFftThreads) fft_xf_kernel(const double* __res
         int64_t l = l0 + li;
         int pr = (int)(l % npy), z = (int)(l / npy);
         int ya = 2 * pr, yb = ya + 1;
-        double2 Z = r[(k) * nlt + li], Zn = r[(((L - k) & (L - 1))) * nlt + li];
+        double2 Z = r[k * nlt + li], Zn = r[((L - k) & (L - 1)) * nlt + li];
         double2 A = make_double2((Z.x + Zn.x) * 0.5, (Z.y - Zn.y) * 0.5);
         double2 B = make_double2((Z.y + Zn.y) * 0.5, -(Z.x - Zn.x) * 0.5);
-        S[((int64_t)z * d.ny + ya) * d.nkxp + k] = A;
-        if (yb < d.gy) S[((int64_t)z * d.ny + yb) * d.nkxp + k] = B;
+        S[((int64_t)z * d.ny + ya) * d.nkxp + k] = from_d<C>(A);
+        if (yb < d.gy) S[((int64_t)z * d.ny + yb) * d.nkxp + k] = from_d<C>(B);
     }
 }
 
 // Y passes: lines (kx, z<gz) along y.  forward: first gy inputs, all ny
 // outputs; inverse: all inputs, first gy outputs.
-__global__ void __launch_bounds__(kFftThreads) fft_y_kernel(double2* S, const double2* __restrict__ tw, Dims d,
+template <typename C>
+__global__ void __launch_bounds__(kFftThreads) fft_y_kernel(C* S, const double2* __restrict__ tw, Dims d,
                                                             int inverse, const ScState* __restrict__ scp)
 {
-    extern __shared__ double2 sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    double2* sm = (double2*)sm_raw;
     if (!scp->valid) return;
     const int L = d.ny, nl = kFftTile / L;
     const int64_t nlines = (int64_t)d.nkx * d.gz;
@@ -493,8 +521,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_y_kernel(double2* S, const do
         int64_t l = l0 + li;
         int kx = (int)(l % d.nkx), z = (int)(l / d.nkx);
         double2 v = make_double2(0.0, 0.0);
-        if (j < nin) v = S[((int64_t)z * d.ny + j) * d.nkxp + kx];
-        b0[(j) * nlt + li] = v;
+        if (j < nin) v = to_d(S[((int64_t)z * d.ny + j) * d.nkxp + kx]);
+        b0[j * nlt + li] = v;
     }
     __syncthreads();
     double2* r = smem_fft(b0, b1, nlt, L, tw, inverse != 0);
@@ -503,18 +531,20 @@ __global__ void __launch_bounds__(kFftThreads) fft_y_kernel(double2* S, const do
         int j = idx / nlt, li = idx - j * nlt;
         int64_t l = l0 + li;
         int kx = (int)(l % d.nkx), z = (int)(l / d.nkx);
-        S[((int64_t)z * d.ny + j) * d.nkxp + kx] = r[(j) * nlt + li];
+        S[((int64_t)z * d.ny + j) * d.nkxp + kx] = from_d<C>(r[j * nlt + li]);
     }
 }
 
 // Z pass: lines (kx, ky) along z: forward (first gz inputs), multiply by
 // the real octant Ghat(kx, min(ky, ny-ky), min(kz, nz-kz)), inverse, first gz
 // outputs.  (alg_cplx_multiplier :350-372 fused between the transforms.)
-__global__ void __launch_bounds__(kFftThreads) fft_z_conv_kernel(double2* S, const double* __restrict__ Ghat,
+template <typename C>
+__global__ void __launch_bounds__(kFftThreads) fft_z_conv_kernel(C* S, const double* __restrict__ Ghat,
                                                                  const double2* __restrict__ tw, Dims d,
                                                                  const ScState* __restrict__ scp)
 {
-    extern __shared__ double2 sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    double2* sm = (double2*)sm_raw;
     if (!scp->valid) return;
     const int L = d.nz, nl = kFftTile / L;
     const int64_t nlines = (int64_t)d.nkx * d.ny;
@@ -528,8 +558,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_z_conv_kernel(double2* S, con
         int64_t l = l0 + li;
         int kx = (int)(l % d.nkx), ky = (int)(l / d.nkx);
         double2 v = make_double2(0.0, 0.0);
-        if (j < d.gz) v = S[((int64_t)j * d.ny + ky) * d.nkxp + kx];
-        b0[(j) * nlt + li] = v;
+        if (j < d.gz) v = to_d(S[((int64_t)j * d.ny + ky) * d.nkxp + kx]);
+        b0[j * nlt + li] = v;
     }
     __syncthreads();
     double2* r = smem_fft(b0, b1, nlt, L, tw, false);
@@ -541,9 +571,9 @@ __global__ void __launch_bounds__(kFftThreads) fft_z_conv_kernel(double2* S, con
         int kx = (int)(l % d.nkx), ky = (int)(l / d.nkx);
         int my = ky <= d.ny / 2 ? ky : d.ny - ky;
         int mz = kz <= d.nz / 2 ? kz : d.nz - kz;
-        double g = Ghat[((int64_t)mz * ogy + my) * ogx + kx];
-        double2 v = r[(kz) * nlt + li];
-        r[(kz) * nlt + li] = make_double2(v.x * g, v.y * g);
+        const double g = Ghat[((int64_t)mz * ogy + my) * ogx + kx];
+        double2 v = r[kz * nlt + li];
+        r[kz * nlt + li] = make_double2(v.x * g, v.y * g);
     }
     __syncthreads();
     double2* q = smem_fft(r, o, nlt, L, tw, true);
@@ -551,18 +581,20 @@ __global__ void __launch_bounds__(kFftThreads) fft_z_conv_kernel(double2* S, con
         int j = idx / nlt, li = idx - j * nlt;
         int64_t l = l0 + li;
         int kx = (int)(l % d.nkx), ky = (int)(l / d.nkx);
-        S[((int64_t)j * d.ny + ky) * d.nkxp + kx] = q[(j) * nlt + li];
+        S[((int64_t)j * d.ny + ky) * d.nkxp + kx] = from_d<C>(q[j * nlt + li]);
     }
 }
 
 // XI: Hermitian pairs of spectrum rows -> real rows (y, y+1) of phi (c2r,
 // first gx outputs); imaginary parts of the k = 0 and k = nx/2 terms are
 // ignored as a c2r transform does.
-__global__ void __launch_bounds__(kFftThreads) fft_xi_kernel(const double2* __restrict__ S, double* phi,
+template <typename C, typename RO>
+__global__ void __launch_bounds__(kFftThreads) fft_xi_kernel(const C* __restrict__ S, RO* phi,
                                                              const double2* __restrict__ tw, Dims d,
                                                              const ScState* __restrict__ scp)
 {
-    extern __shared__ double2 sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    double2* sm = (double2*)sm_raw;
     if (!scp->valid) return;
     const int L = d.nx, nl = kFftTile / L;
     const int npy = (d.gy + 1) / 2;
@@ -579,8 +611,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_xi_kernel(const double2* __re
         int pr = (int)(l % npy), z = (int)(l / npy);
         int ya = 2 * pr, yb = ya + 1;
         int k = j <= half ? j : L - j;
-        double2 A = S[((int64_t)z * d.ny + ya) * d.nkxp + k];
-        double2 B = (yb < d.gy) ? S[((int64_t)z * d.ny + yb) * d.nkxp + k] : make_double2(0.0, 0.0);
+        double2 A = to_d(S[((int64_t)z * d.ny + ya) * d.nkxp + k]);
+        double2 B = (yb < d.gy) ? to_d(S[((int64_t)z * d.ny + yb) * d.nkxp + k]) : make_double2(0.0, 0.0);
         if (k == 0 || k == half) {
             A.y = 0.0;
             B.y = 0.0;
@@ -589,7 +621,7 @@ __global__ void __launch_bounds__(kFftThreads) fft_xi_kernel(const double2* __re
             A.y = -A.y;
             B.y = -B.y;
         }
-        b0[(j) * nlt + li] = make_double2(A.x - B.y, A.y + B.x);
+        b0[j * nlt + li] = make_double2(A.x - B.y, A.y + B.x);
     }
     __syncthreads();
     double2* r = smem_fft(b0, b1, nlt, L, tw, true);
@@ -598,9 +630,9 @@ __global__ void __launch_bounds__(kFftThreads) fft_xi_kernel(const double2* __re
         int64_t l = l0 + li;
         int pr = (int)(l % npy), z = (int)(l / npy);
         int ya = 2 * pr, yb = ya + 1;
-        double2 v = r[(j) * nlt + li];
-        phi[((int64_t)z * d.gy + ya) * d.gx + j] = v.x;
-        if (yb < d.gy) phi[((int64_t)z * d.gy + yb) * d.gx + j] = v.y;
+        double2 v = r[j * nlt + li];
+        phi[((int64_t)z * d.gy + ya) * d.gx + j] = (RO)v.x;
+        if (yb < d.gy) phi[((int64_t)z * d.gy + yb) * d.gx + j] = (RO)v.y;
     }
 }
 
@@ -611,7 +643,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_green_kernel(double* G, const
                                                                 int axis, int L, int ox, int oy, int oz,
                                                                 const ScState* __restrict__ scp)
 {
-    extern __shared__ double2 sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    double2* sm = (double2*)sm_raw;
     if (!scp->valid) return;
     const int nl = kFftTile / L;
     const int half = L / 2;
@@ -649,26 +682,36 @@ __global__ void __launch_bounds__(kFftThreads) fft_green_kernel(double* G, const
 // E = -grad phi by central differences on interior cells of the original
 // grid, zero on the boundary: alg_force_extractor_doubled_domain
 // space_charge_3d_kernels.h:217-307 (h of the doubled domain).
-__global__ void efield_kernel(const double* __restrict__ phi, double2* E, int gx, int gy, int gz,
+__device__ __forceinline__ void store_e(double2* E, int64_t i, double ex, double ey, double ez)
+{
+    E[2 * i] = make_double2(ex, ey);
+    E[2 * i + 1] = make_double2(ez, 0.0);
+}
+__device__ __forceinline__ void store_e(float4* E, int64_t i, float ex, float ey, float ez)
+{
+    E[i] = make_float4(ex, ey, ez, 0.0f);
+}
+
+template <typename R, typename EV>
+__global__ void efield_kernel(const R* __restrict__ phi, EV* E, int gx, int gy, int gz,
                               const ScState* __restrict__ scp)
 {
     const ScState& sc = *scp;
     if (!sc.valid) return;
-    const double ihx = 0.5 / sc.dh[0], ihy = 0.5 / sc.dh[1], ihz = 0.5 / sc.dh[2];
+    const R ihx = (R)(0.5 / sc.dh[0]), ihy = (R)(0.5 / sc.dh[1]), ihz = (R)(0.5 / sc.dh[2]);
     const int64_t total = (int64_t)gx * gy * gz;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
         int ix = (int)(i % gx);
         int iy = (int)((i / gx) % gy);
         int iz = (int)(i / ((int64_t)gx * gy));
-        double ex = 0, ey = 0, ez = 0;
+        R ex = 0, ey = 0, ez = 0;
         if (!(ix == 0 || ix == gx - 1 || iy == 0 || iy == gy - 1 || iz == 0 || iz == gz - 1)) {
             ex = -(phi[i + 1] - phi[i - 1]) * ihx;
             ey = -(phi[i + gx] - phi[i - gx]) * ihy;
             ez = -(phi[i + (int64_t)gx * gy] - phi[i - (int64_t)gx * gy]) * ihz;
         }
-        E[2 * i] = make_double2(ex, ey);
-        E[2 * i + 1] = make_double2(ez, 0.0);
+        store_e(E, i, ex, ey, ez);
     }
 }
 
@@ -700,17 +743,29 @@ cudaError_t launch_deposit(const double* parts, int64_t stride, const uint8_t* m
     return cudaGetLastError();
 }
 
+template <typename C>
+static cudaError_t set_fft_smem_t()
+{
+    const int bytes = kFftSmemBytes;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(fft_xf_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+    if ((e = cudaFuncSetAttribute(fft_y_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+    if ((e = cudaFuncSetAttribute(fft_z_conv_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+    if ((e = cudaFuncSetAttribute(fft_xi_kernel<C, typename CxT<C>::R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  bytes)))
+        return e;
+    return cudaSuccess;
+}
+
 static cudaError_t set_fft_smem()
 {
     static bool done = false;
     if (done) return cudaSuccess;
-    const int bytes = kFftSmemBytes;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(fft_xf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
-    if ((e = cudaFuncSetAttribute(fft_y_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
-    if ((e = cudaFuncSetAttribute(fft_z_conv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
-    if ((e = cudaFuncSetAttribute(fft_xi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
-    if ((e = cudaFuncSetAttribute(fft_green_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
+    if ((e = set_fft_smem_t<double2>())) return e;
+    if ((e = set_fft_smem_t<float2>())) return e;
+    if ((e = cudaFuncSetAttribute(fft_green_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kFftSmemBytes)))
+        return e;
     done = true;
     return cudaSuccess;
 }
@@ -732,28 +787,54 @@ cudaError_t launch_green(const ScState* sc, double* G, const Dims& d, int linear
     return cudaGetLastError();
 }
 
-// rho -> phi through the five line passes.
-cudaError_t launch_convolve(const double* rho, double2* S, const double* Ghat, double* phi, const Dims& d,
-                            const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
-                            cudaStream_t s)
+template <typename C>
+static cudaError_t convolve_t(const double* rho, C* S, const double* Ghat, typename CxT<C>::R* phi, const Dims& d,
+                              const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
+                              cudaStream_t s)
 {
     cudaError_t e = set_fft_smem();
     if (e) return e;
     const size_t sh = kFftSmemBytes;
     const int npy = (d.gy + 1) / 2;
-    fft_xf_kernel<<<ceil_div64((int64_t)npy * d.gz, kFftTile / d.nx), kFftThreads, sh, s>>>(rho, S, tw_x, d, sc);
-    fft_y_kernel<<<ceil_div64((int64_t)d.nkx * d.gz, kFftTile / d.ny), kFftThreads, sh, s>>>(S, tw_y, d, 0, sc);
-    fft_z_conv_kernel<<<ceil_div64((int64_t)d.nkx * d.ny, kFftTile / d.nz), kFftThreads, sh, s>>>(S, Ghat, tw_z, d, sc);
-    fft_y_kernel<<<ceil_div64((int64_t)d.nkx * d.gz, kFftTile / d.ny), kFftThreads, sh, s>>>(S, tw_y, d, 1, sc);
-    fft_xi_kernel<<<ceil_div64((int64_t)npy * d.gz, kFftTile / d.nx), kFftThreads, sh, s>>>(S, phi, tw_x, d, sc);
+    fft_xf_kernel<C><<<ceil_div64((int64_t)npy * d.gz, kFftTile / d.nx), kFftThreads, sh, s>>>(rho, S, tw_x, d, sc);
+    fft_y_kernel<C><<<ceil_div64((int64_t)d.nkx * d.gz, kFftTile / d.ny), kFftThreads, sh, s>>>(S, tw_y, d, 0, sc);
+    fft_z_conv_kernel<C><<<ceil_div64((int64_t)d.nkx * d.ny, kFftTile / d.nz), kFftThreads, sh, s>>>(S, Ghat, tw_z, d, sc);
+    fft_y_kernel<C><<<ceil_div64((int64_t)d.nkx * d.gz, kFftTile / d.ny), kFftThreads, sh, s>>>(S, tw_y, d, 1, sc);
+    fft_xi_kernel<C, typename CxT<C>::R>
+        <<<ceil_div64((int64_t)npy * d.gz, kFftTile / d.nx), kFftThreads, sh, s>>>(S, phi, tw_x, d, sc);
     return cudaGetLastError();
+}
+
+// rho -> phi through the five line passes (FP64).
+cudaError_t launch_convolve(const double* rho, double2* S, const double* Ghat, double* phi, const Dims& d,
+                            const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
+                            cudaStream_t s)
+{
+    return convolve_t<double2>(rho, S, Ghat, phi, d, tw_x, tw_y, tw_z, sc, s);
+}
+
+// rho (FP64 accumulation) -> phi in FP32 (mixed precision: FP32 spectrum
+// and potential storage, FP64 butterflies).
+cudaError_t launch_convolve_f32(const double* rho, float2* S, const double* Ghat, float* phi, const Dims& d,
+                                const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
+                                cudaStream_t s)
+{
+    return convolve_t<float2>(rho, S, Ghat, phi, d, tw_x, tw_y, tw_z, sc, s);
 }
 
 cudaError_t launch_efield(const double* phi, double2* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s)
 {
     int64_t total = (int64_t)gx * gy * gz;
     int nb = (int)std::min<int64_t>((total + 255) / 256, (int64_t)sm_count() * 16);
-    efield_kernel<<<nb, 256, 0, s>>>(phi, E, gx, gy, gz, sc);
+    efield_kernel<double, double2><<<nb, 256, 0, s>>>(phi, E, gx, gy, gz, sc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_efield_f32(const float* phi, float4* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s)
+{
+    int64_t total = (int64_t)gx * gy * gz;
+    int nb = (int)std::min<int64_t>((total + 255) / 256, (int64_t)sm_count() * 16);
+    efield_kernel<float, float4><<<nb, 256, 0, s>>>(phi, E, gx, gy, gz, sc);
     return cudaGetLastError();
 }
 

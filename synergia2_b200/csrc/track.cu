@@ -379,6 +379,30 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
             double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
             const int64_t b0 = ((int64_t)iz * gy + iy) * gx + ix;
             const int64_t b1 = ((int64_t)(iz + 1) * gy + iy) * gx + ix;
+            if (p.efield32) {
+                // mixed precision: FP32 field, one 16-byte load per corner,
+                // interpolation weights and the kick in FP64
+                const float4* F = p.efield32;
+                const float4 f000 = F[b0], f001 = F[b0 + 1], f010 = F[b0 + gx], f011 = F[b0 + gx + 1];
+                const float4 f100 = F[b1], f101 = F[b1 + 1], f110 = F[b1 + gx], f111 = F[b1 + gx + 1];
+                const double w000 = aoz * aoy * aox, w001 = aoz * aoy * ox, w010 = aoz * oy * aox,
+                             w011 = aoz * oy * ox, w100 = oz * aoy * aox, w101 = oz * aoy * ox,
+                             w110 = oz * oy * aox, w111 = oz * oy * ox;
+                const double factor = sc.factor, pref = p.kick_pref, m = p.kick_m;
+                double val = w000 * f000.z + w001 * f001.z + w010 * f010.z + w011 * f011.z + w100 * f100.z +
+                             w101 * f101.z + w110 * f110.z + w111 * f111.z;
+                double pp = pref + dpop * pref;
+                double Eoc_i = sqrt(pp * pp + m * m);
+                double Eoc_f = Eoc_i + factor * (-pref) * val;
+                dpop += (sqrt(Eoc_f * Eoc_f - m * m) - sqrt(Eoc_i * Eoc_i - m * m)) / pref;
+                val = w000 * f000.y + w001 * f001.y + w010 * f010.y + w011 * f011.y + w100 * f100.y +
+                      w101 * f101.y + w110 * f110.y + w111 * f111.y;
+                yp += factor * val;
+                val = w000 * f000.x + w001 * f001.x + w010 * f010.x + w011 * f011.x + w100 * f100.x +
+                      w101 * f101.x + w110 * f110.x + w111 * f111.x;
+                xp += factor * val;
+                break;
+            }
             const double2* E = p.efield;
             // corner fields: .x/.y of [2c] = ex, ey; .x of [2c+1] = ez
             double2 a00 = E[2 * b0], a01 = E[2 * (b0 + 1)], a10 = E[2 * (b0 + gx)], a11 = E[2 * (b0 + gx + 1)];

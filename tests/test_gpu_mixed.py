@@ -1,0 +1,62 @@
+"""Mixed-precision space charge: FP64 particles, maps, deposit accumulation
+and Green function; FP32 spectrum, potential and field.
+
+Acceptance bounds (the configurations' own): field error <= 1e-5 relative L2
+against the FP64 path on the same particles, rms-emittance difference
+<= 1e-4 relative after many kicks.
+"""
+import numpy as np
+import pytest
+
+from helpers import MP, SIG_C0, fodo_cell, gaussian_bunch, product_lattice, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL_MIXED = 1e-5
+EMIT_TOL_MIXED = 1e-4
+
+
+def _kick(syn, p, shape, precision, green_fn=1):
+    opts = syn.Space_charge_3d_open_hockney_options(*shape)
+    opts.precision = precision
+    opts.green_fn = green_fn
+    ref = syn.Reference_particle(1, syn.Four_momentum(MP, MP + 2.5))
+    b = syn.Bunch(ref, p.shape[0], 1e11)
+    b.set_particles(p)
+    sc = syn.Space_charge_3d_open_hockney(opts)
+    sc.apply(b, 1.25 / (0.96 * 299792458.0))
+    return b.get_particles()[0], sc.last()
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 64), (64, 64, 128)])
+@pytest.mark.parametrize("green_fn", [1, 0])
+def test_mixed_field_error(syn, shape, green_fn):
+    p = gaussian_bunch(400000, SIG_C0, 71)
+    p64, f64 = _kick(syn, p, shape, syn.precision_t.fp64, green_fn)
+    p32, f32 = _kick(syn, p, shape, syn.precision_t.mixed, green_fn)
+    assert np.array_equal(f64["rho"], f32["rho"]) or rel_l2(f32["rho"], f64["rho"]) <= 1e-12
+    for c in ("ex", "ey", "ez"):
+        assert rel_l2(f32[c], f64[c]) <= FIELD_TOL_MIXED, c
+    for j in (1, 3, 5):
+        assert rel_l2(p32[:, j] - p[:, j], p64[:, j] - p[:, j]) <= FIELD_TOL_MIXED, j
+
+
+def test_mixed_emittance_after_many_kicks(syn):
+    """FODO cell, 8 kicks per cell, 25 turns (200 kicks): rms emittances of
+    the mixed run within 1e-4 relative of the FP64 run from the same seed."""
+    n, shape, turns = 200000, (32, 32, 64), 25
+    p = gaussian_bunch(n, SIG_C0, 72)
+    emits, parts = [], []
+    for prec in (syn.precision_t.fp64, syn.precision_t.mixed):
+        lat, ref = product_lattice(fodo_cell())
+        opts = syn.Space_charge_3d_open_hockney_options(*shape)
+        opts.precision = prec
+        prop = syn.Propagator(lat, syn.Split_operator_stepper(opts, 8))
+        b = syn.Bunch(ref, n, 1e11)
+        b.set_particles(p)
+        prop.propagate(b, turns)
+        emits.append(b.moments()[2])
+        parts.append(b.get_particles()[0])
+    e64, e32 = emits
+    assert np.all(np.abs(e32 / e64 - 1) <= EMIT_TOL_MIXED), e32 / e64 - 1
+    assert np.array_equal(parts[0][:, 6], parts[1][:, 6])
