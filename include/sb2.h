@@ -181,6 +181,12 @@ sb2_status sb2_propagator_propagate(sb2_propagator* p, sb2_bunch* b, int32_t tur
  * around the turn). */
 sb2_status sb2_propagator_propagate_steps(sb2_propagator* p, sb2_bunch* b, int32_t first,
                                           int32_t count, void* stream);
+/* Replay each turn from a CUDA graph: the first turn with a given launch
+ * signature is captured, later turns whose host-side re-derivation (op
+ * lists, time steps) gives the same signature are replayed with one graph
+ * launch.  The cell-ordered working copy is not used in this mode. */
+sb2_status sb2_propagator_set_graphs(sb2_propagator* p, int32_t on);
+sb2_status sb2_propagator_graph_stats(sb2_propagator* p, int64_t* captures, int64_t* replays);
 /* Charge lost on lattice element `index` through the aperture operations
  * (Lattice_element::deposit_charge, aperture_operation.h:14-24), summed over
  * all bunches this propagator has propagated. */
@@ -190,6 +196,19 @@ sb2_status sb2_propagator_deposited_charge(sb2_propagator* p, int32_t index, dou
  * Any output may be NULL. */
 sb2_status sb2_propagator_sc_last(sb2_propagator* p, double left[3], double h[3], double* rho,
                                   double* phi, double* ex, double* ey, double* ez, double scalars[8]);
+
+/* ---------------------------------------------------------------------
+ * Batch of independent jobs (no counterpart in the reference, which runs
+ * bunch trains through one simulator): each job is a (propagator, bunch)
+ * pair on its own CUDA stream; sb2_batch_run advances the listed slots by
+ * the given number of turns concurrently and returns when all are done.
+ * ------------------------------------------------------------------- */
+typedef struct sb2_batch sb2_batch;
+sb2_status sb2_batch_create(sb2_batch** out);
+sb2_status sb2_batch_destroy(sb2_batch* q);
+sb2_status sb2_batch_add(sb2_batch* q, sb2_propagator* p, sb2_bunch* b, int32_t* slot);
+sb2_status sb2_batch_remove(sb2_batch* q, int32_t slot);
+sb2_status sb2_batch_run(sb2_batch* q, const int32_t* slots, const int32_t* turns, int32_t n);
 
 /* ---------------------------------------------------------------------
  * Collective operator alone: Space_charge_3d_open_hockney::apply_bunch

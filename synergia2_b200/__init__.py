@@ -23,7 +23,7 @@ import numpy as np
 from . import _lib
 from ._lib import SB2Error, check, lib
 
-__all__ = ["pconstants", "Four_momentum", "Reference_particle", "Lattice_element", "Lattice", "Bunch",
+__all__ = ["Batch", "pconstants", "Four_momentum", "Reference_particle", "Lattice_element", "Lattice", "Bunch",
            "Space_charge_3d_open_hockney_options", "Space_charge_3d_open_hockney", "Split_operator_stepper",
            "Split_operator_stepper_elements", "Independent_stepper_elements", "Propagator", "SB2Error",
            "green_fn_t", "precision_t"]
@@ -425,6 +425,15 @@ class Propagator:
     def propagate_steps(self, bunch, first, count, stream=None):
         check(lib().sb2_propagator_propagate_steps(self.h, bunch.h, int(first), int(count), stream))
 
+    def set_graphs(self, on=True):
+        """Replay each turn from a CUDA graph (captured on first use)."""
+        check(lib().sb2_propagator_set_graphs(self.h, 1 if on else 0))
+
+    def graph_stats(self):
+        c, r = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().sb2_propagator_graph_stats(self.h, ctypes.byref(c), ctypes.byref(r)))
+        return c.value, r.value
+
     def deposited_charge(self, index):
         c = ctypes.c_double()
         check(lib().sb2_propagator_deposited_charge(self.h, index, ctypes.byref(c)))
@@ -433,3 +442,42 @@ class Propagator:
     def sc_last(self):
         gx, gy, gz = self.stepper.collective_options.shape
         return _sc_last(lambda *a: lib().sb2_propagator_sc_last(self.h, *a), gx, gy, gz)
+
+
+class Batch:
+    """Independent (propagator, bunch) jobs advanced concurrently, one CUDA
+    stream per job.  A propagator must not be shared between jobs."""
+
+    def __init__(self):
+        h = ctypes.c_void_p()
+        check(lib().sb2_batch_create(ctypes.byref(h)))
+        self.h = h
+        self.jobs = {}
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            try:
+                lib().sb2_batch_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+    def add(self, propagator, bunch):
+        slot = ctypes.c_int32()
+        check(lib().sb2_batch_add(self.h, propagator.h, bunch.h, ctypes.byref(slot)))
+        self.jobs[slot.value] = (propagator, bunch)
+        return slot.value
+
+    def remove(self, slot):
+        check(lib().sb2_batch_remove(self.h, slot))
+        self.jobs.pop(slot, None)
+
+    def run(self, turns_by_slot):
+        """Advance each listed slot by its number of turns, concurrently."""
+        items = list(turns_by_slot.items())
+        if not items:
+            return
+        slots = (ctypes.c_int32 * len(items))(*[k for k, _ in items])
+        turns = (ctypes.c_int32 * len(items))(*[int(v) for _, v in items])
+        check(lib().sb2_batch_run(self.h, slots, turns, len(items)))

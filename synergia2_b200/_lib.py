@@ -66,6 +66,13 @@ SIGNATURES = {
     "sb2_propagator_propagate": (_i32, [_vp, _vp, _i32, _vp]),
     "sb2_propagator_propagate_steps": (_i32, [_vp, _vp, _i32, _i32, _vp]),
     "sb2_propagator_deposited_charge": (_i32, [_vp, _i32, _pd]),
+    "sb2_propagator_set_graphs": (_i32, [_vp, _i32]),
+    "sb2_propagator_graph_stats": (_i32, [_vp, _pi64, _pi64]),
+    "sb2_batch_create": (_i32, [_ppv]),
+    "sb2_batch_destroy": (_i32, [_vp]),
+    "sb2_batch_add": (_i32, [_vp, _vp, _vp, _pi32]),
+    "sb2_batch_remove": (_i32, [_vp, _i32]),
+    "sb2_batch_run": (_i32, [_vp, _pi32, _pi32, _i32]),
     "sb2_propagator_sc_last": (_i32, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd]),
     "sb2_sc3d_create": (_i32, [_popts, _ppv]),
     "sb2_sc3d_destroy": (_i32, [_vp]),

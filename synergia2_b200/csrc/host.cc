@@ -1017,6 +1017,24 @@ static MapOp op_aperture(const Lattice& lat, const std::string& type, const Slic
 
 
 // ---------------------------------------------------------------------------
+// Launch signature: while a turn is captured into a CUDA graph or re-derived
+// on the host, every flush and solve appends the bytes that determine its
+// launches (op lists, bookkeeping program, time step, Ghat refresh).  In
+// dry-run mode nothing is launched; the host state still advances.
+// ---------------------------------------------------------------------------
+struct LaunchSig {
+    bool dry = false;
+    std::vector<unsigned char>* sig = nullptr;
+};
+static thread_local LaunchSig g_sig;
+static void sig_append(const void* p, size_t n)
+{
+    if (!g_sig.sig) return;
+    const unsigned char* c = (const unsigned char*)p;
+    g_sig.sig->insert(g_sig.sig->end(), c, c + n);
+}
+
+// ---------------------------------------------------------------------------
 // Kernel-category timing with CUDA events on the launching stream (the
 // reference's scoped_simple_timer labels, utils/simple_timer.h:50-66).
 // Off unless sb2_profile_enable(1) is called.
@@ -1090,7 +1108,7 @@ struct ProfScope {
     Profiler::Rec r{};
     ProfScope(int c, cudaStream_t st) : cat(c), s(st)
     {
-        if (g_prof.on) r = g_prof.begin(cat, s);
+        if (g_prof.on && !g_sig.sig) r = g_prof.begin(cat, s);
     }
     ~ProfScope()
     {
@@ -1255,6 +1273,12 @@ struct SpaceCharge {
     // in `state`.
     void solve(const Bunch& b, cudaStream_t s)
     {
+        const bool refresh = !o.domain_fixed || !ghat_valid;
+        sig_append(&refresh, sizeof(refresh));
+        if (g_sig.dry) {
+            if (refresh) ghat_valid = true;
+            return;
+        }
         {
             ProfScope ps(PROF_DEPOSIT, s);
             cuda_check(cudaMemsetAsync(rho, 0, sizeof(double) * G, s), "memset rho");
@@ -1395,6 +1419,18 @@ struct Engine {
     void flush(Bunch& b, SpaceCharge* sc, double* elem_charge, bool with_domain, double time_step, cudaStream_t s)
     {
         if (with_domain && !sc->o.domain_fixed) ops.push_back(new_op(OP_MOMENTS));
+        if (g_sig.sig) {
+            uint64_t nops = ops.size();
+            sig_append(&nops, sizeof(nops));
+            if (nops) sig_append(ops.data(), sizeof(MapOp) * nops);
+            sig_append(&book, sizeof(book));
+            sig_append(&with_domain, sizeof(with_domain));
+            sig_append(&time_step, sizeof(time_step));
+        }
+        if (g_sig.dry) {
+            reset();
+            return;
+        }
         size_t i = 0;
         while (i < ops.size()) {
             size_t n = std::min<size_t>(kMaxOpsPerPass, ops.size() - i);
@@ -1491,6 +1527,8 @@ struct Propagator {
     }
     ~Propagator()
     {
+        drop_graphs();
+        if (own_stream) cudaStreamDestroy(own_stream);
         cudaFree(elem_charge);
         free_sort();
     }
@@ -1635,8 +1673,141 @@ struct Propagator {
 
     bool sort_active = false;
 
+    // ----- CUDA-graph turns ------------------------------------------------
+    // A turn's launches are captured once and replayed while the host-side
+    // re-derivation of the turn gives the same launch signature.
+    bool use_graphs = false;
+    cudaStream_t own_stream = nullptr; // capture needs a non-legacy stream
+    cudaStream_t graph_stream(cudaStream_t s)
+    {
+        if (s) return s;
+        if (!own_stream) cuda_check(cudaStreamCreate(&own_stream), "stream");
+        return own_stream;
+    }
+    struct CachedGraph {
+        std::vector<unsigned char> sig;
+        cudaGraphExec_t exec = nullptr;
+        uint64_t last_use = 0;
+    };
+    std::vector<CachedGraph> graphs;
+    uint64_t graph_clock = 0;
+    int64_t graph_captures = 0, graph_replays = 0;
+
+    struct HostSnap {
+        Refpart ref, design;
+        bool design_set;
+        int turns_done;
+        std::vector<MapOp> ops;
+        PassBook book;
+        int nslots;
+        bool ghat_valid;
+    };
+    HostSnap snap(const Bunch& b) const
+    {
+        HostSnap h{b.ref, b.design, b.design_set, b.turns_done, engine_->ops, engine_->book, engine_->nslots,
+                   sc ? sc->ghat_valid : false};
+        return h;
+    }
+    void restore(Bunch& b, const HostSnap& h)
+    {
+        b.ref = h.ref;
+        b.design = h.design;
+        b.design_set = h.design_set;
+        b.turns_done = h.turns_done;
+        engine_->ops = h.ops;
+        engine_->book = h.book;
+        engine_->nslots = h.nslots;
+        if (sc) sc->ghat_valid = h.ghat_valid;
+    }
+    void run_turn(Bunch& b, cudaStream_t s)
+    {
+        b.ref.start_repetition();
+        for (auto const& st : steps) run_step(b, st, s);
+        b.turns_done += 1;
+    }
+    void drop_graphs()
+    {
+        for (auto& g : graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+    }
+
+    void propagate_graph_turn(Bunch& b, cudaStream_t s)
+    {
+        HostSnap s0 = snap(b);
+        std::vector<unsigned char> sig;
+        g_sig.dry = true;
+        g_sig.sig = &sig;
+        try {
+            run_turn(b, s);
+        } catch (...) {
+            g_sig = LaunchSig{};
+            throw;
+        }
+        g_sig = LaunchSig{};
+        ++graph_clock;
+        for (auto& g : graphs)
+            if (g.sig == sig) {
+                g.last_use = graph_clock;
+                ++graph_replays;
+                cuda_check(cudaGraphLaunch(g.exec, s), "graph launch");
+                return;
+            }
+        // capture this turn
+        restore(b, s0);
+        std::vector<unsigned char> sig2;
+        cudaGraph_t graph = nullptr;
+        cuda_check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+        g_sig.sig = &sig2;
+        try {
+            run_turn(b, s);
+        } catch (...) {
+            g_sig = LaunchSig{};
+            cudaStreamEndCapture(s, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        g_sig = LaunchSig{};
+        cuda_check(cudaStreamEndCapture(s, &graph), "end capture");
+        cudaGraphExec_t exec = nullptr;
+        cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        cuda_check(e, "graph instantiate");
+        if (graphs.size() >= 4) { // evict the least recently used
+            size_t lru = 0;
+            for (size_t k = 1; k < graphs.size(); ++k)
+                if (graphs[k].last_use < graphs[lru].last_use) lru = k;
+            cudaGraphExecDestroy(graphs[lru].exec);
+            graphs.erase(graphs.begin() + lru);
+        }
+        graphs.push_back(CachedGraph{sig2, exec, graph_clock});
+        ++graph_captures;
+        cuda_check(cudaGraphLaunch(exec, s), "graph launch");
+    }
+
+    // Turns without the end-of-call synchronisation (batched jobs): the
+    // pending second half of the last step is flushed at the end.
+    void propagate_async(Bunch& b, int turns, cudaStream_t s)
+    {
+        if (use_graphs) s = graph_stream(s);
+        begin(b);
+        for (int t = 0; t < turns; ++t) {
+            if (use_graphs)
+                propagate_graph_turn(b, s);
+            else
+                run_turn(b, s);
+        }
+        engine_->flush(b, sc.get(), elem_charge, false, 0.0, s);
+    }
+
     void propagate(Bunch& b, int turns, cudaStream_t s)
     { // Propagator::propagate propagator.cc:157-283 (one bunch, no diagnostics)
+        if (use_graphs) {
+            cudaStream_t gs = graph_stream(s);
+            propagate_async(b, turns, gs);
+            finish(b, gs);
+            return;
+        }
         begin(b);
         SortScope scope(*this, b, s);
         sort_active = scope.active;
@@ -1685,6 +1856,80 @@ struct ScOperator {
         engine.flush(b, &sc, nullptr, false, 0.0, s);
         cuda_check(cudaStreamSynchronize(s), "sync");
         sc.check_error();
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Batch of independent jobs (propagator + bunch), each on its own stream:
+// one call advances the listed jobs concurrently.  With CUDA-graph turns the
+// host cost per job and turn is one signature check and one graph launch.
+// ---------------------------------------------------------------------------
+struct Batch {
+    struct Job {
+        Propagator* p = nullptr;
+        Bunch* b = nullptr;
+        cudaStream_t s = nullptr;
+        bool used = false;
+    };
+    std::vector<Job> jobs;
+    ~Batch()
+    {
+        for (auto& j : jobs)
+            if (j.s) cudaStreamDestroy(j.s);
+    }
+    int add(Propagator* p, Bunch* b)
+    {
+        for (size_t k = 0; k < jobs.size(); ++k)
+            if (!jobs[k].used) {
+                jobs[k].p = p;
+                jobs[k].b = b;
+                jobs[k].used = true;
+                return (int)k;
+            }
+        Job j;
+        j.p = p;
+        j.b = b;
+        j.used = true;
+        cuda_check(cudaStreamCreateWithFlags(&j.s, cudaStreamNonBlocking), "stream");
+        jobs.push_back(j);
+        return (int)jobs.size() - 1;
+    }
+    void remove(int slot)
+    {
+        if (slot < 0 || slot >= (int)jobs.size() || !jobs[slot].used) throw Error(SB2_ERR_INVALID, "bad batch slot");
+        jobs[slot].used = false;
+        jobs[slot].p = nullptr;
+        jobs[slot].b = nullptr;
+    }
+    void run(const int32_t* slots, const int32_t* turns, int n)
+    {
+        std::string err;
+        sb2_status code = SB2_OK;
+        std::vector<int> launched;
+        for (int k = 0; k < n; ++k) {
+            int sl = slots[k];
+            if (sl < 0 || sl >= (int)jobs.size() || !jobs[sl].used) throw Error(SB2_ERR_INVALID, "bad batch slot");
+            try {
+                jobs[sl].p->propagate_async(*jobs[sl].b, turns[k], jobs[sl].s);
+                launched.push_back(sl);
+            } catch (const Error& e) {
+                if (code == SB2_OK) {
+                    code = e.code;
+                    err = e.what();
+                }
+            }
+        }
+        for (int sl : launched) {
+            try {
+                jobs[sl].p->finish(*jobs[sl].b, jobs[sl].s);
+            } catch (const Error& e) {
+                if (code == SB2_OK) {
+                    code = e.code;
+                    err = e.what();
+                }
+            }
+        }
+        if (code != SB2_OK) throw Error(code, err);
     }
 };
 
@@ -1737,6 +1982,9 @@ struct sb2_propagator {
 };
 struct sb2_sc3d {
     std::unique_ptr<ScOperator> op;
+};
+struct sb2_batch {
+    Batch q;
 };
 
 static thread_local std::string g_last_error;
@@ -2172,6 +2420,63 @@ sb2_status sb2_propagator_propagate_steps(sb2_propagator* p, sb2_bunch* b, int32
     p->p->propagate_steps(b->b, first, count, as_stream(stream));
     SB2_CATCH
 }
+sb2_status sb2_propagator_set_graphs(sb2_propagator* p, int32_t on)
+{
+    SB2_TRY
+    SB2_REQUIRE(p, "null propagator");
+    p->p->use_graphs = on != 0;
+    if (!on) p->p->drop_graphs();
+    SB2_CATCH
+}
+
+sb2_status sb2_propagator_graph_stats(sb2_propagator* p, int64_t* captures, int64_t* replays)
+{
+    SB2_TRY
+    SB2_REQUIRE(p, "null propagator");
+    if (captures) *captures = p->p->graph_captures;
+    if (replays) *replays = p->p->graph_replays;
+    SB2_CATCH
+}
+
+sb2_status sb2_batch_create(sb2_batch** out)
+{
+    SB2_TRY
+    SB2_REQUIRE(out, "null out");
+    *out = new sb2_batch();
+    SB2_CATCH
+}
+
+sb2_status sb2_batch_destroy(sb2_batch* q)
+{
+    SB2_TRY
+    delete q;
+    SB2_CATCH
+}
+
+sb2_status sb2_batch_add(sb2_batch* q, sb2_propagator* p, sb2_bunch* b, int32_t* slot)
+{
+    SB2_TRY
+    SB2_REQUIRE(q && p && b && slot, "null argument");
+    *slot = q->q.add(p->p.get(), &b->b);
+    SB2_CATCH
+}
+
+sb2_status sb2_batch_remove(sb2_batch* q, int32_t slot)
+{
+    SB2_TRY
+    SB2_REQUIRE(q, "null batch");
+    q->q.remove(slot);
+    SB2_CATCH
+}
+
+sb2_status sb2_batch_run(sb2_batch* q, const int32_t* slots, const int32_t* turns, int32_t n)
+{
+    SB2_TRY
+    SB2_REQUIRE(q && (n == 0 || (slots && turns)) && n >= 0, "bad argument");
+    q->q.run(slots, turns, n);
+    SB2_CATCH
+}
+
 sb2_status sb2_propagator_deposited_charge(sb2_propagator* p, int32_t index, double* charge)
 {
     SB2_TRY
