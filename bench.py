@@ -92,6 +92,171 @@ def fodo_lattice(syn):
     return product_lattice(fodo_cell())
 
 
+def c1_propagator(syn, precision, graphs=False):
+    lat, ref = fodo_lattice(syn)
+    opts = syn.Space_charge_3d_open_hockney_options(*GRID)
+    opts.precision = precision
+    prop = syn.Propagator(lat, syn.Split_operator_stepper(opts, KICKS_PER_CELL))
+    if graphs:
+        prop.set_graphs(True)
+    return prop, ref
+
+
+def _emittances(bunch):
+    return [float(e) for e in bunch.moments()[2]]
+
+
+def mixed_vs_fp64(syn, torch, steps, warmup, passes, seed=1):
+    """The FODO workload in mixed precision (FP64 particles and maps, FP32
+    spectrum / potential / field): throughput over `steps` steps with CUDA
+    events; the field error of one solve of each precision on the same
+    particles (the FP64 run's state after `passes` passes); the relative
+    rms-emittance difference per plane after `passes` passes from one
+    seed."""
+    fp64, mixed = syn.precision_t.fp64, syn.precision_t.mixed
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    prop, ref = c1_propagator(syn, mixed)
+    b = syn.Bunch(ref, N_PART, REAL_NUM)
+    b.populate_gaussian(SIGMAS, seed=seed)
+    prop.propagate_steps(b, 0, warmup, stream=sp)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    prop.propagate_steps(b, warmup, steps, stream=sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    rate = b.get_total_num() * steps / (ms * 1e-3)
+    del prop, b
+
+    ends, emits = [], []
+    for prec in (fp64, mixed):
+        prop, ref = c1_propagator(syn, prec)
+        b = syn.Bunch(ref, N_PART, REAL_NUM)
+        b.populate_gaussian(SIGMAS, seed=seed)
+        prop.propagate(b, passes)
+        emits.append(_emittances(b))
+        ends.append(b)
+        del prop
+    e64, e32 = emits
+    demit = [abs(a / c - 1.0) for a, c in zip(e32, e64)]
+
+    # field error: both precisions solve on the FP64 run's final particles
+    parts, masks, _ = ends[0].get_particles()
+    fields = []
+    for prec in (fp64, mixed):
+        opts = syn.Space_charge_3d_open_hockney_options(*GRID)
+        opts.precision = prec
+        bb = syn.Bunch(ends[0].reference_particle, N_PART, REAL_NUM)
+        bb.set_particles(parts, masks)
+        sc = syn.Space_charge_3d_open_hockney(opts)
+        sc.apply(bb, 1.25 / (ends[0].reference_particle.get_beta() * 299792458.0))
+        fields.append(sc.last())
+        del sc, bb
+    num = sum(float(((fields[1][c] - fields[0][c]) ** 2).sum()) for c in ("ex", "ey", "ez"))
+    den = sum(float((fields[0][c] ** 2).sum()) for c in ("ex", "ey", "ez"))
+    return {"value": rate, "unit": "macroparticle-steps/s", "ms_per_step": ms / steps,
+            "precision": "mixed (FP64 particles, maps, deposit and Green function; FP32 spectrum, potential, field)",
+            "field_rel_l2": math.sqrt(num / den), "field_tol": 1e-5,
+            "emittance_rel_diff_xyz": demit, "emittance_tol": 1e-4, "passes": passes}
+
+
+def stream_jobs(syn, njobs, seed, ring_fraction, nmax, turns_max, grids, rate):
+    """Seeded tracking jobs drawn as the served-stream workload: lattice the
+    FODO cell (8 kicks per turn) or the 24-cell ring (16 kicks per cell,
+    384 per turn) with probability `ring_fraction`; macroparticles
+    log-uniform in [5e4, nmax]; grid uniform over `grids`; turns uniform in
+    [1, turns_max]; Gaussian bunch with sigma_x,y uniform in [0.5, 3] mm;
+    Poisson arrivals at `rate` jobs/s."""
+    import numpy as np
+    from helpers import fodo_cell, ring_cell
+    from synergia2_b200.serving import JobSpec, poisson_arrivals
+    g = np.random.Generator(np.random.Philox(seed))
+    arrivals = poisson_arrivals(njobs, rate, seed + 1)
+    jobs = []
+    for i in range(njobs):
+        ring = g.uniform() < ring_fraction
+        n = int(math.exp(g.uniform(math.log(5e4), math.log(nmax))))
+        grid = grids[int(g.integers(len(grids)))]
+        turns = int(g.integers(1, turns_max + 1))
+        sx, sy = g.uniform(0.5e-3, 3e-3, 2)
+        sig = (float(sx), 1e-4, float(sy), 1e-4, 0.3, 1e-4)
+        lattice = ring_cell() * 24 if ring else fodo_cell()
+        jobs.append(JobSpec(job_id=i, lattice=lattice, steps_per_turn=384 if ring else 8, n=n, grid=tuple(grid),
+                            turns=turns, sigmas=sig, seed=1000 + i, arrival=float(arrivals[i])))
+    return jobs
+
+
+def served_stream(syn, njobs, seed, ring_fraction=0.0, nmax=2e6, turns_max=10,
+                  grids=((32, 32, 64), (64, 64, 128)), rate=None, plain_every=1):
+    """Continuous-batching server (mixed precision, CUDA-graph turns,
+    admission by device-memory footprint) on a seeded job stream, and the
+    plain FP64 path on the same jobs one after another (every
+    `plain_every`-th job: a sample of the stream when the full sequential
+    run would be long).  Throughput = macroparticle-steps of finished jobs
+    / wall time."""
+    from synergia2_b200.serving import Server, summarize
+    if rate is None:
+        rate = 1e9
+    jobs = stream_jobs(syn, njobs, seed, ring_fraction, nmax, turns_max, grids, rate)
+    sample = jobs[::plain_every]
+    for j in sample:
+        j.arrival = 0.0
+    seq = Server(hbm_budget=1 << 40, max_active=1, precision=syn.precision_t.fp64, graphs=False)
+    res, wall = seq.run(sample, realtime=False)
+    plain = summarize(res, wall)
+    jobs = stream_jobs(syn, njobs, seed, ring_fraction, nmax, turns_max, grids, rate)
+    srv = Server(hbm_budget=100 << 30, max_active=64)
+    res, wall = srv.run(jobs, realtime=True)
+    served = summarize(res, wall)
+    return {"jobs": njobs, "ring_fraction": ring_fraction, "n_range": [5e4, nmax], "turns_max": turns_max,
+            "grids": [list(g) for g in grids], "arrival_rate_per_s": rate,
+            "served_throughput": served["throughput"], "unit": "macroparticle-steps/s",
+            "latency_p50_s": served["latency_p50_s"], "latency_p99_s": served["latency_p99_s"],
+            "wall_s": served["wall_s"], "macroparticle_steps": served["macroparticle_steps"],
+            "plain_fp64_sequential_throughput": plain["throughput"],
+            "plain_fp64_sample_jobs": len(sample),
+            "speedup_vs_plain_fp64": served["throughput"] / plain["throughput"]}
+
+
+def batched_scan(syn, torch, nbunches, passes, seed):
+    """Quad-strength scan: `nbunches` independent bunches (k1 uniform in
+    [0.4, 0.8], macroparticles log-uniform in [1e5, 4e6], grid drawn from
+    32^2x64, 64^2x128, 64^2x256), mixed precision, CUDA-graph turns, all
+    advanced together by one Batch; throughput over `passes` passes after
+    one warm-up pass."""
+    import numpy as np
+    from helpers import fodo_cell, product_lattice
+    g = np.random.Generator(np.random.Philox(seed))
+    grids = [(32, 32, 64), (64, 64, 128), (64, 64, 256)]
+    batch = syn.Batch()
+    keep = []
+    for i in range(nbunches):
+        k1 = float(g.uniform(0.4, 0.8))
+        n = int(math.exp(g.uniform(math.log(1e5), math.log(4e6))))
+        grid = grids[int(g.integers(3))]
+        lat, ref = product_lattice(fodo_cell(k1))
+        opts = syn.Space_charge_3d_open_hockney_options(*grid)
+        opts.precision = syn.precision_t.mixed
+        prop = syn.Propagator(lat, syn.Split_operator_stepper(opts, KICKS_PER_CELL))
+        prop.set_graphs(True)
+        b = syn.Bunch(ref, n, REAL_NUM)
+        b.populate_gaussian(SIGMAS, seed=10 + i)
+        keep.append((prop, b, batch.add(prop, b)))
+    batch.run({s: 1 for _, _, s in keep})
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch.run({s: passes for _, _, s in keep})
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    alive = sum(b.get_total_num() for _, b, _ in keep)
+    total = sum(b.size() for _, b, _ in keep)
+    return {"bunches": nbunches, "macroparticles": total, "passes": passes, "precision": "mixed",
+            "graphs": True, "value": alive * passes * KICKS_PER_CELL / dt, "unit": "macroparticle-steps/s",
+            "wall_s": dt}
+
+
 def algorithmic_bytes_per_step(n, grid, w=8):
     """Per step: one fused particle pass (6 FP64 columns in and out, mask +
     discards) and one deposit pass (x, y, cdt), plus each grid array moved
@@ -162,6 +327,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--particles", type=int, default=N_PART, help="bunch size (profiling cases only)")
+    ap.add_argument("--config", default="c1", choices=["c1", "c2", "c4"],
+                    help="c1: FODO 4M FP64 + mixed (default); c2: 64-bunch quad scan; c4: served job stream")
+    ap.add_argument("--extras", type=int, default=1, help="0: skip the mixed-precision and served legs of c1")
+    ap.add_argument("--jobs", type=int, default=48, help="c4: jobs in the served stream")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -175,6 +344,25 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    if args.config in ("c2", "c4"):
+        # single-GPU workloads: rank 0 alone runs them
+        import synergia2_b200 as syn
+        if rank == 0:
+            if args.config == "c2":
+                r = batched_scan(syn, torch, 64, 50, seed=7)
+                wl = ("quad-strength scan: 64 FODO bunches, k1 U[0.4,0.8], macroparticles log-uniform [1e5,4e6], "
+                      "grids {32^2x64, 64^2x128, 64^2x256}, 50 passes, mixed precision, CUDA-graph turns")
+            else:
+                r = served_stream(syn, args.jobs, seed=11, ring_fraction=0.5, nmax=8e6, turns_max=50,
+                                  grids=((32, 32, 64), (64, 64, 128), (128, 128, 256)), rate=4.0, plain_every=4)
+                wl = ("served stream: %d jobs (Poisson arrivals 4/s), FODO cell or 24-cell ring (p=0.5), "
+                      "macroparticles log-uniform [5e4,8e6], grids {32^2x64, 64^2x128, 128^2x256}, turns U[1,50]"
+                      % args.jobs)
+            v = r.get("value", r.get("served_throughput"))
+            print(json.dumps({"metric": "macroparticle-steps/s", "value": v, "unit": "macroparticle-steps/s",
+                              "n_gpus": 1, "higher_is_better": True, "dtype": "f64 particles / f32 grid",
+                              "data": "synthetic", "config": {"workload": wl}, "result": r}))
+        return
     dist = None
     if world > 1:
         import datetime
@@ -303,6 +491,9 @@ def main():
             "gpu_launches": gpu_launches,
             "clocks": clk,
         }
+        if args.extras and world == 1 and npart == N_PART:
+            out["mixed"] = mixed_vs_fp64(syn, torch, args.steps, args.warmup, passes=100)
+            out["served"] = served_stream(syn, 24, seed=3)
         if not args.no_cpu_baseline and world == 1 and npart == N_PART:
             out["cpu_baseline"] = cpu_baseline()
         print(json.dumps(out))
