@@ -318,6 +318,18 @@ def run_reference(args, rank):
                               "d2h_bytes_per_step": 0}}))
 
 
+def over_ranks(dist, torch, seconds, work, device):
+    """Whole-job timing over replicas: the slowest rank's time and the sum
+    of all ranks' work (macroparticle-steps)."""
+    if dist is None:
+        return seconds, work
+    t = torch.tensor([float(seconds)], device=device, dtype=torch.float64)
+    w = torch.tensor([float(work)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    return t.item(), w.item()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -415,14 +427,7 @@ def main():
         prof[nm.value.decode()] = (tot.value, cnt.value)
     n_alive = bunch.get_total_num()
 
-    t_max = ms
-    total_steps = n_alive * args.steps
-    if dist is not None:
-        t = torch.tensor([ms, float(total_steps)], device="cuda", dtype=torch.float64)
-        tm = t.clone()
-        dist.all_reduce(tm[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(tm[1:], op=dist.ReduceOp.SUM)
-        t_max, total_steps = tm[0].item(), tm[1].item()
+    t_max, total_steps = over_ranks(dist, torch, ms, n_alive * args.steps, "cuda")
     value = total_steps / (t_max * 1e-3)
 
     # end to end through the public API with host buffers: checkin from pinned
@@ -443,11 +448,7 @@ def main():
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e_total = bunch.get_total_num() * max(e2e_steps, 1)
-    if dist is not None:
-        t = torch.tensor([e2e_s, float(e2e_total)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        e2e_s, e2e_total = t[0].item(), t[1].item()
+    e2e_s, e2e_total = over_ranks(dist, torch, e2e_s, e2e_total, "cuda")
     bunch_bytes = npart * (7 * 8 + 1)
 
     if rank == 0:
