@@ -209,6 +209,13 @@ sb2_status sb2_batch_destroy(sb2_batch* q);
 sb2_status sb2_batch_add(sb2_batch* q, sb2_propagator* p, sb2_bunch* b, int32_t* slot);
 sb2_status sb2_batch_remove(sb2_batch* q, int32_t slot);
 sb2_status sb2_batch_run(sb2_batch* q, const int32_t* slots, const int32_t* turns, int32_t n);
+/* Asynchronous form for request loops: sb2_batch_launch enqueues `turns`
+ * turns of one slot on its stream and returns at once (one launch in
+ * flight per slot); sb2_batch_query sets *done to 1 once they have
+ * finished -- bunch counters updated, device errors reported as the
+ * status -- and to 0 while they run. */
+sb2_status sb2_batch_launch(sb2_batch* q, int32_t slot, int32_t turns);
+sb2_status sb2_batch_query(sb2_batch* q, int32_t slot, int32_t* done);
 
 /* ---------------------------------------------------------------------
  * Collective operator alone: Space_charge_3d_open_hockney::apply_bunch

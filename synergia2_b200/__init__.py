@@ -481,3 +481,13 @@ class Batch:
         slots = (ctypes.c_int32 * len(items))(*[k for k, _ in items])
         turns = (ctypes.c_int32 * len(items))(*[int(v) for _, v in items])
         check(lib().sb2_batch_run(self.h, slots, turns, len(items)))
+
+    def launch(self, slot, turns):
+        """Enqueue `turns` turns of one slot and return at once."""
+        check(lib().sb2_batch_launch(self.h, int(slot), int(turns)))
+
+    def query(self, slot):
+        """True once the slot's launched turns have finished."""
+        d = ctypes.c_int32()
+        check(lib().sb2_batch_query(self.h, int(slot), ctypes.byref(d)))
+        return bool(d.value)

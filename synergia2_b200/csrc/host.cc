@@ -55,6 +55,14 @@ static void cuda_check(cudaError_t e, const char* what)
     }
 }
 
+template <typename T>
+static T* dalloc(size_t count, const char* what)
+{
+    void* p = nullptr;
+    cuda_check(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)), what);
+    return (T*)p;
+}
+
 // ---------------------------------------------------------------------------
 // Reference particle (foundation/four_momentum.cc, reference_particle.cc)
 // ---------------------------------------------------------------------------
@@ -400,6 +408,7 @@ void sext_kick_cb(double x, double& xp, double y, double& yp, const double* k) {
 // ---------------------------------------------------------------------------
 struct Bunch {
     int device = 0;
+    // arrays the kernels work on: the home arrays, or the working copy
     double* parts = nullptr;
     int64_t stride = 0;
     uint8_t* masks = nullptr;
@@ -413,13 +422,100 @@ struct Bunch {
     bool design_set = false;
     int turns_done = 0;
 
+    // Home arrays: the ones the caller handed over or reads back, in the
+    // caller's particle order.
+    double* home_parts = nullptr;
+    int64_t home_stride = 0;
+    uint8_t* home_masks = nullptr;
+    uint8_t* home_discards = nullptr;
+    // Cell-ordered working copy used by space-charge propagation.  It
+    // outlives a propagate call, so consecutive calls keep the particles in
+    // (nearly) cell order; the home arrays are brought up to date by
+    // settle() before anything reads or writes them in the caller's order.
+    SortBuffers wc{};
+    bool permuted = false;    // current data is the working copy
+    int kicks_since_sort = 0; // kicks since the working copy was last sorted
+
+    void set_home()
+    {
+        home_parts = parts;
+        home_stride = stride;
+        home_masks = masks;
+        home_discards = discards;
+    }
+    void free_work()
+    {
+        cudaFree(wc.parts);
+        cudaFree(wc.masks);
+        cudaFree(wc.discards);
+        cudaFree(wc.perm);
+        cudaFree(wc.parts2);
+        cudaFree(wc.masks2);
+        cudaFree(wc.discards2);
+        cudaFree(wc.perm2);
+        wc = SortBuffers{};
+    }
+    // home -> working copy in the caller's order (identity permutation)
+    void enter_work(cudaStream_t s)
+    {
+        if (permuted) return;
+        if (!wc.parts) {
+            const int64_t cap = std::max<int64_t>(n, 1);
+            wc.n = n;
+            wc.stride = cap;
+            wc.parts = dalloc<double>((size_t)7 * cap, "working copy");
+            wc.parts2 = dalloc<double>((size_t)7 * cap, "working copy");
+            wc.masks = dalloc<uint8_t>(cap, "working copy");
+            wc.masks2 = dalloc<uint8_t>(cap, "working copy");
+            wc.discards = dalloc<uint8_t>(cap, "working copy");
+            wc.discards2 = dalloc<uint8_t>(cap, "working copy");
+            wc.perm = dalloc<int32_t>(cap, "working copy");
+            wc.perm2 = dalloc<int32_t>(cap, "working copy");
+        }
+        cuda_check(launch_sort_gather_in(home_parts, home_stride, home_masks, home_discards, wc, s), "sort gather");
+        parts = wc.parts;
+        stride = wc.stride;
+        masks = wc.masks;
+        discards = wc.discards;
+        permuted = true;
+        kicks_since_sort = 0;
+    }
+    // working copy -> home arrays, back in the caller's order
+    void settle(cudaStream_t s)
+    {
+        if (!permuted) return;
+        cuda_check(launch_sort_scatter_out(wc, home_parts, home_stride, home_masks, home_discards, s), "sort scatter");
+        drop_work();
+    }
+    // forget the working copy (the home arrays are about to be overwritten)
+    void drop_work()
+    {
+        permuted = false;
+        parts = home_parts;
+        stride = home_stride;
+        masks = home_masks;
+        discards = home_discards;
+    }
+    // the working copy after a sort (sort.cu writes into the second buffers)
+    void swap_work()
+    {
+        std::swap(wc.parts, wc.parts2);
+        std::swap(wc.masks, wc.masks2);
+        std::swap(wc.discards, wc.discards2);
+        std::swap(wc.perm, wc.perm2);
+        parts = wc.parts;
+        masks = wc.masks;
+        discards = wc.discards;
+    }
+
     ~Bunch()
     {
         if (owns) {
-            cudaFree(parts);
-            cudaFree(masks);
-            cudaFree(discards);
+            cudaFree(home_parts);
+            cudaFree(home_masks);
+            cudaFree(home_discards);
         }
+        free_work();
         cudaFree(counters);
     }
     void sync_counters(cudaStream_t s)
@@ -1127,14 +1223,6 @@ static int ilog2(int v)
     return l;
 }
 
-template <typename T>
-static T* dalloc(size_t count, const char* what)
-{
-    void* p = nullptr;
-    cuda_check(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)), what);
-    return (T*)p;
-}
-
 struct SpaceCharge {
     sb2_sc3d_options o;
     Dims d{};
@@ -1275,6 +1363,8 @@ struct SpaceCharge {
     {
         const bool refresh = !o.domain_fixed || !ghat_valid;
         sig_append(&refresh, sizeof(refresh));
+        const void* arrays[2] = {b.parts, b.masks};
+        sig_append(arrays, sizeof(arrays));
         if (g_sig.dry) {
             if (refresh) ghat_valid = true;
             return;
@@ -1420,6 +1510,9 @@ struct Engine {
     {
         if (with_domain && !sc->o.domain_fixed) ops.push_back(new_op(OP_MOMENTS));
         if (g_sig.sig) {
+            // a replayed graph reads the arrays it was captured with
+            const void* arrays[5] = {b.parts, b.masks, b.discards, b.counters, (const void*)(intptr_t)b.n};
+            sig_append(arrays, sizeof(arrays));
             uint64_t nops = ops.size();
             sig_append(&nops, sizeof(nops));
             if (nops) sig_append(ops.data(), sizeof(MapOp) * nops);
@@ -1506,9 +1599,7 @@ struct Propagator {
     // cell-ordered working copy of the bunch (space-charge runs only)
     bool cell_sort = true;
     int sort_interval = 4; // re-sort before every k-th space-charge kick (measured best of 1, 2, 4, 8 at 4M particles)
-    int kicks_since_sort = 0;
-    SortBuffers sb{};
-    int64_t sb_cap = -1;
+    int32_t* sort_scratch = nullptr; // histogram, offsets, cursors of the counting sort
 
     Propagator(const Lattice& l, int stepper_kind, int n, const sb2_sc3d_options* opts)
         : lat(l), stepper(stepper_kind), num(n)
@@ -1530,103 +1621,48 @@ struct Propagator {
         drop_graphs();
         if (own_stream) cudaStreamDestroy(own_stream);
         cudaFree(elem_charge);
-        free_sort();
-    }
-
-    void free_sort()
-    {
-        cudaFree(sb.parts);
-        cudaFree(sb.masks);
-        cudaFree(sb.discards);
-        cudaFree(sb.perm);
-        cudaFree(sb.parts2);
-        cudaFree(sb.masks2);
-        cudaFree(sb.discards2);
-        cudaFree(sb.perm2);
-        cudaFree(sb.scratch);
-        sb = SortBuffers{};
-        sb_cap = -1;
+        cudaFree(sort_scratch);
     }
 
     bool sorting(const Bunch& b) const { return has_sc && cell_sort && b.n >= 64; }
 
-    // Points the bunch at a cell-ordered working copy for the duration of
-    // a propagate call and restores (scatters back) at the end.
-    struct SortScope {
-        Propagator& P;
-        Bunch& b;
-        cudaStream_t s;
-        bool active = false;
-        double* u_parts;
-        int64_t u_stride;
-        uint8_t *u_masks, *u_discards;
-        SortScope(Propagator& p, Bunch& bb, cudaStream_t st) : P(p), b(bb), s(st)
-        {
-            u_parts = b.parts;
-            u_stride = b.stride;
-            u_masks = b.masks;
-            u_discards = b.discards;
-            if (!P.sorting(b)) return;
-            P.alloc_sort(b.n);
-            ProfScope ps(PROF_SORT, s);
-            cuda_check(launch_sort_gather_in(b.parts, b.stride, b.masks, b.discards, P.sb, s), "sort gather");
-            b.parts = P.sb.parts;
-            b.stride = P.sb.stride;
-            b.masks = P.sb.masks;
-            b.discards = P.sb.discards;
-            active = true;
-        }
-        void restore()
-        {
-            if (!active) return;
-            active = false;
-            b.parts = u_parts;
-            b.stride = u_stride;
-            b.masks = u_masks;
-            b.discards = u_discards;
-            ProfScope ps(PROF_SORT, s);
-            cuda_check(launch_sort_scatter_out(P.sb, u_parts, u_stride, u_masks, u_discards, s), "sort scatter");
-        }
-        ~SortScope()
-        {
-            try {
-                restore();
-            } catch (...) {
-            }
-        }
-    };
-
-    void alloc_sort(int64_t n)
+    // Start of a propagate call: space-charge runs work on the bunch's
+    // cell-ordered working copy (entered from the home arrays if the bunch
+    // is not already there).
+    void enter_sorted(Bunch& b, cudaStream_t s)
     {
-        const int64_t G = (int64_t)sc_opts.shape[0] * sc_opts.shape[1] * sc_opts.shape[2];
-        if (sb_cap == n && sb.scratch) return;
-        free_sort();
-        sb.n = n;
-        sb.stride = n;
-        sb.parts = dalloc<double>((size_t)7 * n, "sort copy");
-        sb.parts2 = dalloc<double>((size_t)7 * n, "sort copy");
-        sb.masks = dalloc<uint8_t>(n, "sort copy");
-        sb.masks2 = dalloc<uint8_t>(n, "sort copy");
-        sb.discards = dalloc<uint8_t>(n, "sort copy");
-        sb.discards2 = dalloc<uint8_t>(n, "sort copy");
-        sb.perm = dalloc<int32_t>(n, "sort copy");
-        sb.perm2 = dalloc<int32_t>(n, "sort copy");
-        sb.scratch = dalloc<int32_t>(sort_scratch_ints(G), "sort scratch");
-        sb_cap = n;
+        sort_active = false;
+        if (!sorting(b)) return;
+        if (!sort_scratch) {
+            const int64_t G = (int64_t)sc_opts.shape[0] * sc_opts.shape[1] * sc_opts.shape[2];
+            sort_scratch = dalloc<int32_t>(sort_scratch_ints(G), "sort scratch");
+        }
+        if (!b.permuted) {
+            ProfScope ps(PROF_SORT, s);
+            b.enter_work(s);
+        }
+        sort_active = true;
+    }
+    // End of a propagate call: a bunch over caller-owned arrays is brought
+    // back to them at once (the caller may read them directly); an owned
+    // bunch stays in the working copy until the caller next touches it.
+    void leave_sorted(Bunch& b, cudaStream_t s)
+    {
+        sort_active = false;
+        if (b.permuted && !b.owns) {
+            ProfScope ps(PROF_SORT, s);
+            b.settle(s);
+        }
     }
 
     // Re-sort the working copy by the cells of the current domain.
     void resort(Bunch& b, cudaStream_t s)
     {
-        ProfScope ps(PROF_SORT, s);
-        cuda_check(launch_cell_sort(sb, sc->state, sc->d.gx, sc->d.gy, sc->d.gz, s), "cell sort");
-        std::swap(sb.parts, sb.parts2);
-        std::swap(sb.masks, sb.masks2);
-        std::swap(sb.discards, sb.discards2);
-        std::swap(sb.perm, sb.perm2);
-        b.parts = sb.parts;
-        b.masks = sb.masks;
-        b.discards = sb.discards;
+        if (!g_sig.dry) {
+            ProfScope ps(PROF_SORT, s);
+            cuda_check(launch_cell_sort(b.wc, sort_scratch, sc->state, sc->d.gx, sc->d.gy, sc->d.gz, s), "cell sort");
+        }
+        b.swap_work();
     }
 
     void ensure_device()
@@ -1657,7 +1693,7 @@ struct Propagator {
                 engine_->add_operator(lat, st.indeps[ii++], b, sc.get(), elem_charge, s);
             } else if (sc) {
                 engine_->flush(b, sc.get(), elem_charge, true, time * 1.0, s);
-                if (sort_active && (kicks_since_sort++ % sort_interval) == 0) resort(b, s);
+                if (sort_active && (b.kicks_since_sort++ % sort_interval) == 0) resort(b, s);
                 sc->solve(b, s);
                 engine_->add_kick();
             }
@@ -1701,11 +1737,17 @@ struct Propagator {
         PassBook book;
         int nslots;
         bool ghat_valid;
+        // working-copy buffers swap at every sort
+        double* parts;
+        uint8_t* masks;
+        uint8_t* discards;
+        SortBuffers wc;
+        int kicks_since_sort;
     };
     HostSnap snap(const Bunch& b) const
     {
         HostSnap h{b.ref, b.design, b.design_set, b.turns_done, engine_->ops, engine_->book, engine_->nslots,
-                   sc ? sc->ghat_valid : false};
+                   sc ? sc->ghat_valid : false, b.parts, b.masks, b.discards, b.wc, b.kicks_since_sort};
         return h;
     }
     void restore(Bunch& b, const HostSnap& h)
@@ -1714,6 +1756,11 @@ struct Propagator {
         b.design = h.design;
         b.design_set = h.design_set;
         b.turns_done = h.turns_done;
+        b.parts = h.parts;
+        b.masks = h.masks;
+        b.discards = h.discards;
+        b.wc = h.wc;
+        b.kicks_since_sort = h.kicks_since_sort;
         engine_->ops = h.ops;
         engine_->book = h.book;
         engine_->nslots = h.nslots;
@@ -1791,6 +1838,7 @@ struct Propagator {
     {
         if (use_graphs) s = graph_stream(s);
         begin(b);
+        enter_sorted(b, s);
         for (int t = 0; t < turns; ++t) {
             if (use_graphs)
                 propagate_graph_turn(b, s);
@@ -1798,37 +1846,20 @@ struct Propagator {
                 run_turn(b, s);
         }
         engine_->flush(b, sc.get(), elem_charge, false, 0.0, s);
+        leave_sorted(b, s);
     }
 
     void propagate(Bunch& b, int turns, cudaStream_t s)
     { // Propagator::propagate propagator.cc:157-283 (one bunch, no diagnostics)
-        if (use_graphs) {
-            cudaStream_t gs = graph_stream(s);
-            propagate_async(b, turns, gs);
-            finish(b, gs);
-            return;
-        }
-        begin(b);
-        SortScope scope(*this, b, s);
-        sort_active = scope.active;
-        kicks_since_sort = 0;
-        for (int t = 0; t < turns; ++t) {
-            b.ref.start_repetition(); // do_start_repetition propagator.cc:25-34
-            for (auto const& st : steps) run_step(b, st, s);
-            b.turns_done += 1;
-        }
-        engine_->flush(b, sc.get(), elem_charge, false, 0.0, s);
-        scope.restore();
-        sort_active = false;
+        if (use_graphs) s = graph_stream(s);
+        propagate_async(b, turns, s);
         finish(b, s);
     }
 
     void propagate_steps(Bunch& b, int first, int count, cudaStream_t s)
     {
         begin(b);
-        SortScope scope(*this, b, s);
-        sort_active = scope.active;
-        kicks_since_sort = 0;
+        enter_sorted(b, s);
         const int ns = (int)steps.size();
         for (int k = first; k < first + count; ++k) {
             int si = ((k % ns) + ns) % ns;
@@ -1837,8 +1868,7 @@ struct Propagator {
             if (si == ns - 1) b.turns_done += 1;
         }
         engine_->flush(b, sc.get(), elem_charge, false, 0.0, s);
-        scope.restore();
-        sort_active = false;
+        leave_sorted(b, s);
         finish(b, s);
     }
 };
@@ -1869,13 +1899,48 @@ struct Batch {
         Propagator* p = nullptr;
         Bunch* b = nullptr;
         cudaStream_t s = nullptr;
+        cudaEvent_t done = nullptr; // recorded after the last launched turn
         bool used = false;
+        bool pending = false; // launched, not yet collected by query()
     };
     std::vector<Job> jobs;
     ~Batch()
     {
-        for (auto& j : jobs)
+        for (auto& j : jobs) {
             if (j.s) cudaStreamDestroy(j.s);
+            if (j.done) cudaEventDestroy(j.done);
+        }
+    }
+    Job& job(int slot)
+    {
+        if (slot < 0 || slot >= (int)jobs.size() || !jobs[slot].used) throw Error(SB2_ERR_INVALID, "bad batch slot");
+        return jobs[slot];
+    }
+    // Enqueue `turns` turns of one job on its stream and return at once.
+    void launch(int slot, int turns)
+    {
+        Job& j = job(slot);
+        if (j.pending) throw Error(SB2_ERR_INVALID, "batch slot already has turns in flight");
+        if (!j.done) cuda_check(cudaEventCreateWithFlags(&j.done, cudaEventDisableTiming), "event");
+        j.p->propagate_async(*j.b, turns, j.s);
+        cuda_check(cudaEventRecord(j.done, j.s), "event record");
+        j.pending = true;
+    }
+    // 1 when the job's launched turns have finished (their bookkeeping and
+    // error checks done), 0 while they run.
+    int query(int slot)
+    {
+        Job& j = job(slot);
+        if (!j.pending) return 1;
+        cudaError_t e = cudaEventQuery(j.done);
+        if (e == cudaErrorNotReady) {
+            cudaGetLastError();
+            return 0;
+        }
+        cuda_check(e, "batch job");
+        j.pending = false;
+        j.p->finish(*j.b, j.s);
+        return 1;
     }
     int add(Propagator* p, Bunch* b)
     {
@@ -1896,7 +1961,9 @@ struct Batch {
     }
     void remove(int slot)
     {
-        if (slot < 0 || slot >= (int)jobs.size() || !jobs[slot].used) throw Error(SB2_ERR_INVALID, "bad batch slot");
+        Job& j = job(slot);
+        if (j.pending) cuda_check(cudaStreamSynchronize(j.s), "batch remove");
+        j.pending = false;
         jobs[slot].used = false;
         jobs[slot].p = nullptr;
         jobs[slot].b = nullptr;
@@ -1908,7 +1975,7 @@ struct Batch {
         std::vector<int> launched;
         for (int k = 0; k < n; ++k) {
             int sl = slots[k];
-            if (sl < 0 || sl >= (int)jobs.size() || !jobs[sl].used) throw Error(SB2_ERR_INVALID, "bad batch slot");
+            if (job(sl).pending) throw Error(SB2_ERR_INVALID, "batch slot already has turns in flight");
             try {
                 jobs[sl].p->propagate_async(*jobs[sl].b, turns[k], jobs[sl].s);
                 launched.push_back(sl);
@@ -2102,6 +2169,7 @@ sb2_status sb2_bunch_create(int32_t charge, double mass, double value, int32_t k
     cuda_check(cudaMemset(b.parts, 0, sizeof(double) * 7 * cap), "memset");
     cuda_check(cudaMemset(b.masks, 1, cap), "memset");
     cuda_check(cudaMemset(b.discards, 0, cap), "memset");
+    b.set_home();
     if (n) { // ids 0..n-1 (bunch_particles.cc:283-300)
         std::vector<double> ids(n);
         for (int64_t i = 0; i < n; ++i) ids[i] = (double)i;
@@ -2128,6 +2196,7 @@ sb2_status sb2_bunch_wrap(int32_t charge, double mass, double value, int32_t kin
     b.masks = masks;
     b.discards = discards;
     b.owns = false;
+    b.set_home();
     bunch_alloc_counters(b, real_num);
     // count valid particles
     std::vector<uint8_t> m(n);
@@ -2152,6 +2221,7 @@ sb2_status sb2_bunch_set_particles(sb2_bunch* h, const double* host_parts, const
     SB2_TRY
     SB2_REQUIRE(h && host_parts, "null argument");
     Bunch& b = h->b;
+    b.settle(0);
     if (b.n == 0) return SB2_OK;
     cuda_check(cudaMemcpy2D(b.parts, sizeof(double) * b.stride, host_parts, sizeof(double) * b.n,
                             sizeof(double) * b.n, 7, cudaMemcpyHostToDevice),
@@ -2175,6 +2245,7 @@ sb2_status sb2_bunch_get_particles(sb2_bunch* h, double* host_parts, uint8_t* ho
     SB2_TRY
     SB2_REQUIRE(h, "null bunch");
     Bunch& b = h->b;
+    b.settle(0);
     if (b.n == 0) return SB2_OK;
     if (host_parts)
         cuda_check(cudaMemcpy2D(host_parts, sizeof(double) * b.n, b.parts, sizeof(double) * b.stride,
@@ -2194,6 +2265,8 @@ sb2_status sb2_bunch_device_arrays(sb2_bunch* h, double** parts, int64_t* stride
 {
     SB2_TRY
     SB2_REQUIRE(h, "null bunch");
+    h->b.settle(0);
+    cuda_check(cudaStreamSynchronize(0), "settle");
     if (parts) *parts = h->b.parts;
     if (stride) *stride = h->b.stride;
     if (masks) *masks = h->b.masks;
@@ -2229,6 +2302,7 @@ sb2_status sb2_bunch_populate_gaussian(sb2_bunch* h, const double sigma[6], uint
     SB2_TRY
     SB2_REQUIRE(h && sigma, "null argument");
     Bunch& b = h->b;
+    b.settle(0);
     if (b.n) cuda_check(launch_populate(b.parts, b.stride, b.masks, b.n, sigma, seed, 0), "populate");
     cuda_check(cudaDeviceSynchronize(), "populate");
     b.host_counters.n_valid = b.host_counters.n_total = (int32_t)b.n;
@@ -2243,6 +2317,7 @@ sb2_status sb2_bunch_moments(sb2_bunch* h, double mean[6], double mom2[36], doub
     SB2_TRY
     SB2_REQUIRE(h, "null bunch");
     Bunch& b = h->b;
+    b.settle(0);
     const int nb = track_grid_blocks();
     double* part = dalloc<double>((size_t)nb * 27, "moment partials");
     double* dmean = dalloc<double>(6, "mean");
@@ -2477,6 +2552,22 @@ sb2_status sb2_batch_run(sb2_batch* q, const int32_t* slots, const int32_t* turn
     SB2_CATCH
 }
 
+sb2_status sb2_batch_launch(sb2_batch* q, int32_t slot, int32_t turns)
+{
+    SB2_TRY
+    SB2_REQUIRE(q && turns >= 0, "bad argument");
+    q->q.launch(slot, turns);
+    SB2_CATCH
+}
+
+sb2_status sb2_batch_query(sb2_batch* q, int32_t slot, int32_t* done)
+{
+    SB2_TRY
+    SB2_REQUIRE(q && done, "bad argument");
+    *done = q->q.query(slot);
+    SB2_CATCH
+}
+
 sb2_status sb2_propagator_deposited_charge(sb2_propagator* p, int32_t index, double* charge)
 {
     SB2_TRY
@@ -2518,6 +2609,7 @@ sb2_status sb2_sc3d_apply(sb2_sc3d* sc, sb2_bunch* b, double time_step, void* st
 {
     SB2_TRY
     SB2_REQUIRE(sc && b, "null argument");
+    b->b.settle(as_stream(stream));
     sc->op->apply(b->b, time_step, as_stream(stream));
     b->b.sync_counters(as_stream(stream));
     SB2_CATCH
@@ -2536,6 +2628,7 @@ sb2_status sb2_libff_apply(const sb2_lattice* lattice, const double* slices, int
     SB2_TRY
     SB2_REQUIRE(lattice && hb && (slices || nslices == 0), "null argument");
     Bunch& b = hb->b;
+    b.settle(as_stream(stream));
     const Lattice& lat = lattice->l;
     if (!b.design_set) {
         b.design = lat.ref;
@@ -2561,6 +2654,7 @@ sb2_status sb2_aperture_apply(const sb2_lattice* lattice, int32_t index, const c
     SB2_REQUIRE(lattice && hb && aperture_type, "null argument");
     SB2_REQUIRE(index >= 0 && index < (int32_t)lattice->l.elements.size(), "element index out of range");
     Bunch& b = hb->b;
+    b.settle(as_stream(stream));
     Engine eng;
     Slice sl = whole_slice(lattice->l, index);
     MapOp m = op_aperture(lattice->l, aperture_type, sl);

@@ -68,7 +68,6 @@ struct SortBuffers {
     uint8_t* discards2;
     int32_t* perm2;
     int64_t n, stride;
-    int32_t* scratch; // sort_scratch_ints(G) ints
 };
 
 // track.cu
@@ -94,7 +93,8 @@ cudaError_t launch_convolve_f32(const double* rho, float2* S, const double* Ghat
 cudaError_t launch_efield_f32(const float* phi, float4* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s);
 // sort.cu
 size_t sort_scratch_ints(int64_t G);
-cudaError_t launch_cell_sort(const SortBuffers& sb, const ScState* sc, int gx, int gy, int gz, cudaStream_t s);
+cudaError_t launch_cell_sort(const SortBuffers& sb, int32_t* scratch, const ScState* sc, int gx, int gy, int gz,
+                             cudaStream_t s);
 cudaError_t launch_sort_gather_in(const double* ups, int64_t ustride, const uint8_t* um, const uint8_t* ud,
                                   const SortBuffers& sb, cudaStream_t s);
 cudaError_t launch_sort_scatter_out(const SortBuffers& sb, double* ups, int64_t ustride, uint8_t* um, uint8_t* ud,

@@ -11,8 +11,9 @@
 //   scan      exclusive prefix sum of the counts (three small kernels)
 //   scatter   every column, the mask, the discard flag and the original
 //             index move to offset[key] + rank
-// The caller's arrays are untouched until the call ends, when the working
-// copy is scattered back to the original order.  The order within a cell
+// The caller's arrays are untouched while the bunch lives in the working
+// copy; they are brought back up to date (the working copy scattered back to
+// the original order) when the caller next reads or writes them.  The order within a cell
 // depends on atomic arrival order; every per-particle result is independent
 // of it.
 #include <cuda_runtime.h>
@@ -223,11 +224,12 @@ size_t sort_scratch_ints(int64_t G)
     return (size_t)(3 * m + (m + kScanBlock - 1) / kScanBlock + 8);
 }
 
-cudaError_t launch_cell_sort(const SortBuffers& sb, const ScState* sc, int gx, int gy, int gz, cudaStream_t s)
+cudaError_t launch_cell_sort(const SortBuffers& sb, int32_t* scratch, const ScState* sc, int gx, int gy, int gz,
+                             cudaStream_t s)
 {
     const int64_t G = (int64_t)gx * gy * gz;
     const int m = (int)(G + 2);
-    int32_t* counts = sb.scratch;
+    int32_t* counts = scratch;
     int32_t* offsets = counts + m;
     int32_t* cursor = offsets + m;
     int32_t* bsums = cursor + m;

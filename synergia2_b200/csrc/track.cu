@@ -470,14 +470,17 @@ __global__ void __launch_bounds__(kTrackThreads, TrackOcc<VARIANT>::value)
     for (int64_t base = blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
         Part P[PPT];
         bool in[PPT];
+        // the mask and the six columns are loaded together (no load waits
+        // on the mask), so all seven requests of every particle are in
+        // flight at once; lost particles' values are read and ignored
+        uint8_t mk[PPT];
 #pragma unroll
         for (int q = 0; q < PPT; ++q) {
             const int64_t i = base + q * blockDim.x + threadIdx.x;
-            P[q].alive = (i < n) && p.masks[i] != 0;
-            in[q] = P[q].alive;
-            P[q].disc = 0;
+            mk[q] = 0;
             P[q].x = P[q].xp = P[q].y = P[q].yp = P[q].cdt = P[q].dpop = 0.0;
-            if (P[q].alive) {
+            if (i < n) {
+                mk[q] = p.masks[i];
                 P[q].x = p.parts[i];
                 P[q].xp = p.parts[i + S];
                 P[q].y = p.parts[i + 2 * S];
@@ -485,6 +488,12 @@ __global__ void __launch_bounds__(kTrackThreads, TrackOcc<VARIANT>::value)
                 P[q].cdt = p.parts[i + 4 * S];
                 P[q].dpop = p.parts[i + 5 * S];
             }
+        }
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+            P[q].alive = mk[q] != 0;
+            in[q] = P[q].alive;
+            P[q].disc = 0;
         }
         for (int o = 0; o < p.nops; ++o) {
             const MapOp& op = p.ops[o];
@@ -612,7 +621,12 @@ int track_grid_blocks()
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        nb = sms * 8;
+        // CTAs per SM of the grid-stride particle passes (SB2_TRACK_CTAS_PER_SM
+        // overrides, 1..12)
+        int per = 8;
+        const char* e = getenv("SB2_TRACK_CTAS_PER_SM");
+        if (e && atoi(e) >= 1 && atoi(e) <= 12) per = atoi(e);
+        nb = sms * per;
     }
     return nb;
 }

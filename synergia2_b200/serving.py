@@ -2,16 +2,16 @@
 
 Jobs (lattice, bunch, grid, turns) arrive over time.  The server admits
 queued jobs in arrival order while the device memory they need fits in its
-budget, keeps every admitted bunch and its space-charge workspace resident
-on the GPU, and advances all active jobs together: each scheduling
-iteration gives every job a quantum of turns sized so that jobs of unequal
-cost per turn advance by similar amounts of work, runs the quanta
-concurrently (one CUDA stream and one CUDA-graph turn per job), retires the
-jobs that finished and admits new arrivals.  Job latency is completion time
-minus arrival time.
+budget and keeps every admitted bunch and its space-charge workspace
+resident on the GPU.  Each admitted job runs on its own CUDA stream in
+quanta of turns (sized so that jobs of unequal cost per turn hold the GPU
+for similar amounts of work; one CUDA graph per turn): the loop launches a
+job's next quantum as soon as its previous one has finished, so the work of
+all active jobs overlaps on the device, and a finished job is retired and
+its memory handed to the next arrival without waiting for the others.  Job
+latency is completion time minus arrival time.
 """
-import heapq
-import math
+import dataclasses
 import time
 from dataclasses import dataclass, field
 
@@ -95,6 +95,7 @@ class Server:
         self.batch = Batch()
         self.active = {}   # slot -> (spec, propagator, bunch, turns_left, admitted)
         self.used = 0
+        self.max_inflight = 0  # most jobs with work on the device at once
 
     def _admit(self, spec, now):
         lat, ref = make_lattice(spec.lattice, spec.kinetic_energy)
@@ -119,47 +120,61 @@ class Server:
         self.used -= footprint_bytes(spec, self.precision)
         del prop, bunch
 
-    def run(self, jobs, realtime=True):
-        """Serve `jobs` (JobSpec with arrival offsets); returns (results,
-        wall seconds)."""
+    def run(self, jobs, realtime=True, poll_s=2e-4):
+        """Serve `jobs` (JobSpec with arrival offsets in seconds); returns
+        (results, wall seconds).  realtime=False ignores the arrival offsets
+        (every job is queued at time 0).  The clock is the wall clock from
+        the start of the call, so admission (allocation, bunch population)
+        is part of every job's latency and of the wall time."""
+        if not realtime:
+            jobs = [dataclasses.replace(j, arrival=0.0) for j in jobs]
         queue = sorted(jobs, key=lambda j: (j.arrival, j.job_id))
         results = []
         t0 = time.perf_counter()
-        clock = (lambda: time.perf_counter() - t0) if realtime else None
-        vnow = 0.0
+
+        def clock():
+            return time.perf_counter() - t0
+
+        def arrival(spec):
+            return spec.arrival
+
+        inflight = {}  # slot -> turns launched
         qi = 0
         while qi < len(queue) or self.active:
-            now = clock() if realtime else vnow
-            # admission in arrival order, by memory footprint
-            while qi < len(queue) and queue[qi].arrival <= now and len(self.active) < self.max_active:
+            now = clock()
+            # admission in arrival order while slots and device memory allow
+            while qi < len(queue) and arrival(queue[qi]) <= now and len(self.active) < self.max_active:
                 need = footprint_bytes(queue[qi], self.precision)
                 if self.active and self.used + need > self.budget:
                     break
                 self._admit(queue[qi], now)
                 qi += 1
-            if not self.active:
-                if qi < len(queue):
-                    wait = queue[qi].arrival - now
-                    if realtime and wait > 0:
-                        time.sleep(min(wait, 0.5))
-                    elif not realtime:
-                        vnow = queue[qi].arrival
-                continue
-            quanta = {}
+            # every admitted job that is not running gets its next quantum
             for slot, (spec, _, _, left, _) in self.active.items():
+                if slot in inflight or left <= 0:
+                    continue
                 per_turn = spec.n * spec.steps_per_turn
-                quanta[slot] = max(1, min(left, int(self.quantum_work // max(per_turn, 1))))
-            it0 = time.perf_counter()
-            self.batch.run(quanta)
-            if not realtime:
-                vnow += time.perf_counter() - it0
-            now = clock() if realtime else vnow
-            for slot, q in quanta.items():
-                self.active[slot][3] -= q
-            for slot in [s for s, a in self.active.items() if a[3] <= 0]:
-                self._retire(slot, now, results)
-        wall = (clock() if realtime else vnow)
-        return results, wall
+                q = max(1, min(left, int(self.quantum_work // max(per_turn, 1))))
+                self.batch.launch(slot, q)
+                inflight[slot] = q
+            self.max_inflight = max(self.max_inflight, len(inflight))
+            # collect finished quanta; retire finished jobs at once
+            progressed = False
+            for slot in list(inflight):
+                if self.batch.query(slot):
+                    q = inflight.pop(slot)
+                    self.active[slot][3] -= q
+                    progressed = True
+                    if self.active[slot][3] <= 0:
+                        self._retire(slot, clock(), results)
+            if not progressed:
+                if not self.active and qi < len(queue):
+                    wait = arrival(queue[qi]) - clock()
+                    if wait > 0:
+                        time.sleep(min(wait, 0.05))
+                else:
+                    time.sleep(poll_s)
+        return results, clock()
 
 
 def poisson_arrivals(n, rate, seed):

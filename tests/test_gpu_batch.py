@@ -87,7 +87,9 @@ def test_served_results_same_alone_and_in_mix(syn):
     from synergia2_b200.serving import Server, summarize
     jobs = _stream(syn)
     alone, _ = Server(hbm_budget=8 << 30, max_active=1, keep_particles=True).run(jobs, realtime=False)
-    mixed_res, wall = Server(hbm_budget=8 << 30, max_active=16, keep_particles=True).run(jobs, realtime=True)
+    srv = Server(hbm_budget=8 << 30, max_active=16, keep_particles=True)
+    mixed_res, wall = srv.run(jobs, realtime=True)
+    assert srv.max_inflight >= 2  # jobs overlapped on the device
     a = {r.job_id: r for r in alone}
     m = {r.job_id: r for r in mixed_res}
     assert set(a) == set(m) == {j.job_id for j in jobs}
@@ -116,3 +118,36 @@ def test_admission_respects_memory_budget(syn):
     srv._admit = admit
     res, _ = srv.run(jobs, realtime=False)
     assert len(res) == len(jobs) and peak[0] <= budget
+
+
+def test_batch_launch_query_matches_run(syn, monkeypatch):
+    """The asynchronous form (launch, then poll) gives the same particles as
+    the blocking batch run, and a slot refuses a second launch while its
+    turns are in flight."""
+    monkeypatch.setenv("SB2_CELL_SORT", "0")
+    specs = [(0.5, 40000, (16, 16, 32), 11), (0.7, 70000, (32, 32, 64), 12)]
+    ref = []
+    b0 = syn.Batch()
+    keep0 = []
+    for k1, n, shape, seed in specs:
+        prop, b = _job(syn, k1, n, shape, seed, syn.precision_t.fp64, True)
+        keep0.append((prop, b, b0.add(prop, b)))
+    b0.run({slot: 2 for _, _, slot in keep0})
+    ref = [b.get_particles()[0] for _, b, _ in keep0]
+    batch = syn.Batch()
+    keep = []
+    for k1, n, shape, seed in specs:
+        prop, b = _job(syn, k1, n, shape, seed, syn.precision_t.fp64, True)
+        keep.append((prop, b, batch.add(prop, b)))
+    for _, _, slot in keep:
+        batch.launch(slot, 2)
+    with pytest.raises(syn.SB2Error, match="in flight"):
+        batch.launch(keep[0][2], 1)
+    pending = {slot for _, _, slot in keep}
+    while pending:
+        pending = {s for s in pending if not batch.query(s)}
+    for (prop, b, slot), r in zip(keep, ref):
+        p = b.get_particles()[0]
+        assert np.array_equal(p[:, 6], r[:, 6])
+        for j in range(6):
+            assert rel_l2(p[:, j], r[:, j]) <= 1e-10, (slot, j)
