@@ -3,8 +3,9 @@
     python -m synergia2_b200.build          # or: python synergia2_b200/build.py
 
 CUDA units are compiled with --fmad=false (the FP64 path keeps IEEE
-rounding of every multiply and add, as the reference does); the host
-runtime with -ffp-contract=off for the same reason.  The CUDA runtime is
+rounding of every multiply and add, as the reference does), except
+track_fast.cu, the mixed-precision path's particle passes, which fuses
+multiply-adds; the host runtime with -ffp-contract=off.  The CUDA runtime is
 linked statically so the library loads without a CUDA toolkit on the
 loader path.
 """
@@ -20,7 +21,8 @@ OUT = os.path.join(HERE, "libsb2.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["track.cu", "sc3d.cu", "sort.cu", "noalloc.cu"]
+CU_SOURCES = ["track.cu", "track_fast.cu", "sc3d.cu", "sort.cu", "noalloc.cu"]
+FMAD = {"track_fast.cu": "--fmad=true"}
 CXX_SOURCES = ["host.cc"]
 
 
@@ -48,7 +50,7 @@ def newer(src_list, target):
 
 def build(verbose=False, force=False):
     os.makedirs(BUILD, exist_ok=True)
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(INCLUDE, "sb2.h"))
     objs = []
     nv = nvcc()
@@ -57,7 +59,7 @@ def build(verbose=False, force=False):
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if force or newer([s] + headers, o):
-            out = run([nv, *ARCH, "-lineinfo", "-O3", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC",
+            out = run([nv, *ARCH, "-lineinfo", "-O3", "-std=c++17", FMAD.get(src, "--fmad=false"), "-Xcompiler", "-fPIC",
                        "-Xptxas", "-v", "-I" + CSRC, "-c", "-o", o, s])
             if verbose:
                 sys.stdout.write(out)

@@ -1552,6 +1552,7 @@ struct Engine {
                 tp.sc = sc->state;
                 tp.efield = sc->E;
                 tp.efield32 = sc->E32;
+                tp.fast_maps = sc->mixed ? 1 : 0;
                 tp.gx = sc->d.gx;
                 tp.gy = sc->d.gy;
                 tp.gz = sc->d.gz;

@@ -27,6 +27,7 @@ struct TrackParams {
     int32_t nops;
     int32_t write_discards;
     int32_t slot_base;          // aperture slots of this launch: slot_base + [0, kMaxOpsPerPass)
+    int32_t fast_maps;          // 1: FMA-contracted maps of the mixed-precision path (track_fast.cu)
     MapOp ops[kMaxOpsPerPass];
 };
 

@@ -638,7 +638,10 @@ __global__ void __launch_bounds__(kFftThreads) fft_xi_kernel(const C* __restrict
 
 // Ghat passes on the real octant (ox, oy, oz) = (nx/2+1, ny/2+1, nz/2+1):
 // axis 0/1/2 transforms even real lines rebuilt by mirroring; real part of
-// the first L/2+1 outputs stored back in place.
+// the first L/2+1 outputs stored back in place.  The transform of a real
+// even line is real, so two lines ride in one complex FFT (line 2q as the
+// real part, line 2q+1 as the imaginary part) and come out as its real and
+// imaginary parts.
 __global__ void __launch_bounds__(kFftThreads) fft_green_kernel(double* G, const double2* __restrict__ tw,
                                                                 int axis, int L, int ox, int oy, int oz,
                                                                 const ScState* __restrict__ scp)
@@ -646,14 +649,15 @@ __global__ void __launch_bounds__(kFftThreads) fft_green_kernel(double* G, const
     extern __shared__ __align__(16) unsigned char sm_raw[];
     double2* sm = (double2*)sm_raw;
     if (!scp->valid) return;
-    const int nl = kFftTile / L;
+    const int nl = kFftTile / L; // complex lines (line pairs) per CTA
     const int half = L / 2;
     int64_t nlines, sj;
     if (axis == 0) { nlines = (int64_t)oy * oz; sj = 1; }
     else if (axis == 1) { nlines = (int64_t)ox * oz; sj = ox; }
     else { nlines = (int64_t)ox * oy; sj = (int64_t)ox * oy; }
+    const int64_t npairs = (nlines + 1) / 2;
     const int64_t l0 = (int64_t)blockIdx.x * nl;
-    const int nlt = (int)min((int64_t)nl, nlines - l0);
+    const int nlt = (int)min((int64_t)nl, npairs - l0);
     if (nlt <= 0) return;
     double2* b0 = sm;
     double2* b1 = sm + kFftTile;
@@ -666,8 +670,11 @@ __global__ void __launch_bounds__(kFftThreads) fft_green_kernel(double* G, const
         int li, j;
         if (axis == 0) { li = idx / L; j = idx - li * L; }
         else { j = idx / nlt; li = idx - j * nlt; }
-        int m = j <= half ? j : L - j;
-        b0[(j) * nlt + li] = make_double2(G[line_base(l0 + li) + m * sj], 0.0);
+        const int m = j <= half ? j : L - j;
+        const int64_t la = 2 * (l0 + li), lb = la + 1;
+        const double va = G[line_base(la) + m * sj];
+        const double vb = lb < nlines ? G[line_base(lb) + m * sj] : 0.0;
+        b0[j * nlt + li] = make_double2(va, vb);
     }
     __syncthreads();
     double2* r = smem_fft(b0, b1, nlt, L, tw, false);
@@ -675,7 +682,10 @@ __global__ void __launch_bounds__(kFftThreads) fft_green_kernel(double* G, const
         int li, k;
         if (axis == 0) { li = idx / (half + 1); k = idx - li * (half + 1); }
         else { k = idx / nlt; li = idx - k * nlt; }
-        G[line_base(l0 + li) + k * sj] = r[(k) * nlt + li].x;
+        const int64_t la = 2 * (l0 + li), lb = la + 1;
+        const double2 v = r[k * nlt + li];
+        G[line_base(la) + k * sj] = v.x;
+        if (lb < nlines) G[line_base(lb) + k * sj] = v.y;
     }
 }
 
@@ -781,9 +791,13 @@ cudaError_t launch_green(const ScState* sc, double* G, const Dims& d, int linear
     const int ox = d.nx / 2 + 1, oy = d.ny / 2 + 1, oz = d.nz / 2 + 1;
     green_octant_kernel<<<sm_count() * 4, 256, 0, s>>>(sc, G, d.gx, d.gy, d.gz, linear);
     const size_t sh = kFftSmemBytes;
-    fft_green_kernel<<<ceil_div64((int64_t)oy * oz, kFftTile / d.nx), kFftThreads, sh, s>>>(G, tw_x, 0, d.nx, ox, oy, oz, sc);
-    fft_green_kernel<<<ceil_div64((int64_t)ox * oz, kFftTile / d.ny), kFftThreads, sh, s>>>(G, tw_y, 1, d.ny, ox, oy, oz, sc);
-    fft_green_kernel<<<ceil_div64((int64_t)ox * oy, kFftTile / d.nz), kFftThreads, sh, s>>>(G, tw_z, 2, d.nz, ox, oy, oz, sc);
+    // one CTA per kFftTile / L line pairs
+    fft_green_kernel<<<ceil_div64(((int64_t)oy * oz + 1) / 2, kFftTile / d.nx), kFftThreads, sh, s>>>(
+        G, tw_x, 0, d.nx, ox, oy, oz, sc);
+    fft_green_kernel<<<ceil_div64(((int64_t)ox * oz + 1) / 2, kFftTile / d.ny), kFftThreads, sh, s>>>(
+        G, tw_y, 1, d.ny, ox, oy, oz, sc);
+    fft_green_kernel<<<ceil_div64(((int64_t)ox * oy + 1) / 2, kFftTile / d.nz), kFftThreads, sh, s>>>(
+        G, tw_z, 2, d.nz, ox, oy, oz, sc);
     return cudaGetLastError();
 }
 

@@ -1,0 +1,11 @@
+// FP64 particle passes with fused multiply-adds and the folded drift
+// (mixed-precision path); see track_impl.cuh.
+#define SB2_FAST_MAPS 1
+#define SB2_TRACK_NS fast
+#include "track_impl.cuh"
+
+namespace sb2 {
+
+cudaError_t launch_track_fast(const TrackParams& p, cudaStream_t s) { return fast::launch_pass(p, s); }
+
+} // namespace sb2

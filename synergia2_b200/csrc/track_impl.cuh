@@ -1,0 +1,631 @@
+// Particle-pass kernels for sm_100a, compiled twice from this file:
+//
+//   track.cu       SB2_FAST_MAPS 0, namespace sb2::exact, --fmad=false: every
+//                  a*b+c keeps two IEEE roundings and sqrt/div are
+//                  IEEE-correct, so the maps reproduce the reference's FP64
+//                  arithmetic (libFF/ff_algorithm.h) operation for operation
+//                  (the plain FP64 drop-in);
+//   track_fast.cu  SB2_FAST_MAPS 1, namespace sb2::fast, --fmad=true: the
+//                  same FP64 maps with fused multiply-adds, the exact drift's
+//                  two square roots and two divisions folded into one
+//                  reciprocal square root (cdt advances by L (1+dpop) / p_z
+//                  / beta, algebraically the same quantity) and the particle's
+//                  1/beta hoisted out of the Yoshida sub-steps; used by the
+//                  mixed-precision path, whose tolerances are set against the
+//                  FP64 path and are far above these last-bit differences.
+//
+// One launch runs a whole sequence of particle-local operations (element
+// slice maps, apertures, the space-charge kick, the spatial-moment sums) on
+// each particle while its six coordinates stay in registers: the column-major
+// N x 7 FP64 array is read once and written once per pass, coalesced (one
+// particle per thread, 32 consecutive particles per warp per column).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdlib>
+
+#include "sb2_kernels.h"
+
+#ifndef SB2_FAST_MAPS
+#error "define SB2_FAST_MAPS (0 or 1) and SB2_TRACK_NS before including track_impl.cuh"
+#endif
+
+namespace sb2 {
+namespace SB2_TRACK_NS {
+
+constexpr double kC = 299792458.0;
+
+// ---------------------------------------------------------------------------
+// ff_algorithm.h units, same operation order as the reference
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void drift_unit(double& x, double xp, double& y, double yp, double& cdt,
+                                           double dpop, double length, double reference_momentum,
+                                           double m, double reference_cdt)
+{ // ff_algorithm.h:47-79
+    const double uni = 1.0;
+    const double sig = (double)((0.0 < length) - (length < 0.0));
+    double dp = dpop + uni;
+    double inv_npz = uni / sqrt(dp * dp - xp * xp - yp * yp);
+    double lxpr = xp * length * inv_npz;
+    double lypr = yp * length * inv_npz;
+    double D2 = lxpr * lxpr + length * length + lypr * lypr;
+    double p = dp * reference_momentum;
+    double E2 = p * p + m * m;
+    double ibeta2 = E2 / (p * p);
+    x = x + lxpr;
+    y = y + lypr;
+    cdt = cdt + sig * sqrt(D2 * ibeta2) - reference_cdt;
+}
+
+#if SB2_FAST_MAPS
+// 1/beta of a particle of relative momentum dp = 1 + dpop: sqrt(1 + m^2 /
+// (dp pref)^2); constant while dpop is (through every map of a pass but the
+// space-charge kick).
+__device__ __forceinline__ double inv_beta(double dp, double pref, double m)
+{
+    const double r = m / (dp * pref);
+    return sqrt(1.0 + r * r);
+}
+
+// drift_unit with the path length folded: with p_z = sqrt(dp^2 - xp^2 -
+// yp^2), the exact drift's sqrt(D2 / beta^2) is |L| dp / p_z / beta, so the
+// whole drift costs one reciprocal square root.
+__device__ __forceinline__ void drift_unit_ib(double& x, double xp, double& y, double yp, double& cdt, double dp,
+                                              double length, double ib, double reference_cdt)
+{
+    const double inv_npz = rsqrt(dp * dp - xp * xp - yp * yp);
+    const double lz = length * inv_npz;
+    x = x + xp * lz;
+    y = y + yp * lz;
+    cdt = cdt + lz * dp * ib - reference_cdt;
+}
+#endif
+
+__device__ __forceinline__ void thin_quadrupole_unit(double x, double& xp, double y, double& yp,
+                                                     double k0, double k1)
+{ // ff_algorithm.h:929-936
+    xp = xp - k0 * x + k1 * y;
+    yp = yp + k0 * y + k1 * x;
+}
+
+__device__ __forceinline__ void thin_sextupole_unit(double x, double& xp, double y, double& yp,
+                                                    double k0, double k1)
+{ // ff_algorithm.h:940-947
+    xp = xp - 0.5 * k0 * (x * x - y * y) + k1 * x * y;
+    yp = yp + k0 * x * y + 0.5 * k1 * (x * x - y * y);
+}
+
+__device__ __forceinline__ void thin_octupole_unit(double x, double& xp, double y, double& yp,
+                                                   double k0, double k1)
+{ // ff_algorithm.h:951-963
+    const double n1 = 0.5, n2 = 1.0 / 3.0;
+    xp = xp - n1 * k0 * (x * x * x * n2 - x * y * y) + n1 * k1 * (x * x * y - y * y * y * n2);
+    yp = yp - n1 * k0 * (y * y * y * n2 - x * x * y) + n1 * k1 * (x * x * x * n2 - x * y * y);
+}
+
+__device__ __forceinline__ double factorial_d(int n)
+{ // ff_algorithm.h:1108-1117
+    if (n == 0) return 1.0;
+    double r = 1;
+    for (int i = 1; i <= n; ++i) r *= i;
+    return r;
+}
+
+__device__ __forceinline__ double qpow_d(double x, int i)
+{ // utils/kokkos_types.h:89-95
+    double r = 1;
+    while (i--) r = r * x;
+    return r;
+}
+
+__device__ __noinline__ void thin_magnet_unit(double x, double& xp, double y, double& yp, double kl0, double kl1,
+                                              int n)
+{ // ff_algorithm.h:1122-1168
+    for (int k = 0; k < n; k += 4)
+        xp = xp - (kl0 * (n - k)) * qpow_d(x, n - k - 1) * qpow_d(y, k) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 2; k < n; k += 4)
+        xp = xp + (kl0 * (n - k)) * qpow_d(x, n - k - 1) * qpow_d(y, k) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 1; k < n; k += 4)
+        xp = xp + (kl1 * (n - k)) * qpow_d(x, n - k - 1) * qpow_d(y, k) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 3; k < n; k += 4)
+        xp = xp - (kl1 * (n - k)) * qpow_d(x, n - k - 1) * qpow_d(y, k) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 4; k <= n; k += 4)
+        yp = yp - (kl0 * k) * qpow_d(x, n - k) * qpow_d(y, k - 1) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 2; k <= n; k += 4)
+        yp = yp + (kl0 * k) * qpow_d(x, n - k) * qpow_d(y, k - 1) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 1; k <= n; k += 4)
+        yp = yp + (kl1 * k) * qpow_d(x, n - k) * qpow_d(y, k - 1) / (factorial_d(n - k) * factorial_d(k));
+    for (int k = 3; k <= n; k += 4)
+        yp = yp - (kl1 * k) * qpow_d(x, n - k) * qpow_d(y, k - 1) / (factorial_d(n - k) * factorial_d(k));
+}
+
+// cf_kick ff_quadrupole.h:22-35
+__device__ __noinline__ void quad_cf_kick(double x, double& xp, double y, double& yp, const double* kL)
+{
+    thin_quadrupole_unit(x, xp, y, yp, kL[0], kL[1]);
+    if (kL[2] || kL[3]) thin_quadrupole_unit(x, xp, y, yp, kL[2], kL[3]);
+    if (kL[4] || kL[5]) thin_sextupole_unit(x, xp, y, yp, kL[4], kL[5]);
+    if (kL[6] || kL[7]) thin_octupole_unit(x, xp, y, yp, kL[6], kL[7]);
+    if (kL[8] || kL[9]) thin_magnet_unit(x, xp, y, yp, kL[8], kL[9], 5);
+    if (kL[10] || kL[11]) thin_magnet_unit(x, xp, y, yp, kL[10], kL[11], 6);
+    if (kL[12] || kL[13]) thin_magnet_unit(x, xp, y, yp, kL[12], kL[13], 7);
+    if (kL[14] || kL[15]) thin_magnet_unit(x, xp, y, yp, kL[14], kL[15], 8);
+}
+
+// slot_unit ff_algorithm.h:83-129
+__device__ __forceinline__ void slot_unit(double& x, double& xp, double& y, double& yp, double& cdt,
+                                          double& dpop, double ct, double st, double pref, double m)
+{
+    const double uni = 1.0;
+    double zp = sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
+    double p = (dpop + uni) * pref;
+    double e = sqrt(p * p + m * m);
+    double b0 = xp * pref / e;
+    double b1 = yp * pref / e;
+    double b2 = zp * pref / e;
+    double bp = st * b0 + ct * b2;
+    double tau = -x * st / bp;
+    double r0 = x + tau * b0;
+    double r1 = y + tau * b1;
+    double r2 = tau * b2;
+    x = r0 * ct - r2 * st;
+    y = r1;
+    cdt = cdt + tau;
+    xp = xp * ct - zp * st;
+}
+
+// bend_unit ff_algorithm.h:255-343
+__device__ __forceinline__ void bend_unit(double& x, double& xp, double& y, double& yp, double& cdt,
+                                          double dpop, double theta, double strength, double p_ref,
+                                          double m, double cdt_ref, double phase_r, double phase_i,
+                                          double term_r, double term_i)
+{
+    const double uni = 1.0;
+    const double tc = kC;
+    double p0 = p_ref;
+    double p = p_ref * (dpop + uni);
+    double E0 = sqrt(p0 * p0 + m * m);
+    double E = sqrt(p * p + m * m);
+    double igamma = m / E0;
+    double ibeta = uni / sqrt(uni - igamma * igamma);
+    double csq = kC * kC * 1e-9;
+    double psq = (dpop + uni) * (dpop + uni);
+    double Ef = uni / sqrt(psq + igamma * igamma * ibeta * ibeta);
+    double beta1 = Ef * xp;
+    double beta2 = Ef * yp;
+    double beta3 = Ef * sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
+    double ui_r = 0.0, ui_i = x;
+    double vui_r = tc * beta3, vui_i = tc * beta1;
+    double iomega = E / (csq * strength);
+    double bi_r = -vui_i * iomega - ui_r;
+    double bi_i = vui_r * iomega - ui_i;
+    double bf_r = bi_r * phase_r - bi_i * phase_i + term_r;
+    double bf_i = bi_r * phase_i + bi_i * phase_r + term_i;
+    double rho = tc * sqrt(beta1 * beta1 + beta3 * beta3) * iomega;
+    double dthmphi = asin(bi_r / rho) - asin(bf_r / rho);
+#if SB2_FAST_MAPS
+    double expf_r, expf_i;
+    sincos(dthmphi, &expf_i, &expf_r);
+#else
+    double expf_r = cos(dthmphi);
+    double expf_i = sin(dthmphi);
+#endif
+    double vuf_i = vui_r * expf_i + vui_i * expf_r;
+    double uf_i = (ui_r + bi_r) * expf_i + (ui_i + bi_i) * expf_r - bf_i;
+    double dtheta = dthmphi + theta;
+    double ncdt = -tc * dtheta * iomega;
+    x = uf_i;
+    xp = vuf_i / (Ef * tc);
+    y = y + beta2 * ncdt;
+    cdt = cdt + ncdt - cdt_ref;
+}
+
+// PropSbendSimd ff_sbend.h:127-215 for one particle (out of line: rare op)
+__device__ __noinline__ void sbend_op(double& x, double& xp, double& y, double& yp, double& cdt, double& dpop,
+                                      const double* d, int flags)
+{
+    if (flags & 1) {
+        slot_unit(x, xp, y, yp, cdt, dpop, d[0], d[1], d[14], d[15]);
+        yp = yp - d[4] * y; // edge_unit ff_algorithm.h:139-148
+        xp = xp + d[5] * y;
+    }
+    bend_unit(x, xp, y, yp, cdt, dpop, d[8], d[13], d[14], d[15], d[16], d[9], d[10], d[11], d[12]);
+    if (flags & 2) {
+        yp = yp - d[6] * y;
+        xp = xp + d[7] * y;
+        slot_unit(x, xp, y, yp, cdt, dpop, d[2], d[3], d[14], d[15]);
+    }
+}
+
+// yoshida6 ff_algorithm.h:1834-2008 with the drift lengths c_i*step_length,
+// the 0.1*step_ref_cdt substep and the d_i-scaled strengths precomputed on
+// the host (identical doubles).  kind selects the kick function.
+template <int KIND>
+__device__ __forceinline__ void yoshida6_op(double& x, double& xp, double& y, double& yp, double& cdt,
+                                            double dpop, const MapOp& op)
+{
+    const double pref = op.d[2], m = op.d[3], sub = op.d[4];
+    const double l1 = op.d[5], l2 = op.d[6], l3 = op.d[7], l4 = op.d[8];
+    const double* k = op.d + 9;
+    constexpr int KS = (KIND == OP_QUAD_CF) ? 16 : 2; // stride between k1..k4
+    auto kick = [&](const double* kk) {
+        if (KIND == OP_QUAD)
+            thin_quadrupole_unit(x, xp, y, yp, kk[0], kk[1]);
+        else if (KIND == OP_SEXT_YOSHIDA)
+            thin_sextupole_unit(x, xp, y, yp, kk[0], kk[1]);
+        else
+            quad_cf_kick(x, xp, y, yp, kk);
+    };
+    const double* k1 = k;
+    const double* k2 = k + KS;
+    const double* k3 = k + 2 * KS;
+    const double* k4 = k + 3 * KS;
+#if SB2_FAST_MAPS
+    const double dp = dpop + 1.0;
+    const double ib = inv_beta(dp, pref, m);
+    auto drift_unit = [&](double& x_, double xp_, double& y_, double yp_, double& cdt_, double, double len, double,
+                          double, double sub_) { drift_unit_ib(x_, xp_, y_, yp_, cdt_, dp, len, ib, sub_); };
+#endif
+    for (int i = 0; i < op.steps; ++i) {
+        drift_unit(x, xp, y, yp, cdt, dpop, l1, pref, m, sub); kick(k1);
+        drift_unit(x, xp, y, yp, cdt, dpop, l2, pref, m, sub); kick(k2);
+        drift_unit(x, xp, y, yp, cdt, dpop, l2, pref, m, sub); kick(k1);
+        drift_unit(x, xp, y, yp, cdt, dpop, l3, pref, m, sub); kick(k3);
+        drift_unit(x, xp, y, yp, cdt, dpop, l4, pref, m, sub); kick(k4);
+        drift_unit(x, xp, y, yp, cdt, dpop, l4, pref, m, sub); kick(k3);
+        drift_unit(x, xp, y, yp, cdt, dpop, l3, pref, m, sub); kick(k1);
+        drift_unit(x, xp, y, yp, cdt, dpop, l2, pref, m, sub); kick(k2);
+        drift_unit(x, xp, y, yp, cdt, dpop, l2, pref, m, sub); kick(k1);
+        drift_unit(x, xp, y, yp, cdt, dpop, l1, pref, m, sub);
+    }
+}
+
+// collective/utils.h:9-18
+__device__ __forceinline__ void leftmost(double pos, double left, double inv, int& idx, double& off)
+{
+    double s = (pos - left) * inv - 0.5;
+    idx = (int)floor(s);
+    off = s - idx;
+}
+
+
+constexpr int kTrackThreads = 256;
+
+// Two compiled variants: FULL runs every op kind; LIGHT omits the Yoshida
+// integrators and the sector bend so that passes made only of drifts, thin
+// kicks, apertures, the space-charge kick and the moment sums fit in fewer
+// registers and run at higher occupancy.
+enum TrackVariant { TRACK_LIGHT = 0, TRACK_FULL = 1, TRACK_FULL_WIDE = 2 };
+
+// Minimum resident CTAs per SM for each variant (register budget).
+template <int V>
+struct TrackOcc {
+    static constexpr int value = V == TRACK_LIGHT ? 3 : (V == TRACK_FULL ? 3 : 2);
+};
+
+// One particle in registers during a pass.
+struct Part {
+    double x, xp, y, yp, cdt, dpop;
+    bool alive;
+    int disc;
+};
+
+// Applies one op to one particle (apertures, moments and maps).
+template <int VARIANT>
+__device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, Part& P, int* s_counts,
+                                         double* s_mom_col)
+{
+    constexpr bool kFull = VARIANT != TRACK_LIGHT;
+    const int kind = op.kind;
+    double& x = P.x;
+    double& xp = P.xp;
+    double& y = P.y;
+    double& yp = P.yp;
+    double& cdt = P.cdt;
+    double& dpop = P.dpop;
+    if (kind >= OP_AP_FINITE && kind <= OP_AP_RECTANGULAR) {
+        // discard_applier bunch_particles.h:484-503: discards(i) is reset by
+        // every aperture, then set if this one discards.
+        P.disc = 0;
+        if (P.alive) {
+            bool d;
+            if (kind == OP_AP_FINITE) {
+                if (!isfinite(x) || !isfinite(xp) || !isfinite(y) || !isfinite(yp) || !isfinite(cdt) ||
+                    !isfinite(dpop))
+                    d = true;
+                else {
+                    double pt = 1.0 + dpop;
+                    d = pt * pt - xp * xp - yp * yp < 0.0;
+                }
+            } else if (kind == OP_AP_CIRCULAR) {
+                double xr = x - op.d[1], yr = y - op.d[2];
+                d = (xr * xr + yr * yr) > op.d[0];
+            } else if (kind == OP_AP_ELLIPTICAL) {
+                double xr = x - op.d[2], yr = y - op.d[3];
+                d = (xr * xr / op.d[0] + yr * yr / op.d[1]) > 1.0;
+            } else {
+                double xr = x - op.d[2], yr = y - op.d[3];
+                d = (fabs(xr) > 0.5 * op.d[0]) || (fabs(yr) > 0.5 * op.d[1]);
+            }
+            if (d) {
+                P.disc = 1;
+                P.alive = false;
+                atomicAdd(&s_counts[op.slot - p.slot_base], 1);
+            }
+        }
+        return;
+    }
+    if (kind == OP_MOMENTS) {
+        if (P.alive) {
+            s_mom_col[0 * kTrackThreads] += x;
+            s_mom_col[1 * kTrackThreads] += y;
+            s_mom_col[2 * kTrackThreads] += cdt;
+            s_mom_col[3 * kTrackThreads] += x * x;
+            s_mom_col[4 * kTrackThreads] += y * y;
+            s_mom_col[5 * kTrackThreads] += cdt * cdt;
+        }
+        return;
+    }
+    if (!P.alive) return;
+        switch (kind) {
+        case OP_DRIFT:
+#if SB2_FAST_MAPS
+            {
+                const double dp = dpop + 1.0;
+                drift_unit_ib(x, xp, y, yp, cdt, dp, op.d[0], inv_beta(dp, op.d[1], op.d[2]), op.d[3]);
+            }
+#else
+            drift_unit(x, xp, y, yp, cdt, dpop, op.d[0], op.d[1], op.d[2], op.d[3]);
+#endif
+            break;
+        case OP_QUAD: {
+            if constexpr (kFull) {
+                double xx = x - op.d[0], yy = y - op.d[1];
+                yoshida6_op<OP_QUAD>(xx, xp, yy, yp, cdt, dpop, op);
+                x = xx + op.d[0];
+                y = yy + op.d[1];
+            }
+            break;
+        }
+        case OP_QUAD_CF: {
+            if constexpr (kFull) {
+                double xx = x - op.d[0], yy = y - op.d[1];
+                yoshida6_op<OP_QUAD_CF>(xx, xp, yy, yp, cdt, dpop, op);
+                x = xx + op.d[0];
+                y = yy + op.d[1];
+            }
+            break;
+        }
+        case OP_SEXT_YOSHIDA:
+            if constexpr (kFull) yoshida6_op<OP_SEXT_YOSHIDA>(x, xp, y, yp, cdt, dpop, op);
+            break;
+        case OP_THIN_QUAD: {
+            double xx = x - op.d[0], yy = y - op.d[1];
+            thin_quadrupole_unit(xx, xp, yy, yp, op.d[2], op.d[3]);
+            break;
+        }
+        case OP_THIN_SEXT:
+            thin_sextupole_unit(x, xp, y, yp, op.d[2], op.d[3]);
+            break;
+        case OP_MPOLE: {
+            const double* kl = op.d;
+            const int on = op.flags;
+            if (on & 1) { xp = xp - kl[0]; yp = yp + kl[1]; }
+            if (on & 2) thin_quadrupole_unit(x, xp, y, yp, kl[2], kl[3]);
+            if (on & 4) thin_sextupole_unit(x, xp, y, yp, kl[4], kl[5]);
+            if (on & 8) thin_octupole_unit(x, xp, y, yp, kl[6], kl[7]);
+            for (int nn = 4; nn < 8; ++nn)
+                if (on & (1 << nn)) thin_magnet_unit(x, xp, y, yp, kl[nn * 2], kl[nn * 2 + 1], nn + 1);
+            break;
+        }
+        case OP_SBEND: {
+            if constexpr (kFull) sbend_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
+            break;
+        }
+        case OP_SC_KICK: {
+            // zyx::alg_kicker space_charge_3d_kernels.h:91-215
+            const ScState& sc = *p.sc;
+            if (!sc.valid) break;
+            int ix, iy, iz;
+            double ox, oy, oz;
+            leftmost(x, sc.left[0], sc.ih[0], ix, ox);
+            leftmost(y, sc.left[1], sc.ih[1], iy, oy);
+            leftmost(cdt, sc.left[2], sc.ih[2], iz, oz);
+            const int gx = p.gx, gy = p.gy, gz = p.gz;
+            if (!((ix >= 0 && ix < gx - 1) && (iy >= 0 && iy < gy - 1) && (iz >= 0 && iz < gz - 1)))
+                break;
+            double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
+            const int64_t b0 = ((int64_t)iz * gy + iy) * gx + ix;
+            const int64_t b1 = ((int64_t)(iz + 1) * gy + iy) * gx + ix;
+            if (p.efield32) {
+                // mixed precision: FP32 field, one 16-byte load per corner,
+                // interpolation weights and the kick in FP64
+                const float4* F = p.efield32;
+                const float4 f000 = F[b0], f001 = F[b0 + 1], f010 = F[b0 + gx], f011 = F[b0 + gx + 1];
+                const float4 f100 = F[b1], f101 = F[b1 + 1], f110 = F[b1 + gx], f111 = F[b1 + gx + 1];
+                const double w000 = aoz * aoy * aox, w001 = aoz * aoy * ox, w010 = aoz * oy * aox,
+                             w011 = aoz * oy * ox, w100 = oz * aoy * aox, w101 = oz * aoy * ox,
+                             w110 = oz * oy * aox, w111 = oz * oy * ox;
+                const double factor = sc.factor, pref = p.kick_pref, m = p.kick_m;
+                double val = w000 * f000.z + w001 * f001.z + w010 * f010.z + w011 * f011.z + w100 * f100.z +
+                             w101 * f101.z + w110 * f110.z + w111 * f111.z;
+                double pp = pref + dpop * pref;
+                double Eoc_i = sqrt(pp * pp + m * m);
+                double Eoc_f = Eoc_i + factor * (-pref) * val;
+                dpop += (sqrt(Eoc_f * Eoc_f - m * m) - sqrt(Eoc_i * Eoc_i - m * m)) / pref;
+                val = w000 * f000.y + w001 * f001.y + w010 * f010.y + w011 * f011.y + w100 * f100.y +
+                      w101 * f101.y + w110 * f110.y + w111 * f111.y;
+                yp += factor * val;
+                val = w000 * f000.x + w001 * f001.x + w010 * f010.x + w011 * f011.x + w100 * f100.x +
+                      w101 * f101.x + w110 * f110.x + w111 * f111.x;
+                xp += factor * val;
+                break;
+            }
+            const double2* E = p.efield;
+            // corner fields: .x/.y of [2c] = ex, ey; .x of [2c+1] = ez
+            double2 a00 = E[2 * b0], a01 = E[2 * (b0 + 1)], a10 = E[2 * (b0 + gx)], a11 = E[2 * (b0 + gx + 1)];
+            double2 c00 = E[2 * b1], c01 = E[2 * (b1 + 1)], c10 = E[2 * (b1 + gx)], c11 = E[2 * (b1 + gx + 1)];
+            double z00 = E[2 * b0 + 1].x, z01 = E[2 * (b0 + 1) + 1].x, z10 = E[2 * (b0 + gx) + 1].x,
+                   z11 = E[2 * (b0 + gx + 1) + 1].x;
+            double w00 = E[2 * b1 + 1].x, w01 = E[2 * (b1 + 1) + 1].x, w10 = E[2 * (b1 + gx) + 1].x,
+                   w11 = E[2 * (b1 + gx + 1) + 1].x;
+            const double factor = sc.factor, pref = p.kick_pref, m = p.kick_m;
+            double val = aoz * aoy * aox * z00;
+            val += aoz * aoy * ox * z01;
+            val += aoz * oy * aox * z10;
+            val += aoz * oy * ox * z11;
+            val += oz * aoy * aox * w00;
+            val += oz * aoy * ox * w01;
+            val += oz * oy * aox * w10;
+            val += oz * oy * ox * w11;
+            double pp = pref + dpop * pref;
+            double Eoc_i = sqrt(pp * pp + m * m);
+            double Eoc_f = Eoc_i + factor * (-pref) * val;
+            double ddp = (sqrt(Eoc_f * Eoc_f - m * m) - sqrt(Eoc_i * Eoc_i - m * m)) / pref;
+            dpop += ddp;
+            val = aoz * aoy * aox * a00.y;
+            val += aoz * aoy * ox * a01.y;
+            val += aoz * oy * aox * a10.y;
+            val += aoz * oy * ox * a11.y;
+            val += oz * aoy * aox * c00.y;
+            val += oz * aoy * ox * c01.y;
+            val += oz * oy * aox * c10.y;
+            val += oz * oy * ox * c11.y;
+            yp += factor * val;
+            val = aoz * aoy * aox * a00.x;
+            val += aoz * aoy * ox * a01.x;
+            val += aoz * oy * aox * a10.x;
+            val += aoz * oy * ox * a11.x;
+            val += oz * aoy * aox * c00.x;
+            val += oz * aoy * ox * c01.x;
+            val += oz * oy * aox * c10.x;
+            val += oz * oy * ox * c11.x;
+            xp += factor * val;
+            break;
+        }
+        default:
+            break;
+        }
+}
+
+// PPT particles per thread travel through the op list together, so their
+// independent load and arithmetic chains overlap (more bytes in flight per
+// thread for the memory-bound passes).
+template <int VARIANT, int PPT>
+__global__ void __launch_bounds__(kTrackThreads, TrackOcc<VARIANT>::value)
+    track_kernel(const __grid_constant__ TrackParams p)
+{
+    __shared__ int s_counts[kMaxOpsPerPass];
+    __shared__ double s_mom[6][kTrackThreads]; // per-thread moment sums
+    for (int i = threadIdx.x; i < kMaxOpsPerPass; i += blockDim.x) s_counts[i] = 0;
+    for (int j = 0; j < 6; ++j) s_mom[j][threadIdx.x] = 0.0;
+    __syncthreads();
+    double* s_mom_col = &s_mom[0][threadIdx.x];
+
+    const int64_t n = p.n;
+    const int64_t S = p.stride;
+    const int64_t tile = (int64_t)blockDim.x * PPT;
+    for (int64_t base = blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
+        Part P[PPT];
+        bool in[PPT];
+        // the mask and the six columns are loaded together (no load waits
+        // on the mask), so all seven requests of every particle are in
+        // flight at once; lost particles' values are read and ignored
+        uint8_t mk[PPT];
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+            const int64_t i = base + q * blockDim.x + threadIdx.x;
+            mk[q] = 0;
+            P[q].x = P[q].xp = P[q].y = P[q].yp = P[q].cdt = P[q].dpop = 0.0;
+            if (i < n) {
+                mk[q] = p.masks[i];
+                P[q].x = p.parts[i];
+                P[q].xp = p.parts[i + S];
+                P[q].y = p.parts[i + 2 * S];
+                P[q].yp = p.parts[i + 3 * S];
+                P[q].cdt = p.parts[i + 4 * S];
+                P[q].dpop = p.parts[i + 5 * S];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+            P[q].alive = mk[q] != 0;
+            in[q] = P[q].alive;
+            P[q].disc = 0;
+        }
+        for (int o = 0; o < p.nops; ++o) {
+            const MapOp& op = p.ops[o];
+#pragma unroll
+            for (int q = 0; q < PPT; ++q) apply_op<VARIANT>(p, op, P[q], s_counts, s_mom_col);
+        }
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+            const int64_t i = base + q * blockDim.x + threadIdx.x;
+            if (i >= n) continue;
+            if (in[q]) {
+                p.parts[i] = P[q].x;
+                p.parts[i + S] = P[q].xp;
+                p.parts[i + 2 * S] = P[q].y;
+                p.parts[i + 3 * S] = P[q].yp;
+                p.parts[i + 4 * S] = P[q].cdt;
+                p.parts[i + 5 * S] = P[q].dpop;
+                if (!P[q].alive) p.masks[i] = 0;
+            }
+            if (p.write_discards && p.discards) p.discards[i] = (uint8_t)P[q].disc;
+        }
+    }
+
+    // per-aperture discard counts
+    __syncthreads();
+    for (int s = threadIdx.x; s < kMaxOpsPerPass; s += blockDim.x)
+        if (s_counts[s]) atomicAdd(&p.ap_counts[p.slot_base + s], s_counts[s]);
+
+    // moments: fixed-order block reduction -> one partial per block
+    bool any_mom = false;
+    for (int o = 0; o < p.nops; ++o) any_mom |= (p.ops[o].kind == OP_MOMENTS);
+    if (any_mom && p.moment_partials) {
+        for (int w = kTrackThreads / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w)
+                for (int j = 0; j < 6; ++j) s_mom[j][threadIdx.x] += s_mom[j][threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x < 6) p.moment_partials[blockIdx.x * 6 + threadIdx.x] = s_mom[threadIdx.x][0];
+    }
+}
+
+bool track_needs_full(const MapOp* ops, int n)
+{
+    for (int i = 0; i < n; ++i) {
+        int k = ops[i].kind;
+        if (k == OP_QUAD || k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_SBEND) return true;
+    }
+    return false;
+}
+
+// Register budget of the full variant: 2 CTAs/SM (128 registers; measured
+// faster for the Yoshida passes) unless SB2_TRACK_FULL_OCC=3 selects
+// 3 CTAs/SM (80 registers).
+static int full_variant()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("SB2_TRACK_FULL_OCC");
+        v = (e && atoi(e) == 3) ? TRACK_FULL : TRACK_FULL_WIDE;
+    }
+    return v;
+}
+
+cudaError_t launch_pass(const TrackParams& p, cudaStream_t s)
+{
+    int nb = track_grid_blocks();
+    if (!track_needs_full(p.ops, p.nops))
+        track_kernel<TRACK_LIGHT, 2><<<nb, kTrackThreads, 0, s>>>(p);
+    else if (full_variant() == TRACK_FULL_WIDE)
+        track_kernel<TRACK_FULL_WIDE, 1><<<nb, kTrackThreads, 0, s>>>(p);
+    else
+        track_kernel<TRACK_FULL, 1><<<nb, kTrackThreads, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+} // namespace SB2_TRACK_NS
+} // namespace sb2

@@ -60,3 +60,32 @@ def test_mixed_emittance_after_many_kicks(syn):
     e64, e32 = emits
     assert np.all(np.abs(e32 / e64 - 1) <= EMIT_TOL_MIXED), e32 / e64 - 1
     assert np.array_equal(parts[0][:, 6], parts[1][:, 6])
+
+
+@pytest.mark.parametrize("cell", ["fodo", "ring"])
+def test_mixed_path_maps_match_fp64(syn, cell):
+    """The mixed-precision path runs the same FP64 maps with fused
+    multiply-adds and the drift's path length folded into one reciprocal
+    square root (track_fast.cu).  With a negligible space-charge kick
+    (real_num = 1), its coordinates after two turns of the FODO cell (Yoshida
+    quadrupoles) or the ring cell (sector bends, thin sextupoles, apertures)
+    agree with the exact FP64 path to 1e-12 relative; ids and masks exact."""
+    from helpers import ring_cell
+    n, shape = 20000, (16, 16, 32)
+    spec, steps = (fodo_cell(), 8) if cell == "fodo" else (ring_cell(), 16)
+    p = gaussian_bunch(n, SIG_C0, 73)
+    out = []
+    for prec in (syn.precision_t.fp64, syn.precision_t.mixed):
+        lat, ref = product_lattice(spec)
+        opts = syn.Space_charge_3d_open_hockney_options(*shape)
+        opts.precision = prec
+        prop = syn.Propagator(lat, syn.Split_operator_stepper(opts, steps))
+        b = syn.Bunch(ref, n, 1.0)
+        b.set_particles(p)
+        prop.propagate(b, 2)
+        out.append(b.get_particles())
+    (a, am, _), (f, fm, _) = out
+    assert np.array_equal(a[:, 6], f[:, 6]) and np.array_equal(am, fm)
+    scale = np.max(np.abs(a[:, :6]), axis=0)
+    err = np.max(np.abs(f[:, :6] - a[:, :6]), axis=0) / scale
+    assert np.all(err <= 1e-12), err
