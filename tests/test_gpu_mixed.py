@@ -69,7 +69,10 @@ def test_mixed_path_maps_match_fp64(syn, cell):
     square root (track_fast.cu).  With a negligible space-charge kick
     (real_num = 1), its coordinates after two turns of the FODO cell (Yoshida
     quadrupoles) or the ring cell (sector bends, thin sextupoles, apertures)
-    agree with the exact FP64 path to 1e-12 relative; ids and masks exact."""
+    agree with the exact FP64 path to 1e-12 relative (FODO) and 1e-11
+    relative (ring: the bend map takes the difference of two arcsines of
+    nearly equal arguments, which magnifies last-bit differences about a
+    thousandfold); ids and masks exact."""
     from helpers import ring_cell
     n, shape = 20000, (16, 16, 32)
     spec, steps = (fodo_cell(), 8) if cell == "fodo" else (ring_cell(), 16)
@@ -88,4 +91,4 @@ def test_mixed_path_maps_match_fp64(syn, cell):
     assert np.array_equal(a[:, 6], f[:, 6]) and np.array_equal(am, fm)
     scale = np.max(np.abs(a[:, :6]), axis=0)
     err = np.max(np.abs(f[:, :6] - a[:, :6]), axis=0) / scale
-    assert np.all(err <= 1e-12), err
+    assert np.all(err <= (1e-12 if cell == "fodo" else 1e-11)), err
