@@ -453,8 +453,6 @@ struct Bunch {
         cudaFree(wc.masks2);
         cudaFree(wc.discards2);
         cudaFree(wc.perm2);
-        cudaFree(wc.keys);
-        cudaFree(wc.ranks);
         wc = SortBuffers{};
     }
     // home -> working copy in the caller's order (identity permutation)
@@ -473,8 +471,6 @@ struct Bunch {
             wc.discards2 = dalloc<uint8_t>(cap, "working copy");
             wc.perm = dalloc<int32_t>(cap, "working copy");
             wc.perm2 = dalloc<int32_t>(cap, "working copy");
-            wc.keys = dalloc<int32_t>(cap, "working copy");
-            wc.ranks = dalloc<int32_t>(cap, "working copy");
         }
         cuda_check(launch_sort_gather_in(home_parts, home_stride, home_masks, home_discards, wc, s), "sort gather");
         parts = wc.parts;
@@ -1604,7 +1600,7 @@ struct Propagator {
     // cell-ordered working copy of the bunch (space-charge runs only)
     bool cell_sort = true;
     int sort_interval = 4; // re-sort before every k-th space-charge kick (measured best of 1, 2, 4, 8 at 4M particles)
-    int32_t* sort_scratch = nullptr; // histogram, offsets and block sums of the counting sort
+    int32_t* sort_scratch = nullptr; // histogram, offsets, cursors and block sums of the counting sort
 
     Propagator(const Lattice& l, int stepper_kind, int n, const sb2_sc3d_options* opts)
         : lat(l), stepper(stepper_kind), num(n)

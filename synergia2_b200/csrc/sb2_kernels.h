@@ -68,8 +68,6 @@ struct SortBuffers {
     uint8_t* masks2;
     uint8_t* discards2;
     int32_t* perm2;
-    int32_t* keys;  // cell key of each particle (sort pass)
-    int32_t* ranks; // its rank inside the cell (sort pass)
     int64_t n, stride;
 };
 

@@ -7,10 +7,9 @@
 // their deposit stencil, rebuilt before each deposit by a counting sort:
 //   key       cell (iz*gy + iy)*gx + ix of the stencil's lower corner;
 //             G for live particles outside the grid, G+1 for lost ones
-//   rank      warp-aggregated atomics on key counts: the histogram and
-//             each particle's rank inside its cell
+//   histogram warp-aggregated atomics on key counts
 //   scan      exclusive prefix sum of the counts (three small kernels)
-//   move      every column, the mask, the discard flag and the original
+//   scatter   every column, the mask, the discard flag and the original
 //             index move to offset[key] + rank
 // The caller's arrays are untouched while the bunch lives in the working
 // copy; they are brought back up to date (the working copy scattered back to
@@ -43,13 +42,10 @@ __device__ __forceinline__ unsigned lanemask_lt()
     return m;
 }
 
-// keys and ranks: counts[key] is the histogram, ranks[i] the particle's
-// place among its cell's particles (warp-aggregated atomics; the order
-// inside a cell is the atomics' arrival order)
-__global__ void __launch_bounds__(256) sort_rank_kernel(const double* __restrict__ parts, int64_t stride,
+__global__ void __launch_bounds__(256) sort_hist_kernel(const double* __restrict__ parts, int64_t stride,
                                                         const uint8_t* __restrict__ masks, int64_t n,
                                                         const ScState* __restrict__ scp, int gx, int gy, int gz,
-                                                        int32_t* counts, int32_t* keys, int32_t* ranks)
+                                                        int32_t* counts)
 {
     const ScState& sc = *scp;
     const int G = gx * gy * gz;
@@ -59,19 +55,13 @@ __global__ void __launch_bounds__(256) sort_rank_kernel(const double* __restrict
         const int64_t i = wb + lane;
         int key = -1;
         if (i < n) {
-            const uint8_t mk = masks[i];
-            const double x = parts[i], y = parts[i + 2 * stride], z = parts[i + 4 * stride];
-            key = (!mk || !sc.valid) ? G + 1 : cell_key(x, y, z, sc, gx, gy, gz);
+            if (!masks[i] || !sc.valid)
+                key = G + 1;
+            else
+                key = cell_key(parts[i], parts[i + 2 * stride], parts[i + 4 * stride], sc, gx, gy, gz);
         }
         const unsigned grp = __match_any_sync(0xffffffffu, key);
-        const int leader = __ffs(grp) - 1;
-        int32_t b = 0;
-        if (key >= 0 && lane == leader) b = atomicAdd(&counts[key], __popc(grp));
-        b = __shfl_sync(0xffffffffu, b, leader);
-        if (key >= 0) {
-            keys[i] = key;
-            ranks[i] = b + __popc(grp & lanemask_lt());
-        }
+        if (key >= 0 && lane == __ffs(grp) - 1) atomicAdd(&counts[key], __popc(grp));
     }
 }
 
@@ -146,28 +136,39 @@ __global__ void scan_add_kernel(int32_t* out, int n, const int32_t* __restrict__
     if (i < n) out[i] += sums[i / kScanBlock];
 }
 
-// every column, the mask, the discard flag and the original index move to
-// offsets[key] + rank: a permutation with known destinations (no atomics)
-__global__ void __launch_bounds__(256) sort_move_kernel(const double* __restrict__ src, const uint8_t* __restrict__ m_src,
-                                                        const uint8_t* __restrict__ d_src,
-                                                        const int32_t* __restrict__ p_src, double* dst,
-                                                        uint8_t* m_dst, uint8_t* d_dst, int32_t* p_dst, int64_t n,
-                                                        int64_t stride, const int32_t* __restrict__ keys,
-                                                        const int32_t* __restrict__ ranks,
-                                                        const int32_t* __restrict__ offsets)
+__global__ void __launch_bounds__(256) sort_scatter_kernel(const double* __restrict__ src, const uint8_t* __restrict__ m_src,
+                                                           const uint8_t* __restrict__ d_src,
+                                                           const int32_t* __restrict__ p_src, double* dst,
+                                                           uint8_t* m_dst, uint8_t* d_dst, int32_t* p_dst, int64_t n,
+                                                           int64_t stride, const ScState* __restrict__ scp, int gx,
+                                                           int gy, int gz, const int32_t* __restrict__ offsets,
+                                                           int32_t* cursor)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t pos = (int64_t)offsets[keys[i]] + ranks[i];
+    const ScState& sc = *scp;
+    const int G = gx * gy * gz;
+    const int lane = threadIdx.x & 31;
+    const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t wb = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane; wb < n; wb += wstride) {
+        const int64_t i = wb + lane;
+        int key = -1;
         double v[7];
-#pragma unroll
-        for (int j = 0; j < 7; ++j) v[j] = src[i + j * stride];
-        const uint8_t mk = m_src[i], dk = d_src[i];
-        const int32_t pk = p_src[i];
-#pragma unroll
+        uint8_t mk = 0;
+        if (i < n) {
+            for (int j = 0; j < 7; ++j) v[j] = src[i + j * stride];
+            mk = m_src[i];
+            key = (!mk || !sc.valid) ? G + 1 : cell_key(v[0], v[2], v[4], sc, gx, gy, gz);
+        }
+        const unsigned grp = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(grp) - 1;
+        int32_t b = 0;
+        if (key >= 0 && lane == leader) b = atomicAdd(&cursor[key], __popc(grp));
+        b = __shfl_sync(0xffffffffu, b, leader);
+        if (key < 0) continue;
+        const int64_t pos = (int64_t)offsets[key] + b + __popc(grp & lanemask_lt());
         for (int j = 0; j < 7; ++j) dst[pos + j * stride] = v[j];
         m_dst[pos] = mk;
-        d_dst[pos] = dk;
-        p_dst[pos] = pk;
+        d_dst[pos] = d_src[i];
+        p_dst[pos] = p_src[i];
     }
 }
 
@@ -218,9 +219,9 @@ static int sm_count_s()
 }
 
 size_t sort_scratch_ints(int64_t G)
-{ // counts, offsets, block sums
+{ // counts, offsets (=cursor base), cursor, block sums
     const int64_t m = G + 2;
-    return (size_t)(2 * m + (m + kScanBlock - 1) / kScanBlock + 8);
+    return (size_t)(3 * m + (m + kScanBlock - 1) / kScanBlock + 8);
 }
 
 cudaError_t launch_cell_sort(const SortBuffers& sb, int32_t* scratch, const ScState* sc, int gx, int gy, int gz,
@@ -230,18 +231,19 @@ cudaError_t launch_cell_sort(const SortBuffers& sb, int32_t* scratch, const ScSt
     const int m = (int)(G + 2);
     int32_t* counts = scratch;
     int32_t* offsets = counts + m;
-    int32_t* bsums = offsets + m;
+    int32_t* cursor = offsets + m;
+    int32_t* bsums = cursor + m;
     const int nb = (m + kScanBlock - 1) / kScanBlock;
     cudaError_t e;
     if ((e = cudaMemsetAsync(counts, 0, sizeof(int32_t) * m, s))) return e;
+    if ((e = cudaMemsetAsync(cursor, 0, sizeof(int32_t) * m, s))) return e;
     const int grid = sm_count_s() * 8;
-    sort_rank_kernel<<<grid, 256, 0, s>>>(sb.parts, sb.stride, sb.masks, sb.n, sc, gx, gy, gz, counts, sb.keys,
-                                          sb.ranks);
+    sort_hist_kernel<<<grid, 256, 0, s>>>(sb.parts, sb.stride, sb.masks, sb.n, sc, gx, gy, gz, counts);
     scan_block_kernel<<<nb, 256, 0, s>>>(counts, offsets, m, bsums);
     scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nb);
     scan_add_kernel<<<(m + 255) / 256, 256, 0, s>>>(offsets, m, bsums);
-    sort_move_kernel<<<grid, 256, 0, s>>>(sb.parts, sb.masks, sb.discards, sb.perm, sb.parts2, sb.masks2,
-                                          sb.discards2, sb.perm2, sb.n, sb.stride, sb.keys, sb.ranks, offsets);
+    sort_scatter_kernel<<<grid, 256, 0, s>>>(sb.parts, sb.masks, sb.discards, sb.perm, sb.parts2, sb.masks2,
+                                             sb.discards2, sb.perm2, sb.n, sb.stride, sc, gx, gy, gz, offsets, cursor);
     return cudaGetLastError();
 }
 
