@@ -18,8 +18,10 @@
 // butterflies in registers.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <type_traits>
 #include <cstdint>
 
+#include "fft.cuh"
 #include "sb2_kernels.h"
 
 namespace sb2 {
@@ -301,318 +303,182 @@ __global__ void green_octant_kernel(const ScState* __restrict__ scp, double* G, 
 }
 
 // ---------------------------------------------------------------------------
-// Shared-memory Stockham FFT with radix-8/4/2 butterflies in registers.
-// A tile holds `nl` lines of length L (power of two, 8..4096) at pitch L in
-// shared memory; each pass reads every element once, does one radix-R
-// butterfly per (line, j) in registers and writes the Stockham-ordered
-// result to the other buffer.  Input and output are in natural order.
-// tw[k] = exp(-2 pi i k / L) for k < L; `sign` > 0 selects the inverse.
+// Line passes of the convolution (register-resident FFT, fft.cuh).  Global
+// storage of the spectrum is C (double2, or float2 for the mixed path);
+// every pass computes in FP64 in registers and shared memory, so the mixed
+// path only rounds at the five pass boundaries.
 // ---------------------------------------------------------------------------
-// Complex helpers for double2 (FP64 path) and float2 (mixed path).
 template <typename C> struct CxT;
 template <> struct CxT<double2> { typedef double R; };
 template <> struct CxT<float2> { typedef float R; };
-__device__ __forceinline__ double2 mkc(double x, double y, double2*) { return make_double2(x, y); }
-__device__ __forceinline__ float2 mkc(float x, float y, float2*) { return make_float2(x, y); }
-template <typename C>
-__device__ __forceinline__ C cplx(typename CxT<C>::R x, typename CxT<C>::R y) { return mkc(x, y, (C*)nullptr); }
-template <typename C>
-__device__ __forceinline__ C cmul(C a, C b) { return cplx<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
-template <typename C>
-__device__ __forceinline__ C cadd(C a, C b) { return cplx<C>(a.x + b.x, a.y + b.y); }
-template <typename C>
-__device__ __forceinline__ C csub(C a, C b) { return cplx<C>(a.x - b.x, a.y - b.y); }
-// multiply by -i (forward) or +i (inverse)
-template <typename C>
-__device__ __forceinline__ C rot90(C a, bool inv) { return inv ? cplx<C>(-a.y, a.x) : cplx<C>(a.y, -a.x); }
-
-// In-register DFT of size R (2, 4, 8) in natural order: X[k] = sum_r v[r] w^(rk),
-// w = exp(-/+ 2 pi i / R).
-template <int RAD, typename C>
-struct DftReg;
-
-template <typename C>
-struct DftReg<2, C> {
-    static __device__ __forceinline__ void run(C* v, bool)
-    {
-        C a = v[0], b = v[1];
-        v[0] = cadd(a, b);
-        v[1] = csub(a, b);
-    }
-};
-
-template <typename C>
-struct DftReg<4, C> {
-    static __device__ __forceinline__ void run(C* v, bool inv)
-    {
-        C s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
-        C s13 = cadd(v[1], v[3]), d13 = rot90(csub(v[1], v[3]), inv);
-        v[0] = cadd(s02, s13);
-        v[2] = csub(s02, s13);
-        v[1] = cadd(d02, d13);
-        v[3] = csub(d02, d13);
-    }
-};
-
-template <typename C>
-struct DftReg<8, C> {
-    static __device__ __forceinline__ void run(C* v, bool inv)
-    {
-        typedef typename CxT<C>::R R;
-        const R h = (R)0.70710678118654752440;
-        // radix-2 first stage (decimation in frequency)
-        C a[4], b[4];
-        for (int r = 0; r < 4; ++r) {
-            a[r] = cadd(v[r], v[r + 4]);
-            b[r] = csub(v[r], v[r + 4]);
-        }
-        // twiddles w8^r on the difference branch
-        b[1] = inv ? cplx<C>(h * (b[1].x - b[1].y), h * (b[1].x + b[1].y))
-                   : cplx<C>(h * (b[1].x + b[1].y), h * (b[1].y - b[1].x));
-        b[2] = rot90(b[2], inv);
-        b[3] = inv ? cplx<C>(-h * (b[3].x + b[3].y), h * (b[3].x - b[3].y))
-                   : cplx<C>(h * (b[3].y - b[3].x), -h * (b[3].x + b[3].y));
-        DftReg<4, C>::run(a, inv); // even outputs
-        DftReg<4, C>::run(b, inv); // odd outputs
-        for (int k = 0; k < 4; ++k) {
-            v[2 * k] = a[k];
-            v[2 * k + 1] = b[k];
-        }
-    }
-};
-
-template <int RAD, typename C>
-__device__ __forceinline__ void stockham_pass(const C* __restrict__ src, C* __restrict__ dst, int nl, int L, int Ns,
-                                              const C* __restrict__ tw, bool inv)
-{
-    // element j of line li sits at j * nl + li: consecutive threads take
-    // consecutive lines, so every read and write below is contiguous
-    const int T = L / RAD;
-    const int total = nl * T;
-    const int tstep = L / (Ns * RAD);
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
-        const int j = t / nl, li = t - j * nl;
-        const int k = j & (Ns - 1);
-        C v[RAD];
-#pragma unroll
-        for (int r = 0; r < RAD; ++r) v[r] = src[(j + r * T) * nl + li];
-        if (Ns > 1) {
-#pragma unroll
-            for (int r = 1; r < RAD; ++r) {
-                C w = tw[(k * r * tstep) & (L - 1)];
-                if (inv) w.y = -w.y;
-                v[r] = cmul(v[r], w);
-            }
-        }
-        DftReg<RAD, C>::run(v, inv);
-        const int idxD = (j / Ns) * Ns * RAD + k;
-#pragma unroll
-        for (int r = 0; r < RAD; ++r) dst[(idxD + r * Ns) * nl + li] = v[r];
-    }
-}
-
-// FFT of the nl lines in b0 (layout j * nl + li); returns the buffer
-// holding the result.
-template <typename C>
-__device__ C* smem_fft(C* b0, C* b1, int nl, int L, const C* __restrict__ tw, bool inv)
-{
-    C* src = b0;
-    C* dst = b1;
-    int Ns = 1;
-    while (Ns < L) {
-        const int rem = L / Ns;
-        if (rem >= 8 && rem != 16) {
-            stockham_pass<8>(src, dst, nl, L, Ns, tw, inv);
-            Ns *= 8;
-        } else if (rem >= 4) {
-            stockham_pass<4>(src, dst, nl, L, Ns, tw, inv);
-            Ns *= 4;
-        } else {
-            stockham_pass<2>(src, dst, nl, L, Ns, tw, inv);
-            Ns *= 2;
-        }
-        __syncthreads();
-        C* t = src;
-        src = dst;
-        dst = t;
-    }
-    return src;
-}
-
-constexpr int kFftTile = 2048; // complex elements per line tile (32 KB; two tiles per CTA)
-constexpr int kFftSmemBytes = 2 * kFftTile * 16;
-constexpr int kFftThreads = 256;
-
-// XF: pairs of real rows (y, y+1) of rho -> S rows (r2c, first gx inputs)
-// Global storage of the spectrum is C (double2, or float2 for the mixed
-// path); every pass converts to double2 on load and computes in FP64 in
-// shared memory and registers, so the mixed path only rounds at the five
-// pass boundaries.
 __device__ __forceinline__ double2 to_d(double2 v) { return v; }
 __device__ __forceinline__ double2 to_d(float2 v) { return make_double2(v.x, v.y); }
 template <typename C> __device__ __forceinline__ C from_d(double2 v);
 template <> __device__ __forceinline__ double2 from_d<double2>(double2 v) { return v; }
 template <> __device__ __forceinline__ float2 from_d<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
 
-// XF: pairs of real rows (y, y+1) of rho -> S rows (r2c, first gx inputs)
-template <typename C>
-__global__ void __launch_bounds__(kFftThreads) fft_xf_kernel(const double* __restrict__ rho, C* S,
-                                                             const double2* __restrict__ tw, Dims d,
-                                                             const ScState* __restrict__ scp)
+// XF: pairs of real rows (y, y+1) of rho -> S rows (r2c, first gx inputs).
+// Lines l = (pair, z); the last pass goes through shared memory so that
+// each output k can combine Z[k] and Z[L-k].
+template <int L, typename C>
+__global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xf_kernel(const double* __restrict__ rho, C* S,
+                                                                        const double2* __restrict__ tw, Dims d,
+                                                                        const ScState* __restrict__ scp)
 {
+    typedef fft::XMajor<L> LAY;
+    constexpr int W = fft::Shape<L>::W, TPL = fft::Shape<L>::TPL;
+    constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     double2* sm = (double2*)sm_raw;
     if (!scp->valid) return;
-    const int L = d.nx, nl = kFftTile / L;
+    const int li = LAY::line(), t = LAY::thr();
     const int npy = (d.gy + 1) / 2;
     const int64_t nlines = (int64_t)npy * d.gz;
-    const int64_t l0 = (int64_t)blockIdx.x * nl;
-    const int nlt = (int)min((int64_t)nl, nlines - l0);
-    if (nlt <= 0) return;
-    double2* b0 = sm;
-    double2* b1 = sm + kFftTile;
-    for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
-        int li = idx / L, j = idx - li * L;
-        int64_t l = l0 + li;
-        int pr = (int)(l % npy), z = (int)(l / npy);
-        int ya = 2 * pr, yb = ya + 1;
-        double2 v = make_double2(0.0, 0.0);
-        if (j < d.gx) {
-            v.x = rho[((int64_t)z * d.gy + ya) * d.gx + j];
-            if (yb < d.gy) v.y = rho[((int64_t)z * d.gy + yb) * d.gx + j];
+    const int64_t l = (int64_t)blockIdx.x * W + li;
+    const bool ok = l < nlines;
+    const int pr = ok ? (int)(l % npy) : 0, z = ok ? (int)(l / npy) : 0;
+    const int ya = 2 * pr, yb = ya + 1;
+    const double* ra = rho + ((int64_t)z * d.gy + ya) * d.gx;
+    const double* rb = rho + ((int64_t)z * d.gy + yb) * d.gx;
+    double2 v[fft::kE];
+#pragma unroll
+    for (int e = 0; e < fft::kE; ++e) {
+        const int pos = fft::io_pos<L, R0>(t, e);
+        v[e] = make_double2(0.0, 0.0);
+        if (ok && pos < d.gx) {
+            v[e].x = ra[pos];
+            if (yb < d.gy) v[e].y = rb[pos];
         }
-        b0[j * nlt + li] = v;
     }
+    fft::run_passes<L, false, LAY>(v, li, t, sm, tw, false);
+#pragma unroll
+    for (int e = 0; e < fft::kE; ++e) sm[LAY::at(li, fft::io_pos<L, RL>(t, e))] = v[e];
     __syncthreads();
-    double2* r = smem_fft(b0, b1, nlt, L, tw, false);
-    const int nk = d.nkx;
-    for (int idx = threadIdx.x; idx < nlt * nk; idx += blockDim.x) {
-        int li = idx / nk, k = idx - li * nk;
-        int64_t l = l0 + li;
-        int pr = (int)(l % npy), z = (int)(l / npy);
-        int ya = 2 * pr, yb = ya + 1;
-        double2 Z = r[k * nlt + li], Zn = r[((L - k) & (L - 1)) * nlt + li];
-        double2 A = make_double2((Z.x + Zn.x) * 0.5, (Z.y - Zn.y) * 0.5);
-        double2 B = make_double2((Z.y + Zn.y) * 0.5, -(Z.x - Zn.x) * 0.5);
-        S[((int64_t)z * d.ny + ya) * d.nkxp + k] = from_d<C>(A);
-        if (yb < d.gy) S[((int64_t)z * d.ny + yb) * d.nkxp + k] = from_d<C>(B);
+    if (!ok) return;
+    C* sa = S + ((int64_t)z * d.ny + ya) * d.nkxp;
+    C* sb = S + ((int64_t)z * d.ny + yb) * d.nkxp;
+    for (int k = t; k < d.nkx; k += TPL) {
+        const double2 Z = sm[LAY::at(li, k)], Zn = sm[LAY::at(li, (L - k) & (L - 1))];
+        sa[k] = from_d<C>(make_double2((Z.x + Zn.x) * 0.5, (Z.y - Zn.y) * 0.5));
+        if (yb < d.gy) sb[k] = from_d<C>(make_double2((Z.y + Zn.y) * 0.5, -(Z.x - Zn.x) * 0.5));
     }
 }
 
-// Y passes: lines (kx, z<gz) along y.  forward: first gy inputs, all ny
-// outputs; inverse: all inputs, first gy outputs.
-template <typename C>
-__global__ void __launch_bounds__(kFftThreads) fft_y_kernel(C* S, const double2* __restrict__ tw, Dims d,
-                                                            int inverse, const ScState* __restrict__ scp)
+// Y passes: lines (kx, z < gz) along y, W consecutive kx per CTA.  forward:
+// first gy inputs, all ny outputs; inverse: all inputs, first gy outputs.
+template <int L, typename C, bool INV>
+__global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_y_kernel(C* S, const double2* __restrict__ tw, Dims d,
+                                                                       const ScState* __restrict__ scp)
 {
+    typedef fft::LMajor<L> LAY;
+    constexpr int W = fft::Shape<L>::W;
+    constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     double2* sm = (double2*)sm_raw;
     if (!scp->valid) return;
-    const int L = d.ny, nl = kFftTile / L;
-    const int64_t nlines = (int64_t)d.nkx * d.gz;
-    const int64_t l0 = (int64_t)blockIdx.x * nl;
-    const int nlt = (int)min((int64_t)nl, nlines - l0);
-    if (nlt <= 0) return;
-    double2* b0 = sm;
-    double2* b1 = sm + kFftTile;
-    const int nin = inverse ? L : d.gy;
-    for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
-        int j = idx / nlt, li = idx - j * nlt; // consecutive threads: consecutive kx
-        int64_t l = l0 + li;
-        int kx = (int)(l % d.nkx), z = (int)(l / d.nkx);
-        double2 v = make_double2(0.0, 0.0);
-        if (j < nin) v = to_d(S[((int64_t)z * d.ny + j) * d.nkxp + kx]);
-        b0[j * nlt + li] = v;
+    const int li = LAY::line(), t = LAY::thr();
+    const int kx = blockIdx.x * W + li, z = blockIdx.y;
+    const bool ok = kx < d.nkx;
+    C* col = S + (int64_t)z * d.ny * d.nkxp + kx;
+    const int nin = INV ? L : d.gy;
+    double2 v[fft::kE];
+#pragma unroll
+    for (int e = 0; e < fft::kE; ++e) {
+        const int pos = fft::io_pos<L, R0>(t, e);
+        v[e] = (ok && pos < nin) ? to_d(col[(int64_t)pos * d.nkxp]) : make_double2(0.0, 0.0);
     }
-    __syncthreads();
-    double2* r = smem_fft(b0, b1, nlt, L, tw, inverse != 0);
-    const int nout = inverse ? d.gy : L;
-    for (int idx = threadIdx.x; idx < nlt * nout; idx += blockDim.x) {
-        int j = idx / nlt, li = idx - j * nlt;
-        int64_t l = l0 + li;
-        int kx = (int)(l % d.nkx), z = (int)(l / d.nkx);
-        S[((int64_t)z * d.ny + j) * d.nkxp + kx] = from_d<C>(r[j * nlt + li]);
+    fft::run_passes<L, false, LAY>(v, li, t, sm, tw, INV);
+    if (!ok) return;
+    const int nout = INV ? d.gy : L;
+#pragma unroll
+    for (int e = 0; e < fft::kE; ++e) {
+        const int pos = fft::io_pos<L, RL>(t, e);
+        if (pos < nout) col[(int64_t)pos * d.nkxp] = from_d<C>(v[e]);
     }
 }
 
-// Z pass: lines (kx, ky) along z: forward (first gz inputs), multiply by
-// the real octant Ghat(kx, min(ky, ny-ky), min(kz, nz-kz)), inverse, first gz
-// outputs.  (alg_cplx_multiplier :350-372 fused between the transforms.)
-template <typename C>
-__global__ void __launch_bounds__(kFftThreads) fft_z_conv_kernel(C* S, const double* __restrict__ Ghat,
-                                                                 const double2* __restrict__ tw, Dims d,
-                                                                 const ScState* __restrict__ scp)
+// Z pass: lines (kx, ky) along z: forward (first gz inputs), multiply by the
+// real octant Ghat(kx, min(ky, ny-ky), min(kz, nz-kz)) in registers, inverse
+// (radices reversed, so it starts from the registers), first gz outputs.
+// (alg_cplx_multiplier space_charge_3d_open_hockney.cc:350-372 fused between
+// the transforms.)
+template <int L, typename C>
+__global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_z_conv_kernel(C* S, const double* __restrict__ Ghat,
+                                                                            const double2* __restrict__ tw, Dims d,
+                                                                            const ScState* __restrict__ scp)
 {
+    typedef fft::LMajor<L> LAY;
+    constexpr int W = fft::Shape<L>::W;
+    constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
+    constexpr int RI = fft::last_radix<L, true>();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     double2* sm = (double2*)sm_raw;
     if (!scp->valid) return;
-    const int L = d.nz, nl = kFftTile / L;
-    const int64_t nlines = (int64_t)d.nkx * d.ny;
-    const int64_t l0 = (int64_t)blockIdx.x * nl;
-    const int nlt = (int)min((int64_t)nl, nlines - l0);
-    if (nlt <= 0) return;
-    double2* b0 = sm;
-    double2* b1 = sm + kFftTile;
-    for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
-        int j = idx / nlt, li = idx - j * nlt;
-        int64_t l = l0 + li;
-        int kx = (int)(l % d.nkx), ky = (int)(l / d.nkx);
-        double2 v = make_double2(0.0, 0.0);
-        if (j < d.gz) v = to_d(S[((int64_t)j * d.ny + ky) * d.nkxp + kx]);
-        b0[j * nlt + li] = v;
+    const int li = LAY::line(), t = LAY::thr();
+    const int kx = blockIdx.x * W + li, ky = blockIdx.y;
+    const bool ok = kx < d.nkx;
+    C* col = S + (int64_t)ky * d.nkxp + kx;
+    const int64_t zs = (int64_t)d.ny * d.nkxp;
+    double2 v[fft::kE];
+#pragma unroll
+    for (int e = 0; e < fft::kE; ++e) {
+        const int pos = fft::io_pos<L, R0>(t, e);
+        v[e] = (ok && pos < d.gz) ? to_d(col[pos * zs]) : make_double2(0.0, 0.0);
     }
-    __syncthreads();
-    double2* r = smem_fft(b0, b1, nlt, L, tw, false);
-    double2* o = (r == b0) ? b1 : b0;
+    fft::run_passes<L, false, LAY>(v, li, t, sm, tw, false);
     const int ogx = d.nx / 2 + 1, ogy = d.ny / 2 + 1;
-    for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
-        int kz = idx / nlt, li = idx - kz * nlt;
-        int64_t l = l0 + li;
-        int kx = (int)(l % d.nkx), ky = (int)(l / d.nkx);
-        int my = ky <= d.ny / 2 ? ky : d.ny - ky;
-        int mz = kz <= d.nz / 2 ? kz : d.nz - kz;
-        const double g = Ghat[((int64_t)mz * ogy + my) * ogx + kx];
-        double2 v = r[kz * nlt + li];
-        r[kz * nlt + li] = make_double2(v.x * g, v.y * g);
+    const int my = ky <= d.ny / 2 ? ky : d.ny - ky;
+    const double* gcol = Ghat + (int64_t)my * ogx + (ok ? kx : 0);
+#pragma unroll
+    for (int e = 0; e < fft::kE; ++e) {
+        const int kz = fft::io_pos<L, RL>(t, e);
+        const int mz = kz <= L / 2 ? kz : L - kz;
+        const double g = ok ? __ldg(&gcol[(int64_t)mz * ogy * ogx]) : 0.0;
+        v[e] = make_double2(v[e].x * g, v[e].y * g);
     }
-    __syncthreads();
-    double2* q = smem_fft(r, o, nlt, L, tw, true);
-    for (int idx = threadIdx.x; idx < nlt * d.gz; idx += blockDim.x) {
-        int j = idx / nlt, li = idx - j * nlt;
-        int64_t l = l0 + li;
-        int kx = (int)(l % d.nkx), ky = (int)(l / d.nkx);
-        S[((int64_t)j * d.ny + ky) * d.nkxp + kx] = from_d<C>(q[j * nlt + li]);
+    fft::run_passes<L, true, LAY>(v, li, t, sm, tw, true);
+    if (!ok) return;
+#pragma unroll
+    for (int e = 0; e < fft::kE; ++e) {
+        const int pos = fft::io_pos<L, RI>(t, e);
+        if (pos < d.gz) col[pos * zs] = from_d<C>(v[e]);
     }
 }
 
 // XI: Hermitian pairs of spectrum rows -> real rows (y, y+1) of phi (c2r,
 // first gx outputs); imaginary parts of the k = 0 and k = nx/2 terms are
 // ignored as a c2r transform does.
-template <typename C, typename RO>
-__global__ void __launch_bounds__(kFftThreads) fft_xi_kernel(const C* __restrict__ S, RO* phi,
-                                                             const double2* __restrict__ tw, Dims d,
-                                                             const ScState* __restrict__ scp)
+template <int L, typename C, typename RO>
+__global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xi_kernel(const C* __restrict__ S, RO* phi,
+                                                                        const double2* __restrict__ tw, Dims d,
+                                                                        const ScState* __restrict__ scp)
 {
+    typedef fft::XMajor<L> LAY;
+    constexpr int W = fft::Shape<L>::W;
+    constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     double2* sm = (double2*)sm_raw;
     if (!scp->valid) return;
-    const int L = d.nx, nl = kFftTile / L;
+    const int li = LAY::line(), t = LAY::thr();
     const int npy = (d.gy + 1) / 2;
     const int64_t nlines = (int64_t)npy * d.gz;
-    const int64_t l0 = (int64_t)blockIdx.x * nl;
-    const int nlt = (int)min((int64_t)nl, nlines - l0);
-    if (nlt <= 0) return;
-    double2* b0 = sm;
-    double2* b1 = sm + kFftTile;
-    const int half = L / 2;
-    for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
-        int li = idx / L, j = idx - li * L;
-        int64_t l = l0 + li;
-        int pr = (int)(l % npy), z = (int)(l / npy);
-        int ya = 2 * pr, yb = ya + 1;
-        int k = j <= half ? j : L - j;
-        double2 A = to_d(S[((int64_t)z * d.ny + ya) * d.nkxp + k]);
-        double2 B = (yb < d.gy) ? to_d(S[((int64_t)z * d.ny + yb) * d.nkxp + k]) : make_double2(0.0, 0.0);
+    const int64_t l = (int64_t)blockIdx.x * W + li;
+    const bool ok = l < nlines;
+    const int pr = ok ? (int)(l % npy) : 0, z = ok ? (int)(l / npy) : 0;
+    const int ya = 2 * pr, yb = ya + 1;
+    const C* sa = S + ((int64_t)z * d.ny + ya) * d.nkxp;
+    const C* sb = S + ((int64_t)z * d.ny + yb) * d.nkxp;
+    constexpr int half = L / 2;
+    double2 v[fft::kE];
+#pragma unroll
+    for (int e = 0; e < fft::kE; ++e) {
+        const int j = fft::io_pos<L, R0>(t, e);
+        const int k = j <= half ? j : L - j;
+        double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
+        if (ok) {
+            A = to_d(sa[k]);
+            if (yb < d.gy) B = to_d(sb[k]);
+        }
         if (k == 0 || k == half) {
             A.y = 0.0;
             B.y = 0.0;
@@ -621,71 +487,74 @@ __global__ void __launch_bounds__(kFftThreads) fft_xi_kernel(const C* __restrict
             A.y = -A.y;
             B.y = -B.y;
         }
-        b0[j * nlt + li] = make_double2(A.x - B.y, A.y + B.x);
+        v[e] = make_double2(A.x - B.y, A.y + B.x);
     }
-    __syncthreads();
-    double2* r = smem_fft(b0, b1, nlt, L, tw, true);
-    for (int idx = threadIdx.x; idx < nlt * d.gx; idx += blockDim.x) {
-        int li = idx / d.gx, j = idx - li * d.gx;
-        int64_t l = l0 + li;
-        int pr = (int)(l % npy), z = (int)(l / npy);
-        int ya = 2 * pr, yb = ya + 1;
-        double2 v = r[j * nlt + li];
-        phi[((int64_t)z * d.gy + ya) * d.gx + j] = (RO)v.x;
-        if (yb < d.gy) phi[((int64_t)z * d.gy + yb) * d.gx + j] = (RO)v.y;
+    fft::run_passes<L, false, LAY>(v, li, t, sm, tw, true);
+    if (!ok) return;
+    RO* pa = phi + ((int64_t)z * d.gy + ya) * d.gx;
+    RO* pb = phi + ((int64_t)z * d.gy + yb) * d.gx;
+#pragma unroll
+    for (int e = 0; e < fft::kE; ++e) {
+        const int j = fft::io_pos<L, RL>(t, e);
+        if (j < d.gx) {
+            pa[j] = (RO)v[e].x;
+            if (yb < d.gy) pb[j] = (RO)v[e].y;
+        }
     }
 }
 
 // Ghat passes on the real octant (ox, oy, oz) = (nx/2+1, ny/2+1, nz/2+1):
-// axis 0/1/2 transforms even real lines rebuilt by mirroring; real part of
-// the first L/2+1 outputs stored back in place.  The transform of a real
-// even line is real, so two lines ride in one complex FFT (line 2q as the
-// real part, line 2q+1 as the imaginary part) and come out as its real and
-// imaginary parts.
-__global__ void __launch_bounds__(kFftThreads) fft_green_kernel(double* G, const double2* __restrict__ tw,
-                                                                int axis, int L, int ox, int oy, int oz,
-                                                                const ScState* __restrict__ scp)
+// along axis 0/1/2, each line is mirrored to the even real line of length L
+// and transformed; the real parts of the first L/2+1 outputs are stored back
+// in place.  The transform of a real even line is real, so two lines ride in
+// one complex transform (lines 2c and 2c+1 as its real and imaginary parts)
+// and come out as its real and imaginary parts.  Axis 0 (x rows, contiguous)
+// uses the x-major tile; axes 1 and 2 take W consecutive line pairs.
+template <int L, int AXIS>
+__global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_green_kernel(double* G,
+                                                                           const double2* __restrict__ tw, int ox,
+                                                                           int oy, int oz,
+                                                                           const ScState* __restrict__ scp)
 {
+    typedef typename std::conditional<AXIS == 0, fft::XMajor<L>, fft::LMajor<L>>::type LAY;
+    constexpr int W = fft::Shape<L>::W;
+    constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
+    constexpr int half = L / 2;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     double2* sm = (double2*)sm_raw;
     if (!scp->valid) return;
-    const int nl = kFftTile / L; // complex lines (line pairs) per CTA
-    const int half = L / 2;
+    const int li = LAY::line(), t = LAY::thr();
     int64_t nlines, sj;
-    if (axis == 0) { nlines = (int64_t)oy * oz; sj = 1; }
-    else if (axis == 1) { nlines = (int64_t)ox * oz; sj = ox; }
+    if (AXIS == 0) { nlines = (int64_t)oy * oz; sj = 1; }
+    else if (AXIS == 1) { nlines = (int64_t)ox * oz; sj = ox; }
     else { nlines = (int64_t)ox * oy; sj = (int64_t)ox * oy; }
-    const int64_t npairs = (nlines + 1) / 2;
-    const int64_t l0 = (int64_t)blockIdx.x * nl;
-    const int nlt = (int)min((int64_t)nl, npairs - l0);
-    if (nlt <= 0) return;
-    double2* b0 = sm;
-    double2* b1 = sm + kFftTile;
     auto line_base = [&](int64_t l) -> int64_t {
-        if (axis == 0) return l * ox;                                  // (y, z) rows
-        if (axis == 1) return (l % ox) + (l / ox) * (int64_t)ox * oy;  // (kx, z)
+        if (AXIS == 0) return l * ox;                                  // (y, z) rows
+        if (AXIS == 1) return (l % ox) + (l / ox) * (int64_t)ox * oy;  // (kx, z)
         return l;                                                      // (kx, ky)
     };
-    for (int idx = threadIdx.x; idx < nlt * L; idx += blockDim.x) {
-        int li, j;
-        if (axis == 0) { li = idx / L; j = idx - li * L; }
-        else { j = idx / nlt; li = idx - j * nlt; }
+    const int64_t c = (int64_t)blockIdx.x * W + li;
+    const int64_t la = 2 * c, lb = la + 1;
+    const bool oka = la < nlines, okb = lb < nlines;
+    const double* ga = G + (oka ? line_base(la) : 0);
+    const double* gb = G + (okb ? line_base(lb) : 0);
+    double2 v[fft::kE];
+#pragma unroll
+    for (int e = 0; e < fft::kE; ++e) {
+        const int j = fft::io_pos<L, R0>(t, e);
         const int m = j <= half ? j : L - j;
-        const int64_t la = 2 * (l0 + li), lb = la + 1;
-        const double va = G[line_base(la) + m * sj];
-        const double vb = lb < nlines ? G[line_base(lb) + m * sj] : 0.0;
-        b0[j * nlt + li] = make_double2(va, vb);
+        v[e] = make_double2(oka ? ga[m * sj] : 0.0, okb ? gb[m * sj] : 0.0);
     }
-    __syncthreads();
-    double2* r = smem_fft(b0, b1, nlt, L, tw, false);
-    for (int idx = threadIdx.x; idx < nlt * (half + 1); idx += blockDim.x) {
-        int li, k;
-        if (axis == 0) { li = idx / (half + 1); k = idx - li * (half + 1); }
-        else { k = idx / nlt; li = idx - k * nlt; }
-        const int64_t la = 2 * (l0 + li), lb = la + 1;
-        const double2 v = r[k * nlt + li];
-        G[line_base(la) + k * sj] = v.x;
-        if (lb < nlines) G[line_base(lb) + k * sj] = v.y;
+    fft::run_passes<L, false, LAY>(v, li, t, sm, tw, false);
+    double* wa = G + (oka ? line_base(la) : 0);
+    double* wb = G + (okb ? line_base(lb) : 0);
+#pragma unroll
+    for (int e = 0; e < fft::kE; ++e) {
+        const int k = fft::io_pos<L, RL>(t, e);
+        if (k <= half) {
+            if (oka) wa[k * sj] = v[e].x;
+            if (okb) wb[k * sj] = v[e].y;
+        }
     }
 }
 
@@ -753,52 +622,109 @@ cudaError_t launch_deposit(const double* parts, int64_t stride, const uint8_t* m
     return cudaGetLastError();
 }
 
-template <typename C>
-static cudaError_t set_fft_smem_t()
-{
-    const int bytes = kFftSmemBytes;
-    cudaError_t e;
-    if ((e = cudaFuncSetAttribute(fft_xf_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
-    if ((e = cudaFuncSetAttribute(fft_y_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
-    if ((e = cudaFuncSetAttribute(fft_z_conv_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes))) return e;
-    if ((e = cudaFuncSetAttribute(fft_xi_kernel<C, typename CxT<C>::R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  bytes)))
-        return e;
-    return cudaSuccess;
-}
-
-static cudaError_t set_fft_smem()
-{
-    static bool done = false;
-    if (done) return cudaSuccess;
-    cudaError_t e;
-    if ((e = set_fft_smem_t<double2>())) return e;
-    if ((e = set_fft_smem_t<float2>())) return e;
-    if ((e = cudaFuncSetAttribute(fft_green_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kFftSmemBytes)))
-        return e;
-    done = true;
-    return cudaSuccess;
-}
-
 static inline int ceil_div64(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// Dynamic shared memory of an FFT pass kernel (above 48 KB for L >= 512):
+// raised once per kernel instantiation.
+template <typename KERN>
+static cudaError_t fft_smem(KERN* k, int bytes)
+{
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+#define SB2_FFT_LENGTHS(X) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048)
+
+template <int L>
+static cudaError_t green_passes_axis0(double* G, const double2* tw, int ox, int oy, int oz, const ScState* sc,
+                                      cudaStream_t s)
+{
+    typedef fft::XMajor<L> LAY;
+    const int bytes = LAY::kSmemElems * 16;
+    static cudaError_t once = fft_smem(fft_green_kernel<L, 0>, bytes);
+    if (once) return once;
+    const int64_t pairs = ((int64_t)oy * oz + 1) / 2;
+    fft_green_kernel<L, 0><<<ceil_div64(pairs, fft::Shape<L>::W), fft::Shape<L>::THREADS, bytes, s>>>(G, tw, ox, oy, oz, sc);
+    return cudaSuccess;
+}
+template <int L, int AXIS>
+static cudaError_t green_passes_lmajor(double* G, const double2* tw, int ox, int oy, int oz, const ScState* sc,
+                                       cudaStream_t s)
+{
+    typedef fft::LMajor<L> LAY;
+    const int bytes = LAY::kSmemElems * 16;
+    static cudaError_t once = fft_smem(fft_green_kernel<L, AXIS>, bytes);
+    if (once) return once;
+    const int64_t nlines = AXIS == 1 ? (int64_t)ox * oz : (int64_t)ox * oy;
+    fft_green_kernel<L, AXIS><<<ceil_div64((nlines + 1) / 2, fft::Shape<L>::W), fft::Shape<L>::THREADS, bytes, s>>>(
+        G, tw, ox, oy, oz, sc);
+    return cudaSuccess;
+}
 
 // Ghat from the current domain: octant G, then the three even-line passes.
 cudaError_t launch_green(const ScState* sc, double* G, const Dims& d, int linear, const double2* tw_x,
                          const double2* tw_y, const double2* tw_z, cudaStream_t s)
 {
-    cudaError_t e = set_fft_smem();
-    if (e) return e;
     const int ox = d.nx / 2 + 1, oy = d.ny / 2 + 1, oz = d.nz / 2 + 1;
     green_octant_kernel<<<sm_count() * 4, 256, 0, s>>>(sc, G, d.gx, d.gy, d.gz, linear);
-    const size_t sh = kFftSmemBytes;
-    // one CTA per kFftTile / L line pairs
-    fft_green_kernel<<<ceil_div64(((int64_t)oy * oz + 1) / 2, kFftTile / d.nx), kFftThreads, sh, s>>>(
-        G, tw_x, 0, d.nx, ox, oy, oz, sc);
-    fft_green_kernel<<<ceil_div64(((int64_t)ox * oz + 1) / 2, kFftTile / d.ny), kFftThreads, sh, s>>>(
-        G, tw_y, 1, d.ny, ox, oy, oz, sc);
-    fft_green_kernel<<<ceil_div64(((int64_t)ox * oy + 1) / 2, kFftTile / d.nz), kFftThreads, sh, s>>>(
-        G, tw_z, 2, d.nz, ox, oy, oz, sc);
+    cudaError_t e = cudaSuccess;
+#define SB2_G0(LL) case LL: e = green_passes_axis0<LL>(G, tw_x, ox, oy, oz, sc, s); break;
+#define SB2_G1(LL) case LL: e = green_passes_lmajor<LL, 1>(G, tw_y, ox, oy, oz, sc, s); break;
+#define SB2_G2(LL) case LL: e = green_passes_lmajor<LL, 2>(G, tw_z, ox, oy, oz, sc, s); break;
+    switch (d.nx) { SB2_FFT_LENGTHS(SB2_G0) default: return cudaErrorInvalidValue; }
+    if (e) return e;
+    switch (d.ny) { SB2_FFT_LENGTHS(SB2_G1) default: return cudaErrorInvalidValue; }
+    if (e) return e;
+    switch (d.nz) { SB2_FFT_LENGTHS(SB2_G2) default: return cudaErrorInvalidValue; }
+    if (e) return e;
+#undef SB2_G0
+#undef SB2_G1
+#undef SB2_G2
     return cudaGetLastError();
+}
+
+template <int L, typename C>
+static cudaError_t pass_xf(const double* rho, C* S, const double2* tw, const Dims& d, const ScState* sc, cudaStream_t s)
+{
+    const int bytes = fft::XMajor<L>::kSmemElems * 16;
+    static cudaError_t once = fft_smem(fft_xf_kernel<L, C>, bytes);
+    if (once) return once;
+    const int64_t nlines = (int64_t)((d.gy + 1) / 2) * d.gz;
+    fft_xf_kernel<L, C><<<ceil_div64(nlines, fft::Shape<L>::W), fft::Shape<L>::THREADS, bytes, s>>>(rho, S, tw, d, sc);
+    return cudaSuccess;
+}
+template <int L, typename C, bool INV>
+static cudaError_t pass_y(C* S, const double2* tw, const Dims& d, const ScState* sc, cudaStream_t s)
+{
+    const int bytes = fft::LMajor<L>::kSmemElems * 16;
+    static cudaError_t once = fft_smem(fft_y_kernel<L, C, INV>, bytes);
+    if (once) return once;
+    dim3 grid(ceil_div64(d.nkx, fft::Shape<L>::W), d.gz);
+    fft_y_kernel<L, C, INV><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, tw, d, sc);
+    return cudaSuccess;
+}
+template <int L, typename C>
+static cudaError_t pass_z(C* S, const double* Ghat, const double2* tw, const Dims& d, const ScState* sc, cudaStream_t s)
+{
+    const int bytes = fft::LMajor<L>::kSmemElems * 16;
+    static cudaError_t once = fft_smem(fft_z_conv_kernel<L, C>, bytes);
+    if (once) return once;
+    dim3 grid(ceil_div64(d.nkx, fft::Shape<L>::W), d.ny);
+    fft_z_conv_kernel<L, C><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, Ghat, tw, d, sc);
+    return cudaSuccess;
+}
+template <int L, typename C>
+static cudaError_t pass_xi(const C* S, typename CxT<C>::R* phi, const double2* tw, const Dims& d, const ScState* sc,
+                           cudaStream_t s)
+{
+    typedef typename CxT<C>::R RO;
+    const int bytes = fft::XMajor<L>::kSmemElems * 16;
+    static cudaError_t once = fft_smem(fft_xi_kernel<L, C, RO>, bytes);
+    if (once) return once;
+    const int64_t nlines = (int64_t)((d.gy + 1) / 2) * d.gz;
+    fft_xi_kernel<L, C, RO><<<ceil_div64(nlines, fft::Shape<L>::W), fft::Shape<L>::THREADS, bytes, s>>>(S, phi, tw, d,
+                                                                                                       sc);
+    return cudaSuccess;
 }
 
 template <typename C>
@@ -806,16 +732,27 @@ static cudaError_t convolve_t(const double* rho, C* S, const double* Ghat, typen
                               const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
                               cudaStream_t s)
 {
-    cudaError_t e = set_fft_smem();
+    cudaError_t e = cudaSuccess;
+#define SB2_XF(LL) case LL: e = pass_xf<LL, C>(rho, S, tw_x, d, sc, s); break;
+#define SB2_YF(LL) case LL: e = pass_y<LL, C, false>(S, tw_y, d, sc, s); break;
+#define SB2_ZC(LL) case LL: e = pass_z<LL, C>(S, Ghat, tw_z, d, sc, s); break;
+#define SB2_YI(LL) case LL: e = pass_y<LL, C, true>(S, tw_y, d, sc, s); break;
+#define SB2_XI(LL) case LL: e = pass_xi<LL, C>(S, phi, tw_x, d, sc, s); break;
+    switch (d.nx) { SB2_FFT_LENGTHS(SB2_XF) default: return cudaErrorInvalidValue; }
     if (e) return e;
-    const size_t sh = kFftSmemBytes;
-    const int npy = (d.gy + 1) / 2;
-    fft_xf_kernel<C><<<ceil_div64((int64_t)npy * d.gz, kFftTile / d.nx), kFftThreads, sh, s>>>(rho, S, tw_x, d, sc);
-    fft_y_kernel<C><<<ceil_div64((int64_t)d.nkx * d.gz, kFftTile / d.ny), kFftThreads, sh, s>>>(S, tw_y, d, 0, sc);
-    fft_z_conv_kernel<C><<<ceil_div64((int64_t)d.nkx * d.ny, kFftTile / d.nz), kFftThreads, sh, s>>>(S, Ghat, tw_z, d, sc);
-    fft_y_kernel<C><<<ceil_div64((int64_t)d.nkx * d.gz, kFftTile / d.ny), kFftThreads, sh, s>>>(S, tw_y, d, 1, sc);
-    fft_xi_kernel<C, typename CxT<C>::R>
-        <<<ceil_div64((int64_t)npy * d.gz, kFftTile / d.nx), kFftThreads, sh, s>>>(S, phi, tw_x, d, sc);
+    switch (d.ny) { SB2_FFT_LENGTHS(SB2_YF) default: return cudaErrorInvalidValue; }
+    if (e) return e;
+    switch (d.nz) { SB2_FFT_LENGTHS(SB2_ZC) default: return cudaErrorInvalidValue; }
+    if (e) return e;
+    switch (d.ny) { SB2_FFT_LENGTHS(SB2_YI) default: return cudaErrorInvalidValue; }
+    if (e) return e;
+    switch (d.nx) { SB2_FFT_LENGTHS(SB2_XI) default: return cudaErrorInvalidValue; }
+    if (e) return e;
+#undef SB2_XF
+#undef SB2_YF
+#undef SB2_ZC
+#undef SB2_YI
+#undef SB2_XI
     return cudaGetLastError();
 }
 
