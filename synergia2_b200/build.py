@@ -2,10 +2,12 @@
 
     python -m synergia2_b200.build          # or: python synergia2_b200/build.py
 
-CUDA units are compiled with --fmad=false (the FP64 path keeps IEEE
-rounding of every multiply and add, as the reference does), except
-track_fast.cu, the mixed-precision path's particle passes, which fuses
-multiply-adds; the host runtime with -ffp-contract=off.  The CUDA runtime is
+The particle maps of the FP64 path (track.cu) are compiled with
+--fmad=false: they keep the IEEE rounding of every multiply and add, as the
+reference does, and match the oracle bit for bit.  The mixed path's
+particle passes (track_fast.cu) and the solver (sc3d.cu, held to
+tolerances) fuse multiply-adds.  The host runtime is built with
+-ffp-contract=off.  The CUDA runtime is
 linked statically so the library loads without a CUDA toolkit on the
 loader path.
 """
@@ -22,7 +24,10 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["track.cu", "track_fast.cu", "sc3d.cu", "sort.cu", "noalloc.cu"]
-FMAD = {"track_fast.cu": "--fmad=true"}
+# fused multiply-adds where the results are held to tolerances, not bits:
+# the mixed path's particle passes and the solver (fields within 1e-10 of
+# the oracle; the FFTs of the reference's own FFT libraries fuse as well)
+FMAD = {"track_fast.cu": "--fmad=true", "sc3d.cu": "--fmad=true"}
 CXX_SOURCES = ["host.cc"]
 
 

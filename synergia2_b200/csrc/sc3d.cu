@@ -1,4 +1,4 @@
-// 3D open-boundary Hockney solver kernels for sm_100a (FP64 path).
+// 3D open-boundary Hockney solver kernels for sm_100a.
 //
 // Layouts in HBM (x fastest everywhere):
 //   rho, phi   dense real (gz, gy, gx) on the original grid
@@ -13,9 +13,9 @@
 // that skip the zero padding: x (pairs of real rows packed as one complex
 // FFT), y (first gy inputs), z forward + Ghat multiply + z inverse in one
 // kernel (first gz inputs, first gz outputs), y inverse (first gy outputs),
-// x inverse (Hermitian pairs, first gx outputs).  Each pass stages a tile of
-// lines in shared memory and runs a Stockham transform there with radix-8/4/2
-// butterflies in registers.
+// x inverse (Hermitian pairs, first gx outputs).  Each pass holds its lines
+// in registers and runs a Stockham transform with radix-8/4/2 butterflies,
+// exchanging values between radix passes through shared memory (fft.cuh).
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <type_traits>
