@@ -119,12 +119,14 @@ __host__ __device__ constexpr int first_radix() { return radix_at<L, REV>(0); }
 template <int L, bool REV>
 __host__ __device__ constexpr int last_radix() { return radix_at<L, REV>(npasses(L) - 1); }
 
-// CTA shape for length L: 256 threads up to L = 256, 512 beyond; W lines.
+// CTA shape for length L: 256 threads up to L = 512 (two CTAs per SM at the
+// pass kernels' ~110 registers, so one CTA's loads overlap another's
+// arithmetic), 512 beyond; W lines.
 template <int L>
 struct Shape {
     static_assert(L >= 8 && L <= 2048 && (L & (L - 1)) == 0, "FFT length");
     static constexpr int TPL = L / kE;                                   // threads per line
-    static constexpr int THREADS = L <= 256 ? 256 : 512;
+    static constexpr int THREADS = L <= 512 ? 256 : 512;
     static constexpr int W = THREADS / TPL;                              // lines per CTA
     static constexpr int PITCH = L + L / 8;                              // x-major line pitch (skewed)
 };

@@ -238,67 +238,76 @@ __global__ void __launch_bounds__(256) deposit_kernel(const double* __restrict__
 // evaluated for ix <= gx, iy <= gy, iz <= gz (doubled shape = 2 * shape,
 // so this octant plus mirroring is the whole doubled-grid G2)
 // ---------------------------------------------------------------------------
+// Linear (z-integrated) Green function on the octant, one chunk of a z
+// column per thread.  With s(k) = sqrt(x^2 + y^2 + (k hz)^2) and P(k) =
+// s(k) + k hz, the reference's per-point terms are
+//   2 s(k) - s(k-1) - s(k+1) + (hz - z) log(P(k)/P(k-1)) + (hz + z) log(P(k+1)/P(k))
+// (alg_g2_linear, space_charge_3d_open_hockney.cc:237-348, z = k hz >= 0 on
+// the octant; k = 0 and k = 1 take the reference's special cases), so along
+// a column every square root and every logarithm is shared by neighbouring
+// points: one sqrt and one log per point instead of three and two.
+constexpr int kGreenChunk = 16;
+
 __global__ void green_octant_kernel(const ScState* __restrict__ scp, double* G, int gx0, int gy0, int gz0,
                                     int linear)
 {
     const ScState& sc = *scp;
     if (!sc.valid) return;
     const int ox = gx0 + 1, oy = gy0 + 1, oz = gz0 + 1;
-    const int64_t total = (int64_t)ox * oy * oz;
     const double hx = sc.dh[0], hy = sc.dh[1], hz = sc.dh[2];
+    if (!linear) { // alg_g2_pointlike :136-180
+        const int64_t total = (int64_t)ox * oy * oz;
+        const double G000 = 2.8 / fmin(hx, fmin(hy, hz));
+        for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+             t += (int64_t)gridDim.x * blockDim.x) {
+            const int ix = (int)(t % ox);
+            const int iy = (int)((t / ox) % oy);
+            const int iz = (int)(t / ((int64_t)ox * oy));
+            const double dx = ix * hx, dy = iy * hy, dz = iz * hz;
+            G[t] = (ix == 0 && iy == 0 && iz == 0) ? G000 : 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
+        }
+        return;
+    }
+    const double rr0 = hx * hx + hy * hy;
+    const double r10 = sqrt(hx * hx + hy * hy + hz * hz);
+    const double G000 = (2.0 / rr0) * (hz * r10 + rr0 * log((hz + r10) / sqrt(rr0)) - hz * hz);
+    const double epsz = 1e-12 * hz;
+    const int nchunks = (oz + kGreenChunk - 1) / kGreenChunk;
+    const int64_t total = (int64_t)ox * oy * nchunks;
+    const int64_t plane = (int64_t)ox * oy;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
          t += (int64_t)gridDim.x * blockDim.x) {
-        int ix = (int)(t % ox);
-        int iy = (int)((t / ox) % oy);
-        int iz = (int)(t / ((int64_t)ox * oy));
-        double Gv;
-        if (!linear) {
-            double G000 = 2.8 / fmin(hx, fmin(hy, hz));
-            double dx = ix * hx, dy = iy * hy, dz = iz * hz;
-            Gv = (ix == 0 && iy == 0 && iz == 0) ? G000 : 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
-        } else {
-            double rr0 = hx * hx + hy * hy;
-            double r10 = sqrt(hx * hx + hy * hy + hz * hz);
-            double G000 = (2.0 / rr0) * (hz * r10 + rr0 * log((hz + r10) / sqrt(rr0)) - hz * hz);
-            double z = iz * hz; // iz <= gz0
-            double y = iy * hy, x = ix * hx;
-            double rr = x * x + y * y;
-            double s0 = sqrt(rr + z * z);
-            double sn = sqrt(rr + (z - hz) * (z - hz));
-            double sp = sqrt(rr + (z + hz) * (z + hz));
-            Gv = 2.0 * s0 - sn - sp;
-            const double epsz = 1e-12 * hz;
-            double T1, T2, r1, r2;
-            if (z < -hz) {
-                r1 = (sn - z + hz) / (s0 - z);
-                T1 = (hz - z) * log(r1);
-                r2 = (s0 - z) / (sp - z - hz);
-                T2 = (hz + z) * log(r2);
-                Gv += T1 + T2;
-            } else if (fabs(z + hz) < epsz) {
-                r1 = (sn - z + hz) / (s0 - z);
-                T1 = (hz - z) * log(r1);
-                Gv += T1;
-            } else if (fabs(z) < epsz) {
-                if (fabs(x) + fabs(y) < 2. * epsz) {
+        const int ix = (int)(t % ox);
+        const int iy = (int)((t / ox) % oy);
+        const int c = (int)(t / plane);
+        const int k0 = c * kGreenChunk, k1 = min(oz, k0 + kGreenChunk);
+        const double x = ix * hx, y = iy * hy;
+        const double rr = x * x + y * y;
+        auto sk = [&](int k) { const double z = k * hz; return sqrt(rr + z * z); };
+        double s_m = sk(k0 - 1), s_0 = sk(k0), s_p = sk(k0 + 1);
+        // log(P(k0)/P(k0-1)), needed from k0 >= 2 on
+        double lr_m = k0 >= 2 ? log((s_0 + k0 * hz) / (s_m + (k0 - 1) * hz)) : 0.0;
+        double* out = G + (int64_t)iy * ox + ix;
+        for (int k = k0; k < k1; ++k) {
+            const double z = k * hz;
+            const double lr_p = log((s_p + (k + 1) * hz) / (s_0 + z)); // log(P(k+1)/P(k))
+            double Gv = 2.0 * s_0 - s_m - s_p;
+            if (k == 0) {
+                if (fabs(x) + fabs(y) < 2. * epsz)
                     Gv += hz * G000;
-                } else {
-                    r1 = (sqrt(hz * hz + rr) + hz) / sqrt(rr);
-                    Gv += 2.0 * hz * log(r1);
-                }
-            } else if (fabs(z - hz) < epsz) {
-                r1 = (sp + z + hz) / (s0 + z);
-                T1 = (hz + z) * log(r1);
-                Gv += T1;
-            } else if (z > hz) {
-                r1 = (s0 + z) / (sn + z - hz);
-                T1 = (hz - z) * log(r1);
-                r2 = (sp + z + hz) / (s0 + z);
-                T2 = (hz + z) * log(r2);
-                Gv += T1 + T2;
+                else
+                    Gv += 2.0 * hz * log((sqrt(hz * hz + rr) + hz) / sqrt(rr));
+            } else if (k == 1) {
+                Gv += (hz + z) * lr_p;
+            } else {
+                Gv += (hz - z) * lr_m + (hz + z) * lr_p;
             }
+            out[(int64_t)k * plane] = Gv;
+            s_m = s_0;
+            s_0 = s_p;
+            s_p = sk(k + 2);
+            lr_m = lr_p;
         }
-        G[t] = Gv;
     }
 }
 
