@@ -511,8 +511,38 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
 // PPT particles per thread travel through the op list together, so their
 // independent load and arithmetic chains overlap (more bytes in flight per
 // thread for the memory-bound passes).
-template <int VARIANT, int PPT>
-__global__ void __launch_bounds__(kTrackThreads, TrackOcc<VARIANT>::value)
+// Raw values of one particle as loaded: six coordinates and the mask.
+struct RawPart {
+    double c[6];
+    uint8_t m;
+};
+
+// The mask and the six columns are loaded together (no load waits on the
+// mask), so all seven requests of a particle are in flight at once; lost
+// particles' values are read and ignored.
+template <int PPT>
+__device__ __forceinline__ void load_tile(const TrackParams& p, int64_t base, RawPart* r)
+{
+    const int64_t n = p.n, S = p.stride;
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) {
+        const int64_t i = base + q * blockDim.x + threadIdx.x;
+        r[q].m = 0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) r[q].c[j] = 0.0;
+        if (i < n) {
+            r[q].m = p.masks[i];
+#pragma unroll
+            for (int j = 0; j < 6; ++j) r[q].c[j] = p.parts[i + j * S];
+        }
+    }
+}
+
+// PF: the next tile's loads are issued before the current tile is computed
+// (memory-bound passes: the loads of one tile overlap the arithmetic of the
+// previous one).
+template <int VARIANT, int PPT, bool PF>
+__global__ void __launch_bounds__(kTrackThreads, PF ? 2 : TrackOcc<VARIANT>::value)
     track_kernel(const __grid_constant__ TrackParams p)
 {
     __shared__ int s_counts[kMaxOpsPerPass];
@@ -525,31 +555,29 @@ __global__ void __launch_bounds__(kTrackThreads, TrackOcc<VARIANT>::value)
     const int64_t n = p.n;
     const int64_t S = p.stride;
     const int64_t tile = (int64_t)blockDim.x * PPT;
-    for (int64_t base = blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
+    const int64_t gstride = (int64_t)gridDim.x * tile;
+    RawPart nxt[PPT];
+    if (PF && (int64_t)blockIdx.x * tile < n) load_tile<PPT>(p, (int64_t)blockIdx.x * tile, nxt);
+    for (int64_t base = blockIdx.x * tile; base < n; base += gstride) {
+        RawPart cur[PPT];
+        if (PF) {
+#pragma unroll
+            for (int q = 0; q < PPT; ++q) cur[q] = nxt[q];
+            if (base + gstride < n) load_tile<PPT>(p, base + gstride, nxt);
+        } else {
+            load_tile<PPT>(p, base, cur);
+        }
         Part P[PPT];
         bool in[PPT];
-        // the mask and the six columns are loaded together (no load waits
-        // on the mask), so all seven requests of every particle are in
-        // flight at once; lost particles' values are read and ignored
-        uint8_t mk[PPT];
 #pragma unroll
         for (int q = 0; q < PPT; ++q) {
-            const int64_t i = base + q * blockDim.x + threadIdx.x;
-            mk[q] = 0;
-            P[q].x = P[q].xp = P[q].y = P[q].yp = P[q].cdt = P[q].dpop = 0.0;
-            if (i < n) {
-                mk[q] = p.masks[i];
-                P[q].x = p.parts[i];
-                P[q].xp = p.parts[i + S];
-                P[q].y = p.parts[i + 2 * S];
-                P[q].yp = p.parts[i + 3 * S];
-                P[q].cdt = p.parts[i + 4 * S];
-                P[q].dpop = p.parts[i + 5 * S];
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < PPT; ++q) {
-            P[q].alive = mk[q] != 0;
+            P[q].x = cur[q].c[0];
+            P[q].xp = cur[q].c[1];
+            P[q].y = cur[q].c[2];
+            P[q].yp = cur[q].c[3];
+            P[q].cdt = cur[q].c[4];
+            P[q].dpop = cur[q].c[5];
+            P[q].alive = cur[q].m != 0;
             in[q] = P[q].alive;
             P[q].disc = 0;
         }
@@ -615,15 +643,36 @@ static int full_variant()
     return v;
 }
 
+// Shape of the light pass: particles per thread and prefetching
+// (SB2_TRACK_LIGHT = 2: two per thread; 1p / 2p: one / two per thread with
+// the next tile prefetched).
+static int light_shape()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("SB2_TRACK_LIGHT");
+        v = 0;
+        if (e && e[0] == '1' && e[1] == 'p') v = 1;
+        if (e && e[0] == '2' && e[1] == 'p') v = 2;
+    }
+    return v;
+}
+
 cudaError_t launch_pass(const TrackParams& p, cudaStream_t s)
 {
     int nb = track_grid_blocks();
-    if (!track_needs_full(p.ops, p.nops))
-        track_kernel<TRACK_LIGHT, 2><<<nb, kTrackThreads, 0, s>>>(p);
-    else if (full_variant() == TRACK_FULL_WIDE)
-        track_kernel<TRACK_FULL_WIDE, 1><<<nb, kTrackThreads, 0, s>>>(p);
+    if (!track_needs_full(p.ops, p.nops)) {
+        const int shape = light_shape();
+        if (shape == 1)
+            track_kernel<TRACK_LIGHT, 1, true><<<nb, kTrackThreads, 0, s>>>(p);
+        else if (shape == 2)
+            track_kernel<TRACK_LIGHT, 2, true><<<nb, kTrackThreads, 0, s>>>(p);
+        else
+            track_kernel<TRACK_LIGHT, 2, false><<<nb, kTrackThreads, 0, s>>>(p);
+    } else if (full_variant() == TRACK_FULL_WIDE)
+        track_kernel<TRACK_FULL_WIDE, 1, false><<<nb, kTrackThreads, 0, s>>>(p);
     else
-        track_kernel<TRACK_FULL, 1><<<nb, kTrackThreads, 0, s>>>(p);
+        track_kernel<TRACK_FULL, 1, false><<<nb, kTrackThreads, 0, s>>>(p);
     return cudaGetLastError();
 }
 
