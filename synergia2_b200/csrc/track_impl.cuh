@@ -21,6 +21,7 @@
 // particle per thread, 32 consecutive particles per warp per column).
 #pragma once
 #include <cuda_runtime.h>
+#include <climits>
 #include <cstdint>
 #include <cstdlib>
 
@@ -310,6 +311,109 @@ struct Part {
     int disc;
 };
 
+// Field corners for the kick.  Corner c of a cell is read as (ex, ey, ez);
+// FP64: two double2 per cell {ex, ey | ez, 0}; mixed: one float4.
+struct Corner {
+    double x, y, z;
+};
+struct GlobalField {
+    const TrackParams& p;
+    __device__ __forceinline__ void load(int64_t c, Corner& v) const
+    {
+        if (p.efield32) {
+            const float4 f = p.efield32[c];
+            v.x = f.x;
+            v.y = f.y;
+            v.z = f.z;
+        } else {
+            const double2 a = p.efield[2 * c];
+            v.x = a.x;
+            v.y = a.y;
+            v.z = p.efield[2 * c + 1].x;
+        }
+    }
+    // corner c (x fastest, then y, then z) of cell (ix, iy, iz)
+    __device__ __forceinline__ void corner(int ix, int iy, int iz, int c, Corner& v) const
+    {
+        const int gx = p.gx, gy = p.gy;
+        load(((int64_t)(iz + (c >> 2)) * gy + iy + ((c >> 1) & 1)) * gx + ix + (c & 1), v);
+    }
+};
+
+// Field of the cells a tile of particles needs, staged in shared memory
+// (box origin o0..o2, extents n0 x n1; cell c of the box at (dz n1 + dy) n0 +
+// dx): corners read from shared memory instead of L2.
+constexpr int kBoxCells = 1024;
+struct BoxField {
+    const TrackParams& p;
+    const double2* box; // FP64: 2 per cell; mixed: reinterpreted as float4
+    int o0, o1, o2, n0, n1;
+    __device__ __forceinline__ void load(int l, Corner& v) const
+    {
+        if (p.efield32) {
+            const float4 f = reinterpret_cast<const float4*>(box)[l];
+            v.x = f.x;
+            v.y = f.y;
+            v.z = f.z;
+        } else {
+            const double2 a = box[2 * l];
+            v.x = a.x;
+            v.y = a.y;
+            v.z = box[2 * l + 1].x;
+        }
+    }
+    __device__ __forceinline__ void corner(int ix, int iy, int iz, int c, Corner& v) const
+    {
+        load(((iz - o2 + (c >> 2)) * n1 + (iy - o1 + ((c >> 1) & 1))) * n0 + (ix - o0 + (c & 1)), v);
+    }
+};
+
+// zyx::alg_kicker space_charge_3d_kernels.h:91-215: trilinear interpolation
+// of E at the particle and the kick of xp, yp, dpop.  F::corners supplies
+// the field at the cell's 8 corners (from global memory, or from a box
+// staged in shared memory); the arithmetic is the same either way.
+template <class F>
+__device__ __forceinline__ void sc_kick(const TrackParams& p, Part& P, const F& field)
+{
+    const ScState& sc = *p.sc;
+    if (!sc.valid) return;
+    int ix, iy, iz;
+    double ox, oy, oz;
+    leftmost(P.x, sc.left[0], sc.ih[0], ix, ox);
+    leftmost(P.y, sc.left[1], sc.ih[1], iy, oy);
+    leftmost(P.cdt, sc.left[2], sc.ih[2], iz, oz);
+    const int gx = p.gx, gy = p.gy, gz = p.gz;
+    if (!((ix >= 0 && ix < gx - 1) && (iy >= 0 && iy < gy - 1) && (iz >= 0 && iz < gz - 1))) return;
+    const double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
+    // each component sums the corners in the reference's order (x fastest,
+    // then y, then z), one corner at a time
+    const double wz[2] = {aoz, oz}, wy[2] = {aoy, oy}, wx[2] = {aox, ox};
+    double vx = 0.0, vy = 0.0, vz = 0.0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        Corner f;
+        field.corner(ix, iy, iz, c, f);
+        const double w = wz[c >> 2] * wy[(c >> 1) & 1] * wx[c & 1];
+        if (c == 0) {
+            vz = w * f.z;
+            vy = w * f.y;
+            vx = w * f.x;
+        } else {
+            vz += w * f.z;
+            vy += w * f.y;
+            vx += w * f.x;
+        }
+    }
+    const double factor = sc.factor, pref = p.kick_pref, m = p.kick_m;
+    double pp = pref + P.dpop * pref;
+    double Eoc_i = sqrt(pp * pp + m * m);
+    double Eoc_f = Eoc_i + factor * (-pref) * vz;
+    double ddp = (sqrt(Eoc_f * Eoc_f - m * m) - sqrt(Eoc_i * Eoc_i - m * m)) / pref;
+    P.dpop += ddp;
+    P.yp += factor * vy;
+    P.xp += factor * vx;
+}
+
 // Applies one op to one particle (apertures, moments and maps).
 template <int VARIANT>
 __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, Part& P, int* s_counts,
@@ -422,87 +526,9 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
             if constexpr (kFull) sbend_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
             break;
         }
-        case OP_SC_KICK: {
-            // zyx::alg_kicker space_charge_3d_kernels.h:91-215
-            const ScState& sc = *p.sc;
-            if (!sc.valid) break;
-            int ix, iy, iz;
-            double ox, oy, oz;
-            leftmost(x, sc.left[0], sc.ih[0], ix, ox);
-            leftmost(y, sc.left[1], sc.ih[1], iy, oy);
-            leftmost(cdt, sc.left[2], sc.ih[2], iz, oz);
-            const int gx = p.gx, gy = p.gy, gz = p.gz;
-            if (!((ix >= 0 && ix < gx - 1) && (iy >= 0 && iy < gy - 1) && (iz >= 0 && iz < gz - 1)))
-                break;
-            double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
-            const int64_t b0 = ((int64_t)iz * gy + iy) * gx + ix;
-            const int64_t b1 = ((int64_t)(iz + 1) * gy + iy) * gx + ix;
-            if (p.efield32) {
-                // mixed precision: FP32 field, one 16-byte load per corner,
-                // interpolation weights and the kick in FP64
-                const float4* F = p.efield32;
-                const float4 f000 = F[b0], f001 = F[b0 + 1], f010 = F[b0 + gx], f011 = F[b0 + gx + 1];
-                const float4 f100 = F[b1], f101 = F[b1 + 1], f110 = F[b1 + gx], f111 = F[b1 + gx + 1];
-                const double w000 = aoz * aoy * aox, w001 = aoz * aoy * ox, w010 = aoz * oy * aox,
-                             w011 = aoz * oy * ox, w100 = oz * aoy * aox, w101 = oz * aoy * ox,
-                             w110 = oz * oy * aox, w111 = oz * oy * ox;
-                const double factor = sc.factor, pref = p.kick_pref, m = p.kick_m;
-                double val = w000 * f000.z + w001 * f001.z + w010 * f010.z + w011 * f011.z + w100 * f100.z +
-                             w101 * f101.z + w110 * f110.z + w111 * f111.z;
-                double pp = pref + dpop * pref;
-                double Eoc_i = sqrt(pp * pp + m * m);
-                double Eoc_f = Eoc_i + factor * (-pref) * val;
-                dpop += (sqrt(Eoc_f * Eoc_f - m * m) - sqrt(Eoc_i * Eoc_i - m * m)) / pref;
-                val = w000 * f000.y + w001 * f001.y + w010 * f010.y + w011 * f011.y + w100 * f100.y +
-                      w101 * f101.y + w110 * f110.y + w111 * f111.y;
-                yp += factor * val;
-                val = w000 * f000.x + w001 * f001.x + w010 * f010.x + w011 * f011.x + w100 * f100.x +
-                      w101 * f101.x + w110 * f110.x + w111 * f111.x;
-                xp += factor * val;
-                break;
-            }
-            const double2* E = p.efield;
-            // corner fields: .x/.y of [2c] = ex, ey; .x of [2c+1] = ez
-            double2 a00 = E[2 * b0], a01 = E[2 * (b0 + 1)], a10 = E[2 * (b0 + gx)], a11 = E[2 * (b0 + gx + 1)];
-            double2 c00 = E[2 * b1], c01 = E[2 * (b1 + 1)], c10 = E[2 * (b1 + gx)], c11 = E[2 * (b1 + gx + 1)];
-            double z00 = E[2 * b0 + 1].x, z01 = E[2 * (b0 + 1) + 1].x, z10 = E[2 * (b0 + gx) + 1].x,
-                   z11 = E[2 * (b0 + gx + 1) + 1].x;
-            double w00 = E[2 * b1 + 1].x, w01 = E[2 * (b1 + 1) + 1].x, w10 = E[2 * (b1 + gx) + 1].x,
-                   w11 = E[2 * (b1 + gx + 1) + 1].x;
-            const double factor = sc.factor, pref = p.kick_pref, m = p.kick_m;
-            double val = aoz * aoy * aox * z00;
-            val += aoz * aoy * ox * z01;
-            val += aoz * oy * aox * z10;
-            val += aoz * oy * ox * z11;
-            val += oz * aoy * aox * w00;
-            val += oz * aoy * ox * w01;
-            val += oz * oy * aox * w10;
-            val += oz * oy * ox * w11;
-            double pp = pref + dpop * pref;
-            double Eoc_i = sqrt(pp * pp + m * m);
-            double Eoc_f = Eoc_i + factor * (-pref) * val;
-            double ddp = (sqrt(Eoc_f * Eoc_f - m * m) - sqrt(Eoc_i * Eoc_i - m * m)) / pref;
-            dpop += ddp;
-            val = aoz * aoy * aox * a00.y;
-            val += aoz * aoy * ox * a01.y;
-            val += aoz * oy * aox * a10.y;
-            val += aoz * oy * ox * a11.y;
-            val += oz * aoy * aox * c00.y;
-            val += oz * aoy * ox * c01.y;
-            val += oz * oy * aox * c10.y;
-            val += oz * oy * ox * c11.y;
-            yp += factor * val;
-            val = aoz * aoy * aox * a00.x;
-            val += aoz * aoy * ox * a01.x;
-            val += aoz * oy * aox * a10.x;
-            val += aoz * oy * ox * a11.x;
-            val += oz * aoy * aox * c00.x;
-            val += oz * aoy * ox * c01.x;
-            val += oz * oy * aox * c10.x;
-            val += oz * oy * ox * c11.x;
-            xp += factor * val;
+        case OP_SC_KICK:
+            sc_kick(p, P, GlobalField{p});
             break;
-        }
         default:
             break;
         }
@@ -511,6 +537,90 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
 // PPT particles per thread travel through the op list together, so their
 // independent load and arithmetic chains overlap (more bytes in flight per
 // thread for the memory-bound passes).
+// Kick of a tile with its field staged in shared memory: the bounding box of
+// the corner cells of the tile's particles (block-wide min/max), the box's
+// field copied in (rows along x, coalesced), then every particle's kick from
+// the box -- or from global memory when the box exceeds kBoxCells.  Called
+// by all threads of the block.
+template <int PPT>
+__device__ __forceinline__ void stage_and_kick(const TrackParams& p, Part* P, double2* s_box, int (*s_red)[6])
+{
+    const ScState& sc = *p.sc;
+    const int gx = p.gx, gy = p.gy, gz = p.gz;
+    int lo0 = INT_MAX, lo1 = INT_MAX, lo2 = INT_MAX, hi0 = INT_MIN, hi1 = INT_MIN, hi2 = INT_MIN;
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) {
+        if (!P[q].alive) continue;
+        int ix, iy, iz;
+        double o;
+        leftmost(P[q].x, sc.left[0], sc.ih[0], ix, o);
+        leftmost(P[q].y, sc.left[1], sc.ih[1], iy, o);
+        leftmost(P[q].cdt, sc.left[2], sc.ih[2], iz, o);
+        if ((ix >= 0 && ix < gx - 1) && (iy >= 0 && iy < gy - 1) && (iz >= 0 && iz < gz - 1)) {
+            lo0 = min(lo0, ix);
+            lo1 = min(lo1, iy);
+            lo2 = min(lo2, iz);
+            hi0 = max(hi0, ix);
+            hi1 = max(hi1, iy);
+            hi2 = max(hi2, iz);
+        }
+    }
+    const unsigned full = 0xffffffffu;
+    lo0 = __reduce_min_sync(full, lo0);
+    lo1 = __reduce_min_sync(full, lo1);
+    lo2 = __reduce_min_sync(full, lo2);
+    hi0 = __reduce_max_sync(full, hi0);
+    hi1 = __reduce_max_sync(full, hi1);
+    hi2 = __reduce_max_sync(full, hi2);
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        s_red[w][0] = lo0;
+        s_red[w][1] = lo1;
+        s_red[w][2] = lo2;
+        s_red[w][3] = hi0;
+        s_red[w][4] = hi1;
+        s_red[w][5] = hi2;
+    }
+    __syncthreads();
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+        lo0 = min(lo0, s_red[k][0]);
+        lo1 = min(lo1, s_red[k][1]);
+        lo2 = min(lo2, s_red[k][2]);
+        hi0 = max(hi0, s_red[k][3]);
+        hi1 = max(hi1, s_red[k][4]);
+        hi2 = max(hi2, s_red[k][5]);
+    }
+    // corners reach ix + 1, iy + 1, iz + 1
+    const int n0 = hi0 - lo0 + 2, n1 = hi1 - lo1 + 2, n2 = hi2 - lo2 + 2;
+    const bool any = hi0 >= lo0;
+    const bool boxed = any && n0 <= kBoxCells && n1 <= kBoxCells && n2 <= kBoxCells && n0 * n1 * n2 <= kBoxCells;
+    if (boxed) {
+        const int nb = n0 * n1 * n2;
+        for (int c = threadIdx.x; c < nb; c += blockDim.x) {
+            const int dx = c % n0, dy = (c / n0) % n1, dz = c / (n0 * n1);
+            const int64_t g = ((int64_t)(lo2 + dz) * gy + (lo1 + dy)) * gx + (lo0 + dx);
+            if (p.efield32)
+                reinterpret_cast<float4*>(s_box)[c] = p.efield32[g];
+            else {
+                s_box[2 * c] = p.efield[2 * g];
+                s_box[2 * c + 1] = p.efield[2 * g + 1];
+            }
+        }
+    }
+    __syncthreads();
+    if (boxed) {
+        const BoxField bf{p, s_box, lo0, lo1, lo2, n0, n1};
+#pragma unroll
+        for (int q = 0; q < PPT; ++q)
+            if (P[q].alive) sc_kick(p, P[q], bf);
+    } else {
+        const GlobalField gf{p};
+#pragma unroll
+        for (int q = 0; q < PPT; ++q)
+            if (P[q].alive) sc_kick(p, P[q], gf);
+    }
+}
+
 // Raw values of one particle as loaded: six coordinates and the mask.
 struct RawPart {
     double c[6];
@@ -547,10 +657,16 @@ __global__ void __launch_bounds__(kTrackThreads, PF ? 2 : TrackOcc<VARIANT>::val
 {
     __shared__ int s_counts[kMaxOpsPerPass];
     __shared__ double s_mom[6][kTrackThreads]; // per-thread moment sums
+    __shared__ double2 s_box[2 * kBoxCells];   // staged field (kick passes)
+    __shared__ int s_red[kTrackThreads / 32][6];
     for (int i = threadIdx.x; i < kMaxOpsPerPass; i += blockDim.x) s_counts[i] = 0;
     for (int j = 0; j < 6; ++j) s_mom[j][threadIdx.x] = 0.0;
     __syncthreads();
     double* s_mom_col = &s_mom[0][threadIdx.x];
+    // a pass that starts with the space-charge kick (the pass after a
+    // solve) stages, per tile, the field of the cells the tile's particles
+    // need in shared memory when they fit in kBoxCells
+    const bool kick_first = p.nops > 0 && p.ops[0].kind == OP_SC_KICK && p.sc && p.sc->valid;
 
     const int64_t n = p.n;
     const int64_t S = p.stride;
@@ -581,7 +697,12 @@ __global__ void __launch_bounds__(kTrackThreads, PF ? 2 : TrackOcc<VARIANT>::val
             in[q] = P[q].alive;
             P[q].disc = 0;
         }
-        for (int o = 0; o < p.nops; ++o) {
+        int op0 = 0;
+        if (kick_first) {
+            op0 = 1;
+            stage_and_kick<PPT>(p, P, s_box, s_red);
+        }
+        for (int o = op0; o < p.nops; ++o) {
             const MapOp& op = p.ops[o];
 #pragma unroll
             for (int q = 0; q < PPT; ++q) apply_op<VARIANT>(p, op, P[q], s_counts, s_mom_col);
@@ -601,6 +722,7 @@ __global__ void __launch_bounds__(kTrackThreads, PF ? 2 : TrackOcc<VARIANT>::val
             }
             if (p.write_discards && p.discards) p.discards[i] = (uint8_t)P[q].disc;
         }
+        if (kick_first) __syncthreads(); // the next tile restages the box
     }
 
     // per-aperture discard counts
@@ -643,17 +765,18 @@ static int full_variant()
     return v;
 }
 
-// Shape of the light pass: particles per thread and prefetching
-// (SB2_TRACK_LIGHT = 2: two per thread; 1p / 2p: one / two per thread with
-// the next tile prefetched).
+// Shape of the light pass: particles per thread and prefetching.  Default
+// 1p: one particle per thread with the next tile prefetched (2 CTAs/SM, no
+// register spills); SB2_TRACK_LIGHT = 2 / 2p selects two per thread without /
+// with prefetching.
 static int light_shape()
 {
     static int v = -1;
     if (v < 0) {
         const char* e = getenv("SB2_TRACK_LIGHT");
-        v = 0;
-        if (e && e[0] == '1' && e[1] == 'p') v = 1;
+        v = 1;
         if (e && e[0] == '2' && e[1] == 'p') v = 2;
+        if (e && e[0] == '2' && e[1] == 0) v = 0;
     }
     return v;
 }
