@@ -18,7 +18,6 @@
 // exchanging values between radix passes through shared memory (fft.cuh).
 #include <cuda_runtime.h>
 #include <algorithm>
-#include <climits>
 #include <type_traits>
 #include <cstdint>
 
@@ -155,173 +154,82 @@ __device__ __forceinline__ void leftmost_d(double pos, double left, double inv, 
     off = s - idx;
 }
 
-// CIC deposit (deposit.cc:309-394 ScatterView reducer): w0 * prod(1-o or o)
-// into the 8 cells of the particle's stencil; cells 0 and g-1 of every axis
-// are never written (deposit.cc:23-30).
-//
-// A CTA takes tiles of kDepTile particles.  Particles whose stencils start in
-// the same cell are first summed inside the warp (a segmented shuffle scan
-// over runs of equal cell keys: a cell-ordered bunch has long runs).  The
-// tile's stencils are then accumulated in a shared-memory box (the bounding
-// box of its cells, at most kDepBox cells) and the box is added to rho with
-// one global atomic per touched cell; a tile whose box is larger falls back
-// to global atomics per run.  Summation order differs from the reference's
-// (as it does between any two atomic schedules).
-constexpr int kDepThreads = 256;
-constexpr int kDepPPT = 4;
-constexpr int kDepTile = kDepThreads * kDepPPT;
-constexpr int kDepBox = 4096; // cells (32 KB)
-
-__global__ void __launch_bounds__(kDepThreads) deposit_kernel(const double* __restrict__ parts, int64_t stride,
-                                                              const uint8_t* __restrict__ masks, int64_t n,
-                                                              const ScState* __restrict__ scp, double* rho,
-                                                              int gx, int gy, int gz)
+// Particles whose stencils start in the same cell are summed inside the
+// warp first (a segmented shuffle scan over runs of equal cell keys), so a
+// cell-ordered bunch issues one set of 8 atomics per run instead of per
+// particle; with no equal neighbours the scan is skipped.
+__global__ void __launch_bounds__(256) deposit_kernel(const double* __restrict__ parts, int64_t stride,
+                                                      const uint8_t* __restrict__ masks, int64_t n,
+                                                      const ScState* __restrict__ scp, double* rho,
+                                                      int gx, int gy, int gz)
 {
-    __shared__ double s_box[kDepBox];
-    __shared__ int s_red[kDepThreads / 32][6];
     const ScState& sc = *scp;
     if (!sc.valid) return;
     const double lx = sc.left[0], ly = sc.left[1], lz = sc.left[2];
     const double ihx = sc.ih[0], ihy = sc.ih[1], ihz = sc.ih[2];
     const double w0 = sc.w0;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned full = 0xffffffffu;
-    for (int64_t base = (int64_t)blockIdx.x * kDepTile; base < n; base += (int64_t)gridDim.x * kDepTile) {
-        int ix[kDepPPT], iy[kDepPPT], iz[kDepPPT];
-        int key[kDepPPT];
-        double ox[kDepPPT], oy[kDepPPT], oz[kDepPPT];
-        int lo0 = INT_MAX, lo1 = INT_MAX, lo2 = INT_MAX, hi0 = INT_MIN, hi1 = INT_MIN, hi2 = INT_MIN;
-#pragma unroll
-        for (int q = 0; q < kDepPPT; ++q) {
-            const int64_t i = base + q * kDepThreads + threadIdx.x;
-            key[q] = -1;
-            ix[q] = iy[q] = iz[q] = 0;
-            ox[q] = oy[q] = oz[q] = 0.0;
-            if (i < n && masks[i]) {
-                leftmost_d(parts[i], lx, ihx, ix[q], ox[q]);
-                leftmost_d(parts[i + 2 * stride], ly, ihy, iy[q], oy[q]);
-                leftmost_d(parts[i + 4 * stride], lz, ihz, iz[q], oz[q]);
-                if (ix[q] >= -1 && ix[q] < gx && iy[q] >= -1 && iy[q] < gy && iz[q] >= -1 && iz[q] < gz) {
-                    key[q] = ((iz[q] + 1) * (gy + 1) + (iy[q] + 1)) * (gx + 1) + (ix[q] + 1);
-                    lo0 = min(lo0, ix[q]);
-                    lo1 = min(lo1, iy[q]);
-                    lo2 = min(lo2, iz[q]);
-                    hi0 = max(hi0, ix[q]);
-                    hi1 = max(hi1, iy[q]);
-                    hi2 = max(hi2, iz[q]);
-                }
-            }
-        }
-        // tile bounding box of the stencils (corners reach +1)
-        lo0 = __reduce_min_sync(full, lo0);
-        lo1 = __reduce_min_sync(full, lo1);
-        lo2 = __reduce_min_sync(full, lo2);
-        hi0 = __reduce_max_sync(full, hi0);
-        hi1 = __reduce_max_sync(full, hi1);
-        hi2 = __reduce_max_sync(full, hi2);
-        if (lane == 0) {
-            s_red[warp][0] = lo0;
-            s_red[warp][1] = lo1;
-            s_red[warp][2] = lo2;
-            s_red[warp][3] = hi0;
-            s_red[warp][4] = hi1;
-            s_red[warp][5] = hi2;
-        }
-        __syncthreads();
-        for (int k = 0; k < kDepThreads / 32; ++k) {
-            lo0 = min(lo0, s_red[k][0]);
-            lo1 = min(lo1, s_red[k][1]);
-            lo2 = min(lo2, s_red[k][2]);
-            hi0 = max(hi0, s_red[k][3]);
-            hi1 = max(hi1, s_red[k][4]);
-            hi2 = max(hi2, s_red[k][5]);
-        }
-        const int n0 = hi0 - lo0 + 2, n1 = hi1 - lo1 + 2, n2 = hi2 - lo2 + 2;
-        const bool any = hi0 >= lo0;
-        const bool boxed = any && n0 <= kDepBox && n1 <= kDepBox && n2 <= kDepBox &&
-                           (int64_t)n0 * n1 * n2 <= kDepBox;
-        const int nb = boxed ? n0 * n1 * n2 : 0;
-        for (int c = threadIdx.x; c < nb; c += kDepThreads) s_box[c] = 0.0;
-        __syncthreads(); // s_red reads done, box zeroed
-#pragma unroll
-        for (int q = 0; q < kDepPPT; ++q) {
-            double w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            if (key[q] >= 0) {
-                const double aox = 1.0 - ox[q], aoy = 1.0 - oy[q], aoz = 1.0 - oz[q];
+    const int lane = threadIdx.x & 31;
+    const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t wb = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane; wb < n; wb += wstride) {
+        const int64_t i = wb + lane;
+        int ix = 0, iy = 0, iz = 0;
+        int64_t key = -1;
+        double w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (i < n && masks[i]) {
+            double ox, oy, oz;
+            leftmost_d(parts[i], lx, ihx, ix, ox);
+            leftmost_d(parts[i + 2 * stride], ly, ihy, iy, oy);
+            leftmost_d(parts[i + 4 * stride], lz, ihz, iz, oz);
+            if (ix >= -1 && ix < gx && iy >= -1 && iy < gy && iz >= -1 && iz < gz) {
+                key = ((int64_t)(iz + 1) * (gy + 1) + (iy + 1)) * (gx + 1) + (ix + 1);
+                double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
                 w[0] = w0 * aox * aoy * aoz;
-                w[1] = w0 * ox[q] * aoy * aoz;
-                w[2] = w0 * aox * oy[q] * aoz;
-                w[3] = w0 * ox[q] * oy[q] * aoz;
-                w[4] = w0 * aox * aoy * oz[q];
-                w[5] = w0 * ox[q] * aoy * oz[q];
-                w[6] = w0 * aox * oy[q] * oz[q];
-                w[7] = w0 * ox[q] * oy[q] * oz[q];
+                w[1] = w0 * ox * aoy * aoz;
+                w[2] = w0 * aox * oy * aoz;
+                w[3] = w0 * ox * oy * aoz;
+                w[4] = w0 * aox * aoy * oz;
+                w[5] = w0 * ox * aoy * oz;
+                w[6] = w0 * aox * oy * oz;
+                w[7] = w0 * ox * oy * oz;
             }
-            const int prev = __shfl_up_sync(full, key[q], 1);
-            const int next = __shfl_down_sync(full, key[q], 1);
-            const bool head = lane == 0 || prev != key[q];
-            const bool tail = lane == 31 || next != key[q];
-            const unsigned heads = __ballot_sync(full, head);
-            if (heads != full) { // some run longer than one particle
-                unsigned le;
-                asm("mov.u32 %0, %%lanemask_le;" : "=r"(le));
-                const int seg = 31 - __clz(heads & le);
+        }
+        const int64_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+        const int64_t next = __shfl_down_sync(0xffffffffu, key, 1);
+        const bool head = lane == 0 || prev != key;
+        const bool tail = lane == 31 || next != key;
+        const unsigned heads = __ballot_sync(0xffffffffu, head);
+        if (heads != 0xffffffffu) { // some run longer than one particle
+            unsigned le;
+            asm("mov.u32 %0, %%lanemask_le;" : "=r"(le));
+            const int seg = 31 - __clz(heads & le);
 #pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    double v = w[c];
-                    for (int o = 1; o < 32; o <<= 1) {
-                        double u = __shfl_up_sync(full, v, o);
-                        if (lane - o >= seg) v += u;
-                    }
-                    w[c] = v;
+            for (int c = 0; c < 8; ++c) {
+                double v = w[c];
+                for (int o = 1; o < 32; o <<= 1) {
+                    double u = __shfl_up_sync(0xffffffffu, v, o);
+                    if (lane - o >= seg) v += u;
                 }
-            }
-            if (!tail || key[q] < 0) continue;
-            if (boxed) {
-                // edge cells are dropped when the box is flushed
-                const int l0 = ((iz[q] - lo2) * n1 + (iy[q] - lo1)) * n0 + (ix[q] - lo0);
-                const int l1 = l0 + n0 * n1;
-                atomicAdd(&s_box[l0], w[0]);
-                atomicAdd(&s_box[l0 + 1], w[1]);
-                atomicAdd(&s_box[l0 + n0], w[2]);
-                atomicAdd(&s_box[l0 + n0 + 1], w[3]);
-                atomicAdd(&s_box[l1], w[4]);
-                atomicAdd(&s_box[l1 + 1], w[5]);
-                atomicAdd(&s_box[l1 + n0], w[6]);
-                atomicAdd(&s_box[l1 + n0 + 1], w[7]);
-                continue;
-            }
-            const int x_ = ix[q], y_ = iy[q], z_ = iz[q];
-            bool x0 = x_ > 0 && x_ < gx - 1, x1 = x_ + 1 > 0 && x_ + 1 < gx - 1;
-            bool y0 = y_ > 0 && y_ < gy - 1, y1 = y_ + 1 > 0 && y_ + 1 < gy - 1;
-            bool z0 = z_ > 0 && z_ < gz - 1, z1 = z_ + 1 > 0 && z_ + 1 < gz - 1;
-            int64_t b = (int64_t)z_ * gx * gy;
-            if (z0) {
-                if (y0 && x0) atomicAdd(&rho[b + y_ * gx + x_], w[0]);
-                if (y0 && x1) atomicAdd(&rho[b + y_ * gx + x_ + 1], w[1]);
-                if (y1 && x0) atomicAdd(&rho[b + (y_ + 1) * gx + x_], w[2]);
-                if (y1 && x1) atomicAdd(&rho[b + (y_ + 1) * gx + x_ + 1], w[3]);
-            }
-            b = (int64_t)(z_ + 1) * gx * gy;
-            if (z1) {
-                if (y0 && x0) atomicAdd(&rho[b + y_ * gx + x_], w[4]);
-                if (y0 && x1) atomicAdd(&rho[b + y_ * gx + x_ + 1], w[5]);
-                if (y1 && x0) atomicAdd(&rho[b + (y_ + 1) * gx + x_], w[6]);
-                if (y1 && x1) atomicAdd(&rho[b + (y_ + 1) * gx + x_ + 1], w[7]);
+                w[c] = v;
             }
         }
-        if (boxed) {
-            __syncthreads();
-            // flush: interior cells only, x fastest (coalesced atomics)
-            for (int c = threadIdx.x; c < nb; c += kDepThreads) {
-                const double v = s_box[c];
-                if (v == 0.0) continue;
-                const int cx = lo0 + c % n0, cy = lo1 + (c / n0) % n1, cz = lo2 + c / (n0 * n1);
-                if (cx > 0 && cx < gx - 1 && cy > 0 && cy < gy - 1 && cz > 0 && cz < gz - 1)
-                    atomicAdd(&rho[((int64_t)cz * gy + cy) * gx + cx], v);
-            }
+        if (!tail || key < 0) continue;
+        bool x0 = ix > 0 && ix < gx - 1, x1 = ix + 1 > 0 && ix + 1 < gx - 1;
+        bool y0 = iy > 0 && iy < gy - 1, y1 = iy + 1 > 0 && iy + 1 < gy - 1;
+        bool z0 = iz > 0 && iz < gz - 1, z1 = iz + 1 > 0 && iz + 1 < gz - 1;
+        int64_t base = (int64_t)iz * gx * gy;
+        if (z0) {
+            if (y0 && x0) atomicAdd(&rho[base + iy * gx + ix], w[0]);
+            if (y0 && x1) atomicAdd(&rho[base + iy * gx + ix + 1], w[1]);
+            if (y1 && x0) atomicAdd(&rho[base + (iy + 1) * gx + ix], w[2]);
+            if (y1 && x1) atomicAdd(&rho[base + (iy + 1) * gx + ix + 1], w[3]);
         }
-        __syncthreads(); // the next tile reuses s_red and the box
+        base = (int64_t)(iz + 1) * gx * gy;
+        if (z1) {
+            if (y0 && x0) atomicAdd(&rho[base + iy * gx + ix], w[4]);
+            if (y0 && x1) atomicAdd(&rho[base + iy * gx + ix + 1], w[5]);
+            if (y1 && x0) atomicAdd(&rho[base + (iy + 1) * gx + ix], w[6]);
+            if (y1 && x1) atomicAdd(&rho[base + (iy + 1) * gx + ix + 1], w[7]);
+        }
     }
 }
 
@@ -719,7 +627,7 @@ cudaError_t launch_book_domain(const DomainParams& p, cudaStream_t s)
 cudaError_t launch_deposit(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
                            const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s)
 {
-    deposit_kernel<<<sm_count() * 4, kDepThreads, 0, s>>>(parts, stride, masks, n, sc, rho, gx, gy, gz);
+    deposit_kernel<<<sm_count() * 8, 256, 0, s>>>(parts, stride, masks, n, sc, rho, gx, gy, gz);
     return cudaGetLastError();
 }
 
