@@ -340,38 +340,9 @@ struct GlobalField {
     }
 };
 
-// Field of the cells a tile of particles needs, staged in shared memory
-// (box origin o0..o2, extents n0 x n1; cell c of the box at (dz n1 + dy) n0 +
-// dx): corners read from shared memory instead of L2.
-constexpr int kBoxCells = 1024;
-struct BoxField {
-    const TrackParams& p;
-    const double2* box; // FP64: 2 per cell; mixed: reinterpreted as float4
-    int o0, o1, o2, n0, n1;
-    __device__ __forceinline__ void load(int l, Corner& v) const
-    {
-        if (p.efield32) {
-            const float4 f = reinterpret_cast<const float4*>(box)[l];
-            v.x = f.x;
-            v.y = f.y;
-            v.z = f.z;
-        } else {
-            const double2 a = box[2 * l];
-            v.x = a.x;
-            v.y = a.y;
-            v.z = box[2 * l + 1].x;
-        }
-    }
-    __device__ __forceinline__ void corner(int ix, int iy, int iz, int c, Corner& v) const
-    {
-        load(((iz - o2 + (c >> 2)) * n1 + (iy - o1 + ((c >> 1) & 1))) * n0 + (ix - o0 + (c & 1)), v);
-    }
-};
-
 // zyx::alg_kicker space_charge_3d_kernels.h:91-215: trilinear interpolation
-// of E at the particle and the kick of xp, yp, dpop.  F::corners supplies
-// the field at the cell's 8 corners (from global memory, or from a box
-// staged in shared memory); the arithmetic is the same either way.
+// of E at the particle and the kick of xp, yp, dpop.  F::corner supplies
+// the field at the cell's corners.
 template <class F>
 __device__ __forceinline__ void sc_kick(const TrackParams& p, Part& P, const F& field)
 {
@@ -537,90 +508,6 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
 // PPT particles per thread travel through the op list together, so their
 // independent load and arithmetic chains overlap (more bytes in flight per
 // thread for the memory-bound passes).
-// Kick of a tile with its field staged in shared memory: the bounding box of
-// the corner cells of the tile's particles (block-wide min/max), the box's
-// field copied in (rows along x, coalesced), then every particle's kick from
-// the box -- or from global memory when the box exceeds kBoxCells.  Called
-// by all threads of the block.
-template <int PPT>
-__device__ __forceinline__ void stage_and_kick(const TrackParams& p, Part* P, double2* s_box, int (*s_red)[6])
-{
-    const ScState& sc = *p.sc;
-    const int gx = p.gx, gy = p.gy, gz = p.gz;
-    int lo0 = INT_MAX, lo1 = INT_MAX, lo2 = INT_MAX, hi0 = INT_MIN, hi1 = INT_MIN, hi2 = INT_MIN;
-#pragma unroll
-    for (int q = 0; q < PPT; ++q) {
-        if (!P[q].alive) continue;
-        int ix, iy, iz;
-        double o;
-        leftmost(P[q].x, sc.left[0], sc.ih[0], ix, o);
-        leftmost(P[q].y, sc.left[1], sc.ih[1], iy, o);
-        leftmost(P[q].cdt, sc.left[2], sc.ih[2], iz, o);
-        if ((ix >= 0 && ix < gx - 1) && (iy >= 0 && iy < gy - 1) && (iz >= 0 && iz < gz - 1)) {
-            lo0 = min(lo0, ix);
-            lo1 = min(lo1, iy);
-            lo2 = min(lo2, iz);
-            hi0 = max(hi0, ix);
-            hi1 = max(hi1, iy);
-            hi2 = max(hi2, iz);
-        }
-    }
-    const unsigned full = 0xffffffffu;
-    lo0 = __reduce_min_sync(full, lo0);
-    lo1 = __reduce_min_sync(full, lo1);
-    lo2 = __reduce_min_sync(full, lo2);
-    hi0 = __reduce_max_sync(full, hi0);
-    hi1 = __reduce_max_sync(full, hi1);
-    hi2 = __reduce_max_sync(full, hi2);
-    const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
-        s_red[w][0] = lo0;
-        s_red[w][1] = lo1;
-        s_red[w][2] = lo2;
-        s_red[w][3] = hi0;
-        s_red[w][4] = hi1;
-        s_red[w][5] = hi2;
-    }
-    __syncthreads();
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
-        lo0 = min(lo0, s_red[k][0]);
-        lo1 = min(lo1, s_red[k][1]);
-        lo2 = min(lo2, s_red[k][2]);
-        hi0 = max(hi0, s_red[k][3]);
-        hi1 = max(hi1, s_red[k][4]);
-        hi2 = max(hi2, s_red[k][5]);
-    }
-    // corners reach ix + 1, iy + 1, iz + 1
-    const int n0 = hi0 - lo0 + 2, n1 = hi1 - lo1 + 2, n2 = hi2 - lo2 + 2;
-    const bool any = hi0 >= lo0;
-    const bool boxed = any && n0 <= kBoxCells && n1 <= kBoxCells && n2 <= kBoxCells && n0 * n1 * n2 <= kBoxCells;
-    if (boxed) {
-        const int nb = n0 * n1 * n2;
-        for (int c = threadIdx.x; c < nb; c += blockDim.x) {
-            const int dx = c % n0, dy = (c / n0) % n1, dz = c / (n0 * n1);
-            const int64_t g = ((int64_t)(lo2 + dz) * gy + (lo1 + dy)) * gx + (lo0 + dx);
-            if (p.efield32)
-                reinterpret_cast<float4*>(s_box)[c] = p.efield32[g];
-            else {
-                s_box[2 * c] = p.efield[2 * g];
-                s_box[2 * c + 1] = p.efield[2 * g + 1];
-            }
-        }
-    }
-    __syncthreads();
-    if (boxed) {
-        const BoxField bf{p, s_box, lo0, lo1, lo2, n0, n1};
-#pragma unroll
-        for (int q = 0; q < PPT; ++q)
-            if (P[q].alive) sc_kick(p, P[q], bf);
-    } else {
-        const GlobalField gf{p};
-#pragma unroll
-        for (int q = 0; q < PPT; ++q)
-            if (P[q].alive) sc_kick(p, P[q], gf);
-    }
-}
-
 // Raw values of one particle as loaded: six coordinates and the mask.
 struct RawPart {
     double c[6];
@@ -657,16 +544,10 @@ __global__ void __launch_bounds__(kTrackThreads, PF ? 2 : TrackOcc<VARIANT>::val
 {
     __shared__ int s_counts[kMaxOpsPerPass];
     __shared__ double s_mom[6][kTrackThreads]; // per-thread moment sums
-    __shared__ double2 s_box[2 * kBoxCells];   // staged field (kick passes)
-    __shared__ int s_red[kTrackThreads / 32][6];
     for (int i = threadIdx.x; i < kMaxOpsPerPass; i += blockDim.x) s_counts[i] = 0;
     for (int j = 0; j < 6; ++j) s_mom[j][threadIdx.x] = 0.0;
     __syncthreads();
     double* s_mom_col = &s_mom[0][threadIdx.x];
-    // a pass that starts with the space-charge kick (the pass after a
-    // solve) stages, per tile, the field of the cells the tile's particles
-    // need in shared memory when they fit in kBoxCells
-    const bool kick_first = p.nops > 0 && p.ops[0].kind == OP_SC_KICK && p.sc && p.sc->valid;
 
     const int64_t n = p.n;
     const int64_t S = p.stride;
@@ -697,12 +578,7 @@ __global__ void __launch_bounds__(kTrackThreads, PF ? 2 : TrackOcc<VARIANT>::val
             in[q] = P[q].alive;
             P[q].disc = 0;
         }
-        int op0 = 0;
-        if (kick_first) {
-            op0 = 1;
-            stage_and_kick<PPT>(p, P, s_box, s_red);
-        }
-        for (int o = op0; o < p.nops; ++o) {
+        for (int o = 0; o < p.nops; ++o) {
             const MapOp& op = p.ops[o];
 #pragma unroll
             for (int q = 0; q < PPT; ++q) apply_op<VARIANT>(p, op, P[q], s_counts, s_mom_col);
@@ -722,7 +598,6 @@ __global__ void __launch_bounds__(kTrackThreads, PF ? 2 : TrackOcc<VARIANT>::val
             }
             if (p.write_discards && p.discards) p.discards[i] = (uint8_t)P[q].disc;
         }
-        if (kick_first) __syncthreads(); // the next tile restages the box
     }
 
     // per-aperture discard counts
