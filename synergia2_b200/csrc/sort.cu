@@ -10,7 +10,8 @@
 //   histogram warp-aggregated atomics on key counts
 //   scan      exclusive prefix sum of the counts (three small kernels)
 //   scatter   every column, the mask, the discard flag and the original
-//             index move to offset[key] + rank
+//             index move to offset[key] + rank, a tile at a time through
+//             shared memory (runs of equal keys leave as coalesced stores)
 // The caller's arrays are untouched while the bunch lives in the working
 // copy; they are brought back up to date (the working copy scattered back to
 // the original order) when the caller next reads or writes them.  The order within a cell
@@ -33,13 +34,6 @@ __device__ __forceinline__ int cell_key(double x, double y, double z, const ScSt
     const int G = gx * gy * gz;
     if (ix < 0 || ix >= gx || iy < 0 || iy >= gy || iz < 0 || iz >= gz) return G;
     return (iz * gy + iy) * gx + ix;
-}
-
-__device__ __forceinline__ unsigned lanemask_lt()
-{
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
 }
 
 __global__ void __launch_bounds__(256) sort_hist_kernel(const double* __restrict__ parts, int64_t stride,
@@ -136,39 +130,143 @@ __global__ void scan_add_kernel(int32_t* out, int n, const int32_t* __restrict__
     if (i < n) out[i] += sums[i / kScanBlock];
 }
 
-__global__ void __launch_bounds__(256) sort_scatter_kernel(const double* __restrict__ src, const uint8_t* __restrict__ m_src,
-                                                           const uint8_t* __restrict__ d_src,
-                                                           const int32_t* __restrict__ p_src, double* dst,
-                                                           uint8_t* m_dst, uint8_t* d_dst, int32_t* p_dst, int64_t n,
-                                                           int64_t stride, const ScState* __restrict__ scp, int gx,
-                                                           int gy, int gz, const int32_t* __restrict__ offsets,
-                                                           int32_t* cursor)
+// Scatter through a CTA-local grouping.  A CTA takes tiles of kTile
+// consecutive particles; the tile's keys go into a shared-memory hash table
+// (key -> count, each particle's rank inside its key), each distinct key of
+// the tile reserves its run of destinations with one global atomic, and the
+// tile is then moved array by array through shared memory so that a warp's
+// stores cover whole runs of consecutive destinations (a nearly ordered
+// bunch keeps most of a tile's particles in a few cells) instead of one
+// scattered 8-byte store per lane.
+constexpr int kTileThreads = 256;
+constexpr int kTile = 1024;
+constexpr int kTable = 2048; // hash slots (power of two)
+constexpr int kEmpty = -2;
+
+// open addressing with linear probing; returns the slot, and the particle's
+// rank inside its key (arrival order of the shared atomics)
+__device__ __forceinline__ int table_insert(int* t_key, int* t_cnt, int key, int& rank)
 {
+    const unsigned h = (unsigned)key * 2654435761u; // multiplicative hashing (Knuth)
+    int e = (int)(h >> 21) & (kTable - 1);
+    for (int probe = 0; probe < kTable; ++probe) {
+        const int old = atomicCAS(&t_key[e], kEmpty, key);
+        if (old == kEmpty || old == key) {
+            rank = atomicAdd(&t_cnt[e], 1);
+            return e;
+        }
+        e = (e + 1) & (kTable - 1);
+    }
+    rank = 0;
+    return -1; // unreachable: the table has more slots than a tile has keys
+}
+
+__global__ void __launch_bounds__(kTileThreads) sort_scatter_tiled_kernel(
+    const double* __restrict__ src, const uint8_t* __restrict__ m_src, const uint8_t* __restrict__ d_src,
+    const int32_t* __restrict__ p_src, double* dst, uint8_t* m_dst, uint8_t* d_dst, int32_t* p_dst, int64_t n,
+    int64_t stride, const ScState* __restrict__ scp, int gx, int gy, int gz, const int32_t* __restrict__ offsets,
+    int32_t* cursor)
+{
+    __shared__ int t_key[kTable];
+    __shared__ int t_cnt[kTable];
+    __shared__ int t_off[kTable];   // local exclusive offsets
+    __shared__ int t_gpos[kTable];  // first global destination of the key's run
+    __shared__ short s_src[kTile];  // tile index of the particle in local slot j
+    __shared__ int s_dst[kTile];    // its global destination
+    __shared__ double s_buf[kTile]; // one array of the tile
+    __shared__ int s_wsum[kTileThreads / 32];
     const ScState& sc = *scp;
     const int G = gx * gy * gz;
-    const int lane = threadIdx.x & 31;
-    const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t wb = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane; wb < n; wb += wstride) {
-        const int64_t i = wb + lane;
-        int key = -1;
-        double v[7];
-        uint8_t mk = 0;
-        if (i < n) {
-            for (int j = 0; j < 7; ++j) v[j] = src[i + j * stride];
-            mk = m_src[i];
-            key = (!mk || !sc.valid) ? G + 1 : cell_key(v[0], v[2], v[4], sc, gx, gy, gz);
+    constexpr int PPT = kTile / kTileThreads;
+    for (int e = threadIdx.x; e < kTable; e += kTileThreads) {
+        t_key[e] = kEmpty;
+        t_cnt[e] = 0;
+    }
+    __syncthreads();
+    for (int64_t base = (int64_t)blockIdx.x * kTile; base < n; base += (int64_t)gridDim.x * kTile) {
+        const int tn = (int)min((int64_t)kTile, n - base);
+        int ent[PPT], rnk[PPT];
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+            const int l = q * kTileThreads + threadIdx.x;
+            ent[q] = -1;
+            if (l < tn) {
+                const int64_t i = base + l;
+                const int key = (!m_src[i] || !sc.valid)
+                                    ? G + 1
+                                    : cell_key(src[i], src[i + 2 * stride], src[i + 4 * stride], sc, gx, gy, gz);
+                ent[q] = table_insert(t_key, t_cnt, key, rnk[q]);
+            }
         }
-        const unsigned grp = __match_any_sync(0xffffffffu, key);
-        const int leader = __ffs(grp) - 1;
-        int32_t b = 0;
-        if (key >= 0 && lane == leader) b = atomicAdd(&cursor[key], __popc(grp));
-        b = __shfl_sync(0xffffffffu, b, leader);
-        if (key < 0) continue;
-        const int64_t pos = (int64_t)offsets[key] + b + __popc(grp & lanemask_lt());
-        for (int j = 0; j < 7; ++j) dst[pos + j * stride] = v[j];
-        m_dst[pos] = mk;
-        d_dst[pos] = d_src[i];
-        p_dst[pos] = p_src[i];
+        __syncthreads();
+        // local exclusive scan of the counts (table order) and one global
+        // reservation per distinct key
+        constexpr int EPT = kTable / kTileThreads;
+        int c[EPT], tot = 0;
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            c[k] = t_cnt[threadIdx.x * EPT + k];
+            tot += c[k];
+        }
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        int inc = tot;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += u;
+        }
+        if (lane == 31) s_wsum[w] = inc;
+        __syncthreads();
+        int run = inc - tot;
+        for (int k = 0; k < w; ++k) run += s_wsum[k];
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            const int e = threadIdx.x * EPT + k;
+            t_off[e] = run;
+            if (c[k]) t_gpos[e] = offsets[t_key[e]] + atomicAdd(&cursor[t_key[e]], c[k]);
+            run += c[k];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+            if (ent[q] < 0) continue;
+            const int slot = t_off[ent[q]] + rnk[q];
+            s_src[slot] = (short)(q * kTileThreads + threadIdx.x);
+            s_dst[slot] = t_gpos[ent[q]] + rnk[q];
+        }
+        __syncthreads();
+        // move the tile array by array: coalesced loads into shared memory,
+        // stores in slot order (runs of consecutive destinations)
+        for (int a = 0; a < 10; ++a) {
+            if (a < 7) {
+                for (int l = threadIdx.x; l < tn; l += kTileThreads) s_buf[l] = src[base + l + a * stride];
+            } else if (a == 7) {
+                for (int l = threadIdx.x; l < tn; l += kTileThreads) s_buf[l] = (double)m_src[base + l];
+            } else if (a == 8) {
+                for (int l = threadIdx.x; l < tn; l += kTileThreads) s_buf[l] = (double)d_src[base + l];
+            } else {
+                for (int l = threadIdx.x; l < tn; l += kTileThreads) s_buf[l] = (double)p_src[base + l];
+            }
+            __syncthreads();
+            for (int j = threadIdx.x; j < tn; j += kTileThreads) {
+                const double v = s_buf[s_src[j]];
+                const int64_t d = s_dst[j];
+                if (a < 7)
+                    dst[d + a * stride] = v;
+                else if (a == 7)
+                    m_dst[d] = (uint8_t)v;
+                else if (a == 8)
+                    d_dst[d] = (uint8_t)v;
+                else
+                    p_dst[d] = (int32_t)v;
+            }
+            __syncthreads();
+        }
+        // clear the table for the next tile
+        for (int e = threadIdx.x; e < kTable; e += kTileThreads) {
+            t_key[e] = kEmpty;
+            t_cnt[e] = 0;
+        }
+        __syncthreads();
     }
 }
 
@@ -242,7 +340,7 @@ cudaError_t launch_cell_sort(const SortBuffers& sb, int32_t* scratch, const ScSt
     scan_block_kernel<<<nb, 256, 0, s>>>(counts, offsets, m, bsums);
     scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nb);
     scan_add_kernel<<<(m + 255) / 256, 256, 0, s>>>(offsets, m, bsums);
-    sort_scatter_kernel<<<grid, 256, 0, s>>>(sb.parts, sb.masks, sb.discards, sb.perm, sb.parts2, sb.masks2,
+    sort_scatter_tiled_kernel<<<grid, kTileThreads, 0, s>>>(sb.parts, sb.masks, sb.discards, sb.perm, sb.parts2, sb.masks2,
                                              sb.discards2, sb.perm2, sb.n, sb.stride, sc, gx, gy, gz, offsets, cursor);
     return cudaGetLastError();
 }
