@@ -53,10 +53,11 @@ const char* sb2_version(void);
 /* Per-category device timing of the library's own launches, measured with
  * CUDA events recorded on the launching stream (the reference's
  * scoped_simple_timer regions, utils/simple_timer.h:50-66).  Categories:
- * 0 track (fused particle passes), 1 domain (bookkeeping + domain),
- * 2 deposit, 3 green (Green-function transform), 4 solve (FFT
- * convolution), 5 efield, 6 sort (cell-ordered working copy).  Off by
- * default. */
+ * 0 track (fused particle passes of drifts, thin kicks, apertures, the
+ * space-charge kick), 1 domain (bookkeeping + domain), 2 deposit, 3 green
+ * (Green-function transform), 4 solve (FFT convolution), 5 efield, 6 sort
+ * (cell-ordered working copy), 7 track_full (particle passes with Yoshida
+ * integrators or sector bends).  Off by default. */
 sb2_status sb2_profile_enable(int32_t on);
 sb2_status sb2_profile_read(int32_t category, const char** name, double* total_ms, int64_t* launches,
                             int32_t reset);

@@ -1135,8 +1135,30 @@ static void sig_append(const void* p, size_t n)
 // reference's scoped_simple_timer labels, utils/simple_timer.h:50-66).
 // Off unless sb2_profile_enable(1) is called.
 // ---------------------------------------------------------------------------
-enum ProfCat { PROF_TRACK = 0, PROF_DOMAIN, PROF_DEPOSIT, PROF_GREEN, PROF_SOLVE, PROF_EFIELD, PROF_SORT, PROF_NCAT };
-static const char* kProfNames[PROF_NCAT] = {"track", "domain", "deposit", "green", "solve", "efield", "sort"};
+enum ProfCat {
+    PROF_TRACK = 0, // particle passes without Yoshida integrators or bends
+    PROF_DOMAIN,
+    PROF_DEPOSIT,
+    PROF_GREEN,
+    PROF_SOLVE,
+    PROF_EFIELD,
+    PROF_SORT,
+    PROF_TRACK_FULL, // particle passes with Yoshida integrators or sector bends
+    PROF_NCAT
+};
+static const char* kProfNames[PROF_NCAT] = {"track", "domain", "deposit", "green", "solve", "efield", "sort",
+                                            "track_full"};
+
+// A particle pass runs the full kernel variant when it holds a Yoshida
+// integrator or a sector bend (track_impl.cuh makes the same choice).
+static bool pass_is_full(const MapOp* ops, int n)
+{
+    for (int i = 0; i < n; ++i) {
+        const int k = ops[i].kind;
+        if (k == OP_QUAD || k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_SBEND) return true;
+    }
+    return false;
+}
 
 struct Profiler {
     bool on = false;
@@ -1561,7 +1583,7 @@ struct Engine {
                 if (has_mom) tp.moment_partials = sc->mom_partials;
             }
             {
-                ProfScope ps(PROF_TRACK, s);
+                ProfScope ps(pass_is_full(tp.ops, tp.nops) ? PROF_TRACK_FULL : PROF_TRACK, s);
                 cuda_check(launch_track(tp, s), "track kernel");
             }
             i += n;
