@@ -155,9 +155,31 @@ __device__ __forceinline__ void leftmost_d(double pos, double left, double inv, 
 }
 
 // Particles whose stencils start in the same cell are summed inside the
-// warp first (a segmented shuffle scan over runs of equal cell keys), so a
-// cell-ordered bunch issues one set of 8 atomics per run instead of per
-// particle; with no equal neighbours the scan is skipped.
+// warp first: the warp's 32 (cell key, lane) pairs are put in key order by a
+// bitonic network over the lanes, each lane takes the particle of its sorted
+// position, and a segmented shuffle scan sums runs of equal keys, so every
+// distinct cell of the warp costs one set of 8 atomics -- also when the
+// cell-ordered working copy has aged and equal keys are no longer adjacent.
+__device__ __forceinline__ void warp_sort_by_key(int& key, int& src, int lane)
+{
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const int ok = __shfl_xor_sync(0xffffffffu, key, j);
+            const int os = __shfl_xor_sync(0xffffffffu, src, j);
+            const bool up = (lane & k) == 0;
+            const bool lower = (lane & j) == 0;
+            const bool other_less = ok < key || (ok == key && os < src);
+            // the lower lane of an ascending pair keeps the smaller element
+            if (lower == up ? other_less : !other_less) {
+                key = ok;
+                src = os;
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) deposit_kernel(const double* __restrict__ parts, int64_t stride,
                                                       const uint8_t* __restrict__ masks, int64_t n,
                                                       const ScState* __restrict__ scp, double* rho,
@@ -169,36 +191,50 @@ __global__ void __launch_bounds__(256) deposit_kernel(const double* __restrict__
     const double ihx = sc.ih[0], ihy = sc.ih[1], ihz = sc.ih[2];
     const double w0 = sc.w0;
     const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
     const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t wb = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane; wb < n; wb += wstride) {
         const int64_t i = wb + lane;
         int ix = 0, iy = 0, iz = 0;
-        int64_t key = -1;
-        double w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        double ox = 0.0, oy = 0.0, oz = 0.0;
+        int key = -1;
         if (i < n && masks[i]) {
-            double ox, oy, oz;
             leftmost_d(parts[i], lx, ihx, ix, ox);
             leftmost_d(parts[i + 2 * stride], ly, ihy, iy, oy);
             leftmost_d(parts[i + 4 * stride], lz, ihz, iz, oz);
-            if (ix >= -1 && ix < gx && iy >= -1 && iy < gy && iz >= -1 && iz < gz) {
-                key = ((int64_t)(iz + 1) * (gy + 1) + (iy + 1)) * (gx + 1) + (ix + 1);
-                double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
-                w[0] = w0 * aox * aoy * aoz;
-                w[1] = w0 * ox * aoy * aoz;
-                w[2] = w0 * aox * oy * aoz;
-                w[3] = w0 * ox * oy * aoz;
-                w[4] = w0 * aox * aoy * oz;
-                w[5] = w0 * ox * aoy * oz;
-                w[6] = w0 * aox * oy * oz;
-                w[7] = w0 * ox * oy * oz;
-            }
+            if (ix >= -1 && ix < gx && iy >= -1 && iy < gy && iz >= -1 && iz < gz)
+                key = ((iz + 1) * (gy + 1) + (iy + 1)) * (gx + 1) + (ix + 1);
         }
-        const int64_t prev = __shfl_up_sync(0xffffffffu, key, 1);
-        const int64_t next = __shfl_down_sync(0xffffffffu, key, 1);
+        // key order inside the warp (skipped when the warp is already ordered)
+        const int prev0 = __shfl_up_sync(full, key, 1);
+        if (!__all_sync(full, lane == 0 || prev0 <= key)) {
+            int src = lane;
+            warp_sort_by_key(key, src, lane);
+            ix = __shfl_sync(full, ix, src);
+            iy = __shfl_sync(full, iy, src);
+            iz = __shfl_sync(full, iz, src);
+            ox = __shfl_sync(full, ox, src);
+            oy = __shfl_sync(full, oy, src);
+            oz = __shfl_sync(full, oz, src);
+        }
+        double w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (key >= 0) {
+            double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
+            w[0] = w0 * aox * aoy * aoz;
+            w[1] = w0 * ox * aoy * aoz;
+            w[2] = w0 * aox * oy * aoz;
+            w[3] = w0 * ox * oy * aoz;
+            w[4] = w0 * aox * aoy * oz;
+            w[5] = w0 * ox * aoy * oz;
+            w[6] = w0 * aox * oy * oz;
+            w[7] = w0 * ox * oy * oz;
+        }
+        const int prev = __shfl_up_sync(full, key, 1);
+        const int next = __shfl_down_sync(full, key, 1);
         const bool head = lane == 0 || prev != key;
         const bool tail = lane == 31 || next != key;
-        const unsigned heads = __ballot_sync(0xffffffffu, head);
-        if (heads != 0xffffffffu) { // some run longer than one particle
+        const unsigned heads = __ballot_sync(full, head);
+        if (heads != full) { // some run longer than one particle
             unsigned le;
             asm("mov.u32 %0, %%lanemask_le;" : "=r"(le));
             const int seg = 31 - __clz(heads & le);
@@ -206,7 +242,7 @@ __global__ void __launch_bounds__(256) deposit_kernel(const double* __restrict__
             for (int c = 0; c < 8; ++c) {
                 double v = w[c];
                 for (int o = 1; o < 32; o <<= 1) {
-                    double u = __shfl_up_sync(0xffffffffu, v, o);
+                    double u = __shfl_up_sync(full, v, o);
                     if (lane - o >= seg) v += u;
                 }
                 w[c] = v;
