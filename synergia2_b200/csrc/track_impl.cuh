@@ -326,10 +326,12 @@ struct GlobalField {
             v.y = f.y;
             v.z = f.z;
         } else {
-            const double2 a = p.efield[2 * c];
-            v.x = a.x;
-            v.y = a.y;
-            v.z = p.efield[2 * c + 1].x;
+            // one 32-byte load per cell {ex, ey, ez, 0} (sm_100 256-bit
+            // loads; cells are 32-byte aligned in the cudaMalloc'd field)
+            double pad;
+            asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+                : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(pad)
+                : "l"(p.efield + 2 * c));
         }
     }
     // corner c (x fastest, then y, then z) of cell (ix, iy, iz)
