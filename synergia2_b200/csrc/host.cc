@@ -55,12 +55,23 @@ static void cuda_check(cudaError_t e, const char* what)
     }
 }
 
+// Device memory comes from the stream-ordered allocator.  Objects are freed
+// only at rest (no kernel of theirs in flight: every propagate, batch job
+// and operator call ends by synchronising its own stream), so a free is
+// ordered on the legacy stream and never waits for the device as cudaFree
+// would -- a request loop retiring one job does not stall the jobs still
+// running on other streams.
 template <typename T>
 static T* dalloc(size_t count, const char* what)
 {
     void* p = nullptr;
-    cuda_check(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)), what);
+    cuda_check(cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), 0), what);
+    cuda_check(cudaStreamSynchronize(0), what);
     return (T*)p;
+}
+static void dfree(void* p)
+{
+    if (p) cudaFreeAsync(p, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -445,14 +456,14 @@ struct Bunch {
     }
     void free_work()
     {
-        cudaFree(wc.parts);
-        cudaFree(wc.masks);
-        cudaFree(wc.discards);
-        cudaFree(wc.perm);
-        cudaFree(wc.parts2);
-        cudaFree(wc.masks2);
-        cudaFree(wc.discards2);
-        cudaFree(wc.perm2);
+        dfree(wc.parts);
+        dfree(wc.masks);
+        dfree(wc.discards);
+        dfree(wc.perm);
+        dfree(wc.parts2);
+        dfree(wc.masks2);
+        dfree(wc.discards2);
+        dfree(wc.perm2);
         wc = SortBuffers{};
     }
     // home -> working copy in the caller's order (identity permutation)
@@ -511,12 +522,12 @@ struct Bunch {
     ~Bunch()
     {
         if (owns) {
-            cudaFree(home_parts);
-            cudaFree(home_masks);
-            cudaFree(home_discards);
+            dfree(home_parts);
+            dfree(home_masks);
+            dfree(home_discards);
         }
         free_work();
-        cudaFree(counters);
+        dfree(counters);
     }
     void sync_counters(cudaStream_t s)
     {
@@ -1323,19 +1334,19 @@ struct SpaceCharge {
     }
     ~SpaceCharge()
     {
-        cudaFree(rho);
-        cudaFree(phi);
-        cudaFree(E);
-        cudaFree(S);
-        cudaFree(ghat);
-        cudaFree(state);
-        cudaFree(mom_partials);
-        cudaFree(tw_x);
-        cudaFree(tw_y);
-        cudaFree(tw_z);
-        cudaFree(S32);
-        cudaFree(phi32);
-        cudaFree(E32);
+        dfree(rho);
+        dfree(phi);
+        dfree(E);
+        dfree(S);
+        dfree(ghat);
+        dfree(state);
+        dfree(mom_partials);
+        dfree(tw_x);
+        dfree(tw_y);
+        dfree(tw_z);
+        dfree(S32);
+        dfree(phi32);
+        dfree(E32);
     }
     // exp(-2 pi i k / L), k < L, from long-double sin/cos
     static double2* twiddles(int L)
@@ -1489,7 +1500,7 @@ struct Engine {
         cuda_check(cudaMemset(ap_counts, 0, sizeof(int32_t) * kMaxSlotsPerPass), "memset");
         reset();
     }
-    ~Engine() { cudaFree(ap_counts); }
+    ~Engine() { dfree(ap_counts); }
     void reset()
     {
         ops.clear();
@@ -1643,8 +1654,8 @@ struct Propagator {
     {
         drop_graphs();
         if (own_stream) cudaStreamDestroy(own_stream);
-        cudaFree(elem_charge);
-        cudaFree(sort_scratch);
+        dfree(elem_charge);
+        dfree(sort_scratch);
     }
 
     bool sorting(const Bunch& b) const { return has_sc && cell_sort && b.n >= 64; }
@@ -2327,7 +2338,7 @@ sb2_status sb2_bunch_populate_gaussian(sb2_bunch* h, const double sigma[6], uint
     Bunch& b = h->b;
     b.settle(0);
     if (b.n) cuda_check(launch_populate(b.parts, b.stride, b.masks, b.n, sigma, seed, 0), "populate");
-    cuda_check(cudaDeviceSynchronize(), "populate");
+    cuda_check(cudaStreamSynchronize(0), "populate");
     b.host_counters.n_valid = b.host_counters.n_total = (int32_t)b.n;
     cuda_check(cudaMemcpy(&b.host_counters.real_num, &b.counters->real_num, sizeof(double), cudaMemcpyDeviceToHost),
                "counters");
@@ -2356,8 +2367,8 @@ sb2_status sb2_bunch_moments(sb2_bunch* h, double mean[6], double mom2[36], doub
     cuda_check(cudaMemcpy(dmean, mu, sizeof(mu), cudaMemcpyHostToDevice), "mean");
     cuda_check(launch_moments(b.parts, b.stride, b.masks, b.n, dmean, part, nb, 0), "moments");
     cuda_check(cudaMemcpy(hp.data(), part, sizeof(double) * nb * 27, cudaMemcpyDeviceToHost), "moments");
-    cudaFree(part);
-    cudaFree(dmean);
+    dfree(part);
+    dfree(dmean);
     double m2[6][6];
     int t = 6;
     double acc[21] = {0};

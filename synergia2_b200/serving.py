@@ -55,7 +55,8 @@ class JobResult:
 
 def footprint_bytes(spec, precision=precision_t.mixed):
     """Device memory of one admitted job: particles (7 FP64 columns, mask,
-    discard flag) and the space-charge workspace."""
+    discard flag) and their cell-ordered working copy (two more copies and
+    two index arrays), and the space-charge workspace."""
     gx, gy, gz = spec.grid
     nx, ny, nz = 2 * gx, 2 * gy, 2 * gz
     G = gx * gy * gz
@@ -64,7 +65,7 @@ def footprint_bytes(spec, precision=precision_t.mixed):
     e_bytes = G * (16 if precision == precision_t.mixed else 32)
     phi_bytes = G * (4 if precision == precision_t.mixed else 8)
     ghat = (nx // 2 + 1) * (ny // 2 + 1) * (nz // 2 + 1) * 8
-    return spec.n * 58 + 8 * G + spec_bytes + e_bytes + phi_bytes + ghat + (1 << 20)
+    return spec.n * (3 * 58 + 8) + 8 * G + spec_bytes + e_bytes + phi_bytes + ghat + (1 << 20)
 
 
 def make_lattice(elements, kinetic_energy):
@@ -139,16 +140,8 @@ class Server:
             return spec.arrival
 
         inflight = {}  # slot -> turns launched
-        qi = 0
-        while qi < len(queue) or self.active:
-            now = clock()
-            # admission in arrival order while slots and device memory allow
-            while qi < len(queue) and arrival(queue[qi]) <= now and len(self.active) < self.max_active:
-                need = footprint_bytes(queue[qi], self.precision)
-                if self.active and self.used + need > self.budget:
-                    break
-                self._admit(queue[qi], now)
-                qi += 1
+
+        def launch_idle():
             # every admitted job that is not running gets its next quantum
             for slot, (spec, _, _, left, _) in self.active.items():
                 if slot in inflight or left <= 0:
@@ -158,6 +151,21 @@ class Server:
                 self.batch.launch(slot, q)
                 inflight[slot] = q
             self.max_inflight = max(self.max_inflight, len(inflight))
+
+        qi = 0
+        while qi < len(queue) or self.active:
+            now = clock()
+            # admission in arrival order while slots and device memory allow;
+            # each admitted job starts at once, so its work overlaps the
+            # admission of the next
+            while qi < len(queue) and arrival(queue[qi]) <= now and len(self.active) < self.max_active:
+                need = footprint_bytes(queue[qi], self.precision)
+                if self.active and self.used + need > self.budget:
+                    break
+                self._admit(queue[qi], now)
+                qi += 1
+                launch_idle()
+            launch_idle()
             # collect finished quanta; retire finished jobs at once
             progressed = False
             for slot in list(inflight):
