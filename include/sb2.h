@@ -198,6 +198,20 @@ sb2_status sb2_propagator_deposited_charge(sb2_propagator* p, int32_t index, dou
 sb2_status sb2_propagator_sc_last(sb2_propagator* p, double left[3], double h[3], double* rho,
                                   double* phi, double* ex, double* ey, double* ez, double scalars[8]);
 
+/* Per-turn diagnostics on the device (Diagnostics_full2::do_update,
+ * bunch/diagnostics_full2.cc:16-37): with capacity > 0 the propagator
+ * appends one record for the initial state of its first propagate call and
+ * one at the end of every turn, without host round trips (turn ends become
+ * particle-pass boundaries).  A record is sb2_diagnostics_record_size()
+ * doubles: num_particles, real_num, mean[6], std[6], min[3] and max[3] of
+ * (x, y, cdt), mom2[36] (row major), corr[36], emitx, emity, emitz, emitxy,
+ * emitxyz.  read copies up to max_records records (and the s_n and turn
+ * count of each); capacity 0 disables. */
+sb2_status sb2_propagator_set_diagnostics(sb2_propagator* p, int32_t capacity);
+sb2_status sb2_propagator_read_diagnostics(sb2_propagator* p, int32_t max_records, int32_t* count, double* records,
+                                           double* s_n, int32_t* turns);
+int32_t sb2_diagnostics_record_size(void);
+
 /* ---------------------------------------------------------------------
  * Batch of independent jobs (no counterpart in the reference, which runs
  * bunch trains through one simulator): each job is a (propagator, bunch)

@@ -74,6 +74,9 @@ SIGNATURES = {
     "sb2_batch_remove": (_i32, [_vp, _i32]),
     "sb2_batch_run": (_i32, [_vp, _pi32, _pi32, _i32]),
     "sb2_batch_launch": (_i32, [_vp, _i32, _i32]),
+    "sb2_propagator_set_diagnostics": (_i32, [_vp, _i32]),
+    "sb2_propagator_read_diagnostics": (_i32, [_vp, _i32, _pi32, _pd, _pd, _pi32]),
+    "sb2_diagnostics_record_size": (_i32, []),
     "sb2_batch_query": (_i32, [_vp, _i32, _pi32]),
     "sb2_propagator_sc_last": (_i32, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd]),
     "sb2_sc3d_create": (_i32, [_popts, _ppv]),

@@ -23,7 +23,7 @@ OUT = os.path.join(HERE, "libsb2.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["track.cu", "track_fast.cu", "sc3d.cu", "sort.cu", "noalloc.cu"]
+CU_SOURCES = ["track.cu", "track_fast.cu", "sc3d.cu", "sort.cu", "noalloc.cu", "diag.cu"]
 # fused multiply-adds where the results are held to tolerances, not bits:
 # the mixed path's particle passes and the solver (fields within 1e-10 of
 # the oracle; the FFTs of the reference's own FFT libraries fuse as well)

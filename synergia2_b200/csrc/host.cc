@@ -1656,6 +1656,10 @@ struct Propagator {
         if (own_stream) cudaStreamDestroy(own_stream);
         dfree(elem_charge);
         dfree(sort_scratch);
+        dfree(diag_records);
+        dfree(diag_count);
+        dfree(diag_partials);
+        dfree(diag_tmp);
     }
 
     bool sorting(const Bunch& b) const { return has_sc && cell_sort && b.n >= 64; }
@@ -1777,11 +1781,13 @@ struct Propagator {
         uint8_t* discards;
         SortBuffers wc;
         int kicks_since_sort;
+        size_t ndiag; // host-side diagnostic entries
     };
     HostSnap snap(const Bunch& b) const
     {
         HostSnap h{b.ref, b.design, b.design_set, b.turns_done, engine_->ops, engine_->book, engine_->nslots,
-                   sc ? sc->ghat_valid : false, b.parts, b.masks, b.discards, b.wc, b.kicks_since_sort};
+                   sc ? sc->ghat_valid : false, b.parts, b.masks, b.discards, b.wc, b.kicks_since_sort,
+                   diag_s.size()};
         return h;
     }
     void restore(Bunch& b, const HostSnap& h)
@@ -1795,16 +1801,62 @@ struct Propagator {
         b.discards = h.discards;
         b.wc = h.wc;
         b.kicks_since_sort = h.kicks_since_sort;
+        diag_s.resize(h.ndiag);
+        diag_turn.resize(h.ndiag);
         engine_->ops = h.ops;
         engine_->book = h.book;
         engine_->nslots = h.nslots;
         if (sc) sc->ghat_valid = h.ghat_valid;
     }
+    // ----- per-turn diagnostics (Diagnostics_full2 at turn ends) ----------
+    int diag_cap = 0;
+    double* diag_records = nullptr; // [diag_cap][kDiagRecord]
+    int32_t* diag_count = nullptr;  // records appended so far (device)
+    double* diag_partials = nullptr;
+    double* diag_tmp = nullptr;
+    std::vector<double> diag_s;     // s_n of each record (host: known at launch)
+    std::vector<int> diag_turn;     // turns completed at each record
+
+    void set_diagnostics(int capacity)
+    {
+        drop_graphs(); // captured turns change shape
+        dfree(diag_records);
+        dfree(diag_count);
+        dfree(diag_partials);
+        dfree(diag_tmp);
+        diag_records = diag_partials = diag_tmp = nullptr;
+        diag_count = nullptr;
+        diag_s.clear();
+        diag_turn.clear();
+        diag_cap = capacity;
+        if (capacity <= 0) return;
+        diag_records = dalloc<double>((size_t)capacity * kDiagRecord, "diagnostics");
+        diag_count = dalloc<int32_t>(1, "diagnostics");
+        diag_partials = dalloc<double>((size_t)track_grid_blocks() * 27, "diagnostics");
+        diag_tmp = dalloc<double>(12, "diagnostics");
+        cuda_check(cudaMemset(diag_count, 0, sizeof(int32_t)), "diagnostics");
+    }
+
+    // Flushes the pending maps (a record sees the bunch at the end of the
+    // turn) and appends one record on the device.
+    void record_diagnostics(Bunch& b, cudaStream_t s)
+    {
+        if (!diag_cap) return;
+        engine_->flush(b, sc.get(), elem_charge, false, 0.0, s);
+        diag_s.push_back(b.ref.s_n);
+        diag_turn.push_back(b.turns_done);
+        if (g_sig.dry) return;
+        cuda_check(launch_diagnostics(b.parts, b.stride, b.masks, b.n, b.counters, diag_partials, track_grid_blocks(),
+                                      diag_tmp, diag_records, diag_count, diag_cap, s),
+                   "diagnostics");
+    }
+
     void run_turn(Bunch& b, cudaStream_t s)
     {
         b.ref.start_repetition();
         for (auto const& st : steps) run_step(b, st, s);
         b.turns_done += 1;
+        record_diagnostics(b, s);
     }
     void drop_graphs()
     {
@@ -1873,6 +1925,7 @@ struct Propagator {
         if (use_graphs) s = graph_stream(s);
         begin(b);
         enter_sorted(b, s);
+        if (diag_cap && diag_s.empty()) record_diagnostics(b, s); // initial state
         for (int t = 0; t < turns; ++t) {
             if (use_graphs)
                 propagate_graph_turn(b, s);
@@ -1894,12 +1947,16 @@ struct Propagator {
     {
         begin(b);
         enter_sorted(b, s);
+        if (diag_cap && diag_s.empty()) record_diagnostics(b, s); // initial state
         const int ns = (int)steps.size();
         for (int k = first; k < first + count; ++k) {
             int si = ((k % ns) + ns) % ns;
             if (si == 0) b.ref.start_repetition();
             run_step(b, steps[si], s);
-            if (si == ns - 1) b.turns_done += 1;
+            if (si == ns - 1) {
+                b.turns_done += 1;
+                record_diagnostics(b, s);
+            }
         }
         engine_->flush(b, sc.get(), elem_charge, false, 0.0, s);
         leave_sorted(b, s);
@@ -2585,6 +2642,38 @@ sb2_status sb2_batch_run(sb2_batch* q, const int32_t* slots, const int32_t* turn
     q->q.run(slots, turns, n);
     SB2_CATCH
 }
+
+sb2_status sb2_propagator_set_diagnostics(sb2_propagator* p, int32_t capacity)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && capacity >= 0, "bad argument");
+    p->p->set_diagnostics(capacity);
+    SB2_CATCH
+}
+
+sb2_status sb2_propagator_read_diagnostics(sb2_propagator* p, int32_t max_records, int32_t* count, double* records,
+                                           double* s_n, int32_t* turns)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && count && max_records >= 0, "bad argument");
+    Propagator& P = *p->p;
+    *count = 0;
+    if (!P.diag_cap) return SB2_OK;
+    int32_t dev_count = 0;
+    cuda_check(cudaMemcpy(&dev_count, P.diag_count, sizeof(int32_t), cudaMemcpyDeviceToHost), "diagnostics");
+    const int n = std::min(std::min(dev_count, P.diag_cap), max_records);
+    *count = n;
+    if (records && n)
+        cuda_check(cudaMemcpy(records, P.diag_records, sizeof(double) * kDiagRecord * n, cudaMemcpyDeviceToHost),
+                   "diagnostics");
+    for (int i = 0; i < n && i < (int)P.diag_s.size(); ++i) {
+        if (s_n) s_n[i] = P.diag_s[i];
+        if (turns) turns[i] = P.diag_turn[i];
+    }
+    SB2_CATCH
+}
+
+int32_t sb2_diagnostics_record_size(void) { return kDiagRecord; }
 
 sb2_status sb2_batch_launch(sb2_batch* q, int32_t slot, int32_t turns)
 {

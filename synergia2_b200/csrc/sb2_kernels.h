@@ -100,6 +100,11 @@ cudaError_t launch_sort_gather_in(const double* ups, int64_t ustride, const uint
                                   const SortBuffers& sb, cudaStream_t s);
 cudaError_t launch_sort_scatter_out(const SortBuffers& sb, double* ups, int64_t ustride, uint8_t* um, uint8_t* ud,
                                     cudaStream_t s);
+// diag.cu: per-turn bunch diagnostics appended to a device record array
+constexpr int kDiagRecord = 97;
+cudaError_t launch_diagnostics(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
+                               const BunchCounters* counters, double* partials, int nb, double* tmp, double* records,
+                               int32_t* count, int capacity, cudaStream_t s);
 // host.cc
 int check_sc_options(const sb2_sc3d_options& o, std::string* msg);
 int ref_kinematics(int charge, double mass, double value, int kind, double* gamma, double* beta, double* p,

@@ -1,0 +1,89 @@
+"""Per-turn bunch diagnostics on the device (Diagnostics_full2::do_update,
+bunch/diagnostics_full2.cc:16-37; calculate_emittances,
+diagnostics_full2_host.cc).
+
+The records are checked against numpy on the particles read back at the
+same points (initial state, end of the run): mean, second moments, min/max
+and emittances to 1e-10 relative (only summation order differs).  Turning
+diagnostics on splits the fused particle pass at turn ends and must not
+change the particles; CUDA-graph turns give the same records.
+"""
+import numpy as np
+import pytest
+
+from helpers import SIG_C0, fodo_cell, gaussian_bunch, product_lattice, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _numpy_record(p, m, total):
+    live = p[m.astype(bool), :6]
+    mean = live.sum(0) / total
+    d = live - mean
+    mom2 = d.T @ d / total
+    emit = [np.sqrt(max(np.linalg.det(mom2[2 * k:2 * k + 2, 2 * k:2 * k + 2]), 0.0)) for k in range(3)]
+    return mean, mom2, emit, live[:, [0, 2, 4]].min(0), live[:, [0, 2, 4]].max(0), np.sqrt(np.linalg.det(mom2[:4, :4]))
+
+
+def _run(syn, graphs, diag, p, turns=3, shape=(16, 16, 32)):
+    lat, ref = product_lattice(fodo_cell())
+    prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(*shape), 8))
+    if graphs:
+        prop.set_graphs(True)
+    if diag:
+        prop.set_diagnostics(16)
+    b = syn.Bunch(ref, p.shape[0], 1e11)
+    b.set_particles(p)
+    prop.propagate(b, turns)
+    return prop, b
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+def test_diagnostics_records_match_numpy(syn, graphs):
+    n = 60000
+    p = gaussian_bunch(n, SIG_C0, 91)
+    prop, b = _run(syn, graphs, True, p)
+    d = prop.diagnostics()
+    assert len(d["num_particles"]) == 4  # initial + 3 turns
+    assert list(d["turns"]) == [0, 1, 2, 3]
+    assert np.allclose(np.diff(d["s_n"]), 10.0)
+    checks = [(0, p, np.ones(n, np.uint8))]
+    gp, gm, _ = b.get_particles()
+    checks.append((3, gp, gm))
+    for k, parts, masks in checks:
+        mean, mom2, emit, mn, mx, exy = _numpy_record(parts, masks, int(d["num_particles"][k]))
+        assert d["num_particles"][k] == masks.sum()
+        sd = np.sqrt(np.diag(mom2))
+        # summation order differs: relative 1e-10, plus 1e-12 of the spread
+        # for entries near zero (means, uncorrelated cross moments)
+        assert np.all(np.abs(d["mean"][k] - mean) <= 1e-10 * np.abs(mean) + 1e-12 * sd)
+        assert np.all(np.abs(d["mom2"][k] - mom2) <= 1e-10 * np.abs(mom2) + 1e-12 * np.outer(sd, sd))
+        assert np.array_equal(d["min"][k], mn) and np.array_equal(d["max"][k], mx)
+        assert np.allclose([d["emitx"][k], d["emity"][k], d["emitz"][k]], emit, rtol=1e-9)
+        assert abs(d["emitxy"][k] / exy - 1) < 1e-8
+        assert np.allclose(d["std"][k], np.sqrt(np.diag(mom2)), rtol=1e-10)
+        assert np.allclose(np.diag(d["corr"][k]), 1.0, rtol=1e-12)
+
+
+def test_diagnostics_do_not_change_tracking(syn):
+    p = gaussian_bunch(40000, SIG_C0, 92)
+    _, b0 = _run(syn, False, False, p)
+    _, b1 = _run(syn, False, True, p)
+    a, _, _ = b0.get_particles()
+    c, _, _ = b1.get_particles()
+    assert np.array_equal(a[:, 6], c[:, 6])
+    for j in range(6):
+        assert rel_l2(c[:, j], a[:, j]) <= 1e-10, j
+
+
+def test_diagnostics_graphs_match_direct(syn, monkeypatch):
+    monkeypatch.setenv("SB2_CELL_SORT", "0")
+    p = gaussian_bunch(40000, SIG_C0, 93)
+    pd, _ = _run(syn, False, True, p)
+    pg, _ = _run(syn, True, True, p)
+    a, g = pd.diagnostics(), pg.diagnostics()
+    assert np.array_equal(a["turns"], g["turns"])
+    for key in ("emitx", "emity", "emitz"):
+        assert np.allclose(a[key], g[key], rtol=1e-10, atol=0), key
+    sd = a["std"]
+    assert np.all(np.abs(a["mean"] - g["mean"]) <= 1e-10 * np.abs(a["mean"]) + 1e-12 * sd)
