@@ -205,11 +205,12 @@ sb2_status sb2_propagator_sc_last(sb2_propagator* p, double left[3], double h[3]
  * particle-pass boundaries).  A record is sb2_diagnostics_record_size()
  * doubles: num_particles, real_num, mean[6], std[6], min[3] and max[3] of
  * (x, y, cdt), mom2[36] (row major), corr[36], emitx, emity, emitz, emitxy,
- * emitxyz.  read copies up to max_records records (and the s_n and turn
- * count of each); capacity 0 disables. */
+ * emitxyz.  read copies up to max_records records (and the path length s
+ * -- Reference_particle::get_s -- and turn count of each); capacity 0
+ * disables. */
 sb2_status sb2_propagator_set_diagnostics(sb2_propagator* p, int32_t capacity);
 sb2_status sb2_propagator_read_diagnostics(sb2_propagator* p, int32_t max_records, int32_t* count, double* records,
-                                           double* s_n, int32_t* turns);
+                                           double* s, int32_t* turns);
 int32_t sb2_diagnostics_record_size(void);
 
 /* ---------------------------------------------------------------------

@@ -446,14 +446,14 @@ class Propagator:
         cap = getattr(self, "_diag_cap", 0)
         rs = lib().sb2_diagnostics_record_size()
         rec = np.zeros((max(cap, 1), rs))
-        s_n = np.zeros(max(cap, 1))
+        s_path = np.zeros(max(cap, 1))
         turns = np.zeros(max(cap, 1), np.int32)
         n = ctypes.c_int32()
-        check(lib().sb2_propagator_read_diagnostics(self.h, cap, ctypes.byref(n), _pd(rec), _pd(s_n),
+        check(lib().sb2_propagator_read_diagnostics(self.h, cap, ctypes.byref(n), _pd(rec), _pd(s_path),
                                                     turns.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
         k = n.value
         r = rec[:k]
-        return {"s_n": s_n[:k], "turns": turns[:k], "num_particles": r[:, 0], "real_num_particles": r[:, 1],
+        return {"s": s_path[:k], "turns": turns[:k], "num_particles": r[:, 0], "real_num_particles": r[:, 1],
                 "mean": r[:, 2:8], "std": r[:, 8:14], "min": r[:, 14:17], "max": r[:, 17:20],
                 "mom2": r[:, 20:56].reshape(k, 6, 6), "corr": r[:, 56:92].reshape(k, 6, 6),
                 "emitx": r[:, 92], "emity": r[:, 93], "emitz": r[:, 94], "emitxy": r[:, 95], "emitxyz": r[:, 96]}

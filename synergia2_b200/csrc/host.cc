@@ -1814,7 +1814,7 @@ struct Propagator {
     int32_t* diag_count = nullptr;  // records appended so far (device)
     double* diag_partials = nullptr;
     double* diag_tmp = nullptr;
-    std::vector<double> diag_s;     // s_n of each record (host: known at launch)
+    std::vector<double> diag_s;     // path length s of each record (host: known at launch)
     std::vector<int> diag_turn;     // turns completed at each record
 
     void set_diagnostics(int capacity)
@@ -1843,7 +1843,7 @@ struct Propagator {
     {
         if (!diag_cap) return;
         engine_->flush(b, sc.get(), elem_charge, false, 0.0, s);
-        diag_s.push_back(b.ref.s_n);
+        diag_s.push_back(b.ref.repetition * b.ref.s + b.ref.s_n); // Reference_particle::get_s
         diag_turn.push_back(b.turns_done);
         if (g_sig.dry) return;
         cuda_check(launch_diagnostics(b.parts, b.stride, b.masks, b.n, b.counters, diag_partials, track_grid_blocks(),
@@ -2652,7 +2652,7 @@ sb2_status sb2_propagator_set_diagnostics(sb2_propagator* p, int32_t capacity)
 }
 
 sb2_status sb2_propagator_read_diagnostics(sb2_propagator* p, int32_t max_records, int32_t* count, double* records,
-                                           double* s_n, int32_t* turns)
+                                           double* s, int32_t* turns)
 {
     SB2_TRY
     SB2_REQUIRE(p && count && max_records >= 0, "bad argument");
@@ -2667,7 +2667,7 @@ sb2_status sb2_propagator_read_diagnostics(sb2_propagator* p, int32_t max_record
         cuda_check(cudaMemcpy(records, P.diag_records, sizeof(double) * kDiagRecord * n, cudaMemcpyDeviceToHost),
                    "diagnostics");
     for (int i = 0; i < n && i < (int)P.diag_s.size(); ++i) {
-        if (s_n) s_n[i] = P.diag_s[i];
+        if (s) s[i] = P.diag_s[i];
         if (turns) turns[i] = P.diag_turn[i];
     }
     SB2_CATCH

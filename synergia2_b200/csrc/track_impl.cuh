@@ -23,8 +23,6 @@
 #include <cuda_runtime.h>
 #include <climits>
 #include <cstdint>
-#include <cstring>
-#include <cstddef>
 #include <cstdlib>
 
 #include "sb2_kernels.h"
@@ -660,78 +658,9 @@ static int light_shape()
     return v;
 }
 
-// The space-charge kick alone (the first op of the pass after a solve):
-// six columns and the mask in, xp, yp, dpop out.  Run as its own launch it
-// needs few registers, so many more warps per SM keep the field gathers in
-// flight than inside the fused pass.
-template <int PPT, int OCC>
-__global__ void __launch_bounds__(kTrackThreads, OCC) kick_kernel(const __grid_constant__ TrackParams p)
-{
-    const int64_t n = p.n, S = p.stride;
-    const int64_t tile = (int64_t)blockDim.x * PPT;
-    const GlobalField gf{p};
-    for (int64_t base = blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
-        RawPart r[PPT];
-        load_tile<PPT>(p, base, r);
-#pragma unroll
-        for (int q = 0; q < PPT; ++q) {
-            if (!r[q].m) continue;
-            const int64_t i = base + q * blockDim.x + threadIdx.x;
-            Part P;
-            P.x = r[q].c[0];
-            P.xp = r[q].c[1];
-            P.y = r[q].c[2];
-            P.yp = r[q].c[3];
-            P.cdt = r[q].c[4];
-            P.dpop = r[q].c[5];
-            P.alive = true;
-            P.disc = 0;
-            sc_kick(p, P, gf);
-            p.parts[i + S] = P.xp;
-            p.parts[i + 3 * S] = P.yp;
-            p.parts[i + 5 * S] = P.dpop;
-        }
-    }
-}
-
-// CTAs per SM of the kick kernel (SB2_KICK_OCC = 3: 80 registers, 4: 64)
-static int kick_occupancy()
-{
-    static int v = -1;
-    if (v < 0) {
-        const char* e = getenv("SB2_KICK_OCC");
-        v = (e && atoi(e) == 4) ? 4 : 3;
-    }
-    return v;
-}
-
-// SB2_SPLIT_KICK=0 keeps the kick inside the fused pass.
-static bool split_kick()
-{
-    static int v = -1;
-    if (v < 0) {
-        const char* e = getenv("SB2_SPLIT_KICK");
-        v = (e && atoi(e) == 0) ? 0 : 1;
-    }
-    return v == 1;
-}
-
-cudaError_t launch_pass(const TrackParams& p0, cudaStream_t s)
+cudaError_t launch_pass(const TrackParams& p, cudaStream_t s)
 {
     int nb = track_grid_blocks();
-    if (split_kick() && p0.nops > 0 && p0.ops[0].kind == OP_SC_KICK && p0.sc) {
-        if (kick_occupancy() == 4)
-            kick_kernel<1, 4><<<nb, kTrackThreads, 0, s>>>(p0);
-        else
-            kick_kernel<1, 3><<<nb, kTrackThreads, 0, s>>>(p0);
-        if (p0.nops == 1) return cudaGetLastError();
-        static thread_local TrackParams rest; // ~25 KB: not on the stack
-        std::memcpy(&rest, &p0, offsetof(TrackParams, ops));
-        rest.nops = p0.nops - 1;
-        std::memcpy(rest.ops, p0.ops + 1, sizeof(MapOp) * rest.nops);
-        return launch_pass(rest, s);
-    }
-    const TrackParams& p = p0;
     if (!track_needs_full(p.ops, p.nops)) {
         const int shape = light_shape();
         if (shape == 1)

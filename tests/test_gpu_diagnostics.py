@@ -46,7 +46,7 @@ def test_diagnostics_records_match_numpy(syn, graphs):
     d = prop.diagnostics()
     assert len(d["num_particles"]) == 4  # initial + 3 turns
     assert list(d["turns"]) == [0, 1, 2, 3]
-    assert np.allclose(np.diff(d["s_n"]), 10.0)
+    assert np.allclose(d["s"], [0.0, 10.0, 20.0, 30.0])
     checks = [(0, p, np.ones(n, np.uint8))]
     gp, gm, _ = b.get_particles()
     checks.append((3, gp, gm))
