@@ -247,3 +247,68 @@ def test_wrapped_bunch_arrays_current_after_each_call(syn, monkeypatch):
             assert rel_l2(got[:, j], expect[:, j]) <= 1e-10, j
     finally:
         L.sb2_bunch_destroy(h)
+
+
+def test_c0_config_matches_oracle(syn, orc):
+    """The CPU-runnable configuration at its own size: FODO cell, 8 kicks
+    per cell, 1,048,576 macroparticles, 32 x 32 x 64 grid, 10 passes (80
+    kicks), FP64.  Ids, masks and the lost set exact; coordinates within
+    1e-8 relative L2 of the oracle after 80 kicks (deposit summation order
+    is the only difference, and it compounds over the kicks); final fields
+    within 1e-8."""
+    n, shape, turns = 1048576, (32, 32, 64), 10
+    p = gaussian_bunch(n, SIG_C0, 0)
+    lat, ref = product_lattice(fodo_cell())
+    opts = syn.Space_charge_3d_open_hockney_options(*shape)
+    prop = syn.Propagator(lat, syn.Split_operator_stepper(opts, 8))
+    b = syn.Bunch(ref, n, 1e11)
+    b.set_particles(p)
+    prop.propagate(b, turns)
+    gp, gm, _ = b.get_particles()
+    g = prop.sc_last()
+    sim = orc.Sim(oracle_lattice(fodo_cell()), n, 1e11, stepper=orc.STEPPER_SPLIT, num=8,
+                  sc=orc.SCOptions.make(*shape), value=2.5 + MP)
+    sim.set_particles(p)
+    sim.propagate(turns)
+    op, om, _ = sim.get_particles()
+    o = sim.sc_last(shape)
+    assert np.array_equal(gm, om) and np.array_equal(gp[:, 6], op[:, 6])
+    for c in ("rho", "ex", "ey", "ez"):
+        assert rel_l2(g[c], o[c]) <= 1e-8, c
+    for j in range(6):
+        assert rel_l2(gp[:, j], op[:, j]) <= 1e-8, j
+
+
+def test_c3_size_ring_properties(syn):
+    """The ring configuration at full size (16,777,216 macroparticles,
+    128 x 128 x 256 grid, 16 kicks per cell, circular aperture), one turn:
+    size-independent properties -- ids stay a permutation of 0..N-1 in the
+    caller's order, lost particles are exactly the masked-out ones and the
+    bunch counters agree with the masks; and on the turn's final particles
+    the mixed-precision field is within 1e-5 relative L2 of the FP64 field."""
+    from helpers import ring_cell
+    n, shape = 16777216, (128, 128, 256)
+    lat, ref = product_lattice(ring_cell() * 24)
+    opts = syn.Space_charge_3d_open_hockney_options(*shape)
+    prop = syn.Propagator(lat, syn.Split_operator_stepper(opts, 384))
+    b = syn.Bunch(ref, n, 1e11)
+    b.populate_gaussian([2e-3, 1e-4, 2e-3, 1e-4, 0.3, 1e-4], seed=3)
+    prop.propagate(b, 1)
+    gp, gm, gd = b.get_particles()
+    assert np.array_equal(gp[:, 6], np.arange(n))
+    c = b.counts()
+    assert c["local_num"] == int(gm.sum()) == c["total_num"]
+    assert np.array_equal(gd.astype(bool) & ~gm.astype(bool), gd.astype(bool))  # discarded => masked
+    fields = []
+    for prec in (syn.precision_t.fp64, syn.precision_t.mixed):
+        o = syn.Space_charge_3d_open_hockney_options(*shape)
+        o.precision = prec
+        bb = syn.Bunch(ref, n, 1e11)
+        bb.set_particles(gp, gm)
+        sc = syn.Space_charge_3d_open_hockney(o)
+        sc.apply(bb, 0.5 / (0.96 * 299792458.0))
+        fields.append(sc.last())
+        del sc, bb
+    num = sum(float(((fields[1][k] - fields[0][k]) ** 2).sum()) for k in ("ex", "ey", "ez"))
+    den = sum(float((fields[0][k] ** 2).sum()) for k in ("ex", "ey", "ez"))
+    assert np.sqrt(num / den) <= 1e-5
