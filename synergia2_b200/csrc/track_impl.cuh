@@ -658,6 +658,18 @@ static int light_shape()
     return v;
 }
 
+// Particles per thread of the full pass (SB2_TRACK_FULL_PPT = 1 or 2): two
+// interleave two independent Yoshida chains per thread.
+static int full_ppt()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("SB2_TRACK_FULL_PPT");
+        v = (e && atoi(e) == 2) ? 2 : 1;
+    }
+    return v;
+}
+
 cudaError_t launch_pass(const TrackParams& p, cudaStream_t s)
 {
     int nb = track_grid_blocks();
@@ -669,8 +681,12 @@ cudaError_t launch_pass(const TrackParams& p, cudaStream_t s)
             track_kernel<TRACK_LIGHT, 2, true><<<nb, kTrackThreads, 0, s>>>(p);
         else
             track_kernel<TRACK_LIGHT, 2, false><<<nb, kTrackThreads, 0, s>>>(p);
-    } else if (full_variant() == TRACK_FULL_WIDE)
-        track_kernel<TRACK_FULL_WIDE, 1, false><<<nb, kTrackThreads, 0, s>>>(p);
+    } else if (full_variant() == TRACK_FULL_WIDE) {
+        if (full_ppt() == 2)
+            track_kernel<TRACK_FULL_WIDE, 2, false><<<nb, kTrackThreads, 0, s>>>(p);
+        else
+            track_kernel<TRACK_FULL_WIDE, 1, false><<<nb, kTrackThreads, 0, s>>>(p);
+    }
     else
         track_kernel<TRACK_FULL, 1, false><<<nb, kTrackThreads, 0, s>>>(p);
     return cudaGetLastError();
