@@ -541,7 +541,7 @@ __device__ __forceinline__ void load_tile(const TrackParams& p, int64_t base, Ra
 // (memory-bound passes: the loads of one tile overlap the arithmetic of the
 // previous one).
 template <int VARIANT, int PPT, bool PF>
-__global__ void __launch_bounds__(kTrackThreads, PF ? 2 : TrackOcc<VARIANT>::value)
+__global__ void __launch_bounds__(kTrackThreads, PF ? 3 : TrackOcc<VARIANT>::value)
     track_kernel(const __grid_constant__ TrackParams p)
 {
     __shared__ int s_counts[kMaxOpsPerPass];
