@@ -198,6 +198,24 @@ sb2_status sb2_propagator_deposited_charge(sb2_propagator* p, int32_t index, dou
 sb2_status sb2_propagator_sc_last(sb2_propagator* p, double left[3], double h[3], double* rho,
                                   double* phi, double* ex, double* ey, double* ez, double scalars[8]);
 
+/* A bunch split over several processes by particle range (one shard per
+ * rank, each rank with its own propagator and bunch; the reference runs this
+ * over MPI).  The library calls fn(ctx, data, count, on_host) wherever the
+ * ranks exchange: the six moment sums of the adaptive domain and the
+ * discard counts of update_total_num at each bookkeeping point
+ * (core_diagnostics.cc:444, bunch.h:363-370), and the charge density after
+ * every deposit (space_charge_3d_open_hockney.cc:572).  fn sums the `count`
+ * doubles at `data` in place over the ranks and returns 0; every rank makes
+ * the same calls in the same order.  The library's own work on its stream
+ * is finished before each call.  on_host != 0: data is pinned host memory
+ * (a host-side collective: gloo, MPI); 0: data is device memory (NCCL).
+ * The bunch's n_total and real_num are then the totals over the ranks (pass
+ * the global real_num to every shard).  CUDA-graph turns and per-turn
+ * diagnostics are not available on a sharded propagator.  fn = NULL
+ * returns to a whole bunch. */
+typedef int32_t (*sb2_allreduce_fn)(void* ctx, double* data, int64_t count, int32_t on_host);
+sb2_status sb2_propagator_set_allreduce(sb2_propagator* p, sb2_allreduce_fn fn, void* ctx, int32_t on_host);
+
 /* Per-turn diagnostics on the device (Diagnostics_full2::do_update,
  * bunch/diagnostics_full2.cc:16-37): with capacity > 0 the propagator
  * appends one record for the initial state of its first propagate call and

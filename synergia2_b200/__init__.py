@@ -434,6 +434,30 @@ class Propagator:
         check(lib().sb2_propagator_graph_stats(self.h, ctypes.byref(c), ctypes.byref(r)))
         return c.value, r.value
 
+    def set_allreduce(self, fn, on_host=True):
+        """Run this propagator on one shard of a bunch split over ranks
+        (sb2_propagator_set_allreduce).  on_host: fn(array) receives a numpy
+        view of pinned host memory and sums it in place over the ranks;
+        otherwise fn(pointer, count) gets the device pointer.  None returns
+        to a whole bunch."""
+        if fn is None:
+            self._allreduce = None
+            check(lib().sb2_propagator_set_allreduce(self.h, None, None, 0))
+            return
+
+        def cb(ctx, data, count, host):
+            try:
+                if host:
+                    fn(np.ctypeslib.as_array(data, shape=(int(count),)))
+                else:
+                    fn(ctypes.cast(data, ctypes.c_void_p).value, int(count))
+                return 0
+            except Exception:  # reported as a failed collective
+                return 1
+
+        self._allreduce = _lib.ALLREDUCE_FN(cb)  # kept alive with the propagator
+        check(lib().sb2_propagator_set_allreduce(self.h, self._allreduce, None, 1 if on_host else 0))
+
     def set_diagnostics(self, capacity):
         """Per-turn Diagnostics_full2 records on the device (initial state of
         the first propagate call, then every turn end); 0 disables."""

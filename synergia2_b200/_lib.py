@@ -75,6 +75,7 @@ SIGNATURES = {
     "sb2_batch_run": (_i32, [_vp, _pi32, _pi32, _i32]),
     "sb2_batch_launch": (_i32, [_vp, _i32, _i32]),
     "sb2_propagator_set_diagnostics": (_i32, [_vp, _i32]),
+    "sb2_propagator_set_allreduce": (_i32, [_vp, _vp, _vp, _i32]),
     "sb2_propagator_read_diagnostics": (_i32, [_vp, _i32, _pi32, _pd, _pd, _pi32]),
     "sb2_diagnostics_record_size": (_i32, []),
     "sb2_batch_query": (_i32, [_vp, _i32, _pi32]),
@@ -110,6 +111,10 @@ def lib():
             f.argtypes = args
         _LIB = L
     return _LIB
+
+
+# sb2_allreduce_fn: int32_t (*)(void* ctx, double* data, int64_t count, int32_t on_host)
+ALLREDUCE_FN = _c.CFUNCTYPE(_c.c_int32, _c.c_void_p, _c.POINTER(_c.c_double), _c.c_int64, _c.c_int32)
 
 
 def check(rc):

@@ -1256,7 +1256,48 @@ static int ilog2(int v)
     return l;
 }
 
+// Sum over the ranks of a bunch split by particle range (the reference's
+// MPI_Allreduce of the moment sums, core_diagnostics.cc:444, of the charge
+// density, space_charge_3d_open_hockney.cc:572, and of the valid counts in
+// update_total_num).  The caller's function sums `count` doubles in place
+// and returns 0; the library has finished its own work on the stream before
+// the call.  With on_host the data is staged through pinned host memory (a
+// host-side collective such as gloo or MPI), otherwise the function gets the
+// device pointer (NCCL).
+struct AllreduceHook {
+    sb2_allreduce_fn fn = nullptr;
+    void* ctx = nullptr;
+    int on_host = 0;
+    double* pinned = nullptr;
+    size_t pinned_n = 0;
+    ~AllreduceHook()
+    {
+        if (pinned) cudaFreeHost(pinned);
+    }
+    explicit operator bool() const { return fn != nullptr; }
+    void run(double* dev, int64_t n, cudaStream_t s)
+    {
+        cuda_check(cudaStreamSynchronize(s), "allreduce");
+        int32_t rc;
+        if (on_host) {
+            if (pinned_n < (size_t)n) {
+                if (pinned) cudaFreeHost(pinned);
+                pinned = nullptr;
+                cuda_check(cudaMallocHost((void**)&pinned, sizeof(double) * n), "allreduce staging");
+                pinned_n = n;
+            }
+            cuda_check(cudaMemcpy(pinned, dev, sizeof(double) * n, cudaMemcpyDeviceToHost), "allreduce staging");
+            rc = fn(ctx, pinned, n, 1);
+            cuda_check(cudaMemcpy(dev, pinned, sizeof(double) * n, cudaMemcpyHostToDevice), "allreduce staging");
+        } else {
+            rc = fn(ctx, dev, n, 0);
+        }
+        if (rc != 0) throw Error(SB2_ERR_RUNTIME, "allreduce callback failed");
+    }
+};
+
 struct SpaceCharge {
+    AllreduceHook* hook = nullptr; // bunch split over ranks
     sb2_sc3d_options o;
     Dims d{};
     int64_t G = 0;
@@ -1407,6 +1448,7 @@ struct SpaceCharge {
             cuda_check(cudaMemsetAsync(rho, 0, sizeof(double) * G, s), "memset rho");
             cuda_check(launch_deposit(b.parts, b.stride, b.masks, b.n, state, rho, d.gx, d.gy, d.gz, s), "deposit");
         }
+        if (hook && *hook) hook->run(rho, G, s); // charge of all ranks
         if (!o.domain_fixed || !ghat_valid) {
             ProfScope ps(PROF_GREEN, s);
             cuda_check(launch_green(state, ghat, d, o.green_fn == SB2_GREEN_LINEAR, tw_x, tw_y, tw_z, s), "green");
@@ -1493,6 +1535,8 @@ struct Engine {
     std::vector<MapOp> ops;
     PassBook book{};
     int nslots = 0;
+    AllreduceHook* hook = nullptr; // bunch split over ranks
+    double* xchg = nullptr;        // [6 moment sums][discards per slot]
 
     Engine()
     {
@@ -1500,7 +1544,11 @@ struct Engine {
         cuda_check(cudaMemset(ap_counts, 0, sizeof(int32_t) * kMaxSlotsPerPass), "memset");
         reset();
     }
-    ~Engine() { dfree(ap_counts); }
+    ~Engine()
+    {
+        dfree(ap_counts);
+        dfree(xchg);
+    }
     void reset()
     {
         ops.clear();
@@ -1610,6 +1658,13 @@ struct Engine {
             dp.ap_counts = ap_counts;
             dp.elem_charge = elem_charge;
             dp.book = book;
+            dp.xchg = nullptr;
+            if (hook && *hook) {
+                if (!xchg) xchg = dalloc<double>(6 + kMaxSlotsPerPass, "exchange");
+                cuda_check(launch_shard_pack(dp, nslots, xchg, s), "shard pack");
+                hook->run(xchg, 6 + nslots, s);
+                dp.xchg = xchg;
+            }
             ProfScope ps(PROF_DOMAIN, s);
             cuda_check(launch_book_domain(dp, s), "domain kernel");
         }
@@ -1703,19 +1758,29 @@ struct Propagator {
         b.swap_work();
     }
 
+    AllreduceHook hook; // set when the bunch is split over ranks
+
     void ensure_device()
     {
         if (!engine_) engine_.reset(new Engine());
         if (has_sc && !sc) sc.reset(new SpaceCharge(sc_opts));
+        engine_->hook = &hook;
+        if (sc) sc->hook = &hook;
         if (!elem_charge) {
             elem_charge = dalloc<double>(lat.elements.size(), "element charge");
             cuda_check(cudaMemset(elem_charge, 0, sizeof(double) * std::max<size_t>(1, lat.elements.size())), "memset");
         }
     }
 
-    void begin(Bunch& b)
+    void begin(Bunch& b, cudaStream_t s)
     { // do_before_start propagator.cc:8-23
         ensure_device();
+        if (hook) { // the bunch's total number is the sum of the ranks' valid counts
+            if (!engine_->xchg) engine_->xchg = dalloc<double>(6 + kMaxSlotsPerPass, "exchange");
+            cuda_check(launch_shard_count(b.counters, engine_->xchg, s), "shard count");
+            hook.run(engine_->xchg, 1, s);
+            cuda_check(launch_shard_total(b.counters, engine_->xchg, s), "shard total");
+        }
         if (b.turns_done == 0 && !b.design_set) {
             b.design = lat.ref;
             b.design_set = true;
@@ -1923,7 +1988,7 @@ struct Propagator {
     void propagate_async(Bunch& b, int turns, cudaStream_t s)
     {
         if (use_graphs) s = graph_stream(s);
-        begin(b);
+        begin(b, s);
         enter_sorted(b, s);
         if (diag_cap && diag_s.empty()) record_diagnostics(b, s); // initial state
         for (int t = 0; t < turns; ++t) {
@@ -1945,7 +2010,7 @@ struct Propagator {
 
     void propagate_steps(Bunch& b, int first, int count, cudaStream_t s)
     {
-        begin(b);
+        begin(b, s);
         enter_sorted(b, s);
         if (diag_cap && diag_s.empty()) record_diagnostics(b, s); // initial state
         const int ns = (int)steps.size();
@@ -2590,6 +2655,7 @@ sb2_status sb2_propagator_set_graphs(sb2_propagator* p, int32_t on)
 {
     SB2_TRY
     SB2_REQUIRE(p, "null propagator");
+    if (on && p->p->hook) throw Error(SB2_ERR_UNSUPPORTED, "CUDA-graph turns are not available on a sharded propagator");
     p->p->use_graphs = on != 0;
     if (!on) p->p->drop_graphs();
     SB2_CATCH
@@ -2647,7 +2713,21 @@ sb2_status sb2_propagator_set_diagnostics(sb2_propagator* p, int32_t capacity)
 {
     SB2_TRY
     SB2_REQUIRE(p && capacity >= 0, "bad argument");
+    if (capacity > 0 && p->p->hook)
+        throw Error(SB2_ERR_UNSUPPORTED, "per-turn diagnostics are not available on a sharded propagator");
     p->p->set_diagnostics(capacity);
+    SB2_CATCH
+}
+
+sb2_status sb2_propagator_set_allreduce(sb2_propagator* p, sb2_allreduce_fn fn, void* ctx, int32_t on_host)
+{
+    SB2_TRY
+    SB2_REQUIRE(p, "null propagator");
+    if (fn && (p->p->use_graphs || p->p->diag_cap))
+        throw Error(SB2_ERR_UNSUPPORTED, "a sharded propagator runs without CUDA-graph turns and per-turn diagnostics");
+    p->p->hook.fn = fn;
+    p->p->hook.ctx = ctx;
+    p->p->hook.on_host = on_host != 0;
     SB2_CATCH
 }
 

@@ -49,6 +49,10 @@ struct DomainParams {
     int32_t charge;
     double pref, gamma, beta;
     double time_step;
+    // bunch split over ranks: [6 moment sums][discards per slot] summed over
+    // the ranks (null for a whole bunch); counters then hold the local
+    // n_valid and the global n_total / real_num
+    const double* xchg;
 };
 
 struct Dims {
@@ -80,6 +84,11 @@ cudaError_t launch_populate(double* parts, int64_t stride, uint8_t* masks, int64
                             uint64_t seed, cudaStream_t s);
 // sc3d.cu
 cudaError_t launch_book_domain(const DomainParams& p, cudaStream_t s);
+// sharded bunch: moment sums and per-slot discards into xchg (to be summed
+// over the ranks), and the global n_total from a summed local count
+cudaError_t launch_shard_pack(const DomainParams& p, int nslots, double* xchg, cudaStream_t s);
+cudaError_t launch_shard_count(const BunchCounters* c, double* xchg, cudaStream_t s);
+cudaError_t launch_shard_total(BunchCounters* c, const double* xchg, cudaStream_t s);
 cudaError_t launch_deposit(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
                            const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s);
 cudaError_t launch_green(const ScState* sc, double* G, const Dims& d, int linear, const double2* tw_x,

@@ -46,8 +46,12 @@ __device__ double smallest_non_tiny(double val, double o1, double o2, double tin
 __global__ void __launch_bounds__(256) book_domain_kernel(const __grid_constant__ DomainParams p)
 {
     __shared__ double s_sum[256][6];
-    // fixed-order reduction of the per-block moment partials
-    if (p.compute_domain && !p.domain_fixed) {
+    // fixed-order reduction of the per-block moment partials (a bunch split
+    // over ranks takes the sums of all ranks from xchg instead)
+    if (p.compute_domain && !p.domain_fixed && p.xchg) {
+        if (threadIdx.x == 0)
+            for (int j = 0; j < 6; ++j) s_sum[0][j] = p.xchg[j];
+    } else if (p.compute_domain && !p.domain_fixed) {
         double acc[6] = {0, 0, 0, 0, 0, 0};
         for (int b = threadIdx.x; b < p.n_partials; b += blockDim.x)
             for (int j = 0; j < 6; ++j) acc[j] += p.moment_partials[b * 6 + j];
@@ -66,17 +70,19 @@ __global__ void __launch_bounds__(256) book_domain_kernel(const __grid_constant_
     // bunch.h:363-370)
     BunchCounters c = *p.counters;
     for (int o = 0; o < p.book.n_operators; ++o) {
-        int nd_op = 0;
+        int nd_op = 0, nd_all = 0;
         for (int s = p.book.slot_begin[o]; s < p.book.slot_end[o]; ++s) {
             int nd = p.ap_counts[s];
             p.ap_counts[s] = 0;
             int el = p.book.slot_elem[s];
             if (p.elem_charge && el >= 0 && nd) p.elem_charge[el] += nd * c.real_num / c.n_total;
             nd_op += nd;
+            if (p.xchg) nd_all += (int)llrint(p.xchg[6 + s]);
             c.n_valid -= nd;
         }
         int old_total = c.n_total;
-        c.n_total = c.n_valid;
+        // update_total_num: total = sum over ranks of the valid counts
+        c.n_total = p.xchg ? old_total - nd_all : c.n_valid;
         c.real_num = old_total ? c.n_total * c.real_num / old_total : 0.0;
     }
     *p.counters = c;
@@ -652,6 +658,47 @@ static int sm_count()
         if (n <= 0) n = 148;
     }
     return n;
+}
+
+// Sharded bunch: this rank's moment sums (fixed-order reduction of the block
+// partials) and discard counts per aperture slot, to be summed over ranks.
+__global__ void __launch_bounds__(256) shard_pack_kernel(const __grid_constant__ DomainParams p, int nslots,
+                                                         double* xchg)
+{
+    __shared__ double s_sum[256][6];
+    const bool sums = p.compute_domain && !p.domain_fixed;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    if (sums)
+        for (int b = threadIdx.x; b < p.n_partials; b += blockDim.x)
+            for (int j = 0; j < 6; ++j) acc[j] += p.moment_partials[b * 6 + j];
+    for (int j = 0; j < 6; ++j) s_sum[threadIdx.x][j] = acc[j];
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int j = 0; j < 6; ++j) s_sum[threadIdx.x][j] += s_sum[threadIdx.x + w][j];
+        __syncthreads();
+    }
+    if (threadIdx.x < 6) xchg[threadIdx.x] = s_sum[0][threadIdx.x];
+    for (int k = threadIdx.x; k < nslots; k += blockDim.x) xchg[6 + k] = (double)p.ap_counts[k];
+}
+
+__global__ void shard_count_kernel(const BunchCounters* c, double* xchg) { xchg[0] = (double)c->n_valid; }
+__global__ void shard_total_kernel(BunchCounters* c, const double* xchg) { c->n_total = (int)llrint(xchg[0]); }
+
+cudaError_t launch_shard_pack(const DomainParams& p, int nslots, double* xchg, cudaStream_t s)
+{
+    shard_pack_kernel<<<1, 256, 0, s>>>(p, nslots, xchg);
+    return cudaGetLastError();
+}
+cudaError_t launch_shard_count(const BunchCounters* c, double* xchg, cudaStream_t s)
+{
+    shard_count_kernel<<<1, 1, 0, s>>>(c, xchg);
+    return cudaGetLastError();
+}
+cudaError_t launch_shard_total(BunchCounters* c, const double* xchg, cudaStream_t s)
+{
+    shard_total_kernel<<<1, 1, 0, s>>>(c, xchg);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_book_domain(const DomainParams& p, cudaStream_t s)

@@ -1,0 +1,42 @@
+"""One bunch split over several processes (one GPU each) by particle range.
+
+The reference runs a bunch over MPI ranks: each rank tracks its own
+particles and the ranks exchange the moment sums of the adaptive domain,
+the valid counts of update_total_num and the charge density of every
+deposit.  Here each rank owns a Propagator and a Bunch holding its shard;
+`attach` gives the propagator a torch.distributed sum-allreduce for those
+exchanges (sb2_propagator_set_allreduce).
+"""
+import numpy as np
+
+
+def shard_range(n, rank, world):
+    """Contiguous particle range [lo, hi) of `rank` among `world` ranks."""
+    base, extra = divmod(n, world)
+    lo = rank * base + min(rank, extra)
+    return lo, lo + base + (1 if rank < extra else 0)
+
+
+def attach(propagator, group=None, on_host=None):
+    """Give `propagator` a torch.distributed sum-allreduce over `group`.
+    on_host (default: True for the gloo backend, False for NCCL) selects host
+    staging or device buffers."""
+    import torch
+    import torch.distributed as dist
+    if on_host is None:
+        on_host = dist.get_backend(group) != "nccl"
+    if on_host:
+        def fn(arr):
+            dist.all_reduce(torch.from_numpy(arr), op=dist.ReduceOp.SUM, group=group)
+    else:
+        class _Dev:  # a device buffer seen through __cuda_array_interface__
+            def __init__(self, ptr, n):
+                self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False),
+                                                 "version": 3, "strides": None}
+
+        def fn(ptr, n):
+            t = torch.as_tensor(_Dev(ptr, n), device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+            torch.cuda.synchronize()
+    propagator.set_allreduce(fn, on_host=on_host)
+    return propagator

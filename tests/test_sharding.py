@@ -1,0 +1,147 @@
+"""One bunch split over two processes by particle range (the reference's
+MPI bunch decomposition): the ranks exchange moment sums, valid counts and
+the charge density through a sum-allreduce (sb2_propagator_set_allreduce).
+
+CPU: the shard ranges and a two-rank gloo sum through the host-staged
+callback type.  GPU: two processes (gloo, host-staged exchanges; both on
+the one GPU: their kernels never wait on each other, the ranks meet on the
+host) against the whole bunch in one process -- coordinates within 1e-10
+relative (the deposit's summation order differs), ids, masks, discards and
+the bunch's total and real numbers exact.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from helpers import ROOT, SIG_C0, fodo_cell, gaussian_bunch, product_lattice, rel_l2, ring_cell
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_shard_ranges_cover_the_bunch():
+    from synergia2_b200.sharding import shard_range
+    for n, w in ((10, 3), (7, 7), (100, 1), (5, 8)):
+        rs = [shard_range(n, r, w) for r in range(w)]
+        assert rs[0][0] == 0 and rs[-1][1] == n
+        assert all(rs[k][1] == rs[k + 1][0] for k in range(w - 1))
+        assert max(h - l for l, h in rs) - min(h - l for l, h in rs) <= 1
+
+
+def _cpu_rank(rank, world, port, q):
+    import sys
+    sys.path.insert(0, ROOT)
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import ctypes
+        from synergia2_b200 import _lib
+        arr = np.full(5, rank + 1.0)
+
+        def fn(a):
+            dist.all_reduce(torch.from_numpy(a), op=dist.ReduceOp.SUM)
+
+        def cb(ctx, data, count, host):
+            fn(np.ctypeslib.as_array(data, shape=(int(count),)))
+            return 0
+        c = _lib.ALLREDUCE_FN(cb)
+        rc = c(None, arr.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 5, 1)
+        q.put((rank, rc, arr.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(120)
+def test_allreduce_callback_sums_over_two_gloo_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_cpu_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(90)
+    assert all(p.exitcode == 0 for p in ps)
+    for _ in range(2):
+        _, rc, vals = q.get(timeout=5)
+        assert rc == 0 and vals == [3.0] * 5
+
+
+def _spec(case):
+    if case == "fodo":
+        return fodo_cell(), 8, SIG_C0
+    return ring_cell(radius=0.004), 16, [2e-3, 1e-4, 2e-3, 1e-4, 0.3, 1e-4]
+
+
+def _gpu_rank(rank, world, port, case, n, q):
+    import sys
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import synergia2_b200 as syn
+        from synergia2_b200.sharding import attach, shard_range
+        spec, steps, sig = _spec(case)
+        p = gaussian_bunch(n, sig, 95)
+        lo, hi = shard_range(n, rank, world)
+        lat, ref = product_lattice(spec)
+        prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(16, 16, 32),
+                                                               steps))
+        attach(prop)
+        b = syn.Bunch(ref, hi - lo, 1e11)  # real_num of the whole bunch on every shard
+        b.set_particles(np.asfortranarray(p[lo:hi]))
+        prop.propagate(b, 2)
+        gp, gm, gd = b.get_particles()
+        q.put((rank, gp, gm, gd, b.get_total_num(), b.get_real_num()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.timeout(300)
+@pytest.mark.parametrize("case", ["fodo", "ring"])
+def test_sharded_bunch_matches_whole_bunch(syn, case):
+    n = 60000
+    spec, steps, sig = _spec(case)
+    p = gaussian_bunch(n, sig, 95)
+    lat, ref = product_lattice(spec)
+    prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(16, 16, 32),
+                                                           steps))
+    b = syn.Bunch(ref, n, 1e11)
+    b.set_particles(p)
+    prop.propagate(b, 2)
+    wp, wm, wd = b.get_particles()
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_gpu_rank, args=(r, 2, port, case, n, q)) for r in range(2)]
+    for pr in ps:
+        pr.start()
+    res = sorted(q.get(timeout=240) for _ in range(2))
+    for pr in ps:
+        pr.join(60)
+    assert all(pr.exitcode == 0 for pr in ps)
+    sp = np.concatenate([r[1] for r in res])
+    sm = np.concatenate([r[2] for r in res])
+    sd = np.concatenate([r[3] for r in res])
+    assert np.array_equal(sp[:, 6], wp[:, 6]) and np.array_equal(sm, wm) and np.array_equal(sd, wd)
+    if case == "ring":
+        assert 0 < int(wm.sum()) < n  # losses happened
+    for r in res:
+        assert r[4] == b.get_total_num()
+        assert r[5] == b.get_real_num()
+    for j in range(6):
+        assert rel_l2(sp[:, j], wp[:, j]) <= 1e-10, j
