@@ -865,6 +865,158 @@ static void sextupole_apply(const Slice& slice, Bunch& b)
     }
 }
 
+inline void oct_kick(double x, double& xp, double y, double& yp, double, const double* kL)
+{ // ff_octupole.h:12-14
+    thin_octupole_unit(x, xp, y, yp, kL);
+}
+inline void kicker_kick(double, double& xp, double, double& yp, double, const double* kL)
+{ // ff_kicker.h:12-14, thin_kicker_unit ff_algorithm.h:994-1000
+    xp = xp + kL[0];
+    yp = yp + kL[1];
+}
+
+// FF_patterned_propagator (ff_patterned_propagator.h) for one slice: the
+// design particle follows k_design, the particles k_parts; thin slices kick,
+// thick ones run yoshida6 (or drift-kick-drift when `simple`); use_drift
+// takes the design particle's time from a plain drift.
+static void patterned_apply(const Slice& slice, Bunch& b, const double* k_design, const double* k_parts, kick_fn kf,
+                            bool thin, bool simple, bool use_drift, int steps)
+{
+    const double length = slice.right - slice.left;
+    Refpart& ref_l = b.design;
+    if (thin) {
+        // get_reference_cdt_zero :227-244
+        double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3];
+        double dpop = 0.0;
+        kf(x, xp, y, yp, dpop, k_design);
+        ref_l.state[1] = xp;
+        ref_l.state[3] = yp;
+        ref_l.state[4] = 0.0;
+        if (b.n_valid) {
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < b.n_active; ++i) {
+                if (!b.masks[i]) continue;
+                double p1 = b.P(i, 1), p3 = b.P(i, 3), p5 = b.P(i, 5);
+                kf(b.P(i, 0), p1, b.P(i, 2), p3, p5, k_parts);
+                b.P(i, 1) = p1;
+                b.P(i, 3) = p3;
+            }
+        }
+        return;
+    }
+    const double pref = b.ref.p, mass = b.ref.mass;
+    if (simple) {
+        // get_reference_cdt_simple :246-273
+        double cdt = 0.0;
+        auto st = ref_l.state;
+        st[5] = 0.0;
+        double str[2] = {k_design[0] * length, k_design[1] * length};
+        drift_unit(st[0], st[1], st[2], st[3], cdt, st[5], length * 0.5, ref_l.p, ref_l.mass, 0.0);
+        kf(st[0], st[1], st[2], st[3], st[5], str);
+        drift_unit(st[0], st[1], st[2], st[3], cdt, st[5], length * 0.5, ref_l.p, ref_l.mass, 0.0);
+        st[4] = cdt;
+        ref_l.state = st;
+        const double ref_cdt = cdt;
+        // simple_kicker :57-100 (the kick takes the strength per unit length as is)
+        if (b.n_valid) {
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < b.n_active; ++i) {
+                if (!b.masks[i]) continue;
+                double p0 = b.P(i, 0), p1 = b.P(i, 1), p2 = b.P(i, 2), p3 = b.P(i, 3), p4 = b.P(i, 4), p5 = b.P(i, 5);
+                drift_unit(p0, p1, p2, p3, p4, p5, length * 0.5, pref, mass, ref_cdt * 0.5);
+                kf(p0, p1, p2, p3, p5, k_parts);
+                drift_unit(p0, p1, p2, p3, p4, p5, length * 0.5, pref, mass, ref_cdt * 0.5);
+                b.P(i, 0) = p0; b.P(i, 1) = p1; b.P(i, 2) = p2; b.P(i, 3) = p3; b.P(i, 4) = p4;
+            }
+        }
+        b.ref.s_n += length;
+        return;
+    }
+    // get_reference_cdt_yoshida :275-316
+    double cdt = 0.0;
+    auto st = ref_l.state;
+    st[5] = 0.0;
+    const double step_len = length / steps;
+    double step_str[2] = {k_design[0] * step_len, k_design[1] * step_len};
+    if (use_drift)
+        drift_unit(st[0], st[1], st[2], st[3], cdt, st[5], length, ref_l.p, ref_l.mass, 0.0);
+    else
+        yoshida_general(6, st[0], st[1], st[2], st[3], cdt, st[5], ref_l.p, ref_l.mass, 0.0, step_len, step_str, steps,
+                        kf, 1);
+    st[4] = cdt;
+    ref_l.state = st;
+    // apply_yoshida_kick :199-225
+    const double step_ref_cdt = cdt / steps;
+    double ss[2] = {k_parts[0] * step_len, k_parts[1] * step_len};
+    if (b.n_valid) {
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < b.n_active; ++i) {
+            if (!b.masks[i]) continue;
+            double p0 = b.P(i, 0), p1 = b.P(i, 1), p2 = b.P(i, 2), p3 = b.P(i, 3), p4 = b.P(i, 4), p5 = b.P(i, 5);
+            yoshida6(p0, p1, p2, p3, p4, p5, pref, mass, step_ref_cdt, step_len, ss, steps, kf, 1);
+            b.P(i, 0) = p0; b.P(i, 1) = p1; b.P(i, 2) = p2; b.P(i, 3) = p3; b.P(i, 4) = p4;
+        }
+    }
+    b.ref.s_n += length;
+}
+
+static void octupole_apply(const Slice& slice, Bunch& b)
+{ // ff_octupole.h:16-88
+    const Element& element = *slice.e;
+    const double length = slice.right - slice.left;
+    double k[2] = {element.get("k3", 0.0), element.get("k3s", 0.0)};
+    const double tilt = element.get("tilt", 0.0);
+    if (tilt != 0.0) {
+        std::complex<double> ck2(k[0], k[1]);
+        ck2 = ck2 * std::exp(std::complex<double>(0.0, -4.0 * tilt));
+        k[0] = ck2.real();
+        k[1] = ck2.imag();
+    }
+    const Refpart& ref_l = b.design;
+    const Refpart& ref_b = b.ref;
+    const double brho_l = ref_l.p / ref_l.charge;
+    const double brho_b = ref_b.p * (1.0 + ref_b.state[5]) / ref_l.charge;
+    const double scale = brho_l / brho_b;
+    k[0] *= scale;
+    k[1] *= scale;
+    const int steps = (int)element.get("yoshida_steps", 4.0);
+    patterned_apply(slice, b, k, k, oct_kick, close_to_zero(length), false, false, steps);
+}
+
+static void kicker_apply(const Slice& slice, Bunch& b)
+{ // ff_kicker.h:17-127, attributes as Lattice_element_processor hkicker / vkicker / kicker
+    const Element& elem = *slice.e;
+    const double length = slice.right - slice.left;
+    const std::string& t = elem.type;
+    double hk0 = elem.get("hkick", 0.0), vk0 = elem.get("vkick", 0.0);
+    if (t == "hkicker") {
+        if (elem.d.count("kick")) hk0 = elem.get("kick", 0.0);
+        vk0 = 0.0;
+    } else if (t == "vkicker") {
+        if (elem.d.count("kick")) vk0 = elem.get("kick", 0.0);
+        hk0 = 0.0;
+    }
+    const double l = elem.get("l", 0.0);
+    const double tilt = elem.get("tilt", 0.0);
+    const double hk = cos(tilt) * hk0 - sin(tilt) * vk0;
+    const double vk = sin(tilt) * hk0 + cos(tilt) * vk0;
+    const double scale = b.design.p / b.ref.p;
+    const double q = (double)b.ref.charge / b.design.charge;
+    double k[2] = {hk, vk};
+    double sk[2] = {hk * q * scale, vk * q * scale};
+    const bool thin = close_to_zero(length);
+    if (!thin) {
+        k[0] = k[0] / l;
+        k[1] = k[1] / l;
+        sk[0] = sk[0] / l;
+        sk[1] = sk[1] / l;
+    }
+    const bool simple = std::fabs(elem.get("simple", 0.0)) > 1e-16;
+    const int steps = (int)elem.get("yoshida_steps", 4.0);
+    const bool use_drift = (int)elem.get("cdt_use_drift", 0.0) != 0;
+    patterned_apply(slice, b, k, sk, kicker_kick, thin, simple, use_drift, steps);
+}
+
 static void element_apply(const Slice& slice, Bunch& b)
 { // ff_element.h:25-67
     const std::string& t = slice.e->type;
@@ -879,6 +1031,10 @@ static void element_apply(const Slice& slice, Bunch& b)
         multipole_apply(slice, b);
     else if (t == "sextupole")
         sextupole_apply(slice, b);
+    else if (t == "octupole")
+        octupole_apply(slice, b);
+    else if (t == "hkicker" || t == "vkicker" || t == "kicker")
+        kicker_apply(slice, b);
     else
         throw std::runtime_error("FF_element::apply() unknown element type = " + t + ", element name = " + slice.e->name);
 }

@@ -140,6 +140,7 @@ struct Element {
                                              " of type " + type + " has no double attribute '" + k + "'");
         return it->second;
     }
+    bool has(const std::string& k) const { return d.count(k) > 0; }
     bool has_string(const std::string& k) const { return s.count(k) > 0; }
     std::string get_string(const std::string& k, const std::string& def) const
     {
@@ -412,6 +413,12 @@ inline void bend_complete(double& x, double& xp, double& y, double& yp, double& 
 
 void quad_kick_cb(double x, double& xp, double y, double& yp, const double* k) { cf_kick(x, xp, y, yp, k); }
 void sext_kick_cb(double x, double& xp, double y, double& yp, const double* k) { thin_sext(x, xp, y, yp, k); }
+void oct_kick_cb(double x, double& xp, double y, double& yp, const double* k) { thin_oct(x, xp, y, yp, k); }
+void kicker_kick_cb(double, double& xp, double, double& yp, const double* k)
+{ // thin_kicker_unit ff_algorithm.h:994-1000
+    xp = xp + k[0];
+    yp = yp + k[1];
+}
 } // namespace hostff
 
 // ---------------------------------------------------------------------------
@@ -1064,6 +1071,136 @@ static void ops_sextupole(const Lattice& lat, const Slice& sl, Bunch& b, std::ve
     b.ref.s_n += length;
 }
 
+// Patterned element slice (FF_patterned_propagator, ff_patterned_propagator.h)
+// with kick kf: the design particle follows k_design (get_reference_cdt_*),
+// the particles k_parts.  Thin slices kick; thick ones run yoshida6 (or a
+// drift-kick-drift with `simple`); use_drift times the design particle by a
+// plain drift.
+static void ops_patterned(const Slice& sl, Bunch& b, std::vector<MapOp>& out, const double* k_design,
+                          const double* k_parts, hostff::kick_fn kf, int thin_kind, int yoshida_kind, bool thin,
+                          bool simple, bool use_drift, int steps)
+{
+    const double length = sl.right - sl.left;
+    Refpart& ref_l = b.design;
+    if (thin) { // get_reference_cdt_zero :227-244
+        double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3];
+        kf(x, xp, y, yp, k_design);
+        ref_l.state[1] = xp;
+        ref_l.state[3] = yp;
+        ref_l.state[4] = 0.0;
+        MapOp o = new_op(thin_kind);
+        o.d[2] = k_parts[0];
+        o.d[3] = k_parts[1];
+        out.push_back(o);
+        return;
+    }
+    if (simple) { // get_reference_cdt_simple :246-273, simple_kicker :57-100
+        double cdt = 0.0;
+        auto st = ref_l.state;
+        st[5] = 0.0;
+        double str[2] = {k_design[0] * length, k_design[1] * length};
+        hostff::drift_unit(st[0], st[1], st[2], st[3], cdt, st[5], length * 0.5, ref_l.p, ref_l.mass, 0.0);
+        kf(st[0], st[1], st[2], st[3], str);
+        hostff::drift_unit(st[0], st[1], st[2], st[3], cdt, st[5], length * 0.5, ref_l.p, ref_l.mass, 0.0);
+        st[4] = cdt;
+        ref_l.state = st;
+        MapOp o = new_op(OP_KICK_SIMPLE);
+        o.d[0] = length * 0.5;
+        o.d[1] = b.ref.p;
+        o.d[2] = b.ref.mass;
+        o.d[3] = cdt * 0.5;
+        o.d[4] = k_parts[0]; // the reference kicks with the per-length strength as is
+        o.d[5] = k_parts[1];
+        out.push_back(o);
+        b.ref.s_n += length;
+        return;
+    }
+    // get_reference_cdt_yoshida :275-316, apply_yoshida_kick :199-225
+    double cdt = 0.0;
+    auto st = ref_l.state;
+    st[5] = 0.0;
+    const double step_len = length / steps;
+    double dstr[2] = {k_design[0] * step_len, k_design[1] * step_len};
+    if (use_drift)
+        hostff::drift_unit(st[0], st[1], st[2], st[3], cdt, st[5], length, ref_l.p, ref_l.mass, 0.0);
+    else
+        for (int i = 0; i < steps; ++i)
+            hostff::yoshida_element(2, st[0], st[1], st[2], st[3], cdt, st[5], ref_l.p, ref_l.mass, 0.0, step_len, dstr,
+                                    1.0, kf, 1);
+    st[4] = cdt;
+    ref_l.state = st;
+    const double step_ref_cdt = cdt / steps;
+    const double pstr[2] = {k_parts[0] * step_len, k_parts[1] * step_len};
+    MapOp o = new_op(yoshida_kind);
+    o.steps = steps;
+    o.d[2] = b.ref.p;
+    o.d[3] = b.ref.mass;
+    o.d[4] = step_ref_cdt * 0.1;
+    o.d[5] = hostff::Y_C1 * step_len;
+    o.d[6] = hostff::Y_C2 * step_len;
+    o.d[7] = hostff::Y_C3 * step_len;
+    o.d[8] = hostff::Y_C4 * step_len;
+    for (int i = 0; i < 2; ++i) {
+        o.d[9 + i] = hostff::Y_D1 * pstr[i];
+        o.d[11 + i] = hostff::Y_D2 * pstr[i];
+        o.d[13 + i] = hostff::Y_D3 * pstr[i];
+        o.d[15 + i] = hostff::Y_D4 * pstr[i];
+    }
+    out.push_back(o);
+    b.ref.s_n += length;
+}
+
+static void ops_octupole(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
+{ // ff_octupole.h:16-88
+    const Element& el = lat.elements[sl.elem];
+    double k[2] = {el.get("k3", 0.0), el.get("k3s", 0.0)};
+    const double tilt = el.get("tilt", 0.0);
+    if (tilt != 0.0) {
+        std::complex<double> ck2(k[0], k[1]);
+        ck2 = ck2 * std::exp(std::complex<double>(0.0, -4.0 * tilt));
+        k[0] = ck2.real();
+        k[1] = ck2.imag();
+    }
+    const double scale = brho_scale(b);
+    k[0] *= scale;
+    k[1] *= scale;
+    ops_patterned(sl, b, out, k, k, hostff::oct_kick_cb, OP_THIN_OCT, OP_OCT_YOSHIDA,
+                  hostff::close_to_zero(sl.right - sl.left), false, false, (int)el.get("yoshida_steps", 4.0));
+}
+
+static void ops_kicker(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
+{ // ff_kicker.h:17-127; attributes as Lattice_element_processor::hkicker / vkicker / kicker
+  // (lattice_element_processor.cc:86-159)
+    const Element& el = lat.elements[sl.elem];
+    const double length = sl.right - sl.left;
+    double hk0 = el.get("hkick", 0.0), vk0 = el.get("vkick", 0.0);
+    if (el.type == "hkicker") {
+        if (el.has("kick")) hk0 = el.get("kick", 0.0);
+        vk0 = 0.0;
+    } else if (el.type == "vkicker") {
+        if (el.has("kick")) vk0 = el.get("kick", 0.0);
+        hk0 = 0.0;
+    }
+    const double l = el.get("l", 0.0);
+    const double tilt = el.get("tilt", 0.0);
+    const double hk = std::cos(tilt) * hk0 - std::sin(tilt) * vk0;
+    const double vk = std::sin(tilt) * hk0 + std::cos(tilt) * vk0;
+    const double scale = b.design.p / b.ref.p;
+    const double q = (double)b.ref.charge / b.design.charge;
+    double k[2] = {hk, vk};
+    double sk[2] = {hk * q * scale, vk * q * scale};
+    const bool thin = hostff::close_to_zero(length);
+    if (!thin) {
+        k[0] = k[0] / l;
+        k[1] = k[1] / l;
+        sk[0] = sk[0] / l;
+        sk[1] = sk[1] / l;
+    }
+    ops_patterned(sl, b, out, k, sk, hostff::kicker_kick_cb, OP_THIN_KICK, OP_KICK_YOSHIDA, thin,
+                  std::fabs(el.get("simple", 0.0)) > 1e-16, (int)el.get("cdt_use_drift", 0.0) != 0,
+                  (int)el.get("yoshida_steps", 4.0));
+}
+
 // FF_element::apply ff_element.h:25-67
 static void ops_slice(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
 {
@@ -1079,8 +1216,12 @@ static void ops_slice(const Lattice& lat, const Slice& sl, Bunch& b, std::vector
         ops_multipole(lat, sl, b, out);
     else if (t == "sextupole")
         ops_sextupole(lat, sl, b, out);
-    else if (t == "octupole" || t == "hkicker" || t == "vkicker" || t == "kicker" || t == "solenoid" ||
-             t == "rfcavity" || t == "elens" || t == "nllens" || t == "foil" || t == "dipedge" || t == "matrix")
+    else if (t == "octupole")
+        ops_octupole(lat, sl, b, out);
+    else if (t == "hkicker" || t == "vkicker" || t == "kicker")
+        ops_kicker(lat, sl, b, out);
+    else if (t == "solenoid" || t == "rfcavity" || t == "elens" || t == "nllens" || t == "foil" || t == "dipedge" ||
+             t == "matrix")
         throw Error(SB2_ERR_UNSUPPORTED, "element type " + t + " is not on the GPU path of this build (element " +
                                              lat.elements[sl.elem].name + ")");
     else
@@ -1166,7 +1307,9 @@ static bool pass_is_full(const MapOp* ops, int n)
 {
     for (int i = 0; i < n; ++i) {
         const int k = ops[i].kind;
-        if (k == OP_QUAD || k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_SBEND) return true;
+        if (k == OP_QUAD || k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_OCT_YOSHIDA || k == OP_KICK_YOSHIDA ||
+            k == OP_SBEND)
+            return true;
     }
     return false;
 }

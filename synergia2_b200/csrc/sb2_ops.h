@@ -20,6 +20,11 @@ enum OpKind : int32_t {
     OP_MPOLE = 6,          // ff_multipole.h:28-78
     OP_THIN_SEXT = 7,      // ff_patterned_propagator.h:21-53 with ff_sextupole kick
     OP_SEXT_YOSHIDA = 8,   // ff_patterned_propagator.h:110-150
+    OP_THIN_OCT = 9,       // ff_patterned_propagator.h:21-53 with ff_octupole kick
+    OP_OCT_YOSHIDA = 10,   // ff_patterned_propagator.h:110-150 with ff_octupole kick
+    OP_THIN_KICK = 11,     // ff_patterned_propagator.h:21-53 with ff_kicker kick
+    OP_KICK_YOSHIDA = 12,  // ff_patterned_propagator.h:110-150 with ff_kicker kick
+    OP_KICK_SIMPLE = 13,   // ff_patterned_propagator.h:57-100 (drift-kick-drift)
     OP_AP_FINITE = 20,     // aperture_operation.h:54-86
     OP_AP_CIRCULAR = 21,   // aperture_operation.h:92-116
     OP_AP_ELLIPTICAL = 22, // aperture_operation.h:123-151

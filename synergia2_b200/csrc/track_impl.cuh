@@ -254,7 +254,12 @@ __device__ __forceinline__ void yoshida6_op(double& x, double& xp, double& y, do
             thin_quadrupole_unit(x, xp, y, yp, kk[0], kk[1]);
         else if (KIND == OP_SEXT_YOSHIDA)
             thin_sextupole_unit(x, xp, y, yp, kk[0], kk[1]);
-        else
+        else if (KIND == OP_OCT_YOSHIDA)
+            thin_octupole_unit(x, xp, y, yp, kk[0], kk[1]);
+        else if (KIND == OP_KICK_YOSHIDA) {
+            xp = xp + kk[0]; // thin_kicker_unit ff_algorithm.h:994-1000
+            yp = yp + kk[1];
+        } else
             quad_cf_kick(x, xp, y, yp, kk);
     };
     const double* k1 = k;
@@ -484,6 +489,37 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
         case OP_THIN_SEXT:
             thin_sextupole_unit(x, xp, y, yp, op.d[2], op.d[3]);
             break;
+        case OP_OCT_YOSHIDA:
+            if constexpr (kFull) yoshida6_op<OP_OCT_YOSHIDA>(x, xp, y, yp, cdt, dpop, op);
+            break;
+        case OP_THIN_OCT:
+            thin_octupole_unit(x, xp, y, yp, op.d[2], op.d[3]);
+            break;
+        case OP_KICK_YOSHIDA:
+            if constexpr (kFull) yoshida6_op<OP_KICK_YOSHIDA>(x, xp, y, yp, cdt, dpop, op);
+            break;
+        case OP_THIN_KICK:
+            xp = xp + op.d[2];
+            yp = yp + op.d[3];
+            break;
+        case OP_KICK_SIMPLE: {
+            // simple_kicker ff_patterned_propagator.h:57-100: half drift, kick,
+            // half drift (d: half length, pref, mass, half reference cdt, k)
+#if SB2_FAST_MAPS
+            const double dp = dpop + 1.0;
+            const double ib = inv_beta(dp, op.d[1], op.d[2]);
+            drift_unit_ib(x, xp, y, yp, cdt, dp, op.d[0], ib, op.d[3]);
+            xp = xp + op.d[4];
+            yp = yp + op.d[5];
+            drift_unit_ib(x, xp, y, yp, cdt, dp, op.d[0], ib, op.d[3]);
+#else
+            drift_unit(x, xp, y, yp, cdt, dpop, op.d[0], op.d[1], op.d[2], op.d[3]);
+            xp = xp + op.d[4];
+            yp = yp + op.d[5];
+            drift_unit(x, xp, y, yp, cdt, dpop, op.d[0], op.d[1], op.d[2], op.d[3]);
+#endif
+            break;
+        }
         case OP_MPOLE: {
             const double* kl = op.d;
             const int on = op.flags;
@@ -624,7 +660,9 @@ bool track_needs_full(const MapOp* ops, int n)
 {
     for (int i = 0; i < n; ++i) {
         int k = ops[i].kind;
-        if (k == OP_QUAD || k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_SBEND) return true;
+        if (k == OP_QUAD || k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_OCT_YOSHIDA || k == OP_KICK_YOSHIDA ||
+            k == OP_SBEND)
+            return true;
     }
     return false;
 }
