@@ -1017,6 +1017,68 @@ static void kicker_apply(const Slice& slice, Bunch& b)
     patterned_apply(slice, b, k, sk, kicker_kick, thin, simple, use_drift, steps);
 }
 
+// solenoid_unit ff_algorithm.h:1317-1356 (the map's callers pass ks*L in
+// the `ks` slot and ks in the `ksl` slot, ff_solenoid.h:130-131,231-236;
+// kept as is), edge kicks :1358-1372
+inline void solenoid_unit(double& x, double& xp, double& y, double& yp, double& cdt, double dpop, double ks,
+                          double ksl, double length, double ref_p, double mass, double ref_cdt)
+{
+    const double uni = 1.0;
+    double p2 = (uni + dpop) * (uni + dpop);
+    double zp = std::sqrt(p2 - xp * xp - yp * yp);
+    double dtheta = ksl / zp;
+    double sn = std::sin(dtheta);
+    double cs = std::cos(dtheta);
+    double xpi = xp, ypi = yp;
+    xp = cs * xpi + sn * ypi;
+    yp = (-sn) * xpi + cs * ypi;
+    cs = cs - uni;
+    x = x + (cs * (-ypi) + sn * xpi) / ks;
+    y = y + ((-sn) * (-ypi) + cs * xpi) / ks;
+    double en = std::sqrt(p2 * ref_p * ref_p + mass * mass);
+    double duration = length / (zp * ref_p / en);
+    cdt = cdt + duration - ref_cdt;
+}
+
+static void solenoid_apply(const Slice& slice, Bunch& b)
+{ // ff_solenoid.h:160-248
+    const double length = slice.right - slice.left;
+    const double mass = b.ref.mass;
+    const bool in_edge = slice.ledge, out_edge = slice.redge;
+    double ks = slice.e->get("ks", 0.0);
+    Refpart& ref_l = b.design;
+    const Refpart& ref_b = b.ref;
+    const double ref_p = ref_b.p * (1.0 + ref_b.state[5]);
+    if (std::fabs(ks) < 1e-12) {
+        drift_apply(slice, b);
+        return;
+    }
+    const double brho_l = ref_l.p * (1.0 + ref_l.state[5]) / ref_l.charge;
+    const double brho_b = ref_b.p * (1.0 + ref_b.state[5]) / ref_l.charge;
+    ks = ks * (brho_l / brho_b);
+    const double ksl = ks * length;
+    const double kse = ks * 0.5;
+    // get_reference_cdt_solenoid :125-155
+    double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3], cdt = 0.0, dpop = 0.0;
+    if (in_edge) { xp = xp + kse * y; yp = yp - kse * x; }
+    solenoid_unit(x, xp, y, yp, cdt, dpop, ksl, ks, length, ref_l.p * (1 + dpop), ref_l.mass, 0.0);
+    if (out_edge) { xp = xp - kse * y; yp = yp + kse * x; }
+    ref_l.state = {x, xp, y, yp, cdt, dpop};
+    const double ref_cdt = cdt;
+    if (b.n_valid) {
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < b.n_active; ++i) {
+            if (!b.masks[i]) continue;
+            double p0 = b.P(i, 0), p1 = b.P(i, 1), p2 = b.P(i, 2), p3 = b.P(i, 3), p4 = b.P(i, 4), p5 = b.P(i, 5);
+            if (in_edge) { p1 = p1 + kse * p2; p3 = p3 - kse * p0; }
+            solenoid_unit(p0, p1, p2, p3, p4, p5, ksl, ks, length, ref_p, mass, ref_cdt);
+            if (out_edge) { p1 = p1 - kse * p2; p3 = p3 + kse * p0; }
+            b.P(i, 0) = p0; b.P(i, 1) = p1; b.P(i, 2) = p2; b.P(i, 3) = p3; b.P(i, 4) = p4;
+        }
+    }
+    b.ref.s_n += length;
+}
+
 static void element_apply(const Slice& slice, Bunch& b)
 { // ff_element.h:25-67
     const std::string& t = slice.e->type;
@@ -1035,6 +1097,8 @@ static void element_apply(const Slice& slice, Bunch& b)
         octupole_apply(slice, b);
     else if (t == "hkicker" || t == "vkicker" || t == "kicker")
         kicker_apply(slice, b);
+    else if (t == "solenoid")
+        solenoid_apply(slice, b);
     else
         throw std::runtime_error("FF_element::apply() unknown element type = " + t + ", element name = " + slice.e->name);
 }

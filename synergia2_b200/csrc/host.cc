@@ -414,6 +414,26 @@ inline void bend_complete(double& x, double& xp, double& y, double& yp, double& 
 void quad_kick_cb(double x, double& xp, double y, double& yp, const double* k) { cf_kick(x, xp, y, yp, k); }
 void sext_kick_cb(double x, double& xp, double y, double& yp, const double* k) { thin_sext(x, xp, y, yp, k); }
 void oct_kick_cb(double x, double& xp, double y, double& yp, const double* k) { thin_oct(x, xp, y, yp, k); }
+// solenoid_unit ff_algorithm.h:1317-1356 (reference argument order)
+inline void solenoid_unit(double& x, double& xp, double& y, double& yp, double& cdt, double dpop, double ks,
+                          double ksl, double length, double ref_p, double mass, double ref_cdt)
+{
+    const double uni = 1.0;
+    double p2 = (uni + dpop) * (uni + dpop);
+    double zp = std::sqrt(p2 - xp * xp - yp * yp);
+    double dtheta = ksl / zp;
+    double sn = std::sin(dtheta);
+    double cs = std::cos(dtheta);
+    double xpi = xp, ypi = yp;
+    xp = cs * xpi + sn * ypi;
+    yp = (-sn) * xpi + cs * ypi;
+    cs = cs - uni;
+    x = x + (cs * (-ypi) + sn * xpi) / ks;
+    y = y + ((-sn) * (-ypi) + cs * xpi) / ks;
+    double en = std::sqrt(p2 * ref_p * ref_p + mass * mass);
+    double duration = length / (zp * ref_p / en);
+    cdt = cdt + duration - ref_cdt;
+}
 void kicker_kick_cb(double, double& xp, double, double& yp, const double* k)
 { // thin_kicker_unit ff_algorithm.h:994-1000
     xp = xp + k[0];
@@ -1201,6 +1221,48 @@ static void ops_kicker(const Lattice& lat, const Slice& sl, Bunch& b, std::vecto
                   (int)el.get("yoshida_steps", 4.0));
 }
 
+static void ops_solenoid(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
+{ // ff_solenoid.h:160-248
+    const Element& el = lat.elements[sl.elem];
+    const double length = sl.right - sl.left;
+    double ks = el.get("ks");
+    Refpart& ref_l = b.design;
+    const Refpart& ref_b = b.ref;
+    if (std::fabs(ks) < 1e-12) {
+        ops_drift(sl, b, out);
+        return;
+    }
+    const double ref_p = ref_b.p * (1.0 + ref_b.state[5]);
+    const double brho_l = ref_l.p * (1.0 + ref_l.state[5]) / ref_l.charge;
+    const double brho_b = ref_b.p * (1.0 + ref_b.state[5]) / ref_l.charge;
+    ks = ks * (brho_l / brho_b);
+    const double ksl = ks * length;
+    const double kse = ks * 0.5;
+    // get_reference_cdt_solenoid :125-155
+    double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3], cdt = 0.0, dpop = 0.0;
+    if (sl.ledge) {
+        xp = xp + kse * y;
+        yp = yp - kse * x;
+    }
+    hostff::solenoid_unit(x, xp, y, yp, cdt, dpop, ksl, ks, length, ref_l.p * (1 + dpop), ref_l.mass, 0.0);
+    if (sl.redge) {
+        xp = xp - kse * y;
+        yp = yp + kse * x;
+    }
+    ref_l.state = {x, xp, y, yp, cdt, dpop};
+    MapOp o = new_op(OP_SOLENOID);
+    o.flags = (sl.ledge ? 1 : 0) | (sl.redge ? 2 : 0);
+    o.d[0] = ksl; // passed as `ks`, as the reference does
+    o.d[1] = ks;  // passed as `ksl`
+    o.d[2] = length;
+    o.d[3] = ref_p;
+    o.d[4] = b.ref.mass;
+    o.d[5] = cdt;
+    o.d[6] = kse;
+    out.push_back(o);
+    b.ref.s_n += length;
+}
+
 // FF_element::apply ff_element.h:25-67
 static void ops_slice(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
 {
@@ -1220,8 +1282,9 @@ static void ops_slice(const Lattice& lat, const Slice& sl, Bunch& b, std::vector
         ops_octupole(lat, sl, b, out);
     else if (t == "hkicker" || t == "vkicker" || t == "kicker")
         ops_kicker(lat, sl, b, out);
-    else if (t == "solenoid" || t == "rfcavity" || t == "elens" || t == "nllens" || t == "foil" || t == "dipedge" ||
-             t == "matrix")
+    else if (t == "solenoid")
+        ops_solenoid(lat, sl, b, out);
+    else if (t == "rfcavity" || t == "elens" || t == "nllens" || t == "foil" || t == "dipedge" || t == "matrix")
         throw Error(SB2_ERR_UNSUPPORTED, "element type " + t + " is not on the GPU path of this build (element " +
                                              lat.elements[sl.elem].name + ")");
     else
@@ -1308,7 +1371,7 @@ static bool pass_is_full(const MapOp* ops, int n)
     for (int i = 0; i < n; ++i) {
         const int k = ops[i].kind;
         if (k == OP_QUAD || k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_OCT_YOSHIDA || k == OP_KICK_YOSHIDA ||
-            k == OP_SBEND)
+            k == OP_SBEND || k == OP_SOLENOID)
             return true;
     }
     return false;

@@ -175,6 +175,43 @@ __device__ __forceinline__ void slot_unit(double& x, double& xp, double& y, doub
     xp = xp * ct - zp * st;
 }
 
+// solenoid_unit ff_algorithm.h:1317-1356 in the reference's argument order
+// (its caller passes ks*L as `ks` and ks as `ksl`), with the edge kicks
+// :1358-1372 (flags: 1 entry edge, 2 exit edge); out of line: rare op
+__device__ __noinline__ void solenoid_op(double& x, double& xp, double& y, double& yp, double& cdt, double dpop,
+                                         const double* d, int flags)
+{
+    const double ks = d[0], ksl = d[1], length = d[2], ref_p = d[3], mass = d[4], ref_cdt = d[5], kse = d[6];
+    if (flags & 1) {
+        xp = xp + kse * y;
+        yp = yp - kse * x;
+    }
+    const double uni = 1.0;
+    double p2 = (uni + dpop) * (uni + dpop);
+    double zp = sqrt(p2 - xp * xp - yp * yp);
+    double dtheta = ksl / zp;
+#if SB2_FAST_MAPS
+    double sn, cs;
+    sincos(dtheta, &sn, &cs);
+#else
+    double sn = sin(dtheta);
+    double cs = cos(dtheta);
+#endif
+    double xpi = xp, ypi = yp;
+    xp = cs * xpi + sn * ypi;
+    yp = (-sn) * xpi + cs * ypi;
+    cs = cs - uni;
+    x = x + (cs * (-ypi) + sn * xpi) / ks;
+    y = y + ((-sn) * (-ypi) + cs * xpi) / ks;
+    double en = sqrt(p2 * ref_p * ref_p + mass * mass);
+    double duration = length / (zp * ref_p / en);
+    cdt = cdt + duration - ref_cdt;
+    if (flags & 2) {
+        xp = xp - kse * y;
+        yp = yp + kse * x;
+    }
+}
+
 // bend_unit ff_algorithm.h:255-343
 __device__ __forceinline__ void bend_unit(double& x, double& xp, double& y, double& yp, double& cdt,
                                           double dpop, double theta, double strength, double p_ref,
@@ -535,6 +572,9 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
             if constexpr (kFull) sbend_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
             break;
         }
+        case OP_SOLENOID:
+            if constexpr (kFull) solenoid_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
+            break;
         case OP_SC_KICK:
             sc_kick(p, P, GlobalField{p});
             break;
@@ -661,7 +701,7 @@ bool track_needs_full(const MapOp* ops, int n)
     for (int i = 0; i < n; ++i) {
         int k = ops[i].kind;
         if (k == OP_QUAD || k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_OCT_YOSHIDA || k == OP_KICK_YOSHIDA ||
-            k == OP_SBEND)
+            k == OP_SBEND || k == OP_SOLENOID)
             return true;
     }
     return false;

@@ -55,7 +55,11 @@ def test_gpu_madx_golden(syn, orc, case):
     exp = np.array(case["expected"])
     tol = np.array(case["tol"])
     assert np.all(np.abs(gp[:, :6] - exp) <= tol)
-    assert np.array_equal(gp, op)
+    if case["name"] == "solenoid":  # CUDA's sin/cos vs libm: last-bit differences
+        scale = np.max(np.abs(op[:, :6]), axis=0)
+        assert np.all(np.abs(gp[:, :6] - op[:, :6]) <= 1e-12 * scale)
+    else:
+        assert np.array_equal(gp, op)
     assert gm.all()
 
 
@@ -220,3 +224,17 @@ def test_gpu_octupole_and_kickers_sliced(syn, orc):
     assert np.array_equal(gm, om)
     assert np.array_equal(gp, op)
     assert np.array_equal(b.design_state()[0], sim.design_state()[0])
+
+
+def test_gpu_solenoid_sliced(syn, orc):
+    """Solenoid (FF_solenoid) cut into slices by the split-operator stepper:
+    entry and exit edge kicks only on the end slices; within 1e-12 of the
+    oracle (CUDA's sin/cos vs libm)."""
+    spec = [elem("drift", "d0", l=0.2), elem("solenoid", "s1", l=1.3, ks=0.4), elem("drift", "d1", l=0.5),
+            elem("solenoid", "s2", l=0.6, ks=0.0)]
+    n = 10000
+    p = gaussian_bunch(n, [2e-3, 2e-4, 2e-3, 2e-4, 0.3, 1e-3], 14)
+    (gp, gm, _, b, _), (op, om, _, sim) = run_both(syn, orc, spec, p, "split", 4, 2)
+    assert np.array_equal(gm, om) and np.array_equal(gp[:, 6], op[:, 6])
+    scale = np.max(np.abs(op[:, :6]), axis=0)
+    assert np.all(np.abs(gp[:, :6] - op[:, :6]) <= 1e-12 * scale)
