@@ -1079,6 +1079,85 @@ static void solenoid_apply(const Slice& slice, Bunch& b)
     b.ref.s_n += length;
 }
 
+// thin_rfcavity_pnew / thin_rfcavity_unit ff_algorithm.h:1017-1082
+inline double thin_rfcavity_pnew(double pref, double m, double volt, double phi_s)
+{
+    double E0 = std::sqrt(pref * pref + m * m);
+    double E1 = E0 + volt * std::sin(phi_s);
+    return std::sqrt(E1 * E1 - m * m);
+}
+inline void thin_rfcavity_unit(double& px, double& py, double cdt, double& dpop, double w_rf, double volt,
+                               double phi_s, double m, double old_ref_p, double new_ref_p, const double* mhp, int nh)
+{
+    if (volt == 0.0) return;
+    const double anh_phase = 0.0;
+    double phase_slip_argument = (cdt * (w_rf / pc::c)) + anh_phase;
+    double strength_factor = 0.0;
+    for (int i = 0; i < nh; ++i)
+        strength_factor = strength_factor + mhp[i * 3 + 1] * std::sin(mhp[i * 3] * (phi_s + phase_slip_argument) +
+                                                                      mhp[i * 3 + 2]);
+    double p = old_ref_p * (dpop + 1.0);
+    double E = std::sqrt(p * p + m * m);
+    E = E + volt * strength_factor;
+    px = px * (old_ref_p / new_ref_p);
+    py = py * (old_ref_p / new_ref_p);
+    dpop = std::sqrt((E - m) * (E + m)) / new_ref_p - 1.0;
+}
+
+static void rfcavity_apply(const Slice& slice, Bunch& b)
+{ // ff_rfcavity.h:134-330
+    const Element& elm = *slice.e;
+    const double length = slice.right - slice.left;
+    const double volt = elm.get("volt", 0.0);
+    double lag = elm.get("lag", 0.0);
+    const double freq = elm.get("freq", -1.0);
+    const double delta_freq = elm.get("delta_freq", 0.0);
+    int nh = 1;
+    double mhp[12] = {1.0, 1.0, 0.0};
+    for (int h = 2; h <= 4; ++h) {
+        const std::string sk = "h" + std::to_string(h) + "_str", pk = "h" + std::to_string(h) + "_phase";
+        if (elm.d.count(sk)) {
+            mhp[nh * 3 + 0] = h;
+            mhp[nh * 3 + 1] = elm.get(sk, 0.0);
+            mhp[nh * 3 + 2] = elm.get(pk, 0.0);
+            ++nh;
+        }
+    }
+    const double str = volt * 1.0e-3;
+    while (lag < 0.0) lag += 1.0;
+    while (lag >= 1.0) lag -= 1.0;
+    const double phi_s = 2.0 * M_PI * lag;
+    const double w_rf = 2.0 * M_PI * (freq + delta_freq) * 1.0e6;
+    Refpart& ref_l = b.design;
+    const double pref_b = b.ref.p, m_b = b.ref.mass;
+    const double new_pref_b = thin_rfcavity_pnew(pref_b, m_b, str, phi_s);
+    double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3], cdt = 0.0, dpop = 0.0;
+    const double lp = ref_l.p, lm = ref_l.mass;
+    drift_unit(x, xp, y, yp, cdt, dpop, 0.5 * length, lp, lm, 0.0);
+    double total = cdt;
+    const double ref_cdt_1 = cdt;
+    cdt = 0.0;
+    thin_rfcavity_unit(xp, yp, cdt, dpop, w_rf, str, phi_s, lm, lp, lp, mhp, nh);
+    drift_unit(x, xp, y, yp, cdt, dpop, 0.5 * length, lp, lm, 0.0);
+    total += cdt;
+    const double ref_cdt_2 = cdt;
+    ref_l.state = {x, xp, y, yp, total, 0.0};
+    const bool thin = close_to_zero(length);
+    if (b.n_valid) {
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < b.n_active; ++i) {
+            if (!b.masks[i]) continue;
+            double p0 = b.P(i, 0), p1 = b.P(i, 1), p2 = b.P(i, 2), p3 = b.P(i, 3), p4 = b.P(i, 4), p5 = b.P(i, 5);
+            if (!thin) drift_unit(p0, p1, p2, p3, p4, p5, 0.5 * length, pref_b, m_b, ref_cdt_1);
+            thin_rfcavity_unit(p1, p3, p4, p5, w_rf, str, phi_s, m_b, pref_b, new_pref_b, mhp, nh);
+            if (!thin) drift_unit(p0, p1, p2, p3, p4, p5, 0.5 * length, pref_b, m_b, ref_cdt_2);
+            b.P(i, 0) = p0; b.P(i, 1) = p1; b.P(i, 2) = p2; b.P(i, 3) = p3; b.P(i, 4) = p4; b.P(i, 5) = p5;
+        }
+    }
+    b.ref.set_momentum(new_pref_b);
+    b.ref.s_n += length;
+}
+
 static void element_apply(const Slice& slice, Bunch& b)
 { // ff_element.h:25-67
     const std::string& t = slice.e->type;
@@ -1099,6 +1178,8 @@ static void element_apply(const Slice& slice, Bunch& b)
         kicker_apply(slice, b);
     else if (t == "solenoid")
         solenoid_apply(slice, b);
+    else if (t == "rfcavity")
+        rfcavity_apply(slice, b);
     else
         throw std::runtime_error("FF_element::apply() unknown element type = " + t + ", element name = " + slice.e->name);
 }

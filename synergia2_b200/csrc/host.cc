@@ -1263,6 +1263,79 @@ static void ops_solenoid(const Lattice& lat, const Slice& sl, Bunch& b, std::vec
     b.ref.s_n += length;
 }
 
+static void ops_rfcavity(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
+{ // ff_rfcavity.h:134-330; the bunch reference momentum changes to the new one
+    const Element& elm = lat.elements[sl.elem];
+    const double length = sl.right - sl.left;
+    const double volt = elm.get("volt", 0.0);
+    double lag = elm.get("lag", 0.0);
+    const double freq = elm.get("freq", -1.0);
+    const double delta_freq = elm.get("delta_freq", 0.0);
+    int nh = 1;
+    double mhp[12] = {1.0, 1.0, 0.0};
+    for (int h = 2; h <= 4; ++h) {
+        const std::string sk = "h" + std::to_string(h) + "_str", pk = "h" + std::to_string(h) + "_phase";
+        if (elm.has(sk)) {
+            mhp[nh * 3 + 0] = h;
+            mhp[nh * 3 + 1] = elm.get(sk, 0.0);
+            mhp[nh * 3 + 2] = elm.get(pk, 0.0);
+            ++nh;
+        }
+    }
+    const double str = volt * 1.0e-3;
+    while (lag < 0.0) lag += 1.0;
+    while (lag >= 1.0) lag -= 1.0;
+    const double pi = 3.14159265358979323846;
+    const double phi_s = 2.0 * pi * lag;
+    const double w_rf = 2.0 * pi * (freq + delta_freq) * 1.0e6;
+    Refpart& ref_l = b.design;
+    const double pref_b = b.ref.p, m_b = b.ref.mass;
+    // thin_rfcavity_pnew ff_algorithm.h:1016-1022
+    const double E0 = std::sqrt(pref_b * pref_b + m_b * m_b);
+    const double E1 = E0 + str * std::sin(phi_s);
+    const double new_pref_b = std::sqrt(E1 * E1 - m_b * m_b);
+    // design particle: half drift, cavity at its own momentum, half drift
+    double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3], cdt = 0.0, dpop = 0.0;
+    const double lp = ref_l.p, lm = ref_l.mass;
+    hostff::drift_unit(x, xp, y, yp, cdt, dpop, 0.5 * length, lp, lm, 0.0);
+    double total = cdt;
+    const double ref_cdt_1 = cdt;
+    cdt = 0.0;
+    if (str != 0.0) { // thin_rfcavity_unit with old = new = the design momentum
+        double phase_slip_argument = (cdt * (w_rf / pc::c)) + 0.0;
+        double strength_factor = 0.0;
+        for (int i = 0; i < nh; ++i)
+            strength_factor = strength_factor + mhp[i * 3 + 1] * std::sin(mhp[i * 3] * (phi_s + phase_slip_argument) +
+                                                                          mhp[i * 3 + 2]);
+        double p = lp * (dpop + 1.0);
+        double E = std::sqrt(p * p + lm * lm);
+        E = E + str * strength_factor;
+        xp = xp * (lp / lp);
+        yp = yp * (lp / lp);
+        dpop = std::sqrt((E - lm) * (E + lm)) / lp - 1.0;
+    }
+    hostff::drift_unit(x, xp, y, yp, cdt, dpop, 0.5 * length, lp, lm, 0.0);
+    total += cdt;
+    const double ref_cdt_2 = cdt;
+    ref_l.state = {x, xp, y, yp, total, 0.0};
+    MapOp o = new_op(OP_RFCAVITY);
+    o.steps = nh;
+    o.flags = hostff::close_to_zero(length) ? 1 : 0;
+    o.d[0] = 0.5 * length;
+    o.d[1] = pref_b;
+    o.d[2] = m_b;
+    o.d[3] = ref_cdt_1;
+    o.d[4] = ref_cdt_2;
+    o.d[5] = w_rf;
+    o.d[6] = str;
+    o.d[7] = phi_s;
+    o.d[8] = new_pref_b;
+    for (int i = 0; i < 12; ++i) o.d[9 + i] = mhp[i];
+    out.push_back(o);
+    b.ref.set(b.ref.charge, b.ref.mass, new_pref_b, SB2_REF_MOMENTUM);
+    b.ref.s_n += length;
+}
+
 // FF_element::apply ff_element.h:25-67
 static void ops_slice(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
 {
@@ -1284,7 +1357,9 @@ static void ops_slice(const Lattice& lat, const Slice& sl, Bunch& b, std::vector
         ops_kicker(lat, sl, b, out);
     else if (t == "solenoid")
         ops_solenoid(lat, sl, b, out);
-    else if (t == "rfcavity" || t == "elens" || t == "nllens" || t == "foil" || t == "dipedge" || t == "matrix")
+    else if (t == "rfcavity")
+        ops_rfcavity(lat, sl, b, out);
+    else if (t == "elens" || t == "nllens" || t == "foil" || t == "dipedge" || t == "matrix")
         throw Error(SB2_ERR_UNSUPPORTED, "element type " + t + " is not on the GPU path of this build (element " +
                                              lat.elements[sl.elem].name + ")");
     else
@@ -1371,7 +1446,7 @@ static bool pass_is_full(const MapOp* ops, int n)
     for (int i = 0; i < n; ++i) {
         const int k = ops[i].kind;
         if (k == OP_QUAD || k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_OCT_YOSHIDA || k == OP_KICK_YOSHIDA ||
-            k == OP_SBEND || k == OP_SOLENOID)
+            k == OP_SBEND || k == OP_SOLENOID || k == OP_RFCAVITY)
             return true;
     }
     return false;

@@ -26,6 +26,7 @@ enum OpKind : int32_t {
     OP_KICK_YOSHIDA = 12,  // ff_patterned_propagator.h:110-150 with ff_kicker kick
     OP_KICK_SIMPLE = 13,   // ff_patterned_propagator.h:57-100 (drift-kick-drift)
     OP_SOLENOID = 14,      // ff_solenoid.h:160-248 (edge kicks, solenoid_unit)
+    OP_RFCAVITY = 15,      // ff_rfcavity.h:23-132 (thin, or half drift - kick - half drift)
     OP_AP_FINITE = 20,     // aperture_operation.h:54-86
     OP_AP_CIRCULAR = 21,   // aperture_operation.h:92-116
     OP_AP_ELLIPTICAL = 22, // aperture_operation.h:123-151

@@ -212,6 +212,34 @@ __device__ __noinline__ void solenoid_op(double& x, double& xp, double& y, doubl
     }
 }
 
+// PropThinRFCavity / PropRFCavity ff_rfcavity.h:23-132 with
+// thin_rfcavity_unit ff_algorithm.h:1025-1082 (d: half length, pref,
+// mass, ref_cdt_1, ref_cdt_2, w_rf, volt, phi_s, new pref, mhp[12]; steps =
+// number of harmonics; flags 1: thin)
+__device__ __noinline__ void rfcavity_op(double& x, double& xp, double& y, double& yp, double& cdt, double& dpop,
+                                         const double* d, int nh, int flags)
+{
+    const double half = d[0], pref = d[1], m = d[2], w_rf = d[5], volt = d[6], phi_s = d[7], new_p = d[8];
+    const double* mhp = d + 9;
+    const bool thin = flags & 1;
+    if (!thin) drift_unit(x, xp, y, yp, cdt, dpop, half, pref, m, d[3]);
+    if (volt != 0.0) {
+        const double anh_phase = 0.0;
+        double phase_slip_argument = (cdt * (w_rf / kC)) + anh_phase;
+        double strength_factor = 0.0;
+        for (int i = 0; i < nh; ++i)
+            strength_factor = strength_factor + mhp[i * 3 + 1] * sin(mhp[i * 3] * (phi_s + phase_slip_argument) +
+                                                                     mhp[i * 3 + 2]);
+        double p = pref * (dpop + 1.0);
+        double E = sqrt(p * p + m * m);
+        E = E + volt * strength_factor;
+        xp = xp * (pref / new_p);
+        yp = yp * (pref / new_p);
+        dpop = sqrt((E - m) * (E + m)) / new_p - 1.0;
+    }
+    if (!thin) drift_unit(x, xp, y, yp, cdt, dpop, half, pref, m, d[4]);
+}
+
 // bend_unit ff_algorithm.h:255-343
 __device__ __forceinline__ void bend_unit(double& x, double& xp, double& y, double& yp, double& cdt,
                                           double dpop, double theta, double strength, double p_ref,
@@ -575,6 +603,9 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
         case OP_SOLENOID:
             if constexpr (kFull) solenoid_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
             break;
+        case OP_RFCAVITY:
+            if constexpr (kFull) rfcavity_op(x, xp, y, yp, cdt, dpop, op.d, op.steps, op.flags);
+            break;
         case OP_SC_KICK:
             sc_kick(p, P, GlobalField{p});
             break;
@@ -701,7 +732,7 @@ bool track_needs_full(const MapOp* ops, int n)
     for (int i = 0; i < n; ++i) {
         int k = ops[i].kind;
         if (k == OP_QUAD || k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_OCT_YOSHIDA || k == OP_KICK_YOSHIDA ||
-            k == OP_SBEND || k == OP_SOLENOID)
+            k == OP_SBEND || k == OP_SOLENOID || k == OP_RFCAVITY)
             return true;
     }
     return false;

@@ -120,11 +120,11 @@ def ring_positions(offset=1.0e-3):
 def main():
     cases = []
     # test_madx_elements.cc: drift, quad, sext, quad_long (1e-8), sext_long,
-    # octupole, kickers, solenoid (:248-320)
+    # octupole, kickers, rf cavity, solenoid (:248-320)
     for name, tol in [("drift", 1e-10), ("quad", 1e-10), ("sext", 1e-10), ("quad_long", 1e-8),
                       ("sext_long", 1e-10), ("oct", 1e-10), ("oct_long", 1e-10), ("kicker", 1e-10),
                       ("hkicker", 1e-10), ("vkicker", 1e-10), ("kicker_long", 1e-10), ("hkicker_long", 1e-10),
-                      ("vkicker_long", 1e-10), ("solenoid", 1e-10)]:
+                      ("vkicker_long", 1e-10), ("solenoid", 1e-10), ("rfc", 1e-10)]:
         lattice = parse_seq(os.path.join(LAT, "l_" + name + ".seq"))
         for el in lattice:  # the fixture sets cdt_use_drift on every element (:32-33)
             el["double"]["cdt_use_drift"] = 1.0
