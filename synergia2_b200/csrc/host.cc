@@ -1864,7 +1864,15 @@ struct Engine {
         ++book.n_operators;
     }
 
-    void add_kick() { ops.push_back(new_op(OP_SC_KICK)); }
+    // the kick uses the bunch's reference momentum at the kick (an rf
+    // cavity later in the same pass changes it)
+    void add_kick(const Bunch& b)
+    {
+        MapOp o = new_op(OP_SC_KICK);
+        o.d[0] = b.ref.p;
+        o.d[1] = b.ref.mass;
+        ops.push_back(o);
+    }
 
     // Launch the pending ops.  with_domain: append the moment sums and run
     // the domain computation for a space-charge kick of `time_step`.
@@ -1918,8 +1926,6 @@ struct Engine {
                 tp.gx = sc->d.gx;
                 tp.gy = sc->d.gy;
                 tp.gz = sc->d.gz;
-                tp.kick_pref = b.ref.p;
-                tp.kick_m = b.ref.mass;
                 if (has_mom) tp.moment_partials = sc->mom_partials;
             }
             {
@@ -2079,7 +2085,7 @@ struct Propagator {
                 engine_->flush(b, sc.get(), elem_charge, true, time * 1.0, s);
                 if (sort_active && (b.kicks_since_sort++ % sort_interval) == 0) resort(b, s);
                 sc->solve(b, s);
-                engine_->add_kick();
+                engine_->add_kick(b);
             }
         }
     }
@@ -2319,7 +2325,7 @@ struct ScOperator {
     {
         engine.flush(b, &sc, nullptr, true, time_step, s);
         sc.solve(b, s);
-        engine.add_kick();
+        engine.add_kick(b);
         engine.flush(b, &sc, nullptr, false, 0.0, s);
         cuda_check(cudaStreamSynchronize(s), "sync");
         sc.check_error();

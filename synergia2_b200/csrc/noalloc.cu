@@ -209,8 +209,6 @@ extern "C" sb2_status sb2_sc3d_apply_noalloc(const sb2_sc3d_options* opts, doubl
     tp.gx = d.gx;
     tp.gy = d.gy;
     tp.gz = d.gz;
-    tp.kick_pref = pref;
-    tp.kick_m = mass;
     tp.nops = 1;
     tp.ops[0].kind = OP_MOMENTS;
     if (!o.domain_fixed && (e = launch_track(tp, s))) return cuda_fail(e, "moments pass");
@@ -248,6 +246,8 @@ extern "C" sb2_status sb2_sc3d_apply_noalloc(const sb2_sc3d_options* opts, doubl
     if ((e = launch_convolve(rho, S, ghat, phi, d, tw_x, tw_y, tw_z, state, s))) return cuda_fail(e, "convolve");
     if ((e = launch_efield(phi, E, d.gx, d.gy, d.gz, state, s))) return cuda_fail(e, "efield");
     tp.ops[0].kind = OP_SC_KICK;
+    tp.ops[0].d[0] = pref; // reference momentum and mass of the kick
+    tp.ops[0].d[1] = mass;
     if ((e = launch_track(tp, s))) return cuda_fail(e, "kick pass");
 
     ScState st;

@@ -23,7 +23,6 @@ struct TrackParams {
     const double2* efield;      // (gz,gy,gx) cells x {ex,ey | ez,0}, FP64 path
     const float4* efield32;     // (gz,gy,gx) cells x {ex,ey,ez,0}, mixed path (used when set)
     int32_t gx, gy, gz;
-    double kick_pref, kick_m;
     int32_t nops;
     int32_t write_discards;
     int32_t slot_base;          // aperture slots of this launch: slot_base + [0, kMaxOpsPerPass)

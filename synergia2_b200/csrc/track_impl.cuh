@@ -416,7 +416,7 @@ struct GlobalField {
 // of E at the particle and the kick of xp, yp, dpop.  F::corner supplies
 // the field at the cell's corners.
 template <class F>
-__device__ __forceinline__ void sc_kick(const TrackParams& p, Part& P, const F& field)
+__device__ __forceinline__ void sc_kick(const TrackParams& p, Part& P, const F& field, double pref, double m)
 {
     const ScState& sc = *p.sc;
     if (!sc.valid) return;
@@ -447,7 +447,7 @@ __device__ __forceinline__ void sc_kick(const TrackParams& p, Part& P, const F& 
             vx += w * f.x;
         }
     }
-    const double factor = sc.factor, pref = p.kick_pref, m = p.kick_m;
+    const double factor = sc.factor;
     double pp = pref + P.dpop * pref;
     double Eoc_i = sqrt(pp * pp + m * m);
     double Eoc_f = Eoc_i + factor * (-pref) * vz;
@@ -607,7 +607,7 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
             if constexpr (kFull) rfcavity_op(x, xp, y, yp, cdt, dpop, op.d, op.steps, op.flags);
             break;
         case OP_SC_KICK:
-            sc_kick(p, P, GlobalField{p});
+            sc_kick(p, P, GlobalField{p}, op.d[0], op.d[1]);
             break;
         default:
             break;
