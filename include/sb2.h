@@ -231,6 +231,16 @@ sb2_status sb2_propagator_read_diagnostics(sb2_propagator* p, int32_t max_record
                                            double* s, int32_t* turns);
 int32_t sb2_diagnostics_record_size(void);
 
+/* Lost-particle records (Diagnostics_loss, bunch.h:727-740,
+ * diagnostics_loss.cc:6-34): with capacity > 0, every particle an aperture
+ * discards is recorded on the device with its coordinates at that aperture.
+ * read_losses returns up to max_records records of 10 doubles -- x, xp, y,
+ * yp, cdt, dpop, id, and the repetition, s and s_n of the bunch reference at
+ * the aperture -- ordered by aperture and id.  Not available with CUDA-graph
+ * turns; capacity 0 disables. */
+sb2_status sb2_propagator_set_loss_diagnostics(sb2_propagator* p, int32_t capacity);
+sb2_status sb2_propagator_read_losses(sb2_propagator* p, int32_t max_records, int32_t* count, double* records);
+
 /* ---------------------------------------------------------------------
  * Batch of independent jobs (no counterpart in the reference, which runs
  * bunch trains through one simulator): each job is a (propagator, bunch)

@@ -458,6 +458,21 @@ class Propagator:
         self._allreduce = _lib.ALLREDUCE_FN(cb)  # kept alive with the propagator
         check(lib().sb2_propagator_set_allreduce(self.h, self._allreduce, None, 1 if on_host else 0))
 
+    def set_loss_diagnostics(self, capacity):
+        """Record every particle an aperture discards (Diagnostics_loss),
+        up to `capacity` records; 0 disables."""
+        check(lib().sb2_propagator_set_loss_diagnostics(self.h, int(capacity)))
+        self._loss_cap = int(capacity)
+
+    def losses(self):
+        """Lost-particle records: (k, 10) array of x, xp, y, yp, cdt, dpop,
+        id, repetition, s, s_n, ordered by aperture and id."""
+        cap = getattr(self, "_loss_cap", 0)
+        out = np.zeros((max(cap, 1), 10))
+        n = ctypes.c_int32()
+        check(lib().sb2_propagator_read_losses(self.h, cap, ctypes.byref(n), _pd(out)))
+        return out[: n.value]
+
     def set_diagnostics(self, capacity):
         """Per-turn Diagnostics_full2 records on the device (initial state of
         the first propagate call, then every turn end); 0 disables."""

@@ -78,6 +78,8 @@ SIGNATURES = {
     "sb2_propagator_set_allreduce": (_i32, [_vp, _vp, _vp, _i32]),
     "sb2_propagator_read_diagnostics": (_i32, [_vp, _i32, _pi32, _pd, _pd, _pi32]),
     "sb2_diagnostics_record_size": (_i32, []),
+    "sb2_propagator_set_loss_diagnostics": (_i32, [_vp, _i32]),
+    "sb2_propagator_read_losses": (_i32, [_vp, _i32, _pi32, _pd]),
     "sb2_batch_query": (_i32, [_vp, _i32, _pi32]),
     "sb2_propagator_sc_last": (_i32, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd]),
     "sb2_sc3d_create": (_i32, [_popts, _ppv]),

@@ -1818,6 +1818,12 @@ struct Engine {
     int nslots = 0;
     AllreduceHook* hook = nullptr; // bunch split over ranks
     double* xchg = nullptr;        // [6 moment sums][discards per slot]
+    // Diagnostics_loss: lost-particle records on the device, and per
+    // aperture the (repetition, s, s_n) of the bunch reference at it
+    double* loss_buf = nullptr;
+    int32_t* loss_count = nullptr;
+    int32_t loss_cap = 0;
+    std::vector<std::array<double, 3>>* loss_tags = nullptr;
 
     Engine()
     {
@@ -1852,6 +1858,10 @@ struct Engine {
             if (o.aperture) {
                 MapOp m = op_aperture(lat, o.ap_type, o.ap_slice);
                 m.slot = nslots;
+                if (loss_tags) {
+                    m.d[10] = (double)loss_tags->size();
+                    loss_tags->push_back({(double)b.ref.repetition, b.ref.repetition * b.ref.s + b.ref.s_n, b.ref.s_n});
+                }
                 book.slot_elem[nslots] = o.ap_slice.elem;
                 ++nslots;
                 ops.push_back(m);
@@ -1928,6 +1938,11 @@ struct Engine {
                 tp.gz = sc->d.gz;
                 if (has_mom) tp.moment_partials = sc->mom_partials;
             }
+            if (loss_buf) {
+                tp.loss_buf = loss_buf;
+                tp.loss_count = loss_count;
+                tp.loss_cap = loss_cap;
+            }
             {
                 ProfScope ps(pass_is_full(tp.ops, tp.nops) ? PROF_TRACK_FULL : PROF_TRACK, s);
                 cuda_check(launch_track(tp, s), "track kernel");
@@ -2002,6 +2017,8 @@ struct Propagator {
         dfree(diag_count);
         dfree(diag_partials);
         dfree(diag_tmp);
+        dfree(loss_buf);
+        dfree(loss_count);
     }
 
     bool sorting(const Bunch& b) const { return has_sc && cell_sort && b.n >= 64; }
@@ -2053,6 +2070,7 @@ struct Propagator {
         if (has_sc && !sc) sc.reset(new SpaceCharge(sc_opts));
         engine_->hook = &hook;
         if (sc) sc->hook = &hook;
+        wire_loss();
         if (!elem_charge) {
             elem_charge = dalloc<double>(lat.elements.size(), "element charge");
             cuda_check(cudaMemset(elem_charge, 0, sizeof(double) * std::max<size_t>(1, lat.elements.size())), "memset");
@@ -2168,6 +2186,36 @@ struct Propagator {
     double* diag_tmp = nullptr;
     std::vector<double> diag_s;     // path length s of each record (host: known at launch)
     std::vector<int> diag_turn;     // turns completed at each record
+
+    // ----- Diagnostics_loss ------------------------------------------------
+    int loss_cap = 0;
+    double* loss_buf = nullptr;
+    int32_t* loss_count = nullptr;
+    std::vector<std::array<double, 3>> loss_tags;
+
+    void set_loss_diagnostics(int capacity)
+    {
+        dfree(loss_buf);
+        dfree(loss_count);
+        loss_buf = nullptr;
+        loss_count = nullptr;
+        loss_tags.clear();
+        loss_cap = capacity;
+        if (capacity > 0) {
+            loss_buf = dalloc<double>((size_t)capacity * 8, "loss diagnostics");
+            loss_count = dalloc<int32_t>(1, "loss diagnostics");
+            cuda_check(cudaMemset(loss_count, 0, sizeof(int32_t)), "loss diagnostics");
+        }
+        wire_loss();
+    }
+    void wire_loss()
+    {
+        if (!engine_) return;
+        engine_->loss_buf = loss_buf;
+        engine_->loss_count = loss_count;
+        engine_->loss_cap = loss_cap;
+        engine_->loss_tags = loss_cap > 0 ? &loss_tags : nullptr;
+    }
 
     void set_diagnostics(int capacity)
     {
@@ -2943,6 +2991,8 @@ sb2_status sb2_propagator_set_graphs(sb2_propagator* p, int32_t on)
     SB2_TRY
     SB2_REQUIRE(p, "null propagator");
     if (on && p->p->hook) throw Error(SB2_ERR_UNSUPPORTED, "CUDA-graph turns are not available on a sharded propagator");
+    if (on && p->p->loss_cap)
+        throw Error(SB2_ERR_UNSUPPORTED, "loss diagnostics are not available with CUDA-graph turns");
     p->p->use_graphs = on != 0;
     if (!on) p->p->drop_graphs();
     SB2_CATCH
@@ -3041,6 +3091,49 @@ sb2_status sb2_propagator_read_diagnostics(sb2_propagator* p, int32_t max_record
 }
 
 int32_t sb2_diagnostics_record_size(void) { return kDiagRecord; }
+
+sb2_status sb2_propagator_set_loss_diagnostics(sb2_propagator* p, int32_t capacity)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && capacity >= 0, "bad argument");
+    if (capacity > 0 && p->p->use_graphs)
+        throw Error(SB2_ERR_UNSUPPORTED, "loss diagnostics are not available with CUDA-graph turns");
+    p->p->set_loss_diagnostics(capacity);
+    SB2_CATCH
+}
+
+sb2_status sb2_propagator_read_losses(sb2_propagator* p, int32_t max_records, int32_t* count, double* records)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && count && max_records >= 0, "bad argument");
+    Propagator& P = *p->p;
+    *count = 0;
+    if (!P.loss_cap) return SB2_OK;
+    int32_t dev = 0;
+    cuda_check(cudaMemcpy(&dev, P.loss_count, sizeof(int32_t), cudaMemcpyDeviceToHost), "losses");
+    const int n = std::min(std::min(dev, P.loss_cap), max_records);
+    std::vector<double> raw((size_t)std::max(n, 1) * 8);
+    if (n) cuda_check(cudaMemcpy(raw.data(), P.loss_buf, sizeof(double) * 8 * n, cudaMemcpyDeviceToHost), "losses");
+    // appended in atomic order: sort by (aperture, id) for a stable listing
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+        const double ta = raw[a * 8 + 7], tb = raw[b * 8 + 7];
+        return ta != tb ? ta < tb : raw[a * 8 + 6] < raw[b * 8 + 6];
+    });
+    for (int k = 0; k < n; ++k) {
+        const double* r = &raw[(size_t)order[k] * 8];
+        double* o = records + (size_t)k * 10;
+        for (int j = 0; j < 7; ++j) o[j] = r[j];
+        const size_t tag = (size_t)r[7];
+        const auto t = tag < P.loss_tags.size() ? P.loss_tags[tag] : std::array<double, 3>{-1.0, -1.0, -1.0};
+        o[7] = t[0];
+        o[8] = t[1];
+        o[9] = t[2];
+    }
+    *count = n;
+    SB2_CATCH
+}
 
 sb2_status sb2_batch_launch(sb2_batch* q, int32_t slot, int32_t turns)
 {

@@ -27,6 +27,9 @@ struct TrackParams {
     int32_t write_discards;
     int32_t slot_base;          // aperture slots of this launch: slot_base + [0, kMaxOpsPerPass)
     int32_t fast_maps;          // 1: FMA-contracted maps of the mixed-precision path (track_fast.cu)
+    double* loss_buf;           // lost-particle records [loss_cap][8] (null: off)
+    int32_t* loss_count;        // records appended (device)
+    int32_t loss_cap;
     MapOp ops[kMaxOpsPerPass];
 };
 

@@ -379,6 +379,7 @@ struct Part {
     double x, xp, y, yp, cdt, dpop;
     bool alive;
     int disc;
+    int64_t idx; // position in the bunch arrays (loss records read the id there)
 };
 
 // Field corners for the kick.  Corner c of a cell is read as (ex, ey, ez);
@@ -498,6 +499,20 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
                 P.disc = 1;
                 P.alive = false;
                 atomicAdd(&s_counts[op.slot - p.slot_base], 1);
+                if (p.loss_buf) { // Diagnostics_loss: coordinates at the aperture
+                    const int r = atomicAdd(p.loss_count, 1);
+                    if (r < p.loss_cap) {
+                        double* rec = p.loss_buf + (int64_t)r * 8;
+                        rec[0] = x;
+                        rec[1] = xp;
+                        rec[2] = y;
+                        rec[3] = yp;
+                        rec[4] = cdt;
+                        rec[5] = dpop;
+                        rec[6] = p.parts[P.idx + 6 * p.stride];
+                        rec[7] = op.d[10]; // aperture tag (host table: repetition, s, s_n)
+                    }
+                }
             }
         }
         return;
@@ -686,6 +701,7 @@ __global__ void __launch_bounds__(kTrackThreads, PF ? 3 : TrackOcc<VARIANT>::val
             P[q].alive = cur[q].m != 0;
             in[q] = P[q].alive;
             P[q].disc = 0;
+            P[q].idx = base + q * blockDim.x + threadIdx.x;
         }
         for (int o = 0; o < p.nops; ++o) {
             const MapOp& op = p.ops[o];

@@ -87,3 +87,30 @@ def test_diagnostics_graphs_match_direct(syn, monkeypatch):
         assert np.allclose(a[key], g[key], rtol=1e-10, atol=0), key
     sd = a["std"]
     assert np.all(np.abs(a["mean"] - g["mean"]) <= 1e-10 * np.abs(a["mean"]) + 1e-12 * sd)
+
+
+def test_loss_records_cover_every_lost_particle(syn):
+    """Diagnostics_loss (bunch.h:727-740): every particle an aperture
+    discards is recorded once, with its coordinates at the aperture (the
+    coordinates it keeps afterwards, lost particles being frozen), and with
+    the repetition and path length of the bunch reference there."""
+    from helpers import ring_cell
+    n = 30000
+    p = gaussian_bunch(n, [2e-3, 1e-4, 2e-3, 1e-4, 0.3, 1e-4], 94)
+    lat, ref = product_lattice(ring_cell(radius=0.004))
+    prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(16, 16, 32), 16))
+    prop.set_loss_diagnostics(n)
+    b = syn.Bunch(ref, n, 1e11)
+    b.set_particles(p)
+    prop.propagate(b, 2)
+    gp, gm, gd = b.get_particles()
+    rec = prop.losses()
+    lost = np.where(gm == 0)[0]
+    assert 0 < len(lost) < n
+    ids = rec[:, 6].astype(np.int64)
+    assert np.array_equal(np.sort(ids), lost)
+    assert np.array_equal(rec[:, :6], gp[ids, :6])
+    assert set(np.unique(rec[:, 7])) <= {0.0, 1.0}
+    assert np.all((rec[:, 8] >= 0) & (rec[:, 8] <= 16.0 + 1e-9)) and np.all(rec[:, 9] <= 8.0 + 1e-9)
+    with pytest.raises(syn.SB2Error, match="CUDA-graph"):
+        prop.set_graphs(True)

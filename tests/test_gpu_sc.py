@@ -312,3 +312,39 @@ def test_c3_size_ring_properties(syn):
     num = sum(float(((fields[1][k] - fields[0][k]) ** 2).sum()) for k in ("ex", "ey", "ez"))
     den = sum(float((fields[0][k] ** 2).sum()) for k in ("ex", "ey", "ez"))
     assert np.sqrt(num / den) <= 1e-5
+
+
+@pytest.mark.parametrize("green_fn,fixed", [(0, None), (1, ((0.0, 0.0, 0.0), (1.2e-2, 1.2e-2, 3.0)))])
+def test_split_operator_elements_with_space_charge(syn, orc, green_fn, fixed):
+    """Split_operator_stepper_elements (split_operator_stepper_elements.cc:
+    4-47: kicks per element) with space charge, pointlike Green function and
+    adaptive domain, or linear Green function and a fixed domain: two turns
+    of the ring cell (bends, thin sextupoles, apertures) within 1e-10 of the
+    oracle; lost sets exact."""
+    from helpers import ring_cell
+    n, shape = 40000, (16, 16, 32)
+    p = gaussian_bunch(n, [2e-3, 1e-4, 2e-3, 1e-4, 0.3, 1e-4], 33)
+    spec = ring_cell(radius=0.006)
+    lat, ref = product_lattice(spec)
+    opts = syn.Space_charge_3d_open_hockney_options(*shape)
+    opts.green_fn = green_fn
+    if fixed is not None:
+        opts.set_fixed_domain(*fixed)
+    prop = syn.Propagator(lat, syn.Split_operator_stepper_elements(opts, 2))
+    b = syn.Bunch(ref, n, 1e11)
+    b.set_particles(p)
+    prop.propagate(b, 2)
+    gp, gm, gd = b.get_particles()
+    sim = orc.Sim(oracle_lattice(spec), n, 1e11, stepper=orc.STEPPER_SPLIT_ELEMENTS, num=2,
+                  sc=orc.SCOptions.make(*shape, green_fn=green_fn, fixed=fixed), value=2.5 + MP)
+    sim.set_particles(p)
+    sim.propagate(2)
+    op, om, od = sim.get_particles()
+    assert np.array_equal(gm, om) and np.array_equal(gd, od) and np.array_equal(gp[:, 6], op[:, 6])
+    assert 0 < int(gm.sum()) < n
+    alive = gm.astype(bool)
+    for j in range(6):
+        assert rel_l2(gp[alive, j], op[alive, j]) <= 1e-10, j
+    c = b.counts()
+    nv, nt, rn = sim.counts()
+    assert c["total_num"] == nt and c["real_num"] == rn
