@@ -383,6 +383,7 @@ def main():
     import synergia2_b200 as syn
     from helpers import MP
     L = syn.lib()
+    syn.check(L.sb2_set_device(local))  # the library's own (static) CUDA runtime
     stream = torch.cuda.current_stream()
     sp = ctypes.c_void_p(stream.cuda_stream)
 

@@ -49,6 +49,10 @@ enum {
 const char* sb2_last_error(void);
 /* Library version string. */
 const char* sb2_version(void);
+/* The library links the CUDA runtime statically: sb2_set_device selects the
+ * GPU for this thread's later calls (as cudaSetDevice does for the caller's
+ * own runtime; one process per GPU calls it with its local rank). */
+sb2_status sb2_set_device(int32_t device);
 
 /* Per-category device timing of the library's own launches, measured with
  * CUDA events recorded on the launching stream (the reference's

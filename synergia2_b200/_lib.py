@@ -36,6 +36,7 @@ _ppv = _c.POINTER(_c.c_void_p)
 SIGNATURES = {
     "sb2_last_error": (_cp, []),
     "sb2_version": (_cp, []),
+    "sb2_set_device": (_i32, [_i32]),
     "sb2_profile_enable": (_i32, [_i32]),
     "sb2_profile_read": (_i32, [_i32, _c.POINTER(_cp), _pd, _pi64, _i32]),
     "sb2_sc3d_options_init": (_i32, [_popts, _c.c_int, _c.c_int, _c.c_int]),

@@ -2578,6 +2578,13 @@ extern "C" {
 const char* sb2_last_error(void) { return g_last_error.c_str(); }
 const char* sb2_version(void) { return "synergia2_b200 0.1 (sm_100a)"; }
 
+sb2_status sb2_set_device(int32_t device)
+{
+    SB2_TRY
+    cuda_check(cudaSetDevice(device), "set device");
+    SB2_CATCH
+}
+
 sb2_status sb2_profile_enable(int32_t on)
 {
     SB2_TRY

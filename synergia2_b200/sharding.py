@@ -25,6 +25,9 @@ def attach(propagator, group=None, on_host=None):
     import torch.distributed as dist
     if on_host is None:
         on_host = dist.get_backend(group) != "nccl"
+    if torch.cuda.is_available():  # the library's own (static) CUDA runtime follows torch's device
+        from . import _lib
+        _lib.check(_lib.lib().sb2_set_device(torch.cuda.current_device()))
     if on_host:
         def fn(arr):
             dist.all_reduce(torch.from_numpy(arr), op=dist.ReduceOp.SUM, group=group)
