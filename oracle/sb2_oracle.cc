@@ -322,6 +322,135 @@ inline void bend_unit(double& x, double& xp, double& y, double& yp, double& cdt,
     cdt = cdt + ncdt - cdt_ref;
 }
 
+// bend_edge ff_algorithm.h:366-450: a pole face of angle e as a pure
+// rotation of the particle's circle (bend_unit with term = 0, the face angle
+// in place of the bend angle, no reference-time subtraction)
+inline void bend_edge(double& x, double& xp, double& y, double& yp, double& cdt, double dpop, double e,
+                      std::complex<double> phase, double strength, double p_ref, double m)
+{
+    const double tc = pc::c;
+    double p = p_ref * (dpop + 1.0);
+    double E0 = std::sqrt(p_ref * p_ref + m * m);
+    double E = std::sqrt(p * p + m * m);
+    double igamma = m / E0;
+    double ibeta = 1.0 / std::sqrt(1.0 - igamma * igamma);
+    double csq = pc::c * pc::c * 1e-9;
+    double psq = (dpop + 1.0) * (dpop + 1.0);
+    double Ef = 1.0 / std::sqrt(psq + igamma * igamma * ibeta * ibeta);
+    double beta1 = Ef * xp, beta2 = Ef * yp;
+    double beta3 = Ef * std::sqrt((dpop + 1.0) * (dpop + 1.0) - xp * xp - yp * yp);
+    double vui_r = tc * beta3, vui_i = tc * beta1;
+    double iomega = E / (csq * strength);
+    double bi_r = -vui_i * iomega - 0.0;
+    double bi_i = vui_r * iomega - x;
+    double bf_r = bi_r * phase.real() - bi_i * phase.imag();
+    double bf_i = bi_r * phase.imag() + bi_i * phase.real();
+    double rho = tc * std::sqrt(beta1 * beta1 + beta3 * beta3) * iomega;
+    double dthmphi = std::asin(bi_r / rho) - std::asin(bf_r / rho);
+    double cr = std::cos(dthmphi), ci = std::sin(dthmphi);
+    double vuf_i = vui_r * ci + vui_i * cr;
+    double uf_i = (0.0 + bi_r) * ci + (x + bi_i) * cr - bf_i;
+    double ncdt = -tc * (dthmphi + e) * iomega;
+    x = uf_i;
+    xp = vuf_i / (Ef * tc);
+    y = y + beta2 * ncdt;
+    cdt = cdt + ncdt;
+}
+
+// Sector-magnet multipole potentials (Zolkin, PRAB 20, 043501 (2017),
+// table XII; ff_algorithm.h:596-733): for order n the normal (N) and skew
+// (S) field components in the cylindrical variables rho = 1 + x/r0,
+// v = y/r0.  fr_* is the rho derivative (the y kick), fy_* the v
+// derivative (the x kick).
+namespace zolkin {
+inline double fr_n2(double r, double v) { return -1.0 * (v / r); }
+inline double fr_n3(double r, double v) { return -0.5 * (v / r) * (r * r - 1.0); }
+inline double fr_n4(double r, double v)
+{
+    return (-1.0 / 6.0) * (v / r) * ((-3.0 / 2.0) * (r * r - 1.0) - v * v + 3.0 * r * r * std::log(r));
+}
+inline double fr_n5(double r, double v)
+{
+    return (-1.0 / 12.0) * (v / r) * ((r * r - 1.0) * ((3.0 / 4.0) * (r * r + 1.0) - v * v) - 3.0 * r * r * std::log(r));
+}
+inline double fy_n2(double r, double) { return std::log(r); }
+inline double fy_n3(double r, double v) { return 0.5 * (0.5 * (r * r - 1.0) - v * v - std::log(r)); }
+inline double fy_n4(double r, double v)
+{
+    return -0.25 * (r * r - 1.0) + 0.5 * (0.5 * (r * r + 1.0) - v * v) * std::log(r);
+}
+inline double fy_n5(double r, double v)
+{
+    return 0.125 * (0.125 * (r * r * r * r + 4.0 * r * r - 5.0) - (r * r - 1.0) * v * v + v * v * v * v -
+                    (0.5 + r * r - 2.0 * v * v) * std::log(r));
+}
+inline double fr_s2(double r, double) { return 0.5 / r * (r * r - 1.0); }
+inline double fr_s3(double r, double v) { return 0.5 / r * (-0.5 * (r * r - 1.0) - v * v + r * r * std::log(r)); }
+inline double fr_s4(double r, double v)
+{
+    return 0.25 / r * (0.25 * (r * r * r * r - 1.0) - (r * r - 1.0) * v * v - r * r * std::log(r));
+}
+inline double fr_s5(double r, double v)
+{
+    return 0.125 / r *
+           (-0.625 * r * r * r * r + 0.5 * r * r + 0.125 + (r * r - 1.0) * v * v + v * v * v * v / 3.0 +
+            (1.0 + 0.5 * r * r - 2.0 * v * v) * r * r * std::log(r));
+}
+inline double fy_s2(double, double v) { return v; }
+inline double fy_s3(double r, double v) { return v * std::log(r); }
+inline double fy_s4(double r, double v) { return 0.5 * v * (0.5 * (r * r - 1.0) - v * v / 3.0 - std::log(r)); }
+inline double fy_s5(double r, double v)
+{
+    return -0.25 * v * (r * r - 1.0) + (1.0 / 6.0) * v * (1.5 * (r * r + 1.0) - v * v) * std::log(r);
+}
+} // namespace zolkin
+
+// thin_cf_kick_5 ff_algorithm.h:736-800: orders 2..5 of a combined-function
+// sector bend; prefactor k rho r0^(n-1) multiplied left to right
+inline void thin_cf_kick_5(double x, double& xp, double y, double& yp, double r0, const double* kL)
+{
+    using namespace zolkin;
+    typedef double (*F)(double, double);
+    static const F FYN[4] = {fy_n2, fy_n3, fy_n4, fy_n5}, FYS[4] = {fy_s2, fy_s3, fy_s4, fy_s5};
+    static const F FRN[4] = {fr_n2, fr_n3, fr_n4, fr_n5}, FRS[4] = {fr_s2, fr_s3, fr_s4, fr_s5};
+    double rho = 1.0 + x / r0;
+    double v = y / r0;
+    for (int o = 0; o < 4; ++o) {
+        double kn = kL[2 * o], ks = kL[2 * o + 1];
+        if (!(kn || ks)) continue;
+        double an = kn * rho, as = ks * rho;
+        for (int i = 0; i <= o; ++i) {
+            an = an * r0;
+            as = as * r0;
+        }
+        xp = xp - an * FYN[o](rho, v) + as * FYS[o](rho, v);
+        yp = yp - an * FRN[o](rho, v) + as * FRS[o](rho, v);
+    }
+}
+
+// bend_yoshida6 ff_algorithm.h:2194-2440: per step 10 bend pieces of angle
+// c_j * step angle around 9 cf kicks of d_j * step strength
+inline void bend_yoshida6(double& x, double& xp, double& y, double& yp, double& cdt, double dpop, double pref,
+                          double m, double step_ref_cdt, const double* step_kl, const double* dphi,
+                          const std::complex<double>* phase, const std::complex<double>* term, double r0,
+                          double strength, int steps)
+{
+    const double d[4] = {1.58722492772224294589251207526, -1.99977809735512250728995471397,
+                         -1.82324266348482825773733634154, 2.29714181079092974648453380998};
+    double k[4][10];
+    for (int j = 0; j < 4; ++j)
+        for (int i = 0; i < 10; ++i) k[j][i] = d[j] * step_kl[i];
+    double sub = step_ref_cdt * 0.1;
+    static const int bseq[10] = {0, 1, 1, 2, 3, 3, 2, 1, 1, 0};
+    static const int kseq[9] = {0, 1, 0, 2, 3, 2, 0, 1, 0};
+    for (int s = 0; s < steps; ++s)
+        for (int u = 0; u < 10; ++u) {
+            int j = bseq[u];
+            bend_unit(x, xp, y, yp, cdt, dpop, dphi[j], strength, pref, m, sub, phase[j], term[j]);
+            if (u < 9) thin_cf_kick_5(x, xp, y, yp, r0, k[kseq[u]]);
+        }
+}
+
 // thin kicks ff_algorithm.h:919-963
 inline void thin_dipole_unit(double, double& xp, double, double& yp, const double* kL)
 {
@@ -618,8 +747,10 @@ struct SbendParams { // ff_sbend.h:14-53
     double us_edge_k_x, us_edge_k_y, ds_edge_k_x, ds_edge_k_y;
 };
 
+static void sbend_cf_apply(SbendParams& sp, Bunch& b);
+
 static void sbend_apply(const Slice& slice, Bunch& b)
-{ // ff_sbend.h:741-969, pure dipole branch (cf == 0, no a/b multipoles)
+{ // ff_sbend.h:741-969
     const Element& ele = *slice.e;
     SbendParams sp{};
     double a = ele.get("angle");
@@ -633,16 +764,27 @@ static void sbend_apply(const Slice& slice, Bunch& b)
     sp.e1 = ele.get("e1", 0.0);
     sp.e2 = ele.get("e2", 0.0);
     static const char* kn_names[10] = {"k1", "k1s", "k2", "k2s", "k3", "k3s", "k4", "k4s", "k5", "k5s"};
-    for (int i = 0; i < 10; ++i) sp.k_l[i] = ele.get(kn_names[i], 0.0);
-    for (int i = 0; i < 10; ++i)
-        if (sp.k_l[i] != 0.0)
-            throw std::runtime_error("oracle: combined-function sbend is not part of the restated path");
+    int cf = 0;
+    for (int i = 0; i < 10; ++i) {
+        sp.k_l[i] = ele.get(kn_names[i], 0.0);
+        if (sp.k_l[i] != 0.0) cf = 1 + i / 2;
+    }
+    bool has_mp = false; // ff_sbend.h:790-828: b_i, a_i -> k_l of order i+1
     for (int i = 1; i < 5; ++i) {
         std::string an = "a0", bn = "b0";
         an[1] = '0' + i;
         bn[1] = '0' + i;
-        if (ele.get(an, 0.0) != 0.0 || ele.get(bn, 0.0) != 0.0)
-            throw std::runtime_error("oracle: sbend multipole errors are not part of the restated path");
+        double knv = ele.get(bn, 0.0), ksv = ele.get(an, 0.0);
+        if (knv || ksv) {
+            has_mp = true;
+            double coeff = factorial(i);
+            knv *= a * coeff;
+            ksv *= a * coeff;
+            if (sp.k_l[(i - 1) * 2 + 0] || sp.k_l[(i - 1) * 2 + 1])
+                throw std::runtime_error("having both kn/ks and a/b coefficents are forbidden in sbends");
+            sp.k_l[(i - 1) * 2 + 0] = knv;
+            sp.k_l[(i - 1) * 2 + 1] = ksv;
+        }
     }
     Refpart& ref_l = b.design;
     const Refpart& ref_b = b.ref;
@@ -669,6 +811,10 @@ static void sbend_apply(const Slice& slice, Bunch& b)
     sp.us_edge_k_p = sgn * sp.strength / brho_b;
     sp.ds_edge_k_p = -sgn * sp.strength / brho_b;
     sp.us_edge_k_x = sp.us_edge_k_y = sp.ds_edge_k_x = sp.ds_edge_k_y = 0.0;
+    if (cf != 0 || has_mp) {
+        sbend_cf_apply(sp, b);
+        return;
+    }
 
     // prop_reference ff_sbend.h:478-566
     {
@@ -718,6 +864,80 @@ static void sbend_apply(const Slice& slice, Bunch& b)
             }
             bend_unit(p0, p1, p2, p3, p4, p5, dphi, sp.strength, sp.pref_b, sp.m_b, sp.ref_cdt, phase, term);
             if (sp.redge) {
+                edge_unit(p2, p1, p3, sp.ds_edge_k_x, sp.ds_edge_k_y);
+                slot_unit(p0, p1, p2, p3, p4, p5, sp.ce2, sp.se2, sp.pref_b, sp.m_b);
+            }
+            b.P(i, 0) = p0; b.P(i, 1) = p1; b.P(i, 2) = p2; b.P(i, 3) = p3; b.P(i, 4) = p4; b.P(i, 5) = p5;
+        }
+    }
+    b.ref.s_n += sp.length;
+}
+
+// Combined-function bend: prop_reference_cf ff_sbend.h:568-660 for the
+// design particle, then PropSbendCF ff_sbend.h:221-339 on every particle.
+static void sbend_cf_apply(SbendParams& sp, Bunch& b)
+{
+    const double c[4] = {0.79361246386112147294625603763, -0.206276584816439780698721319354,
+                         -0.118008867881292655922412133144, 0.236949573653050744373598734219};
+    Refpart& ref_l = b.design;
+    const std::complex<double> phase_e1 = std::exp(std::complex<double>(0.0, -sp.e1));
+    const std::complex<double> phase_e2 = std::exp(std::complex<double>(0.0, -sp.e2));
+    const double step_angle = sp.angle / sp.steps;
+    std::complex<double> step_phase[4], step_term[4];
+    double step_dphi[4];
+    for (int j = 0; j < 4; ++j) {
+        double th = c[j] * step_angle;
+        step_phase[j] = std::exp(std::complex<double>(0.0, th));
+        step_term[j] = std::complex<double>(0.0, sp.r0) * std::complex<double>(1.0 - std::cos(th), -std::sin(th));
+        step_dphi[j] = -c[j] * step_angle;
+    }
+    {
+        double pref_l = ref_l.p, m_l = ref_l.mass;
+        double x_l = ref_l.state[0], xp_l = ref_l.state[1], y_l = ref_l.state[2], yp_l = ref_l.state[3];
+        double cdt_l = 0.0, dpop_l = 0.0;
+        double step_length = sp.length / sp.steps;
+        double step_kl[10];
+        for (int i = 0; i < 10; ++i) step_kl[i] = sp.k_l[i] * step_length;
+        if (sp.ledge) {
+            slot_unit(x_l, xp_l, y_l, yp_l, cdt_l, dpop_l, sp.ce1, sp.se1, pref_l, m_l);
+            double p_l = 1.0 + dpop_l;
+            double zp_l = std::sqrt(p_l * p_l - xp_l * xp_l - yp_l * yp_l);
+            sp.us_edge_k_x = sp.us_edge_k_p * (xp_l / zp_l);
+            sp.us_edge_k_y = sp.us_edge_k_p * (yp_l / zp_l);
+            edge_unit(y_l, xp_l, yp_l, sp.us_edge_k_x / sp.scale, sp.us_edge_k_y / sp.scale);
+            bend_edge(x_l, xp_l, y_l, yp_l, cdt_l, dpop_l, sp.e1, phase_e1, sp.strength, pref_l, m_l);
+        }
+        bend_yoshida6(x_l, xp_l, y_l, yp_l, cdt_l, dpop_l, pref_l, m_l, 0.0, step_kl, step_dphi, step_phase,
+                      step_term, sp.r0, sp.strength, sp.steps);
+        if (sp.redge) {
+            bend_edge(x_l, xp_l, y_l, yp_l, cdt_l, dpop_l, sp.e2, phase_e2, sp.strength, pref_l, m_l);
+            double p_l = 1.0 + dpop_l;
+            double zp_l = std::sqrt(p_l * p_l - xp_l * xp_l - yp_l * yp_l);
+            sp.ds_edge_k_x = sp.ds_edge_k_p * (xp_l / zp_l);
+            sp.ds_edge_k_y = sp.ds_edge_k_p * (yp_l / zp_l);
+            edge_unit(y_l, xp_l, yp_l, sp.ds_edge_k_x / sp.scale, sp.ds_edge_k_y / sp.scale);
+            slot_unit(x_l, xp_l, y_l, yp_l, cdt_l, dpop_l, sp.ce2, sp.se2, pref_l, m_l);
+        }
+        ref_l.state = {x_l, xp_l, y_l, yp_l, cdt_l, dpop_l};
+        sp.ref_cdt = cdt_l;
+    }
+    const double step_ref_cdt = sp.ref_cdt / sp.steps;
+    double step_kl[10];
+    for (int i = 0; i < 10; ++i) step_kl[i] = sp.k_l[i] * sp.scale * sp.length / sp.steps;
+    if (b.n_valid) {
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < b.n_active; ++i) {
+            if (!b.masks[i]) continue;
+            double p0 = b.P(i, 0), p1 = b.P(i, 1), p2 = b.P(i, 2), p3 = b.P(i, 3), p4 = b.P(i, 4), p5 = b.P(i, 5);
+            if (sp.ledge) {
+                slot_unit(p0, p1, p2, p3, p4, p5, sp.ce1, sp.se1, sp.pref_b, sp.m_b);
+                edge_unit(p2, p1, p3, sp.us_edge_k_x, sp.us_edge_k_y);
+                bend_edge(p0, p1, p2, p3, p4, p5, sp.e1, phase_e1, sp.strength, sp.pref_b, sp.m_b);
+            }
+            bend_yoshida6(p0, p1, p2, p3, p4, p5, sp.pref_b, sp.m_b, step_ref_cdt, step_kl, step_dphi, step_phase,
+                          step_term, sp.r0, sp.strength, sp.steps);
+            if (sp.redge) {
+                bend_edge(p0, p1, p2, p3, p4, p5, sp.e2, phase_e2, sp.strength, sp.pref_b, sp.m_b);
                 edge_unit(p2, p1, p3, sp.ds_edge_k_x, sp.ds_edge_k_y);
                 slot_unit(p0, p1, p2, p3, p4, p5, sp.ce2, sp.se2, sp.pref_b, sp.m_b);
             }

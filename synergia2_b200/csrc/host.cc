@@ -439,6 +439,13 @@ void kicker_kick_cb(double, double& xp, double, double& yp, const double* k)
     xp = xp + k[0];
     yp = yp + k[1];
 }
+// bend_unit, bend_edge, cf_kick5, bend_yoshida6 (ff_algorithm.h), shared
+// with the particle kernels
+#define SB2_FF inline
+#define SB2_FF_SINCOS 0
+#include "ff_bend.h"
+#undef SB2_FF
+#undef SB2_FF_SINCOS
 } // namespace hostff
 
 // ---------------------------------------------------------------------------
@@ -891,7 +898,12 @@ static void ops_quad(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<
     b.ref.s_n += length;
 }
 
-// FF_sbend::apply ff_sbend.h:741-969 (pure dipole: no k1..k5 / a_n b_n)
+// FF_sbend::apply ff_sbend.h:741-969.  Pure dipoles run PropSbendSimd
+// (one exact bend unit); k1..k5(s) or a_n/b_n multipoles select the
+// combined-function path (prop_reference_cf + PropSbendCF).
+static void ops_sbend_cf(const Slice& sl, Bunch& b, std::vector<MapOp>& out, double a, double l, double length,
+                         double angle, const double* k_l, double e1, double e2);
+
 static void ops_sbend(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
 {
     const Element& ele = lat.elements[sl.elem];
@@ -902,15 +914,34 @@ static void ops_sbend(const Lattice& lat, const Slice& sl, Bunch& b, std::vector
     bool ledge = sl.ledge, redge = sl.redge;
     double e1 = ele.get("e1", 0.0), e2 = ele.get("e2", 0.0);
     static const char* kn_names[10] = {"k1", "k1s", "k2", "k2s", "k3", "k3s", "k4", "k4s", "k5", "k5s"};
-    for (auto nm : kn_names)
-        if (ele.get(nm, 0.0) != 0.0)
-            throw Error(SB2_ERR_UNSUPPORTED, "combined-function sbend (bend_yoshida6) is not supported by this build");
+    double k_l[10];
+    bool cf = false;
+    for (int i = 0; i < 10; ++i) {
+        k_l[i] = ele.get(kn_names[i], 0.0);
+        if (k_l[i] != 0.0) cf = true;
+    }
+    // b_n / a_n multipole moments become the k_l of order n+1, scaled by
+    // angle * n! (ff_sbend.h:790-828)
+    bool has_mp = false;
     for (int i = 1; i < 5; ++i) {
         std::string an = "a0", bn = "b0";
         an[1] = (char)('0' + i);
         bn[1] = (char)('0' + i);
-        if (ele.get(an, 0.0) != 0.0 || ele.get(bn, 0.0) != 0.0)
-            throw Error(SB2_ERR_UNSUPPORTED, "sbend multipole errors are not supported by this build");
+        double kn = ele.get(bn, 0.0), ks = ele.get(an, 0.0);
+        if (kn != 0.0 || ks != 0.0) {
+            has_mp = true;
+            double coeff = hostff::factorial(i);
+            kn *= a * coeff;
+            ks *= a * coeff;
+            if (k_l[(i - 1) * 2 + 0] != 0.0 || k_l[(i - 1) * 2 + 1] != 0.0)
+                throw Error(SB2_ERR_RUNTIME, "having both kn/ks and a/b coefficents are forbidden in sbends");
+            k_l[(i - 1) * 2 + 0] = kn;
+            k_l[(i - 1) * 2 + 1] = ks;
+        }
+    }
+    if (cf || has_mp) {
+        ops_sbend_cf(sl, b, out, a, l, length, angle, k_l, e1, e2);
+        return;
     }
     Refpart& ref_l = b.design;
     const Refpart& ref_b = b.ref;
@@ -970,6 +1001,108 @@ static void ops_sbend(const Lattice& lat, const Slice& sl, Bunch& b, std::vector
         o.d[13] = strength; o.d[14] = pref_b; o.d[15] = m_b; o.d[16] = cdt;
         out.push_back(o);
     }
+    b.ref.s_n += length;
+}
+
+// Combined-function sector bend (ff_sbend.h:568-660 prop_reference_cf,
+// then PropSbendCF :221-339 on the particles).
+static void ops_sbend_cf(const Slice& sl, Bunch& b, std::vector<MapOp>& out, double a, double l, double length,
+                         double angle, const double* k_l, double e1, double e2)
+{
+    const bool ledge = sl.ledge, redge = sl.redge;
+    const double r0 = l / a;
+    const int steps = 6; // FF_algorithm::default_steps
+    Refpart& ref_l = b.design;
+    const Refpart& ref_b = b.ref;
+    const double scale = ref_l.p / (ref_b.p * (1.0 + ref_b.state[5]));
+    if (!redge) e2 = 0;
+    if (!ledge) e1 = 0;
+    const double cnv = 1.0e-9 * pc::c;
+    const double pref_l = ref_l.p;
+    const double brho_l = pref_l / cnv;
+    const double m_l = ref_l.mass;
+    const int charge_l = ref_l.charge;
+    const double pref_b = ref_b.p;
+    const double brho_b = pref_b / cnv;
+    const double m_b = b.ref.mass;
+    const double strength = brho_l * a / l;
+    const double ce1 = std::cos(-e1), se1 = std::sin(-e1), ce2 = std::cos(-e2), se2 = std::sin(-e2);
+    const double sgn = (charge_l > 0) ? 1.0 : -1.0;
+    const double us_edge_k_p = sgn * strength / brho_b;
+    const double ds_edge_k_p = -sgn * strength / brho_b;
+    // bend_edge_phase(e) = exp(-i e); sbend_unit_phase(c, d) = exp(i c d);
+    // sbend_unit_term(c, d, r0) = i r0 (1 - cos(c d) - i sin(c d));
+    // sbend_dphi(c, d) = -c d  (ff_algorithm.h:346-362, 2143-2175)
+    const double pe1_r = std::cos(-e1), pe1_i = std::sin(-e1);
+    const double pe2_r = std::cos(-e2), pe2_i = std::sin(-e2);
+    const double step_angle = angle / steps;
+    double dphi[4], phase[8], term[8];
+    for (int j = 0; j < 4; ++j) {
+        const double th = hostff::kBY6_C[j] * step_angle;
+        phase[2 * j] = std::cos(th);
+        phase[2 * j + 1] = std::sin(th);
+        const double re = 1.0 - std::cos(th), im = -std::sin(th);
+        term[2 * j] = 0.0 * re - r0 * im;
+        term[2 * j + 1] = 0.0 * im + r0 * re;
+        dphi[j] = -hostff::kBY6_C[j] * step_angle;
+    }
+    double us_kx = 0, us_ky = 0, ds_kx = 0, ds_ky = 0;
+    { // prop_reference_cf: the design particle, from dp/p = 0, strengths unscaled
+        double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3];
+        double cdt = 0.0, dpop = 0.0;
+        const double step_length = length / steps;
+        double kr[4][8];
+        for (int i = 0; i < 8; ++i) {
+            const double skl = k_l[i] * step_length;
+            for (int j = 0; j < 4; ++j) kr[j][i] = hostff::kBY6_D[j] * skl;
+        }
+        if (ledge) {
+            hostff::slot_unit(x, xp, y, yp, cdt, dpop, ce1, se1, pref_l, m_l);
+            double p_l = 1.0 + dpop;
+            double zp = std::sqrt(p_l * p_l - xp * xp - yp * yp);
+            us_kx = us_edge_k_p * (xp / zp);
+            us_ky = us_edge_k_p * (yp / zp);
+            double kx = us_kx / scale, ky = us_ky / scale;
+            yp = yp - kx * y;
+            xp = xp + ky * y;
+            hostff::bend_edge(x, xp, y, yp, cdt, dpop, e1, pe1_r, pe1_i, strength, pref_l, m_l);
+        }
+        hostff::bend_yoshida6(x, xp, y, yp, cdt, dpop, pref_l, m_l, 0.0 * 0.1, kr[0], kr[1], kr[2], kr[3], dphi, phase,
+                              term, r0, strength, steps);
+        if (redge) {
+            hostff::bend_edge(x, xp, y, yp, cdt, dpop, e2, pe2_r, pe2_i, strength, pref_l, m_l);
+            double p_l = 1.0 + dpop;
+            double zp = std::sqrt(p_l * p_l - xp * xp - yp * yp);
+            ds_kx = ds_edge_k_p * (xp / zp);
+            ds_ky = ds_edge_k_p * (yp / zp);
+            double kx = ds_kx / scale, ky = ds_ky / scale;
+            yp = yp - kx * y;
+            xp = xp + ky * y;
+            hostff::slot_unit(x, xp, y, yp, cdt, dpop, ce2, se2, pref_l, m_l);
+        }
+        ref_l.state = {x, xp, y, yp, cdt, dpop};
+    }
+    const double ref_cdt = ref_l.state[4];
+    MapOp o = new_op(OP_SBEND_CF);
+    o.flags = (ledge ? 1 : 0) | (redge ? 2 : 0);
+    o.steps = steps;
+    o.d[0] = ce1; o.d[1] = se1; o.d[2] = ce2; o.d[3] = se2;
+    o.d[4] = us_kx; o.d[5] = us_ky; o.d[6] = ds_kx; o.d[7] = ds_ky;
+    o.d[8] = e1; o.d[9] = e2;
+    o.d[10] = pe1_r; o.d[11] = pe1_i; o.d[12] = pe2_r; o.d[13] = pe2_i;
+    o.d[14] = strength; o.d[15] = pref_b; o.d[16] = m_b;
+    o.d[17] = (ref_cdt / steps) * 0.1;
+    o.d[18] = r0;
+    for (int j = 0; j < 4; ++j) o.d[19 + j] = dphi[j];
+    for (int j = 0; j < 8; ++j) {
+        o.d[23 + j] = phase[j];
+        o.d[31 + j] = term[j];
+    }
+    for (int i = 0; i < 8; ++i) { // PropSbendCF step strengths, d_j-scaled
+        const double skl = k_l[i] * scale * length / steps;
+        for (int j = 0; j < 4; ++j) o.d[39 + 8 * j + i] = hostff::kBY6_D[j] * skl;
+    }
+    out.push_back(o);
     b.ref.s_n += length;
 }
 
@@ -1446,7 +1579,7 @@ static bool pass_is_full(const MapOp* ops, int n)
     for (int i = 0; i < n; ++i) {
         const int k = ops[i].kind;
         if (k == OP_QUAD || k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_OCT_YOSHIDA || k == OP_KICK_YOSHIDA ||
-            k == OP_SBEND || k == OP_SOLENOID || k == OP_RFCAVITY)
+            k == OP_SBEND || k == OP_SBEND_CF || k == OP_SOLENOID || k == OP_RFCAVITY)
             return true;
     }
     return false;

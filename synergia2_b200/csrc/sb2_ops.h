@@ -27,6 +27,7 @@ enum OpKind : int32_t {
     OP_KICK_SIMPLE = 13,   // ff_patterned_propagator.h:57-100 (drift-kick-drift)
     OP_SOLENOID = 14,      // ff_solenoid.h:160-248 (edge kicks, solenoid_unit)
     OP_RFCAVITY = 15,      // ff_rfcavity.h:23-132 (thin, or half drift - kick - half drift)
+    OP_SBEND_CF = 16,      // ff_sbend.h:221-339 (bend_yoshida6 with thin_cf_kick_5)
     OP_AP_FINITE = 20,     // aperture_operation.h:54-86
     OP_AP_CIRCULAR = 21,   // aperture_operation.h:92-116
     OP_AP_ELLIPTICAL = 22, // aperture_operation.h:123-151
@@ -47,6 +48,11 @@ enum OpKind : int32_t {
 //  SBEND:        flags bit0 ledge, bit1 redge; 0 ce1 1 se1 2 ce2 3 se2
 //                4 us_kx 5 us_ky 6 ds_kx 7 ds_ky 8 dphi 9 phase_r 10 phase_i
 //                11 term_r 12 term_i 13 strength 14 pref_b 15 m_b 16 ref_cdt
+//  SBEND_CF:     flags as SBEND; steps = Yoshida steps; 0 ce1 1 se1 2 ce2
+//                3 se2 4 us_kx 5 us_ky 6 ds_kx 7 ds_ky 8 e1 9 e2 10-11 entry
+//                face phase 12-13 exit face phase 14 strength 15 pref_b
+//                16 m_b 17 substep ref_cdt 18 r0 19-22 dphi[4] 23-30
+//                phase[4] 31-38 term[4] 39-70 k1..k4 (8 strengths each)
 //  MPOLE:        flags = bitmask of active orders (bit n: order n+1),
 //                kl[16] at 0..15
 //  AP_CIRCULAR:  0 r2, 1 xoff, 2 yoff

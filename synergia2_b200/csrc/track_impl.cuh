@@ -240,51 +240,13 @@ __device__ __noinline__ void rfcavity_op(double& x, double& xp, double& y, doubl
     if (!thin) drift_unit(x, xp, y, yp, cdt, dpop, half, pref, m, d[4]);
 }
 
-// bend_unit ff_algorithm.h:255-343
-__device__ __forceinline__ void bend_unit(double& x, double& xp, double& y, double& yp, double& cdt,
-                                          double dpop, double theta, double strength, double p_ref,
-                                          double m, double cdt_ref, double phase_r, double phase_i,
-                                          double term_r, double term_i)
-{
-    const double uni = 1.0;
-    const double tc = kC;
-    double p0 = p_ref;
-    double p = p_ref * (dpop + uni);
-    double E0 = sqrt(p0 * p0 + m * m);
-    double E = sqrt(p * p + m * m);
-    double igamma = m / E0;
-    double ibeta = uni / sqrt(uni - igamma * igamma);
-    double csq = kC * kC * 1e-9;
-    double psq = (dpop + uni) * (dpop + uni);
-    double Ef = uni / sqrt(psq + igamma * igamma * ibeta * ibeta);
-    double beta1 = Ef * xp;
-    double beta2 = Ef * yp;
-    double beta3 = Ef * sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
-    double ui_r = 0.0, ui_i = x;
-    double vui_r = tc * beta3, vui_i = tc * beta1;
-    double iomega = E / (csq * strength);
-    double bi_r = -vui_i * iomega - ui_r;
-    double bi_i = vui_r * iomega - ui_i;
-    double bf_r = bi_r * phase_r - bi_i * phase_i + term_r;
-    double bf_i = bi_r * phase_i + bi_i * phase_r + term_i;
-    double rho = tc * sqrt(beta1 * beta1 + beta3 * beta3) * iomega;
-    double dthmphi = asin(bi_r / rho) - asin(bf_r / rho);
-#if SB2_FAST_MAPS
-    double expf_r, expf_i;
-    sincos(dthmphi, &expf_i, &expf_r);
-#else
-    double expf_r = cos(dthmphi);
-    double expf_i = sin(dthmphi);
-#endif
-    double vuf_i = vui_r * expf_i + vui_i * expf_r;
-    double uf_i = (ui_r + bi_r) * expf_i + (ui_i + bi_i) * expf_r - bf_i;
-    double dtheta = dthmphi + theta;
-    double ncdt = -tc * dtheta * iomega;
-    x = uf_i;
-    xp = vuf_i / (Ef * tc);
-    y = y + beta2 * ncdt;
-    cdt = cdt + ncdt - cdt_ref;
-}
+// bend_unit, bend_edge, cf_kick5, bend_yoshida6 (ff_algorithm.h), shared
+// with the host's design-particle propagation
+#define SB2_FF __device__ __forceinline__
+#define SB2_FF_SINCOS SB2_FAST_MAPS
+#include "ff_bend.h"
+#undef SB2_FF
+#undef SB2_FF_SINCOS
 
 // PropSbendSimd ff_sbend.h:127-215 for one particle (out of line: rare op)
 __device__ __noinline__ void sbend_op(double& x, double& xp, double& y, double& yp, double& cdt, double& dpop,
@@ -300,6 +262,31 @@ __device__ __noinline__ void sbend_op(double& x, double& xp, double& y, double& 
         yp = yp - d[6] * y;
         xp = xp + d[7] * y;
         slot_unit(x, xp, y, yp, cdt, dpop, d[2], d[3], d[14], d[15]);
+    }
+}
+
+// PropSbendCF ff_sbend.h:221-339 for one particle (combined-function or
+// a_n/b_n multipole bend; out of line: rare op).  d: 0 ce1 1 se1 2 ce2
+// 3 se2 4 us_kx 5 us_ky 6 ds_kx 7 ds_ky 8 e1 9 e2 10-11 entry-face phase
+// 12-13 exit-face phase 14 strength 15 pref_b 16 m_b 17 substep ref_cdt
+// 18 r0 19-22 dphi[4] 23-30 phase[4] 31-38 term[4] 39-70 k1..k4 (8 each);
+// steps in `steps`, flags bit0 entry edge, bit1 exit edge
+__device__ __noinline__ void sbend_cf_op(double& x, double& xp, double& y, double& yp, double& cdt, double& dpop,
+                                         const double* d, int steps, int flags)
+{
+    if (flags & 1) {
+        slot_unit(x, xp, y, yp, cdt, dpop, d[0], d[1], d[15], d[16]);
+        yp = yp - d[4] * y; // edge_unit ff_algorithm.h:139-148
+        xp = xp + d[5] * y;
+        bend_edge(x, xp, y, yp, cdt, dpop, d[8], d[10], d[11], d[14], d[15], d[16]);
+    }
+    bend_yoshida6(x, xp, y, yp, cdt, dpop, d[15], d[16], d[17], d + 39, d + 47, d + 55, d + 63, d + 19, d + 23,
+                  d + 31, d[18], d[14], steps);
+    if (flags & 2) {
+        bend_edge(x, xp, y, yp, cdt, dpop, d[9], d[12], d[13], d[14], d[15], d[16]);
+        yp = yp - d[6] * y;
+        xp = xp + d[7] * y;
+        slot_unit(x, xp, y, yp, cdt, dpop, d[2], d[3], d[15], d[16]);
     }
 }
 
@@ -615,6 +602,10 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
             if constexpr (kFull) sbend_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
             break;
         }
+        case OP_SBEND_CF: {
+            if constexpr (kFull) sbend_cf_op(x, xp, y, yp, cdt, dpop, op.d, op.steps, op.flags);
+            break;
+        }
         case OP_SOLENOID:
             if constexpr (kFull) solenoid_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
             break;
@@ -748,7 +739,7 @@ bool track_needs_full(const MapOp* ops, int n)
     for (int i = 0; i < n; ++i) {
         int k = ops[i].kind;
         if (k == OP_QUAD || k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_OCT_YOSHIDA || k == OP_KICK_YOSHIDA ||
-            k == OP_SBEND || k == OP_SOLENOID || k == OP_RFCAVITY)
+            k == OP_SBEND || k == OP_SBEND_CF || k == OP_SOLENOID || k == OP_RFCAVITY)
             return true;
     }
     return false;

@@ -7,9 +7,11 @@ Sources (paths inside the synergia2 project):
   src/synergia/libFF/tests/test_madx_elements.cc:10-16,100-230   fixture,
       16-particle initial state, de_to_dp, tolerances (1e-10; quad_long 1e-8;
       cdt 100x looser)
-  src/synergia/libFF/tests/test_madx_multipoles.cc:86-190        multipole
-      fixture (positions only), tolerance 1e-15
-  src/synergia/libFF/tests/lattices/l_*.seq, mpole_*.seq           element
+  src/synergia/libFF/tests/test_madx_multipoles.cc:86-212        multipole
+      fixture (positions only), tolerance 1e-15 (combined-function
+      sbends 1e-7)
+  src/synergia/libFF/tests/lattices/l_*.seq, mpole_*.seq,
+      cfsbend_*.seq                                                 element
       definitions
   src/synergia/libFF/tests/lattices/madx_*.out                     MAD-X
       TRACKONE output; rows >= 26 hold the final coordinates, columns 2..7
@@ -88,6 +90,8 @@ def parse_seq(path):
     assert len(elements) == 1, path
     el = list(elements.values())[0]
     lattice = [el]
+    if seq_len is None:  # "machine: line=(...)": no sequence length, no tail drift
+        return lattice
     tail = seq_len - el["double"].get("l", 0.0)
     if tail > 1.0e-6:
         lattice.append({"type": "drift", "name": "auto_drift", "double": {"l": tail}, "vector": {}})
@@ -147,6 +151,15 @@ def main():
             cases.append({"name": name, "lattice": lattice, "p0": P0, "initial": ring_positions(),
                           "expected": expect, "tol": [1e-15] * 6,
                           "source": "src/synergia/libFF/tests/test_madx_multipoles.cc"})
+    # test_madx_multipoles.cc:194-212: combined-function sector bends,
+    # tolerance 1e-7
+    for name in ("cfsbend_dipole", "cfsbend_dipole_skew", "cfsbend_sext", "cfsbend_sext_skew"):
+        lattice = parse_seq(os.path.join(LAT, name + ".seq"))
+        madx = read_madx_output(name)
+        expect = [[r[0], r[1], r[2], r[3], -r[4], r[5]] for r in madx]
+        cases.append({"name": name, "lattice": lattice, "p0": P0, "initial": ring_positions(),
+                      "expected": expect, "tol": [1e-7] * 6,
+                      "source": "src/synergia/libFF/tests/test_madx_multipoles.cc"})
     json.dump({"generated_by": "tests/golden/make_golden.py", "cases": cases}, open(OUT, "w"), indent=0)
     print("wrote", OUT, len(cases), "cases")
 

@@ -55,7 +55,8 @@ def test_gpu_madx_golden(syn, orc, case):
     exp = np.array(case["expected"])
     tol = np.array(case["tol"])
     assert np.all(np.abs(gp[:, :6] - exp) <= tol)
-    if case["name"] in ("solenoid", "rfc"):  # CUDA's sin/cos vs libm: last-bit differences
+    if case["name"] in ("solenoid", "rfc") or case["name"].startswith("cfsbend"):
+        # CUDA's sin/cos/asin/log vs libm: last-bit differences
         scale = np.max(np.abs(op[:, :6]), axis=0)
         assert np.all(np.abs(gp[:, :6] - op[:, :6]) <= 1e-12 * scale)
     else:
@@ -265,3 +266,82 @@ def test_gpu_rfcavity_accelerates_with_space_charge(syn, orc):
     from helpers import rel_l2
     for j in range(6):
         assert rel_l2(gp[:, j], op[:, j]) <= 1e-10, j
+
+
+def _close_to_oracle(gp, gm, op, om, rel=1e-12):
+    assert np.array_equal(gm, om) and np.array_equal(gp[:, 6], op[:, 6])
+    alive = om.astype(bool)
+    scale = np.max(np.abs(op[alive, :6]), axis=0)
+    err = np.max(np.abs(gp[alive, :6] - op[alive, :6]), axis=0) / scale
+    assert np.all(err <= rel), err
+
+
+def test_gpu_cf_sbend_sliced_with_faces(syn, orc):
+    """Combined-function sector bends (FF_sbend with k1..k4(s): PropSbendCF,
+    bend_yoshida6 with thin_cf_kick_5) with entry/exit face angles in a
+    focusing cell, cut into slices by the split-operator stepper so that
+    only the end slices carry the edges, two turns.  The bend map computes
+    x as the difference of two numbers of the size of the bend radius, so
+    last-bit differences (CUDA's asin/sin/cos/log vs libm) grow along the
+    lattice: the GPU must stay within 4x the oracle's own spread under a
+    one-ulp change of the initial coordinates, and that spread itself below
+    1e-8 relative.  The design particle (host side in both) is exact."""
+    spec = [elem("quadrupole", "qf", l=0.5, k1=0.6), elem("drift", "d0", l=0.4),
+            elem("sbend", "b1", l=1.5, angle=0.12, k1=0.05, k2=0.8, k2s=-0.4, e1=0.03, e2=0.05),
+            elem("drift", "d1", l=0.6), elem("quadrupole", "qd", l=0.5, k1=-0.6), elem("drift", "d2", l=0.4),
+            elem("sbend", "b2", l=1.0, angle=0.08, k1s=0.02, k3=3.0, k4=-10.0, k4s=5.0), elem("drift", "d3", l=0.6)]
+    n = 20000
+    p = gaussian_bunch(n, SIG_C0, 21)
+    (gp, gm, _, b, _), (op, om, _, sim) = run_both(syn, orc, spec, p, "split", 6, 2)
+    assert np.array_equal(gm, om) and np.array_equal(gp[:, 6], op[:, 6])
+    q = p.copy()
+    q[:, :6] *= 1.0 + 2.0 ** -52
+    sim2 = orc.Sim(oracle_lattice(spec), n, 1e11, stepper=orc.STEPPER_SPLIT, num=6, value=2.5 + MP)
+    sim2.set_particles(q)
+    sim2.propagate(2)
+    oq = sim2.get_particles()[0]
+    scale = np.max(np.abs(op[:, :6]), axis=0)
+    spread = np.max(np.abs(oq[:, :6] - op[:, :6]), axis=0)
+    assert np.all(spread <= 1e-8 * scale), spread / scale
+    err = np.max(np.abs(gp[:, :6] - op[:, :6]), axis=0)
+    assert np.all(err <= 4.0 * spread + 1e-15 * scale), (err / scale, spread / scale)
+    assert np.array_equal(b.design_state()[0], sim.design_state()[0])  # both on the host (libm)
+
+
+def test_gpu_sbend_multipole_moments_use_cf_path(syn, orc):
+    """An sbend with b_n / a_n moments (ff_sbend.h:790-828: scaled by angle
+    * n! into the combined-function strengths) runs the combined-function
+    integrator, here with space charge in the same passes: one turn agrees
+    with the oracle to 1e-10 (libm vs CUDA and the deposit order), ids and
+    masks exact."""
+    spec = [elem("quadrupole", "q", l=0.4, k1=0.5),
+            elem("sbend", "b", l=2.0, angle=0.1, b1=0.05, a2=0.3, b3=2.0),
+            elem("drift", "d", l=1.0)]
+    n, shape = 30000, (16, 16, 32)
+    p = gaussian_bunch(n, SIG_C0, 22)
+    lat, ref = product_lattice(spec)
+    prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(*shape), 4))
+    b = syn.Bunch(ref, n, 1e11)
+    b.set_particles(p)
+    prop.propagate(b, 1)
+    gp, gm, _ = b.get_particles()
+    sim = orc.Sim(oracle_lattice(spec), n, 1e11, stepper=orc.STEPPER_SPLIT, num=4, sc=orc.SCOptions.make(*shape),
+                  value=2.5 + MP)
+    sim.set_particles(p)
+    sim.propagate(1)
+    op, om, _ = sim.get_particles()
+    assert np.array_equal(gm, om) and np.array_equal(gp[:, 6], op[:, 6])
+    from helpers import rel_l2
+    for j in range(6):
+        assert rel_l2(gp[:, j], op[:, j]) <= 1e-10, j
+    assert np.array_equal(b.design_state()[0], sim.design_state()[0])
+
+
+def test_gpu_sbend_both_k_and_moments_is_an_error(syn):
+    """ff_sbend.h:815-819: k_n and a/b moments of the same order are
+    forbidden together."""
+    lat, ref = product_lattice([elem("sbend", "b", l=1.0, angle=0.1, k1=0.2, b1=0.1)])
+    prop = syn.Propagator(lat, syn.Independent_stepper_elements(1))
+    b = syn.Bunch(ref, 16, 1e10)
+    with pytest.raises(syn.SB2Error, match="forbidden in sbends"):
+        prop.propagate(b, 1)
