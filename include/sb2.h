@@ -132,6 +132,46 @@ sb2_status sb2_bunch_counts(sb2_bunch* b, int64_t* n_active, int64_t* n_valid, i
 /* State [x, xp, y, yp, cdt, dpop] of the design reference particle and
  * s_n of the bunch reference particle. */
 sb2_status sb2_bunch_design_state(sb2_bunch* b, double state[6], double* s_n);
+/* Host-side state of a bunch beyond its particle arrays: the bunch and the
+ * design reference particle (Reference_particle, foundation/
+ * reference_particle.h: charge, four momentum, state, s, s_n, repetition),
+ * the number of turns propagated and the particle counts kept by
+ * update_total_num (bunch_particles.cc:388).  get + set restore a bunch
+ * exactly, which is what a checkpoint needs (simulation/checkpoint.cc:18). */
+typedef struct sb2_refpart_state {
+    int32_t charge;
+    int32_t repetition;
+    double mass, gamma, beta, momentum, energy;
+    double state[6];
+    double s, s_n;
+} sb2_refpart_state;
+typedef struct sb2_bunch_state {
+    sb2_refpart_state ref;    /* the bunch's reference particle */
+    sb2_refpart_state design; /* the lattice (design) reference particle */
+    int32_t design_set;       /* 0 until the first propagate call sets `design` */
+    int32_t turns_done;
+    int64_t n_valid, n_total;
+    double real_num;
+} sb2_bunch_state;
+/* Current state (reads the device counters; synchronous). */
+sb2_status sb2_bunch_get_state(sb2_bunch* b, sb2_bunch_state* out);
+/* Restores a state taken by sb2_bunch_get_state (device counters included);
+ * the mass and charge must match the bunch's. */
+sb2_status sb2_bunch_set_state(sb2_bunch* b, const sb2_bunch_state* in);
+/* Discard flags (bunch_particles.h:40), host N bytes -> device. */
+sb2_status sb2_bunch_set_discards(sb2_bunch* b, const uint8_t* host_discards);
+/* Stream-ordered copy of the resident particles, masks and discards (each
+ * output may be NULL; give pinned host memory for a copy that does not
+ * block) plus the device counts, enqueued on `stream` (cudaStream_t or NULL) behind the work
+ * already queued there, without a host synchronisation.  A bunch that is
+ * in its cell-ordered working copy is scattered back to the caller's order
+ * on the device first and keeps using the working copy afterwards, so a
+ * checkpoint costs one scatter and the copies; later propagate calls on
+ * the same stream are ordered after it.  The counts of the snapshot are
+ * read with sb2_bunch_snapshot_counts once the stream has reached it. */
+sb2_status sb2_bunch_snapshot_async(sb2_bunch* b, double* host_parts, uint8_t* host_masks,
+                                    uint8_t* host_discards, void* stream);
+sb2_status sb2_bunch_snapshot_counts(sb2_bunch* b, int64_t* n_valid, int64_t* n_total, double* real_num);
 /* Synthetic seeded 6D uncorrelated Gaussian on the device (zero means;
  * sigmas for x, xp, y, yp, cdt, dpop); counter-based generator, ids 0..n-1. */
 sb2_status sb2_bunch_populate_gaussian(sb2_bunch* b, const double sigma[6], uint64_t seed);

@@ -26,7 +26,7 @@ from ._lib import SB2Error, check, lib
 __all__ = ["Batch", "pconstants", "Four_momentum", "Reference_particle", "Lattice_element", "Lattice", "Bunch",
            "Space_charge_3d_open_hockney_options", "Space_charge_3d_open_hockney", "Split_operator_stepper",
            "Split_operator_stepper_elements", "Independent_stepper_elements", "Propagator", "SB2Error",
-           "green_fn_t", "precision_t"]
+           "green_fn_t", "precision_t", "BunchSnapshot", "checkpoint_save", "checkpoint_load", "resume"]
 
 
 class pconstants:
@@ -278,12 +278,116 @@ class Bunch:
         check(lib().sb2_bunch_moments(self.h, _pd(mean), _pd(mom2), _pd(emit)))
         return mean, mom2.reshape(6, 6), emit
 
+    def get_state(self):
+        """Host-side state (reference particles, turns, counts): an
+        sb2_bunch_state (include/sb2.h)."""
+        st = _lib.sb2_bunch_state()
+        check(lib().sb2_bunch_get_state(self.h, ctypes.byref(st)))
+        return st
+
+    def set_state(self, st):
+        check(lib().sb2_bunch_set_state(self.h, ctypes.byref(st)))
+
+    def set_discards(self, discards):
+        d = np.ascontiguousarray(discards, dtype=np.uint8)
+        assert d.shape == (self.n,)
+        check(lib().sb2_bunch_set_discards(self.h, _pu8(d)))
+
+    def snapshot(self, stream=None, pinned=True):
+        """Stream-ordered device -> host copy of the resident particles
+        (sb2_bunch_snapshot_async): returns a BunchSnapshot at once; its
+        wait() returns (parts, masks, discards, state) when the copy is done.
+        Later propagate calls on the same stream may be queued meanwhile."""
+        return BunchSnapshot(self, stream, pinned)
+
+    def write_openpmd_file(self, filename, num_part=-1, offset=0):
+        """Bunch::write_openpmd_file (bunch.cc:466-600), openPMD JSON series."""
+        from . import particle_io
+        particle_io.check_extension(filename, (".json",))
+        parts, masks, _ = self.get_particles()
+        st = self.get_state()
+        particle_io.write_openpmd_json(filename, parts, masks, st.ref.mass, st.ref.beta, st.ref.gamma,
+                                       num_part=num_part, offset=offset)
+
+    def read_openpmd_file(self, filename, iteration=None):
+        """Bunch::read_openpmd_file (bunch.cc:189-320): particles, masks and
+        the reference particle's four momentum (from beta_ref / gamma_ref)."""
+        from . import particle_io
+        particle_io.check_extension(filename, (".json",))
+        parts, masks, mass, beta_ref, gamma_ref = particle_io.read_openpmd_json(filename, iteration)
+        if parts.shape[0] != self.n:
+            raise ValueError("file holds %d particles, the bunch %d" % (parts.shape[0], self.n))
+        self.set_particles(parts, masks)
+        st = self.get_state()
+        st.ref.gamma = gamma_ref  # Four_momentum::set_gamma (four_momentum.cc:8-16)
+        st.ref.energy = gamma_ref * st.ref.mass
+        st.ref.beta = math.sqrt(1.0 - 1.0 / (gamma_ref * gamma_ref))
+        st.ref.momentum = gamma_ref * st.ref.beta * st.ref.mass
+        self.set_state(st)
+
+    def write_file(self, filename, num_part=-1, offset=0):
+        """Bunch::write_file (bunch_particles.cc:677-702): datasets
+        "particles" and "particles_masks" in a .npz archive."""
+        from . import particle_io
+        particle_io.check_extension(filename, (".npz",))
+        parts, masks, _ = self.get_particles()
+        particle_io.write_npz(filename, parts, masks, num_part, offset)
+
+    def read_file(self, filename):
+        from . import particle_io
+        particle_io.check_extension(filename, (".npz",))
+        parts, masks = particle_io.read_npz(filename)
+        if parts.shape[0] != self.n:
+            raise ValueError("file holds %d particles, the bunch %d" % (parts.shape[0], self.n))
+        self.set_particles(parts, masks)
+
     def device_arrays(self):
         p, m, d = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
         st = ctypes.c_int64()
         check(lib().sb2_bunch_device_arrays(self.h, ctypes.byref(p), ctypes.byref(st), ctypes.byref(m),
                                             ctypes.byref(d)))
         return p.value, st.value, m.value, d.value
+
+
+class BunchSnapshot:
+    """A pending sb2_bunch_snapshot_async: host buffers (pinned when torch
+    with CUDA is available, so the copy does not block) and the bunch's
+    host-side state captured when the snapshot was queued."""
+
+    def __init__(self, bunch, stream, pinned):
+        n = bunch.n
+        self.bunch, self.stream = bunch, stream
+        self.state = bunch.get_state()
+        self._keep = None
+        if pinned:
+            try:
+                import torch
+                if torch.cuda.is_available():
+                    t = (torch.empty(7 * n, dtype=torch.float64, pin_memory=True),
+                         torch.empty(n, dtype=torch.uint8, pin_memory=True),
+                         torch.empty(n, dtype=torch.uint8, pin_memory=True))
+                    self._keep = t
+                    self.parts = t[0].numpy().reshape((n, 7), order="F")
+                    self.masks, self.discards = t[1].numpy(), t[2].numpy()
+            except ImportError:
+                pass
+        if self._keep is None:
+            self.parts = np.zeros((n, 7), order="F")
+            self.masks = np.zeros(n, np.uint8)
+            self.discards = np.zeros(n, np.uint8)
+        check(lib().sb2_bunch_snapshot_async(bunch.h, _pd(self.parts), _pu8(self.masks), _pu8(self.discards),
+                                             stream))
+
+    def wait(self):
+        import torch
+        if self.stream is None:
+            torch.cuda.synchronize()
+        else:
+            torch.cuda.ExternalStream(int(self.stream)).synchronize()
+        nv, nt, rn = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_double()
+        check(lib().sb2_bunch_snapshot_counts(self.bunch.h, ctypes.byref(nv), ctypes.byref(nt), ctypes.byref(rn)))
+        self.state.n_valid, self.state.n_total, self.state.real_num = nv.value, nt.value, rn.value
+        return self.parts, self.masks, self.discards, self.state
 
 
 class Space_charge_3d_open_hockney_options:
@@ -554,3 +658,6 @@ class Batch:
         d = ctypes.c_int32()
         check(lib().sb2_batch_query(self.h, int(slot), ctypes.byref(d)))
         return bool(d.value)
+
+
+from .checkpoint import checkpoint_load, checkpoint_save, resume  # noqa: E402

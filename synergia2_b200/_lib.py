@@ -31,6 +31,21 @@ class sb2_sc3d_options(ctypes.Structure):
 
 
 _popts = _c.POINTER(sb2_sc3d_options)
+
+
+class sb2_refpart_state(ctypes.Structure):
+    _fields_ = [("charge", _c.c_int32), ("repetition", _c.c_int32), ("mass", _c.c_double), ("gamma", _c.c_double),
+                ("beta", _c.c_double), ("momentum", _c.c_double), ("energy", _c.c_double),
+                ("state", _c.c_double * 6), ("s", _c.c_double), ("s_n", _c.c_double)]
+
+
+class sb2_bunch_state(ctypes.Structure):
+    _fields_ = [("ref", sb2_refpart_state), ("design", sb2_refpart_state), ("design_set", _c.c_int32),
+                ("turns_done", _c.c_int32), ("n_valid", _c.c_int64), ("n_total", _c.c_int64),
+                ("real_num", _c.c_double)]
+
+
+_pstate = _c.POINTER(sb2_bunch_state)
 _ppv = _c.POINTER(_c.c_void_p)
 
 SIGNATURES = {
@@ -49,6 +64,11 @@ SIGNATURES = {
     "sb2_bunch_device_arrays": (_i32, [_vp, _ppv, _pi64, _ppv, _ppv]),
     "sb2_bunch_counts": (_i32, [_vp, _pi64, _pi64, _pi64, _pd]),
     "sb2_bunch_design_state": (_i32, [_vp, _pd, _pd]),
+    "sb2_bunch_get_state": (_i32, [_vp, _pstate]),
+    "sb2_bunch_set_state": (_i32, [_vp, _pstate]),
+    "sb2_bunch_set_discards": (_i32, [_vp, _pu8]),
+    "sb2_bunch_snapshot_async": (_i32, [_vp, _pd, _pu8, _pu8, _vp]),
+    "sb2_bunch_snapshot_counts": (_i32, [_vp, _pi64, _pi64, _pd]),
     "sb2_bunch_populate_gaussian": (_i32, [_vp, _pd, _u64]),
     "sb2_bunch_moments": (_i32, [_vp, _pd, _pd, _pd]),
     "sb2_lattice_create": (_i32, [_cp, _ppv]),

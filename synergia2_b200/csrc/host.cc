@@ -478,6 +478,7 @@ struct Bunch {
     // (nearly) cell order; the home arrays are brought up to date by
     // settle() before anything reads or writes them in the caller's order.
     SortBuffers wc{};
+    BunchCounters* snap_counters = nullptr; // pinned: counts of the last snapshot
     bool permuted = false;    // current data is the working copy
     int kicks_since_sort = 0; // kicks since the working copy was last sorted
 
@@ -525,6 +526,13 @@ struct Bunch {
         permuted = true;
         kicks_since_sort = 0;
     }
+    // home arrays brought up to date from the working copy, which stays in
+    // use (a snapshot for I/O reads the home arrays)
+    void sync_home(cudaStream_t s)
+    {
+        if (!permuted) return;
+        cuda_check(launch_sort_scatter_out(wc, home_parts, home_stride, home_masks, home_discards, s), "sort scatter");
+    }
     // working copy -> home arrays, back in the caller's order
     void settle(cudaStream_t s)
     {
@@ -562,6 +570,7 @@ struct Bunch {
         }
         free_work();
         dfree(counters);
+        if (snap_counters) cudaFreeHost(snap_counters);
     }
     void sync_counters(cudaStream_t s)
     {
@@ -2925,6 +2934,121 @@ sb2_status sb2_bunch_design_state(sb2_bunch* h, double state[6], double* s_n)
     if (state)
         for (int i = 0; i < 6; ++i) state[i] = h->b.design.state[i];
     if (s_n) *s_n = h->b.ref.s_n;
+    SB2_CATCH
+}
+
+static void export_refpart(const Refpart& r, sb2_refpart_state& o)
+{
+    o.charge = r.charge;
+    o.repetition = r.repetition;
+    o.mass = r.mass;
+    o.gamma = r.gamma;
+    o.beta = r.beta;
+    o.momentum = r.p;
+    o.energy = r.energy;
+    for (int i = 0; i < 6; ++i) o.state[i] = r.state[i];
+    o.s = r.s;
+    o.s_n = r.s_n;
+}
+
+static void import_refpart(const sb2_refpart_state& o, Refpart& r)
+{
+    r.charge = o.charge;
+    r.repetition = o.repetition;
+    r.mass = o.mass;
+    r.gamma = o.gamma;
+    r.beta = o.beta;
+    r.p = o.momentum;
+    r.energy = o.energy;
+    for (int i = 0; i < 6; ++i) r.state[i] = o.state[i];
+    r.s = o.s;
+    r.s_n = o.s_n;
+}
+
+sb2_status sb2_bunch_get_state(sb2_bunch* h, sb2_bunch_state* out)
+{
+    SB2_TRY
+    SB2_REQUIRE(h && out, "null argument");
+    Bunch& b = h->b;
+    cuda_check(cudaMemcpy(&b.host_counters, b.counters, sizeof(BunchCounters), cudaMemcpyDeviceToHost), "counters");
+    export_refpart(b.ref, out->ref);
+    export_refpart(b.design, out->design);
+    out->design_set = b.design_set ? 1 : 0;
+    out->turns_done = b.turns_done;
+    out->n_valid = b.host_counters.n_valid;
+    out->n_total = b.host_counters.n_total;
+    out->real_num = b.host_counters.real_num;
+    SB2_CATCH
+}
+
+sb2_status sb2_bunch_set_state(sb2_bunch* h, const sb2_bunch_state* in)
+{
+    SB2_TRY
+    SB2_REQUIRE(h && in, "null argument");
+    Bunch& b = h->b;
+    SB2_REQUIRE(in->ref.mass == b.ref.mass && in->ref.charge == b.ref.charge,
+                "bunch state of a different particle species");
+    SB2_REQUIRE(in->n_valid >= 0 && in->n_valid <= b.n && in->n_total >= in->n_valid, "bunch state counts");
+    import_refpart(in->ref, b.ref);
+    import_refpart(in->design, b.design);
+    b.design_set = in->design_set != 0;
+    b.turns_done = in->turns_done;
+    b.host_counters.n_valid = (int32_t)in->n_valid;
+    b.host_counters.n_total = (int32_t)in->n_total;
+    b.host_counters.real_num = in->real_num;
+    cuda_check(cudaMemcpy(b.counters, &b.host_counters, sizeof(BunchCounters), cudaMemcpyHostToDevice), "counters");
+    SB2_CATCH
+}
+
+sb2_status sb2_bunch_set_discards(sb2_bunch* h, const uint8_t* host_discards)
+{
+    SB2_TRY
+    SB2_REQUIRE(h && host_discards, "null argument");
+    Bunch& b = h->b;
+    b.settle(0);
+    SB2_REQUIRE(b.discards != nullptr, "bunch has no discard array");
+    if (b.n) cuda_check(cudaMemcpy(b.discards, host_discards, b.n, cudaMemcpyHostToDevice), "discards");
+    SB2_CATCH
+}
+
+sb2_status sb2_bunch_snapshot_async(sb2_bunch* h, double* host_parts, uint8_t* host_masks, uint8_t* host_discards,
+                                    void* stream)
+{
+    SB2_TRY
+    SB2_REQUIRE(h, "null bunch");
+    Bunch& b = h->b;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!b.snap_counters)
+        cuda_check(cudaMallocHost((void**)&b.snap_counters, sizeof(BunchCounters)), "snapshot counts");
+    b.sync_home(s);
+    if (b.n > 0) {
+        if (host_parts)
+            cuda_check(cudaMemcpy2DAsync(host_parts, sizeof(double) * b.n, b.home_parts, sizeof(double) * b.home_stride,
+                                         sizeof(double) * b.n, 7, cudaMemcpyDeviceToHost, s),
+                       "snapshot");
+        if (host_masks) cuda_check(cudaMemcpyAsync(host_masks, b.home_masks, b.n, cudaMemcpyDeviceToHost, s), "masks");
+        if (host_discards) {
+            if (b.home_discards)
+                cuda_check(cudaMemcpyAsync(host_discards, b.home_discards, b.n, cudaMemcpyDeviceToHost, s),
+                           "discards");
+            else
+                std::memset(host_discards, 0, b.n);
+        }
+    }
+    cuda_check(cudaMemcpyAsync(b.snap_counters, b.counters, sizeof(BunchCounters), cudaMemcpyDeviceToHost, s),
+               "snapshot counts");
+    SB2_CATCH
+}
+
+sb2_status sb2_bunch_snapshot_counts(sb2_bunch* h, int64_t* n_valid, int64_t* n_total, double* real_num)
+{
+    SB2_TRY
+    SB2_REQUIRE(h, "null bunch");
+    Bunch& b = h->b;
+    SB2_REQUIRE(b.snap_counters != nullptr, "no snapshot taken");
+    if (n_valid) *n_valid = b.snap_counters->n_valid;
+    if (n_total) *n_total = b.snap_counters->n_total;
+    if (real_num) *real_num = b.snap_counters->real_num;
     SB2_CATCH
 }
 
