@@ -11,6 +11,7 @@
 // emitz, emitxy, emitxyz.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "sb2_kernels.h"
@@ -145,6 +146,50 @@ __global__ void diag_final_kernel(const double* __restrict__ partials, int nb, c
     }
     r[95] = sqrt(eliminate_small_negative(det_lead(m2, 4)));
     r[96] = sqrt(eliminate_small_negative(det_lead(m2, 6)));
+}
+
+// update_total_num (bunch_particles.cc:388) after a checkin: n_valid =
+// n_total = number of set masks, counted on the device (16 bytes per thread
+// per load, one atomic per block)
+__global__ void __launch_bounds__(256) count_valid_kernel(const uint8_t* __restrict__ masks, int64_t n,
+                                                          bool aligned16, BunchCounters* c)
+{
+    __shared__ int s_part[8];
+    int cnt = 0;
+    const int64_t nv = aligned16 ? n / 16 : 0; // caller-owned masks may start anywhere
+    const uint4* m16 = reinterpret_cast<const uint4*>(masks);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint4 v = m16[i];
+        const unsigned w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            for (int b = 0; b < 4; ++b) cnt += ((w[k] >> (8 * b)) & 0xffu) != 0;
+    }
+    for (int64_t i = nv * 16 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        cnt += masks[i] != 0;
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += s_part[k];
+        if (t) atomicAdd(&c->n_valid, t);
+    }
+}
+
+__global__ void count_valid_finish_kernel(BunchCounters* c) { c->n_total = c->n_valid; }
+
+cudaError_t launch_count_valid(const uint8_t* masks, int64_t n, BunchCounters* c, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(&c->n_valid, 0, sizeof(int32_t), s);
+    if (e) return e;
+    if (n > 0) {
+        const int64_t blocks = std::min<int64_t>((n / 16 + 255) / 256 + 1, 148 * 8);
+        count_valid_kernel<<<(int)blocks, 256, 0, s>>>(masks, n, ((uintptr_t)masks & 15) == 0, c);
+    }
+    count_valid_finish_kernel<<<1, 1, 0, s>>>(c);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_diagnostics(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,

@@ -2866,17 +2866,17 @@ sb2_status sb2_bunch_set_particles(sb2_bunch* h, const double* host_parts, const
     cuda_check(cudaMemcpy2D(b.parts, sizeof(double) * b.stride, host_parts, sizeof(double) * b.n,
                             sizeof(double) * b.n, 7, cudaMemcpyHostToDevice),
                "checkin");
-    int64_t nv = b.n;
     if (host_masks) {
         cuda_check(cudaMemcpy(b.masks, host_masks, b.n, cudaMemcpyHostToDevice), "masks");
-        nv = 0;
-        for (int64_t i = 0; i < b.n; ++i) nv += host_masks[i] ? 1 : 0;
+        cuda_check(launch_count_valid(b.masks, b.n, b.counters, 0), "count valid");
     } else {
         cuda_check(cudaMemset(b.masks, 1, b.n), "masks");
+        b.host_counters.n_valid = b.host_counters.n_total = (int32_t)b.n;
+        cuda_check(cudaMemcpy(&b.counters->n_valid, &b.host_counters.n_valid, 2 * sizeof(int32_t),
+                              cudaMemcpyHostToDevice),
+                   "counters");
     }
     cuda_check(cudaMemcpy(&b.host_counters, b.counters, sizeof(BunchCounters), cudaMemcpyDeviceToHost), "counters");
-    b.host_counters.n_valid = b.host_counters.n_total = (int32_t)nv;
-    cuda_check(cudaMemcpy(b.counters, &b.host_counters, sizeof(BunchCounters), cudaMemcpyHostToDevice), "counters");
     SB2_CATCH
 }
 

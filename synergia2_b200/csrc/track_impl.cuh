@@ -406,37 +406,50 @@ struct Part {
 struct Corner {
     double x, y, z;
 };
-struct GlobalField {
-    const TrackParams& p;
-    __device__ __forceinline__ void load(int64_t c, Corner& v) const
+// The field of the cell (ix, iy, iz): one base address and the x, y, z
+// strides of the {ex, ey, ez, pad} cells, so the 8 corner loads share one
+// 64-bit index.  FP64 cells are 32 bytes (one 256-bit load each; the
+// cudaMalloc'd field is 32-byte aligned), FP32 cells 16 bytes.
+template <typename T>
+struct CellField;
+template <>
+struct CellField<double> {
+    const double* b;
+    int64_t sy, sz;
+    __device__ __forceinline__ CellField(const TrackParams& p, int ix, int iy, int iz)
+        : b(reinterpret_cast<const double*>(p.efield) + 4 * (((int64_t)iz * p.gy + iy) * p.gx + ix)), sy(4 * (int64_t)p.gx),
+          sz(4 * (int64_t)p.gx * p.gy)
     {
-        if (p.efield32) {
-            const float4 f = p.efield32[c];
-            v.x = f.x;
-            v.y = f.y;
-            v.z = f.z;
-        } else {
-            // one 32-byte load per cell {ex, ey, ez, 0} (sm_100 256-bit
-            // loads; cells are 32-byte aligned in the cudaMalloc'd field)
-            double pad;
-            asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
-                : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(pad)
-                : "l"(p.efield + 2 * c));
-        }
     }
-    // corner c (x fastest, then y, then z) of cell (ix, iy, iz)
-    __device__ __forceinline__ void corner(int ix, int iy, int iz, int c, Corner& v) const
+    // corner c (x fastest, then y, then z)
+    __device__ __forceinline__ void corner(int c, Corner& v) const
     {
-        const int gx = p.gx, gy = p.gy;
-        load(((int64_t)(iz + (c >> 2)) * gy + iy + ((c >> 1) & 1)) * gx + ix + (c & 1), v);
+        const double* a = b + ((c & 1) ? 4 : 0) + (((c >> 1) & 1) ? sy : 0) + ((c >> 2) ? sz : 0);
+        double pad;
+        asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(pad) : "l"(a));
+    }
+};
+template <>
+struct CellField<float> {
+    const float4* b;
+    int64_t sy, sz;
+    __device__ __forceinline__ CellField(const TrackParams& p, int ix, int iy, int iz)
+        : b(p.efield32 + (((int64_t)iz * p.gy + iy) * p.gx + ix)), sy(p.gx), sz((int64_t)p.gx * p.gy)
+    {
+    }
+    __device__ __forceinline__ void corner(int c, Corner& v) const
+    {
+        const float4 f = __ldg(b + ((c & 1) ? 1 : 0) + (((c >> 1) & 1) ? sy : 0) + ((c >> 2) ? sz : 0));
+        v.x = f.x;
+        v.y = f.y;
+        v.z = f.z;
     }
 };
 
 // zyx::alg_kicker space_charge_3d_kernels.h:91-215: trilinear interpolation
-// of E at the particle and the kick of xp, yp, dpop.  F::corner supplies
-// the field at the cell's corners.
-template <class F>
-__device__ __forceinline__ void sc_kick(const TrackParams& p, Part& P, const F& field, double pref, double m)
+// of E (FP64 or FP32 cells, T) at the particle and the kick of xp, yp, dpop.
+template <typename T>
+__device__ __forceinline__ void sc_kick(const TrackParams& p, Part& P, double pref, double m)
 {
     const ScState& sc = *p.sc;
     if (!sc.valid) return;
@@ -452,10 +465,11 @@ __device__ __forceinline__ void sc_kick(const TrackParams& p, Part& P, const F& 
     // then y, then z), one corner at a time
     const double wz[2] = {aoz, oz}, wy[2] = {aoy, oy}, wx[2] = {aox, ox};
     double vx = 0.0, vy = 0.0, vz = 0.0;
+    const CellField<T> field(p, ix, iy, iz);
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
         Corner f;
-        field.corner(ix, iy, iz, c, f);
+        field.corner(c, f);
         const double w = wz[c >> 2] * wy[(c >> 1) & 1] * wx[c & 1];
         if (c == 0) {
             vz = w * f.z;
@@ -646,7 +660,10 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
             if constexpr (kFull) rfcavity_op(x, xp, y, yp, cdt, dpop, op.d, op.steps, op.flags);
             break;
         case OP_SC_KICK:
-            sc_kick(p, P, GlobalField{p}, op.d[0], op.d[1]);
+            if (p.efield32)
+                sc_kick<float>(p, P, op.d[0], op.d[1]);
+            else
+                sc_kick<double>(p, P, op.d[0], op.d[1]);
             break;
         default:
             break;
