@@ -430,23 +430,29 @@ def main():
     value = total_steps / (t_max * 1e-3)
 
     # end to end through the public API with host buffers: checkin from pinned
-    # host memory, K steps (each returning the bunch counts to the host),
-    # checkout to pinned host memory.
+    # host memory, K steps in one propagate call with every step's bunch
+    # counts copied to pinned host memory as the step completes
+    # (sb2_propagator_set_step_counts), checkout to pinned host memory.
     host = torch.empty((7, npart), dtype=torch.float64, pin_memory=True)
     hmask = torch.empty(npart, dtype=torch.uint8, pin_memory=True)
     pd = ctypes.cast(host.data_ptr(), ctypes.POINTER(ctypes.c_double))
     pm = ctypes.cast(hmask.data_ptr(), ctypes.POINTER(ctypes.c_uint8))
     syn.check(L.sb2_bunch_get_particles(bunch.h, pd, pm, None))
-    barrier()
     e2e_steps = 0 if args.no_e2e else args.steps
+    prop.set_step_counts(max(e2e_steps, 1))
+    barrier()
     t0 = time.perf_counter()
     syn.check(L.sb2_bunch_set_particles(bunch.h, pd, pm))
-    for k in range(e2e_steps):
-        syn.check(L.sb2_propagator_propagate_steps(prop.h, bunch.h, args.warmup + k, 1, sp))
+    if e2e_steps:
+        syn.check(L.sb2_propagator_propagate_steps(prop.h, bunch.h, args.warmup + args.steps, e2e_steps, sp))
     syn.check(L.sb2_bunch_get_particles(bunch.h, pd, pm, None))
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    e2e_total = bunch.get_total_num() * max(e2e_steps, 1)
+    step_counts = prop.step_counts()
+    prop.set_step_counts(0)
+    if len(step_counts) != e2e_steps:
+        raise RuntimeError("per-step counts: %d records for %d steps" % (len(step_counts), e2e_steps))
+    e2e_total = sum(c[1] for c in step_counts) if e2e_steps else bunch.get_total_num()
     e2e_s, e2e_total = over_ranks(dist, torch, e2e_s, e2e_total, "cuda")
     bunch_bytes = npart * (7 * 8 + 1)
 
@@ -489,8 +495,8 @@ def main():
             "e2e": {"value": e2e_total / e2e_s, "unit": "macroparticle-steps/s",
                     "h2d_bytes_per_step": bunch_bytes / args.steps,
                     "d2h_bytes_per_step": bunch_bytes / args.steps + 16,
-                    "how": "checkin from pinned host, K steps via the C ABI (bunch counts read back each step), "
-                           "checkout to pinned host"},
+                    "how": "checkin from pinned host, K steps in one C-ABI propagate call with each step's bunch "
+                           "counts copied to pinned host as the step completes, checkout to pinned host"},
             "gpu_launches": gpu_launches,
             "clocks": clk,
         }

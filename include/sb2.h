@@ -285,6 +285,24 @@ int32_t sb2_diagnostics_record_size(void);
 sb2_status sb2_propagator_set_loss_diagnostics(sb2_propagator* p, int32_t capacity);
 sb2_status sb2_propagator_read_losses(sb2_propagator* p, int32_t max_records, int32_t* count, double* records);
 
+/* Per-step counts (the bunch counts a diagnostics registered with
+ * Bunch_simulator::reg_diag_per_step, bunch_simulator.h:230-238, sees at
+ * every step end): with capacity > 0, the k-th step propagated after this
+ * call writes record k -- n_valid (local_num), n_total and real_num after
+ * the step's apertures -- into `host` (pinned memory for copies that do not
+ * block).  The records are written on the device by the pass bookkeeping
+ * and copied in stream order as the passes complete, so the steps of one
+ * propagate call stay fused; they are complete when the call returns.
+ * step_counts_written gives the number of records written.  Not available
+ * with CUDA-graph turns; capacity 0 disables. */
+typedef struct sb2_step_counts {
+    int32_t n_valid;
+    int32_t n_total;
+    double real_num;
+} sb2_step_counts;
+sb2_status sb2_propagator_set_step_counts(sb2_propagator* p, sb2_step_counts* host, int32_t capacity);
+sb2_status sb2_propagator_step_counts_written(sb2_propagator* p, int32_t* count);
+
 /* ---------------------------------------------------------------------
  * Batch of independent jobs (no counterpart in the reference, which runs
  * bunch trains through one simulator): each job is a (propagator, bunch)

@@ -577,6 +577,40 @@ class Propagator:
         check(lib().sb2_propagator_read_losses(self.h, cap, ctypes.byref(n), _pd(out)))
         return out[: n.value]
 
+    def set_step_counts(self, capacity):
+        """Per-step count records (sb2_propagator_set_step_counts): the k-th
+        step propagated from now on writes (n_valid, n_total, real_num) into
+        a host buffer (pinned when torch with CUDA is available)."""
+        self._step_buf = None
+        if capacity > 0:
+            nbytes = ctypes.sizeof(_lib.sb2_step_counts) * capacity
+            keep = None
+            try:
+                import torch
+                if torch.cuda.is_available():
+                    keep = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+            except ImportError:
+                pass
+            if keep is None:
+                keep = np.zeros(nbytes, np.uint8)
+                ptr = keep.ctypes.data
+            else:
+                ptr = keep.data_ptr()
+            self._step_buf = (keep, ptr, capacity)
+            check(lib().sb2_propagator_set_step_counts(self.h, ctypes.c_void_p(ptr), capacity))
+        else:
+            check(lib().sb2_propagator_set_step_counts(self.h, None, 0))
+
+    def step_counts(self):
+        """Records written so far: a list of (n_valid, n_total, real_num)."""
+        if not getattr(self, "_step_buf", None):
+            return []
+        n = ctypes.c_int32()
+        check(lib().sb2_propagator_step_counts_written(self.h, ctypes.byref(n)))
+        _, ptr, cap = self._step_buf
+        recs = (_lib.sb2_step_counts * cap).from_address(ptr)
+        return [(recs[i].n_valid, recs[i].n_total, recs[i].real_num) for i in range(min(n.value, cap))]
+
     def set_diagnostics(self, capacity):
         """Per-turn Diagnostics_full2 records on the device (initial state of
         the first propagate call, then every turn end); 0 disables."""

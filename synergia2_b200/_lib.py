@@ -46,6 +46,10 @@ class sb2_bunch_state(ctypes.Structure):
 
 
 _pstate = _c.POINTER(sb2_bunch_state)
+
+
+class sb2_step_counts(ctypes.Structure):
+    _fields_ = [("n_valid", _c.c_int32), ("n_total", _c.c_int32), ("real_num", _c.c_double)]
 _ppv = _c.POINTER(_c.c_void_p)
 
 SIGNATURES = {
@@ -101,6 +105,8 @@ SIGNATURES = {
     "sb2_diagnostics_record_size": (_i32, []),
     "sb2_propagator_set_loss_diagnostics": (_i32, [_vp, _i32]),
     "sb2_propagator_read_losses": (_i32, [_vp, _i32, _pi32, _pd]),
+    "sb2_propagator_set_step_counts": (_i32, [_vp, _vp, _i32]),
+    "sb2_propagator_step_counts_written": (_i32, [_vp, _pi32]),
     "sb2_batch_query": (_i32, [_vp, _i32, _pi32]),
     "sb2_propagator_sc_last": (_i32, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd]),
     "sb2_sc3d_create": (_i32, [_popts, _ppv]),

@@ -1966,6 +1966,14 @@ struct Engine {
     int32_t* loss_count = nullptr;
     int32_t loss_cap = 0;
     std::vector<std::array<double, 3>>* loss_tags = nullptr;
+    // Per-step count records (the counts Bunch_simulator::reg_diag_per_step
+    // would see): the bookkeeping writes the counters after each step's last
+    // operator into rec_dev; every flush copies the records it completed to
+    // the caller's host buffer in stream order.
+    BunchCounters* rec_dev = nullptr;
+    BunchCounters* rec_host = nullptr;
+    int32_t rec_cap = 0, rec_next = 0;
+    int32_t rec_first = -1, rec_count = 0; // records completed by the pending book
 
     Engine()
     {
@@ -1982,7 +1990,24 @@ struct Engine {
     {
         ops.clear();
         std::memset(&book, 0, sizeof(book));
+        for (int o = 0; o < kMaxOperatorsPerPass; ++o) book.op_record[o] = -1;
         nslots = 0;
+        rec_first = -1;
+        rec_count = 0;
+    }
+
+    // End of a step: an empty operator whose bookkeeping writes the next
+    // count record (when records are enabled and capacity is left).
+    void mark_step_end(Bunch& b, SpaceCharge* sc, double* elem_charge, cudaStream_t s)
+    {
+        if (!rec_cap || rec_next >= rec_cap) return;
+        if (book.n_operators == kMaxOperatorsPerPass) flush(b, sc, elem_charge, false, 0.0, s);
+        const int o = book.n_operators++;
+        book.slot_begin[o] = book.slot_end[o] = nslots;
+        book.op_record[o] = rec_next;
+        if (rec_first < 0) rec_first = rec_next;
+        ++rec_count;
+        ++rec_next;
     }
 
     // One independent operator: its libFF groups and apertures, then
@@ -2103,14 +2128,21 @@ struct Engine {
             dp.elem_charge = elem_charge;
             dp.book = book;
             dp.xchg = nullptr;
+            dp.step_records = rec_count ? rec_dev : nullptr;
             if (hook && *hook) {
                 if (!xchg) xchg = dalloc<double>(6 + kMaxSlotsPerPass, "exchange");
                 cuda_check(launch_shard_pack(dp, nslots, xchg, s), "shard pack");
                 hook->run(xchg, 6 + nslots, s);
                 dp.xchg = xchg;
             }
-            ProfScope ps(PROF_DOMAIN, s);
-            cuda_check(launch_book_domain(dp, s), "domain kernel");
+            {
+                ProfScope ps(PROF_DOMAIN, s);
+                cuda_check(launch_book_domain(dp, s), "domain kernel");
+            }
+            if (rec_count)
+                cuda_check(cudaMemcpyAsync(rec_host + rec_first, rec_dev + rec_first, sizeof(BunchCounters) * rec_count,
+                                           cudaMemcpyDeviceToHost, s),
+                           "step records");
         }
         reset();
     }
@@ -2160,6 +2192,7 @@ struct Propagator {
         dfree(diag_partials);
         dfree(diag_tmp);
         dfree(loss_buf);
+        dfree(step_rec_dev);
         dfree(loss_count);
     }
 
@@ -2213,6 +2246,7 @@ struct Propagator {
         engine_->hook = &hook;
         if (sc) sc->hook = &hook;
         wire_loss();
+        wire_step_counts(false);
         if (!elem_charge) {
             elem_charge = dalloc<double>(lat.elements.size(), "element charge");
             cuda_check(cudaMemset(elem_charge, 0, sizeof(double) * std::max<size_t>(1, lat.elements.size())), "memset");
@@ -2248,6 +2282,7 @@ struct Propagator {
                 engine_->add_kick(b);
             }
         }
+        engine_->mark_step_end(b, sc.get(), elem_charge, s);
     }
 
     void finish(Bunch& b, cudaStream_t s)
@@ -2334,6 +2369,28 @@ struct Propagator {
     double* loss_buf = nullptr;
     int32_t* loss_count = nullptr;
     std::vector<std::array<double, 3>> loss_tags;
+
+    // ----- per-step count records -----------------------------------------
+    int step_rec_cap = 0;
+    BunchCounters* step_rec_dev = nullptr;
+    BunchCounters* step_rec_host = nullptr;
+    void set_step_counts(BunchCounters* host, int capacity)
+    {
+        dfree(step_rec_dev);
+        step_rec_dev = nullptr;
+        step_rec_host = capacity > 0 ? host : nullptr;
+        step_rec_cap = capacity > 0 ? capacity : 0;
+        if (step_rec_cap) step_rec_dev = dalloc<BunchCounters>((size_t)step_rec_cap, "step records");
+        wire_step_counts(true);
+    }
+    void wire_step_counts(bool restart)
+    {
+        if (!engine_) return;
+        engine_->rec_dev = step_rec_dev;
+        engine_->rec_host = step_rec_host;
+        engine_->rec_cap = step_rec_cap;
+        if (restart) engine_->rec_next = 0;
+    }
 
     void set_loss_diagnostics(int capacity)
     {
@@ -3257,6 +3314,8 @@ sb2_status sb2_propagator_set_graphs(sb2_propagator* p, int32_t on)
     if (on && p->p->hook) throw Error(SB2_ERR_UNSUPPORTED, "CUDA-graph turns are not available on a sharded propagator");
     if (on && p->p->loss_cap)
         throw Error(SB2_ERR_UNSUPPORTED, "loss diagnostics are not available with CUDA-graph turns");
+    if (on && p->p->step_rec_cap)
+        throw Error(SB2_ERR_UNSUPPORTED, "per-step count records are not available with CUDA-graph turns");
     p->p->use_graphs = on != 0;
     if (!on) p->p->drop_graphs();
     SB2_CATCH
@@ -3363,6 +3422,25 @@ sb2_status sb2_propagator_set_loss_diagnostics(sb2_propagator* p, int32_t capaci
     if (capacity > 0 && p->p->use_graphs)
         throw Error(SB2_ERR_UNSUPPORTED, "loss diagnostics are not available with CUDA-graph turns");
     p->p->set_loss_diagnostics(capacity);
+    SB2_CATCH
+}
+
+sb2_status sb2_propagator_set_step_counts(sb2_propagator* p, sb2_step_counts* host, int32_t capacity)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && capacity >= 0 && (host || capacity == 0), "bad argument");
+    static_assert(sizeof(sb2_step_counts) == sizeof(BunchCounters), "step record layout");
+    if (capacity > 0 && p->p->use_graphs)
+        throw Error(SB2_ERR_UNSUPPORTED, "per-step count records are not available with CUDA-graph turns");
+    p->p->set_step_counts(reinterpret_cast<BunchCounters*>(host), capacity);
+    SB2_CATCH
+}
+
+sb2_status sb2_propagator_step_counts_written(sb2_propagator* p, int32_t* count)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && count, "bad argument");
+    *count = p->p->engine_ ? p->p->engine_->rec_next : 0;
     SB2_CATCH
 }
 

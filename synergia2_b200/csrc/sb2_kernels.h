@@ -55,6 +55,8 @@ struct DomainParams {
     // the ranks (null for a whole bunch); counters then hold the local
     // n_valid and the global n_total / real_num
     const double* xchg;
+    // per-step count records (PassBook::op_record), may be null
+    BunchCounters* step_records;
 };
 
 struct Dims {

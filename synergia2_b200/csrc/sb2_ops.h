@@ -107,6 +107,9 @@ struct PassBook {
     int32_t slot_begin[kMaxOperatorsPerPass];
     int32_t slot_end[kMaxOperatorsPerPass];
     int32_t slot_elem[kMaxSlotsPerPass];  // lattice element index per slot (or -1)
+    // per-step count record written after this operator (the last one of a
+    // step), or -1
+    int32_t op_record[kMaxOperatorsPerPass];
 };
 
 } // namespace sb2

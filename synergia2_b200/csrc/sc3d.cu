@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(256) book_domain_kernel(const __grid_constant_
         // update_total_num: total = sum over ranks of the valid counts
         c.n_total = p.xchg ? old_total - nd_all : c.n_valid;
         c.real_num = old_total ? c.n_total * c.real_num / old_total : 0.0;
+        if (p.step_records && p.book.op_record[o] >= 0) p.step_records[p.book.op_record[o]] = c;
     }
     *p.counters = c;
     if (!p.compute_domain) return;

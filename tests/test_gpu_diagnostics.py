@@ -114,3 +114,53 @@ def test_loss_records_cover_every_lost_particle(syn):
     assert np.all((rec[:, 8] >= 0) & (rec[:, 8] <= 16.0 + 1e-9)) and np.all(rec[:, 9] <= 8.0 + 1e-9)
     with pytest.raises(syn.SB2Error, match="CUDA-graph"):
         prop.set_graphs(True)
+
+
+def test_gpu_step_counts_match_per_step_calls(syn):
+    """Per-step count records (reg_diag_per_step): the counts after every
+    step of one fused propagate call equal the counts read after each of
+    the same steps run one call at a time (ring cell with losses)."""
+    from helpers import gaussian_bunch, product_lattice, ring_cell
+    n = 20000
+    p = gaussian_bunch(n, [2e-3, 1e-4, 2e-3, 1e-4, 0.3, 1e-4], 41)
+    lat, ref = product_lattice(ring_cell(radius=0.004))
+    a = syn.Propagator(lat, syn.Split_operator_stepper(None, 16))
+    b = syn.Propagator(lat, syn.Split_operator_stepper(None, 16))
+    ns = a.num_steps()
+    ba, bb = syn.Bunch(ref, n, 1e11), syn.Bunch(ref, n, 1e11)
+    ba.set_particles(p)
+    bb.set_particles(p)
+    a.set_step_counts(4 * ns)
+    a.propagate(ba, 2)
+    recs = a.step_counts()
+    assert len(recs) == 2 * ns
+    seen = []
+    for k in range(2 * ns):
+        b.propagate_steps(bb, k, 1)
+        c = bb.counts()
+        seen.append((c["local_num"], c["total_num"], c["real_num"]))
+    assert recs == seen
+    assert recs[-1][0] < n  # particles were lost along the way
+    assert np.array_equal(ba.get_particles()[1], bb.get_particles()[1])
+
+
+def test_gpu_step_counts_with_space_charge_and_graph_refusal(syn):
+    """One record per step with space charge; records continue across calls;
+    CUDA-graph turns and per-step records exclude each other."""
+    from helpers import SIG_C0, fodo_cell, gaussian_bunch, product_lattice
+    n = 20000
+    lat, ref = product_lattice(fodo_cell())
+    prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(16, 16, 32), 8))
+    bunch = syn.Bunch(ref, n, 1e11)
+    bunch.set_particles(gaussian_bunch(n, SIG_C0, 42))
+    prop.set_step_counts(20)
+    prop.propagate_steps(bunch, 0, 5)
+    prop.propagate_steps(bunch, 5, 7)
+    recs = prop.step_counts()
+    assert len(recs) == 12 and all(r == (n, n, 1e11) for r in recs)
+    with pytest.raises(syn.SB2Error, match="graph"):
+        prop.set_graphs(True)
+    prop.set_step_counts(0)
+    prop.set_graphs(True)
+    with pytest.raises(syn.SB2Error, match="graph"):
+        prop.set_step_counts(4)
