@@ -40,7 +40,7 @@ def sc_both(syn, orc, parts, shape, time_step, real_num=1e11, green_fn=1, fixed=
     return gp, g, op, o
 
 
-@pytest.mark.parametrize("shape", [(16, 16, 32), (32, 16, 64), (8, 32, 16)])
+@pytest.mark.parametrize("shape", [(16, 16, 32), (32, 16, 64), (8, 32, 16), (8, 8, 256), (8, 256, 16)])
 @pytest.mark.parametrize("green_fn", [1, 0])
 def test_sc_fields_match_oracle(syn, orc, shape, green_fn):
     n = 200000
