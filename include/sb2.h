@@ -285,6 +285,32 @@ int32_t sb2_diagnostics_record_size(void);
 sb2_status sb2_propagator_set_loss_diagnostics(sb2_propagator* p, int32_t capacity);
 sb2_status sb2_propagator_read_losses(sb2_propagator* p, int32_t max_records, int32_t* count, double* records);
 
+/* Launch shape of the particle passes and the re-sort interval of the
+ * cell-ordered working copy: the search space of the project's autotuner.
+ * light_shape: light passes with 1 particle per thread and the next tile
+ * prefetched (1), 2 per thread with (2) or without (0) prefetch; full_occ:
+ * passes with Yoshida integrators or bends at 2 (128 registers) or 3
+ * (80 registers) CTAs per SM; full_ppt: particles per thread of the 2-CTA
+ * variant (1, 2); quad_variant: passes whose only integrator is the
+ * quadrupole Yoshida use the variant without the others (1) or not (0);
+ * ctas_per_sm: grid of the particle passes (1..12 x the SM count);
+ * sort_interval: re-sort before every k-th space-charge kick.  The defaults
+ * are the values measured best on the FODO workload of 4M macroparticles. */
+typedef struct sb2_tune {
+    int32_t light_shape, full_occ, full_ppt, quad_variant, ctas_per_sm, sort_interval;
+} sb2_tune;
+sb2_status sb2_propagator_get_tune(sb2_propagator* p, sb2_tune* out);
+sb2_status sb2_propagator_set_tune(sb2_propagator* p, const sb2_tune* in);
+/* Coordinate descent over the sb2_tune fields: every candidate propagates
+ * `steps` steps of a scratch copy of `b` (timed with CUDA events) and the
+ * fastest is kept and applied.  The bunch, diagnostics, loss and step
+ * records are left as they were.  trials (may be NULL) receives up to
+ * max_trials rows of 7 doubles -- the six fields and the milliseconds --
+ * and ntrials the number of trials run.  Not available on a sharded
+ * propagator. */
+sb2_status sb2_propagator_autotune(sb2_propagator* p, sb2_bunch* b, int32_t steps, sb2_tune* best, double* trials,
+                                   int32_t max_trials, int32_t* ntrials);
+
 /* Per-step counts (the bunch counts a diagnostics registered with
  * Bunch_simulator::reg_diag_per_step, bunch_simulator.h:230-238, sees at
  * every step end): with capacity > 0, the k-th step propagated after this

@@ -577,6 +577,36 @@ class Propagator:
         check(lib().sb2_propagator_read_losses(self.h, cap, ctypes.byref(n), _pd(out)))
         return out[: n.value]
 
+    _TUNE_FIELDS = ("light_shape", "full_occ", "full_ppt", "quad_variant", "ctas_per_sm", "sort_interval")
+
+    def get_tune(self):
+        """Launch shape of the particle passes and the re-sort interval
+        (sb2_tune) as a dict."""
+        t = _lib.sb2_tune()
+        check(lib().sb2_propagator_get_tune(self.h, ctypes.byref(t)))
+        return {k: getattr(t, k) for k in self._TUNE_FIELDS}
+
+    def set_tune(self, **fields):
+        cur = self.get_tune()
+        cur.update(fields)
+        t = _lib.sb2_tune(*[int(cur[k]) for k in self._TUNE_FIELDS])
+        check(lib().sb2_propagator_set_tune(self.h, ctypes.byref(t)))
+
+    def autotune(self, bunch, steps=16):
+        """The project's autotuner (sb2_propagator_autotune): coordinate
+        descent over get_tune()'s fields, each candidate timed on `steps`
+        steps of a scratch copy of `bunch`; applies and returns the best
+        configuration and the list of trials (fields + milliseconds)."""
+        best = _lib.sb2_tune()
+        cap = 64
+        trials = np.zeros(7 * cap)
+        nt = ctypes.c_int32()
+        check(lib().sb2_propagator_autotune(self.h, bunch.h, int(steps), ctypes.byref(best), _pd(trials), cap,
+                                            ctypes.byref(nt)))
+        rows = trials[: 7 * min(nt.value, cap)].reshape(-1, 7)
+        log = [dict(zip(self._TUNE_FIELDS + ("ms",), [int(v) for v in r[:6]] + [float(r[6])])) for r in rows]
+        return {k: getattr(best, k) for k in self._TUNE_FIELDS}, log
+
     def set_step_counts(self, capacity):
         """Per-step count records (sb2_propagator_set_step_counts): the k-th
         step propagated from now on writes (n_valid, n_total, real_num) into

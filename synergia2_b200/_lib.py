@@ -48,6 +48,11 @@ class sb2_bunch_state(ctypes.Structure):
 _pstate = _c.POINTER(sb2_bunch_state)
 
 
+class sb2_tune(ctypes.Structure):
+    _fields_ = [("light_shape", _c.c_int32), ("full_occ", _c.c_int32), ("full_ppt", _c.c_int32),
+                ("quad_variant", _c.c_int32), ("ctas_per_sm", _c.c_int32), ("sort_interval", _c.c_int32)]
+
+
 class sb2_step_counts(ctypes.Structure):
     _fields_ = [("n_valid", _c.c_int32), ("n_total", _c.c_int32), ("real_num", _c.c_double)]
 _ppv = _c.POINTER(_c.c_void_p)
@@ -105,6 +110,9 @@ SIGNATURES = {
     "sb2_diagnostics_record_size": (_i32, []),
     "sb2_propagator_set_loss_diagnostics": (_i32, [_vp, _i32]),
     "sb2_propagator_read_losses": (_i32, [_vp, _i32, _pi32, _pd]),
+    "sb2_propagator_get_tune": (_i32, [_vp, _vp]),
+    "sb2_propagator_set_tune": (_i32, [_vp, _vp]),
+    "sb2_propagator_autotune": (_i32, [_vp, _vp, _i32, _vp, _pd, _i32, _pi32]),
     "sb2_propagator_set_step_counts": (_i32, [_vp, _vp, _i32]),
     "sb2_propagator_step_counts_written": (_i32, [_vp, _pi32]),
     "sb2_batch_query": (_i32, [_vp, _i32, _pi32]),

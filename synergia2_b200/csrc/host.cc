@@ -1790,7 +1790,7 @@ struct SpaceCharge {
         ghat = dalloc<double>((size_t)(d.nx / 2 + 1) * (d.ny / 2 + 1) * (d.nz / 2 + 1), "ghat");
         state = dalloc<ScState>(1, "sc state");
         n_partials = track_grid_blocks();
-        mom_partials = dalloc<double>((size_t)n_partials * 6, "moments");
+        mom_partials = dalloc<double>((size_t)track_grid_blocks(kMaxCtasPerSm) * 6, "moments"); // any tuned grid
         cuda_check(cudaMemset(state, 0, sizeof(ScState)), "memset");
         tw_x = twiddles(d.nx);
         tw_y = twiddles(d.ny);
@@ -1972,6 +1972,7 @@ struct Engine {
     // the caller's host buffer in stream order.
     BunchCounters* rec_dev = nullptr;
     BunchCounters* rec_host = nullptr;
+    TrackTune tune = track_tune_defaults(); // launch shape of the particle passes
     int32_t rec_cap = 0, rec_next = 0;
     int32_t rec_first = -1, rec_count = 0; // records completed by the pending book
 
@@ -2056,6 +2057,7 @@ struct Engine {
     void flush(Bunch& b, SpaceCharge* sc, double* elem_charge, bool with_domain, double time_step, cudaStream_t s)
     {
         if (with_domain && !sc->o.domain_fixed) ops.push_back(new_op(OP_MOMENTS));
+        if (sc) sc->n_partials = track_grid_blocks(tune.ctas_per_sm); // one moment partial per pass block
         if (g_sig.sig) {
             // a replayed graph reads the arrays it was captured with
             const void* arrays[5] = {b.parts, b.masks, b.discards, b.counters, (const void*)(intptr_t)b.n};
@@ -2064,6 +2066,7 @@ struct Engine {
             sig_append(&nops, sizeof(nops));
             if (nops) sig_append(ops.data(), sizeof(MapOp) * nops);
             sig_append(&book, sizeof(book));
+            sig_append(&tune, sizeof(tune));
             sig_append(&with_domain, sizeof(with_domain));
             sig_append(&time_step, sizeof(time_step));
         }
@@ -2112,7 +2115,7 @@ struct Engine {
             }
             {
                 ProfScope ps(pass_is_full(tp.ops, tp.nops) ? PROF_TRACK_FULL : PROF_TRACK, s);
-                cuda_check(launch_track(tp, s), "track kernel");
+                cuda_check(launch_track(tp, tune, s), "track kernel");
             }
             i += n;
         }
@@ -2164,6 +2167,7 @@ struct Propagator {
     // cell-ordered working copy of the bunch (space-charge runs only)
     bool cell_sort = true;
     int sort_interval = 4; // re-sort before every k-th space-charge kick (measured best of 1, 2, 4, 8 at 4M particles)
+    TrackTune tune = track_tune_defaults(); // launch shape of the particle passes
     int32_t* sort_scratch = nullptr; // histogram, offsets, cursors and block sums of the counting sort
 
     Propagator(const Lattice& l, int stepper_kind, int n, const sb2_sc3d_options* opts)
@@ -2244,6 +2248,7 @@ struct Propagator {
         if (!engine_) engine_.reset(new Engine());
         if (has_sc && !sc) sc.reset(new SpaceCharge(sc_opts));
         engine_->hook = &hook;
+        engine_->tune = tune;
         if (sc) sc->hook = &hook;
         wire_loss();
         wire_step_counts(false);
@@ -2369,6 +2374,143 @@ struct Propagator {
     double* loss_buf = nullptr;
     int32_t* loss_count = nullptr;
     std::vector<std::array<double, 3>> loss_tags;
+
+    // ----- autotuning -------------------------------------------------------
+    // Coordinate descent over the particle-pass launch shapes and the re-sort
+    // interval: every candidate propagates `steps` steps of a scratch copy of
+    // the bunch (CUDA events around the call) and the fastest is kept.  The
+    // bunch, the diagnostics, the loss and step records and the per-element
+    // lost charge are left as they were.  Each trial appends (light_shape,
+    // full_occ, full_ppt, quad_variant, ctas_per_sm, sort_interval, ms).
+    void apply_tune(const TrackTune& t, int si)
+    {
+        tune = t;
+        sort_interval = si;
+        if (engine_) engine_->tune = t;
+        drop_graphs();
+    }
+    void autotune(Bunch& b, int steps, std::vector<std::array<double, 7>>& log)
+    {
+        if (hook) throw Error(SB2_ERR_UNSUPPORTED, "autotuning is not available on a sharded propagator");
+        if (steps < 1) throw Error(SB2_ERR_INVALID, "autotune: steps must be >= 1");
+        ensure_device();
+        b.sync_home(0);
+        Bunch t;
+        t.device = b.device;
+        t.n = b.n;
+        t.stride = std::max<int64_t>(b.n, 1);
+        t.owns = true;
+        t.parts = dalloc<double>((size_t)7 * t.stride, "autotune bunch");
+        t.masks = dalloc<uint8_t>(t.stride, "autotune bunch");
+        t.discards = dalloc<uint8_t>(t.stride, "autotune bunch");
+        t.counters = dalloc<BunchCounters>(1, "autotune bunch");
+        t.set_home();
+        const size_t ne = std::max<size_t>(1, lat.elements.size());
+        double* keep_charge = dalloc<double>(ne, "autotune");
+        cuda_check(cudaMemcpy(keep_charge, elem_charge, sizeof(double) * ne, cudaMemcpyDeviceToDevice), "autotune");
+        const int keep_diag = diag_cap, keep_loss = loss_cap, keep_rec = step_rec_cap;
+        const bool keep_graphs = use_graphs;
+        const TrackTune t0 = tune;
+        const int si0 = sort_interval;
+        diag_cap = 0;
+        loss_cap = 0;
+        step_rec_cap = 0;
+        use_graphs = false;
+        wire_loss();
+        wire_step_counts(false);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        auto restore = [&]() {
+            diag_cap = keep_diag;
+            loss_cap = keep_loss;
+            step_rec_cap = keep_rec;
+            use_graphs = keep_graphs;
+            wire_loss();
+            wire_step_counts(false);
+            cudaMemcpy(elem_charge, keep_charge, sizeof(double) * ne, cudaMemcpyDeviceToDevice);
+            dfree(keep_charge);
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        };
+        try {
+            cuda_check(cudaEventCreate(&e0), "event");
+            cuda_check(cudaEventCreate(&e1), "event");
+            auto trial = [&](const TrackTune& tt, int si) -> double {
+                apply_tune(tt, si);
+                t.drop_work();
+                t.kicks_since_sort = 0;
+                if (b.n) {
+                    cuda_check(cudaMemcpy2D(t.parts, sizeof(double) * t.stride, b.home_parts,
+                                            sizeof(double) * b.home_stride, sizeof(double) * b.n, 7,
+                                            cudaMemcpyDeviceToDevice),
+                               "autotune copy");
+                    cuda_check(cudaMemcpy(t.masks, b.home_masks, b.n, cudaMemcpyDeviceToDevice), "autotune copy");
+                    if (b.home_discards)
+                        cuda_check(cudaMemcpy(t.discards, b.home_discards, b.n, cudaMemcpyDeviceToDevice),
+                                   "autotune copy");
+                }
+                cuda_check(cudaMemcpy(t.counters, b.counters, sizeof(BunchCounters), cudaMemcpyDeviceToDevice),
+                           "autotune copy");
+                t.host_counters = b.host_counters;
+                t.ref = b.ref;
+                t.design = b.design;
+                t.design_set = b.design_set;
+                t.turns_done = b.turns_done;
+                cuda_check(cudaEventRecord(e0, 0), "event");
+                propagate_steps(t, 0, steps, 0);
+                cuda_check(cudaEventRecord(e1, 0), "event");
+                cuda_check(cudaEventSynchronize(e1), "event");
+                float ms = 0.f;
+                cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event");
+                log.push_back({(double)tt.light_shape, (double)tt.full_occ, (double)tt.full_ppt,
+                               (double)tt.quad_variant, (double)tt.ctas_per_sm, (double)si, (double)ms});
+                return ms;
+            };
+            trial(t0, si0); // warm-up: allocations of the scratch working copy
+            log.clear();
+            TrackTune best = t0;
+            int best_si = si0;
+            double best_ms = trial(best, best_si);
+            auto consider = [&](TrackTune c, int si) {
+                if (!std::memcmp(&c, &best, sizeof(c)) && si == best_si) return;
+                const double ms = trial(c, si);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = c;
+                    best_si = si;
+                }
+            };
+            for (int v : {1, 2, 0}) {
+                TrackTune c = best;
+                c.light_shape = v;
+                consider(c, best_si);
+            }
+            const int fulls[3][2] = {{2, 1}, {2, 2}, {3, 1}};
+            for (auto& f : fulls) {
+                TrackTune c = best;
+                c.full_occ = f[0];
+                c.full_ppt = f[1];
+                consider(c, best_si);
+            }
+            for (int v : {1, 0}) {
+                TrackTune c = best;
+                c.quad_variant = v;
+                consider(c, best_si);
+            }
+            for (int v : {4, 8, 12}) {
+                TrackTune c = best;
+                c.ctas_per_sm = v;
+                consider(c, best_si);
+            }
+            if (has_sc && cell_sort)
+                for (int v : {2, 4, 8}) consider(best, v);
+            apply_tune(best, best_si);
+        } catch (...) {
+            apply_tune(t0, si0);
+            restore();
+            throw;
+        }
+        restore();
+    }
 
     // ----- per-step count records -----------------------------------------
     int step_rec_cap = 0;
@@ -3422,6 +3564,62 @@ sb2_status sb2_propagator_set_loss_diagnostics(sb2_propagator* p, int32_t capaci
     if (capacity > 0 && p->p->use_graphs)
         throw Error(SB2_ERR_UNSUPPORTED, "loss diagnostics are not available with CUDA-graph turns");
     p->p->set_loss_diagnostics(capacity);
+    SB2_CATCH
+}
+
+static void check_tune(const sb2_tune& t)
+{
+    SB2_REQUIRE(t.light_shape >= 0 && t.light_shape <= 2, "tune: light_shape is 0, 1 or 2");
+    SB2_REQUIRE(t.full_occ == 2 || t.full_occ == 3, "tune: full_occ is 2 or 3");
+    SB2_REQUIRE(t.full_ppt == 1 || t.full_ppt == 2, "tune: full_ppt is 1 or 2");
+    SB2_REQUIRE(t.quad_variant == 0 || t.quad_variant == 1, "tune: quad_variant is 0 or 1");
+    SB2_REQUIRE(t.ctas_per_sm >= 1 && t.ctas_per_sm <= kMaxCtasPerSm, "tune: ctas_per_sm is 1..12");
+    SB2_REQUIRE(t.sort_interval >= 1, "tune: sort_interval >= 1");
+}
+
+static sb2_tune export_tune(const Propagator& P)
+{
+    sb2_tune t;
+    t.light_shape = P.tune.light_shape;
+    t.full_occ = P.tune.full_occ;
+    t.full_ppt = P.tune.full_ppt;
+    t.quad_variant = P.tune.quad_variant;
+    t.ctas_per_sm = P.tune.ctas_per_sm;
+    t.sort_interval = P.sort_interval;
+    return t;
+}
+
+sb2_status sb2_propagator_get_tune(sb2_propagator* p, sb2_tune* out)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && out, "null argument");
+    *out = export_tune(*p->p);
+    SB2_CATCH
+}
+
+sb2_status sb2_propagator_set_tune(sb2_propagator* p, const sb2_tune* in)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && in, "null argument");
+    check_tune(*in);
+    TrackTune t{in->light_shape, in->full_occ, in->full_ppt, in->quad_variant, in->ctas_per_sm};
+    p->p->apply_tune(t, in->sort_interval);
+    SB2_CATCH
+}
+
+sb2_status sb2_propagator_autotune(sb2_propagator* p, sb2_bunch* b, int32_t steps, sb2_tune* best, double* trials,
+                                   int32_t max_trials, int32_t* ntrials)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && b, "null argument");
+    std::vector<std::array<double, 7>> log;
+    p->p->autotune(b->b, steps, log);
+    if (best) *best = export_tune(*p->p);
+    const int n = (int)log.size();
+    if (ntrials) *ntrials = n;
+    if (trials)
+        for (int i = 0; i < std::min(n, (int)max_trials); ++i)
+            for (int j = 0; j < 7; ++j) trials[7 * i + j] = log[i][j];
     SB2_CATCH
 }
 

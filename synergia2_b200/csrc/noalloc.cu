@@ -211,7 +211,7 @@ extern "C" sb2_status sb2_sc3d_apply_noalloc(const sb2_sc3d_options* opts, doubl
     tp.gz = d.gz;
     tp.nops = 1;
     tp.ops[0].kind = OP_MOMENTS;
-    if (!o.domain_fixed && (e = launch_track(tp, s))) return cuda_fail(e, "moments pass");
+    if (!o.domain_fixed && (e = launch_track(tp, track_tune_defaults(), s))) return cuda_fail(e, "moments pass");
 
     DomainParams dp;
     std::memset(&dp, 0, sizeof(dp));
@@ -248,7 +248,7 @@ extern "C" sb2_status sb2_sc3d_apply_noalloc(const sb2_sc3d_options* opts, doubl
     tp.ops[0].kind = OP_SC_KICK;
     tp.ops[0].d[0] = pref; // reference momentum and mass of the kick
     tp.ops[0].d[1] = mass;
-    if ((e = launch_track(tp, s))) return cuda_fail(e, "kick pass");
+    if ((e = launch_track(tp, track_tune_defaults(), s))) return cuda_fail(e, "kick pass");
 
     ScState st;
     if ((e = cudaMemcpyAsync(&st, state, sizeof(st), cudaMemcpyDeviceToHost, s)) || (e = cudaStreamSynchronize(s)))

@@ -79,9 +79,25 @@ struct SortBuffers {
     int64_t n, stride;
 };
 
+// Launch shape of the particle passes: the autotuner's search space
+// (host.cc, Propagator::autotune).
+struct TrackTune {
+    int32_t light_shape;  // light passes: 1 one particle per thread with the next tile prefetched,
+                          // 2 two per thread with prefetch, 0 two per thread without
+    int32_t full_occ;     // full passes: 2 (128 registers, TRACK_FULL_WIDE) or 3 CTAs/SM (80, TRACK_FULL)
+    int32_t full_ppt;     // particles per thread of the 2-CTA full variant (1 or 2)
+    int32_t quad_variant; // 1: passes whose only integrator is the quadrupole run TRACK_QUAD
+    int32_t ctas_per_sm;  // grid of the grid-stride particle passes, 1..12 CTAs per SM
+};
+// measured defaults, overridden by SB2_TRACK_LIGHT, SB2_TRACK_FULL_OCC,
+// SB2_TRACK_FULL_PPT, SB2_TRACK_QUAD, SB2_TRACK_CTAS_PER_SM
+TrackTune track_tune_defaults();
+constexpr int kMaxCtasPerSm = 12;
+
 // track.cu
-int track_grid_blocks();
-cudaError_t launch_track(const TrackParams& p, cudaStream_t s);
+int track_grid_blocks();                // grid at the default CTAs per SM
+int track_grid_blocks(int ctas_per_sm); // SM count x ctas_per_sm
+cudaError_t launch_track(const TrackParams& p, const TrackTune& t, cudaStream_t s);
 cudaError_t launch_moments(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
                            const double* mean, double* partials, int nblocks, cudaStream_t s);
 cudaError_t launch_populate(double* parts, int64_t stride, uint8_t* masks, int64_t n, const double* sig,

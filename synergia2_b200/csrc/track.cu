@@ -6,7 +6,7 @@
 
 namespace sb2 {
 
-cudaError_t launch_track_fast(const TrackParams& p, cudaStream_t s); // track_fast.cu
+cudaError_t launch_track_fast(const TrackParams& p, const TrackTune& t, cudaStream_t s); // track_fast.cu
 
 // Masked sums for diagnostics: mean (6) or central second moments (21 lower
 // triangle) per block, core_diagnostics.cc:105-111,174-186.
@@ -87,26 +87,54 @@ __global__ void populate_kernel(double* parts, int64_t stride, uint8_t* masks, i
 // ---------------------------------------------------------------------------
 // launchers (called from host.cc)
 // ---------------------------------------------------------------------------
-int track_grid_blocks()
+static int sm_count_cached()
 {
-    static int nb = 0;
-    if (!nb) {
-        int dev = 0, sms = 148;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        // CTAs per SM of the grid-stride particle passes (SB2_TRACK_CTAS_PER_SM
-        // overrides, 1..12)
-        int per = 8;
-        const char* e = getenv("SB2_TRACK_CTAS_PER_SM");
-        if (e && atoi(e) >= 1 && atoi(e) <= 12) per = atoi(e);
-        nb = sms * per;
     }
-    return nb;
+    return sms;
 }
 
-cudaError_t launch_track(const TrackParams& p, cudaStream_t s)
+TrackTune track_tune_defaults()
 {
-    return p.fast_maps ? launch_track_fast(p, s) : exact::launch_pass(p, s);
+    TrackTune t;
+    t.light_shape = 1;
+    t.full_occ = 2;
+    t.full_ppt = 1;
+    t.quad_variant = 1;
+    t.ctas_per_sm = 8;
+    const char* e = getenv("SB2_TRACK_LIGHT");
+    if (e && e[0] == '2' && e[1] == 'p') t.light_shape = 2;
+    if (e && e[0] == '2' && e[1] == 0) t.light_shape = 0;
+    e = getenv("SB2_TRACK_FULL_OCC");
+    if (e && atoi(e) == 3) t.full_occ = 3;
+    e = getenv("SB2_TRACK_FULL_PPT");
+    if (e && atoi(e) == 2) t.full_ppt = 2;
+    e = getenv("SB2_TRACK_QUAD");
+    if (e && e[0] == '0') t.quad_variant = 0;
+    e = getenv("SB2_TRACK_CTAS_PER_SM");
+    if (e && atoi(e) >= 1 && atoi(e) <= kMaxCtasPerSm) t.ctas_per_sm = atoi(e);
+    return t;
+}
+
+int track_grid_blocks(int ctas_per_sm)
+{
+    return sm_count_cached() * std::max(1, std::min(ctas_per_sm, kMaxCtasPerSm));
+}
+
+int track_grid_blocks()
+{
+    static int per = track_tune_defaults().ctas_per_sm;
+    return track_grid_blocks(per);
+}
+
+cudaError_t launch_track(const TrackParams& p, const TrackTune& t, cudaStream_t s)
+{
+    return p.fast_maps ? launch_track_fast(p, t, s) : exact::launch_pass(p, t, s);
 }
 
 cudaError_t launch_moments(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,

@@ -6,6 +6,9 @@
 
 namespace sb2 {
 
-cudaError_t launch_track_fast(const TrackParams& p, cudaStream_t s) { return fast::launch_pass(p, s); }
+cudaError_t launch_track_fast(const TrackParams& p, const TrackTune& t, cudaStream_t s)
+{
+    return fast::launch_pass(p, t, s);
+}
 
 } // namespace sb2

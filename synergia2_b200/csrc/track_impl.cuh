@@ -807,80 +807,28 @@ bool track_needs_full(const MapOp* ops, int n)
     return false;
 }
 
-// Register budget of the full variant: 2 CTAs/SM (128 registers; measured
-// faster for the Yoshida passes) unless SB2_TRACK_FULL_OCC=3 selects
-// 3 CTAs/SM (80 registers).
-static int full_variant()
+// The launch shape comes from the propagator's TrackTune (the measured
+// defaults of track_tune_defaults, or what its autotuner chose).
+cudaError_t launch_pass(const TrackParams& p, const TrackTune& t, cudaStream_t s)
 {
-    static int v = -1;
-    if (v < 0) {
-        const char* e = getenv("SB2_TRACK_FULL_OCC");
-        v = (e && atoi(e) == 3) ? TRACK_FULL : TRACK_FULL_WIDE;
-    }
-    return v;
-}
-
-// Shape of the light pass: particles per thread and prefetching.  Default
-// 1p: one particle per thread with the next tile prefetched (2 CTAs/SM, no
-// register spills); SB2_TRACK_LIGHT = 2 / 2p selects two per thread without /
-// with prefetching.
-static int light_shape()
-{
-    static int v = -1;
-    if (v < 0) {
-        const char* e = getenv("SB2_TRACK_LIGHT");
-        v = 1;
-        if (e && e[0] == '2' && e[1] == 'p') v = 2;
-        if (e && e[0] == '2' && e[1] == 0) v = 0;
-    }
-    return v;
-}
-
-// Particles per thread of the full pass (SB2_TRACK_FULL_PPT = 1 or 2): two
-// interleave two independent Yoshida chains per thread.
-static int full_ppt()
-{
-    static int v = -1;
-    if (v < 0) {
-        const char* e = getenv("SB2_TRACK_FULL_PPT");
-        v = (e && atoi(e) == 2) ? 2 : 1;
-    }
-    return v;
-}
-
-// Passes whose only integrator is the pure-quadrupole Yoshida run the
-// TRACK_QUAD variant unless SB2_TRACK_QUAD=0.
-static bool quad_variant()
-{
-    static int v = -1;
-    if (v < 0) {
-        const char* e = getenv("SB2_TRACK_QUAD");
-        v = (e && e[0] == '0') ? 0 : 1;
-    }
-    return v == 1;
-}
-
-cudaError_t launch_pass(const TrackParams& p, cudaStream_t s)
-{
-    int nb = track_grid_blocks();
+    const int nb = track_grid_blocks(t.ctas_per_sm);
     if (!track_needs_full(p.ops, p.nops)) {
-        const int shape = light_shape();
-        if (shape == 1)
+        if (t.light_shape == 1)
             track_kernel<TRACK_LIGHT, 1, true><<<nb, kTrackThreads, 0, s>>>(p);
-        else if (shape == 2)
+        else if (t.light_shape == 2)
             track_kernel<TRACK_LIGHT, 2, true><<<nb, kTrackThreads, 0, s>>>(p);
         else
             track_kernel<TRACK_LIGHT, 2, false><<<nb, kTrackThreads, 0, s>>>(p);
-    } else if (quad_variant() && track_quad_only(p.ops, p.nops)) {
+    } else if (t.quad_variant && track_quad_only(p.ops, p.nops)) {
         track_kernel<TRACK_QUAD, 1, false><<<nb, kTrackThreads, 0, s>>>(p);
-    } else if (full_variant() == TRACK_FULL_WIDE) {
-        if (full_ppt() == 2)
+    } else if (t.full_occ != 3) {
+        if (t.full_ppt == 2)
             track_kernel<TRACK_FULL_WIDE, 2, false><<<nb, kTrackThreads, 0, s>>>(p);
         else
             track_kernel<TRACK_FULL_WIDE, 1, false><<<nb, kTrackThreads, 0, s>>>(p);
-    }
-    else
+    } else {
         track_kernel<TRACK_FULL, 1, false><<<nb, kTrackThreads, 0, s>>>(p);
+    }
     return cudaGetLastError();
 }
 
