@@ -292,7 +292,8 @@ sb2_status sb2_propagator_read_losses(sb2_propagator* p, int32_t max_records, in
  * passes with Yoshida integrators or bends at 2 (128 registers) or 3
  * (80 registers) CTAs per SM; full_ppt: particles per thread of the 2-CTA
  * variant (1, 2); quad_variant: passes whose only integrator is the
- * quadrupole Yoshida use the variant without the others (1) or not (0);
+ * quadrupole Yoshida use the variant without the others, with one (1) or
+ * two (2, at 2 CTAs per SM) particles per thread, or not (0);
  * ctas_per_sm: grid of the particle passes (1..12 x the SM count);
  * sort_interval: re-sort before every k-th space-charge kick.  The defaults
  * are the values measured best on the FODO workload of 4M macroparticles. */

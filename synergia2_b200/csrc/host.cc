@@ -2491,7 +2491,7 @@ struct Propagator {
                 c.full_ppt = f[1];
                 consider(c, best_si);
             }
-            for (int v : {1, 0}) {
+            for (int v : {1, 2, 0}) {
                 TrackTune c = best;
                 c.quad_variant = v;
                 consider(c, best_si);
@@ -3572,7 +3572,7 @@ static void check_tune(const sb2_tune& t)
     SB2_REQUIRE(t.light_shape >= 0 && t.light_shape <= 2, "tune: light_shape is 0, 1 or 2");
     SB2_REQUIRE(t.full_occ == 2 || t.full_occ == 3, "tune: full_occ is 2 or 3");
     SB2_REQUIRE(t.full_ppt == 1 || t.full_ppt == 2, "tune: full_ppt is 1 or 2");
-    SB2_REQUIRE(t.quad_variant == 0 || t.quad_variant == 1, "tune: quad_variant is 0 or 1");
+    SB2_REQUIRE(t.quad_variant >= 0 && t.quad_variant <= 2, "tune: quad_variant is 0, 1 or 2");
     SB2_REQUIRE(t.ctas_per_sm >= 1 && t.ctas_per_sm <= kMaxCtasPerSm, "tune: ctas_per_sm is 1..12");
     SB2_REQUIRE(t.sort_interval >= 1, "tune: sort_interval >= 1");
 }

@@ -86,7 +86,8 @@ struct TrackTune {
                           // 2 two per thread with prefetch, 0 two per thread without
     int32_t full_occ;     // full passes: 2 (128 registers, TRACK_FULL_WIDE) or 3 CTAs/SM (80, TRACK_FULL)
     int32_t full_ppt;     // particles per thread of the 2-CTA full variant (1 or 2)
-    int32_t quad_variant; // 1: passes whose only integrator is the quadrupole run TRACK_QUAD
+    int32_t quad_variant; // passes whose only integrator is the quadrupole run TRACK_QUAD with 1 (1) or
+                          // 2 (2) particles per thread, or the full variant (0)
     int32_t ctas_per_sm;  // grid of the grid-stride particle passes, 1..12 CTAs per SM
 };
 // measured defaults, overridden by SB2_TRACK_LIGHT, SB2_TRACK_FULL_OCC,

@@ -388,9 +388,10 @@ enum TrackVariant { TRACK_LIGHT = 0, TRACK_FULL = 1, TRACK_FULL_WIDE = 2, TRACK_
 #define SB2_QUAD_OCC 3
 #endif
 // Minimum resident CTAs per SM for each variant (register budget).
-template <int V>
+template <int V, int PPT = 1>
 struct TrackOcc {
-    static constexpr int value = V == TRACK_LIGHT ? 3 : (V == TRACK_FULL ? 3 : (V == TRACK_QUAD ? SB2_QUAD_OCC : 2));
+    static constexpr int value =
+        V == TRACK_LIGHT ? 3 : (V == TRACK_FULL ? 3 : (V == TRACK_QUAD ? (PPT == 1 ? SB2_QUAD_OCC : 2) : 2));
 };
 
 // One particle in registers during a pass.
@@ -704,7 +705,7 @@ __device__ __forceinline__ void load_tile(const TrackParams& p, int64_t base, Ra
 // (memory-bound passes: the loads of one tile overlap the arithmetic of the
 // previous one).
 template <int VARIANT, int PPT, bool PF>
-__global__ void __launch_bounds__(kTrackThreads, PF ? 3 : TrackOcc<VARIANT>::value)
+__global__ void __launch_bounds__(kTrackThreads, PF ? 3 : TrackOcc<VARIANT, PPT>::value)
     track_kernel(const __grid_constant__ TrackParams p)
 {
     __shared__ int s_counts[kMaxOpsPerPass];
@@ -820,7 +821,10 @@ cudaError_t launch_pass(const TrackParams& p, const TrackTune& t, cudaStream_t s
         else
             track_kernel<TRACK_LIGHT, 2, false><<<nb, kTrackThreads, 0, s>>>(p);
     } else if (t.quad_variant && track_quad_only(p.ops, p.nops)) {
-        track_kernel<TRACK_QUAD, 1, false><<<nb, kTrackThreads, 0, s>>>(p);
+        if (t.quad_variant == 2)
+            track_kernel<TRACK_QUAD, 2, false><<<nb, kTrackThreads, 0, s>>>(p);
+        else
+            track_kernel<TRACK_QUAD, 1, false><<<nb, kTrackThreads, 0, s>>>(p);
     } else if (t.full_occ != 3) {
         if (t.full_ppt == 2)
             track_kernel<TRACK_FULL_WIDE, 2, false><<<nb, kTrackThreads, 0, s>>>(p);
