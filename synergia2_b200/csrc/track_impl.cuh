@@ -384,6 +384,11 @@ constexpr int kTrackThreads = 256;
 // faster on the FODO quadrupole passes than TRACK_FULL_WIDE at 2 CTAs/SM.
 enum TrackVariant { TRACK_LIGHT = 0, TRACK_FULL = 1, TRACK_FULL_WIDE = 2, TRACK_QUAD = 3 };
 
+// CTAs per SM of the prefetching light variants: 4 (64 registers, a few
+// spilled to L1) measured 2% faster than 3 (80 registers) on the C1 passes.
+#ifndef SB2_LIGHT_OCC
+#define SB2_LIGHT_OCC 4
+#endif
 #ifndef SB2_QUAD_OCC
 #define SB2_QUAD_OCC 3
 #endif
@@ -705,7 +710,7 @@ __device__ __forceinline__ void load_tile(const TrackParams& p, int64_t base, Ra
 // (memory-bound passes: the loads of one tile overlap the arithmetic of the
 // previous one).
 template <int VARIANT, int PPT, bool PF>
-__global__ void __launch_bounds__(kTrackThreads, PF ? 3 : TrackOcc<VARIANT, PPT>::value)
+__global__ void __launch_bounds__(kTrackThreads, PF ? SB2_LIGHT_OCC : TrackOcc<VARIANT, PPT>::value)
     track_kernel(const __grid_constant__ TrackParams p)
 {
     __shared__ int s_counts[kMaxOpsPerPass];
