@@ -708,10 +708,13 @@ cudaError_t launch_book_domain(const DomainParams& p, cudaStream_t s)
     return cudaGetLastError();
 }
 
+#ifndef SB2_DEPOSIT_CTAS
+#define SB2_DEPOSIT_CTAS 8 // CTAs per SM of the grid-stride deposit (5 / 8 / 16: 0.163 / 0.142 / 0.146 ms per C1 step)
+#endif
 cudaError_t launch_deposit(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
                            const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s)
 {
-    deposit_kernel<<<sm_count() * 8, 256, 0, s>>>(parts, stride, masks, n, sc, rho, gx, gy, gz);
+    deposit_kernel<<<sm_count() * SB2_DEPOSIT_CTAS, 256, 0, s>>>(parts, stride, masks, n, sc, rho, gx, gy, gz);
     return cudaGetLastError();
 }
 
