@@ -24,6 +24,7 @@
 #include <array>
 #include <cmath>
 #include <complex>
+#include <limits>
 #include <cstdint>
 #include <cstring>
 #include <map>
@@ -1095,6 +1096,38 @@ inline void kicker_kick(double, double& xp, double, double& yp, double, const do
     yp = yp + kL[1];
 }
 
+// nllens_unit ff_algorithm.h:1180-1270: thin nonlinear lens (Danilov-
+// Nagaitsev potential) with k = {1/cnll, -knll/cnll}; the derivative of the
+// complex potential F(z) is evaluated with z = (x + i y)/cnll as
+// z/(1 - z^2) + arcsin(z)/(1 - z^2), taking the square root of 1 - z^2 with a
+// non-negative imaginary part and arcsin(z) = -i log(i z + sqrt(1 - z^2)),
+// as the reference's arithmetic does.  On the cut (y = 0, |x| >= cnll) the
+// angles become NaN.
+inline void nllens_kick(double x, double& xp, double y, double& yp, double, const double* k)
+{
+    const double zr = x * k[0], zi = y * k[0];
+    if (zi == 0 && (zr >= 1.0 || zr <= -1.0)) {
+        xp = std::numeric_limits<double>::quiet_NaN();
+        yp = std::numeric_limits<double>::quiet_NaN();
+        return;
+    }
+    std::complex<double> c(1.0 - zr * zr + zi * zi, -2.0 * zr * zi);   // 1 - z^2
+    const double mod = std::sqrt(c.real() * c.real() + c.imag() * c.imag());
+    std::complex<double> root(std::sqrt(0.5 * (c.real() + mod)), std::sqrt(0.5 * (-c.real() + mod)));
+    std::complex<double> co(root.real() - zi, root.imag() + zr);         // i z + root
+    const double r = std::sqrt(co.real() * co.real() + co.imag() * co.imag());
+    const double theta = (co.real() > 0) ? std::atan(co.imag() / co.real()) + 0.0
+                                         : std::atan(co.imag() / co.real()) + 3.14159265358979323846;
+    const double asin_r = theta, asin_i = -std::log(r);                  // -i log(co)
+    const double c2r = root.real() * root.real() - root.imag() * root.imag();
+    const double c2i = 2.0 * root.real() * root.imag();
+    const double den = c2r * c2r + c2i * c2i;
+    const double d1r = (c2r * zr + c2i * zi) / den, d1i = (c2r * zi - c2i * zr) / den;
+    const double d2r = (c2r * asin_r + c2i * asin_i) / den, d2i = (c2r * asin_i - c2i * asin_r) / den;
+    xp = xp + k[1] * (d1r + d2r);
+    yp = yp + -k[1] * (d1i + d2i);
+}
+
 // FF_patterned_propagator (ff_patterned_propagator.h) for one slice: the
 // design particle follows k_design, the particles k_parts; thin slices kick,
 // thick ones run yoshida6 (or drift-kick-drift when `simple`); use_drift
@@ -1178,6 +1211,21 @@ static void patterned_apply(const Slice& slice, Bunch& b, const double* k_design
         }
     }
     b.ref.s_n += length;
+}
+
+static void nllens_apply(const Slice& slice, Bunch& b)
+{ // ff_nllens.h:9-50
+    const Element& element = *slice.e;
+    const double l = element.get("l", 0.0);
+    const double knll = element.get("knll");
+    const double cnll = element.get("cnll");
+    if (!close_to_zero(l)) throw std::runtime_error("nonlinear lens has non-zero length");
+    const double icnll = 1.0 / cnll;
+    const double k[2] = {icnll, -knll * icnll};
+    patterned_apply(slice, b, k, k, nllens_kick, true, false, false, 1);
+    if (std::isnan(b.design.state[1]) || std::isnan(b.design.state[3]))
+        throw std::runtime_error("the bunch reference particle hits the sigularity region "
+                                 "when propagating through a nonlinearlens");
 }
 
 static void octupole_apply(const Slice& slice, Bunch& b)
@@ -1394,6 +1442,8 @@ static void element_apply(const Slice& slice, Bunch& b)
         sextupole_apply(slice, b);
     else if (t == "octupole")
         octupole_apply(slice, b);
+    else if (t == "nllens")
+        nllens_apply(slice, b);
     else if (t == "hkicker" || t == "vkicker" || t == "kicker")
         kicker_apply(slice, b);
     else if (t == "solenoid")

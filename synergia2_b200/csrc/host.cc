@@ -444,6 +444,7 @@ void kicker_kick_cb(double, double& xp, double, double& yp, const double* k)
 #define SB2_FF inline
 #define SB2_FF_SINCOS 0
 #include "ff_bend.h"
+#include "ff_nllens.h"
 #undef SB2_FF
 #undef SB2_FF_SINCOS
 } // namespace hostff
@@ -1330,6 +1331,26 @@ static void ops_octupole(const Lattice& lat, const Slice& sl, Bunch& b, std::vec
                   hostff::close_to_zero(sl.right - sl.left), false, false, (int)el.get("yoshida_steps", 4.0));
 }
 
+static void nllens_kick_cb(double x, double& xp, double y, double& yp, const double* k)
+{
+    hostff::nllens_unit(x, xp, y, yp, k);
+}
+
+static void ops_nllens(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
+{ // ff_nllens.h:9-50: thin only, through FF_patterned_propagator's thin kick
+    const Element& el = lat.elements[sl.elem];
+    const double l = el.get("l", 0.0);
+    const double knll = el.get("knll");
+    const double cnll = el.get("cnll");
+    if (!hostff::close_to_zero(l)) throw Error(SB2_ERR_RUNTIME, "nonlinear lens has non-zero length");
+    const double icnll = 1.0 / cnll;
+    const double k[2] = {icnll, -knll * icnll};
+    ops_patterned(sl, b, out, k, k, nllens_kick_cb, OP_THIN_NLLENS, -1, true, false, false, 1);
+    if (std::isnan(b.design.state[1]) || std::isnan(b.design.state[3]))
+        throw Error(SB2_ERR_RUNTIME, "the bunch reference particle hits the sigularity region "
+                                     "when propagating through a nonlinearlens");
+}
+
 static void ops_kicker(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
 { // ff_kicker.h:17-127; attributes as Lattice_element_processor::hkicker / vkicker / kicker
   // (lattice_element_processor.cc:86-159)
@@ -1501,7 +1522,9 @@ static void ops_slice(const Lattice& lat, const Slice& sl, Bunch& b, std::vector
         ops_solenoid(lat, sl, b, out);
     else if (t == "rfcavity")
         ops_rfcavity(lat, sl, b, out);
-    else if (t == "elens" || t == "nllens" || t == "foil" || t == "dipedge" || t == "matrix")
+    else if (t == "nllens")
+        ops_nllens(lat, sl, b, out);
+    else if (t == "elens" || t == "foil" || t == "dipedge" || t == "matrix")
         throw Error(SB2_ERR_UNSUPPORTED, "element type " + t + " is not on the GPU path of this build (element " +
                                              lat.elements[sl.elem].name + ")");
     else

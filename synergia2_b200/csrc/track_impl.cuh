@@ -281,6 +281,15 @@ __device__ __noinline__ void sbend_op(double& x, double& xp, double& y, double& 
     }
 }
 
+#define SB2_FF __device__ __forceinline__
+#include "ff_nllens.h"
+#undef SB2_FF
+// FF_nllens thin kick (out of line: rare op with atan and log)
+__device__ __noinline__ void nllens_op(double x, double& xp, double y, double& yp, const double* d)
+{
+    nllens_unit(x, xp, y, yp, d + 2);
+}
+
 // PropSbendCF ff_sbend.h:221-339 for one particle (combined-function or
 // a_n/b_n multipole bend; out of line: rare op).  d: 0 ce1 1 se1 2 ce2
 // 3 se2 4 us_kx 5 us_ky 6 ds_kx 7 ds_ky 8 e1 9 e2 10-11 entry-face phase
@@ -617,6 +626,9 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
             break;
         case OP_KICK_YOSHIDA:
             if constexpr (kFull) yoshida6_op<OP_KICK_YOSHIDA>(x, xp, y, yp, cdt, dpop, op);
+            break;
+        case OP_THIN_NLLENS:
+            nllens_op(x, xp, y, yp, op.d);
             break;
         case OP_THIN_KICK:
             xp = xp + op.d[2];

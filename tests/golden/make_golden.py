@@ -121,6 +121,26 @@ def ring_positions(offset=1.0e-3):
     return [[x, 0.0, y, 0.0, 0.0, 0.0] for x, y in xy]
 
 
+def nllens_golden():
+    """src/synergia/libFF/tests/lattices/track_nllensone.npy and
+    nllens_channel.seq (README.nllens.txt): 32 particles -- the 16-point ring
+    of radius 1 mm around the axis and the same ring around (0.5, -0.25) mm,
+    zero angles -- after the thin nonlinear lens (knll 5.479576037e-6, cnll
+    8.105461952e-3) between two 0.5 um drifts.  No reference test reads this
+    file; its angles are the analytic Danilov-Nagaitsev kick (principal
+    square root, asin(z)/(1 - z^2)^(3/2)), which the reference's
+    nllens_unit does not compute (tests/test_nllens.py)."""
+    import numpy as np
+    a = np.load(os.path.join(LAT, "track_nllensone.npy"))
+    init = ring_positions() + [[0.5e-3 + r[0], 0.0, -0.25e-3 + r[2], 0.0, 0.0, 0.0] for r in ring_positions()]
+    out = os.path.join(os.path.dirname(OUT), "nllens_track.json")
+    json.dump({"generated_by": "tests/golden/make_golden.py",
+               "source": "src/synergia/libFF/tests/lattices/track_nllensone.npy, nllens_channel.seq",
+               "knll": 5.479576037e-06, "cnll": 0.008105461952, "drift": 0.5e-6,
+               "initial": init, "final": a.tolist()}, open(out, "w"), indent=0)
+    print("wrote", out)
+
+
 def main():
     cases = []
     # test_madx_elements.cc: drift, quad, sext, quad_long (1e-8), sext_long,
@@ -160,6 +180,7 @@ def main():
         cases.append({"name": name, "lattice": lattice, "p0": P0, "initial": ring_positions(),
                       "expected": expect, "tol": [1e-7] * 6,
                       "source": "src/synergia/libFF/tests/test_madx_multipoles.cc"})
+    nllens_golden()
     json.dump({"generated_by": "tests/golden/make_golden.py", "cases": cases}, open(OUT, "w"), indent=0)
     print("wrote", OUT, len(cases), "cases")
 

@@ -198,10 +198,10 @@ def test_gpu_empty_bunch(syn):
 
 
 def test_gpu_unsupported_element_is_reported(syn):
-    lat, ref = product_lattice([elem("nllens", "nl", l=0.0, knll=1e-3, cnll=1e-2)])
+    lat, ref = product_lattice([elem("elens", "el", l=0.0, current=1.0, eenergy=0.01, radius=1e-3)])
     prop = syn.Propagator(lat, syn.Independent_stepper_elements(1))
     b = syn.Bunch(ref, 16, 1e10)
-    with pytest.raises(syn.SB2Error, match="nllens"):
+    with pytest.raises(syn.SB2Error, match="elens"):
         prop.propagate(b, 1)
 
 
@@ -344,4 +344,39 @@ def test_gpu_sbend_both_k_and_moments_is_an_error(syn):
     prop = syn.Propagator(lat, syn.Independent_stepper_elements(1))
     b = syn.Bunch(ref, 16, 1e10)
     with pytest.raises(syn.SB2Error, match="forbidden in sbends"):
+        prop.propagate(b, 1)
+
+
+def test_gpu_nllens_matches_oracle(syn, orc):
+    """Thin nonlinear lens (FF_nllens) between two 0.5 um drifts: the
+    golden file's 32 points plus random ones and a particle on the cut
+    (y = 0, |x| > cnll), whose angles become NaN and which the Finite
+    aperture at the end of the operator then removes.  Within 1e-12 of the
+    oracle (CUDA's atan and log vs libm); masks and ids exact."""
+    import json
+    g = json.load(open(os.path.join(ROOT, "tests", "golden", "nllens_track.json")))
+    knll, cnll, d = g["knll"], g["cnll"], g["drift"]
+    spec = [elem("drift", "d1", l=d), elem("nllens", "nll", l=0.0, knll=knll, cnll=cnll), elem("drift", "d2", l=d)]
+    init = np.array(g["initial"])
+    rng = np.random.default_rng(6)
+    n = 32 + 200 + 1
+    p = np.zeros((n, 7), order="F")
+    p[:32, :6] = init
+    p[32:232, 0] = rng.uniform(-6e-3, 6e-3, 200)
+    p[32:232, 2] = rng.uniform(-6e-3, 6e-3, 200)
+    p[232, 0] = 1.5 * cnll  # on the cut
+    p[:, 6] = np.arange(n)
+    (gp, gm, _, _, _), (op, om, _, _) = run_both(syn, orc, spec, p, "indep", 1, 1, real_num=1e10)
+    assert np.array_equal(gm, om) and not gm[232] and gm[:232].all()
+    assert np.array_equal(gp[:, 6], op[:, 6])
+    alive = om.astype(bool)
+    scale = np.max(np.abs(op[alive, :4]), axis=0)
+    assert np.all(np.abs(gp[alive, :4] - op[alive, :4]) <= 1e-12 * scale)
+
+
+def test_gpu_nllens_with_length_is_an_error(syn):
+    lat, ref = product_lattice([elem("nllens", "nll", l=0.2, knll=1e-6, cnll=1e-2)])
+    prop = syn.Propagator(lat, syn.Independent_stepper_elements(1))
+    b = syn.Bunch(ref, 16, 1e10)
+    with pytest.raises(syn.SB2Error, match="non-zero length"):
         prop.propagate(b, 1)
