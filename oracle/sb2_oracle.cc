@@ -1213,6 +1213,66 @@ static void patterned_apply(const Slice& slice, Bunch& b, const double* k_design
     b.ref.s_n += length;
 }
 
+// dipedge_unit ff_algorithm.h:1284-1316 (MAD-X tmfrng): linear edge
+// focusing re_2_1, re_4_3 and the optional second-order terms te[10]
+inline void dipedge_unit(double& x, double& xp, double& y, double& yp, double re21, double re43, const double* te)
+{
+    double nx, nxp, ny, nyp;
+    nxp = xp + re21 * x;
+    nyp = yp + re43 * y;
+    nx = x + te[0] * x * x + te[1] * y * y;
+    nxp = nxp + te[2] * x * x + te[4] * y * y + te[3] * x * xp * 2.0 + te[5] * y * yp * 2.0;
+    ny = y + te[6] * x * y * 2.0;
+    nyp = nyp + te[7] * x * y * 2.0 + te[8] * x * yp * 2.0 + te[9] * y * xp * 2.0;
+    x = nx;
+    xp = nxp;
+    y = ny;
+    yp = nyp;
+}
+
+static void dipedge_apply(const Slice& slice, Bunch& b)
+{ // ff_dipedge.h:196-330
+    const Element& ele = *slice.e;
+    const double sig = 1.0, he = 0.0, sk1 = 0.0;
+    const double edge = ele.get("e1", 0.0);
+    const double h = ele.get("h", 0.0);
+    const double fint = ele.get("fint", 0.0);
+    const double hgap = ele.get("hgap", 0.0);
+    const double corr = (h + h) * hgap * fint;
+    const double tanedg = std::tan(edge);
+    const double secedg = 1.0 / std::cos(edge);
+    const double sn = std::sin(edge);
+    const double psip = edge - corr * secedg * (1.0 + sn * sn);
+    const double re21 = h * tanedg;
+    const double re43 = -h * std::tan(psip);
+    double te[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (ele.get("second_order", 0.0) != 0.0) {
+        const double hh = sig * (h / 2.0);
+        te[0] = -hh * tanedg * tanedg;
+        te[1] = hh * secedg * secedg;
+        te[2] = (h / 2.0) * he * (secedg * secedg * secedg) + sk1 * tanedg;
+        te[3] = -te[0];
+        te[4] = hh * h * (tanedg * tanedg * tanedg) - te[2];
+        te[5] = te[0];
+        te[6] = -te[0];
+        te[7] = -te[2];
+        te[8] = te[0];
+        te[9] = -te[1];
+        te[4] += (h * secedg) * (h * secedg) * (tanedg / 2.0); // sig > 0
+    }
+    if (b.n_valid) { // prop_reference runs inside the per-group apply (:300-318)
+        Refpart& ref_l = b.design;
+        double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3];
+        dipedge_unit(x, xp, y, yp, re21, re43, te);
+        ref_l.state = {x, xp, y, yp, 0.0, ref_l.state[5]};
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < b.n_active; ++i) {
+            if (!b.masks[i]) continue;
+            dipedge_unit(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), re21, re43, te);
+        }
+    }
+}
+
 static void nllens_apply(const Slice& slice, Bunch& b)
 { // ff_nllens.h:9-50
     const Element& element = *slice.e;
@@ -1444,6 +1504,8 @@ static void element_apply(const Slice& slice, Bunch& b)
         octupole_apply(slice, b);
     else if (t == "nllens")
         nllens_apply(slice, b);
+    else if (t == "dipedge")
+        dipedge_apply(slice, b);
     else if (t == "hkicker" || t == "vkicker" || t == "kicker")
         kicker_apply(slice, b);
     else if (t == "solenoid")

@@ -1331,6 +1331,54 @@ static void ops_octupole(const Lattice& lat, const Slice& sl, Bunch& b, std::vec
                   hostff::close_to_zero(sl.right - sl.left), false, false, (int)el.get("yoshida_steps", 4.0));
 }
 
+// FF_dipedge::apply ff_dipedge.h:196-330: MAD-X tmfrng edge focusing
+// (linear, or with the second-order terms when `second_order` is set); the
+// design particle takes the same map with its cdt zeroed.  (The reference
+// propagates it inside the per-particle-group loop, so a bunch without valid
+// particles leaves it alone; here it always moves, which changes nothing
+// for a design particle on the axis.)
+static void ops_dipedge(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
+{
+    const Element& ele = lat.elements[sl.elem];
+    const double sig = 1.0, he = 0.0, sk1 = 0.0;
+    const double edge = ele.get("e1", 0.0);
+    const double h = ele.get("h", 0.0);
+    const double fint = ele.get("fint", 0.0);
+    const double hgap = ele.get("hgap", 0.0);
+    const double corr = (h + h) * hgap * fint;
+    const double tanedg = std::tan(edge);
+    const double secedg = 1.0 / std::cos(edge);
+    const double sn = std::sin(edge);
+    const double psip = edge - corr * secedg * (1.0 + sn * sn);
+    MapOp o = new_op(OP_DIPEDGE);
+    o.d[0] = h * tanedg;
+    o.d[1] = -h * std::tan(psip);
+    double* te = o.d + 2;
+    if (ele.get("second_order", 0.0) != 0.0) {
+        const double hh = sig * (h / 2.0);
+        te[0] = -hh * tanedg * tanedg;
+        te[1] = hh * secedg * secedg;
+        te[2] = (h / 2.0) * he * (secedg * secedg * secedg) + sk1 * tanedg;
+        te[3] = -te[0];
+        te[4] = hh * h * (tanedg * tanedg * tanedg) - te[2];
+        te[5] = te[0];
+        te[6] = -te[0];
+        te[7] = -te[2];
+        te[8] = te[0];
+        te[9] = -te[1];
+        te[4] += (h * secedg) * (h * secedg) * (tanedg / 2.0); // sig > 0
+    }
+    Refpart& ref_l = b.design;
+    double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3];
+    double nxp = xp + o.d[0] * x, nyp = yp + o.d[1] * y;
+    double nx = x + te[0] * x * x + te[1] * y * y;
+    nxp = nxp + te[2] * x * x + te[4] * y * y + te[3] * x * xp * 2.0 + te[5] * y * yp * 2.0;
+    double ny = y + te[6] * x * y * 2.0;
+    nyp = nyp + te[7] * x * y * 2.0 + te[8] * x * yp * 2.0 + te[9] * y * xp * 2.0;
+    ref_l.state = {nx, nxp, ny, nyp, 0.0, ref_l.state[5]};
+    out.push_back(o);
+}
+
 static void nllens_kick_cb(double x, double& xp, double y, double& yp, const double* k)
 {
     hostff::nllens_unit(x, xp, y, yp, k);
@@ -1524,7 +1572,9 @@ static void ops_slice(const Lattice& lat, const Slice& sl, Bunch& b, std::vector
         ops_rfcavity(lat, sl, b, out);
     else if (t == "nllens")
         ops_nllens(lat, sl, b, out);
-    else if (t == "elens" || t == "foil" || t == "dipedge" || t == "matrix")
+    else if (t == "dipedge")
+        ops_dipedge(lat, sl, b, out);
+    else if (t == "elens" || t == "foil" || t == "matrix")
         throw Error(SB2_ERR_UNSUPPORTED, "element type " + t + " is not on the GPU path of this build (element " +
                                              lat.elements[sl.elem].name + ")");
     else

@@ -284,6 +284,24 @@ __device__ __noinline__ void sbend_op(double& x, double& xp, double& y, double& 
 #define SB2_FF __device__ __forceinline__
 #include "ff_nllens.h"
 #undef SB2_FF
+// dipedge_unit ff_algorithm.h:1284-1316 (MAD-X tmfrng): edge focusing
+// d[0] = re_2_1, d[1] = re_4_3 and second-order terms d[2..11]
+__device__ __noinline__ void dipedge_op(double& x, double& xp, double& y, double& yp, const double* d)
+{
+    const double* te = d + 2;
+    double nx, nxp, ny, nyp;
+    nxp = xp + d[0] * x;
+    nyp = yp + d[1] * y;
+    nx = x + te[0] * x * x + te[1] * y * y;
+    nxp = nxp + te[2] * x * x + te[4] * y * y + te[3] * x * xp * 2.0 + te[5] * y * yp * 2.0;
+    ny = y + te[6] * x * y * 2.0;
+    nyp = nyp + te[7] * x * y * 2.0 + te[8] * x * yp * 2.0 + te[9] * y * xp * 2.0;
+    x = nx;
+    xp = nxp;
+    y = ny;
+    yp = nyp;
+}
+
 // FF_nllens thin kick (out of line: rare op with atan and log)
 __device__ __noinline__ void nllens_op(double x, double& xp, double y, double& yp, const double* d)
 {
@@ -626,6 +644,9 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
             break;
         case OP_KICK_YOSHIDA:
             if constexpr (kFull) yoshida6_op<OP_KICK_YOSHIDA>(x, xp, y, yp, cdt, dpop, op);
+            break;
+        case OP_DIPEDGE:
+            dipedge_op(x, xp, y, yp, op.d);
             break;
         case OP_THIN_NLLENS:
             nllens_op(x, xp, y, yp, op.d);

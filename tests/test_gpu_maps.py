@@ -380,3 +380,19 @@ def test_gpu_nllens_with_length_is_an_error(syn):
     b = syn.Bunch(ref, 16, 1e10)
     with pytest.raises(syn.SB2Error, match="non-zero length"):
         prop.propagate(b, 1)
+
+
+def test_gpu_dipedge_bit_exact(syn, orc):
+    """Dipole edges (FF_dipedge, MAD-X tmfrng), linear and with the
+    second-order terms, around a quadrupole and a drift, split-operator
+    stepper, two turns: bit-identical to the oracle, design particle too."""
+    spec = [elem("dipedge", "de1", l=0.0, e1=0.12, h=0.8, hgap=0.03, fint=0.4),
+            elem("quadrupole", "q", l=0.5, k1=0.3),
+            elem("dipedge", "de2", l=0.0, e1=-0.05, h=0.8, hgap=0.03, fint=0.4, second_order=1.0),
+            elem("drift", "d", l=0.7)]
+    n = 20000
+    p = gaussian_bunch(n, [2e-3, 2e-4, 2e-3, 2e-4, 0.3, 1e-3], 23)
+    (gp, gm, _, b, _), (op, om, _, sim) = run_both(syn, orc, spec, p, "split", 4, 2)
+    assert np.array_equal(gm, om)
+    assert np.array_equal(gp, op)
+    assert np.array_equal(b.design_state()[0], sim.design_state()[0])
