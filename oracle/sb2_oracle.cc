@@ -1273,6 +1273,44 @@ static void dipedge_apply(const Slice& slice, Bunch& b)
     }
 }
 
+// matrix_unit ff_algorithm.h:2439-2700 and FF_matrix::apply
+// ff_matrix.h:140-515: the design particle's image is computed but never
+// stored by the reference, so it stays; a non-zero length throws (with
+// valid particles).
+static void matrix_apply(const Slice& slice, Bunch& b)
+{
+    const Element& ele = *slice.e;
+    double k[6], rm[6][6], tm[6][6][6];
+    for (int i = 0; i < 6; ++i) k[i] = ele.get("kick" + std::to_string(i + 1), 0.0);
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+            rm[i][j] = ele.get("rm" + std::to_string(i + 1) + std::to_string(j + 1), i == j ? 1.0 : 0.0);
+            for (int l = 0; l < 6; ++l)
+                tm[i][j][l] = ele.get("tm" + std::to_string(i + 1) + std::to_string(j + 1) + std::to_string(l + 1), 0.0);
+        }
+    if (!b.n_valid) return;
+    if (ele.get("l", 0.0) != 0) throw std::runtime_error("error, matrix element has non-zero length");
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < b.n_active; ++p) {
+        if (!b.masks[p]) continue;
+        double v[6];
+        for (int i = 0; i < 6; ++i) v[i] = b.P(p, i);
+        double out[6];
+        for (int i = 0; i < 6; ++i) {
+            double a = k[i];
+            for (int j = 0; j < 6; ++j) a = a + rm[i][j] * v[j];
+            out[i] = a;
+        }
+        for (int i = 0; i < 6; ++i) {
+            double a = out[i];
+            for (int j = 0; j < 6; ++j)
+                for (int l = 0; l < 6; ++l) a = a + tm[i][j][l] * v[j] * v[l];
+            out[i] = a;
+        }
+        for (int i = 0; i < 6; ++i) b.P(p, i) = out[i];
+    }
+}
+
 static void nllens_apply(const Slice& slice, Bunch& b)
 { // ff_nllens.h:9-50
     const Element& element = *slice.e;
@@ -1506,6 +1544,8 @@ static void element_apply(const Slice& slice, Bunch& b)
         nllens_apply(slice, b);
     else if (t == "dipedge")
         dipedge_apply(slice, b);
+    else if (t == "matrix")
+        matrix_apply(slice, b);
     else if (t == "hkicker" || t == "vkicker" || t == "kicker")
         kicker_apply(slice, b);
     else if (t == "solenoid")

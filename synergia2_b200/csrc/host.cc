@@ -155,6 +155,9 @@ struct Lattice {
     std::vector<Element> elements;
     Refpart ref;
     bool has_ref = false;
+    // device copies of the second-order tensors of matrix elements (216
+    // doubles each), by element index; made with the propagator
+    std::map<int, std::shared_ptr<double>> matrix_tensors;
 
     double length() const
     { // lattice.cc:195-201
@@ -1331,6 +1334,29 @@ static void ops_octupole(const Lattice& lat, const Slice& sl, Bunch& b, std::vec
                   hostff::close_to_zero(sl.right - sl.left), false, false, (int)el.get("yoshida_steps", 4.0));
 }
 
+// FF_matrix::apply ff_matrix.h:140-515: MAD-X MATRIX element, kick + linear
+// map + second-order tensor (matrix_unit ff_algorithm.h:2439-2700).  The
+// reference computes the design particle's image but never stores it, so
+// the design particle is unchanged; a non-zero length is an error.
+static void ops_matrix(const Lattice& lat, const Slice& sl, Bunch& b, std::vector<MapOp>& out)
+{
+    const Element& ele = lat.elements[sl.elem];
+    if (ele.get("l", 0.0) != 0) throw Error(SB2_ERR_RUNTIME, "error, matrix element has non-zero length");
+    MapOp o = new_op(OP_MATRIX);
+    for (int i = 0; i < 6; ++i) o.d[i] = ele.get("kick" + std::to_string(i + 1), 0.0);
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j)
+            o.d[6 + i * 6 + j] = ele.get("rm" + std::to_string(i + 1) + std::to_string(j + 1), i == j ? 1.0 : 0.0);
+    auto it = lat.matrix_tensors.find(sl.elem);
+    if (it != lat.matrix_tensors.end()) {
+        o.flags = 1;
+        const uint64_t bits = (uint64_t)(uintptr_t)it->second.get();
+        std::memcpy(&o.d[42], &bits, sizeof(bits));
+    }
+    out.push_back(o);
+    (void)b;
+}
+
 // FF_dipedge::apply ff_dipedge.h:196-330: MAD-X tmfrng edge focusing
 // (linear, or with the second-order terms when `second_order` is set); the
 // design particle takes the same map with its cdt zeroed.  (The reference
@@ -1574,7 +1600,9 @@ static void ops_slice(const Lattice& lat, const Slice& sl, Bunch& b, std::vector
         ops_nllens(lat, sl, b, out);
     else if (t == "dipedge")
         ops_dipedge(lat, sl, b, out);
-    else if (t == "elens" || t == "foil" || t == "matrix")
+    else if (t == "matrix")
+        ops_matrix(lat, sl, b, out);
+    else if (t == "elens" || t == "foil")
         throw Error(SB2_ERR_UNSUPPORTED, "element type " + t + " is not on the GPU path of this build (element " +
                                              lat.elements[sl.elem].name + ")");
     else
@@ -2253,6 +2281,23 @@ struct Propagator {
             has_sc = true;
         }
         steps = make_steps(lat, stepper, num, has_sc);
+        for (size_t i = 0; i < lat.elements.size(); ++i) { // FF_matrix second-order terms, on the device
+            const Element& e = lat.elements[i];
+            if (e.type != "matrix") continue;
+            std::vector<double> tm(216);
+            bool any = false;
+            for (int a = 0; a < 6; ++a)
+                for (int j = 0; j < 6; ++j)
+                    for (int l = 0; l < 6; ++l) {
+                        const std::string k = "tm" + std::to_string(a + 1) + std::to_string(j + 1) + std::to_string(l + 1);
+                        tm[(a * 6 + j) * 6 + l] = e.get(k, 0.0);
+                        any |= tm[(a * 6 + j) * 6 + l] != 0.0;
+                    }
+            if (!any) continue;
+            double* dev = dalloc<double>(216, "matrix tensor");
+            cuda_check(cudaMemcpy(dev, tm.data(), sizeof(double) * 216, cudaMemcpyHostToDevice), "matrix tensor");
+            lat.matrix_tensors[(int)i] = std::shared_ptr<double>(dev, [](double* p) { dfree(p); });
+        }
         const char* e = getenv("SB2_CELL_SORT");
         if (e && atoi(e) == 0) cell_sort = false;
         const char* k = getenv("SB2_SORT_INTERVAL");

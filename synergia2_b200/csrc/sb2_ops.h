@@ -30,6 +30,7 @@ enum OpKind : int32_t {
     OP_SBEND_CF = 16,      // ff_sbend.h:221-339 (bend_yoshida6 with thin_cf_kick_5)
     OP_THIN_NLLENS = 17,   // ff_nllens.h:9-50 with nllens_unit ff_algorithm.h:1180-1270
     OP_DIPEDGE = 18,       // ff_dipedge.h:196-330 with dipedge_unit ff_algorithm.h:1284-1316
+    OP_MATRIX = 19,        // ff_matrix.h:140-515 with matrix_unit ff_algorithm.h:2439-2700
     OP_AP_FINITE = 20,     // aperture_operation.h:54-86
     OP_AP_CIRCULAR = 21,   // aperture_operation.h:92-116
     OP_AP_ELLIPTICAL = 22, // aperture_operation.h:123-151
@@ -49,6 +50,9 @@ enum OpKind : int32_t {
 //  THIN_SEXT:    2 k0, 3 k1
 //  THIN_NLLENS:  2 1/cnll, 3 -knll/cnll
 //  DIPEDGE:      0 re_2_1, 1 re_4_3, 2..11 te[10]
+//  MATRIX:       0..5 kick, 6..41 rm (row major); flags bit0: second-order
+//                tensor (216 doubles, [i][j][l]) at the device address whose
+//                bits are stored in d[42]
 //  SBEND:        flags bit0 ledge, bit1 redge; 0 ce1 1 se1 2 ce2 3 se2
 //                4 us_kx 5 us_ky 6 ds_kx 7 ds_ky 8 dphi 9 phase_r 10 phase_i
 //                11 term_r 12 term_i 13 strength 14 pref_b 15 m_b 16 ref_cdt

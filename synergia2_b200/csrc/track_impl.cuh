@@ -302,6 +302,37 @@ __device__ __noinline__ void dipedge_op(double& x, double& xp, double& y, double
     yp = nyp;
 }
 
+// matrix_unit ff_algorithm.h:2439-2700: kick + linear map + optional
+// second-order tensor, summed in the reference's order
+__device__ __noinline__ void matrix_op(double& x, double& xp, double& y, double& yp, double& cdt, double& dpop,
+                                       const double* d, int flags)
+{
+    const double v[6] = {x, xp, y, yp, cdt, dpop};
+    double nv[6];
+    for (int i = 0; i < 6; ++i) {
+        double a = d[i];
+        for (int j = 0; j < 6; ++j) a = a + d[6 + i * 6 + j] * v[j];
+        nv[i] = a;
+    }
+    if (flags & 1) {
+        uint64_t bits;
+        memcpy(&bits, &d[42], sizeof(bits));
+        const double* tm = reinterpret_cast<const double*>((uintptr_t)bits);
+        for (int i = 0; i < 6; ++i) {
+            double a = nv[i];
+            for (int j = 0; j < 6; ++j)
+                for (int l = 0; l < 6; ++l) a = a + __ldg(&tm[(i * 6 + j) * 6 + l]) * v[j] * v[l];
+            nv[i] = a;
+        }
+    }
+    x = nv[0];
+    xp = nv[1];
+    y = nv[2];
+    yp = nv[3];
+    cdt = nv[4];
+    dpop = nv[5];
+}
+
 // FF_nllens thin kick (out of line: rare op with atan and log)
 __device__ __noinline__ void nllens_op(double x, double& xp, double y, double& yp, const double* d)
 {
@@ -644,6 +675,9 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
             break;
         case OP_KICK_YOSHIDA:
             if constexpr (kFull) yoshida6_op<OP_KICK_YOSHIDA>(x, xp, y, yp, cdt, dpop, op);
+            break;
+        case OP_MATRIX:
+            matrix_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
             break;
         case OP_DIPEDGE:
             dipedge_op(x, xp, y, yp, op.d);

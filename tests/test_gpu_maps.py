@@ -396,3 +396,22 @@ def test_gpu_dipedge_bit_exact(syn, orc):
     assert np.array_equal(gm, om)
     assert np.array_equal(gp, op)
     assert np.array_equal(b.design_state()[0], sim.design_state()[0])
+
+
+def test_gpu_matrix_element_bit_exact(syn, orc):
+    """MAD-X MATRIX elements (FF_matrix): one linear with kicks, one with a
+    second-order tensor held in device memory, between drifts, two turns:
+    bit-identical to the oracle; the design particle is not moved by them."""
+    from test_matrix_element import BOOSTER, matrix_attrs
+    g = np.random.default_rng(10)
+    rm = np.eye(6) + 0.05 * g.standard_normal((6, 6))
+    tm = np.zeros((6, 6, 6))
+    tm[0, 0, 0], tm[1, 0, 2], tm[3, 2, 3], tm[4, 5, 5], tm[5, 1, 4] = 2.0, -3.0, 0.5, 10.0, 0.25
+    spec = [elem("drift", "d0", l=0.3), elem("matrix", "m1", **matrix_attrs(BOOSTER, kick=[1e-5, 0, -2e-5, 0, 0, 0])),
+            elem("drift", "d1", l=0.3), elem("matrix", "m2", **matrix_attrs(rm, tm=tm))]
+    n = 5000
+    p = gaussian_bunch(n, [1e-4, 1e-5, 1e-4, 1e-5, 0.01, 1e-5], 24)
+    (gp, gm, _, b, _), (op, om, _, sim) = run_both(syn, orc, spec, p, "indep", 1, 2)
+    assert np.array_equal(gm, om)
+    assert np.array_equal(gp, op)
+    assert np.array_equal(b.design_state()[0], sim.design_state()[0])
