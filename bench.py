@@ -87,6 +87,45 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def ring_c3(syn, torch, turns=1, warmup_steps=16):
+    """Config 3: the 24-cell ring (QF 0.5, SF thin, D 0.75, B 2.0, D 0.75,
+    QD 0.5, SD thin, D 0.75, B 2.0, D 0.75 per cell; circular aperture 5 cm on
+    every element), 2^24 macroparticles, 128x128x256 grid, 16 kicks per cell
+    (384 steps per turn), FP64 and mixed precision, device time with CUDA
+    events per turn."""
+    from helpers import product_lattice, ring_cell
+    spec = []
+    for c in range(24):
+        for e in ring_cell(radius=0.05):
+            e = dict(e)
+            e["name"] = "%s_%d" % (e["name"], c)
+            spec.append(e)
+    lat, ref = product_lattice(spec)
+    n = 1 << 24
+    out = {"macroparticles": n, "grid": [128, 128, 256], "steps_per_turn": 384, "turns": turns}
+    for prec in ("fp64", "mixed"):
+        opts = syn.Space_charge_3d_open_hockney_options(128, 128, 256)
+        opts.precision = getattr(syn.precision_t, prec)
+        prop = syn.Propagator(lat, syn.Split_operator_stepper(opts, 16 * 24))
+        bunch = syn.Bunch(ref, n, REAL_NUM)
+        bunch.populate_gaussian([2e-3, 1e-4, 2e-3, 1e-4, 0.3, 1e-4], 3)
+        prop.propagate_steps(bunch, 0, warmup_steps)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        prop.propagate_steps(bunch, warmup_steps, 384 * turns)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        alive = bunch.get_total_num()
+        out[prec] = {"value": alive * 384 * turns / (ms * 1e-3), "ms_per_step": ms / (384 * turns), "alive": alive,
+                     "emittance": [float(x) for x in bunch.moments()[2]]}
+        del prop, bunch
+        torch.cuda.empty_cache()
+    out["value"] = out["mixed"]["value"]
+    return out
+
+
 def fodo_lattice(syn):
     from helpers import MP, fodo_cell, product_lattice
     return product_lattice(fodo_cell())
@@ -338,8 +377,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="time the default launch shapes")
     ap.add_argument("--particles", type=int, default=N_PART, help="bunch size (profiling cases only)")
-    ap.add_argument("--config", default="c1", choices=["c1", "c2", "c4"],
-                    help="c1: FODO 4M FP64 + mixed (default); c2: 64-bunch quad scan; c4: served job stream")
+    ap.add_argument("--config", default="c1", choices=["c1", "c2", "c3", "c4"],
+                    help="c1: FODO 4M FP64 + mixed (default); c2: 64-bunch quad scan; c3: 24-cell ring, 2^24 "
+                         "macroparticles, 128^2x256; c4: served job stream")
     ap.add_argument("--extras", type=int, default=1, help="0: skip the mixed-precision and served legs of c1")
     ap.add_argument("--jobs", type=int, default=48, help="c4: jobs in the served stream")
     args = ap.parse_args()
@@ -355,11 +395,15 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
-    if args.config in ("c2", "c4"):
+    if args.config in ("c2", "c3", "c4"):
         # single-GPU workloads: rank 0 alone runs them
         import synergia2_b200 as syn
         if rank == 0:
-            if args.config == "c2":
+            if args.config == "c3":
+                r = ring_c3(syn, torch)
+                wl = ("24-cell ring (QF, SF thin, B 2 m, QD, SD thin; circular aperture 5 cm), 2^24 macroparticles, "
+                      "128^2x256 grid, 16 kicks per cell, one turn (384 steps) in FP64 and in mixed precision")
+            elif args.config == "c2":
                 r = batched_scan(syn, torch, 64, 50, seed=7)
                 wl = ("quad-strength scan: 64 FODO bunches, k1 U[0.4,0.8], macroparticles log-uniform [1e5,4e6], "
                       "grids {32^2x64, 64^2x128, 64^2x256}, 50 passes, mixed precision, CUDA-graph turns")
