@@ -111,15 +111,25 @@ def ring_c3(syn, torch, turns=1, warmup_steps=16):
         bunch.populate_gaussian([2e-3, 1e-4, 2e-3, 1e-4, 0.3, 1e-4], 3)
         prop.propagate_steps(bunch, 0, warmup_steps)
         torch.cuda.synchronize()
+        L = syn.lib()
+        L.sb2_profile_enable(1)
+        for c in range(8):
+            L.sb2_profile_read(c, None, None, None, 1)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         prop.propagate_steps(bunch, warmup_steps, 384 * turns)
         e1.record()
         torch.cuda.synchronize()
+        L.sb2_profile_enable(0)
         ms = e0.elapsed_time(e1)
+        brk = {}
+        for c in range(8):
+            nm, tot, cnt = ctypes.c_char_p(), ctypes.c_double(), ctypes.c_int64()
+            syn.check(L.sb2_profile_read(c, ctypes.byref(nm), ctypes.byref(tot), ctypes.byref(cnt), 1))
+            brk[nm.value.decode()] = round(tot.value / (384 * turns), 4)
         alive = bunch.get_total_num()
         out[prec] = {"value": alive * 384 * turns / (ms * 1e-3), "ms_per_step": ms / (384 * turns), "alive": alive,
-                     "emittance": [float(x) for x in bunch.moments()[2]]}
+                     "step_breakdown_ms": brk, "emittance": [float(x) for x in bunch.moments()[2]]}
         del prop, bunch
         torch.cuda.empty_cache()
     out["value"] = out["mixed"]["value"]
