@@ -436,9 +436,9 @@ constexpr int kTrackThreads = 256;
 // integrators and the sector bend so that passes made only of drifts, thin
 // kicks, apertures, the space-charge kick and the moment sums fit in fewer
 // registers and run at higher occupancy.
-// TRACK_QUAD: the light ops plus the pure-quadrupole Yoshida integrator only
-// (the FODO and ring passes), a smaller body than the variant that inlines
-// every integrator: 3 CTAs/SM (80 registers, a 20-byte spill) measured 8%
+// TRACK_QUAD: the light ops plus the pure-quadrupole Yoshida integrator and
+// the (out-of-line) pure-dipole sector bend (the FODO and ring passes), a
+// smaller body than the variant that inlines every integrator: 3 CTAs/SM (80 registers, a 20-byte spill) measured 8%
 // faster on the FODO quadrupole passes than TRACK_FULL_WIDE at 2 CTAs/SM.
 enum TrackVariant { TRACK_LIGHT = 0, TRACK_FULL = 1, TRACK_FULL_WIDE = 2, TRACK_QUAD = 3 };
 
@@ -719,7 +719,7 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
             break;
         }
         case OP_SBEND: {
-            if constexpr (kFull) sbend_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
+            if constexpr (kQuad) sbend_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
             break;
         }
         case OP_SBEND_CF: {
@@ -857,12 +857,13 @@ __global__ void __launch_bounds__(kTrackThreads, PF ? SB2_LIGHT_OCC : TrackOcc<V
     }
 }
 
-// true when the only integrator of the pass is the pure-quadrupole Yoshida
+// true when the pass needs no integrator beyond the pure-quadrupole Yoshida
+// and the pure-dipole sector bend (FODO and ring lattices)
 static bool track_quad_only(const MapOp* ops, int n)
 {
     for (int i = 0; i < n; ++i) {
         int k = ops[i].kind;
-        if (k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_OCT_YOSHIDA || k == OP_KICK_YOSHIDA || k == OP_SBEND ||
+        if (k == OP_QUAD_CF || k == OP_SEXT_YOSHIDA || k == OP_OCT_YOSHIDA || k == OP_KICK_YOSHIDA ||
             k == OP_SBEND_CF || k == OP_SOLENOID || k == OP_RFCAVITY)
             return false;
     }
