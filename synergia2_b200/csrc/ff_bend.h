@@ -26,29 +26,46 @@
 
 constexpr double kBendC = 299792458.0;
 
+// Constants of the bend units that depend only on the reference momentum,
+// the mass and the bend strength.  The reference evaluates them for every
+// particle and unit (ff_algorithm.h:276-285); computed once with the same
+// operations they are the same doubles: igib2 = (m/E0)^2 / (1 - (m/E0)^2)
+// as ((1/gamma)(1/gamma))(1/beta)(1/beta), cs = (c c 1e-9) strength.
+struct BendConst {
+    double igib2, cs;
+};
+SB2_FF BendConst bend_const(double p_ref, double m, double strength)
+{
+    const double uni = 1.0;
+    double p0 = p_ref;
+    double E0 = sqrt(p0 * p0 + m * m);
+    double igamma = m / E0;
+    double ibeta = uni / sqrt(uni - igamma * igamma);
+    double csq = kBendC * kBendC * 1e-9;
+    BendConst k;
+    k.igib2 = igamma * igamma * ibeta * ibeta;
+    k.cs = csq * strength;
+    return k;
+}
+
 // ff_algorithm.h:255-343: the particle moves on its circle through the
 // rotation `phase` / translation `term` of one bend piece of angle -theta.
 SB2_FF void bend_unit(double& x, double& xp, double& y, double& yp, double& cdt, double dpop, double theta,
-                      double strength, double p_ref, double m, double cdt_ref, double phase_r, double phase_i,
+                      const BendConst& bk, double p_ref, double m, double cdt_ref, double phase_r, double phase_i,
                       double term_r, double term_i)
 {
     const double uni = 1.0;
     const double tc = kBendC;
-    double p0 = p_ref;
     double p = p_ref * (dpop + uni);
-    double E0 = sqrt(p0 * p0 + m * m);
     double E = sqrt(p * p + m * m);
-    double igamma = m / E0;
-    double ibeta = uni / sqrt(uni - igamma * igamma);
-    double csq = kBendC * kBendC * 1e-9;
     double psq = (dpop + uni) * (dpop + uni);
-    double Ef = uni / sqrt(psq + igamma * igamma * ibeta * ibeta);
+    double Ef = uni / sqrt(psq + bk.igib2);
     double beta1 = Ef * xp;
     double beta2 = Ef * yp;
     double beta3 = Ef * sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
     double ui_r = 0.0, ui_i = x;
     double vui_r = tc * beta3, vui_i = tc * beta1;
-    double iomega = E / (csq * strength);
+    double iomega = E / bk.cs;
     double bi_r = -vui_i * iomega - ui_r;
     double bi_i = vui_r * iomega - ui_i;
     double bf_r = bi_r * phase_r - bi_i * phase_i + term_r;
@@ -75,25 +92,20 @@ SB2_FF void bend_unit(double& x, double& xp, double& y, double& yp, double& cdt,
 // ff_algorithm.h:366-450: the same circle through the pure rotation of a
 // pole face of angle e (no translation, no reference-time subtraction).
 SB2_FF void bend_edge(double& x, double& xp, double& y, double& yp, double& cdt, double dpop, double e,
-                      double phase_r, double phase_i, double strength, double p_ref, double m)
+                      double phase_r, double phase_i, const BendConst& bk, double p_ref, double m)
 {
     const double uni = 1.0;
     const double tc = kBendC;
-    double p0 = p_ref;
     double p = p_ref * (dpop + uni);
-    double E0 = sqrt(p0 * p0 + m * m);
     double E = sqrt(p * p + m * m);
-    double igamma = m / E0;
-    double ibeta = uni / sqrt(uni - igamma * igamma);
-    double csq = kBendC * kBendC * 1e-9;
     double psq = (dpop + uni) * (dpop + uni);
-    double Ef = uni / sqrt(psq + igamma * igamma * ibeta * ibeta);
+    double Ef = uni / sqrt(psq + bk.igib2);
     double beta1 = Ef * xp;
     double beta2 = Ef * yp;
     double beta3 = Ef * sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
     double ui_r = 0.0, ui_i = x;
     double vui_r = tc * beta3, vui_i = tc * beta1;
-    double iomega = E / (csq * strength);
+    double iomega = E / bk.cs;
     double bi_r = -vui_i * iomega - ui_r;
     double bi_i = vui_r * iomega - ui_i;
     double bf_r = bi_r * phase_r - bi_i * phase_i;
@@ -192,11 +204,11 @@ constexpr double kBY6_D[4] = {1.58722492772224294589251207526, -1.99977809735512
 SB2_FF void bend_yoshida6(double& x, double& xp, double& y, double& yp, double& cdt, double dpop, double pref,
                           double m, double sub_ref_cdt, const double* k1, const double* k2, const double* k3,
                           const double* k4, const double* dphi, const double* phase, const double* term, double r0,
-                          double strength, int steps)
+                          const BendConst& bk, int steps)
 {
     for (int s = 0; s < steps; ++s) {
 #define SB2_BY6_B(j)                                                                                                  \
-    bend_unit(x, xp, y, yp, cdt, dpop, dphi[j], strength, pref, m, sub_ref_cdt, phase[2 * (j)], phase[2 * (j) + 1],   \
+    bend_unit(x, xp, y, yp, cdt, dpop, dphi[j], bk, pref, m, sub_ref_cdt, phase[2 * (j)], phase[2 * (j) + 1],         \
               term[2 * (j)], term[2 * (j) + 1])
         SB2_BY6_B(0); cf_kick5(x, xp, y, yp, r0, k1);
         SB2_BY6_B(1); cf_kick5(x, xp, y, yp, r0, k2);

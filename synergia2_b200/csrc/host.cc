@@ -1012,6 +1012,9 @@ static void ops_sbend(const Lattice& lat, const Slice& sl, Bunch& b, std::vector
         o.d[8] = dphi; o.d[9] = phase.real(); o.d[10] = phase.imag();
         o.d[11] = term.real(); o.d[12] = term.imag();
         o.d[13] = strength; o.d[14] = pref_b; o.d[15] = m_b; o.d[16] = cdt;
+        const hostff::BendConst bk = hostff::bend_const(pref_b, m_b, strength);
+        o.d[17] = bk.igib2;
+        o.d[18] = bk.cs;
         out.push_back(o);
     }
     b.ref.s_n += length;
@@ -1061,6 +1064,7 @@ static void ops_sbend_cf(const Slice& sl, Bunch& b, std::vector<MapOp>& out, dou
     }
     double us_kx = 0, us_ky = 0, ds_kx = 0, ds_ky = 0;
     { // prop_reference_cf: the design particle, from dp/p = 0, strengths unscaled
+        const hostff::BendConst bk_l = hostff::bend_const(pref_l, m_l, strength);
         double x = ref_l.state[0], xp = ref_l.state[1], y = ref_l.state[2], yp = ref_l.state[3];
         double cdt = 0.0, dpop = 0.0;
         const double step_length = length / steps;
@@ -1078,12 +1082,12 @@ static void ops_sbend_cf(const Slice& sl, Bunch& b, std::vector<MapOp>& out, dou
             double kx = us_kx / scale, ky = us_ky / scale;
             yp = yp - kx * y;
             xp = xp + ky * y;
-            hostff::bend_edge(x, xp, y, yp, cdt, dpop, e1, pe1_r, pe1_i, strength, pref_l, m_l);
+            hostff::bend_edge(x, xp, y, yp, cdt, dpop, e1, pe1_r, pe1_i, bk_l, pref_l, m_l);
         }
         hostff::bend_yoshida6(x, xp, y, yp, cdt, dpop, pref_l, m_l, 0.0 * 0.1, kr[0], kr[1], kr[2], kr[3], dphi, phase,
-                              term, r0, strength, steps);
+                              term, r0, bk_l, steps);
         if (redge) {
-            hostff::bend_edge(x, xp, y, yp, cdt, dpop, e2, pe2_r, pe2_i, strength, pref_l, m_l);
+            hostff::bend_edge(x, xp, y, yp, cdt, dpop, e2, pe2_r, pe2_i, bk_l, pref_l, m_l);
             double p_l = 1.0 + dpop;
             double zp = std::sqrt(p_l * p_l - xp * xp - yp * yp);
             ds_kx = ds_edge_k_p * (xp / zp);
@@ -1115,6 +1119,9 @@ static void ops_sbend_cf(const Slice& sl, Bunch& b, std::vector<MapOp>& out, dou
         const double skl = k_l[i] * scale * length / steps;
         for (int j = 0; j < 4; ++j) o.d[39 + 8 * j + i] = hostff::kBY6_D[j] * skl;
     }
+    const hostff::BendConst bk_b = hostff::bend_const(pref_b, m_b, strength);
+    o.d[71] = bk_b.igib2;
+    o.d[72] = bk_b.cs;
     out.push_back(o);
     b.ref.s_n += length;
 }

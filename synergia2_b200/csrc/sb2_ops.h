@@ -56,11 +56,13 @@ enum OpKind : int32_t {
 //  SBEND:        flags bit0 ledge, bit1 redge; 0 ce1 1 se1 2 ce2 3 se2
 //                4 us_kx 5 us_ky 6 ds_kx 7 ds_ky 8 dphi 9 phase_r 10 phase_i
 //                11 term_r 12 term_i 13 strength 14 pref_b 15 m_b 16 ref_cdt
+//                17-18 BendConst (igib2, cs) of (pref_b, m_b, strength)
 //  SBEND_CF:     flags as SBEND; steps = Yoshida steps; 0 ce1 1 se1 2 ce2
 //                3 se2 4 us_kx 5 us_ky 6 ds_kx 7 ds_ky 8 e1 9 e2 10-11 entry
 //                face phase 12-13 exit face phase 14 strength 15 pref_b
 //                16 m_b 17 substep ref_cdt 18 r0 19-22 dphi[4] 23-30
 //                phase[4] 31-38 term[4] 39-70 k1..k4 (8 strengths each)
+//                71-72 BendConst (igib2, cs) of (pref_b, m_b, strength)
 //  MPOLE:        flags = bitmask of active orders (bit n: order n+1),
 //                kl[16] at 0..15
 //  AP_CIRCULAR:  0 r2, 1 xoff, 2 yoff

@@ -273,7 +273,8 @@ __device__ __noinline__ void sbend_op(double& x, double& xp, double& y, double& 
         yp = yp - d[4] * y; // edge_unit ff_algorithm.h:139-148
         xp = xp + d[5] * y;
     }
-    bend_unit(x, xp, y, yp, cdt, dpop, d[8], d[13], d[14], d[15], d[16], d[9], d[10], d[11], d[12]);
+    const BendConst bk{d[17], d[18]};
+    bend_unit(x, xp, y, yp, cdt, dpop, d[8], bk, d[14], d[15], d[16], d[9], d[10], d[11], d[12]);
     if (flags & 2) {
         yp = yp - d[6] * y;
         xp = xp + d[7] * y;
@@ -348,16 +349,17 @@ __device__ __noinline__ void nllens_op(double x, double& xp, double y, double& y
 __device__ __noinline__ void sbend_cf_op(double& x, double& xp, double& y, double& yp, double& cdt, double& dpop,
                                          const double* d, int steps, int flags)
 {
+    const BendConst bk{d[71], d[72]};
     if (flags & 1) {
         slot_unit(x, xp, y, yp, cdt, dpop, d[0], d[1], d[15], d[16]);
         yp = yp - d[4] * y; // edge_unit ff_algorithm.h:139-148
         xp = xp + d[5] * y;
-        bend_edge(x, xp, y, yp, cdt, dpop, d[8], d[10], d[11], d[14], d[15], d[16]);
+        bend_edge(x, xp, y, yp, cdt, dpop, d[8], d[10], d[11], bk, d[15], d[16]);
     }
     bend_yoshida6(x, xp, y, yp, cdt, dpop, d[15], d[16], d[17], d + 39, d + 47, d + 55, d + 63, d + 19, d + 23,
-                  d + 31, d[18], d[14], steps);
+                  d + 31, d[18], bk, steps);
     if (flags & 2) {
-        bend_edge(x, xp, y, yp, cdt, dpop, d[9], d[12], d[13], d[14], d[15], d[16]);
+        bend_edge(x, xp, y, yp, cdt, dpop, d[9], d[12], d[13], bk, d[15], d[16]);
         yp = yp - d[6] * y;
         xp = xp + d[7] * y;
         slot_unit(x, xp, y, yp, cdt, dpop, d[2], d[3], d[15], d[16]);
