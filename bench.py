@@ -91,8 +91,8 @@ def ring_c3(syn, torch, turns=1, warmup_steps=16):
     """Config 3: the 24-cell ring (QF 0.5, SF thin, D 0.75, B 2.0, D 0.75,
     QD 0.5, SD thin, D 0.75, B 2.0, D 0.75 per cell; circular aperture 5 cm on
     every element), 2^24 macroparticles, 128x128x256 grid, 16 kicks per cell
-    (384 steps per turn), FP64 and mixed precision, device time with CUDA
-    events per turn."""
+    (384 steps per turn), FP64 and mixed precision, each propagator
+    autotuned first; device time with CUDA events per turn."""
     from helpers import product_lattice, ring_cell
     spec = []
     for c in range(24):
@@ -110,6 +110,7 @@ def ring_c3(syn, torch, turns=1, warmup_steps=16):
         bunch = syn.Bunch(ref, n, REAL_NUM)
         bunch.populate_gaussian([2e-3, 1e-4, 2e-3, 1e-4, 0.3, 1e-4], 3)
         prop.propagate_steps(bunch, 0, warmup_steps)
+        best, trials = prop.autotune(bunch, steps=16)
         torch.cuda.synchronize()
         L = syn.lib()
         L.sb2_profile_enable(1)
@@ -129,7 +130,9 @@ def ring_c3(syn, torch, turns=1, warmup_steps=16):
             brk[nm.value.decode()] = round(tot.value / (384 * turns), 4)
         alive = bunch.get_total_num()
         out[prec] = {"value": alive * 384 * turns / (ms * 1e-3), "ms_per_step": ms / (384 * turns), "alive": alive,
-                     "step_breakdown_ms": brk, "emittance": [float(x) for x in bunch.moments()[2]]}
+                     "step_breakdown_ms": brk, "emittance": [float(x) for x in bunch.moments()[2]],
+                     "autotune": {"best": best, "trials": len(trials), "default_ms": round(trials[0]["ms"], 3),
+                                  "best_ms": round(min(r["ms"] for r in trials), 3)}}
         del prop, bunch
         torch.cuda.empty_cache()
     out["value"] = out["mixed"]["value"]
