@@ -87,6 +87,34 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def fp64_roofline(syn, workload, n, light, full):
+    """FP64 side of the particle passes: algorithmic FP64 operations per
+    launch (the per-macroparticle counts of profiles/fp64_flops_per_particle.json,
+    made by running the oracle's particle code on a counting scalar, times the
+    macroparticles) over the measured average launch time, against the FP64
+    FMA peak of this GPU measured now.  light / full are (total ms, launches)
+    of the two kernel variants over the timed region."""
+    path = os.path.join(ROOT, "profiles", "fp64_flops_per_particle.json")
+    try:
+        w = json.load(open(path))["workloads"][workload]
+    except (OSError, KeyError, ValueError):
+        return None
+    pk = ctypes.c_double()
+    syn.check(syn.lib().sb2_fp64_peak_probe(ctypes.byref(pk), None))
+    out = {"bound": "fp64", "unit": "TFLOP/s", "peak": pk.value,
+           "peak_source": "measured in this run: sb2_fp64_peak_probe, independent FP64 FMA chains on every SM "
+                          "(an FMA counts 2)",
+           "flops_source": "profiles/fp64_flops_per_particle.json (python oracle/count_flops.py)"}
+    for name, (ms, cnt), key in (("full_variant", full, "full_pass_flops_mean"),
+                                 ("light_variant", light, "light_pass_flops_mean")):
+        if cnt:
+            fl = w[key] * n
+            ach = fl / (ms / cnt * 1e-3) / 1e12
+            out[name] = {"flops_per_particle": w[key], "algorithmic_flops_per_launch": fl,
+                         "avg_launch_ms": ms / cnt, "achieved": ach, "frac": ach / pk.value}
+    return out
+
+
 def ring_c3(syn, torch, turns=1, warmup_steps=16):
     """Config 3: the 24-cell ring (QF 0.5, SF thin, D 0.75, B 2.0, D 0.75,
     QD 0.5, SD thin, D 0.75, B 2.0, D 0.75 per cell; circular aperture 5 cm on
@@ -123,14 +151,17 @@ def ring_c3(syn, torch, turns=1, warmup_steps=16):
         torch.cuda.synchronize()
         L.sb2_profile_enable(0)
         ms = e0.elapsed_time(e1)
-        brk = {}
+        brk, raw = {}, {}
         for c in range(8):
             nm, tot, cnt = ctypes.c_char_p(), ctypes.c_double(), ctypes.c_int64()
             syn.check(L.sb2_profile_read(c, ctypes.byref(nm), ctypes.byref(tot), ctypes.byref(cnt), 1))
             brk[nm.value.decode()] = round(tot.value / (384 * turns), 4)
+            raw[nm.value.decode()] = (tot.value, cnt.value)
         alive = bunch.get_total_num()
         out[prec] = {"value": alive * 384 * turns / (ms * 1e-3), "ms_per_step": ms / (384 * turns), "alive": alive,
                      "step_breakdown_ms": brk, "emittance": [float(x) for x in bunch.moments()[2]],
+                     "roofline_fp64": fp64_roofline(syn, "ring_c3", alive, raw.get("track", (0.0, 0)),
+                                                    raw.get("track_full", (0.0, 0))),
                      "autotune": {"best": best, "trials": len(trials), "default_ms": round(trials[0]["ms"], 3),
                                   "best_ms": round(min(r["ms"] for r in trials), 3)}}
         del prop, bunch
@@ -558,7 +589,8 @@ def main():
                          "algorithmic_bytes_per_launch": alg_track,
                          "launches": tr_n, "avg_launch_ms": tr_ms / max(tr_n, 1),
                          "full_variant": {"bound": "fp64 pipe", "launches": tf_n,
-                                          "avg_launch_ms": tf_ms / max(tf_n, 1)}},
+                                          "avg_launch_ms": tf_ms / max(tf_n, 1)},
+                         "fp64": fp64_roofline(syn, "fodo_c1", n_alive, (tr_ms, tr_n), (tf_ms, tf_n))},
             "e2e": {"value": e2e_total / e2e_s, "unit": "macroparticle-steps/s",
                     "h2d_bytes_per_step": bunch_bytes / args.steps,
                     "d2h_bytes_per_step": bunch_bytes / args.steps + 16,

@@ -66,6 +66,12 @@ sb2_status sb2_profile_enable(int32_t on);
 sb2_status sb2_profile_read(int32_t category, const char** name, double* total_ms, int64_t* launches,
                             int32_t reset);
 
+/* FP64 peak of the current device at its present clocks, in TFLOP/s (an FMA
+ * counts 2): a kernel of independent FMA chains on every SM, best of six
+ * timed launches on `stream` (CUDA events), synchronous.  The denominator of
+ * the FP64-bound particle passes' roofline. */
+sb2_status sb2_fp64_peak_probe(double* tflops, void* stream);
+
 /* ---------------------------------------------------------------------
  * Options of the 3D open-boundary Hockney solver.
  * Replaces Space_charge_3d_open_hockney_options

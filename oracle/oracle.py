@@ -11,6 +11,12 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 
+# operation counting (orc_flops_*): categories and operation kinds, in the
+# order of the oracle's FlopCat / FlopOp
+FLOP_CATEGORIES = ("drift", "quadrupole", "sbend", "thin", "thick_other", "aperture", "sc_domain",
+                   "sc_deposit", "sc_kick")
+FLOP_OPS = ("add", "mul", "div", "sqrt", "fn")
+
 STEPPER_SPLIT, STEPPER_SPLIT_ELEMENTS, STEPPER_INDEP_ELEMENTS = 0, 1, 2
 REF_TOTAL_ENERGY, REF_MOMENTUM, REF_KINETIC_ENERGY = 0, 1, 2
 MP = 0.938272046
@@ -83,6 +89,9 @@ def lib():
         L.orc_fft3d.argtypes = [pd, i, i, i, i]
         L.orc_green.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), pd, i, pd]
         L.orc_set_threads.argtypes = [i]
+        L.orc_flops_begin.argtypes = [i64]
+        L.orc_flops_end.argtypes = [ctypes.POINTER(i)]
+        L.orc_flops_record.argtypes = [i, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(i64)]
         _LIB = L
     return _LIB
 
@@ -185,6 +194,33 @@ class Sim:
 
     def propagate_steps(self, first, count):
         _check(lib().orc_sim_propagate_steps(self.h, first, count))
+
+    def count_flops(self, index, first, count):
+        """Runs steps [first, first+count) as propagate_steps does and
+        counts the algorithmic FP64 operations of particle `index` in the
+        oracle's own particle code.  Returns one record per operator of each
+        step: (step, 'I' or 'C', counts) with counts[category][op] (see
+        FLOP_CATEGORIES, FLOP_OPS).  Raises if an element kind whose particle
+        loop is not instrumented ran."""
+        L = lib()
+        L.orc_flops_begin(index)
+        try:
+            rc = L.orc_sim_propagate_steps(self.h, first, count)
+        finally:
+            unc = ctypes.c_int()
+            nrec = L.orc_flops_end(ctypes.byref(unc))
+        _check(rc)
+        if unc.value:
+            raise RuntimeError("operation counting: an element kind without an instrumented particle loop ran")
+        out = []
+        buf = (ctypes.c_int64 * (len(FLOP_CATEGORIES) * len(FLOP_OPS)))()
+        st, kd = ctypes.c_int(), ctypes.c_int()
+        for r in range(nrec):
+            _check(L.orc_flops_record(r, ctypes.byref(st), ctypes.byref(kd), buf))
+            a = np.array(buf[:], dtype=np.int64).reshape(len(FLOP_CATEGORIES), len(FLOP_OPS))
+            out.append((st.value, chr(kd.value), {c: dict(zip(FLOP_OPS, map(int, a[i])))
+                                                  for i, c in enumerate(FLOP_CATEGORIES)}))
+        return out
 
     def sc_last(self, shape):
         gx, gy, gz = shape

@@ -31,6 +31,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -53,6 +54,85 @@ constexpr double rp = e / (4 * pi * epsilon0 * mp * 1.0e9);
 } // namespace pc
 
 thread_local std::string g_err;
+
+// ---------------------------------------------------------------------------
+// FP64 operation counting: the algorithmic flops per particle of each
+// operation, counted by running the oracle's own per-particle code on a
+// counting scalar.  CD is a double that tallies every add or subtract,
+// multiply, divide, square root and elementary function (asin, sin, cos,
+// log, exp) it takes part in; sign changes, comparisons, floor and fabs are
+// not counted.  The particle loops below write their per-particle work as a
+// body generic in the scalar type; with counting on, count_particle() runs
+// that body once more on CD copies of one chosen particle (its results are
+// discarded), so the particles' doubles are exactly those of a run without
+// counting.  Counts are kept per operation category and cut into one record
+// per operator of a step (first half, collective, second half).
+// ---------------------------------------------------------------------------
+enum FlopCat { FC_DRIFT, FC_QUAD, FC_SBEND, FC_THIN, FC_THICK_OTHER, FC_APERTURE, FC_DOMAIN, FC_DEPOSIT, FC_KICK, FC_N };
+enum FlopOp { FO_ADD, FO_MUL, FO_DIV, FO_SQRT, FO_FN, FO_N };
+
+struct FlopRecord {
+    int step;
+    char kind; // 'I' independent operator, 'C' collective operator
+    int64_t n[FC_N][FO_N];
+};
+
+struct FlopState {
+    bool on = false;
+    bool uncounted = false; // an element kind whose particle loop is not instrumented ran
+    int64_t index = -1;     // the particle whose work is counted
+    int cat = 0;
+    int64_t n[FC_N][FO_N] = {};
+    std::vector<FlopRecord> records;
+
+    void mark(int step, char kind)
+    {
+        if (!on) return;
+        FlopRecord r{step, kind, {}};
+        std::memcpy(r.n, n, sizeof(n));
+        std::memset(n, 0, sizeof(n));
+        records.push_back(r);
+    }
+};
+inline FlopState g_flops;
+
+struct CD {
+    double v;
+    CD() : v(0.0) {}
+    CD(double a) : v(a) {}
+};
+inline void tally(int op) { ++g_flops.n[g_flops.cat][op]; }
+inline CD operator+(CD a, CD b) { tally(FO_ADD); return CD(a.v + b.v); }
+inline CD operator-(CD a, CD b) { tally(FO_ADD); return CD(a.v - b.v); }
+inline CD operator*(CD a, CD b) { tally(FO_MUL); return CD(a.v * b.v); }
+inline CD operator/(CD a, CD b) { tally(FO_DIV); return CD(a.v / b.v); }
+inline CD operator-(CD a) { return CD(-a.v); }
+inline CD& operator+=(CD& a, CD b) { return a = a + b; }
+inline CD& operator-=(CD& a, CD b) { return a = a - b; }
+inline CD& operator*=(CD& a, CD b) { return a = a * b; }
+inline CD& operator/=(CD& a, CD b) { return a = a / b; }
+inline bool operator<(CD a, CD b) { return a.v < b.v; }
+inline bool operator>(CD a, CD b) { return a.v > b.v; }
+inline bool operator<=(CD a, CD b) { return a.v <= b.v; }
+inline bool operator>=(CD a, CD b) { return a.v >= b.v; }
+inline CD sqrt(CD a) { tally(FO_SQRT); return CD(std::sqrt(a.v)); }
+inline CD asin(CD a) { tally(FO_FN); return CD(std::asin(a.v)); }
+inline CD sin(CD a) { tally(FO_FN); return CD(std::sin(a.v)); }
+inline CD cos(CD a) { tally(FO_FN); return CD(std::cos(a.v)); }
+inline CD log(CD a) { tally(FO_FN); return CD(std::log(a.v)); }
+inline CD floor(CD a) { return CD(std::floor(a.v)); }
+inline CD fabs(CD a) { return CD(std::fabs(a.v)); }
+inline bool isfinite(CD a) { return std::isfinite(a.v); }
+inline double val(double a) { return a; }
+inline double val(CD a) { return a.v; }
+using std::asin;
+using std::cos;
+using std::fabs;
+using std::floor;
+using std::isfinite;
+using std::log;
+using std::sin;
+using std::sqrt;
 
 // ---------------------------------------------------------------------------
 // Four_momentum / Reference_particle (foundation/four_momentum.cc:8-16,
@@ -190,45 +270,64 @@ struct Bunch {
     }
 };
 
+// Counting mode: runs `body` once on CD copies of the counted particle's six
+// coordinates, the tallies going to category `cat`; the copies are dropped.
+template <class F>
+inline void count_particle(int cat, Bunch& b, F&& body)
+{
+    if (!g_flops.on) return;
+    const int64_t i = g_flops.index;
+    if (i < 0 || i >= b.n_active || !b.masks[i]) return;
+    CD p[6];
+    for (int j = 0; j < 6; ++j) p[j] = CD(b.P(i, j));
+    const int saved = g_flops.cat;
+    g_flops.cat = cat;
+    body(p[0], p[1], p[2], p[3], p[4], p[5]);
+    g_flops.cat = saved;
+}
+
 // ---------------------------------------------------------------------------
-// ff_algorithm.h units
+// ff_algorithm.h units, generic in the scalar type R (double, or CD when
+// counting)
 // ---------------------------------------------------------------------------
 inline bool close_to_zero(double v) { return std::fabs(v) < 1e-13; } // :18-22
 
 // drift_unit ff_algorithm.h:47-79
-inline void drift_unit(double& x, double xp, double& y, double yp, double& cdt, double dpop,
+template <class R>
+inline void drift_unit(R& x, R xp, R& y, R yp, R& cdt, R dpop,
                        double length, double reference_momentum, double m, double reference_cdt)
 {
     double uni = 1.0;
     double sig = (double)((0.0 < length) - (length < 0.0));
-    double vl = length, vm = m, vrm = reference_momentum, vrc = reference_cdt;
-    double dp = dpop + uni;
-    double inv_npz = uni / std::sqrt(dp * dp - xp * xp - yp * yp);
-    double lxpr = xp * vl * inv_npz;
-    double lypr = yp * vl * inv_npz;
-    double D2 = lxpr * lxpr + vl * vl + lypr * lypr;
-    double p = dp * vrm;
-    double E2 = p * p + vm * vm;
-    double ibeta2 = E2 / (p * p);
+    R vl = length, vm = m, vrm = reference_momentum, vrc = reference_cdt;
+    R dp = dpop + uni;
+    R inv_npz = uni / sqrt(dp * dp - xp * xp - yp * yp);
+    R lxpr = xp * vl * inv_npz;
+    R lypr = yp * vl * inv_npz;
+    R D2 = lxpr * lxpr + vl * vl + lypr * lypr;
+    R p = dp * vrm;
+    R E2 = p * p + vm * vm;
+    R ibeta2 = E2 / (p * p);
     x = x + lxpr;
     y = y + lypr;
-    cdt = cdt + sig * std::sqrt(D2 * ibeta2) - vrc;
+    cdt = cdt + sig * sqrt(D2 * ibeta2) - vrc;
 }
 
 // slot_unit ff_algorithm.h:83-129
-inline void slot_unit(double& x, double& xp, double& y, double& yp, double& cdt, double& dpop,
+template <class R>
+inline void slot_unit(R& x, R& xp, R& y, R& yp, R& cdt, R& dpop,
                       double ct, double st, double pref, double m)
 {
     const double uni = 1.0;
-    double r0 = x, r1 = y, r2 = 0.0;
-    double zp = std::sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
-    double p = (dpop + uni) * pref;
-    double e = std::sqrt(p * p + m * m);
-    double b0 = xp * pref / e;
-    double b1 = yp * pref / e;
-    double b2 = zp * pref / e;
-    double bp = st * b0 + ct * b2;
-    double tau = -x * st / bp;
+    R r0 = x, r1 = y, r2 = 0.0;
+    R zp = sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
+    R p = (dpop + uni) * pref;
+    R e = sqrt(p * p + m * m);
+    R b0 = xp * pref / e;
+    R b1 = yp * pref / e;
+    R b2 = zp * pref / e;
+    R bp = st * b0 + ct * b2;
+    R tau = -x * st / bp;
     r0 = x + tau * b0;
     r1 = y + tau * b1;
     r2 = tau * b2;
@@ -239,7 +338,8 @@ inline void slot_unit(double& x, double& xp, double& y, double& yp, double& cdt,
 }
 
 // edge_unit (ref particle angle form) ff_algorithm.h:139-148
-inline void edge_unit(double y, double& xp, double& yp, double kx, double ky)
+template <class R>
+inline void edge_unit(R y, R& xp, R& yp, double kx, double ky)
 {
     yp = yp - kx * y;
     xp = xp + ky * y;
@@ -283,40 +383,41 @@ inline void bend_complete(double& x, double& xp, double& y, double& yp, double& 
 }
 
 // bend_unit ff_algorithm.h:255-343 (device form, real arithmetic)
-inline void bend_unit(double& x, double& xp, double& y, double& yp, double& cdt, double dpop,
+template <class R>
+inline void bend_unit(R& x, R& xp, R& y, R& yp, R& cdt, R dpop,
                       double theta, double strength, double p_ref, double m, double cdt_ref,
                       std::complex<double> phase, std::complex<double> term)
 {
     const double uni = 1.0;
     const double tc = pc::c;
-    double p0 = p_ref;
-    double p = p_ref * (dpop + uni);
-    double E0 = std::sqrt(p0 * p0 + m * m);
-    double E = std::sqrt(p * p + m * m);
-    double igamma = m / E0;
-    double ibeta = uni / std::sqrt(uni - igamma * igamma);
-    double csq = pc::c * pc::c * 1e-9;
-    double psq = (dpop + uni) * (dpop + uni);
-    double Ef = uni / std::sqrt(psq + igamma * igamma * ibeta * ibeta);
-    double beta1 = Ef * xp;
-    double beta2 = Ef * yp;
-    double beta3 = Ef * std::sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
-    double ui_r = 0.0, ui_i = x;
-    double vui_r = tc * beta3, vui_i = tc * beta1;
-    double iomega = E / (csq * strength);
-    double bi_r = -vui_i * iomega - ui_r;
-    double bi_i = vui_r * iomega - ui_i;
+    R p0 = p_ref;
+    R p = p_ref * (dpop + uni);
+    R E0 = sqrt(p0 * p0 + m * m);
+    R E = sqrt(p * p + m * m);
+    R igamma = m / E0;
+    R ibeta = uni / sqrt(uni - igamma * igamma);
+    R csq = pc::c * pc::c * 1e-9;
+    R psq = (dpop + uni) * (dpop + uni);
+    R Ef = uni / sqrt(psq + igamma * igamma * ibeta * ibeta);
+    R beta1 = Ef * xp;
+    R beta2 = Ef * yp;
+    R beta3 = Ef * sqrt((dpop + uni) * (dpop + uni) - xp * xp - yp * yp);
+    R ui_r = 0.0, ui_i = x;
+    R vui_r = tc * beta3, vui_i = tc * beta1;
+    R iomega = E / (csq * strength);
+    R bi_r = -vui_i * iomega - ui_r;
+    R bi_i = vui_r * iomega - ui_i;
     double phase_r = phase.real(), phase_i = phase.imag();
-    double bf_r = bi_r * phase_r - bi_i * phase_i + term.real();
-    double bf_i = bi_r * phase_i + bi_i * phase_r + term.imag();
-    double rho = tc * std::sqrt(beta1 * beta1 + beta3 * beta3) * iomega;
-    double dthmphi = std::asin(bi_r / rho) - std::asin(bf_r / rho);
-    double expf_r = std::cos(dthmphi);
-    double expf_i = std::sin(dthmphi);
-    double vuf_i = vui_r * expf_i + vui_i * expf_r;
-    double uf_i = (ui_r + bi_r) * expf_i + (ui_i + bi_i) * expf_r - bf_i;
-    double dtheta = dthmphi + theta;
-    double ncdt = -tc * dtheta * iomega;
+    R bf_r = bi_r * phase_r - bi_i * phase_i + term.real();
+    R bf_i = bi_r * phase_i + bi_i * phase_r + term.imag();
+    R rho = tc * sqrt(beta1 * beta1 + beta3 * beta3) * iomega;
+    R dthmphi = asin(bi_r / rho) - asin(bf_r / rho);
+    R expf_r = cos(dthmphi);
+    R expf_i = sin(dthmphi);
+    R vuf_i = vui_r * expf_i + vui_i * expf_r;
+    R uf_i = (ui_r + bi_r) * expf_i + (ui_i + bi_i) * expf_r - bf_i;
+    R dtheta = dthmphi + theta;
+    R ncdt = -tc * dtheta * iomega;
     x = uf_i;
     xp = vuf_i / (Ef * tc);
     y = y + beta2 * ncdt;
@@ -453,24 +554,28 @@ inline void bend_yoshida6(double& x, double& xp, double& y, double& yp, double& 
 }
 
 // thin kicks ff_algorithm.h:919-963
-inline void thin_dipole_unit(double, double& xp, double, double& yp, const double* kL)
+template <class R>
+inline void thin_dipole_unit(R, R& xp, R, R& yp, const double* kL)
 {
     xp = xp - kL[0];
     yp = yp + kL[1];
 }
-inline void thin_quadrupole_unit(double x, double& xp, double y, double& yp, const double* kL)
+template <class R>
+inline void thin_quadrupole_unit(R x, R& xp, R y, R& yp, const double* kL)
 {
     double vk0 = kL[0], vk1 = kL[1];
     xp = xp - vk0 * x + vk1 * y;
     yp = yp + vk0 * y + vk1 * x;
 }
-inline void thin_sextupole_unit(double x, double& xp, double y, double& yp, const double* kL)
+template <class R>
+inline void thin_sextupole_unit(R x, R& xp, R y, R& yp, const double* kL)
 {
     double vk0 = kL[0], vk1 = kL[1];
     xp = xp - 0.5 * vk0 * (x * x - y * y) + vk1 * x * y;
     yp = yp + vk0 * x * y + 0.5 * vk1 * (x * x - y * y);
 }
-inline void thin_octupole_unit(double x, double& xp, double y, double& yp, const double* kL)
+template <class R>
+inline void thin_octupole_unit(R x, R& xp, R y, R& yp, const double* kL)
 {
     double vk0 = kL[0], vk1 = kL[1];
     double n1 = 0.5, n2 = 1.0 / 3.0;
@@ -485,15 +590,17 @@ inline double factorial(int n)
     for (int i = 1; i <= n; ++i) r *= i;
     return r;
 }
-inline double qpow(double x, int i)
+template <class R>
+inline R qpow(R x, int i)
 { // utils/kokkos_types.h:89-95
-    double r = 1;
+    R r = 1.0;
     while (i--) r = r * x;
     return r;
 }
 
 // thin_magnet_unit ff_algorithm.h:1122-1168
-inline void thin_magnet_unit(double x, double& xp, double y, double& yp, const double* kL, int n)
+template <class R>
+inline void thin_magnet_unit(R x, R& xp, R y, R& yp, const double* kL, int n)
 {
     for (int k = 0; k < n; k += 4)
         xp = xp - (kL[0] * (n - k)) * qpow(x, n - k - 1) * qpow(y, k) / (factorial(n - k) * factorial(k));
@@ -516,30 +623,48 @@ inline void thin_magnet_unit(double x, double& xp, double y, double& yp, const d
 // Kick functor forms used by the integrators.
 using kick_fn = void (*)(double, double&, double, double&, double, const double*);
 
-inline void quad_kick(double x, double& xp, double y, double& yp, double, const double* kL)
-{ // ff_quadrupole.h:16-19
-    thin_quadrupole_unit(x, xp, y, yp, kL);
+struct QuadKick { // ff_quadrupole.h:16-19
+    template <class R>
+    void operator()(R x, R& xp, R y, R& yp, R, const double* kL) const
+    {
+        thin_quadrupole_unit(x, xp, y, yp, kL);
+    }
+};
+struct QuadCFKick { // ff_quadrupole.h:22-35
+    template <class R>
+    void operator()(R x, R& xp, R y, R& yp, R, const double* kL) const
+    {
+        thin_quadrupole_unit(x, xp, y, yp, kL);
+        if (kL[2] || kL[3]) thin_quadrupole_unit(x, xp, y, yp, kL + 2);
+        if (kL[4] || kL[5]) thin_sextupole_unit(x, xp, y, yp, kL + 4);
+        if (kL[6] || kL[7]) thin_octupole_unit(x, xp, y, yp, kL + 6);
+        if (kL[8] || kL[9]) thin_magnet_unit(x, xp, y, yp, kL + 8, 5);
+        if (kL[10] || kL[11]) thin_magnet_unit(x, xp, y, yp, kL + 10, 6);
+        if (kL[12] || kL[13]) thin_magnet_unit(x, xp, y, yp, kL + 12, 7);
+        if (kL[14] || kL[15]) thin_magnet_unit(x, xp, y, yp, kL + 14, 8);
+    }
+};
+struct SextKick { // ff_sextupole.h:11-13
+    template <class R>
+    void operator()(R x, R& xp, R y, R& yp, R, const double* kL) const
+    {
+        thin_sextupole_unit(x, xp, y, yp, kL);
+    }
+};
+inline void quad_cf_kick(double x, double& xp, double y, double& yp, double c, const double* kL)
+{
+    QuadCFKick{}(x, xp, y, yp, c, kL);
 }
-inline void quad_cf_kick(double x, double& xp, double y, double& yp, double, const double* kL)
-{ // ff_quadrupole.h:22-35
-    thin_quadrupole_unit(x, xp, y, yp, kL);
-    if (kL[2] || kL[3]) thin_quadrupole_unit(x, xp, y, yp, kL + 2);
-    if (kL[4] || kL[5]) thin_sextupole_unit(x, xp, y, yp, kL + 4);
-    if (kL[6] || kL[7]) thin_octupole_unit(x, xp, y, yp, kL + 6);
-    if (kL[8] || kL[9]) thin_magnet_unit(x, xp, y, yp, kL + 8, 5);
-    if (kL[10] || kL[11]) thin_magnet_unit(x, xp, y, yp, kL + 10, 6);
-    if (kL[12] || kL[13]) thin_magnet_unit(x, xp, y, yp, kL + 12, 7);
-    if (kL[14] || kL[15]) thin_magnet_unit(x, xp, y, yp, kL + 14, 8);
-}
-inline void sext_kick(double x, double& xp, double y, double& yp, double, const double* kL)
-{ // ff_sextupole.h:11-13
-    thin_sextupole_unit(x, xp, y, yp, kL);
+inline void sext_kick(double x, double& xp, double y, double& yp, double c, const double* kL)
+{
+    SextKick{}(x, xp, y, yp, c, kL);
 }
 
 // yoshida6 ff_algorithm.h:1834-2008 (hardwired 6th order, 10 drifts/step)
-inline void yoshida6(double& x, double& xp, double& y, double& yp, double& cdt, double dpop,
+template <class R, class K>
+inline void yoshida6(R& x, R& xp, R& y, R& yp, R& cdt, R dpop,
                      double reference_momentum, double m, double step_reference_cdt,
-                     double step_length, const double* step_strength, int steps, kick_fn kf,
+                     double step_length, const double* step_strength, int steps, K kf,
                      int components)
 {
     const double c1 = 0.79361246386112147294625603763;
@@ -626,11 +751,14 @@ static void drift_apply(const Slice& slice, Bunch& b)
     drift_unit(x, xp, y, yp, cdt, dpop, length, ref_l.p, ref_l.mass, 0.0);
     ref_l.state = {x, xp, y, yp, cdt, dpop};
     const double ref_cdt = cdt;
+    auto body = [&](auto& x, auto& xp, auto& y, auto& yp, auto& cdt, auto& dpop) {
+        drift_unit(x, xp, y, yp, cdt, dpop, length, ref_p, mass, ref_cdt);
+    };
     if (b.n_valid) {
+        count_particle(FC_DRIFT, b, body);
 #pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < b.n_active; ++i)
-            if (b.masks[i])
-                drift_unit(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), b.P(i, 4), b.P(i, 5), length, ref_p, mass, ref_cdt);
+            if (b.masks[i]) body(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), b.P(i, 4), b.P(i, 5));
     }
     b.ref.s_n += length;
 }
@@ -701,14 +829,16 @@ static void quad_apply(const Slice& slice, Bunch& b)
     if (close_to_zero(length)) {
         ref_cdt_fn(0);
         double k2[2] = {kn[0], kn[1]};
+        auto body = [&](auto& x, auto& xp, auto& y, auto& yp, auto&, auto&) {
+            auto xr = x - xoff;
+            auto yr = y - yoff;
+            thin_quadrupole_unit(xr, xp, yr, yp, k2);
+        };
         if (b.n_valid) {
+            count_particle(FC_THIN, b, body);
 #pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < b.n_active; ++i)
-                if (b.masks[i]) {
-                    double x = b.P(i, 0) - xoff;
-                    double y = b.P(i, 2) - yoff;
-                    thin_quadrupole_unit(x, b.P(i, 1), y, b.P(i, 3), k2);
-                }
+                if (b.masks[i]) body(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), b.P(i, 4), b.P(i, 5));
         }
     } else {
         int steps = (int)ele.get("yoshida_steps", 4.0);
@@ -716,22 +846,20 @@ static void quad_apply(const Slice& slice, Bunch& b)
         double ref_p = ref_b.p, ref_m = ref_b.mass;
         double ref_t = ref_cdt_fn(steps);
         double step_ref_t = ref_t / steps, step_l = length / steps;
+        auto body = [&](auto& x, auto& xp, auto& y, auto& yp, auto& cdt, auto& dpop) {
+            auto p0 = x - xoff, p2 = y - yoff;
+            if (has_mp)
+                yoshida6(p0, xp, p2, yp, cdt, dpop, ref_p, ref_m, step_ref_t, step_l, kn, steps, QuadCFKick{}, 8);
+            else
+                yoshida6(p0, xp, p2, yp, cdt, dpop, ref_p, ref_m, step_ref_t, step_l, kn, steps, QuadKick{}, 1);
+            x = p0 + xoff;
+            y = p2 + yoff;
+        };
         if (b.n_valid) {
+            count_particle(FC_QUAD, b, body);
 #pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < b.n_active; ++i)
-                if (b.masks[i]) {
-                    double p0 = b.P(i, 0) - xoff, p2 = b.P(i, 2) - yoff;
-                    double p1 = b.P(i, 1), p3 = b.P(i, 3), p4 = b.P(i, 4), p5 = b.P(i, 5);
-                    if (has_mp)
-                        yoshida6(p0, p1, p2, p3, p4, p5, ref_p, ref_m, step_ref_t, step_l, kn, steps, quad_cf_kick, 8);
-                    else
-                        yoshida6(p0, p1, p2, p3, p4, p5, ref_p, ref_m, step_ref_t, step_l, kn, steps, quad_kick, 1);
-                    b.P(i, 0) = p0 + xoff;
-                    b.P(i, 1) = p1;
-                    b.P(i, 2) = p2 + yoff;
-                    b.P(i, 3) = p3;
-                    b.P(i, 4) = p4;
-                }
+                if (b.masks[i]) body(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), b.P(i, 4), b.P(i, 5));
         }
         b.ref.s_n += length;
     }
@@ -854,22 +982,22 @@ static void sbend_apply(const Slice& slice, Bunch& b)
     const std::complex<double> term = std::complex<double>(0.0, sp.length / sp.angle) *
                                       std::complex<double>(1.0 - std::cos(sp.angle), -std::sin(sp.angle)) *
                                       std::complex<double>(std::cos(sp.e2), -std::sin(sp.e2));
-    if (b.n_valid) {
-#pragma omp parallel for schedule(static)
-        for (int64_t i = 0; i < b.n_active; ++i) {
-            if (!b.masks[i]) continue;
-            double p0 = b.P(i, 0), p1 = b.P(i, 1), p2 = b.P(i, 2), p3 = b.P(i, 3), p4 = b.P(i, 4), p5 = b.P(i, 5);
-            if (sp.ledge) {
-                slot_unit(p0, p1, p2, p3, p4, p5, sp.ce1, sp.se1, sp.pref_b, sp.m_b);
-                edge_unit(p2, p1, p3, sp.us_edge_k_x, sp.us_edge_k_y);
-            }
-            bend_unit(p0, p1, p2, p3, p4, p5, dphi, sp.strength, sp.pref_b, sp.m_b, sp.ref_cdt, phase, term);
-            if (sp.redge) {
-                edge_unit(p2, p1, p3, sp.ds_edge_k_x, sp.ds_edge_k_y);
-                slot_unit(p0, p1, p2, p3, p4, p5, sp.ce2, sp.se2, sp.pref_b, sp.m_b);
-            }
-            b.P(i, 0) = p0; b.P(i, 1) = p1; b.P(i, 2) = p2; b.P(i, 3) = p3; b.P(i, 4) = p4; b.P(i, 5) = p5;
+    auto body = [&](auto& p0, auto& p1, auto& p2, auto& p3, auto& p4, auto& p5) {
+        if (sp.ledge) {
+            slot_unit(p0, p1, p2, p3, p4, p5, sp.ce1, sp.se1, sp.pref_b, sp.m_b);
+            edge_unit(p2, p1, p3, sp.us_edge_k_x, sp.us_edge_k_y);
         }
+        bend_unit(p0, p1, p2, p3, p4, p5, dphi, sp.strength, sp.pref_b, sp.m_b, sp.ref_cdt, phase, term);
+        if (sp.redge) {
+            edge_unit(p2, p1, p3, sp.ds_edge_k_x, sp.ds_edge_k_y);
+            slot_unit(p0, p1, p2, p3, p4, p5, sp.ce2, sp.se2, sp.pref_b, sp.m_b);
+        }
+    };
+    if (b.n_valid) {
+        count_particle(FC_SBEND, b, body);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < b.n_active; ++i)
+            if (b.masks[i]) body(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), b.P(i, 4), b.P(i, 5));
     }
     b.ref.s_n += sp.length;
 }
@@ -878,6 +1006,8 @@ static void sbend_apply(const Slice& slice, Bunch& b)
 // design particle, then PropSbendCF ff_sbend.h:221-339 on every particle.
 static void sbend_cf_apply(SbendParams& sp, Bunch& b)
 {
+    if (g_flops.on) g_flops.uncounted = true; // no instrumented particle loop
+
     const double c[4] = {0.79361246386112147294625603763, -0.206276584816439780698721319354,
                          -0.118008867881292655922412133144, 0.236949573653050744373598734219};
     Refpart& ref_l = b.design;
@@ -1008,20 +1138,19 @@ static void multipole_apply(const Slice& slice, Bunch& b)
     for (int n = 0; n < max_order; ++n)
         if (kn_on[n]) thin_magnet_unit(x, xp, y, yp, &kl[n * 2], n + 1);
     ref_l.state = {x, xp, y, yp, 0.0, dpop};
+    auto body = [&](auto& p0, auto& p1, auto& p2, auto& p3, auto&, auto&) {
+        if (kn_on[0]) thin_dipole_unit(p0, p1, p2, p3, &kl[0]);
+        if (kn_on[1]) thin_quadrupole_unit(p0, p1, p2, p3, &kl[2]);
+        if (kn_on[2]) thin_sextupole_unit(p0, p1, p2, p3, &kl[4]);
+        if (kn_on[3]) thin_octupole_unit(p0, p1, p2, p3, &kl[6]);
+        for (int n = 4; n < max_order; ++n)
+            if (kn_on[n]) thin_magnet_unit(p0, p1, p2, p3, &kl[n * 2], n + 1);
+    };
     if (b.n_valid) {
+        count_particle(FC_THIN, b, body);
 #pragma omp parallel for schedule(static)
-        for (int64_t i = 0; i < b.n_active; ++i) {
-            if (!b.masks[i]) continue;
-            double p0 = b.P(i, 0), p1 = b.P(i, 1), p2 = b.P(i, 2), p3 = b.P(i, 3);
-            if (kn_on[0]) thin_dipole_unit(p0, p1, p2, p3, &kl[0]);
-            if (kn_on[1]) thin_quadrupole_unit(p0, p1, p2, p3, &kl[2]);
-            if (kn_on[2]) thin_sextupole_unit(p0, p1, p2, p3, &kl[4]);
-            if (kn_on[3]) thin_octupole_unit(p0, p1, p2, p3, &kl[6]);
-            for (int n = 4; n < max_order; ++n)
-                if (kn_on[n]) thin_magnet_unit(p0, p1, p2, p3, &kl[n * 2], n + 1);
-            b.P(i, 1) = p1;
-            b.P(i, 3) = p3;
-        }
+        for (int64_t i = 0; i < b.n_active; ++i)
+            if (b.masks[i]) body(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), b.P(i, 4), b.P(i, 5));
     }
 }
 
@@ -1052,10 +1181,12 @@ static void sextupole_apply(const Slice& slice, Bunch& b)
         ref_l.state[1] = xp;
         ref_l.state[3] = yp;
         ref_l.state[4] = 0.0;
+        auto body = [&](auto& x, auto& xp, auto& y, auto& yp, auto&, auto&) { thin_sextupole_unit(x, xp, y, yp, k); };
         if (b.n_valid) {
+            count_particle(FC_THIN, b, body);
 #pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < b.n_active; ++i)
-                if (b.masks[i]) thin_sextupole_unit(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), k);
+                if (b.masks[i]) body(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), b.P(i, 4), b.P(i, 5));
         }
     } else {
         double pref = b.ref.p, mass = b.ref.mass;
@@ -1073,14 +1204,14 @@ static void sextupole_apply(const Slice& slice, Bunch& b)
         // apply_yoshida_kick ff_patterned_propagator.h:199-225
         double step_ref_cdt = ref_cdt / steps;
         double ss[2] = {k[0] * step_len, k[1] * step_len};
+        auto body = [&](auto& p0, auto& p1, auto& p2, auto& p3, auto& p4, auto& p5) {
+            yoshida6(p0, p1, p2, p3, p4, p5, pref, mass, step_ref_cdt, step_len, ss, steps, SextKick{}, 1);
+        };
         if (b.n_valid) {
+            count_particle(FC_THICK_OTHER, b, body);
 #pragma omp parallel for schedule(static)
-            for (int64_t i = 0; i < b.n_active; ++i) {
-                if (!b.masks[i]) continue;
-                double p0 = b.P(i, 0), p1 = b.P(i, 1), p2 = b.P(i, 2), p3 = b.P(i, 3), p4 = b.P(i, 4), p5 = b.P(i, 5);
-                yoshida6(p0, p1, p2, p3, p4, p5, pref, mass, step_ref_cdt, step_len, ss, steps, sext_kick, 1);
-                b.P(i, 0) = p0; b.P(i, 1) = p1; b.P(i, 2) = p2; b.P(i, 3) = p3; b.P(i, 4) = p4;
-            }
+            for (int64_t i = 0; i < b.n_active; ++i)
+                if (b.masks[i]) body(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), b.P(i, 4), b.P(i, 5));
         }
         b.ref.s_n += length;
     }
@@ -1527,6 +1658,10 @@ static void rfcavity_apply(const Slice& slice, Bunch& b)
 static void element_apply(const Slice& slice, Bunch& b)
 { // ff_element.h:25-67
     const std::string& t = slice.e->type;
+    if (g_flops.on && !(t == "drift" || t == "monitor" || t == "hmonitor" || t == "vmonitor" || t == "marker" ||
+                        t == "instrument" || t == "rcollimator" || t == "sbend" || t == "quadrupole" ||
+                        t == "multipole" || t == "sextupole"))
+        g_flops.uncounted = true; // no instrumented particle loop for this kind
     if (t == "drift" || t == "monitor" || t == "hmonitor" || t == "vmonitor" || t == "marker" ||
         t == "instrument" || t == "rcollimator")
         drift_apply(slice, b);
@@ -1602,41 +1737,43 @@ static Aperture make_aperture(const std::string& type, const Slice& slice)
 
 static int aperture_apply(const Aperture& ap, Bunch& b)
 {
+    auto decide = [&](auto& x, auto& xp, auto& y, auto& yp, auto& cdt, auto& dpop) -> bool {
+        bool discard = false;
+        switch (ap.kind) {
+        case AP_FINITE: {
+            if (!isfinite(x) || !isfinite(xp) || !isfinite(y) || !isfinite(yp) || !isfinite(cdt) || !isfinite(dpop))
+                discard = true;
+            else {
+                auto pt = 1.0 + dpop;
+                discard = pt * pt - xp * xp - yp * yp < 0.0;
+            }
+            break;
+        }
+        case AP_CIRCULAR: {
+            auto xr = x - ap.xoff, yr = y - ap.yoff;
+            discard = (xr * xr + yr * yr) > ap.r2;
+            break;
+        }
+        case AP_ELLIPTICAL: {
+            auto xr = x - ap.xoff, yr = y - ap.yoff;
+            discard = (xr * xr / ap.h2 + yr * yr / ap.v2) > 1.0;
+            break;
+        }
+        case AP_RECTANGULAR: {
+            auto xr = x - ap.xoff, yr = y - ap.yoff;
+            discard = (fabs(xr) > 0.5 * ap.width) || (fabs(yr) > 0.5 * ap.height);
+            break;
+        }
+        }
+        return discard;
+    };
+    count_particle(FC_APERTURE, b, decide);
     int nd = 0;
 #pragma omp parallel for reduction(+ : nd) schedule(static)
     for (int64_t i = 0; i < b.n_active; ++i) {
         b.discards[i] = 0;
         if (!b.masks[i]) continue;
-        bool discard = false;
-        switch (ap.kind) {
-        case AP_FINITE: {
-            bool fin = true;
-            for (int j = 0; j < 6; ++j)
-                if (!std::isfinite(b.P(i, j))) fin = false;
-            if (!fin)
-                discard = true;
-            else {
-                double pt = 1.0 + b.P(i, 5), px = b.P(i, 1), py = b.P(i, 3);
-                discard = pt * pt - px * px - py * py < 0.0;
-            }
-            break;
-        }
-        case AP_CIRCULAR: {
-            double xr = b.P(i, 0) - ap.xoff, yr = b.P(i, 2) - ap.yoff;
-            discard = (xr * xr + yr * yr) > ap.r2;
-            break;
-        }
-        case AP_ELLIPTICAL: {
-            double xr = b.P(i, 0) - ap.xoff, yr = b.P(i, 2) - ap.yoff;
-            discard = (xr * xr / ap.h2 + yr * yr / ap.v2) > 1.0;
-            break;
-        }
-        case AP_RECTANGULAR: {
-            double xr = b.P(i, 0) - ap.xoff, yr = b.P(i, 2) - ap.yoff;
-            discard = (std::fabs(xr) > 0.5 * ap.width) || (std::fabs(yr) > 0.5 * ap.height);
-            break;
-        }
-        }
+        const bool discard = decide(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), b.P(i, 4), b.P(i, 5));
         if (discard) {
             b.discards[i] = 1;
             b.masks[i] = 0;
@@ -1753,10 +1890,11 @@ static double smallest_non_tiny(double val, double o1, double o2, double tiny)
 }
 
 // collective/utils.h:9-18
-inline void leftmost_index_offset(double pos, double left, double inv_cell, int& idx, double& off)
+template <class R>
+inline void leftmost_index_offset(R pos, double left, double inv_cell, int& idx, R& off)
 {
-    double s = (pos - left) * inv_cell - 0.5;
-    idx = (int)std::floor(s);
+    R s = (pos - left) * inv_cell - 0.5;
+    idx = (int)std::floor(val(s));
     off = s - idx;
 }
 
@@ -1785,13 +1923,17 @@ struct SC3D {
     void update_domain(Bunch& b)
     { // :494-540 with core_diagnostics.cc:422-460
         if (o.domain_fixed) return;
+        auto acc = [](auto* s, auto x, auto y, auto z) {
+            s[0] += x; s[1] += y; s[2] += z;
+            s[3] += x * x; s[4] += y * y; s[5] += z * z;
+        };
+        count_particle(FC_DOMAIN, b, [&](auto& x, auto&, auto& y, auto&, auto& z, auto&) {
+            CD cs[6];
+            acc(cs, x, y, z);
+        });
         double s[6] = {0, 0, 0, 0, 0, 0};
         for (int64_t i = 0; i < b.n_active; ++i)
-            if (b.masks[i]) {
-                double x = b.P(i, 0), y = b.P(i, 2), z = b.P(i, 4);
-                s[0] += x; s[1] += y; s[2] += z;
-                s[3] += x * x; s[4] += y * y; s[5] += z * z;
-            }
+            if (b.masks[i]) acc(s, b.P(i, 0), b.P(i, 2), b.P(i, 4));
         double ms[6];
         for (int j = 0; j < 3; ++j) {
             ms[j] = s[j] / b.n_total;
@@ -1832,6 +1974,28 @@ struct SC3D {
         auto ingrid = [&](int ix, int iy, int iz) {
             return ix > 0 && ix < gx - 1 && iy > 0 && iy < gy - 1 && iz > 0 && iz < gz - 1;
         };
+        // one particle's CIC weights, add(cell, w) for each interior corner
+        auto dep = [&](auto px, auto py, auto pz, auto&& add) {
+            int ix, iy, iz;
+            decltype(px) ox, oy, oz;
+            leftmost_index_offset(px, lx, ihx, ix, ox);
+            leftmost_index_offset(py, ly, ihy, iy, oy);
+            leftmost_index_offset(pz, lz, ihz, iz, oz);
+            int64_t base = (int64_t)iz * gx * gy;
+            if (ingrid(ix, iy, iz)) add(base + iy * gx + ix, w0 * (1 - ox) * (1 - oy) * (1 - oz));
+            if (ingrid(ix + 1, iy, iz)) add(base + iy * gx + ix + 1, w0 * (ox) * (1 - oy) * (1 - oz));
+            if (ingrid(ix, iy + 1, iz)) add(base + (iy + 1) * gx + ix, w0 * (1 - ox) * (oy) * (1 - oz));
+            if (ingrid(ix + 1, iy + 1, iz)) add(base + (iy + 1) * gx + ix + 1, w0 * (ox) * (oy) * (1 - oz));
+            base = (int64_t)(iz + 1) * gx * gy;
+            if (ingrid(ix, iy, iz + 1)) add(base + iy * gx + ix, w0 * (1 - ox) * (1 - oy) * (oz));
+            if (ingrid(ix + 1, iy, iz + 1)) add(base + iy * gx + ix + 1, w0 * (ox) * (1 - oy) * (oz));
+            if (ingrid(ix, iy + 1, iz + 1)) add(base + (iy + 1) * gx + ix, w0 * (1 - ox) * (oy) * (oz));
+            if (ingrid(ix + 1, iy + 1, iz + 1)) add(base + (iy + 1) * gx + ix + 1, w0 * (ox) * (oy) * (oz));
+        };
+        count_particle(FC_DEPOSIT, b, [&](auto& x, auto&, auto& y, auto&, auto& z, auto&) {
+            CD sink; // the grid accumulation: one add per deposited corner
+            dep(x, y, z, [&](int64_t, CD w) { sink += w; });
+        });
 #pragma omp parallel num_threads(nt)
         {
             int it = 0, ntt = 1;
@@ -1844,21 +2008,7 @@ struct SC3D {
             double* r = rl.data() + (size_t)it * nc;
             for (int64_t n = ps; n < pe; ++n) {
                 if (!b.masks[n]) continue;
-                int ix, iy, iz;
-                double ox, oy, oz;
-                leftmost_index_offset(b.P(n, 0), lx, ihx, ix, ox);
-                leftmost_index_offset(b.P(n, 2), ly, ihy, iy, oy);
-                leftmost_index_offset(b.P(n, 4), lz, ihz, iz, oz);
-                int64_t base = (int64_t)iz * gx * gy;
-                if (ingrid(ix, iy, iz)) r[base + iy * gx + ix] += w0 * (1 - ox) * (1 - oy) * (1 - oz);
-                if (ingrid(ix + 1, iy, iz)) r[base + iy * gx + ix + 1] += w0 * (ox) * (1 - oy) * (1 - oz);
-                if (ingrid(ix, iy + 1, iz)) r[base + (iy + 1) * gx + ix] += w0 * (1 - ox) * (oy) * (1 - oz);
-                if (ingrid(ix + 1, iy + 1, iz)) r[base + (iy + 1) * gx + ix + 1] += w0 * (ox) * (oy) * (1 - oz);
-                base = (int64_t)(iz + 1) * gx * gy;
-                if (ingrid(ix, iy, iz + 1)) r[base + iy * gx + ix] += w0 * (1 - ox) * (1 - oy) * (oz);
-                if (ingrid(ix + 1, iy, iz + 1)) r[base + iy * gx + ix + 1] += w0 * (ox) * (1 - oy) * (oz);
-                if (ingrid(ix, iy + 1, iz + 1)) r[base + (iy + 1) * gx + ix] += w0 * (1 - ox) * (oy) * (oz);
-                if (ingrid(ix + 1, iy + 1, iz + 1)) r[base + (iy + 1) * gx + ix + 1] += w0 * (ox) * (oy) * (oz);
+                dep(b.P(n, 0), b.P(n, 2), b.P(n, 4), [&](int64_t c, double w) { r[c] += w; });
             }
         }
 #pragma omp parallel for schedule(static)
@@ -2013,40 +2163,43 @@ struct SC3D {
         const int gx = dom.g[0], gy = dom.g[1], gz = dom.g[2];
         double ihx = 1.0 / dom.h[0], ihy = 1.0 / dom.h[1], ihz = 1.0 / dom.h[2];
         double lx = dom.left[0], ly = dom.left[1], lz = dom.left[2];
-#pragma omp parallel for schedule(static)
-        for (int64_t i = 0; i < b.n_active; ++i) {
-            if (!b.masks[i]) continue;
+        auto body = [&](auto& x, auto& xp, auto& y, auto& yp, auto& cdt, auto& dpop) {
+            typedef std::remove_reference_t<decltype(x)> R;
             int ix, iy, iz;
-            double ox, oy, oz;
-            leftmost_index_offset(b.P(i, 0), lx, ihx, ix, ox);
-            leftmost_index_offset(b.P(i, 2), ly, ihy, iy, oy);
-            leftmost_index_offset(b.P(i, 4), lz, ihz, iz, oz);
-            double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
-            if (!((ix >= 0 && ix < gx - 1) && (iy >= 0 && iy < gy - 1) && (iz >= 0 && iz < gz - 1))) continue;
+            R ox, oy, oz;
+            leftmost_index_offset(x, lx, ihx, ix, ox);
+            leftmost_index_offset(y, ly, ihy, iy, oy);
+            leftmost_index_offset(cdt, lz, ihz, iz, oz);
+            R aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
+            if (!((ix >= 0 && ix < gx - 1) && (iy >= 0 && iy < gy - 1) && (iz >= 0 && iz < gz - 1))) return;
             auto interp = [&](const std::vector<double>& e) {
                 int64_t base = ((int64_t)iz * gy + iy) * gx + ix;
-                double val = aoz * aoy * aox * e[base];
-                val += aoz * aoy * ox * e[base + 1];
-                val += aoz * oy * aox * e[base + gx];
-                val += aoz * oy * ox * e[base + gx + 1];
+                R a = aoz * aoy * aox * e[base];
+                a += aoz * aoy * ox * e[base + 1];
+                a += aoz * oy * aox * e[base + gx];
+                a += aoz * oy * ox * e[base + gx + 1];
                 base = ((int64_t)(iz + 1) * gy + iy) * gx + ix;
-                val += oz * aoy * aox * e[base];
-                val += oz * aoy * ox * e[base + 1];
-                val += oz * oy * aox * e[base + gx];
-                val += oz * oy * ox * e[base + gx + 1];
-                return val;
+                a += oz * aoy * aox * e[base];
+                a += oz * aoy * ox * e[base + 1];
+                a += oz * oy * aox * e[base + gx];
+                a += oz * oy * ox * e[base + gx + 1];
+                return a;
             };
-            double val = interp(enz);
-            double p = pref + b.P(i, 5) * pref;
-            double Eoc_i = std::sqrt(p * p + m * m);
-            double Eoc_f = Eoc_i + factor * (-pref) * val;
-            double dpop = (std::sqrt(Eoc_f * Eoc_f - m * m) - std::sqrt(Eoc_i * Eoc_i - m * m)) / pref;
-            b.P(i, 5) += dpop;
-            val = interp(eny);
-            b.P(i, 3) += factor * val;
-            val = interp(enx);
-            b.P(i, 1) += factor * val;
-        }
+            R v = interp(enz);
+            R p = pref + dpop * pref;
+            R Eoc_i = sqrt(p * p + m * m);
+            R Eoc_f = Eoc_i + factor * (-pref) * v;
+            R ddp = (sqrt(Eoc_f * Eoc_f - m * m) - sqrt(Eoc_i * Eoc_i - m * m)) / pref;
+            dpop += ddp;
+            v = interp(eny);
+            yp += factor * v;
+            v = interp(enx);
+            xp += factor * v;
+        };
+        count_particle(FC_KICK, b, body);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < b.n_active; ++i)
+            if (b.masks[i]) body(b.P(i, 0), b.P(i, 1), b.P(i, 2), b.P(i, 3), b.P(i, 4), b.P(i, 5));
     }
 
     void apply(Bunch& b, double time_step)
@@ -2432,9 +2585,37 @@ int orc_sim_propagate_steps(void* sp, int first, int count)
                 st.indeps[ii++].apply(s->b, s->losses);
             else if (s->sc)
                 s->sc->apply(s->b, time);
+            g_flops.mark(k, kk);
         }
     }
     ORC_CATCH
+}
+
+// Operation counting (see FlopState): counts the algorithmic FP64 work of
+// particle `index` through the oracle's own particle code while the Sim
+// runs as usual; one record per operator of each step run.
+int orc_flops_begin(int64_t index)
+{
+    g_flops = FlopState();
+    g_flops.on = true;
+    g_flops.index = index;
+    return 0;
+}
+int orc_flops_end(int* uncounted)
+{
+    g_flops.on = false;
+    *uncounted = g_flops.uncounted ? 1 : 0;
+    return (int)g_flops.records.size();
+}
+// record r: its step and operator kind ('I' or 'C'), counts[FC_N][FO_N]
+int orc_flops_record(int r, int* step, int* kind, int64_t* counts)
+{
+    if (r < 0 || r >= (int)g_flops.records.size()) return 1;
+    const auto& rec = g_flops.records[r];
+    *step = rec.step;
+    *kind = rec.kind;
+    std::memcpy(counts, rec.n, sizeof(rec.n));
+    return 0;
 }
 
 // Last space-charge solve of a Sim: domain (left[3], h[3]), rho, phi and E on

@@ -63,6 +63,7 @@ SIGNATURES = {
     "sb2_set_device": (_i32, [_i32]),
     "sb2_profile_enable": (_i32, [_i32]),
     "sb2_profile_read": (_i32, [_i32, _c.POINTER(_cp), _pd, _pi64, _i32]),
+    "sb2_fp64_peak_probe": (_i32, [_pd, _vp]),
     "sb2_sc3d_options_init": (_i32, [_popts, _c.c_int, _c.c_int, _c.c_int]),
     "sb2_sc3d_options_set_fixed_domain": (_i32, [_popts, _pd, _pd]),
     "sb2_bunch_create": (_i32, [_i32, _d, _d, _i32, _i64, _d, _ppv]),

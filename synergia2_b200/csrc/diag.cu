@@ -192,6 +192,32 @@ cudaError_t launch_count_valid(const uint8_t* masks, int64_t n, BunchCounters* c
     return cudaGetLastError();
 }
 
+// FP64 issue-rate probe: eight independent fused multiply-add chains per
+// thread, so the FP64 pipe, not latency, bounds the kernel.  The values
+// stay finite (|a| < 1) and the sums are stored so no chain is dropped.
+__global__ void __launch_bounds__(256) fp64_fma_probe_kernel(double* out, int iters, double a, double b)
+{
+    double r0 = threadIdx.x * 1e-6, r1 = r0 + 0.125, r2 = r0 + 0.25, r3 = r0 + 0.375;
+    double r4 = r0 + 0.5, r5 = r0 + 0.625, r6 = r0 + 0.75, r7 = r0 + 0.875;
+    for (int i = 0; i < iters; ++i) {
+        r0 = __fma_rn(r0, a, b);
+        r1 = __fma_rn(r1, a, b);
+        r2 = __fma_rn(r2, a, b);
+        r3 = __fma_rn(r3, a, b);
+        r4 = __fma_rn(r4, a, b);
+        r5 = __fma_rn(r5, a, b);
+        r6 = __fma_rn(r6, a, b);
+        r7 = __fma_rn(r7, a, b);
+    }
+    out[blockIdx.x * (int64_t)blockDim.x + threadIdx.x] = ((r0 + r1) + (r2 + r3)) + ((r4 + r5) + (r6 + r7));
+}
+
+cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s)
+{
+    fp64_fma_probe_kernel<<<blocks, 256, 0, s>>>(out, iters, 0.9999999, 1e-7);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_diagnostics(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
                                const BunchCounters* counters, double* partials, int nb, double* tmp, double* records,
                                int32_t* count, int capacity, cudaStream_t s)

@@ -3073,6 +3073,45 @@ sb2_status sb2_profile_read(int32_t category, const char** name, double* total_m
     SB2_CATCH
 }
 
+sb2_status sb2_fp64_peak_probe(double* tflops, void* stream)
+{
+    SB2_TRY
+    SB2_REQUIRE(tflops, "null output");
+    cudaStream_t s = (cudaStream_t)stream;
+    int dev = 0, sms = 0;
+    cuda_check(cudaGetDevice(&dev), "device");
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    const int blocks = sms * 8, iters = 4096;
+    double* out = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    auto release = [&]() {
+        if (out) cudaFree(out);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    };
+    try {
+        cuda_check(cudaMalloc(&out, sizeof(double) * blocks * 256), "probe buffer");
+        cuda_check(cudaEventCreate(&e0), "event");
+        cuda_check(cudaEventCreate(&e1), "event");
+        float best = 0.0f;
+        for (int rep = 0; rep < 8; ++rep) {
+            cuda_check(cudaEventRecord(e0, s), "event");
+            cuda_check(launch_fp64_probe(out, blocks, iters, s), "fp64 probe");
+            cuda_check(cudaEventRecord(e1, s), "event");
+            cuda_check(cudaEventSynchronize(e1), "event");
+            float ms = 0.0f;
+            cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event");
+            if (rep >= 2 && (best == 0.0f || ms < best)) best = ms; // two warm-up launches
+        }
+        *tflops = 2.0 * 8.0 * iters * (double)blocks * 256.0 / (best * 1e-3) / 1e12;
+    } catch (...) {
+        release();
+        throw;
+    }
+    release();
+    SB2_CATCH
+}
+
 sb2_status sb2_sc3d_options_init(sb2_sc3d_options* o, int gx, int gy, int gz)
 {
     SB2_TRY

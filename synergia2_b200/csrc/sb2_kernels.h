@@ -133,6 +133,9 @@ cudaError_t launch_sort_scatter_out(const SortBuffers& sb, double* ups, int64_t 
 // diag.cu: per-turn bunch diagnostics appended to a device record array
 constexpr int kDiagRecord = 97;
 cudaError_t launch_count_valid(const uint8_t* masks, int64_t n, BunchCounters* c, cudaStream_t s);
+// blocks x 256 threads, each 8 x iters dependent-free FP64 FMAs; out holds
+// blocks x 256 doubles
+cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s);
 cudaError_t launch_diagnostics(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
                                const BunchCounters* counters, double* partials, int nb, double* tmp, double* records,
                                int32_t* count, int capacity, cudaStream_t s);

@@ -164,3 +164,12 @@ def test_gpu_step_counts_with_space_charge_and_graph_refusal(syn):
     prop.set_graphs(True)
     with pytest.raises(syn.SB2Error, match="graph"):
         prop.set_step_counts(4)
+
+
+def test_gpu_fp64_peak_probe(syn):
+    """The FP64 FMA probe behind the particle passes' FP64 roofline returns
+    a plausible rate for a B200 (tens of TFLOP/s)."""
+    import ctypes
+    v = ctypes.c_double()
+    syn.check(syn.lib().sb2_fp64_peak_probe(ctypes.byref(v), None))
+    assert 5.0 < v.value < 200.0, v.value
