@@ -387,8 +387,12 @@ __device__ __forceinline__ void yoshida6_op(double& x, double& xp, double& y, do
         else if (KIND == OP_KICK_YOSHIDA) {
             xp = xp + kk[0]; // thin_kicker_unit ff_algorithm.h:994-1000
             yp = yp + kk[1];
-        } else
-            quad_cf_kick(x, xp, y, yp, kk);
+        } else {
+            double cxp = xp, cyp = yp; // copies: see on_copies
+            quad_cf_kick(x, cxp, y, cyp, kk);
+            xp = cxp;
+            yp = cyp;
+        }
     };
     const double* k1 = k;
     const double* k2 = k + KS;
@@ -458,6 +462,25 @@ struct TrackOcc {
     static constexpr int value =
         V == TRACK_LIGHT ? 3 : (V == TRACK_FULL ? 3 : (V == TRACK_QUAD ? (PPT == 1 ? SB2_QUAD_OCC : 2) : 2));
 };
+
+// Runs an out-of-line op on copies of the six coordinates.  A coordinate
+// whose address reaches a call that is not inlined is given a stack slot for
+// the whole pass, and every op then reloads it from local memory (through
+// L1); on copies only the copies live in the stack frame, and only while
+// the op runs.
+template <class F>
+__device__ __forceinline__ void on_copies(double& x, double& xp, double& y, double& yp, double& cdt, double& dpop,
+                                          F&& f)
+{
+    double c0 = x, c1 = xp, c2 = y, c3 = yp, c4 = cdt, c5 = dpop;
+    f(c0, c1, c2, c3, c4, c5);
+    x = c0;
+    xp = c1;
+    y = c2;
+    yp = c3;
+    cdt = c4;
+    dpop = c5;
+}
 
 // One particle in registers during a pass.
 struct Part {
@@ -679,13 +702,19 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
             if constexpr (kFull) yoshida6_op<OP_KICK_YOSHIDA>(x, xp, y, yp, cdt, dpop, op);
             break;
         case OP_MATRIX:
-            matrix_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
+            on_copies(x, xp, y, yp, cdt, dpop, [&](double& a, double& b, double& c, double& d, double& e, double& f) {
+                matrix_op(a, b, c, d, e, f, op.d, op.flags);
+            });
             break;
         case OP_DIPEDGE:
-            dipedge_op(x, xp, y, yp, op.d);
+            on_copies(x, xp, y, yp, cdt, dpop, [&](double& a, double& b, double& c, double& d, double&, double&) {
+                dipedge_op(a, b, c, d, op.d);
+            });
             break;
         case OP_THIN_NLLENS:
-            nllens_op(x, xp, y, yp, op.d);
+            on_copies(x, xp, y, yp, cdt, dpop, [&](double& a, double& b, double& c, double& d, double&, double&) {
+                nllens_op(a, b, c, d, op.d);
+            });
             break;
         case OP_THIN_KICK:
             xp = xp + op.d[2];
@@ -717,22 +746,37 @@ __device__ __forceinline__ void apply_op(const TrackParams& p, const MapOp& op, 
             if (on & 4) thin_sextupole_unit(x, xp, y, yp, kl[4], kl[5]);
             if (on & 8) thin_octupole_unit(x, xp, y, yp, kl[6], kl[7]);
             for (int nn = 4; nn < 8; ++nn)
-                if (on & (1 << nn)) thin_magnet_unit(x, xp, y, yp, kl[nn * 2], kl[nn * 2 + 1], nn + 1);
+                if (on & (1 << nn))
+                    on_copies(x, xp, y, yp, cdt, dpop, [&](double& a, double& b, double& c, double& d, double&, double&) {
+                        thin_magnet_unit(a, b, c, d, kl[nn * 2], kl[nn * 2 + 1], nn + 1);
+                    });
             break;
         }
         case OP_SBEND: {
-            if constexpr (kQuad) sbend_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
+            if constexpr (kQuad)
+                on_copies(x, xp, y, yp, cdt, dpop, [&](double& a, double& b, double& c, double& d, double& e, double& f) {
+                    sbend_op(a, b, c, d, e, f, op.d, op.flags);
+                });
             break;
         }
         case OP_SBEND_CF: {
-            if constexpr (kFull) sbend_cf_op(x, xp, y, yp, cdt, dpop, op.d, op.steps, op.flags);
+            if constexpr (kFull)
+                on_copies(x, xp, y, yp, cdt, dpop, [&](double& a, double& b, double& c, double& d, double& e, double& f) {
+                    sbend_cf_op(a, b, c, d, e, f, op.d, op.steps, op.flags);
+                });
             break;
         }
         case OP_SOLENOID:
-            if constexpr (kFull) solenoid_op(x, xp, y, yp, cdt, dpop, op.d, op.flags);
+            if constexpr (kFull)
+                on_copies(x, xp, y, yp, cdt, dpop, [&](double& a, double& b, double& c, double& d, double& e, double& f) {
+                    solenoid_op(a, b, c, d, e, f, op.d, op.flags);
+                });
             break;
         case OP_RFCAVITY:
-            if constexpr (kFull) rfcavity_op(x, xp, y, yp, cdt, dpop, op.d, op.steps, op.flags);
+            if constexpr (kFull)
+                on_copies(x, xp, y, yp, cdt, dpop, [&](double& a, double& b, double& c, double& d, double& e, double& f) {
+                    rfcavity_op(a, b, c, d, e, f, op.d, op.steps, op.flags);
+                });
             break;
         case OP_SC_KICK:
             if (p.efield32)
