@@ -294,7 +294,9 @@ sb2_status sb2_propagator_read_losses(sb2_propagator* p, int32_t max_records, in
 /* Launch shape of the particle passes and the re-sort interval of the
  * cell-ordered working copy: the search space of the project's autotuner.
  * light_shape: light passes with 1 particle per thread and the next tile
- * prefetched (1), 2 per thread with (2) or without (0) prefetch; full_occ:
+ * prefetched (1), 2 per thread with (2) or without (0) prefetch, 1 per
+ * thread with the next tile prefetched into shared memory by asynchronous
+ * copies (3); full_occ:
  * passes with Yoshida integrators or bends at 2 (128 registers) or 3
  * (80 registers) CTAs per SM; full_ppt: particles per thread of the 2-CTA
  * variant (1, 2); quad_variant: passes whose only integrator is the
@@ -302,7 +304,8 @@ sb2_status sb2_propagator_read_losses(sb2_propagator* p, int32_t max_records, in
  * two (2, at 2 CTAs per SM) particles per thread, or not (0);
  * ctas_per_sm: grid of the particle passes (1..12 x the SM count);
  * sort_interval: re-sort before every k-th space-charge kick.  The defaults
- * are the values measured best on the FODO workload of 4M macroparticles. */
+ * are the values measured best on the FODO workload of 4M macroparticles
+ * (light_shape 3). */
 typedef struct sb2_tune {
     int32_t light_shape, full_occ, full_ppt, quad_variant, ctas_per_sm, sort_interval;
 } sb2_tune;

@@ -2604,7 +2604,7 @@ struct Propagator {
                     best_si = si;
                 }
             };
-            for (int v : {1, 2, 0}) {
+            for (int v : {1, 3, 2, 0}) {
                 TrackTune c = best;
                 c.light_shape = v;
                 consider(c, best_si);
@@ -3733,7 +3733,7 @@ sb2_status sb2_propagator_set_loss_diagnostics(sb2_propagator* p, int32_t capaci
 
 static void check_tune(const sb2_tune& t)
 {
-    SB2_REQUIRE(t.light_shape >= 0 && t.light_shape <= 2, "tune: light_shape is 0, 1 or 2");
+    SB2_REQUIRE(t.light_shape >= 0 && t.light_shape <= 3, "tune: light_shape is 0, 1, 2 or 3");
     SB2_REQUIRE(t.full_occ == 2 || t.full_occ == 3, "tune: full_occ is 2 or 3");
     SB2_REQUIRE(t.full_ppt == 1 || t.full_ppt == 2, "tune: full_ppt is 1 or 2");
     SB2_REQUIRE(t.quad_variant >= 0 && t.quad_variant <= 2, "tune: quad_variant is 0, 1 or 2");

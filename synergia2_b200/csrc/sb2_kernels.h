@@ -83,7 +83,8 @@ struct SortBuffers {
 // (host.cc, Propagator::autotune).
 struct TrackTune {
     int32_t light_shape;  // light passes: 1 one particle per thread with the next tile prefetched,
-                          // 2 two per thread with prefetch, 0 two per thread without
+                          // 2 two per thread with prefetch, 0 two per thread without, 3 one per
+                          // thread with the next tile prefetched into shared memory (cp.async)
     int32_t full_occ;     // full passes: 2 (128 registers, TRACK_FULL_WIDE) or 3 CTAs/SM (80, TRACK_FULL)
     int32_t full_ppt;     // particles per thread of the 2-CTA full variant (1 or 2)
     int32_t quad_variant; // passes whose only integrator is the quadrupole run TRACK_QUAD with 1 (1) or

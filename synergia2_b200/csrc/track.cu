@@ -102,7 +102,7 @@ static int sm_count_cached()
 TrackTune track_tune_defaults()
 {
     TrackTune t;
-    t.light_shape = 1;
+    t.light_shape = 3;
     t.full_occ = 2;
     t.full_ppt = 1;
     t.quad_variant = 1;
@@ -110,6 +110,7 @@ TrackTune track_tune_defaults()
     const char* e = getenv("SB2_TRACK_LIGHT");
     if (e && e[0] == '2' && e[1] == 'p') t.light_shape = 2;
     if (e && e[0] == '2' && e[1] == 0) t.light_shape = 0;
+    if (e && e[0] == '1') t.light_shape = 1;
     e = getenv("SB2_TRACK_FULL_OCC");
     if (e && atoi(e) == 3) t.full_occ = 3;
     e = getenv("SB2_TRACK_FULL_PPT");

@@ -903,6 +903,101 @@ __global__ void __launch_bounds__(kTrackThreads, PF ? SB2_LIGHT_OCC : TrackOcc<V
     }
 }
 
+// Light pass with the next tile's coordinates prefetched into shared memory
+// by per-thread asynchronous copies (cp.async, 8 bytes each) instead of
+// registers: each thread copies only its own particle's six values and reads
+// back only its own slots, so no block barrier is needed; two buffers, the
+// copy of tile k+1 goes to the buffer whose values tile k-1 already consumed.
+// The mask byte is prefetched in a register.
+__device__ __forceinline__ void cp_async8(void* dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+
+template <int VARIANT>
+__global__ void __launch_bounds__(kTrackThreads, SB2_LIGHT_OCC) track_kernel_lds(const __grid_constant__ TrackParams p)
+{
+    __shared__ int s_counts[kMaxOpsPerPass];
+    __shared__ double s_mom[6][kTrackThreads]; // per-thread moment sums
+    __shared__ __align__(16) double s_pf[2][6][kTrackThreads];
+    for (int i = threadIdx.x; i < kMaxOpsPerPass; i += blockDim.x) s_counts[i] = 0;
+    for (int j = 0; j < 6; ++j) s_mom[j][threadIdx.x] = 0.0;
+    __syncthreads();
+    double* s_mom_col = &s_mom[0][threadIdx.x];
+
+    const int64_t n = p.n;
+    const int64_t S = p.stride;
+    const int64_t tile = kTrackThreads;
+    const int64_t gstride = (int64_t)gridDim.x * tile;
+    auto issue = [&](int buf, int64_t i) {
+        if (i < n)
+#pragma unroll
+            for (int j = 0; j < 6; ++j) cp_async8(&s_pf[buf][j][threadIdx.x], p.parts + i + j * S);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    int64_t base = blockIdx.x * tile;
+    uint8_t m_next = 0;
+    if (base < n) {
+        issue(0, base + threadIdx.x);
+        if (base + threadIdx.x < n) m_next = p.masks[base + threadIdx.x];
+    }
+    for (int it = 0; base < n; base += gstride, ++it) {
+        const int b = it & 1;
+        const int64_t i = base + threadIdx.x;
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        RawPart cur;
+        cur.m = m_next;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) cur.c[j] = i < n ? s_pf[b][j][threadIdx.x] : 0.0;
+        const int64_t nb = base + gstride;
+        if (nb < n) {
+            issue(b ^ 1, nb + threadIdx.x);
+            m_next = nb + threadIdx.x < n ? p.masks[nb + threadIdx.x] : 0;
+        }
+        Part P;
+        P.x = cur.c[0];
+        P.xp = cur.c[1];
+        P.y = cur.c[2];
+        P.yp = cur.c[3];
+        P.cdt = cur.c[4];
+        P.dpop = cur.c[5];
+        P.alive = cur.m != 0;
+        const bool in = P.alive;
+        P.disc = 0;
+        P.idx = i;
+        for (int o = 0; o < p.nops; ++o) apply_op<VARIANT>(p, p.ops[o], P, s_counts, s_mom_col);
+        if (i < n) {
+            if (in) {
+                p.parts[i] = P.x;
+                p.parts[i + S] = P.xp;
+                p.parts[i + 2 * S] = P.y;
+                p.parts[i + 3 * S] = P.yp;
+                p.parts[i + 4 * S] = P.cdt;
+                p.parts[i + 5 * S] = P.dpop;
+                if (!P.alive) p.masks[i] = 0;
+            }
+            if (p.write_discards && p.discards) p.discards[i] = (uint8_t)P.disc;
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+
+    __syncthreads();
+    for (int s = threadIdx.x; s < kMaxOpsPerPass; s += blockDim.x)
+        if (s_counts[s]) atomicAdd(&p.ap_counts[p.slot_base + s], s_counts[s]);
+    bool any_mom = false;
+    for (int o = 0; o < p.nops; ++o) any_mom |= (p.ops[o].kind == OP_MOMENTS);
+    if (any_mom && p.moment_partials) {
+        for (int w = kTrackThreads / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w)
+                for (int j = 0; j < 6; ++j) s_mom[j][threadIdx.x] += s_mom[j][threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x < 6) p.moment_partials[blockIdx.x * 6 + threadIdx.x] = s_mom[threadIdx.x][0];
+    }
+}
+
 // true when the pass needs no integrator beyond the pure-quadrupole Yoshida
 // and the pure-dipole sector bend (FODO and ring lattices)
 static bool track_quad_only(const MapOp* ops, int n)
@@ -933,7 +1028,9 @@ cudaError_t launch_pass(const TrackParams& p, const TrackTune& t, cudaStream_t s
 {
     const int nb = track_grid_blocks(t.ctas_per_sm);
     if (!track_needs_full(p.ops, p.nops)) {
-        if (t.light_shape == 1)
+        if (t.light_shape == 3)
+            track_kernel_lds<TRACK_LIGHT><<<nb, kTrackThreads, 0, s>>>(p);
+        else if (t.light_shape == 1)
             track_kernel<TRACK_LIGHT, 1, true><<<nb, kTrackThreads, 0, s>>>(p);
         else if (t.light_shape == 2)
             track_kernel<TRACK_LIGHT, 2, true><<<nb, kTrackThreads, 0, s>>>(p);

@@ -11,7 +11,8 @@ pytestmark = pytest.mark.gpu
 
 CONFIGS = [dict(light_shape=1, full_occ=2, full_ppt=1, quad_variant=1, ctas_per_sm=8),
            dict(light_shape=2, full_occ=2, full_ppt=2, quad_variant=0, ctas_per_sm=4),
-           dict(light_shape=0, full_occ=3, full_ppt=1, quad_variant=1, ctas_per_sm=12)]
+           dict(light_shape=0, full_occ=3, full_ppt=1, quad_variant=1, ctas_per_sm=12),
+           dict(light_shape=3, full_occ=2, full_ppt=1, quad_variant=1, ctas_per_sm=4)]
 
 
 def test_gpu_launch_shapes_give_identical_tracks(syn):
@@ -41,7 +42,7 @@ def test_gpu_launch_shapes_with_space_charge(syn):
     p = gaussian_bunch(n, SIG_C0, 52)
     lat, ref = product_lattice(fodo_cell())
     out = []
-    for cfg, si in zip(CONFIGS, (4, 2, 8)):
+    for cfg, si in zip(CONFIGS, (4, 2, 8, 1)):
         prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(16, 16, 32), 8))
         prop.set_tune(sort_interval=si, **cfg)
         b = syn.Bunch(ref, n, 1e11)
@@ -75,7 +76,7 @@ def test_gpu_autotune_leaves_state_and_applies_best(syn):
     nrec, ndiag = len(prop.step_counts()), len(prop.diagnostics()["s"])
     best, log = prop.autotune(b, steps=8)
     assert len(log) >= 10
-    assert {r["light_shape"] for r in log} == {0, 1, 2} and {r["ctas_per_sm"] for r in log} == {4, 8, 12}
+    assert {r["light_shape"] for r in log} == {0, 1, 2, 3} and {r["ctas_per_sm"] for r in log} == {4, 8, 12}
     assert {r["sort_interval"] for r in log} == {2, 4, 8}
     fastest = min(log, key=lambda r: r["ms"])
     assert best == {k: fastest[k] for k in best} == prop.get_tune()
