@@ -448,8 +448,8 @@ constexpr int kTrackThreads = 256;
 // faster on the FODO quadrupole passes than TRACK_FULL_WIDE at 2 CTAs/SM.
 enum TrackVariant { TRACK_LIGHT = 0, TRACK_FULL = 1, TRACK_FULL_WIDE = 2, TRACK_QUAD = 3 };
 
-// CTAs per SM of the prefetching light variants: 4 (64 registers, a few
-// spilled to L1) measured 2% faster than 3 (80 registers) on the C1 passes.
+// CTAs per SM of the prefetching light variants: on the C1 passes 4 (64
+// registers) measured 8% faster than 3 (80 registers); 5 was 35% slower.
 #ifndef SB2_LIGHT_OCC
 #define SB2_LIGHT_OCC 4
 #endif
