@@ -115,6 +115,35 @@ def fp64_roofline(syn, workload, n, light, full):
     return out
 
 
+def cpu_baseline_c3(steps=2):
+    """The oracle on all host cores for a bounded sample of the ring
+    workload: the same 2^24-macroparticle bunch and 128^2 x 256 grid, the
+    first `steps` split-operator steps of the turn; one turn (384 steps) and
+    100 turns are extrapolated from the per-step time."""
+    from helpers import MP, gaussian_bunch, oracle_lattice, ring_cell
+    from oracle import oracle as O
+    threads = O.set_threads(os.cpu_count() or 1)
+    spec = []
+    for c in range(24):
+        for e in ring_cell(radius=0.05):
+            e = dict(e)
+            e["name"] = "%s_%d" % (e["name"], c)
+            spec.append(e)
+    n = 1 << 24
+    p = gaussian_bunch(n, [2e-3, 1e-4, 2e-3, 1e-4, 0.3, 1e-4], 3)
+    sim = O.Sim(oracle_lattice(spec), n, REAL_NUM, stepper=O.STEPPER_SPLIT, num=16 * 24,
+                sc=O.SCOptions.make(128, 128, 256), value=2.5 + MP)
+    sim.set_particles(p)
+    del p
+    t0 = time.perf_counter()
+    sim.propagate_steps(0, steps)
+    dt = time.perf_counter() - t0
+    nv, _, _ = sim.counts()
+    return {"value": nv * steps / dt, "unit": "macroparticle-steps/s", "cores": threads, "kind": "port",
+            "sample": "%d macroparticles x %d steps (the first of the turn) of the same workload, %.1f s" % (n, steps, dt),
+            "one_turn_s_extrapolated": dt / steps * 384, "hundred_turns_h_extrapolated": dt / steps * 38400 / 3600}
+
+
 def ring_c3(syn, torch, turns=1, warmup_steps=16):
     """Config 3: the 24-cell ring (QF 0.5, SF thin, D 0.75, B 2.0, D 0.75,
     QD 0.5, SD thin, D 0.75, B 2.0, D 0.75 per cell; circular aperture 5 cm on
@@ -445,6 +474,8 @@ def main():
         if rank == 0:
             if args.config == "c3":
                 r = ring_c3(syn, torch)
+                if not args.no_cpu_baseline:
+                    r["cpu_baseline"] = cpu_baseline_c3()
                 wl = ("24-cell ring (QF, SF thin, B 2 m, QD, SD thin; circular aperture 5 cm), 2^24 macroparticles, "
                       "128^2x256 grid, 16 kicks per cell, one turn (384 steps) in FP64 and in mixed precision")
             elif args.config == "c2":
