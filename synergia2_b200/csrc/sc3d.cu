@@ -162,31 +162,9 @@ __device__ __forceinline__ void leftmost_d(double pos, double left, double inv, 
 }
 
 // Particles whose stencils start in the same cell are summed inside the
-// warp first: the warp's 32 (cell key, lane) pairs are put in key order by a
-// bitonic network over the lanes, each lane takes the particle of its sorted
-// position, and a segmented shuffle scan sums runs of equal keys, so every
-// distinct cell of the warp costs one set of 8 atomics -- also when the
-// cell-ordered working copy has aged and equal keys are no longer adjacent.
-__device__ __forceinline__ void warp_sort_by_key(int& key, int& src, int lane)
-{
-#pragma unroll
-    for (int k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            const int ok = __shfl_xor_sync(0xffffffffu, key, j);
-            const int os = __shfl_xor_sync(0xffffffffu, src, j);
-            const bool up = (lane & k) == 0;
-            const bool lower = (lane & j) == 0;
-            const bool other_less = ok < key || (ok == key && os < src);
-            // the lower lane of an ascending pair keeps the smaller element
-            if (lower == up ? other_less : !other_less) {
-                key = ok;
-                src = os;
-            }
-        }
-    }
-}
-
+// warp first (lanes grouped by cell key, in any order), so every distinct
+// cell of the warp costs one set of 8 atomics -- also when the cell-ordered
+// working copy has aged and equal keys are no longer adjacent.
 __global__ void __launch_bounds__(256) deposit_kernel(const double* __restrict__ parts, int64_t stride,
                                                       const uint8_t* __restrict__ masks, int64_t n,
                                                       const ScState* __restrict__ scp, double* rho,
@@ -212,18 +190,6 @@ __global__ void __launch_bounds__(256) deposit_kernel(const double* __restrict__
             if (ix >= -1 && ix < gx && iy >= -1 && iy < gy && iz >= -1 && iz < gz)
                 key = ((iz + 1) * (gy + 1) + (iy + 1)) * (gx + 1) + (ix + 1);
         }
-        // key order inside the warp (skipped when the warp is already ordered)
-        const int prev0 = __shfl_up_sync(full, key, 1);
-        if (!__all_sync(full, lane == 0 || prev0 <= key)) {
-            int src = lane;
-            warp_sort_by_key(key, src, lane);
-            ix = __shfl_sync(full, ix, src);
-            iy = __shfl_sync(full, iy, src);
-            iz = __shfl_sync(full, iz, src);
-            ox = __shfl_sync(full, ox, src);
-            oy = __shfl_sync(full, oy, src);
-            oz = __shfl_sync(full, oz, src);
-        }
         double w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         if (key >= 0) {
             double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
@@ -236,25 +202,30 @@ __global__ void __launch_bounds__(256) deposit_kernel(const double* __restrict__
             w[6] = w0 * aox * oy * oz;
             w[7] = w0 * ox * oy * oz;
         }
-        const int prev = __shfl_up_sync(full, key, 1);
-        const int next = __shfl_down_sync(full, key, 1);
-        const bool head = lane == 0 || prev != key;
-        const bool tail = lane == 31 || next != key;
-        const unsigned heads = __ballot_sync(full, head);
-        if (heads != full) { // some run longer than one particle
-            unsigned le;
-            asm("mov.u32 %0, %%lanemask_le;" : "=r"(le));
-            const int seg = 31 - __clz(heads & le);
+        // Lanes whose stencils start in the same cell (__match_any_sync,
+        // in any lane order) sum their 8 weights by a tree over their ranks
+        // among those peers: in each round a lane adds the partial sum of the
+        // next peer above it that is still live, and the peers whose rank
+        // has the round's bit set drop out.  The lowest peer ends up with the
+        // group's sums and issues its 8 atomics.
+        const unsigned peers = __match_any_sync(full, key);
+        unsigned below;
+        asm("mov.u32 %0, %%lanemask_lt;" : "=r"(below));
+        const bool leader = (peers & below) == 0;
+        unsigned rest = peers & ~below & ~(1u << lane); // peers above this lane
+        int rank = __popc(peers & below);
+        while (__any_sync(full, rest != 0)) {
+            const int nxt = __ffs(rest) - 1;
+            const int from = nxt < 0 ? lane : nxt;
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
-                double v = w[c];
-                for (int o = 1; o < 32; o <<= 1) {
-                    double u = __shfl_up_sync(full, v, o);
-                    if (lane - o >= seg) v += u;
-                }
-                w[c] = v;
+                const double t = __shfl_sync(full, w[c], from);
+                if (nxt >= 0) w[c] += t;
             }
+            rest &= ~__ballot_sync(full, rank & 1);
+            rank >>= 1;
         }
+        const bool tail = leader;
         if (!tail || key < 0) continue;
         bool x0 = ix > 0 && ix < gx - 1, x1 = ix + 1 > 0 && ix + 1 < gx - 1;
         bool y0 = iy > 0 && iy < gy - 1, y1 = iy + 1 > 0 && iy + 1 < gy - 1;
