@@ -82,6 +82,8 @@ def lib():
         L.orc_sim_design_state.argtypes = [vp, pd, pd]
         L.orc_sim_propagate.argtypes = [vp, i]
         L.orc_sim_propagate_steps.argtypes = [vp, i, i]
+        L.orc_sim_libff_apply.argtypes = [vp, pd, i]
+        L.orc_sim_aperture_apply.argtypes = [vp, i, ctypes.c_char_p, ctypes.POINTER(i)]
         L.orc_sim_sc_last.argtypes = [vp, pd, pd, pd, pd, pd, pd, pd, pd]
         L.orc_sc_apply.argtypes = [ctypes.POINTER(SCOptions), i, d, d, i, i64, d, i, pd, pu8, d,
                                    pd, pd, pd, pd, pd, pd, pd, pd]
@@ -194,6 +196,19 @@ class Sim:
 
     def propagate_steps(self, first, count):
         _check(lib().orc_sim_propagate_steps(self.h, first, count))
+
+    def libff_apply(self, slices):
+        """LibFF_operation over explicit slices: rows (element index, left,
+        right), applied in order."""
+        a = np.ascontiguousarray(slices, dtype=np.float64).reshape(-1, 3)
+        _check(lib().orc_sim_libff_apply(self.h, _pd(a), a.shape[0]))
+
+    def aperture_apply(self, index, aperture_type):
+        """Aperture_operation with the attributes of element `index`;
+        returns the number of particles discarded."""
+        nd = ctypes.c_int()
+        _check(lib().orc_sim_aperture_apply(self.h, index, aperture_type.encode(), ctypes.byref(nd)))
+        return nd.value
 
     def count_flops(self, index, first, count):
         """Runs steps [first, first+count) as propagate_steps does and

@@ -2591,6 +2591,41 @@ int orc_sim_propagate_steps(void* sp, int first, int count)
     ORC_CATCH
 }
 
+// LibFF_operation::apply_impl (simulation/independent_operation.h:45-60) on
+// explicit slices of the Sim's lattice: triples (element index, left, right),
+// each through FF_element::apply (ff_element.h:25-67) in order.  The design
+// reference particle starts from the lattice's on first use, as
+// Propagator::do_before_start sets it.
+int orc_sim_libff_apply(void* sp, const double* slices, int nslices)
+{
+    ORC_TRY
+    auto* s = (Sim*)sp;
+    if (!s->started) {
+        s->b.design = s->lat.ref;
+        s->started = true;
+    }
+    for (int i = 0; i < nslices; ++i) {
+        const int ei = (int)slices[3 * i];
+        if (ei < 0 || ei >= (int)s->lat.elements.size()) throw std::runtime_error("slice element out of range");
+        element_apply(Slice(s->lat.elements[ei], slices[3 * i + 1], slices[3 * i + 2]), s->b);
+    }
+    ORC_CATCH
+}
+
+// Aperture_operation<AP>::apply_impl (simulation/aperture_operation.h:14-24)
+// with the attributes of element `index` (operation_extractor.cc:55-75):
+// Bunch::apply_aperture alone, so n_valid drops by the discards and n_total
+// is left to the next update_total_num.
+int orc_sim_aperture_apply(void* sp, int index, const char* type, int* ndiscarded)
+{
+    ORC_TRY
+    auto* s = (Sim*)sp;
+    if (index < 0 || index >= (int)s->lat.elements.size()) throw std::runtime_error("element index out of range");
+    const Slice whole(s->lat.elements[index]);
+    *ndiscarded = aperture_apply(make_aperture(type, whole), s->b);
+    ORC_CATCH
+}
+
 // Operation counting (see FlopState): counts the algorithmic FP64 work of
 // particle `index` through the oracle's own particle code while the Sim
 // runs as usual; one record per operator of each step run.

@@ -486,6 +486,46 @@ class Independent_stepper_elements(_Stepper):
         super().__init__(None, steps_per_element)
 
 
+class LibFF_operation:
+    """simulation/independent_operation.h:45-60: the libFF maps of a list of
+    lattice slices, rows (element index, left, right), applied in order by
+    FF_element::apply (libFF/ff_element.h:25-67); the bunch's design
+    reference particle moves with them."""
+
+    def __init__(self, lattice, slices):
+        self.lattice = lattice
+        self.slices = np.ascontiguousarray(slices, dtype=np.float64).reshape(-1, 3)
+
+    def apply(self, bunch, stream=None):
+        lh = self.lattice._handle()
+        try:
+            check(lib().sb2_libff_apply(lh, _pd(self.slices), self.slices.shape[0], bunch.h, stream))
+        finally:
+            lib().sb2_lattice_destroy(lh)
+
+
+class Aperture_operation:
+    """simulation/aperture_operation.h:8-115: Bunch::apply_aperture with the
+    attributes of lattice element `index`; aperture_type "finite",
+    "circular", "elliptical" or "rectangular"."""
+
+    def __init__(self, lattice, index, aperture_type):
+        self.lattice = lattice
+        self.index = int(index)
+        self.aperture_type = aperture_type
+
+    def apply(self, bunch, stream=None):
+        """Returns the number of particles discarded."""
+        lh = self.lattice._handle()
+        nd = ctypes.c_int32()
+        try:
+            check(lib().sb2_aperture_apply(lh, self.index, self.aperture_type.encode(), bunch.h, ctypes.byref(nd),
+                                           stream))
+        finally:
+            lib().sb2_lattice_destroy(lh)
+        return nd.value
+
+
 class Propagator:
     """simulation/propagator.cc: Propagator(lattice, stepper).propagate."""
 

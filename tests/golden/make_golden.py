@@ -1,7 +1,10 @@
 """Extract golden tracking vectors from the synergia2 reference's own libFF tests.
 
-Run once in a container that has the reference checkout (read-only); writes
-tests/golden/madx_tracks.json, which the tests read on any machine.
+Run once with SYNERGIA_REF set to the root of a synergia2 checkout (read
+only); writes tests/golden/madx_tracks.json, which the tests read on any
+machine:
+
+    SYNERGIA_REF=<synergia2 checkout> python tests/golden/make_golden.py
 
 Sources (paths inside the synergia2 project):
   src/synergia/libFF/tests/test_madx_elements.cc:10-16,100-230   fixture,
@@ -25,8 +28,10 @@ import os
 import re
 import sys
 
-REF = os.environ.get("SYNERGIA_REF", "/root/reference")
-LAT = os.path.join(REF, "src/synergia/libFF/tests/lattices")
+REF = os.environ.get("SYNERGIA_REF")
+if not REF and __name__ == "__main__":
+    sys.exit("set SYNERGIA_REF to the root of a synergia2 checkout")
+LAT = os.path.join(REF or "", "src/synergia/libFF/tests/lattices")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "madx_tracks.json")
 
 P0 = 1.5

@@ -113,8 +113,9 @@ def test_sc_degenerate_domain_error(syn):
 def test_propagate_with_space_charge_matches_oracle(syn, orc):
     """FODO cell, split operator with 8 kicks per cell, adaptive domain,
     linear Green function, 2 turns (16 kicks): last solve's fields within
-    1e-10 of the oracle's, coordinates within 1e-10 relative, ids and masks
-    exact."""
+    1e-10 of the oracle's, coordinates within 1e-12 relative (the deposit
+    order moves them by ~1e-14, measured at full size in
+    test_gpu_parity_scale.py), ids and masks exact."""
     n, shape, turns = 100000, (16, 16, 32), 2
     p = gaussian_bunch(n, SIG_C0, 31)
     lat, ref = product_lattice(fodo_cell())
@@ -135,7 +136,7 @@ def test_propagate_with_space_charge_matches_oracle(syn, orc):
     for c in ("rho", "ex", "ey", "ez"):
         assert rel_l2(g[c], o[c]) <= FIELD_TOL, c
     for j in range(6):
-        assert rel_l2(gp[:, j], op[:, j]) <= 1e-10, j
+        assert rel_l2(gp[:, j], op[:, j]) <= 1e-12, j
 
 
 def test_bunch_moments_and_emittance(syn):
@@ -247,36 +248,6 @@ def test_wrapped_bunch_arrays_current_after_each_call(syn, monkeypatch):
             assert rel_l2(got[:, j], expect[:, j]) <= 1e-10, j
     finally:
         L.sb2_bunch_destroy(h)
-
-
-def test_c0_config_matches_oracle(syn, orc):
-    """The CPU-runnable configuration at its own size: FODO cell, 8 kicks
-    per cell, 1,048,576 macroparticles, 32 x 32 x 64 grid, 10 passes (80
-    kicks), FP64.  Ids, masks and the lost set exact; coordinates within
-    1e-8 relative L2 of the oracle after 80 kicks (deposit summation order
-    is the only difference, and it compounds over the kicks); final fields
-    within 1e-8."""
-    n, shape, turns = 1048576, (32, 32, 64), 10
-    p = gaussian_bunch(n, SIG_C0, 0)
-    lat, ref = product_lattice(fodo_cell())
-    opts = syn.Space_charge_3d_open_hockney_options(*shape)
-    prop = syn.Propagator(lat, syn.Split_operator_stepper(opts, 8))
-    b = syn.Bunch(ref, n, 1e11)
-    b.set_particles(p)
-    prop.propagate(b, turns)
-    gp, gm, _ = b.get_particles()
-    g = prop.sc_last()
-    sim = orc.Sim(oracle_lattice(fodo_cell()), n, 1e11, stepper=orc.STEPPER_SPLIT, num=8,
-                  sc=orc.SCOptions.make(*shape), value=2.5 + MP)
-    sim.set_particles(p)
-    sim.propagate(turns)
-    op, om, _ = sim.get_particles()
-    o = sim.sc_last(shape)
-    assert np.array_equal(gm, om) and np.array_equal(gp[:, 6], op[:, 6])
-    for c in ("rho", "ex", "ey", "ez"):
-        assert rel_l2(g[c], o[c]) <= 1e-8, c
-    for j in range(6):
-        assert rel_l2(gp[:, j], op[:, j]) <= 1e-8, j
 
 
 def test_c3_size_ring_properties(syn):
