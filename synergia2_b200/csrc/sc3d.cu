@@ -20,6 +20,8 @@
 #include <algorithm>
 #include <type_traits>
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
 
 #include "fft.cuh"
 #include "sb2_kernels.h"
@@ -243,6 +245,311 @@ __global__ void __launch_bounds__(256) deposit_kernel(const double* __restrict__
             if (y0 && x1) atomicAdd(&rho[base + iy * gx + ix + 1], w[5]);
             if (y1 && x0) atomicAdd(&rho[base + (iy + 1) * gx + ix], w[6]);
             if (y1 && x1) atomicAdd(&rho[base + (iy + 1) * gx + ix + 1], w[7]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Deposit by shared-memory tiles (same weights as deposit_kernel; only the
+// summation differs).
+//
+// A CTA takes kDepT * K consecutive particles of the (cell-ordered) bunch.
+//   1. coalesced: each thread loads K particles (stride kDepT), computes the
+//      stencil cell and the CIC offsets, and stores them in shared memory at
+//      the particle's slot of a per-thread-consecutive layout (slot(i) =
+//      i + i / K: thread t later reads particles t*K .. t*K+K-1, conflict
+//      free); the CTA reduces the bounding box of the stencil cells.
+//   2. if the box's grid points fit the tile (kDepTile points), each thread
+//      walks its K consecutive particles summing the 8 corner weights of a
+//      run of equal cells in FP64 registers (the bunch is ordered by cell, so
+//      runs are long) and adds each finished run to the tile; the last run of
+//      every thread is first summed over the warp's lanes with the same cell
+//      (a transpose reduction when the whole warp shares one cell, the dense
+//      core of a freshly ordered bunch; peer groups otherwise).  The tile
+//      holds fixed-point sums in 32-bit words, because 32-bit integer
+//      atomics are native in shared memory while FP64 (and 64-bit integer)
+//      shared atomics are compare-and-swap loops: a run's corner weight is
+//      w0 * u with u in [0, 32 K], u * 2^kFrac (< 2^63) is rounded to an
+//      integer and split into three 21-bit digits, each added to its own word
+//      (every addition carries at least one particle, so a word takes at most
+//      kDepT * K <= 2^11 additions of < 2^21 and does not overflow).
+//      Resolution 2^-kFrac w0 per addition, far below FP64 summation noise;
+//      integer sums do not depend on the order of the additions.
+//   3. the tile's non-zero interior points go to rho, the three digits
+//      recombined in FP64 and scaled by w0 2^-kFrac, with one global FP64
+//      atomic each -- the only global atomics, on the points the CTA's box
+//      shares with its neighbours' boxes.
+// A chunk whose box does not fit (tails of the bunch, or a bunch that is not
+// cell ordered) deposits straight to rho with per-warp peer groups, as
+// deposit_kernel does.  Only stencil cells with 0 <= i <= g-2 in every axis
+// can reach an interior grid point (0 < i < g-1, deposit.cc:23-30); others
+// are skipped.
+// ---------------------------------------------------------------------------
+constexpr int kDepT = 256;
+constexpr int kDepTile = 1536;
+
+template <int K>
+struct DepositSmem {
+    static constexpr int kSlots = kDepT * (K + 1);
+    // fixed-point scale: one addition carries the sum u <= 32 K of a warp's
+    // peer group, so u * 2^kFrac <= 2^63 (three 21-bit digits)
+    static constexpr int kFrac = K <= 4 ? 56 : 55;
+    double ox[kSlots], oy[kSlots], oz[kSlots];
+    int32_t cell[kSlots]; // ix | iy << 10 | iz << 20, or -1
+    uint32_t d0[kDepTile], d1[kDepTile], d2[kDepTile];
+    int32_t box[kDepT / 32][6];
+};
+
+// The 8 CIC weights of one particle divided by w0: products of the offsets
+// (deposit.cc:309-394 multiplies w0 in front; factored out here and applied
+// when the tile is flushed, the same product to rounding).
+__device__ __forceinline__ void cic_unit_weights(double ox, double oy, double oz, double* u)
+{
+    const double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
+    u[0] = aox * aoy * aoz;
+    u[1] = ox * aoy * aoz;
+    u[2] = aox * oy * aoz;
+    u[3] = ox * oy * aoz;
+    u[4] = aox * aoy * oz;
+    u[5] = ox * aoy * oz;
+    u[6] = aox * oy * oz;
+    u[7] = ox * oy * oz;
+}
+
+__device__ __forceinline__ void cic_weights(double w0, double ox, double oy, double oz, double* w)
+{
+    const double aox = 1.0 - ox, aoy = 1.0 - oy, aoz = 1.0 - oz;
+    w[0] = w0 * aox * aoy * aoz;
+    w[1] = w0 * ox * aoy * aoz;
+    w[2] = w0 * aox * oy * aoz;
+    w[3] = w0 * ox * oy * aoz;
+    w[4] = w0 * aox * aoy * oz;
+    w[5] = w0 * ox * aoy * oz;
+    w[6] = w0 * aox * oy * oz;
+    w[7] = w0 * ox * oy * oz;
+}
+
+// Sums w over the lanes of the warp whose `key` is equal (peer groups, in any
+// lane order, by a tree over the lanes' ranks among their peers); returns
+// true on the lowest lane of each group, which then holds the group's sums.
+// Every lane of the warp calls it.
+__device__ __forceinline__ bool peer_sum8(int key, double* w)
+{
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned peers = __match_any_sync(full, key);
+    unsigned below;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(below));
+    unsigned rest = peers & ~below & ~(1u << lane);
+    int rank = __popc(peers & below);
+    while (__any_sync(full, rest != 0)) {
+        const int nxt = __ffs(rest) - 1;
+        const int from = nxt < 0 ? lane : nxt;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const double t = __shfl_sync(full, w[c], from);
+            if (nxt >= 0) w[c] += t;
+        }
+        rest &= ~__ballot_sync(full, rank & 1);
+        rank >>= 1;
+    }
+    return (peers & below) == 0;
+}
+
+// Sum of a[0..7] over the warp's 32 lanes, corner c ending on lanes 4c..4c+3:
+// each halving exchange keeps half of the values (9 FP64 shuffles in all).
+__device__ __forceinline__ double transpose_sum8(const double* a)
+{
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    double h4[4], h2[2];
+    const bool b16 = lane & 16, b8 = lane & 8, b4 = lane & 4;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double keep = b16 ? a[k + 4] : a[k], send = b16 ? a[k] : a[k + 4];
+        h4[k] = keep + __shfl_xor_sync(full, send, 16);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const double keep = b8 ? h4[k + 2] : h4[k], send = b8 ? h4[k] : h4[k + 2];
+        h2[k] = keep + __shfl_xor_sync(full, send, 8);
+    }
+    double h = (b4 ? h2[1] : h2[0]) + __shfl_xor_sync(full, b4 ? h2[0] : h2[1], 4);
+    h += __shfl_xor_sync(full, h, 2);
+    h += __shfl_xor_sync(full, h, 1);
+    return h; // corner (b16 ? 4 : 0) + (b8 ? 2 : 0) + (b4 ? 1 : 0) = lane >> 2
+}
+
+template <int K>
+__device__ __forceinline__ void tile_add(DepositSmem<K>& sm, int at, double u, double scale)
+{
+    const unsigned long long q = __double2ull_rn(u * scale);
+    atomicAdd(&sm.d0[at], (uint32_t)(q & 0x1fffffu));
+    atomicAdd(&sm.d1[at], (uint32_t)((q >> 21) & 0x1fffffu));
+    atomicAdd(&sm.d2[at], (uint32_t)(q >> 42));
+}
+
+template <int K>
+__global__ void __launch_bounds__(kDepT) deposit_tile_kernel(const double* __restrict__ parts, int64_t stride,
+                                                             const uint8_t* __restrict__ masks, int64_t n,
+                                                             const ScState* __restrict__ scp, double* rho, int gx,
+                                                             int gy, int gz)
+{
+    extern __shared__ __align__(16) unsigned char dep_raw[];
+    DepositSmem<K>& sm = *reinterpret_cast<DepositSmem<K>*>(dep_raw);
+    const ScState& sc = *scp;
+    if (!sc.valid) return;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int64_t base = (int64_t)blockIdx.x * (kDepT * K);
+    const unsigned full = 0xffffffffu;
+
+    // 1. cells and offsets, coalesced
+    double px[K], py[K], pz[K];
+    uint8_t pm[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const int64_t i = base + j * kDepT + t;
+        pm[j] = 0;
+        if (i < n) {
+            pm[j] = masks[i];
+            px[j] = parts[i];
+            py[j] = parts[i + 2 * stride];
+            pz[j] = parts[i + 4 * stride];
+        }
+    }
+    int bmin[3] = {1 << 30, 1 << 30, 1 << 30}, bmax[3] = {-1, -1, -1};
+    const double lx = sc.left[0], ly = sc.left[1], lz = sc.left[2];
+    const double ihx = sc.ih[0], ihy = sc.ih[1], ihz = sc.ih[2];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const int li = j * kDepT + t;
+        const int s = li + li / K;
+        int32_t cell = -1;
+        double ox = 0.0, oy = 0.0, oz = 0.0;
+        if (pm[j]) {
+            int ix, iy, iz;
+            leftmost_d(px[j], lx, ihx, ix, ox);
+            leftmost_d(py[j], ly, ihy, iy, oy);
+            leftmost_d(pz[j], lz, ihz, iz, oz);
+            if (ix >= 0 && ix <= gx - 2 && iy >= 0 && iy <= gy - 2 && iz >= 0 && iz <= gz - 2) {
+                cell = ix | (iy << 10) | (iz << 20);
+                bmin[0] = min(bmin[0], ix); bmax[0] = max(bmax[0], ix);
+                bmin[1] = min(bmin[1], iy); bmax[1] = max(bmax[1], iy);
+                bmin[2] = min(bmin[2], iz); bmax[2] = max(bmax[2], iz);
+            }
+        }
+        sm.cell[s] = cell;
+        sm.ox[s] = ox;
+        sm.oy[s] = oy;
+        sm.oz[s] = oz;
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        bmin[a] = __reduce_min_sync(full, bmin[a]);
+        bmax[a] = __reduce_max_sync(full, bmax[a]);
+    }
+    if (lane == 0) {
+        sm.box[warp][0] = bmin[0]; sm.box[warp][1] = bmin[1]; sm.box[warp][2] = bmin[2];
+        sm.box[warp][3] = bmax[0]; sm.box[warp][4] = bmax[1]; sm.box[warp][5] = bmax[2];
+    }
+    __syncthreads();
+    {
+        const int w = lane & (kDepT / 32 - 1);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            bmin[a] = __reduce_min_sync(full, sm.box[w][a]);
+            bmax[a] = __reduce_max_sync(full, sm.box[w][3 + a]);
+        }
+    }
+    if (bmax[0] < 0) return; // no particle of the chunk reaches an interior point
+    const int BX = bmax[0] - bmin[0] + 2, BY = bmax[1] - bmin[1] + 2, BZ = bmax[2] - bmin[2] + 2;
+    const int BXY = BX * BY, V = BXY * BZ;
+    const double w0 = sc.w0;
+
+    if (V <= kDepTile) {
+        // 2. runs of equal cells into the fixed-point tile
+        for (int v = t; v < V; v += kDepT) {
+            sm.d0[v] = 0u;
+            sm.d1[v] = 0u;
+            sm.d2[v] = 0u;
+        }
+        __syncthreads();
+        const double scale = (double)(1ull << DepositSmem<K>::kFrac);
+        const int off[8] = {0, 1, BX, BX + 1, BXY, BXY + 1, BXY + BX, BXY + BX + 1};
+        int cur = -1;
+        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const int sj = t * (K + 1) + j;
+            const int32_t c = sm.cell[sj];
+            if (c < 0) continue;
+            const int lk = (((c >> 20) - bmin[2]) * BY + (((c >> 10) & 1023) - bmin[1])) * BX + ((c & 1023) - bmin[0]);
+            double u[8];
+            cic_unit_weights(sm.ox[sj], sm.oy[sj], sm.oz[sj], u);
+            if (lk != cur) {
+                if (cur >= 0)
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) tile_add(sm, cur + off[q], acc[q], scale);
+                cur = lk;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) acc[q] = u[q];
+            } else {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) acc[q] += u[q];
+            }
+        }
+        if (__all_sync(full, cur == __shfl_sync(full, cur, 0))) {
+            // one cell for the whole warp: lane l ends with corner (l >> 2) of
+            // the warp's sum
+            const double v = transpose_sum8(acc);
+            const int c = lane >> 2;
+            if (cur >= 0 && (lane & 3) == 0) tile_add(sm, cur + (c & 1) + ((c >> 1) & 1) * BX + (c >> 2) * BXY, v, scale);
+        } else if (peer_sum8(cur, acc) && cur >= 0) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) tile_add(sm, cur + off[q], acc[q], scale);
+        }
+        __syncthreads();
+        // 3. the tile's interior points to rho
+        const double back = w0 / scale;
+        for (int v = t; v < V; v += kDepT) {
+            const uint32_t a0 = sm.d0[v], a1 = sm.d1[v], a2 = sm.d2[v];
+            if ((a0 | a1 | a2) == 0u) continue;
+            const int r = v / BX;
+            const int X = bmin[0] + (v - r * BX), Y = bmin[1] + (r % BY), Z = bmin[2] + r / BY;
+            if (X > 0 && X < gx - 1 && Y > 0 && Y < gy - 1 && Z > 0 && Z < gz - 1) {
+                const double sum = ((double)a2 * 4398046511104.0 + (double)a1 * 2097152.0) + (double)a0;
+                atomicAdd(&rho[((int64_t)Z * gy + Y) * gx + X], sum * back);
+            }
+        }
+        return;
+    }
+
+    // box too large for the tile: per-warp peer groups straight to rho
+#pragma unroll 1
+    for (int j = 0; j < K; ++j) {
+        const int li = j * kDepT + t;
+        const int s = li + li / K;
+        const int32_t c = sm.cell[s];
+        double w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (c >= 0) cic_weights(w0, sm.ox[s], sm.oy[s], sm.oz[s], w);
+        if (!peer_sum8(c, w) || c < 0) continue;
+        const int ix = c & 1023, iy = (c >> 10) & 1023, iz = c >> 20;
+        const bool x0 = ix > 0, x1 = ix + 1 < gx - 1;
+        const bool y0 = iy > 0, y1 = iy + 1 < gy - 1;
+        const bool z0 = iz > 0, z1 = iz + 1 < gz - 1;
+        const int64_t b0 = (int64_t)iz * gx * gy + (int64_t)iy * gx + ix;
+        const int64_t P = (int64_t)gx * gy;
+        if (z0) {
+            if (y0 && x0) atomicAdd(&rho[b0], w[0]);
+            if (y0 && x1) atomicAdd(&rho[b0 + 1], w[1]);
+            if (y1 && x0) atomicAdd(&rho[b0 + gx], w[2]);
+            if (y1 && x1) atomicAdd(&rho[b0 + gx + 1], w[3]);
+        }
+        if (z1) {
+            if (y0 && x0) atomicAdd(&rho[b0 + P], w[4]);
+            if (y0 && x1) atomicAdd(&rho[b0 + P + 1], w[5]);
+            if (y1 && x0) atomicAdd(&rho[b0 + P + gx], w[6]);
+            if (y1 && x1) atomicAdd(&rho[b0 + P + gx + 1], w[7]);
         }
     }
 }
@@ -682,11 +989,44 @@ cudaError_t launch_book_domain(const DomainParams& p, cudaStream_t s)
 #ifndef SB2_DEPOSIT_CTAS
 #define SB2_DEPOSIT_CTAS 8 // CTAs per SM of the grid-stride deposit (5 / 8 / 16: 0.163 / 0.142 / 0.146 ms per C1 step)
 #endif
+template <int K>
+static cudaError_t deposit_tile(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
+                                const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s)
+{
+    const int bytes = (int)sizeof(DepositSmem<K>);
+    static cudaError_t once =
+        cudaFuncSetAttribute(deposit_tile_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (once) return once;
+    const int64_t chunk = (int64_t)kDepT * K;
+    const int64_t nb = (n + chunk - 1) / chunk;
+    if (nb > 0) deposit_tile_kernel<K><<<(unsigned)nb, kDepT, bytes, s>>>(parts, stride, masks, n, sc, rho, gx, gy, gz);
+    return cudaGetLastError();
+}
+
+// Deposit variant: SB2_DEPOSIT=tile (default: shared-memory tiles of 256 x K
+// particles, K from SB2_DEPOSIT_K, 4 or 8) or warp (per-warp peer groups and
+// global atomics only).
+static int deposit_variant()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("SB2_DEPOSIT");
+        const char* k = getenv("SB2_DEPOSIT_K");
+        v = (e && !strcmp(e, "warp")) ? 0 : ((k && atoi(k) == 8) ? 8 : 4);
+    }
+    return v;
+}
+
 cudaError_t launch_deposit(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
                            const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s)
 {
-    deposit_kernel<<<sm_count() * SB2_DEPOSIT_CTAS, 256, 0, s>>>(parts, stride, masks, n, sc, rho, gx, gy, gz);
-    return cudaGetLastError();
+    switch (deposit_variant()) {
+    case 4: return deposit_tile<4>(parts, stride, masks, n, sc, rho, gx, gy, gz, s);
+    case 8: return deposit_tile<8>(parts, stride, masks, n, sc, rho, gx, gy, gz, s);
+    default:
+        deposit_kernel<<<sm_count() * SB2_DEPOSIT_CTAS, 256, 0, s>>>(parts, stride, masks, n, sc, rho, gx, gy, gz);
+        return cudaGetLastError();
+    }
 }
 
 static inline int ceil_div64(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
