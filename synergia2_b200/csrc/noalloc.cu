@@ -24,6 +24,7 @@
 //     without ordering) race on it.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -42,7 +43,9 @@ constexpr size_t kNoAllocBytes = (size_t)12 << 20; // 12 MiB
 __device__ __align__(256) unsigned char g_sc_scratch[kNoAllocBytes];
 
 constexpr int kMaxDevices = 64;
-void* g_scratch_ptr[kMaxDevices] = {nullptr};
+// device address of g_sc_scratch per device, looked up on the first call on
+// that device (atomic: host threads may make their first calls at once)
+std::atomic<void*> g_scratch_ptr[kMaxDevices];
 
 size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
@@ -138,9 +141,17 @@ extern "C" sb2_status sb2_sc3d_apply_noalloc(const sb2_sc3d_options* opts, doubl
         return fail(SB2_ERR_INVALID, "sb2_sc3d_apply_noalloc: grid exceeds the fixed workspace (at most 65536 cells "
                                      "and doubled dimensions <= 128)");
     Layout lay = layout_for(d);
+    // Guard only: with at most 65,536 cells and doubled dimensions <= 128 the
+    // layout stays below 8 MiB (the spectrum, 2gz * 2gy * (gx+2) complex
+    // values, is the largest part at about 4.3 MiB), so no accepted grid
+    // reaches this check.
     if (lay.total > kNoAllocBytes)
         return fail(SB2_ERR_INVALID, "sb2_sc3d_apply_noalloc: grid exceeds the 12 MiB fixed workspace");
-    if (track_grid_blocks() > kNoAllocMaxPartials)
+    // one launch shape for both particle passes, so the moment partials the
+    // first pass writes are the ones the domain kernel reduces
+    const TrackTune tune = track_tune_defaults();
+    const int nblocks = track_grid_blocks(tune.ctas_per_sm);
+    if (nblocks > kNoAllocMaxPartials)
         return fail(SB2_ERR_UNSUPPORTED, "sb2_sc3d_apply_noalloc: device has more SMs than the workspace allows");
     double gamma, beta, pref;
     rc = ref_kinematics(charge, mass, value, kind, &gamma, &beta, &pref, &msg);
@@ -151,13 +162,13 @@ extern "C" sb2_status sb2_sc3d_apply_noalloc(const sb2_sc3d_options* opts, doubl
     cudaError_t e = cudaGetDevice(&dev);
     if (e) return cuda_fail(e, "cudaGetDevice");
     if (dev < 0 || dev >= kMaxDevices) return fail(SB2_ERR_UNSUPPORTED, "sb2_sc3d_apply_noalloc: device ordinal");
-    if (!g_scratch_ptr[dev]) {
-        void* ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_sc_scratch);
+    void* sym = g_scratch_ptr[dev].load(std::memory_order_acquire);
+    if (!sym) {
+        e = cudaGetSymbolAddress(&sym, g_sc_scratch);
         if (e) return cuda_fail(e, "cudaGetSymbolAddress");
-        g_scratch_ptr[dev] = ptr;
+        g_scratch_ptr[dev].store(sym, std::memory_order_release); // every thread finds the same address
     }
-    unsigned char* base = (unsigned char*)g_scratch_ptr[dev];
+    unsigned char* base = (unsigned char*)sym;
     cudaStream_t s = (cudaStream_t)stream;
     ScState* state = (ScState*)(base + lay.state);
     BunchCounters* counters = (BunchCounters*)(base + lay.counters);
@@ -211,14 +222,14 @@ extern "C" sb2_status sb2_sc3d_apply_noalloc(const sb2_sc3d_options* opts, doubl
     tp.gz = d.gz;
     tp.nops = 1;
     tp.ops[0].kind = OP_MOMENTS;
-    if (!o.domain_fixed && (e = launch_track(tp, track_tune_defaults(), s))) return cuda_fail(e, "moments pass");
+    if (!o.domain_fixed && (e = launch_track(tp, tune, s))) return cuda_fail(e, "moments pass");
 
     DomainParams dp;
     std::memset(&dp, 0, sizeof(dp));
     dp.counters = counters;
     dp.ap_counts = ap_counts;
     dp.moment_partials = partials;
-    dp.n_partials = track_grid_blocks();
+    dp.n_partials = nblocks;
     dp.compute_domain = 1;
     dp.sc = state;
     for (int i = 0; i < 3; ++i) {
@@ -248,7 +259,7 @@ extern "C" sb2_status sb2_sc3d_apply_noalloc(const sb2_sc3d_options* opts, doubl
     tp.ops[0].kind = OP_SC_KICK;
     tp.ops[0].d[0] = pref; // reference momentum and mass of the kick
     tp.ops[0].d[1] = mass;
-    if ((e = launch_track(tp, track_tune_defaults(), s))) return cuda_fail(e, "kick pass");
+    if ((e = launch_track(tp, tune, s))) return cuda_fail(e, "kick pass");
 
     ScState st;
     if ((e = cudaMemcpyAsync(&st, state, sizeof(st), cudaMemcpyDeviceToHost, s)) || (e = cudaStreamSynchronize(s)))
