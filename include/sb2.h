@@ -256,15 +256,22 @@ sb2_status sb2_propagator_sc_last(sb2_propagator* p, double left[3], double h[3]
  * (core_diagnostics.cc:444, bunch.h:363-370), and the charge density after
  * every deposit (space_charge_3d_open_hockney.cc:572).  fn sums the `count`
  * doubles at `data` in place over the ranks and returns 0; every rank makes
- * the same calls in the same order.  The library's own work on its stream
- * is finished before each call.  on_host != 0: data is pinned host memory
- * (a host-side collective: gloo, MPI); 0: data is device memory (NCCL).
+ * the same calls in the same order.  on_host != 0: data is pinned host
+ * memory (a host-side collective: gloo, MPI), and the library's work on its
+ * stream is finished before each call; 0: data is device memory (NCCL), the
+ * call comes without a host synchronisation, and fn must order its
+ * collective after the work already queued on sb2_allreduce_stream() and
+ * before the work queued there after fn returns (e.g. ncclAllReduce on that
+ * stream).
  * The bunch's n_total and real_num are then the totals over the ranks (pass
  * the global real_num to every shard).  CUDA-graph turns and per-turn
  * diagnostics are not available on a sharded propagator.  fn = NULL
  * returns to a whole bunch. */
 typedef int32_t (*sb2_allreduce_fn)(void* ctx, double* data, int64_t count, int32_t on_host);
 sb2_status sb2_propagator_set_allreduce(sb2_propagator* p, sb2_allreduce_fn fn, void* ctx, int32_t on_host);
+/* Inside a sum-allreduce callback: the cudaStream_t of the exchange (the
+ * stream of the propagate call); NULL outside a callback. */
+void* sb2_allreduce_stream(void);
 
 /* Per-turn diagnostics on the device (Diagnostics_full2::do_update,
  * bunch/diagnostics_full2.cc:16-37): with capacity > 0 the propagator

@@ -1795,6 +1795,9 @@ static int ilog2(int v)
 // the call.  With on_host the data is staged through pinned host memory (a
 // host-side collective such as gloo or MPI), otherwise the function gets the
 // device pointer (NCCL).
+// stream of the exchange a sum-allreduce callback is running for
+static thread_local cudaStream_t g_hook_stream = nullptr;
+
 struct AllreduceHook {
     sb2_allreduce_fn fn = nullptr;
     void* ctx = nullptr;
@@ -1806,11 +1809,21 @@ struct AllreduceHook {
         if (pinned) cudaFreeHost(pinned);
     }
     explicit operator bool() const { return fn != nullptr; }
+    // Host buffers: the stream is drained, the data staged through pinned
+    // memory, summed by fn and copied back.  Device buffers: fn is called at
+    // once with the device pointer and must order its collective on the
+    // library's stream (sb2_allreduce_stream() inside the callback), so
+    // nothing waits on the host.
     void run(double* dev, int64_t n, cudaStream_t s)
     {
-        cuda_check(cudaStreamSynchronize(s), "allreduce");
+        struct StreamScope {
+            cudaStream_t prev;
+            explicit StreamScope(cudaStream_t st) : prev(g_hook_stream) { g_hook_stream = st; }
+            ~StreamScope() { g_hook_stream = prev; }
+        } scope(s);
         int32_t rc;
         if (on_host) {
+            cuda_check(cudaStreamSynchronize(s), "allreduce");
             if (pinned_n < (size_t)n) {
                 if (pinned) cudaFreeHost(pinned);
                 pinned = nullptr;
@@ -3684,6 +3697,8 @@ sb2_status sb2_propagator_set_diagnostics(sb2_propagator* p, int32_t capacity)
     p->p->set_diagnostics(capacity);
     SB2_CATCH
 }
+
+void* sb2_allreduce_stream(void) { return (void*)g_hook_stream; }
 
 sb2_status sb2_propagator_set_allreduce(sb2_propagator* p, sb2_allreduce_fn fn, void* ctx, int32_t on_host)
 {

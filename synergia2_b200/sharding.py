@@ -37,9 +37,16 @@ def attach(propagator, group=None, on_host=None):
                 self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False),
                                                  "version": 3, "strides": None}
 
+        from . import _lib
+
         def fn(ptr, n):
-            t = torch.as_tensor(_Dev(ptr, n), device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
-            torch.cuda.synchronize()
+            # the collective is ordered on the library's stream: NCCL waits
+            # for the deposit queued there, and the library's next kernels
+            # wait for NCCL; the host does not wait
+            ptr_s = _lib.lib().sb2_allreduce_stream()
+            st = torch.cuda.ExternalStream(ptr_s) if ptr_s else torch.cuda.default_stream()
+            with torch.cuda.stream(st):
+                t = torch.as_tensor(_Dev(ptr, n), device="cuda")
+                dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     propagator.set_allreduce(fn, on_host=on_host)
     return propagator

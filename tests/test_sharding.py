@@ -145,3 +145,93 @@ def test_sharded_bunch_matches_whole_bunch(syn, case):
         assert r[5] == b.get_real_num()
     for j in range(6):
         assert rel_l2(sp[:, j], wp[:, j]) <= 1e-10, j
+
+
+def _nccl_rank(port, n, q):
+    """World size 1 over NCCL: the device-buffer exchange (the library's
+    stream handed to the collective) runs for real on the one GPU."""
+    import sys
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), NCCL_NVLS_ENABLE="0")
+    torch.cuda.set_device(0)
+    import datetime
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
+                            device_id=torch.device("cuda", 0))
+    try:
+        import synergia2_b200 as syn
+        from synergia2_b200.sharding import attach
+        calls = [0]
+        orig = dist.all_reduce
+
+        def counted(*a, **k):
+            calls[0] += 1
+            return orig(*a, **k)
+        dist.all_reduce = counted
+        spec, steps, sig = _spec("ring")
+        p = gaussian_bunch(n, sig, 96)
+        lat, ref = product_lattice(spec)
+        prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(16, 16, 32),
+                                                               steps))
+        attach(prop)
+        b = syn.Bunch(ref, n, 1e11)
+        b.set_particles(p)
+        prop.propagate(b, 2)
+        gp, gm, gd = b.get_particles()
+        q.put((dist.get_backend(), calls[0], gp, gm, gd, b.get_total_num(), b.get_real_num()))
+        del prop
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.timeout(300)
+def test_nccl_device_exchange_world_one_matches_whole_bunch(syn):
+    """The NCCL branch of sharding.attach (device buffers, the collective
+    ordered on the library's stream, no host synchronisation) at world size
+    1 against the same bunch without an exchange: ring cell with losses, two
+    turns; ids, masks, discards, total and real numbers exact, coordinates
+    within 1e-10 (the deposit's summation order)."""
+    n = 40000
+    spec, steps, sig = _spec("ring")
+    p = gaussian_bunch(n, sig, 96)
+    lat, ref = product_lattice(spec)
+    prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(16, 16, 32),
+                                                           steps))
+    b = syn.Bunch(ref, n, 1e11)
+    b.set_particles(p)
+    prop.propagate(b, 2)
+    wp, wm, wd = b.get_particles()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    pr = ctx.Process(target=_nccl_rank, args=(_free_port(), n, q))
+    pr.start()
+    backend, calls, gp, gm, gd, total, real = q.get(timeout=240)
+    pr.join(60)
+    assert pr.exitcode == 0
+    assert backend == "nccl" and calls > 0
+    assert np.array_equal(gp[:, 6], wp[:, 6]) and np.array_equal(gm, wm) and np.array_equal(gd, wd)
+    assert 0 < int(wm.sum()) < n
+    assert total == b.get_total_num() and real == b.get_real_num()
+    for j in range(6):
+        assert rel_l2(gp[:, j], wp[:, j]) <= 1e-10, j
+
+
+@pytest.mark.gpu
+def test_device_exchange_failure_is_reported(syn):
+    """A device-buffer exchange whose collective fails makes the propagate
+    call return the library's error, not a silent result."""
+    n = 5000
+    p = gaussian_bunch(n, SIG_C0, 97)
+    lat, ref = product_lattice(fodo_cell())
+    prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(16, 16, 32), 8))
+
+    def broken(ptr, count):
+        raise RuntimeError("collective failed")
+    prop.set_allreduce(broken, on_host=False)
+    b = syn.Bunch(ref, n, 1e11)
+    b.set_particles(p)
+    with pytest.raises(syn.SB2Error, match="allreduce callback failed"):
+        prop.propagate(b, 1)
