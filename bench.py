@@ -269,7 +269,7 @@ def mixed_vs_fp64(syn, torch, steps, warmup, passes, seed=1):
     num = sum(float(((fields[1][c] - fields[0][c]) ** 2).sum()) for c in ("ex", "ey", "ez"))
     den = sum(float((fields[0][c] ** 2).sum()) for c in ("ex", "ey", "ez"))
     return {"value": rate, "unit": "macroparticle-steps/s", "ms_per_step": ms / steps,
-            "precision": "mixed (FP64 particles, maps, deposit and Green function; FP32 spectrum, potential, field)",
+            "precision": "mixed (FP64 particles, maps and Green function; FP32 charge grid from exact fixed-point tile sums; FP32 spectrum, potential, field; FP64 butterflies)",
             "field_rel_l2": math.sqrt(num / den), "field_tol": 1e-5,
             "emittance_rel_diff_xyz": demit, "emittance_tol": 1e-4, "passes": passes}
 

@@ -4,7 +4,7 @@
 // is handled by L/8 threads holding 8 complex values in registers; a pass of
 // radix R (8, 4 or 2) is 8/R butterflies per thread, done in registers, and
 // consecutive passes exchange their values through one shared-memory tile
-// (W x L complex FP64).  The first pass reads its inputs straight from global
+// (W x L complex values).  The first pass reads its inputs straight from global
 // memory and the last pass writes its outputs straight back, so a length-L
 // transform costs (passes - 1) shared-memory round trips and no extra global
 // traffic; a forward transform, a pointwise product and an inverse transform
@@ -27,33 +27,43 @@ namespace fft {
 
 constexpr int kE = 8; // complex values per thread
 
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+// Complex arithmetic in the transform's compute type: double2 (FP64 path) or
+// float2 (FP32 butterflies of the mixed-precision path).
+template <typename C> struct CxR;
+template <> struct CxR<double2> { typedef double R; };
+template <> struct CxR<float2> { typedef float R; };
+__device__ __forceinline__ double2 mk(double2, double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ float2 mk(float2, float a, float b) { return make_float2(a, b); }
+
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mk(a, a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mk(a, a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b)
 {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return mk(a, a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 // multiply by -i (forward) or +i (inverse)
-__device__ __forceinline__ double2 rot90(double2 a, bool inv) { return inv ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x); }
+template <typename C> __device__ __forceinline__ C rot90(C a, bool inv) { return inv ? mk(a, -a.y, a.x) : mk(a, a.y, -a.x); }
 
 // In-register DFT of size R in natural order: X[k] = sum_r v[r] w^(rk).
 template <int R>
 struct Dft;
 template <>
 struct Dft<2> {
-    static __device__ __forceinline__ void run(double2* v, bool)
+    template <typename C>
+    static __device__ __forceinline__ void run(C* v, bool)
     {
-        double2 a = v[0], b = v[1];
+        C a = v[0], b = v[1];
         v[0] = cadd(a, b);
         v[1] = csub(a, b);
     }
 };
 template <>
 struct Dft<4> {
-    static __device__ __forceinline__ void run(double2* v, bool inv)
+    template <typename C>
+    static __device__ __forceinline__ void run(C* v, bool inv)
     {
-        double2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
-        double2 s13 = cadd(v[1], v[3]), d13 = rot90(csub(v[1], v[3]), inv);
+        C s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+        C s13 = cadd(v[1], v[3]), d13 = rot90(csub(v[1], v[3]), inv);
         v[0] = cadd(s02, s13);
         v[2] = csub(s02, s13);
         v[1] = cadd(d02, d13);
@@ -62,21 +72,23 @@ struct Dft<4> {
 };
 template <>
 struct Dft<8> {
-    static __device__ __forceinline__ void run(double2* v, bool inv)
+    template <typename C>
+    static __device__ __forceinline__ void run(C* v, bool inv)
     {
-        const double h = 0.70710678118654752440; // cos(pi/4)
-        double2 a[4], b[4];
+        typedef typename CxR<C>::R R;
+        const R h = (R)0.70710678118654752440; // cos(pi/4)
+        C a[4], b[4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             a[r] = cadd(v[r], v[r + 4]);
             b[r] = csub(v[r], v[r + 4]);
         }
         // w8^r on the difference branch (decimation in frequency)
-        b[1] = inv ? make_double2(h * (b[1].x - b[1].y), h * (b[1].x + b[1].y))
-                   : make_double2(h * (b[1].x + b[1].y), h * (b[1].y - b[1].x));
+        b[1] = inv ? mk(b[1], h * (b[1].x - b[1].y), h * (b[1].x + b[1].y))
+                   : mk(b[1], h * (b[1].x + b[1].y), h * (b[1].y - b[1].x));
         b[2] = rot90(b[2], inv);
-        b[3] = inv ? make_double2(-h * (b[3].x + b[3].y), h * (b[3].x - b[3].y))
-                   : make_double2(h * (b[3].y - b[3].x), -h * (b[3].x + b[3].y));
+        b[3] = inv ? mk(b[3], -h * (b[3].x + b[3].y), h * (b[3].x - b[3].y))
+                   : mk(b[3], h * (b[3].y - b[3].x), -h * (b[3].x + b[3].y));
         Dft<4>::run(a, inv);
         Dft<4>::run(b, inv);
 #pragma unroll
@@ -151,8 +163,8 @@ struct XMajor {
 };
 
 // One pass's arithmetic on the registers: twiddles, then the butterflies.
-template <int L, int R>
-__device__ __forceinline__ void pass_math(double2* v, int t, int Ns, const double2* __restrict__ tw, bool inv)
+template <int L, int R, typename C>
+__device__ __forceinline__ void pass_math(C* v, int t, int Ns, const C* __restrict__ tw, bool inv)
 {
     constexpr int NB = kE / R;
     const int tstep = L / (Ns * R);
@@ -163,7 +175,7 @@ __device__ __forceinline__ void pass_math(double2* v, int t, int Ns, const doubl
         if (Ns > 1) {
 #pragma unroll
             for (int r = 1; r < R; ++r) {
-                double2 w = __ldg(&tw[(k * r * tstep) & (L - 1)]);
+                C w = __ldg(&tw[(k * r * tstep) & (L - 1)]);
                 if (inv) w.y = -w.y;
                 v[q * R + r] = cmul(v[q * R + r], w);
             }
@@ -173,8 +185,8 @@ __device__ __forceinline__ void pass_math(double2* v, int t, int Ns, const doubl
 }
 
 // Stores the registers of pass p (radix R, span Ns) at their output positions.
-template <int L, int R, class LAY>
-__device__ __forceinline__ void pass_store(const double2* v, int li, int t, int Ns, double2* sm)
+template <int L, int R, class LAY, typename C>
+__device__ __forceinline__ void pass_store(const C* v, int li, int t, int Ns, C* sm)
 {
     constexpr int NB = kE / R;
 #pragma unroll
@@ -188,8 +200,8 @@ __device__ __forceinline__ void pass_store(const double2* v, int li, int t, int 
 }
 
 // Loads the inputs of a pass of radix R (positions b + r L/R).
-template <int L, int R, class LAY>
-__device__ __forceinline__ void pass_load(double2* v, int li, int t, const double2* sm)
+template <int L, int R, class LAY, typename C>
+__device__ __forceinline__ void pass_load(C* v, int li, int t, const C* sm)
 {
     constexpr int NB = kE / R;
 #pragma unroll
@@ -212,21 +224,20 @@ __device__ __forceinline__ int io_pos(int t, int e)
 // The passes of one transform.  On entry v holds the first pass's inputs,
 // on return the last pass's outputs.  Every thread of the CTA calls it (it
 // synchronises the CTA).
-template <int L, bool REV, class LAY, int P = 0>
-__device__ __forceinline__ void run_passes(double2* v, int li, int t, double2* sm, const double2* __restrict__ tw,
-                                           bool inv)
+template <int L, bool REV, class LAY, int P = 0, typename C>
+__device__ __forceinline__ void run_passes(C* v, int li, int t, C* sm, const C* __restrict__ tw, bool inv)
 {
     if constexpr (P < npasses(L)) {
         constexpr int R = radix_at<L, REV>(P);
         constexpr int Ns = span_at<L, REV>(P);
-        pass_math<L, R>(v, t, Ns, tw, inv);
+        pass_math<L, R, C>(v, t, Ns, tw, inv);
         if constexpr (P + 1 < npasses(L)) {
             constexpr int R2 = radix_at<L, REV>(P + 1);
-            pass_store<L, R, LAY>(v, li, t, Ns, sm);
+            pass_store<L, R, LAY, C>(v, li, t, Ns, sm);
             __syncthreads();
-            pass_load<L, R2, LAY>(v, li, t, sm);
+            pass_load<L, R2, LAY, C>(v, li, t, sm);
             __syncthreads();
-            run_passes<L, REV, LAY, P + 1>(v, li, t, sm, tw, inv);
+            run_passes<L, REV, LAY, P + 1, C>(v, li, t, sm, tw, inv);
         }
     }
 }

@@ -1852,10 +1852,19 @@ struct SpaceCharge {
     double* phi = nullptr;
     double2* E = nullptr;
     double2 *tw_x = nullptr, *tw_y = nullptr, *tw_z = nullptr;
-    // mixed precision: FP32 spectrum, potential and field
+    // mixed precision: FP32 charge grid (FP64 when the charge is exchanged
+    // between ranks), spectrum, potential and field; FP64 butterflies.
+    // SB2_MIXED_BUTTERFLIES=fp32 selects FP32 butterflies: 3% faster on the
+    // 4M-particle FODO step but 1.0e-5 / 1.8e-5 field error at 64^2 x 128 /
+    // 128^2 x 256 (the finite-difference field magnifies the transforms'
+    // rounding about 100x), against 4.4e-6 / 7.0e-6 with FP64 butterflies
+    float* rho32 = nullptr;
     float2* S32 = nullptr;
     float* phi32 = nullptr;
     float4* E32 = nullptr;
+    float2 *tw32_x = nullptr, *tw32_y = nullptr, *tw32_z = nullptr;
+    int fp32_butterflies = 0;
+    bool last_rho32 = false; // the last solve's charge is in rho32
     ScState* state = nullptr;
     double* mom_partials = nullptr;
     int n_partials = 0;
@@ -1896,13 +1905,14 @@ struct SpaceCharge {
         d.lz = ilog2(d.nz);
         G = (int64_t)d.gx * d.gy * d.gz;
         mixed = o.precision == SB2_PRECISION_MIXED;
-        rho = dalloc<double>(G, "rho");
         if (mixed) {
+            rho32 = dalloc<float>(G, "rho");
             phi32 = dalloc<float>(G, "phi");
             E32 = dalloc<float4>(G, "E");
             S32 = dalloc<float2>((size_t)d.nz * d.ny * d.nkxp, "spectrum");
             cuda_check(cudaMemset(E32, 0, sizeof(float4) * G), "memset");
         } else {
+            rho = dalloc<double>(G, "rho");
             phi = dalloc<double>(G, "phi");
             E = dalloc<double2>(2 * G, "E");
             S = dalloc<double2>((size_t)d.nz * d.ny * d.nkxp, "spectrum");
@@ -1916,6 +1926,13 @@ struct SpaceCharge {
         tw_x = twiddles(d.nx);
         tw_y = twiddles(d.ny);
         tw_z = twiddles(d.nz);
+        if (mixed) {
+            tw32_x = twiddles32(d.nx);
+            tw32_y = twiddles32(d.ny);
+            tw32_z = twiddles32(d.nz);
+            const char* e = getenv("SB2_MIXED_BUTTERFLIES");
+            if (e && !strcmp(e, "fp32")) fp32_butterflies = 1;
+        }
     }
     ~SpaceCharge()
     {
@@ -1932,6 +1949,10 @@ struct SpaceCharge {
         dfree(S32);
         dfree(phi32);
         dfree(E32);
+        dfree(rho32);
+        dfree(tw32_x);
+        dfree(tw32_y);
+        dfree(tw32_z);
     }
     // exp(-2 pi i k / L), k < L, from long-double sin/cos
     static double2* twiddles(int L)
@@ -1943,6 +1964,18 @@ struct SpaceCharge {
         }
         double2* dp = dalloc<double2>(L, "twiddles");
         cuda_check(cudaMemcpy(dp, h.data(), sizeof(double2) * L, cudaMemcpyHostToDevice), "twiddles");
+        return dp;
+    }
+    // the same in FP32, each rounded once from the long-double value
+    static float2* twiddles32(int L)
+    {
+        std::vector<float2> h(L);
+        for (int k = 0; k < L; ++k) {
+            long double a = -2.0L * 3.14159265358979323846264338327950288L * k / L;
+            h[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        float2* dp = dalloc<float2>(L, "twiddles");
+        cuda_check(cudaMemcpy(dp, h.data(), sizeof(float2) * L, cudaMemcpyHostToDevice), "twiddles");
         return dp;
     }
 
@@ -1987,12 +2020,22 @@ struct SpaceCharge {
             if (refresh) ghat_valid = true;
             return;
         }
+        const bool exchange = hook && *hook;
+        last_rho32 = mixed && !exchange;
         {
             ProfScope ps(PROF_DEPOSIT, s);
-            cuda_check(cudaMemsetAsync(rho, 0, sizeof(double) * G, s), "memset rho");
-            cuda_check(launch_deposit(b.parts, b.stride, b.masks, b.n, state, rho, d.gx, d.gy, d.gz, s), "deposit");
+            if (last_rho32) {
+                cuda_check(cudaMemsetAsync(rho32, 0, sizeof(float) * G, s), "memset rho");
+                cuda_check(launch_deposit_f32(b.parts, b.stride, b.masks, b.n, state, rho32, d.gx, d.gy, d.gz, s),
+                           "deposit");
+            } else {
+                if (!rho) rho = dalloc<double>(G, "rho"); // mixed precision with an exchange: FP64 charge
+                cuda_check(cudaMemsetAsync(rho, 0, sizeof(double) * G, s), "memset rho");
+                cuda_check(launch_deposit(b.parts, b.stride, b.masks, b.n, state, rho, d.gx, d.gy, d.gz, s),
+                           "deposit");
+            }
         }
-        if (hook && *hook) hook->run(rho, G, s); // charge of all ranks
+        if (exchange) hook->run(rho, G, s); // charge of all ranks
         if (!o.domain_fixed || !ghat_valid) {
             ProfScope ps(PROF_GREEN, s);
             cuda_check(launch_green(state, ghat, d, o.green_fn == SB2_GREEN_LINEAR, tw_x, tw_y, tw_z, s), "green");
@@ -2000,9 +2043,19 @@ struct SpaceCharge {
         }
         {
             ProfScope ps(PROF_SOLVE, s);
-            if (mixed)
-                cuda_check(launch_convolve_f32(rho, S32, ghat, phi32, d, tw_x, tw_y, tw_z, state, s), "convolve");
-            else
+            if (mixed) {
+                MixedConv m;
+                m.rho32 = last_rho32 ? rho32 : nullptr;
+                m.rho64 = last_rho32 ? nullptr : rho;
+                m.tw64[0] = tw_x;
+                m.tw64[1] = tw_y;
+                m.tw64[2] = tw_z;
+                m.tw32[0] = tw32_x;
+                m.tw32[1] = tw32_y;
+                m.tw32[2] = tw32_z;
+                m.fp32_butterflies = fp32_butterflies;
+                cuda_check(launch_convolve_mixed(m, S32, ghat, phi32, d, state, s), "convolve");
+            } else
                 cuda_check(launch_convolve(rho, S, ghat, phi, d, tw_x, tw_y, tw_z, state, s), "convolve");
         }
         {
@@ -2023,7 +2076,15 @@ struct SpaceCharge {
             for (int i = 0; i < 3; ++i) left[i] = st.left[i];
         if (h)
             for (int i = 0; i < 3; ++i) h[i] = st.h[i];
-        if (rho_o) cuda_check(cudaMemcpy(rho_o, rho, sizeof(double) * G, cudaMemcpyDeviceToHost), "rho");
+        if (rho_o) {
+            if (last_rho32) {
+                std::vector<float> f(G);
+                cuda_check(cudaMemcpy(f.data(), rho32, sizeof(float) * G, cudaMemcpyDeviceToHost), "rho");
+                for (int64_t i = 0; i < G; ++i) rho_o[i] = f[i];
+            } else if (rho) {
+                cuda_check(cudaMemcpy(rho_o, rho, sizeof(double) * G, cudaMemcpyDeviceToHost), "rho");
+            }
+        }
         if (phi_o) {
             if (mixed) {
                 std::vector<float> f(G);

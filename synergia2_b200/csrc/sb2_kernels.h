@@ -113,15 +113,28 @@ cudaError_t launch_shard_count(const BunchCounters* c, double* xchg, cudaStream_
 cudaError_t launch_shard_total(BunchCounters* c, const double* xchg, cudaStream_t s);
 cudaError_t launch_deposit(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
                            const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s);
+// the same deposit into an FP32 charge grid (the tiles' sums are exact; only
+// the merge of neighbouring tiles rounds to FP32)
+cudaError_t launch_deposit_f32(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
+                               const ScState* sc, float* rho, int gx, int gy, int gz, cudaStream_t s);
 cudaError_t launch_green(const ScState* sc, double* G, const Dims& d, int linear, const double2* tw_x,
                          const double2* tw_y, const double2* tw_z, cudaStream_t s);
 cudaError_t launch_convolve(const double* rho, double2* S, const double* Ghat, double* phi, const Dims& d,
                             const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
                             cudaStream_t s);
 cudaError_t launch_efield(const double* phi, double2* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s);
-cudaError_t launch_convolve_f32(const double* rho, float2* S, const double* Ghat, float* phi, const Dims& d,
-                                const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
-                                cudaStream_t s);
+// inputs of the mixed-precision convolution: the charge density in FP32
+// (rho32) or FP64 (rho64, the other null), the twiddles of the x, y, z
+// lengths in both precisions, and the butterflies' precision
+struct MixedConv {
+    const float* rho32;
+    const double* rho64;
+    const double2* tw64[3];
+    const float2* tw32[3];
+    int32_t fp32_butterflies;
+};
+cudaError_t launch_convolve_mixed(const MixedConv& m, float2* S, const double* Ghat, float* phi, const Dims& d,
+                                  const ScState* sc, cudaStream_t s);
 cudaError_t launch_efield_f32(const float* phi, float4* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s);
 // sort.cu
 size_t sort_scratch_ints(int64_t G);

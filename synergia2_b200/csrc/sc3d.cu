@@ -389,10 +389,10 @@ __device__ __forceinline__ void tile_add(DepositSmem<K>& sm, int at, double u, d
     atomicAdd(&sm.d2[at], (uint32_t)(q >> 42));
 }
 
-template <int K>
+template <int K, typename RT>
 __global__ void __launch_bounds__(kDepT) deposit_tile_kernel(const double* __restrict__ parts, int64_t stride,
                                                              const uint8_t* __restrict__ masks, int64_t n,
-                                                             const ScState* __restrict__ scp, double* rho, int gx,
+                                                             const ScState* __restrict__ scp, RT* rho, int gx,
                                                              int gy, int gz)
 {
     extern __shared__ __align__(16) unsigned char dep_raw[];
@@ -518,7 +518,7 @@ __global__ void __launch_bounds__(kDepT) deposit_tile_kernel(const double* __res
             const int X = bmin[0] + (v - r * BX), Y = bmin[1] + (r % BY), Z = bmin[2] + r / BY;
             if (X > 0 && X < gx - 1 && Y > 0 && Y < gy - 1 && Z > 0 && Z < gz - 1) {
                 const double sum = ((double)a2 * 4398046511104.0 + (double)a1 * 2097152.0) + (double)a0;
-                atomicAdd(&rho[((int64_t)Z * gy + Y) * gx + X], sum * back);
+                atomicAdd(&rho[((int64_t)Z * gy + Y) * gx + X], (RT)(sum * back));
             }
         }
         return;
@@ -540,16 +540,16 @@ __global__ void __launch_bounds__(kDepT) deposit_tile_kernel(const double* __res
         const int64_t b0 = (int64_t)iz * gx * gy + (int64_t)iy * gx + ix;
         const int64_t P = (int64_t)gx * gy;
         if (z0) {
-            if (y0 && x0) atomicAdd(&rho[b0], w[0]);
-            if (y0 && x1) atomicAdd(&rho[b0 + 1], w[1]);
-            if (y1 && x0) atomicAdd(&rho[b0 + gx], w[2]);
-            if (y1 && x1) atomicAdd(&rho[b0 + gx + 1], w[3]);
+            if (y0 && x0) atomicAdd(&rho[b0], (RT)w[0]);
+            if (y0 && x1) atomicAdd(&rho[b0 + 1], (RT)w[1]);
+            if (y1 && x0) atomicAdd(&rho[b0 + gx], (RT)w[2]);
+            if (y1 && x1) atomicAdd(&rho[b0 + gx + 1], (RT)w[3]);
         }
         if (z1) {
-            if (y0 && x0) atomicAdd(&rho[b0 + P], w[4]);
-            if (y0 && x1) atomicAdd(&rho[b0 + P + 1], w[5]);
-            if (y1 && x0) atomicAdd(&rho[b0 + P + gx], w[6]);
-            if (y1 && x1) atomicAdd(&rho[b0 + P + gx + 1], w[7]);
+            if (y0 && x0) atomicAdd(&rho[b0 + P], (RT)w[4]);
+            if (y0 && x1) atomicAdd(&rho[b0 + P + 1], (RT)w[5]);
+            if (y1 && x0) atomicAdd(&rho[b0 + P + gx], (RT)w[6]);
+            if (y1 && x1) atomicAdd(&rho[b0 + P + gx + 1], (RT)w[7]);
         }
     }
 }
@@ -634,50 +634,55 @@ __global__ void green_octant_kernel(const ScState* __restrict__ scp, double* G, 
 
 // ---------------------------------------------------------------------------
 // Line passes of the convolution (register-resident FFT, fft.cuh).  Global
-// storage of the spectrum is C (double2, or float2 for the mixed path);
-// every pass computes in FP64 in registers and shared memory, so the mixed
-// path only rounds at the five pass boundaries.
+// storage of the spectrum is C (double2, or float2 for the mixed path); the
+// butterflies, the twiddles and the shared-memory exchanges are in W
+// (double2, or float2 for FP32 butterflies).  FP64 storage with FP64
+// butterflies is the drop-in; float2 storage rounds only at the five pass
+// boundaries when W is double2.
 // ---------------------------------------------------------------------------
 template <typename C> struct CxT;
 template <> struct CxT<double2> { typedef double R; };
 template <> struct CxT<float2> { typedef float R; };
-__device__ __forceinline__ double2 to_d(double2 v) { return v; }
-__device__ __forceinline__ double2 to_d(float2 v) { return make_double2(v.x, v.y); }
-template <typename C> __device__ __forceinline__ C from_d(double2 v);
-template <> __device__ __forceinline__ double2 from_d<double2>(double2 v) { return v; }
-template <> __device__ __forceinline__ float2 from_d<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+template <typename W> __device__ __forceinline__ W cvt_c(double2 v);
+template <typename W> __device__ __forceinline__ W cvt_c(float2 v);
+template <> __device__ __forceinline__ double2 cvt_c<double2>(double2 v) { return v; }
+template <> __device__ __forceinline__ double2 cvt_c<double2>(float2 v) { return make_double2(v.x, v.y); }
+template <> __device__ __forceinline__ float2 cvt_c<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+template <> __device__ __forceinline__ float2 cvt_c<float2>(float2 v) { return v; }
+template <typename W> __device__ __forceinline__ W czero() { return cvt_c<W>(make_double2(0.0, 0.0)); }
 
 // XF: pairs of real rows (y, y+1) of rho -> S rows (r2c, first gx inputs).
 // Lines l = (pair, z); the last pass goes through shared memory so that
 // each output k can combine Z[k] and Z[L-k].
-template <int L, typename C>
-__global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xf_kernel(const double* __restrict__ rho, C* S,
-                                                                        const double2* __restrict__ tw, Dims d,
+template <int L, typename RI, typename C, typename W>
+__global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xf_kernel(const RI* __restrict__ rho, C* S,
+                                                                        const W* __restrict__ tw, Dims d,
                                                                         const ScState* __restrict__ scp)
 {
     typedef fft::XMajor<L> LAY;
-    constexpr int W = fft::Shape<L>::W, TPL = fft::Shape<L>::TPL;
+    typedef typename CxT<W>::R R;
+    constexpr int NW = fft::Shape<L>::W, TPL = fft::Shape<L>::TPL;
     constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    double2* sm = (double2*)sm_raw;
+    W* sm = (W*)sm_raw;
     if (!scp->valid) return;
     const int li = LAY::line(), t = LAY::thr();
     const int npy = (d.gy + 1) / 2;
     const int64_t nlines = (int64_t)npy * d.gz;
-    const int64_t l = (int64_t)blockIdx.x * W + li;
+    const int64_t l = (int64_t)blockIdx.x * NW + li;
     const bool ok = l < nlines;
     const int pr = ok ? (int)(l % npy) : 0, z = ok ? (int)(l / npy) : 0;
     const int ya = 2 * pr, yb = ya + 1;
-    const double* ra = rho + ((int64_t)z * d.gy + ya) * d.gx;
-    const double* rb = rho + ((int64_t)z * d.gy + yb) * d.gx;
-    double2 v[fft::kE];
+    const RI* ra = rho + ((int64_t)z * d.gy + ya) * d.gx;
+    const RI* rb = rho + ((int64_t)z * d.gy + yb) * d.gx;
+    W v[fft::kE];
 #pragma unroll
     for (int e = 0; e < fft::kE; ++e) {
         const int pos = fft::io_pos<L, R0>(t, e);
-        v[e] = make_double2(0.0, 0.0);
+        v[e] = czero<W>();
         if (ok && pos < d.gx) {
-            v[e].x = ra[pos];
-            if (yb < d.gy) v[e].y = rb[pos];
+            v[e].x = (R)ra[pos];
+            if (yb < d.gy) v[e].y = (R)rb[pos];
         }
     }
     fft::run_passes<L, false, LAY>(v, li, t, sm, tw, false);
@@ -687,35 +692,36 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xf_kernel(const do
     if (!ok) return;
     C* sa = S + ((int64_t)z * d.ny + ya) * d.nkxp;
     C* sb = S + ((int64_t)z * d.ny + yb) * d.nkxp;
+    const R half = (R)0.5;
     for (int k = t; k < d.nkx; k += TPL) {
-        const double2 Z = sm[LAY::at(li, k)], Zn = sm[LAY::at(li, (L - k) & (L - 1))];
-        sa[k] = from_d<C>(make_double2((Z.x + Zn.x) * 0.5, (Z.y - Zn.y) * 0.5));
-        if (yb < d.gy) sb[k] = from_d<C>(make_double2((Z.y + Zn.y) * 0.5, -(Z.x - Zn.x) * 0.5));
+        const W Z = sm[LAY::at(li, k)], Zn = sm[LAY::at(li, (L - k) & (L - 1))];
+        sa[k] = cvt_c<C>(fft::mk(Z, (Z.x + Zn.x) * half, (Z.y - Zn.y) * half));
+        if (yb < d.gy) sb[k] = cvt_c<C>(fft::mk(Z, (Z.y + Zn.y) * half, -(Z.x - Zn.x) * half));
     }
 }
 
-// Y passes: lines (kx, z < gz) along y, W consecutive kx per CTA.  forward:
+// Y passes: lines (kx, z < gz) along y, NW consecutive kx per CTA.  forward:
 // first gy inputs, all ny outputs; inverse: all inputs, first gy outputs.
-template <int L, typename C, bool INV>
-__global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_y_kernel(C* S, const double2* __restrict__ tw, Dims d,
+template <int L, typename C, typename W, bool INV>
+__global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_y_kernel(C* S, const W* __restrict__ tw, Dims d,
                                                                        const ScState* __restrict__ scp)
 {
     typedef fft::LMajor<L> LAY;
-    constexpr int W = fft::Shape<L>::W;
+    constexpr int NW = fft::Shape<L>::W;
     constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    double2* sm = (double2*)sm_raw;
+    W* sm = (W*)sm_raw;
     if (!scp->valid) return;
     const int li = LAY::line(), t = LAY::thr();
-    const int kx = blockIdx.x * W + li, z = blockIdx.y;
+    const int kx = blockIdx.x * NW + li, z = blockIdx.y;
     const bool ok = kx < d.nkx;
     C* col = S + (int64_t)z * d.ny * d.nkxp + kx;
     const int nin = INV ? L : d.gy;
-    double2 v[fft::kE];
+    W v[fft::kE];
 #pragma unroll
     for (int e = 0; e < fft::kE; ++e) {
         const int pos = fft::io_pos<L, R0>(t, e);
-        v[e] = (ok && pos < nin) ? to_d(col[(int64_t)pos * d.nkxp]) : make_double2(0.0, 0.0);
+        v[e] = (ok && pos < nin) ? cvt_c<W>(col[(int64_t)pos * d.nkxp]) : czero<W>();
     }
     fft::run_passes<L, false, LAY>(v, li, t, sm, tw, INV);
     if (!ok) return;
@@ -723,7 +729,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_y_kernel(C* S, con
 #pragma unroll
     for (int e = 0; e < fft::kE; ++e) {
         const int pos = fft::io_pos<L, RL>(t, e);
-        if (pos < nout) col[(int64_t)pos * d.nkxp] = from_d<C>(v[e]);
+        if (pos < nout) col[(int64_t)pos * d.nkxp] = cvt_c<C>(v[e]);
     }
 }
 
@@ -732,28 +738,29 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_y_kernel(C* S, con
 // (radices reversed, so it starts from the registers), first gz outputs.
 // (alg_cplx_multiplier space_charge_3d_open_hockney.cc:350-372 fused between
 // the transforms.)
-template <int L, typename C>
+template <int L, typename C, typename W>
 __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_z_conv_kernel(C* S, const double* __restrict__ Ghat,
-                                                                            const double2* __restrict__ tw, Dims d,
+                                                                            const W* __restrict__ tw, Dims d,
                                                                             const ScState* __restrict__ scp)
 {
     typedef fft::LMajor<L> LAY;
-    constexpr int W = fft::Shape<L>::W;
+    typedef typename CxT<W>::R R;
+    constexpr int NW = fft::Shape<L>::W;
     constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
     constexpr int RI = fft::last_radix<L, true>();
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    double2* sm = (double2*)sm_raw;
+    W* sm = (W*)sm_raw;
     if (!scp->valid) return;
     const int li = LAY::line(), t = LAY::thr();
-    const int kx = blockIdx.x * W + li, ky = blockIdx.y;
+    const int kx = blockIdx.x * NW + li, ky = blockIdx.y;
     const bool ok = kx < d.nkx;
     C* col = S + (int64_t)ky * d.nkxp + kx;
     const int64_t zs = (int64_t)d.ny * d.nkxp;
-    double2 v[fft::kE];
+    W v[fft::kE];
 #pragma unroll
     for (int e = 0; e < fft::kE; ++e) {
         const int pos = fft::io_pos<L, R0>(t, e);
-        v[e] = (ok && pos < d.gz) ? to_d(col[pos * zs]) : make_double2(0.0, 0.0);
+        v[e] = (ok && pos < d.gz) ? cvt_c<W>(col[pos * zs]) : czero<W>();
     }
     fft::run_passes<L, false, LAY>(v, li, t, sm, tw, false);
     const int ogx = d.nx / 2 + 1, ogy = d.ny / 2 + 1;
@@ -763,61 +770,61 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_z_conv_kernel(C* S
     for (int e = 0; e < fft::kE; ++e) {
         const int kz = fft::io_pos<L, RL>(t, e);
         const int mz = kz <= L / 2 ? kz : L - kz;
-        const double g = ok ? __ldg(&gcol[(int64_t)mz * ogy * ogx]) : 0.0;
-        v[e] = make_double2(v[e].x * g, v[e].y * g);
+        const R g = ok ? (R)__ldg(&gcol[(int64_t)mz * ogy * ogx]) : (R)0;
+        v[e] = fft::mk(v[e], v[e].x * g, v[e].y * g);
     }
     fft::run_passes<L, true, LAY>(v, li, t, sm, tw, true);
     if (!ok) return;
 #pragma unroll
     for (int e = 0; e < fft::kE; ++e) {
         const int pos = fft::io_pos<L, RI>(t, e);
-        if (pos < d.gz) col[pos * zs] = from_d<C>(v[e]);
+        if (pos < d.gz) col[pos * zs] = cvt_c<C>(v[e]);
     }
 }
 
 // XI: Hermitian pairs of spectrum rows -> real rows (y, y+1) of phi (c2r,
 // first gx outputs); imaginary parts of the k = 0 and k = nx/2 terms are
 // ignored as a c2r transform does.
-template <int L, typename C, typename RO>
+template <int L, typename C, typename W, typename RO>
 __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xi_kernel(const C* __restrict__ S, RO* phi,
-                                                                        const double2* __restrict__ tw, Dims d,
+                                                                        const W* __restrict__ tw, Dims d,
                                                                         const ScState* __restrict__ scp)
 {
     typedef fft::XMajor<L> LAY;
-    constexpr int W = fft::Shape<L>::W;
+    constexpr int NW = fft::Shape<L>::W;
     constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    double2* sm = (double2*)sm_raw;
+    W* sm = (W*)sm_raw;
     if (!scp->valid) return;
     const int li = LAY::line(), t = LAY::thr();
     const int npy = (d.gy + 1) / 2;
     const int64_t nlines = (int64_t)npy * d.gz;
-    const int64_t l = (int64_t)blockIdx.x * W + li;
+    const int64_t l = (int64_t)blockIdx.x * NW + li;
     const bool ok = l < nlines;
     const int pr = ok ? (int)(l % npy) : 0, z = ok ? (int)(l / npy) : 0;
     const int ya = 2 * pr, yb = ya + 1;
     const C* sa = S + ((int64_t)z * d.ny + ya) * d.nkxp;
     const C* sb = S + ((int64_t)z * d.ny + yb) * d.nkxp;
     constexpr int half = L / 2;
-    double2 v[fft::kE];
+    W v[fft::kE];
 #pragma unroll
     for (int e = 0; e < fft::kE; ++e) {
         const int j = fft::io_pos<L, R0>(t, e);
         const int k = j <= half ? j : L - j;
-        double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
+        W A = czero<W>(), B = czero<W>();
         if (ok) {
-            A = to_d(sa[k]);
-            if (yb < d.gy) B = to_d(sb[k]);
+            A = cvt_c<W>(sa[k]);
+            if (yb < d.gy) B = cvt_c<W>(sb[k]);
         }
         if (k == 0 || k == half) {
-            A.y = 0.0;
-            B.y = 0.0;
+            A.y = 0;
+            B.y = 0;
         }
         if (j > half) {
             A.y = -A.y;
             B.y = -B.y;
         }
-        v[e] = make_double2(A.x - B.y, A.y + B.x);
+        v[e] = fft::mk(A, A.x - B.y, A.y + B.x);
     }
     fft::run_passes<L, false, LAY>(v, li, t, sm, tw, true);
     if (!ok) return;
@@ -989,17 +996,18 @@ cudaError_t launch_book_domain(const DomainParams& p, cudaStream_t s)
 #ifndef SB2_DEPOSIT_CTAS
 #define SB2_DEPOSIT_CTAS 8 // CTAs per SM of the grid-stride deposit (5 / 8 / 16: 0.163 / 0.142 / 0.146 ms per C1 step)
 #endif
-template <int K>
+template <int K, typename RT>
 static cudaError_t deposit_tile(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
-                                const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s)
+                                const ScState* sc, RT* rho, int gx, int gy, int gz, cudaStream_t s)
 {
     const int bytes = (int)sizeof(DepositSmem<K>);
     static cudaError_t once =
-        cudaFuncSetAttribute(deposit_tile_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(deposit_tile_kernel<K, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (once) return once;
     const int64_t chunk = (int64_t)kDepT * K;
     const int64_t nb = (n + chunk - 1) / chunk;
-    if (nb > 0) deposit_tile_kernel<K><<<(unsigned)nb, kDepT, bytes, s>>>(parts, stride, masks, n, sc, rho, gx, gy, gz);
+    if (nb > 0)
+        deposit_tile_kernel<K, RT><<<(unsigned)nb, kDepT, bytes, s>>>(parts, stride, masks, n, sc, rho, gx, gy, gz);
     return cudaGetLastError();
 }
 
@@ -1021,12 +1029,18 @@ cudaError_t launch_deposit(const double* parts, int64_t stride, const uint8_t* m
                            const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s)
 {
     switch (deposit_variant()) {
-    case 4: return deposit_tile<4>(parts, stride, masks, n, sc, rho, gx, gy, gz, s);
-    case 8: return deposit_tile<8>(parts, stride, masks, n, sc, rho, gx, gy, gz, s);
+    case 4: return deposit_tile<4, double>(parts, stride, masks, n, sc, rho, gx, gy, gz, s);
+    case 8: return deposit_tile<8, double>(parts, stride, masks, n, sc, rho, gx, gy, gz, s);
     default:
         deposit_kernel<<<sm_count() * SB2_DEPOSIT_CTAS, 256, 0, s>>>(parts, stride, masks, n, sc, rho, gx, gy, gz);
         return cudaGetLastError();
     }
+}
+
+cudaError_t launch_deposit_f32(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
+                               const ScState* sc, float* rho, int gx, int gy, int gz, cudaStream_t s)
+{
+    return deposit_tile<4, float>(parts, stride, masks, n, sc, rho, gx, gy, gz, s);
 }
 
 static inline int ceil_div64(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
@@ -1090,61 +1104,61 @@ cudaError_t launch_green(const ScState* sc, double* G, const Dims& d, int linear
     return cudaGetLastError();
 }
 
-template <int L, typename C>
-static cudaError_t pass_xf(const double* rho, C* S, const double2* tw, const Dims& d, const ScState* sc, cudaStream_t s)
+template <int L, typename RI, typename C, typename W>
+static cudaError_t pass_xf(const RI* rho, C* S, const W* tw, const Dims& d, const ScState* sc, cudaStream_t s)
 {
-    const int bytes = fft::XMajor<L>::kSmemElems * 16;
-    static cudaError_t once = fft_smem(fft_xf_kernel<L, C>, bytes);
+    const int bytes = fft::XMajor<L>::kSmemElems * (int)sizeof(W);
+    static cudaError_t once = fft_smem(fft_xf_kernel<L, RI, C, W>, bytes);
     if (once) return once;
     const int64_t nlines = (int64_t)((d.gy + 1) / 2) * d.gz;
-    fft_xf_kernel<L, C><<<ceil_div64(nlines, fft::Shape<L>::W), fft::Shape<L>::THREADS, bytes, s>>>(rho, S, tw, d, sc);
+    fft_xf_kernel<L, RI, C, W><<<ceil_div64(nlines, fft::Shape<L>::W), fft::Shape<L>::THREADS, bytes, s>>>(rho, S, tw, d,
+                                                                                                           sc);
     return cudaSuccess;
 }
-template <int L, typename C, bool INV>
-static cudaError_t pass_y(C* S, const double2* tw, const Dims& d, const ScState* sc, cudaStream_t s)
+template <int L, typename C, typename W, bool INV>
+static cudaError_t pass_y(C* S, const W* tw, const Dims& d, const ScState* sc, cudaStream_t s)
 {
-    const int bytes = fft::LMajor<L>::kSmemElems * 16;
-    static cudaError_t once = fft_smem(fft_y_kernel<L, C, INV>, bytes);
+    const int bytes = fft::LMajor<L>::kSmemElems * (int)sizeof(W);
+    static cudaError_t once = fft_smem(fft_y_kernel<L, C, W, INV>, bytes);
     if (once) return once;
     dim3 grid(ceil_div64(d.nkx, fft::Shape<L>::W), d.gz);
-    fft_y_kernel<L, C, INV><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, tw, d, sc);
+    fft_y_kernel<L, C, W, INV><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, tw, d, sc);
     return cudaSuccess;
 }
-template <int L, typename C>
-static cudaError_t pass_z(C* S, const double* Ghat, const double2* tw, const Dims& d, const ScState* sc, cudaStream_t s)
+template <int L, typename C, typename W>
+static cudaError_t pass_z(C* S, const double* Ghat, const W* tw, const Dims& d, const ScState* sc, cudaStream_t s)
 {
-    const int bytes = fft::LMajor<L>::kSmemElems * 16;
-    static cudaError_t once = fft_smem(fft_z_conv_kernel<L, C>, bytes);
+    const int bytes = fft::LMajor<L>::kSmemElems * (int)sizeof(W);
+    static cudaError_t once = fft_smem(fft_z_conv_kernel<L, C, W>, bytes);
     if (once) return once;
     dim3 grid(ceil_div64(d.nkx, fft::Shape<L>::W), d.ny);
-    fft_z_conv_kernel<L, C><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, Ghat, tw, d, sc);
+    fft_z_conv_kernel<L, C, W><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, Ghat, tw, d, sc);
     return cudaSuccess;
 }
-template <int L, typename C>
-static cudaError_t pass_xi(const C* S, typename CxT<C>::R* phi, const double2* tw, const Dims& d, const ScState* sc,
+template <int L, typename C, typename W>
+static cudaError_t pass_xi(const C* S, typename CxT<C>::R* phi, const W* tw, const Dims& d, const ScState* sc,
                            cudaStream_t s)
 {
     typedef typename CxT<C>::R RO;
-    const int bytes = fft::XMajor<L>::kSmemElems * 16;
-    static cudaError_t once = fft_smem(fft_xi_kernel<L, C, RO>, bytes);
+    const int bytes = fft::XMajor<L>::kSmemElems * (int)sizeof(W);
+    static cudaError_t once = fft_smem(fft_xi_kernel<L, C, W, RO>, bytes);
     if (once) return once;
     const int64_t nlines = (int64_t)((d.gy + 1) / 2) * d.gz;
-    fft_xi_kernel<L, C, RO><<<ceil_div64(nlines, fft::Shape<L>::W), fft::Shape<L>::THREADS, bytes, s>>>(S, phi, tw, d,
-                                                                                                       sc);
+    fft_xi_kernel<L, C, W, RO><<<ceil_div64(nlines, fft::Shape<L>::W), fft::Shape<L>::THREADS, bytes, s>>>(S, phi, tw,
+                                                                                                          d, sc);
     return cudaSuccess;
 }
 
-template <typename C>
-static cudaError_t convolve_t(const double* rho, C* S, const double* Ghat, typename CxT<C>::R* phi, const Dims& d,
-                              const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
-                              cudaStream_t s)
+template <typename RI, typename C, typename W>
+static cudaError_t convolve_t(const RI* rho, C* S, const double* Ghat, typename CxT<C>::R* phi, const Dims& d,
+                              const W* tw_x, const W* tw_y, const W* tw_z, const ScState* sc, cudaStream_t s)
 {
     cudaError_t e = cudaSuccess;
-#define SB2_XF(LL) case LL: e = pass_xf<LL, C>(rho, S, tw_x, d, sc, s); break;
-#define SB2_YF(LL) case LL: e = pass_y<LL, C, false>(S, tw_y, d, sc, s); break;
-#define SB2_ZC(LL) case LL: e = pass_z<LL, C>(S, Ghat, tw_z, d, sc, s); break;
-#define SB2_YI(LL) case LL: e = pass_y<LL, C, true>(S, tw_y, d, sc, s); break;
-#define SB2_XI(LL) case LL: e = pass_xi<LL, C>(S, phi, tw_x, d, sc, s); break;
+#define SB2_XF(LL) case LL: e = pass_xf<LL, RI, C, W>(rho, S, tw_x, d, sc, s); break;
+#define SB2_YF(LL) case LL: e = pass_y<LL, C, W, false>(S, tw_y, d, sc, s); break;
+#define SB2_ZC(LL) case LL: e = pass_z<LL, C, W>(S, Ghat, tw_z, d, sc, s); break;
+#define SB2_YI(LL) case LL: e = pass_y<LL, C, W, true>(S, tw_y, d, sc, s); break;
+#define SB2_XI(LL) case LL: e = pass_xi<LL, C, W>(S, phi, tw_x, d, sc, s); break;
     switch (d.nx) { SB2_FFT_LENGTHS(SB2_XF) default: return cudaErrorInvalidValue; }
     if (e) return e;
     switch (d.ny) { SB2_FFT_LENGTHS(SB2_YF) default: return cudaErrorInvalidValue; }
@@ -1168,16 +1182,23 @@ cudaError_t launch_convolve(const double* rho, double2* S, const double* Ghat, d
                             const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
                             cudaStream_t s)
 {
-    return convolve_t<double2>(rho, S, Ghat, phi, d, tw_x, tw_y, tw_z, sc, s);
+    return convolve_t<double, double2, double2>(rho, S, Ghat, phi, d, tw_x, tw_y, tw_z, sc, s);
 }
 
-// rho (FP64 accumulation) -> phi in FP32 (mixed precision: FP32 spectrum
-// and potential storage, FP64 butterflies).
-cudaError_t launch_convolve_f32(const double* rho, float2* S, const double* Ghat, float* phi, const Dims& d,
-                                const double2* tw_x, const double2* tw_y, const double2* tw_z, const ScState* sc,
-                                cudaStream_t s)
+// Mixed precision: rho (FP32, or FP64 where the charge is exchanged between
+// ranks) -> phi in FP32 with an FP32 spectrum; butterflies in FP32 (float2
+// twiddles rounded from long double) or FP64 (double2 twiddles).
+cudaError_t launch_convolve_mixed(const MixedConv& m, float2* S, const double* Ghat, float* phi, const Dims& d,
+                                  const ScState* sc, cudaStream_t s)
 {
-    return convolve_t<float2>(rho, S, Ghat, phi, d, tw_x, tw_y, tw_z, sc, s);
+    if (m.fp32_butterflies) {
+        if (m.rho32)
+            return convolve_t<float, float2, float2>(m.rho32, S, Ghat, phi, d, m.tw32[0], m.tw32[1], m.tw32[2], sc, s);
+        return convolve_t<double, float2, float2>(m.rho64, S, Ghat, phi, d, m.tw32[0], m.tw32[1], m.tw32[2], sc, s);
+    }
+    if (m.rho32)
+        return convolve_t<float, float2, double2>(m.rho32, S, Ghat, phi, d, m.tw64[0], m.tw64[1], m.tw64[2], sc, s);
+    return convolve_t<double, float2, double2>(m.rho64, S, Ghat, phi, d, m.tw64[0], m.tw64[1], m.tw64[2], sc, s);
 }
 
 cudaError_t launch_efield(const double* phi, double2* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s)

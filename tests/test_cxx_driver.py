@@ -44,5 +44,9 @@ def test_cxx_driver_matches_python_mirror(tmp_path, syn, mixed):
     mean, mom2, emit = b.moments()
     assert out["total_num"] == b.get_total_num()
     sd = np.sqrt(np.diag(mom2))
-    assert np.all(np.abs(np.array(out["mean"]) - mean) <= 1e-12 * sd)  # deposit order only
-    assert np.allclose(out["emit"], emit, rtol=1e-9, atol=0)
+    # run to run, only the deposit's summation order differs: FP64 sums in
+    # the drop-in, an FP32 charge grid (merged from neighbouring tiles in any
+    # order) in mixed precision
+    tol = 1e-8 if mixed else 1e-12
+    assert np.all(np.abs(np.array(out["mean"]) - mean) <= tol * sd)
+    assert np.allclose(out["emit"], emit, rtol=1e-7 if mixed else 1e-9, atol=0)

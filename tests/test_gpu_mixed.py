@@ -1,9 +1,12 @@
-"""Mixed-precision space charge: FP64 particles, maps, deposit accumulation
-and Green function; FP32 spectrum, potential and field.
+"""Mixed-precision space charge: FP64 particles, maps and Green function;
+the charge deposited into an FP32 grid (exact fixed-point sums inside each
+CTA's tile, FP32 only where neighbouring tiles meet); FP32 spectrum,
+potential and field with FP64 butterflies.
 
 Acceptance bounds (the configurations' own): field error <= 1e-5 relative L2
 against the FP64 path on the same particles, rms-emittance difference
-<= 1e-4 relative after many kicks.
+<= 1e-4 relative after many kicks.  The FP32 charge grid itself: <= 1e-6
+relative L2 (FP32 rounding of the sums).
 """
 import numpy as np
 import pytest
@@ -34,7 +37,7 @@ def test_mixed_field_error(syn, shape, green_fn):
     p = gaussian_bunch(400000, SIG_C0, 71)
     p64, f64 = _kick(syn, p, shape, syn.precision_t.fp64, green_fn)
     p32, f32 = _kick(syn, p, shape, syn.precision_t.mixed, green_fn)
-    assert np.array_equal(f64["rho"], f32["rho"]) or rel_l2(f32["rho"], f64["rho"]) <= 1e-12
+    assert rel_l2(f32["rho"], f64["rho"]) <= 1e-6
     for c in ("ex", "ey", "ez"):
         assert rel_l2(f32[c], f64[c]) <= FIELD_TOL_MIXED, c
     for j in (1, 3, 5):
@@ -92,3 +95,20 @@ def test_mixed_path_maps_match_fp64(syn, cell):
     scale = np.max(np.abs(a[:, :6]), axis=0)
     err = np.max(np.abs(f[:, :6] - a[:, :6]), axis=0) / scale
     assert np.all(err <= (1e-12 if cell == "fodo" else 1e-11)), err
+
+
+@pytest.mark.parametrize("shape,bound", [((64, 64, 128), 3e-5)])
+def test_fp32_butterflies_option_measured(syn, monkeypatch, shape, bound):
+    """SB2_MIXED_BUTTERFLIES=fp32 (FP32 butterflies, twiddles rounded from
+    long double) runs and stays near the FP64-butterfly result; its field
+    error (1.0e-5 measured at 64 x 64 x 128) is above the 1e-5 bound, which
+    is why FP64 butterflies are the default."""
+    p = gaussian_bunch(400000, SIG_C0, 73)
+    _, f64 = _kick(syn, p, shape, syn.precision_t.fp64)
+    monkeypatch.setenv("SB2_MIXED_BUTTERFLIES", "fp32")
+    _, f32b = _kick(syn, p, shape, syn.precision_t.mixed)
+    monkeypatch.delenv("SB2_MIXED_BUTTERFLIES")
+    _, f64b = _kick(syn, p, shape, syn.precision_t.mixed)
+    e32 = rel_l2(np.stack([f32b[c] for c in ("ex", "ey", "ez")]), np.stack([f64[c] for c in ("ex", "ey", "ez")]))
+    e64 = rel_l2(np.stack([f64b[c] for c in ("ex", "ey", "ez")]), np.stack([f64[c] for c in ("ex", "ey", "ez")]))
+    assert e64 <= FIELD_TOL_MIXED and e32 <= bound and e32 > e64
