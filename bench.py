@@ -328,12 +328,13 @@ def served_stream(syn, njobs, seed, ring_fraction=0.0, nmax=2e6, turns_max=10,
     return out
 
 
-def batched_scan(syn, torch, nbunches, passes, seed):
+def batched_scan(syn, torch, nbunches, passes, seed, lockstep=True):
     """Quad-strength scan: `nbunches` independent bunches (k1 uniform in
     [0.4, 0.8], macroparticles log-uniform in [1e5, 4e6], grid drawn from
-    32^2x64, 64^2x128, 64^2x256), mixed precision, CUDA-graph turns, all
-    advanced together by one Batch; throughput over `passes` passes after
-    one warm-up pass."""
+    32^2x64, 64^2x128, 64^2x256), mixed precision, all advanced together by
+    one Batch: in lockstep (one work-list launch per kernel kind and grid
+    shape per step for all bunches) or with a stream and CUDA-graph turns
+    per bunch; throughput over `passes` passes after one warm-up pass."""
     import numpy as np
     from helpers import fodo_cell, product_lattice
     g = np.random.Generator(np.random.Philox(seed))
@@ -348,21 +349,28 @@ def batched_scan(syn, torch, nbunches, passes, seed):
         opts = syn.Space_charge_3d_open_hockney_options(*grid)
         opts.precision = syn.precision_t.mixed
         prop = syn.Propagator(lat, syn.Split_operator_stepper(opts, KICKS_PER_CELL))
-        prop.set_graphs(True)
+        prop.set_graphs(not lockstep)
         b = syn.Bunch(ref, n, REAL_NUM)
         b.populate_gaussian(SIGMAS, seed=10 + i)
         keep.append((prop, b, batch.add(prop, b)))
-    batch.run({s: 1 for _, _, s in keep})
+    slots = [s for _, _, s in keep]
+
+    def advance(turns):
+        if lockstep:
+            batch.run_lockstep(slots, turns)
+        else:
+            batch.run({s: turns for s in slots})
+    advance(1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    batch.run({s: passes for _, _, s in keep})
+    advance(passes)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     alive = sum(b.get_total_num() for _, b, _ in keep)
     total = sum(b.size() for _, b, _ in keep)
     return {"bunches": nbunches, "macroparticles": total, "passes": passes, "precision": "mixed",
-            "graphs": True, "value": alive * passes * KICKS_PER_CELL / dt, "unit": "macroparticle-steps/s",
-            "wall_s": dt}
+            "mode": "lockstep work lists" if lockstep else "stream and CUDA-graph turns per bunch",
+            "value": alive * passes * KICKS_PER_CELL / dt, "unit": "macroparticle-steps/s", "wall_s": dt}
 
 
 def algorithmic_bytes_per_step(n, grid, w=8):
@@ -479,9 +487,11 @@ def main():
                 wl = ("24-cell ring (QF, SF thin, B 2 m, QD, SD thin; circular aperture 5 cm), 2^24 macroparticles, "
                       "128^2x256 grid, 16 kicks per cell, one turn (384 steps) in FP64 and in mixed precision")
             elif args.config == "c2":
-                r = batched_scan(syn, torch, 64, 50, seed=7)
+                r = batched_scan(syn, torch, 64, 50, seed=7, lockstep=True)
+                r["streams_and_graphs"] = batched_scan(syn, torch, 64, 50, seed=7, lockstep=False)
                 wl = ("quad-strength scan: 64 FODO bunches, k1 U[0.4,0.8], macroparticles log-uniform [1e5,4e6], "
-                      "grids {32^2x64, 64^2x128, 64^2x256}, 50 passes, mixed precision, CUDA-graph turns")
+                      "grids {32^2x64, 64^2x128, 64^2x256}, 50 passes, mixed precision, advanced in lockstep "
+                      "(one work-list launch per kernel kind and grid shape per step)")
             else:
                 r = served_stream(syn, args.jobs, seed=11, ring_fraction=0.5, nmax=8e6, turns_max=50,
                                   grids=((32, 32, 64), (64, 64, 128), (128, 128, 256)), rate=4.0)

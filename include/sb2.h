@@ -364,6 +364,17 @@ sb2_status sb2_batch_run(sb2_batch* q, const int32_t* slots, const int32_t* turn
  * finished -- bunch counters updated, device errors reported as the
  * status -- and to 0 while they run. */
 sb2_status sb2_batch_launch(sb2_batch* q, int32_t slot, int32_t turns);
+/* The listed slots advance `turns` turns in lockstep (one launch per kernel
+ * kind per step for all of them): each job's step runs on the host as
+ * usual, and its kernels go out as work-list launches over all listed
+ * jobs -- the particle passes of every bunch in one launch per pass kernel,
+ * the bookkeeping and domains in one, the charge deposits, Green functions,
+ * convolutions and fields in one per grid shape.  Jobs need the same number
+ * of steps per turn and the same launch sequence per step (one lattice with
+ * different strengths; bunch sizes and grids may differ), otherwise
+ * SB2_ERR_UNSUPPORTED; per-turn diagnostics, step-count records and
+ * sharded propagators are not available.  Returns when the turns are done. */
+sb2_status sb2_batch_run_lockstep(sb2_batch* q, const int32_t* slots, int32_t n, int32_t turns);
 sb2_status sb2_batch_query(sb2_batch* q, int32_t slot, int32_t* done);
 
 /* ---------------------------------------------------------------------

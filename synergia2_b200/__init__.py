@@ -753,6 +753,14 @@ class Batch:
         turns = (ctypes.c_int32 * len(items))(*[int(v) for _, v in items])
         check(lib().sb2_batch_run(self.h, slots, turns, len(items)))
 
+    def run_lockstep(self, slots, turns):
+        """Advance the listed slots by `turns` turns together, one work-list
+        launch per kernel kind (and grid shape) per step for all of them
+        (sb2_batch_run_lockstep)."""
+        slots = list(slots)
+        arr = (ctypes.c_int32 * len(slots))(*slots)
+        check(lib().sb2_batch_run_lockstep(self.h, arr, len(slots), int(turns)))
+
     def launch(self, slot, turns):
         """Enqueue `turns` turns of one slot and return at once."""
         check(lib().sb2_batch_launch(self.h, int(slot), int(turns)))

@@ -21,6 +21,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -1777,6 +1778,31 @@ struct ProfScope {
 };
 
 // ---------------------------------------------------------------------------
+// Launch recording for a batch in lockstep: while g_rec is set, the launch
+// sites of one bunch's step append what they would launch to it instead of
+// launching; Batch::run_lockstep then issues the records of all bunches as
+// work-list launches, one per kernel kind (and grid shape).
+// ---------------------------------------------------------------------------
+struct LaunchRec {
+    enum Kind { TRACK, DOMAIN, ZERO, DEPOSIT, GREEN, CONV, EFIELD, SORT } kind = TRACK;
+    std::vector<unsigned char> tp; // TRACK: TrackParams header and its nops ops
+    int choice = 0, ctas_per_sm = 8;
+    bool fast = false, has_mom = false;
+    int64_t n = 0;
+    DomainParams dp;   // DOMAIN
+    ZeroItem z{};      // ZERO
+    DepositItem dep{}; // DEPOSIT
+    bool f32 = false;
+    ConvItem ci{}; // GREEN, CONV, EFIELD
+    Dims d{};
+    int linear = 0, mode = 0;
+    const double2* tw64[3] = {nullptr, nullptr, nullptr};
+    const float2* tw32[3] = {nullptr, nullptr, nullptr};
+    std::function<void(cudaStream_t)> run; // SORT: the bunch's own launches
+};
+static thread_local std::vector<LaunchRec>* g_rec = nullptr;
+
+// ---------------------------------------------------------------------------
 // Space-charge operator: options, workspaces, solve
 // ---------------------------------------------------------------------------
 static bool is_pow2(int v) { return v > 1 && (v & (v - 1)) == 0; }
@@ -2022,6 +2048,10 @@ struct SpaceCharge {
         }
         const bool exchange = hook && *hook;
         last_rho32 = mixed && !exchange;
+        if (g_rec) {
+            record_solve(b);
+            return;
+        }
         {
             ProfScope ps(PROF_DEPOSIT, s);
             if (last_rho32) {
@@ -2065,6 +2095,60 @@ struct SpaceCharge {
             else
                 cuda_check(launch_efield(phi, E, d.gx, d.gy, d.gz, state, s), "efield");
         }
+    }
+
+    // solve() recorded for a batch in lockstep (the same launches)
+    void record_solve(const Bunch& b)
+    {
+        if (!last_rho32 && !rho) rho = dalloc<double>(G, "rho");
+        LaunchRec z;
+        z.kind = LaunchRec::ZERO;
+        z.z.ptr = last_rho32 ? (void*)rho32 : (void*)rho;
+        z.z.bytes = (last_rho32 ? (int64_t)sizeof(float) : (int64_t)sizeof(double)) * G;
+        g_rec->push_back(z);
+        LaunchRec dep;
+        dep.kind = LaunchRec::DEPOSIT;
+        dep.dep = DepositItem{b.parts, b.stride, b.masks, b.n, state, z.z.ptr};
+        dep.f32 = last_rho32;
+        dep.d = d;
+        g_rec->push_back(dep);
+        ConvItem ci{};
+        ci.rho = z.z.ptr;
+        ci.S = mixed ? (void*)S32 : (void*)S;
+        ci.ghat = ghat;
+        ci.phi = mixed ? (void*)phi32 : (void*)phi;
+        ci.E = mixed ? (void*)E32 : (void*)E;
+        ci.sc = state;
+        if (!o.domain_fixed || !ghat_valid) {
+            LaunchRec g;
+            g.kind = LaunchRec::GREEN;
+            g.ci = ci;
+            g.d = d;
+            g.linear = o.green_fn == SB2_GREEN_LINEAR;
+            g.tw64[0] = tw_x;
+            g.tw64[1] = tw_y;
+            g.tw64[2] = tw_z;
+            g_rec->push_back(g);
+            ghat_valid = true;
+        }
+        LaunchRec c;
+        c.kind = LaunchRec::CONV;
+        c.ci = ci;
+        c.d = d;
+        c.mode = !mixed ? 0 : last_rho32 ? (fp32_butterflies ? 1 : 3) : (fp32_butterflies ? 2 : 4);
+        c.tw64[0] = tw_x;
+        c.tw64[1] = tw_y;
+        c.tw64[2] = tw_z;
+        c.tw32[0] = tw32_x;
+        c.tw32[1] = tw32_y;
+        c.tw32[2] = tw32_z;
+        g_rec->push_back(c);
+        LaunchRec e;
+        e.kind = LaunchRec::EFIELD;
+        e.ci = ci;
+        e.d = d;
+        e.f32 = mixed;
+        g_rec->push_back(e);
     }
 
     void copy_last(double* left, double* h, double* rho_o, double* phi_o, double* ex, double* ey, double* ez,
@@ -2295,7 +2379,18 @@ struct Engine {
                 tp.loss_count = loss_count;
                 tp.loss_cap = loss_cap;
             }
-            {
+            if (g_rec) {
+                LaunchRec r;
+                r.kind = LaunchRec::TRACK;
+                const size_t bytes = offsetof(TrackParams, ops) + sizeof(MapOp) * (size_t)tp.nops;
+                r.tp.assign((const unsigned char*)&tp, (const unsigned char*)&tp + bytes);
+                r.choice = track_pass_choice(tp, tune);
+                r.ctas_per_sm = tune.ctas_per_sm;
+                r.fast = tp.fast_maps != 0;
+                r.has_mom = tp.moment_partials != nullptr;
+                r.n = tp.n;
+                g_rec->push_back(std::move(r));
+            } else {
                 ProfScope ps(pass_is_full(tp.ops, tp.nops) ? PROF_TRACK_FULL : PROF_TRACK, s);
                 cuda_check(launch_track(tp, tune, s), "track kernel");
             }
@@ -2320,7 +2415,12 @@ struct Engine {
                 hook->run(xchg, 6 + nslots, s);
                 dp.xchg = xchg;
             }
-            {
+            if (g_rec) {
+                LaunchRec r;
+                r.kind = LaunchRec::DOMAIN;
+                r.dp = dp;
+                g_rec->push_back(std::move(r));
+            } else {
                 ProfScope ps(PROF_DOMAIN, s);
                 cuda_check(launch_book_domain(dp, s), "domain kernel");
             }
@@ -2433,7 +2533,19 @@ struct Propagator {
     // Re-sort the working copy by the cells of the current domain.
     void resort(Bunch& b, cudaStream_t s)
     {
-        if (!g_sig.dry) {
+        if (g_rec) {
+            LaunchRec r;
+            r.kind = LaunchRec::SORT;
+            const SortBuffers wc = b.wc;
+            int32_t* scr = sort_scratch;
+            const ScState* st = sc->state;
+            const int gx = sc->d.gx, gy = sc->d.gy, gz = sc->d.gz;
+            r.run = [wc, scr, st, gx, gy, gz](cudaStream_t ss) {
+                ProfScope ps(PROF_SORT, ss);
+                cuda_check(launch_cell_sort(wc, scr, st, gx, gy, gz, ss), "cell sort");
+            };
+            g_rec->push_back(std::move(r));
+        } else if (!g_sig.dry) {
             ProfScope ps(PROF_SORT, s);
             cuda_check(launch_cell_sort(b.wc, sort_scratch, sc->state, sc->d.gx, sc->d.gy, sc->d.gz, s), "cell sort");
         }
@@ -2941,6 +3053,7 @@ struct Batch {
             if (j.s) cudaStreamDestroy(j.s);
             if (j.done) cudaEventDestroy(j.done);
         }
+        lock_groups.clear();
     }
     Job& job(int slot)
     {
@@ -2999,6 +3112,372 @@ struct Batch {
         jobs[slot].p = nullptr;
         jobs[slot].b = nullptr;
     }
+    // ----- lockstep: one work-list launch per kernel kind and step ---------
+    // The listed jobs advance `turns` turns together.  Every job runs the
+    // host side of its step as usual (its op lists, design particle,
+    // bookkeeping programs), with its launches recorded (g_rec); the records
+    // of all jobs, position by position, then go out as work-list launches
+    // on one stream: the particle passes of all bunches in one launch per
+    // pass kernel, the bookkeeping and domain of all bunches in one launch,
+    // the charge grids cleared in one, the deposits in one per grid shape,
+    // the Green functions, convolutions and fields in one per grid shape.
+    // The item arrays of a step travel to the device in one copy.  Jobs must
+    // have the same number of steps per turn and the same launch sequence
+    // per step (e.g. one lattice with different strengths, or bunch sizes
+    // and grids that differ); per-turn diagnostics, step-count records and
+    // sharded propagators are not available here.
+    // The listed jobs are split into groups of about equal particle count
+    // (SB2_LOCKSTEP_GROUPS, default 2), each group's launches on its own
+    // stream, so one group's grid work overlaps the other's particle passes.
+    // A group stages its item arrays through a ring of three areas.
+    struct LockGroup {
+        cudaStream_t s = nullptr;
+        unsigned char* host[3] = {nullptr, nullptr, nullptr};
+        unsigned char* dev[3] = {nullptr, nullptr, nullptr};
+        cudaEvent_t done[3] = {nullptr, nullptr, nullptr};
+        size_t cap = 0;
+        int next = 0;
+        void free_arena()
+        {
+            for (int k = 0; k < 3; ++k) {
+                if (host[k]) cudaFreeHost(host[k]);
+                if (dev[k]) dfree(dev[k]);
+                host[k] = dev[k] = nullptr;
+            }
+            cap = 0;
+        }
+        ~LockGroup()
+        {
+            if (s) cudaStreamSynchronize(s);
+            free_arena();
+            for (auto& e : done)
+                if (e) cudaEventDestroy(e);
+            if (s) cudaStreamDestroy(s);
+        }
+    };
+    std::vector<std::unique_ptr<LockGroup>> lock_groups;
+
+    struct Merge {
+        std::vector<unsigned char> host; // the step's item arrays, in the order they are used
+        size_t add(const void* p, size_t bytes)
+        {
+            size_t at = (host.size() + 255) & ~(size_t)255;
+            host.resize(at + bytes);
+            std::memcpy(host.data() + at, p, bytes);
+            return at;
+        }
+    };
+
+    void execute(std::vector<std::vector<LaunchRec>>& recs, LockGroup& G)
+    {
+        cudaStream_t s = G.s;
+        const size_t nj = recs.size();
+        const size_t npos = recs[0].size();
+        for (size_t j = 1; j < nj; ++j)
+            if (recs[j].size() != npos)
+                throw Error(SB2_ERR_UNSUPPORTED, "batch jobs are not in lockstep (different launch sequences)");
+        for (size_t k = 0; k < npos; ++k)
+            for (size_t j = 1; j < nj; ++j)
+                if (recs[j][k].kind != recs[0][k].kind)
+                    throw Error(SB2_ERR_UNSUPPORTED, "batch jobs are not in lockstep (different launch sequences)");
+        // 1. item arrays of every position, laid out in one host block
+        Merge m;
+        struct Op {
+            int kind, variant, max_ops;
+            bool f32;
+            size_t items, first;
+            int nitems, nblocks;
+            Dims d;
+            int linear, mode;
+            const double2* tw64[3];
+            const float2* tw32[3];
+            size_t sort_job;
+        };
+        std::vector<Op> ops;
+        std::vector<int> mom_blocks(nj, 0);
+        for (size_t k = 0; k < npos; ++k) {
+            const int kind = recs[0][k].kind;
+            if (kind == LaunchRec::SORT) {
+                for (size_t j = 0; j < nj; ++j) {
+                    Op o{};
+                    o.kind = kind;
+                    o.sort_job = j;
+                    o.variant = (int)k;
+                    ops.push_back(o);
+                }
+                continue;
+            }
+            if (kind == LaunchRec::DOMAIN) {
+                std::vector<DomainParams> items(nj);
+                for (size_t j = 0; j < nj; ++j) {
+                    items[j] = recs[j][k].dp;
+                    // one moment partial per block the bunch had in the last pass
+                    if (items[j].compute_domain && !items[j].domain_fixed && items[j].moment_partials)
+                        items[j].n_partials = mom_blocks[j];
+                }
+                Op o{};
+                o.kind = kind;
+                o.items = m.add(items.data(), sizeof(DomainParams) * nj);
+                o.nitems = (int)nj;
+                ops.push_back(o);
+                continue;
+            }
+            if (kind == LaunchRec::ZERO) {
+                std::vector<ZeroItem> items(nj);
+                for (size_t j = 0; j < nj; ++j) items[j] = recs[j][k].z;
+                Op o{};
+                o.kind = kind;
+                o.items = m.add(items.data(), sizeof(ZeroItem) * nj);
+                o.nitems = (int)nj;
+                ops.push_back(o);
+                continue;
+            }
+            // grouped kinds: the key decides which jobs share a launch
+            std::vector<std::vector<size_t>> groups;
+            auto key_of = [&](const LaunchRec& r) {
+                std::vector<int> key = {r.kind, r.choice, r.fast ? 1 : 0, r.f32 ? 1 : 0, r.d.gx, r.d.gy, r.d.gz,
+                                        r.linear, r.mode};
+                return key;
+            };
+            {
+                std::vector<std::vector<int>> keys;
+                for (size_t j = 0; j < nj; ++j) {
+                    auto key = key_of(recs[j][k]);
+                    size_t g = 0;
+                    while (g < keys.size() && keys[g] != key) ++g;
+                    if (g == keys.size()) {
+                        keys.push_back(key);
+                        groups.emplace_back();
+                    }
+                    groups[g].push_back(j);
+                }
+            }
+            for (auto const& grp : groups) {
+                const LaunchRec& r0 = recs[grp[0]][k];
+                Op o{};
+                o.kind = kind;
+                o.nitems = (int)grp.size();
+                o.d = r0.d;
+                o.linear = r0.linear;
+                o.mode = r0.mode;
+                o.f32 = r0.f32;
+                for (int a = 0; a < 3; ++a) {
+                    o.tw64[a] = r0.tw64[a];
+                    o.tw32[a] = r0.tw32[a];
+                }
+                if (kind == LaunchRec::TRACK) {
+                    o.variant = r0.choice;
+                    o.f32 = r0.fast;
+                    std::vector<size_t> at(grp.size());
+                    std::vector<int> first(grp.size() + 1, 0);
+                    const int tile = track_pass_tile(r0.choice);
+                    for (size_t q = 0; q < grp.size(); ++q) {
+                        const LaunchRec& r = recs[grp[q]][k];
+                        at[q] = m.add(r.tp.data(), r.tp.size());
+                        o.max_ops = std::max(o.max_ops, ((const TrackParams*)r.tp.data())->nops);
+                        const int64_t need = std::max<int64_t>(1, (r.n + tile - 1) / tile);
+                        const int vg = (int)std::min<int64_t>(need, track_grid_blocks(r.ctas_per_sm));
+                        first[q + 1] = first[q] + vg;
+                        if (r.has_mom) mom_blocks[grp[q]] = vg;
+                    }
+                    // item pointers are arena offsets here, made device addresses below
+                    std::vector<uint64_t> ptrs(at.begin(), at.end());
+                    o.items = m.add(ptrs.data(), sizeof(uint64_t) * ptrs.size());
+                    o.first = m.add(first.data(), sizeof(int) * first.size());
+                    o.nblocks = first.back();
+                } else if (kind == LaunchRec::DEPOSIT) {
+                    std::vector<DepositItem> items;
+                    std::vector<int> first(1, 0);
+                    for (size_t j : grp) {
+                        items.push_back(recs[j][k].dep);
+                        first.push_back(first.back() + std::max(1, deposit_list_blocks(recs[j][k].dep.n)));
+                    }
+                    o.items = m.add(items.data(), sizeof(DepositItem) * items.size());
+                    o.first = m.add(first.data(), sizeof(int) * first.size());
+                    o.nblocks = first.back();
+                } else {
+                    std::vector<ConvItem> items;
+                    for (size_t j : grp) items.push_back(recs[j][k].ci);
+                    o.items = m.add(items.data(), sizeof(ConvItem) * items.size());
+                }
+                ops.push_back(o);
+            }
+        }
+        // 2. the block to the device (a ring of three staging areas)
+        const size_t bytes = std::max<size_t>(m.host.size(), 256);
+        if (bytes > G.cap) {
+            cuda_check(cudaStreamSynchronize(s), "lockstep");
+            G.free_arena();
+            G.cap = bytes * 2;
+            for (int k = 0; k < 3; ++k) {
+                cuda_check(cudaMallocHost((void**)&G.host[k], G.cap), "lockstep staging");
+                G.dev[k] = dalloc<unsigned char>(G.cap, "lockstep items");
+                if (!G.done[k]) cuda_check(cudaEventCreateWithFlags(&G.done[k], cudaEventDisableTiming), "event");
+            }
+        }
+        const int slot = G.next;
+        G.next = (G.next + 1) % 3;
+        cuda_check(cudaEventSynchronize(G.done[slot]), "lockstep staging"); // its last copy has run
+        unsigned char* dev = G.dev[slot];
+        for (auto const& o : ops) // TRACK item pointers: arena offsets -> device addresses
+            if (o.kind == LaunchRec::TRACK) {
+                uint64_t* ptrs = (uint64_t*)(m.host.data() + o.items);
+                for (int q = 0; q < o.nitems; ++q) ptrs[q] = (uint64_t)(uintptr_t)(dev + ptrs[q]);
+            }
+        std::memcpy(G.host[slot], m.host.data(), m.host.size());
+        cuda_check(cudaMemcpyAsync(dev, G.host[slot], m.host.size(), cudaMemcpyHostToDevice, s), "lockstep items");
+        cuda_check(cudaEventRecord(G.done[slot], s), "event");
+        // 3. the launches, in the recorded order
+        for (auto const& o : ops) {
+            const unsigned char* items = dev + o.items;
+            const int* first = (const int*)(dev + o.first);
+            switch (o.kind) {
+            case LaunchRec::TRACK: {
+                ProfScope ps(PROF_TRACK, s);
+                cuda_check(launch_track_list(o.variant, o.f32, (const TrackParams* const*)items, first, o.nitems,
+                                             o.nblocks, o.max_ops, s),
+                           "track list");
+                break;
+            }
+            case LaunchRec::DOMAIN: {
+                ProfScope ps(PROF_DOMAIN, s);
+                cuda_check(launch_book_domain_list((const DomainParams*)items, o.nitems, s), "domain list");
+                break;
+            }
+            case LaunchRec::ZERO: {
+                ProfScope ps(PROF_DEPOSIT, s);
+                cuda_check(launch_zero_list((const ZeroItem*)items, o.nitems, s), "zero list");
+                break;
+            }
+            case LaunchRec::DEPOSIT: {
+                ProfScope ps(PROF_DEPOSIT, s);
+                cuda_check(launch_deposit_list(o.f32, (const DepositItem*)items, first, o.nitems, o.nblocks, o.d.gx,
+                                               o.d.gy, o.d.gz, s),
+                           "deposit list");
+                break;
+            }
+            case LaunchRec::GREEN: {
+                ProfScope ps(PROF_GREEN, s);
+                cuda_check(launch_green_list((const ConvItem*)items, o.nitems, o.d, o.linear, o.tw64[0], o.tw64[1],
+                                             o.tw64[2], s),
+                           "green list");
+                break;
+            }
+            case LaunchRec::CONV: {
+                ProfScope ps(PROF_SOLVE, s);
+                cuda_check(launch_convolve_list(o.mode, (const ConvItem*)items, o.nitems, o.d, o.tw64, o.tw32, s),
+                           "convolve list");
+                break;
+            }
+            case LaunchRec::EFIELD: {
+                ProfScope ps(PROF_EFIELD, s);
+                cuda_check(launch_efield_list(o.f32, (const ConvItem*)items, o.nitems, o.d.gx, o.d.gy, o.d.gz, s),
+                           "efield list");
+                break;
+            }
+            case LaunchRec::SORT:
+                recs[o.sort_job][o.variant].run(s);
+                break;
+            }
+        }
+    }
+
+    void run_lockstep(const int32_t* slots, int n, int turns)
+    {
+        if (n < 1 || turns < 0) throw Error(SB2_ERR_INVALID, "run_lockstep: bad job list");
+        std::vector<Job*> js;
+        for (int k = 0; k < n; ++k) {
+            Job& j = job(slots[k]);
+            if (j.pending) throw Error(SB2_ERR_INVALID, "batch slot already has turns in flight");
+            for (Job* o : js)
+                if (o == &j) throw Error(SB2_ERR_INVALID, "run_lockstep: a slot is listed twice");
+            Propagator& P = *j.p;
+            if (P.hook) throw Error(SB2_ERR_UNSUPPORTED, "run_lockstep: sharded propagators are not supported");
+            if (P.diag_cap || P.step_rec_cap)
+                throw Error(SB2_ERR_UNSUPPORTED, "run_lockstep: per-turn diagnostics and step-count records are not "
+                                                 "supported");
+            if (!js.empty() && P.steps.size() != js[0]->p->steps.size())
+                throw Error(SB2_ERR_UNSUPPORTED, "batch jobs are not in lockstep (different steps per turn)");
+            js.push_back(&j);
+        }
+        // groups of about equal particle count (largest jobs first)
+        int ngroups = 2;
+        if (const char* e = getenv("SB2_LOCKSTEP_GROUPS")) ngroups = std::max(1, atoi(e));
+        ngroups = std::min<int>(ngroups, (int)js.size());
+        while ((int)lock_groups.size() < ngroups) {
+            lock_groups.emplace_back(new LockGroup());
+            cuda_check(cudaStreamCreateWithFlags(&lock_groups.back()->s, cudaStreamNonBlocking), "stream");
+        }
+        std::vector<std::vector<Job*>> part(ngroups);
+        {
+            std::vector<Job*> order = js;
+            std::stable_sort(order.begin(), order.end(), [](Job* a, Job* b) { return a->b->n > b->b->n; });
+            std::vector<int64_t> load(ngroups, 0);
+            for (Job* j : order) {
+                const int g = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+                part[g].push_back(j);
+                load[g] += j->b->n;
+            }
+        }
+        for (int g = 0; g < ngroups; ++g) // work queued on the jobs' own streams comes first
+            for (Job* j : part[g]) {
+                if (!j->done) cuda_check(cudaEventCreateWithFlags(&j->done, cudaEventDisableTiming), "event");
+                cuda_check(cudaEventRecord(j->done, j->s), "event");
+                cuda_check(cudaStreamWaitEvent(lock_groups[g]->s, j->done, 0), "event");
+            }
+        const int ns = (int)js[0]->p->steps.size();
+        std::vector<std::vector<std::vector<LaunchRec>>> recs(ngroups);
+        for (int g = 0; g < ngroups; ++g) recs[g].resize(part[g].size());
+        auto record = [&](auto&& fn) {
+            for (int g = 0; g < ngroups; ++g) {
+                for (size_t q = 0; q < part[g].size(); ++q) {
+                    recs[g][q].clear();
+                    g_rec = &recs[g][q];
+                    try {
+                        fn(*part[g][q], lock_groups[g]->s);
+                    } catch (...) {
+                        g_rec = nullptr;
+                        throw;
+                    }
+                    g_rec = nullptr;
+                }
+                execute(recs[g], *lock_groups[g]);
+            }
+        };
+        for (int g = 0; g < ngroups; ++g)
+            for (Job* j : part[g]) {
+                j->p->begin(*j->b, lock_groups[g]->s);
+                j->p->enter_sorted(*j->b, lock_groups[g]->s);
+            }
+        for (int t = 0; t < turns; ++t)
+            for (int si = 0; si < ns; ++si)
+                record([&](Job& j, cudaStream_t s) {
+                    if (si == 0) j.b->ref.start_repetition();
+                    j.p->run_step(*j.b, j.p->steps[si], s);
+                    if (si == ns - 1) j.b->turns_done += 1;
+                });
+        record([&](Job& j, cudaStream_t s) {
+            j.p->engine_->flush(*j.b, j.p->sc.get(), j.p->elem_charge, false, 0.0, s);
+        });
+        for (int g = 0; g < ngroups; ++g)
+            for (Job* j : part[g]) j->p->leave_sorted(*j->b, lock_groups[g]->s);
+        for (int g = 0; g < ngroups; ++g) // later work on the jobs' own streams sees the result
+            cuda_check(cudaStreamSynchronize(lock_groups[g]->s), "lockstep");
+        std::string err;
+        sb2_status code = SB2_OK;
+        for (Job* j : js) {
+            try {
+                j->p->finish(*j->b, lock_groups[0]->s);
+            } catch (const Error& e) {
+                if (code == SB2_OK) {
+                    code = e.code;
+                    err = e.what();
+                }
+            }
+        }
+        if (code != SB2_OK) throw Error(code, err);
+    }
+
     void run(const int32_t* slots, const int32_t* turns, int n)
     {
         std::string err;
@@ -3912,6 +4391,14 @@ sb2_status sb2_propagator_read_losses(sb2_propagator* p, int32_t max_records, in
         o[9] = t[2];
     }
     *count = n;
+    SB2_CATCH
+}
+
+sb2_status sb2_batch_run_lockstep(sb2_batch* q, const int32_t* slots, int32_t n, int32_t turns)
+{
+    SB2_TRY
+    SB2_REQUIRE(q && slots, "null argument");
+    q->q.run_lockstep(slots, n, turns);
     SB2_CATCH
 }
 

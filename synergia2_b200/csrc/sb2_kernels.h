@@ -100,12 +100,59 @@ constexpr int kMaxCtasPerSm = 12;
 int track_grid_blocks();                // grid at the default CTAs per SM
 int track_grid_blocks(int ctas_per_sm); // SM count x ctas_per_sm
 cudaError_t launch_track(const TrackParams& p, const TrackTune& t, cudaStream_t s);
+// work lists (a batch in lockstep): the kernel a pass runs, the particles a
+// block of it takes per iteration, and one launch of many bunches' passes
+// with the same kernel (items in device memory, item i on blocks
+// [first[i], first[i+1]) of nblocks; max_ops the largest op count of an
+// item)
+int track_pass_choice(const TrackParams& p, const TrackTune& t);
+int track_pass_tile(int choice);
+cudaError_t launch_track_list(int choice, bool fast_maps, const TrackParams* const* items, const int* first,
+                              int nitems, int nblocks, int max_ops, cudaStream_t s);
 cudaError_t launch_moments(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
                            const double* mean, double* partials, int nblocks, cudaStream_t s);
 cudaError_t launch_populate(double* parts, int64_t stride, uint8_t* masks, int64_t n, const double* sig,
                             uint64_t seed, cudaStream_t s);
+// Work-list items of the space-charge kernels (a batch in lockstep): one
+// per bunch; the grid kernels' items share a grid shape.
+struct ZeroItem {
+    void* ptr;
+    int64_t bytes; // a multiple of 8
+};
+struct DepositItem {
+    const double* parts;
+    int64_t stride;
+    const uint8_t* masks;
+    int64_t n;
+    const ScState* sc;
+    void* rho; // double, or float for the FP32 charge grid
+};
+struct ConvItem {
+    const void* rho; // charge density (double or float)
+    void* S;         // spectrum (double2 or float2)
+    double* ghat;    // Green function octant
+    void* phi;       // potential (double or float)
+    void* E;         // field (double2 pairs or float4)
+    const ScState* sc;
+};
+
 // sc3d.cu
 cudaError_t launch_book_domain(const DomainParams& p, cudaStream_t s);
+cudaError_t launch_book_domain_list(const DomainParams* items, int nitems, cudaStream_t s);
+cudaError_t launch_zero_list(const ZeroItem* items, int nitems, cudaStream_t s);
+// the deposit of many bunches: item i on blocks [first[i], first[i+1]),
+// deposit_list_blocks(n) blocks for a bunch of n particles
+int deposit_list_blocks(int64_t n);
+cudaError_t launch_deposit_list(bool f32, const DepositItem* items, const int* first, int nitems, int nblocks, int gx,
+                                int gy, int gz, cudaStream_t s);
+// Green function, convolution (mode 0: FP64; 1..4: mixed with FP32 / FP64
+// charge and FP32 / FP64 butterflies as MixedConv) and field of nitems
+// bunches with the grid shape d
+cudaError_t launch_green_list(const ConvItem* items, int nitems, const Dims& d, int linear, const double2* tw_x,
+                              const double2* tw_y, const double2* tw_z, cudaStream_t s);
+cudaError_t launch_convolve_list(int mode, const ConvItem* items, int nitems, const Dims& d, const double2* const* tw64,
+                                 const float2* const* tw32, cudaStream_t s);
+cudaError_t launch_efield_list(bool f32, const ConvItem* items, int nitems, int gx, int gy, int gz, cudaStream_t s);
 // sharded bunch: moment sums and per-slot discards into xchg (to be summed
 // over the ranks), and the global n_total from a summed local count
 cudaError_t launch_shard_pack(const DomainParams& p, int nslots, double* xchg, cudaStream_t s);

@@ -45,7 +45,7 @@ __device__ double smallest_non_tiny(double val, double o1, double o2, double tin
     return fmax(o1, o2);
 }
 
-__global__ void __launch_bounds__(256) book_domain_kernel(const __grid_constant__ DomainParams p)
+__device__ __forceinline__ void book_domain_body(const DomainParams& p)
 {
     __shared__ double s_sum[256][6];
     // fixed-order reduction of the per-block moment partials (a bunch split
@@ -150,6 +150,24 @@ __global__ void __launch_bounds__(256) book_domain_kernel(const __grid_constant_
                 (p.pref * p.gamma * p.gamma * p.beta);
     st.valid = 1;
     *p.sc = st;
+}
+
+__global__ void __launch_bounds__(256) book_domain_kernel(const __grid_constant__ DomainParams p) { book_domain_body(p); }
+
+// one block per bunch of a batch in lockstep
+__global__ void __launch_bounds__(256) book_domain_list_kernel(const DomainParams* __restrict__ items)
+{
+    book_domain_body(items[blockIdx.x]);
+}
+
+// grid (x, nitems): item blockIdx.y zeroes its range
+__global__ void zero_list_kernel(const ZeroItem* __restrict__ items)
+{
+    const ZeroItem it = items[blockIdx.y];
+    double* d = (double*)it.ptr;
+    const int64_t n = it.bytes / 8;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        d[i] = 0.0;
 }
 
 // ---------------------------------------------------------------------------
@@ -390,17 +408,17 @@ __device__ __forceinline__ void tile_add(DepositSmem<K>& sm, int at, double u, d
 }
 
 template <int K, typename RT>
-__global__ void __launch_bounds__(kDepT) deposit_tile_kernel(const double* __restrict__ parts, int64_t stride,
-                                                             const uint8_t* __restrict__ masks, int64_t n,
-                                                             const ScState* __restrict__ scp, RT* rho, int gx,
-                                                             int gy, int gz)
+__device__ __forceinline__ void deposit_tile_body(const double* __restrict__ parts, int64_t stride,
+                                                  const uint8_t* __restrict__ masks, int64_t n,
+                                                  const ScState* __restrict__ scp, RT* rho, int gx, int gy, int gz,
+                                                  int vb)
 {
     extern __shared__ __align__(16) unsigned char dep_raw[];
     DepositSmem<K>& sm = *reinterpret_cast<DepositSmem<K>*>(dep_raw);
     const ScState& sc = *scp;
     if (!sc.valid) return;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int64_t base = (int64_t)blockIdx.x * (kDepT * K);
+    const int64_t base = (int64_t)vb * (kDepT * K);
     const unsigned full = 0xffffffffu;
 
     // 1. cells and offsets, coalesced
@@ -554,6 +572,35 @@ __global__ void __launch_bounds__(kDepT) deposit_tile_kernel(const double* __res
     }
 }
 
+template <int K, typename RT>
+__global__ void __launch_bounds__(kDepT) deposit_tile_kernel(const double* __restrict__ parts, int64_t stride,
+                                                             const uint8_t* __restrict__ masks, int64_t n,
+                                                             const ScState* __restrict__ scp, RT* rho, int gx,
+                                                             int gy, int gz)
+{
+    deposit_tile_body<K, RT>(parts, stride, masks, n, scp, rho, gx, gy, gz, blockIdx.x);
+}
+
+// The deposits of many bunches with one grid shape: item i on blocks
+// [first[i], first[i+1]).
+template <int K, typename RT>
+__global__ void __launch_bounds__(kDepT) deposit_list_kernel(const DepositItem* __restrict__ items,
+                                                             const int* __restrict__ first, int nitems, int gx,
+                                                             int gy, int gz)
+{
+    int lo = 0, hi = nitems;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (first[mid] <= (int)blockIdx.x)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    const DepositItem it = items[lo];
+    deposit_tile_body<K, RT>(it.parts, it.stride, it.masks, it.n, it.sc, (RT*)it.rho, gx, gy, gz,
+                             (int)blockIdx.x - first[lo]);
+}
+
 // ---------------------------------------------------------------------------
 // Green function octant: alg_g2_linear :230-348 / alg_g2_pointlike :136-228
 // evaluated for ix <= gx, iy <= gy, iz <= gz (doubled shape = 2 * shape,
@@ -570,8 +617,12 @@ __global__ void __launch_bounds__(kDepT) deposit_tile_kernel(const double* __res
 constexpr int kGreenChunk = 16;
 
 __global__ void green_octant_kernel(const ScState* __restrict__ scp, double* G, int gx0, int gy0, int gz0,
-                                    int linear)
+                                    int linear, const ConvItem* __restrict__ list)
 {
+    if (list) { // item blockIdx.y of a batch in lockstep
+        scp = list[blockIdx.y].sc;
+        G = list[blockIdx.y].ghat;
+    }
     const ScState& sc = *scp;
     if (!sc.valid) return;
     const int ox = gx0 + 1, oy = gy0 + 1, oz = gz0 + 1;
@@ -657,8 +708,14 @@ template <typename W> __device__ __forceinline__ W czero() { return cvt_c<W>(mak
 template <int L, typename RI, typename C, typename W>
 __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xf_kernel(const RI* __restrict__ rho, C* S,
                                                                         const W* __restrict__ tw, Dims d,
-                                                                        const ScState* __restrict__ scp)
+                                                                        const ScState* __restrict__ scp,
+                                                                        const ConvItem* __restrict__ list)
 {
+    if (list) { // item blockIdx.z of a batch in lockstep
+        rho = (const RI*)list[blockIdx.z].rho;
+        S = (C*)list[blockIdx.z].S;
+        scp = list[blockIdx.z].sc;
+    }
     typedef fft::XMajor<L> LAY;
     typedef typename CxT<W>::R R;
     constexpr int NW = fft::Shape<L>::W, TPL = fft::Shape<L>::TPL;
@@ -704,8 +761,13 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xf_kernel(const RI
 // first gy inputs, all ny outputs; inverse: all inputs, first gy outputs.
 template <int L, typename C, typename W, bool INV>
 __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_y_kernel(C* S, const W* __restrict__ tw, Dims d,
-                                                                       const ScState* __restrict__ scp)
+                                                                       const ScState* __restrict__ scp,
+                                                                       const ConvItem* __restrict__ list)
 {
+    if (list) {
+        S = (C*)list[blockIdx.z].S;
+        scp = list[blockIdx.z].sc;
+    }
     typedef fft::LMajor<L> LAY;
     constexpr int NW = fft::Shape<L>::W;
     constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
@@ -741,8 +803,14 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_y_kernel(C* S, con
 template <int L, typename C, typename W>
 __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_z_conv_kernel(C* S, const double* __restrict__ Ghat,
                                                                             const W* __restrict__ tw, Dims d,
-                                                                            const ScState* __restrict__ scp)
+                                                                            const ScState* __restrict__ scp,
+                                                                            const ConvItem* __restrict__ list)
 {
+    if (list) {
+        S = (C*)list[blockIdx.z].S;
+        Ghat = list[blockIdx.z].ghat;
+        scp = list[blockIdx.z].sc;
+    }
     typedef fft::LMajor<L> LAY;
     typedef typename CxT<W>::R R;
     constexpr int NW = fft::Shape<L>::W;
@@ -788,8 +856,14 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_z_conv_kernel(C* S
 template <int L, typename C, typename W, typename RO>
 __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xi_kernel(const C* __restrict__ S, RO* phi,
                                                                         const W* __restrict__ tw, Dims d,
-                                                                        const ScState* __restrict__ scp)
+                                                                        const ScState* __restrict__ scp,
+                                                                        const ConvItem* __restrict__ list)
 {
+    if (list) {
+        S = (const C*)list[blockIdx.z].S;
+        phi = (RO*)list[blockIdx.z].phi;
+        scp = list[blockIdx.z].sc;
+    }
     typedef fft::XMajor<L> LAY;
     constexpr int NW = fft::Shape<L>::W;
     constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
@@ -851,8 +925,13 @@ template <int L, int AXIS>
 __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_green_kernel(double* G,
                                                                            const double2* __restrict__ tw, int ox,
                                                                            int oy, int oz,
-                                                                           const ScState* __restrict__ scp)
+                                                                           const ScState* __restrict__ scp,
+                                                                           const ConvItem* __restrict__ list)
 {
+    if (list) {
+        G = list[blockIdx.z].ghat;
+        scp = list[blockIdx.z].sc;
+    }
     typedef typename std::conditional<AXIS == 0, fft::XMajor<L>, fft::LMajor<L>>::type LAY;
     constexpr int W = fft::Shape<L>::W;
     constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
@@ -910,8 +989,13 @@ __device__ __forceinline__ void store_e(float4* E, int64_t i, float ex, float ey
 
 template <typename R, typename EV>
 __global__ void efield_kernel(const R* __restrict__ phi, EV* E, int gx, int gy, int gz,
-                              const ScState* __restrict__ scp)
+                              const ScState* __restrict__ scp, const ConvItem* __restrict__ list)
 {
+    if (list) { // item blockIdx.y of a batch in lockstep
+        phi = (const R*)list[blockIdx.y].phi;
+        E = (EV*)list[blockIdx.y].E;
+        scp = list[blockIdx.y].sc;
+    }
     const ScState& sc = *scp;
     if (!sc.valid) return;
     const R ihx = (R)(0.5 / sc.dh[0]), ihy = (R)(0.5 / sc.dh[1]), ihz = (R)(0.5 / sc.dh[2]);
@@ -993,6 +1077,18 @@ cudaError_t launch_book_domain(const DomainParams& p, cudaStream_t s)
     return cudaGetLastError();
 }
 
+cudaError_t launch_book_domain_list(const DomainParams* items, int nitems, cudaStream_t s)
+{
+    book_domain_list_kernel<<<nitems, 256, 0, s>>>(items);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_zero_list(const ZeroItem* items, int nitems, cudaStream_t s)
+{
+    zero_list_kernel<<<dim3(std::max(1, sm_count() * 8 / nitems), nitems), 256, 0, s>>>(items);
+    return cudaGetLastError();
+}
+
 #ifndef SB2_DEPOSIT_CTAS
 #define SB2_DEPOSIT_CTAS 8 // CTAs per SM of the grid-stride deposit (5 / 8 / 16: 0.163 / 0.142 / 0.146 ms per C1 step)
 #endif
@@ -1037,6 +1133,27 @@ cudaError_t launch_deposit(const double* parts, int64_t stride, const uint8_t* m
     }
 }
 
+int deposit_list_blocks(int64_t n) { return (int)((n + kDepT * 4 - 1) / (kDepT * 4)); }
+
+template <typename RT>
+static cudaError_t deposit_list(const DepositItem* items, const int* first, int nitems, int nblocks, int gx, int gy,
+                                int gz, cudaStream_t s)
+{
+    const int bytes = (int)sizeof(DepositSmem<4>);
+    static cudaError_t once =
+        cudaFuncSetAttribute(deposit_list_kernel<4, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (once) return once;
+    if (nblocks > 0) deposit_list_kernel<4, RT><<<nblocks, kDepT, bytes, s>>>(items, first, nitems, gx, gy, gz);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_deposit_list(bool f32, const DepositItem* items, const int* first, int nitems, int nblocks, int gx,
+                                int gy, int gz, cudaStream_t s)
+{
+    return f32 ? deposit_list<float>(items, first, nitems, nblocks, gx, gy, gz, s)
+               : deposit_list<double>(items, first, nitems, nblocks, gx, gy, gz, s);
+}
+
 cudaError_t launch_deposit_f32(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
                                const ScState* sc, float* rho, int gx, int gy, int gz, cudaStream_t s)
 {
@@ -1056,42 +1173,47 @@ static cudaError_t fft_smem(KERN* k, int bytes)
 
 #define SB2_FFT_LENGTHS(X) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048)
 
+// Every launcher below runs one bunch (list null, nitems 1) or, for a batch
+// in lockstep, nitems bunches of the same grid shape whose pointers are in
+// the device array `list` (the kernels take item blockIdx.z, or blockIdx.y
+// for the field and the octant).
 template <int L>
 static cudaError_t green_passes_axis0(double* G, const double2* tw, int ox, int oy, int oz, const ScState* sc,
-                                      cudaStream_t s)
+                                      const ConvItem* list, int nitems, cudaStream_t s)
 {
     typedef fft::XMajor<L> LAY;
     const int bytes = LAY::kSmemElems * 16;
     static cudaError_t once = fft_smem(fft_green_kernel<L, 0>, bytes);
     if (once) return once;
     const int64_t pairs = ((int64_t)oy * oz + 1) / 2;
-    fft_green_kernel<L, 0><<<ceil_div64(pairs, fft::Shape<L>::W), fft::Shape<L>::THREADS, bytes, s>>>(G, tw, ox, oy, oz, sc);
+    dim3 grid(ceil_div64(pairs, fft::Shape<L>::W), 1, nitems);
+    fft_green_kernel<L, 0><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(G, tw, ox, oy, oz, sc, list);
     return cudaSuccess;
 }
 template <int L, int AXIS>
 static cudaError_t green_passes_lmajor(double* G, const double2* tw, int ox, int oy, int oz, const ScState* sc,
-                                       cudaStream_t s)
+                                       const ConvItem* list, int nitems, cudaStream_t s)
 {
     typedef fft::LMajor<L> LAY;
     const int bytes = LAY::kSmemElems * 16;
     static cudaError_t once = fft_smem(fft_green_kernel<L, AXIS>, bytes);
     if (once) return once;
     const int64_t nlines = AXIS == 1 ? (int64_t)ox * oz : (int64_t)ox * oy;
-    fft_green_kernel<L, AXIS><<<ceil_div64((nlines + 1) / 2, fft::Shape<L>::W), fft::Shape<L>::THREADS, bytes, s>>>(
-        G, tw, ox, oy, oz, sc);
+    dim3 grid(ceil_div64((nlines + 1) / 2, fft::Shape<L>::W), 1, nitems);
+    fft_green_kernel<L, AXIS><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(G, tw, ox, oy, oz, sc, list);
     return cudaSuccess;
 }
 
-// Ghat from the current domain: octant G, then the three even-line passes.
-cudaError_t launch_green(const ScState* sc, double* G, const Dims& d, int linear, const double2* tw_x,
-                         const double2* tw_y, const double2* tw_z, cudaStream_t s)
+static cudaError_t green_t(const ScState* sc, double* G, const Dims& d, int linear, const double2* tw_x,
+                           const double2* tw_y, const double2* tw_z, const ConvItem* list, int nitems, cudaStream_t s)
 {
     const int ox = d.nx / 2 + 1, oy = d.ny / 2 + 1, oz = d.nz / 2 + 1;
-    green_octant_kernel<<<sm_count() * 4, 256, 0, s>>>(sc, G, d.gx, d.gy, d.gz, linear);
+    const int nb = list ? std::max(1, sm_count() * 4 / nitems) : sm_count() * 4;
+    green_octant_kernel<<<dim3(nb, nitems), 256, 0, s>>>(sc, G, d.gx, d.gy, d.gz, linear, list);
     cudaError_t e = cudaSuccess;
-#define SB2_G0(LL) case LL: e = green_passes_axis0<LL>(G, tw_x, ox, oy, oz, sc, s); break;
-#define SB2_G1(LL) case LL: e = green_passes_lmajor<LL, 1>(G, tw_y, ox, oy, oz, sc, s); break;
-#define SB2_G2(LL) case LL: e = green_passes_lmajor<LL, 2>(G, tw_z, ox, oy, oz, sc, s); break;
+#define SB2_G0(LL) case LL: e = green_passes_axis0<LL>(G, tw_x, ox, oy, oz, sc, list, nitems, s); break;
+#define SB2_G1(LL) case LL: e = green_passes_lmajor<LL, 1>(G, tw_y, ox, oy, oz, sc, list, nitems, s); break;
+#define SB2_G2(LL) case LL: e = green_passes_lmajor<LL, 2>(G, tw_z, ox, oy, oz, sc, list, nitems, s); break;
     switch (d.nx) { SB2_FFT_LENGTHS(SB2_G0) default: return cudaErrorInvalidValue; }
     if (e) return e;
     switch (d.ny) { SB2_FFT_LENGTHS(SB2_G1) default: return cudaErrorInvalidValue; }
@@ -1104,61 +1226,78 @@ cudaError_t launch_green(const ScState* sc, double* G, const Dims& d, int linear
     return cudaGetLastError();
 }
 
+// Ghat from the current domain: octant G, then the three even-line passes.
+cudaError_t launch_green(const ScState* sc, double* G, const Dims& d, int linear, const double2* tw_x,
+                         const double2* tw_y, const double2* tw_z, cudaStream_t s)
+{
+    return green_t(sc, G, d, linear, tw_x, tw_y, tw_z, nullptr, 1, s);
+}
+
+cudaError_t launch_green_list(const ConvItem* items, int nitems, const Dims& d, int linear, const double2* tw_x,
+                              const double2* tw_y, const double2* tw_z, cudaStream_t s)
+{
+    return green_t(nullptr, nullptr, d, linear, tw_x, tw_y, tw_z, items, nitems, s);
+}
+
 template <int L, typename RI, typename C, typename W>
-static cudaError_t pass_xf(const RI* rho, C* S, const W* tw, const Dims& d, const ScState* sc, cudaStream_t s)
+static cudaError_t pass_xf(const RI* rho, C* S, const W* tw, const Dims& d, const ScState* sc, const ConvItem* list,
+                           int nitems, cudaStream_t s)
 {
     const int bytes = fft::XMajor<L>::kSmemElems * (int)sizeof(W);
     static cudaError_t once = fft_smem(fft_xf_kernel<L, RI, C, W>, bytes);
     if (once) return once;
     const int64_t nlines = (int64_t)((d.gy + 1) / 2) * d.gz;
-    fft_xf_kernel<L, RI, C, W><<<ceil_div64(nlines, fft::Shape<L>::W), fft::Shape<L>::THREADS, bytes, s>>>(rho, S, tw, d,
-                                                                                                           sc);
+    dim3 grid(ceil_div64(nlines, fft::Shape<L>::W), 1, nitems);
+    fft_xf_kernel<L, RI, C, W><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(rho, S, tw, d, sc, list);
     return cudaSuccess;
 }
 template <int L, typename C, typename W, bool INV>
-static cudaError_t pass_y(C* S, const W* tw, const Dims& d, const ScState* sc, cudaStream_t s)
+static cudaError_t pass_y(C* S, const W* tw, const Dims& d, const ScState* sc, const ConvItem* list, int nitems,
+                          cudaStream_t s)
 {
     const int bytes = fft::LMajor<L>::kSmemElems * (int)sizeof(W);
     static cudaError_t once = fft_smem(fft_y_kernel<L, C, W, INV>, bytes);
     if (once) return once;
-    dim3 grid(ceil_div64(d.nkx, fft::Shape<L>::W), d.gz);
-    fft_y_kernel<L, C, W, INV><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, tw, d, sc);
+    dim3 grid(ceil_div64(d.nkx, fft::Shape<L>::W), d.gz, nitems);
+    fft_y_kernel<L, C, W, INV><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, tw, d, sc, list);
     return cudaSuccess;
 }
 template <int L, typename C, typename W>
-static cudaError_t pass_z(C* S, const double* Ghat, const W* tw, const Dims& d, const ScState* sc, cudaStream_t s)
+static cudaError_t pass_z(C* S, const double* Ghat, const W* tw, const Dims& d, const ScState* sc, const ConvItem* list,
+                          int nitems, cudaStream_t s)
 {
     const int bytes = fft::LMajor<L>::kSmemElems * (int)sizeof(W);
     static cudaError_t once = fft_smem(fft_z_conv_kernel<L, C, W>, bytes);
     if (once) return once;
-    dim3 grid(ceil_div64(d.nkx, fft::Shape<L>::W), d.ny);
-    fft_z_conv_kernel<L, C, W><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, Ghat, tw, d, sc);
+    dim3 grid(ceil_div64(d.nkx, fft::Shape<L>::W), d.ny, nitems);
+    fft_z_conv_kernel<L, C, W><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, Ghat, tw, d, sc, list);
     return cudaSuccess;
 }
 template <int L, typename C, typename W>
 static cudaError_t pass_xi(const C* S, typename CxT<C>::R* phi, const W* tw, const Dims& d, const ScState* sc,
-                           cudaStream_t s)
+                           const ConvItem* list, int nitems, cudaStream_t s)
 {
     typedef typename CxT<C>::R RO;
     const int bytes = fft::XMajor<L>::kSmemElems * (int)sizeof(W);
     static cudaError_t once = fft_smem(fft_xi_kernel<L, C, W, RO>, bytes);
     if (once) return once;
     const int64_t nlines = (int64_t)((d.gy + 1) / 2) * d.gz;
-    fft_xi_kernel<L, C, W, RO><<<ceil_div64(nlines, fft::Shape<L>::W), fft::Shape<L>::THREADS, bytes, s>>>(S, phi, tw,
-                                                                                                          d, sc);
+    dim3 grid(ceil_div64(nlines, fft::Shape<L>::W), 1, nitems);
+    fft_xi_kernel<L, C, W, RO><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, phi, tw, d, sc, list);
     return cudaSuccess;
 }
 
 template <typename RI, typename C, typename W>
 static cudaError_t convolve_t(const RI* rho, C* S, const double* Ghat, typename CxT<C>::R* phi, const Dims& d,
-                              const W* tw_x, const W* tw_y, const W* tw_z, const ScState* sc, cudaStream_t s)
+                              const W* tw_x, const W* tw_y, const W* tw_z, const ScState* sc, cudaStream_t s,
+                              const ConvItem* list = nullptr, int nitems = 1)
 {
     cudaError_t e = cudaSuccess;
-#define SB2_XF(LL) case LL: e = pass_xf<LL, RI, C, W>(rho, S, tw_x, d, sc, s); break;
-#define SB2_YF(LL) case LL: e = pass_y<LL, C, W, false>(S, tw_y, d, sc, s); break;
-#define SB2_ZC(LL) case LL: e = pass_z<LL, C, W>(S, Ghat, tw_z, d, sc, s); break;
-#define SB2_YI(LL) case LL: e = pass_y<LL, C, W, true>(S, tw_y, d, sc, s); break;
-#define SB2_XI(LL) case LL: e = pass_xi<LL, C, W>(S, phi, tw_x, d, sc, s); break;
+#define SB2_XF(LL) case LL: e = pass_xf<LL, RI, C, W>(rho, S, tw_x, d, sc, list, nitems, s); break;
+#define SB2_YF(LL) case LL: e = pass_y<LL, C, W, false>(S, tw_y, d, sc, list, nitems, s); break;
+#define SB2_ZC(LL) case LL: e = pass_z<LL, C, W>(S, Ghat, tw_z, d, sc, list, nitems, s); break;
+#define SB2_YI(LL) case LL: e = pass_y<LL, C, W, true>(S, tw_y, d, sc, list, nitems, s); break;
+#define SB2_XI(LL) case LL: e = pass_xi<LL, C, W>(S, phi, tw_x, d, sc, list, nitems, s); break;
     switch (d.nx) { SB2_FFT_LENGTHS(SB2_XF) default: return cudaErrorInvalidValue; }
     if (e) return e;
     switch (d.ny) { SB2_FFT_LENGTHS(SB2_YF) default: return cudaErrorInvalidValue; }
@@ -1201,11 +1340,33 @@ cudaError_t launch_convolve_mixed(const MixedConv& m, float2* S, const double* G
     return convolve_t<double, float2, double2>(m.rho64, S, Ghat, phi, d, m.tw64[0], m.tw64[1], m.tw64[2], sc, s);
 }
 
+cudaError_t launch_convolve_list(int mode, const ConvItem* items, int nitems, const Dims& d, const double2* const* tw64,
+                                 const float2* const* tw32, cudaStream_t s)
+{
+    switch (mode) {
+    case 0:
+        return convolve_t<double, double2, double2>(nullptr, nullptr, nullptr, nullptr, d, tw64[0], tw64[1], tw64[2],
+                                                    nullptr, s, items, nitems);
+    case 1: // FP32 charge, FP32 butterflies
+        return convolve_t<float, float2, float2>(nullptr, nullptr, nullptr, nullptr, d, tw32[0], tw32[1], tw32[2],
+                                                 nullptr, s, items, nitems);
+    case 2: // FP64 charge, FP32 butterflies
+        return convolve_t<double, float2, float2>(nullptr, nullptr, nullptr, nullptr, d, tw32[0], tw32[1], tw32[2],
+                                                  nullptr, s, items, nitems);
+    case 3: // FP32 charge, FP64 butterflies
+        return convolve_t<float, float2, double2>(nullptr, nullptr, nullptr, nullptr, d, tw64[0], tw64[1], tw64[2],
+                                                  nullptr, s, items, nitems);
+    default: // FP64 charge, FP64 butterflies, FP32 spectrum
+        return convolve_t<double, float2, double2>(nullptr, nullptr, nullptr, nullptr, d, tw64[0], tw64[1], tw64[2],
+                                                   nullptr, s, items, nitems);
+    }
+}
+
 cudaError_t launch_efield(const double* phi, double2* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s)
 {
     int64_t total = (int64_t)gx * gy * gz;
     int nb = (int)std::min<int64_t>((total + 255) / 256, (int64_t)sm_count() * 16);
-    efield_kernel<double, double2><<<nb, 256, 0, s>>>(phi, E, gx, gy, gz, sc);
+    efield_kernel<double, double2><<<nb, 256, 0, s>>>(phi, E, gx, gy, gz, sc, nullptr);
     return cudaGetLastError();
 }
 
@@ -1213,7 +1374,18 @@ cudaError_t launch_efield_f32(const float* phi, float4* E, int gx, int gy, int g
 {
     int64_t total = (int64_t)gx * gy * gz;
     int nb = (int)std::min<int64_t>((total + 255) / 256, (int64_t)sm_count() * 16);
-    efield_kernel<float, float4><<<nb, 256, 0, s>>>(phi, E, gx, gy, gz, sc);
+    efield_kernel<float, float4><<<nb, 256, 0, s>>>(phi, E, gx, gy, gz, sc, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_efield_list(bool f32, const ConvItem* items, int nitems, int gx, int gy, int gz, cudaStream_t s)
+{
+    int64_t total = (int64_t)gx * gy * gz;
+    int nb = (int)std::min<int64_t>((total + 255) / 256, std::max<int64_t>(1, (int64_t)sm_count() * 16 / nitems));
+    if (f32)
+        efield_kernel<float, float4><<<dim3(nb, nitems), 256, 0, s>>>(nullptr, nullptr, gx, gy, gz, nullptr, items);
+    else
+        efield_kernel<double, double2><<<dim3(nb, nitems), 256, 0, s>>>(nullptr, nullptr, gx, gy, gz, nullptr, items);
     return cudaGetLastError();
 }
 

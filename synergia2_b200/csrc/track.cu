@@ -7,6 +7,8 @@
 namespace sb2 {
 
 cudaError_t launch_track_fast(const TrackParams& p, const TrackTune& t, cudaStream_t s); // track_fast.cu
+cudaError_t launch_track_list_fast(int choice, const TrackParams* const* items, const int* first, int nitems, int nblocks,
+                                   int max_ops, cudaStream_t s);
 
 // Masked sums for diagnostics: mean (6) or central second moments (21 lower
 // triangle) per block, core_diagnostics.cc:105-111,174-186.
@@ -136,6 +138,20 @@ int track_grid_blocks()
 cudaError_t launch_track(const TrackParams& p, const TrackTune& t, cudaStream_t s)
 {
     return p.fast_maps ? launch_track_fast(p, t, s) : exact::launch_pass(p, t, s);
+}
+
+int track_pass_choice(const TrackParams& p, const TrackTune& t) { return exact::pass_choice(p, t); }
+
+int track_pass_tile(int choice)
+{ // particles a block takes per iteration
+    return exact::kTrackThreads * ((choice == 2 || choice == 3 || choice == 5 || choice == 7) ? 2 : 1);
+}
+
+cudaError_t launch_track_list(int choice, bool fast_maps, const TrackParams* const* items, const int* first, int nitems,
+                              int nblocks, int max_ops, cudaStream_t s)
+{
+    return fast_maps ? launch_track_list_fast(choice, items, first, nitems, nblocks, max_ops, s)
+                     : exact::launch_pass_list(choice, items, first, nitems, nblocks, max_ops, s);
 }
 
 cudaError_t launch_moments(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,

@@ -11,4 +11,10 @@ cudaError_t launch_track_fast(const TrackParams& p, const TrackTune& t, cudaStre
     return fast::launch_pass(p, t, s);
 }
 
+cudaError_t launch_track_list_fast(int choice, const TrackParams* const* items, const int* first, int nitems, int nblocks,
+                                   int max_ops, cudaStream_t s)
+{
+    return fast::launch_pass_list(choice, items, first, nitems, nblocks, max_ops, s);
+}
+
 } // namespace sb2

@@ -822,9 +822,11 @@ __device__ __forceinline__ void load_tile(const TrackParams& p, int64_t base, Ra
 // PF: the next tile's loads are issued before the current tile is computed
 // (memory-bound passes: the loads of one tile overlap the arithmetic of the
 // previous one).
+// The pass over the particles of one bunch by the vg blocks of a grid
+// (vb: this block among them): a launch for one bunch uses the whole grid,
+// a work-list launch (track_list_kernel) a range of blocks per bunch.
 template <int VARIANT, int PPT, bool PF>
-__global__ void __launch_bounds__(kTrackThreads, PF ? SB2_LIGHT_OCC : TrackOcc<VARIANT, PPT>::value)
-    track_kernel(const __grid_constant__ TrackParams p)
+__device__ __forceinline__ void track_body(const TrackParams& p, const int vb, const int vg)
 {
     __shared__ int s_counts[kMaxOpsPerPass];
     __shared__ double s_mom[6][kTrackThreads]; // per-thread moment sums
@@ -836,10 +838,10 @@ __global__ void __launch_bounds__(kTrackThreads, PF ? SB2_LIGHT_OCC : TrackOcc<V
     const int64_t n = p.n;
     const int64_t S = p.stride;
     const int64_t tile = (int64_t)blockDim.x * PPT;
-    const int64_t gstride = (int64_t)gridDim.x * tile;
+    const int64_t gstride = (int64_t)vg * tile;
     RawPart nxt[PPT];
-    if (PF && (int64_t)blockIdx.x * tile < n) load_tile<PPT>(p, (int64_t)blockIdx.x * tile, nxt);
-    for (int64_t base = blockIdx.x * tile; base < n; base += gstride) {
+    if (PF && (int64_t)vb * tile < n) load_tile<PPT>(p, (int64_t)vb * tile, nxt);
+    for (int64_t base = (int64_t)vb * tile; base < n; base += gstride) {
         RawPart cur[PPT];
         if (PF) {
 #pragma unroll
@@ -899,8 +901,57 @@ __global__ void __launch_bounds__(kTrackThreads, PF ? SB2_LIGHT_OCC : TrackOcc<V
                 for (int j = 0; j < 6; ++j) s_mom[j][threadIdx.x] += s_mom[j][threadIdx.x + w];
             __syncthreads();
         }
-        if (threadIdx.x < 6) p.moment_partials[blockIdx.x * 6 + threadIdx.x] = s_mom[threadIdx.x][0];
+        if (threadIdx.x < 6) p.moment_partials[vb * 6 + threadIdx.x] = s_mom[threadIdx.x][0];
     }
+}
+
+template <int VARIANT, int PPT, bool PF>
+__global__ void __launch_bounds__(kTrackThreads, PF ? SB2_LIGHT_OCC : TrackOcc<VARIANT, PPT>::value)
+    track_kernel(const __grid_constant__ TrackParams p)
+{
+    track_body<VARIANT, PPT, PF>(p, blockIdx.x, gridDim.x);
+}
+
+// Block range of the work list: item i owns blocks [first[i], first[i+1]).
+__device__ __forceinline__ int list_item(const int* __restrict__ first, int nitems)
+{
+    int lo = 0, hi = nitems;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (first[mid] <= (int)blockIdx.x)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// A block's bunch parameters (header and its nops ops) copied from global
+// memory into dynamic shared memory: the op loop reads its descriptors
+// thousands of times per block, which from global memory costs an L1 round
+// trip each and from shared memory a broadcast.
+__device__ __forceinline__ const TrackParams& stage_params(const TrackParams* src)
+{
+    extern __shared__ __align__(16) unsigned char s_params[];
+    const int nops = src->nops;
+    const int words = (int)((offsetof(TrackParams, ops) + sizeof(MapOp) * (size_t)nops + 15) / 16);
+    const int4* from = (const int4*)src;
+    int4* to = (int4*)s_params;
+    for (int w = threadIdx.x; w < words; w += blockDim.x) to[w] = from[w];
+    __syncthreads();
+    return *(const TrackParams*)s_params;
+}
+
+// One launch for the passes of many bunches (a batch advanced in lockstep):
+// items[i] points at bunch i's parameters (only its nops ops are present;
+// the dynamic shared memory of the launch holds the largest of them).
+template <int VARIANT, int PPT, bool PF>
+__global__ void __launch_bounds__(kTrackThreads, PF ? SB2_LIGHT_OCC : TrackOcc<VARIANT, PPT>::value)
+    track_list_kernel(const TrackParams* const* __restrict__ items, const int* __restrict__ first, int nitems)
+{
+    const int it = list_item(first, nitems);
+    const TrackParams& p = stage_params(items[it]);
+    track_body<VARIANT, PPT, PF>(p, (int)blockIdx.x - first[it], first[it + 1] - first[it]);
 }
 
 // Light pass with the next tile's coordinates prefetched into shared memory
@@ -917,7 +968,7 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src)
 }
 
 template <int VARIANT>
-__global__ void __launch_bounds__(kTrackThreads, SB2_LIGHT_OCC) track_kernel_lds(const __grid_constant__ TrackParams p)
+__device__ __forceinline__ void track_body_lds(const TrackParams& p, const int vb, const int vg)
 {
     __shared__ int s_counts[kMaxOpsPerPass];
     __shared__ double s_mom[6][kTrackThreads]; // per-thread moment sums
@@ -930,14 +981,14 @@ __global__ void __launch_bounds__(kTrackThreads, SB2_LIGHT_OCC) track_kernel_lds
     const int64_t n = p.n;
     const int64_t S = p.stride;
     const int64_t tile = kTrackThreads;
-    const int64_t gstride = (int64_t)gridDim.x * tile;
+    const int64_t gstride = (int64_t)vg * tile;
     auto issue = [&](int buf, int64_t i) {
         if (i < n)
 #pragma unroll
             for (int j = 0; j < 6; ++j) cp_async8(&s_pf[buf][j][threadIdx.x], p.parts + i + j * S);
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    int64_t base = blockIdx.x * tile;
+    int64_t base = (int64_t)vb * tile;
     uint8_t m_next = 0;
     if (base < n) {
         issue(0, base + threadIdx.x);
@@ -994,8 +1045,23 @@ __global__ void __launch_bounds__(kTrackThreads, SB2_LIGHT_OCC) track_kernel_lds
                 for (int j = 0; j < 6; ++j) s_mom[j][threadIdx.x] += s_mom[j][threadIdx.x + w];
             __syncthreads();
         }
-        if (threadIdx.x < 6) p.moment_partials[blockIdx.x * 6 + threadIdx.x] = s_mom[threadIdx.x][0];
+        if (threadIdx.x < 6) p.moment_partials[vb * 6 + threadIdx.x] = s_mom[threadIdx.x][0];
     }
+}
+
+template <int VARIANT>
+__global__ void __launch_bounds__(kTrackThreads, SB2_LIGHT_OCC) track_kernel_lds(const __grid_constant__ TrackParams p)
+{
+    track_body_lds<VARIANT>(p, blockIdx.x, gridDim.x);
+}
+
+template <int VARIANT>
+__global__ void __launch_bounds__(kTrackThreads, SB2_LIGHT_OCC)
+    track_list_kernel_lds(const TrackParams* const* __restrict__ items, const int* __restrict__ first, int nitems)
+{
+    const int it = list_item(first, nitems);
+    const TrackParams& p = stage_params(items[it]);
+    track_body_lds<VARIANT>(p, (int)blockIdx.x - first[it], first[it + 1] - first[it]);
 }
 
 // true when the pass needs no integrator beyond the pure-quadrupole Yoshida
@@ -1020,6 +1086,50 @@ bool track_needs_full(const MapOp* ops, int n)
             return true;
     }
     return false;
+}
+
+// Kernel of a pass (the launch_pass dispatch below as a number): 0..3 light
+// shapes (lds, 1 with prefetch, 2 with prefetch, 2 without), 4/5 quadrupole
+// variant with 1/2 particles per thread, 6/7 wide full variant with 1/2,
+// 8 full variant at 3 CTAs/SM.
+int pass_choice(const TrackParams& p, const TrackTune& t)
+{
+    if (!track_needs_full(p.ops, p.nops))
+        return t.light_shape == 3 ? 0 : t.light_shape == 1 ? 1 : t.light_shape == 2 ? 2 : 3;
+    if (t.quad_variant && track_quad_only(p.ops, p.nops)) return t.quad_variant == 2 ? 5 : 4;
+    if (t.full_occ != 3) return t.full_ppt == 2 ? 7 : 6;
+    return 8;
+}
+
+// Work-list launch of passes that share a kernel choice: items[i] runs on
+// blocks [first[i], first[i+1]) of an nblocks grid.
+template <typename KERN>
+static cudaError_t list_launch(KERN* k, int nblocks, int smem, const TrackParams* const* items, const int* first,
+                               int nitems, cudaStream_t s)
+{
+    static cudaError_t once =
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrackParams) + 16);
+    if (once) return once;
+    k<<<nblocks, kTrackThreads, smem, s>>>(items, first, nitems);
+    return cudaGetLastError();
+}
+
+// max_ops: the largest op count among the items (sizes the staged parameters)
+cudaError_t launch_pass_list(int choice, const TrackParams* const* items, const int* first, int nitems, int nblocks,
+                             int max_ops, cudaStream_t s)
+{
+    const int smem = (int)((offsetof(TrackParams, ops) + sizeof(MapOp) * (size_t)max_ops + 15) / 16 * 16);
+    switch (choice) {
+    case 0: return list_launch(track_list_kernel_lds<TRACK_LIGHT>, nblocks, smem, items, first, nitems, s);
+    case 1: return list_launch(track_list_kernel<TRACK_LIGHT, 1, true>, nblocks, smem, items, first, nitems, s);
+    case 2: return list_launch(track_list_kernel<TRACK_LIGHT, 2, true>, nblocks, smem, items, first, nitems, s);
+    case 3: return list_launch(track_list_kernel<TRACK_LIGHT, 2, false>, nblocks, smem, items, first, nitems, s);
+    case 4: return list_launch(track_list_kernel<TRACK_QUAD, 1, false>, nblocks, smem, items, first, nitems, s);
+    case 5: return list_launch(track_list_kernel<TRACK_QUAD, 2, false>, nblocks, smem, items, first, nitems, s);
+    case 6: return list_launch(track_list_kernel<TRACK_FULL_WIDE, 1, false>, nblocks, smem, items, first, nitems, s);
+    case 7: return list_launch(track_list_kernel<TRACK_FULL_WIDE, 2, false>, nblocks, smem, items, first, nitems, s);
+    default: return list_launch(track_list_kernel<TRACK_FULL, 1, false>, nblocks, smem, items, first, nitems, s);
+    }
 }
 
 // The launch shape comes from the propagator's TrackTune (the measured

@@ -151,3 +151,80 @@ def test_batch_launch_query_matches_run(syn, monkeypatch):
         assert np.array_equal(p[:, 6], r[:, 6])
         for j in range(6):
             assert rel_l2(p[:, j], r[:, j]) <= 1e-10, (slot, j)
+
+
+def _lockstep_specs():
+    # quad-strength scan: own k1, bunch size and grid per job (two grid shapes)
+    return [(0.45, 30000, (16, 16, 32), 11), (0.6, 80000, (32, 32, 64), 12), (0.75, 20000, (16, 16, 32), 13),
+            (0.55, 50000, (32, 32, 64), 14), (0.7, 5000, (16, 16, 32), 15)]
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 1e-6)])
+def test_lockstep_batch_matches_alone(syn, precision, tol):
+    """Jobs advanced in lockstep (one work-list launch per kernel kind and
+    grid shape per step for all of them) give each job's result alone: ids
+    and masks exact; coordinates within the deposit-order tolerance (FP64
+    1e-10; mixed precision 1e-6, an FP32 rounding of the charge grid or the
+    spectrum can flip)."""
+    prec = getattr(syn.precision_t, precision)
+    specs = _lockstep_specs()
+    alone = []
+    for k1, n, shape, seed in specs:
+        prop, b = _job(syn, k1, n, shape, seed, prec, False)
+        prop.propagate(b, 3)
+        alone.append(b.get_particles())
+    batch = syn.Batch()
+    keep = []
+    for k1, n, shape, seed in specs:
+        prop, b = _job(syn, k1, n, shape, seed, prec, False)
+        keep.append((prop, b, batch.add(prop, b)))
+    batch.run_lockstep([slot for _, _, slot in keep], 2)
+    batch.run_lockstep([slot for _, _, slot in keep], 1)  # a second call continues from the first
+    for (prop, b, slot), (ap, am, _) in zip(keep, alone):
+        p, m, _ = b.get_particles()
+        assert np.array_equal(p[:, 6], ap[:, 6]) and np.array_equal(m, am)
+        for j in range(6):
+            assert rel_l2(p[:, j], ap[:, j]) <= tol, (slot, j)
+        assert b.get_total_num() == int(am.sum())
+
+
+def test_lockstep_batch_ring_losses_exact(syn):
+    """Ring cells with apertures in lockstep: lost sets, discards, counts and
+    real numbers equal the jobs run alone."""
+    from helpers import ring_cell
+    out = []
+    for lockstep in (False, True):
+        batch = syn.Batch()
+        keep = []
+        for i, (n, shape) in enumerate(((40000, (16, 16, 32)), (25000, (16, 16, 32)), (60000, (32, 32, 64)))):
+            lat, ref = product_lattice(ring_cell(radius=0.004 + 0.001 * i))
+            prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(*shape), 16))
+            b = syn.Bunch(ref, n, 1e11)
+            b.set_particles(gaussian_bunch(n, [2e-3, 1e-4, 2e-3, 1e-4, 0.3, 1e-4], 20 + i))
+            if lockstep:
+                keep.append((prop, b, batch.add(prop, b)))
+            else:
+                prop.propagate(b, 2)
+                keep.append((prop, b, None))
+        if lockstep:
+            batch.run_lockstep([slot for _, _, slot in keep], 2)
+        out.append([(b.get_particles(), b.counts()) for _, b, _ in keep])
+    for ((ap, am, ad), ac), ((lp, lm, ld), lc) in zip(out[0], out[1]):
+        assert np.array_equal(am, lm) and np.array_equal(ad, ld) and 0 < int(am.sum()) < len(am)
+        assert ac == lc
+        alive = am.astype(bool)
+        for j in range(6):
+            assert rel_l2(lp[alive, j], ap[alive, j]) <= 1e-10, j
+
+
+def test_lockstep_rejects_jobs_out_of_step(syn):
+    """Jobs whose turns have different step counts cannot share launches."""
+    batch = syn.Batch()
+    a = _job(syn, 0.6, 10000, (16, 16, 32), 1, syn.precision_t.fp64, False)
+    lat, ref = product_lattice(fodo_cell(0.6))
+    p2 = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(16, 16, 32), 4))
+    b2 = syn.Bunch(ref, 10000, 1e11)
+    b2.set_particles(gaussian_bunch(10000, SIG_C0, 2))
+    s1, s2 = batch.add(*a), batch.add(p2, b2)
+    with pytest.raises(syn.SB2Error, match="lockstep"):
+        batch.run_lockstep([s1, s2], 1)
