@@ -41,16 +41,54 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons of this process's GPU sampled during
+    the timed region: NVML polled every 2 ms from a thread (a timed region of
+    20 steps lasts only ~15 ms), the device matched by PCI bus id; falls back
+    to nvidia-smi (200 ms samples) when NVML is unavailable.  Read-only
+    queries: nothing about the GPU's settings is changed."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, dev):
         self.dev = dev
         self.p = None
+        self.thread = None
+        self.samples = []
+        self.smax = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.dev)
+        bus = "%08x:%02x:%02x.0" % (getattr(props, "pci_domain_id", 0), props.pci_bus_id, props.pci_device_id)
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
 
     def start(self):
+        try:
+            import threading
+            nv, h = self._nvml_handle()
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop_flag = threading.Event()
+
+            def poll():
+                while not self.stop_flag.is_set():
+                    try:
+                        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                             int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))))
+                    except Exception:
+                        pass
+                    time.sleep(0.002)
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            time.sleep(0.005)  # the first sample precedes the timed region
+            return
+        except Exception:
+            self.thread = None
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q,
                                        "--format=csv,noheader,nounits", "-lms", "200"],
@@ -59,6 +97,18 @@ class Clocks:
             self.p = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=1.0)
+            if not self.samples:
+                return None
+            reasons = set()
+            for _, r in self.samples:
+                for bit, nm in self.REASONS.items():
+                    if r & bit:
+                        reasons.add(nm)
+            return {"sm_mhz": statistics.median(c for c, _ in self.samples), "sm_max_mhz": self.smax,
+                    "reasons": sorted(reasons), "samples": len(self.samples), "source": "nvml, 2 ms"}
         if self.p is None:
             return None
         self.p.terminate()
@@ -84,7 +134,7 @@ class Clocks:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 def fp64_roofline(syn, workload, n, light, full):
@@ -170,23 +220,28 @@ def ring_c3(syn, torch, turns=1, warmup_steps=16):
         best, trials = prop.autotune(bunch, steps=16)
         torch.cuda.synchronize()
         L = syn.lib()
-        L.sb2_profile_enable(1)
-        for c in range(8):
-            L.sb2_profile_read(c, None, None, None, 1)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         prop.propagate_steps(bunch, warmup_steps, 384 * turns)
         e1.record()
         torch.cuda.synchronize()
-        L.sb2_profile_enable(0)
         ms = e0.elapsed_time(e1)
+        alive = bunch.get_total_num()
+        # breakdown: the first 96 steps of the next turn with CUDA events
+        # around every launch (outside the timed turn)
+        nprof = 96
+        L.sb2_profile_enable(1)
+        for c in range(8):
+            L.sb2_profile_read(c, None, None, None, 1)
+        prop.propagate_steps(bunch, warmup_steps + 384 * turns, nprof)
+        torch.cuda.synchronize()
+        L.sb2_profile_enable(0)
         brk, raw = {}, {}
         for c in range(8):
             nm, tot, cnt = ctypes.c_char_p(), ctypes.c_double(), ctypes.c_int64()
             syn.check(L.sb2_profile_read(c, ctypes.byref(nm), ctypes.byref(tot), ctypes.byref(cnt), 1))
-            brk[nm.value.decode()] = round(tot.value / (384 * turns), 4)
+            brk[nm.value.decode()] = round(tot.value / nprof, 4)
             raw[nm.value.decode()] = (tot.value, cnt.value)
-        alive = bunch.get_total_num()
         out[prec] = {"value": alive * 384 * turns / (ms * 1e-3), "ms_per_step": ms / (384 * turns), "alive": alive,
                      "step_breakdown_ms": brk, "emittance": [float(x) for x in bunch.moments()[2]],
                      "roofline_fp64": fp64_roofline(syn, "ring_c3", alive, raw.get("track", (0.0, 0)),
@@ -546,10 +601,9 @@ def main():
     barrier()
 
     # timed region: device time with CUDA events on the launching stream
+    # (the library's per-category profiler is off: its event pairs around
+    # every launch would be timed too)
     clocks = Clocks(local)
-    L.sb2_profile_enable(1)
-    for c in range(8):
-        L.sb2_profile_read(c, None, None, None, 1)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
@@ -558,14 +612,28 @@ def main():
     e1.record(stream)
     barrier()
     clk = clocks.stop()
-    L.sb2_profile_enable(0)
     ms = e0.elapsed_time(e1)
+    n_alive = bunch.get_total_num()
+
+    # the same K steps once more with the per-category profiler (CUDA events
+    # around every launch on the launching stream): the step breakdown and
+    # the kernels' launch times of the rooflines
+    L.sb2_profile_enable(1)
+    for c in range(8):
+        L.sb2_profile_read(c, None, None, None, 1)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    p0.record(stream)
+    prop.propagate_steps(bunch, args.warmup + args.steps, args.steps, stream=sp)
+    p1.record(stream)
+    barrier()
+    L.sb2_profile_enable(0)
+    prof_ms = p0.elapsed_time(p1)
     prof = {}
     for c in range(8):
         nm, tot, cnt = ctypes.c_char_p(), ctypes.c_double(), ctypes.c_int64()
         syn.check(L.sb2_profile_read(c, ctypes.byref(nm), ctypes.byref(tot), ctypes.byref(cnt), 1))
         prof[nm.value.decode()] = (tot.value, cnt.value)
-    n_alive = bunch.get_total_num()
 
     t_max, total_steps = over_ranks(dist, torch, ms, n_alive * args.steps, "cuda")
     value = total_steps / (t_max * 1e-3)
@@ -585,7 +653,7 @@ def main():
     t0 = time.perf_counter()
     syn.check(L.sb2_bunch_set_particles(bunch.h, pd, pm))
     if e2e_steps:
-        syn.check(L.sb2_propagator_propagate_steps(prop.h, bunch.h, args.warmup + args.steps, e2e_steps, sp))
+        syn.check(L.sb2_propagator_propagate_steps(prop.h, bunch.h, args.warmup + 2 * args.steps, e2e_steps, sp))
     syn.check(L.sb2_bunch_get_particles(bunch.h, pd, pm, None))
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
@@ -625,7 +693,9 @@ def main():
                        "global_batch": npart * world, "grid": list(GRID),
                        "precision": "fp64 (drop-in)", "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (bunch 235 MB per GPU)",
-                       "step_breakdown_ms": {k: round(v[0] / args.steps, 4) for k, v in prof.items()}},
+                       "step_breakdown_ms": {k: round(v[0] / args.steps, 4) for k, v in prof.items()},
+                       "step_breakdown_how": "a second run of the same K steps with CUDA events around every "
+                                             "launch (%.4f ms/step with those events)" % (prof_ms / args.steps)},
             "roofline": {"kernel": "track_kernel light variant (fused particle pass)", "bound": "hbm",
                          "achieved": achieved, "peak": pk["hbm_gbs"], "peak_source": src, "unit": "GB/s",
                          "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
@@ -645,7 +715,10 @@ def main():
         }
         if args.extras and world == 1 and npart == N_PART:
             out["mixed"] = mixed_vs_fp64(syn, torch, args.steps, args.warmup, passes=100)
-            out["served"] = served_stream(syn, 24, seed=3)
+            # a sample of the served-stream configuration: its job mix, sizes,
+            # grids and turns, Poisson arrivals
+            out["served"] = served_stream(syn, 16, seed=11, ring_fraction=0.5, nmax=8e6, turns_max=50,
+                                          grids=((32, 32, 64), (64, 64, 128), (128, 128, 256)), rate=4.0)
         if not args.no_cpu_baseline and world == 1 and npart == N_PART:
             out["cpu_baseline"] = cpu_baseline()
         print(json.dumps(out))

@@ -319,8 +319,9 @@ typedef struct sb2_tune {
 sb2_status sb2_propagator_get_tune(sb2_propagator* p, sb2_tune* out);
 sb2_status sb2_propagator_set_tune(sb2_propagator* p, const sb2_tune* in);
 /* Coordinate descent over the sb2_tune fields: every candidate propagates
- * `steps` steps of a scratch copy of `b` (timed with CUDA events) and the
- * fastest is kept and applied.  The bunch, diagnostics, loss and step
+ * `steps` untimed steps of a scratch copy of `b` (so the copy's cell order
+ * has aged as in a long run), then `steps` more timed with CUDA events, and
+ * the fastest is kept and applied.  The bunch, diagnostics, loss and step
  * records are left as they were.  trials (may be NULL) receives up to
  * max_trials rows of 7 doubles -- the six fields and the milliseconds --
  * and ntrials the number of trials run.  Not available on a sharded

@@ -2688,8 +2688,9 @@ struct Propagator {
 
     // ----- autotuning -------------------------------------------------------
     // Coordinate descent over the particle-pass launch shapes and the re-sort
-    // interval: every candidate propagates `steps` steps of a scratch copy of
-    // the bunch (CUDA events around the call) and the fastest is kept.  The
+    // interval: every candidate propagates `steps` untimed steps of a scratch
+    // copy of the bunch and then `steps` more timed with CUDA events, and the
+    // fastest is kept.  The
     // bunch, the diagnostics, the loss and step records and the per-element
     // lost charge are left as they were.  Each trial appends (light_shape,
     // full_occ, full_ppt, quad_variant, ctas_per_sm, sort_interval, ms).
@@ -2766,8 +2767,12 @@ struct Propagator {
                 t.design = b.design;
                 t.design_set = b.design_set;
                 t.turns_done = b.turns_done;
-                cuda_check(cudaEventRecord(e0, 0), "event");
+                // an untimed lead-in of the same length brings the scratch
+                // copy to the state the timed steps see in a long run (its
+                // cell order aged as the re-sort interval lets it)
                 propagate_steps(t, 0, steps, 0);
+                cuda_check(cudaEventRecord(e0, 0), "event");
+                propagate_steps(t, steps, steps, 0);
                 cuda_check(cudaEventRecord(e1, 0), "event");
                 cuda_check(cudaEventSynchronize(e1), "event");
                 float ms = 0.f;

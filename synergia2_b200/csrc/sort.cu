@@ -137,22 +137,24 @@ __global__ void scan_add_kernel(int32_t* out, int n, const int32_t* __restrict__
 // tile is then moved array by array through shared memory so that a warp's
 // stores cover whole runs of consecutive destinations (a nearly ordered
 // bunch keeps most of a tile's particles in a few cells) instead of one
-// scattered 8-byte store per lane.
+// scattered 8-byte store per lane.  The lanes of a warp with the same key
+// make one table insertion.
 constexpr int kTileThreads = 256;
 constexpr int kTile = 1024;
 constexpr int kTable = 2048; // hash slots (power of two)
 constexpr int kEmpty = -2;
 
-// open addressing with linear probing; returns the slot, and the particle's
-// rank inside its key (arrival order of the shared atomics)
-__device__ __forceinline__ int table_insert(int* t_key, int* t_cnt, int key, int& rank)
+// open addressing with linear probing; returns the slot, and the first of
+// `count` consecutive ranks inside its key (arrival order of the shared
+// atomics)
+__device__ __forceinline__ int table_insert_n(int* t_key, int* t_cnt, int key, int count, int& rank)
 {
     const unsigned h = (unsigned)key * 2654435761u; // multiplicative hashing (Knuth)
     int e = (int)(h >> 21) & (kTable - 1);
     for (int probe = 0; probe < kTable; ++probe) {
         const int old = atomicCAS(&t_key[e], kEmpty, key);
         if (old == kEmpty || old == key) {
-            rank = atomicAdd(&t_cnt[e], 1);
+            rank = atomicAdd(&t_cnt[e], count);
             return e;
         }
         e = (e + 1) & (kTable - 1);
@@ -190,12 +192,25 @@ __global__ void __launch_bounds__(kTileThreads) sort_scatter_tiled_kernel(
         for (int q = 0; q < PPT; ++q) {
             const int l = q * kTileThreads + threadIdx.x;
             ent[q] = -1;
+            int key = -1;
             if (l < tn) {
                 const int64_t i = base + l;
-                const int key = (!m_src[i] || !sc.valid)
-                                    ? G + 1
-                                    : cell_key(src[i], src[i + 2 * stride], src[i + 4 * stride], sc, gx, gy, gz);
-                ent[q] = table_insert(t_key, t_cnt, key, rnk[q]);
+                key = (!m_src[i] || !sc.valid) ? G + 1
+                                               : cell_key(src[i], src[i + 2 * stride], src[i + 4 * stride], sc, gx, gy, gz);
+            }
+            // lanes with the same key insert once: the lowest one reserves
+            // the group's ranks, the others take theirs by lane order
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            const int lead = __ffs(peers) - 1;
+            unsigned below;
+            asm("mov.u32 %0, %%lanemask_lt;" : "=r"(below));
+            int e = -1, r0 = 0;
+            if (key >= 0 && (int)(threadIdx.x & 31) == lead) e = table_insert_n(t_key, t_cnt, key, __popc(peers), r0);
+            e = __shfl_sync(0xffffffffu, e, lead);
+            r0 = __shfl_sync(0xffffffffu, r0, lead);
+            if (key >= 0) {
+                ent[q] = e;
+                rnk[q] = r0 + __popc(peers & below);
             }
         }
         __syncthreads();

@@ -64,8 +64,9 @@ def footprint_bytes(spec, precision=precision_t.mixed):
     spec_bytes = nz * ny * nkxp * (8 if precision == precision_t.mixed else 16)
     e_bytes = G * (16 if precision == precision_t.mixed else 32)
     phi_bytes = G * (4 if precision == precision_t.mixed else 8)
+    rho_bytes = G * (4 if precision == precision_t.mixed else 8)
     ghat = (nx // 2 + 1) * (ny // 2 + 1) * (nz // 2 + 1) * 8
-    return spec.n * (3 * 58 + 8) + 8 * G + spec_bytes + e_bytes + phi_bytes + ghat + (1 << 20)
+    return spec.n * (3 * 58 + 8) + rho_bytes + spec_bytes + e_bytes + phi_bytes + ghat + (1 << 20)
 
 
 def make_lattice(elements, kinetic_energy):
