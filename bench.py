@@ -227,6 +227,7 @@ def ring_c3(syn, torch, turns=1, warmup_steps=16):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         alive = bunch.get_total_num()
+        emit = [float(x) for x in bunch.moments()[2]]
         # breakdown: the first 96 steps of the next turn with CUDA events
         # around every launch (outside the timed turn)
         nprof = 96
@@ -243,7 +244,7 @@ def ring_c3(syn, torch, turns=1, warmup_steps=16):
             brk[nm.value.decode()] = round(tot.value / nprof, 4)
             raw[nm.value.decode()] = (tot.value, cnt.value)
         out[prec] = {"value": alive * 384 * turns / (ms * 1e-3), "ms_per_step": ms / (384 * turns), "alive": alive,
-                     "step_breakdown_ms": brk, "emittance": [float(x) for x in bunch.moments()[2]],
+                     "step_breakdown_ms": brk, "emittance": emit,
                      "roofline_fp64": fp64_roofline(syn, "ring_c3", alive, raw.get("track", (0.0, 0)),
                                                     raw.get("track_full", (0.0, 0))),
                      "autotune": {"best": best, "trials": len(trials), "default_ms": round(trials[0]["ms"], 3),
@@ -251,6 +252,9 @@ def ring_c3(syn, torch, turns=1, warmup_steps=16):
         del prop, bunch
         torch.cuda.empty_cache()
     out["value"] = out["mixed"]["value"]
+    # rms emittances of the two precisions after the same turns from one seed
+    out["emittance_rel_diff_xyz"] = [abs(a / b - 1.0) for a, b in zip(out["mixed"]["emittance"],
+                                                                     out["fp64"]["emittance"])]
     return out
 
 
@@ -518,6 +522,7 @@ def main():
                          "macroparticles, 128^2x256; c4: served job stream")
     ap.add_argument("--extras", type=int, default=1, help="0: skip the mixed-precision and served legs of c1")
     ap.add_argument("--jobs", type=int, default=48, help="c4: jobs in the served stream")
+    ap.add_argument("--turns", type=int, default=1, help="c3: turns of the ring per precision")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -536,7 +541,7 @@ def main():
         import synergia2_b200 as syn
         if rank == 0:
             if args.config == "c3":
-                r = ring_c3(syn, torch)
+                r = ring_c3(syn, torch, turns=args.turns)
                 if not args.no_cpu_baseline:
                     r["cpu_baseline"] = cpu_baseline_c3()
                 wl = ("24-cell ring (QF, SF thin, B 2 m, QD, SD thin; circular aperture 5 cm), 2^24 macroparticles, "
