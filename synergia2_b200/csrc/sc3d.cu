@@ -312,11 +312,15 @@ struct DepositSmem {
     // fixed-point scale: one addition carries the sum u <= 32 K of a warp's
     // peer group, so u * 2^kFrac <= 2^63 (three 21-bit digits)
     static constexpr int kFrac = K <= 4 ? 56 : 55;
+    // the chunk's particles in cell order, slot(i) = i + i / K
     double ox[kSlots], oy[kSlots], oz[kSlots];
-    int32_t cell[kSlots]; // ix | iy << 10 | iz << 20, or -1
-    uint32_t d0[kDepTile], d1[kDepTile], d2[kDepTile];
+    int16_t lk[kSlots];                             // tile cell of the stencil's lower corner
+    uint32_t d0[kDepTile], d1[kDepTile], d2[kDepTile]; // d0: cell counts, then offsets, then digit 0
     int32_t box[kDepT / 32][6];
+    int32_t wsum[kDepT / 32];
+    int32_t nvalid;
 };
+static_assert(kDepTile < 32768, "tile cells are stored as int16");
 
 // The 8 CIC weights of one particle divided by w0: products of the offsets
 // (deposit.cc:309-394 multiplies w0 in front; factored out here and applied
@@ -421,46 +425,51 @@ __device__ __forceinline__ void deposit_tile_body(const double* __restrict__ par
     const int64_t base = (int64_t)vb * (kDepT * K);
     const unsigned full = 0xffffffffu;
 
-    // 1. cells and offsets, coalesced
-    double px[K], py[K], pz[K];
-    uint8_t pm[K];
+    // 1. cells and offsets of this thread's K particles (stride kDepT), kept
+    //    in registers; the CTA's bounding box of stencil cells
+    int cell[K];
+    double ox[K], oy[K], oz[K];
+    {
+        double px[K], py[K], pz[K];
+        uint8_t pm[K];
 #pragma unroll
-    for (int j = 0; j < K; ++j) {
-        const int64_t i = base + j * kDepT + t;
-        pm[j] = 0;
-        if (i < n) {
-            pm[j] = masks[i];
-            px[j] = parts[i];
-            py[j] = parts[i + 2 * stride];
-            pz[j] = parts[i + 4 * stride];
+        for (int j = 0; j < K; ++j) {
+            const int64_t i = base + j * kDepT + t;
+            pm[j] = 0;
+            if (i < n) {
+                pm[j] = masks[i];
+                px[j] = parts[i];
+                py[j] = parts[i + 2 * stride];
+                pz[j] = parts[i + 4 * stride];
+            }
+        }
+        const double lx = sc.left[0], ly = sc.left[1], lz = sc.left[2];
+        const double ihx = sc.ih[0], ihy = sc.ih[1], ihz = sc.ih[2];
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            cell[j] = -1;
+            ox[j] = oy[j] = oz[j] = 0.0;
+            if (pm[j]) {
+                int ix, iy, iz;
+                leftmost_d(px[j], lx, ihx, ix, ox[j]);
+                leftmost_d(py[j], ly, ihy, iy, oy[j]);
+                leftmost_d(pz[j], lz, ihz, iz, oz[j]);
+                if (ix >= 0 && ix <= gx - 2 && iy >= 0 && iy <= gy - 2 && iz >= 0 && iz <= gz - 2)
+                    cell[j] = ix | (iy << 10) | (iz << 20);
+            }
         }
     }
     int bmin[3] = {1 << 30, 1 << 30, 1 << 30}, bmax[3] = {-1, -1, -1};
-    const double lx = sc.left[0], ly = sc.left[1], lz = sc.left[2];
-    const double ihx = sc.ih[0], ihy = sc.ih[1], ihz = sc.ih[2];
 #pragma unroll
-    for (int j = 0; j < K; ++j) {
-        const int li = j * kDepT + t;
-        const int s = li + li / K;
-        int32_t cell = -1;
-        double ox = 0.0, oy = 0.0, oz = 0.0;
-        if (pm[j]) {
-            int ix, iy, iz;
-            leftmost_d(px[j], lx, ihx, ix, ox);
-            leftmost_d(py[j], ly, ihy, iy, oy);
-            leftmost_d(pz[j], lz, ihz, iz, oz);
-            if (ix >= 0 && ix <= gx - 2 && iy >= 0 && iy <= gy - 2 && iz >= 0 && iz <= gz - 2) {
-                cell = ix | (iy << 10) | (iz << 20);
-                bmin[0] = min(bmin[0], ix); bmax[0] = max(bmax[0], ix);
-                bmin[1] = min(bmin[1], iy); bmax[1] = max(bmax[1], iy);
-                bmin[2] = min(bmin[2], iz); bmax[2] = max(bmax[2], iz);
+    for (int j = 0; j < K; ++j)
+        if (cell[j] >= 0) {
+            const int c[3] = {cell[j] & 1023, (cell[j] >> 10) & 1023, cell[j] >> 20};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                bmin[a] = min(bmin[a], c[a]);
+                bmax[a] = max(bmax[a], c[a]);
             }
         }
-        sm.cell[s] = cell;
-        sm.ox[s] = ox;
-        sm.oy[s] = oy;
-        sm.oz[s] = oz;
-    }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         bmin[a] = __reduce_min_sync(full, bmin[a]);
@@ -485,30 +494,93 @@ __device__ __forceinline__ void deposit_tile_body(const double* __restrict__ par
     const double w0 = sc.w0;
 
     if (V <= kDepTile) {
-        // 2. runs of equal cells into the fixed-point tile
+        // 2. counting sort of the chunk by tile cell: counts (warp-aggregated
+        //    32-bit shared atomics, which also give each particle its rank in
+        //    its cell), exclusive scan, particles written to their cell-ordered
+        //    slots.  Runs of equal cells are then as long as the chunk allows,
+        //    however far the particles have drifted since the bunch's last
+        //    re-sort.
+        int lk[K], rk[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            lk[j] = cell[j] < 0 ? -1
+                                : (((cell[j] >> 20) - bmin[2]) * BY + (((cell[j] >> 10) & 1023) - bmin[1])) * BX +
+                                      ((cell[j] & 1023) - bmin[0]);
+        for (int v = t; v < V; v += kDepT) sm.d0[v] = 0u;
+        __syncthreads();
+        unsigned below;
+        asm("mov.u32 %0, %%lanemask_lt;" : "=r"(below));
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const unsigned peers = __match_any_sync(full, lk[j]);
+            const int lead = __ffs(peers) - 1;
+            int r0 = 0;
+            if (lane == lead && lk[j] >= 0) r0 = (int)atomicAdd(&sm.d0[lk[j]], (uint32_t)__popc(peers));
+            rk[j] = __shfl_sync(full, r0, lead) + __popc(peers & below);
+        }
+        __syncthreads();
+        {   // exclusive scan of the counts, E consecutive cells per thread
+            const int E = (V + kDepT - 1) / kDepT;
+            const int v0 = t * E;
+            int tot = 0;
+            for (int e = 0; e < E; ++e)
+                if (v0 + e < V) tot += (int)sm.d0[v0 + e];
+            int inc = tot;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(full, inc, o);
+                if (lane >= o) inc += u;
+            }
+            if (lane == 31) sm.wsum[warp] = inc;
+            __syncthreads();
+            int run = inc - tot;
+            for (int w = 0; w < warp; ++w) run += sm.wsum[w];
+            if (t == kDepT - 1) sm.nvalid = run + tot;
+            for (int e = 0; e < E; ++e)
+                if (v0 + e < V) {
+                    const int c = (int)sm.d0[v0 + e];
+                    sm.d0[v0 + e] = (uint32_t)run;
+                    run += c;
+                }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            if (lk[j] >= 0) {
+                const int dest = (int)sm.d0[lk[j]] + rk[j];
+                const int sl = dest + dest / K;
+                sm.lk[sl] = (int16_t)lk[j];
+                sm.ox[sl] = ox[j];
+                sm.oy[sl] = oy[j];
+                sm.oz[sl] = oz[j];
+            }
+        __syncthreads();
+        const int nvalid = sm.nvalid;
         for (int v = t; v < V; v += kDepT) {
             sm.d0[v] = 0u;
             sm.d1[v] = 0u;
             sm.d2[v] = 0u;
         }
         __syncthreads();
+        // 3. each thread's K consecutive cell-ordered particles: runs of equal
+        //    cells summed in FP64 registers, finished runs into the tile
         const double scale = (double)(1ull << DepositSmem<K>::kFrac);
         const int off[8] = {0, 1, BX, BX + 1, BXY, BXY + 1, BXY + BX, BXY + BX + 1};
         int cur = -1;
         double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
         for (int j = 0; j < K; ++j) {
-            const int sj = t * (K + 1) + j;
-            const int32_t c = sm.cell[sj];
-            if (c < 0) continue;
-            const int lk = (((c >> 20) - bmin[2]) * BY + (((c >> 10) & 1023) - bmin[1])) * BX + ((c & 1023) - bmin[0]);
+            const int pos = t * K + j;
+            if (pos >= nvalid) continue;
+            const int sj = pos + pos / K;
+            const int c = sm.lk[sj];
             double u[8];
             cic_unit_weights(sm.ox[sj], sm.oy[sj], sm.oz[sj], u);
-            if (lk != cur) {
+            if (c != cur) {
                 if (cur >= 0)
 #pragma unroll
                     for (int q = 0; q < 8; ++q) tile_add(sm, cur + off[q], acc[q], scale);
-                cur = lk;
+                cur = c;
 #pragma unroll
                 for (int q = 0; q < 8; ++q) acc[q] = u[q];
             } else {
@@ -527,7 +599,7 @@ __device__ __forceinline__ void deposit_tile_body(const double* __restrict__ par
             for (int q = 0; q < 8; ++q) tile_add(sm, cur + off[q], acc[q], scale);
         }
         __syncthreads();
-        // 3. the tile's interior points to rho
+        // 4. the tile's interior points to rho
         const double back = w0 / scale;
         for (int v = t; v < V; v += kDepT) {
             const uint32_t a0 = sm.d0[v], a1 = sm.d1[v], a2 = sm.d2[v];
@@ -543,13 +615,11 @@ __device__ __forceinline__ void deposit_tile_body(const double* __restrict__ par
     }
 
     // box too large for the tile: per-warp peer groups straight to rho
-#pragma unroll 1
+#pragma unroll
     for (int j = 0; j < K; ++j) {
-        const int li = j * kDepT + t;
-        const int s = li + li / K;
-        const int32_t c = sm.cell[s];
+        const int c = cell[j];
         double w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        if (c >= 0) cic_weights(w0, sm.ox[s], sm.oy[s], sm.oz[s], w);
+        if (c >= 0) cic_weights(w0, ox[j], oy[j], oz[j], w);
         if (!peer_sum8(c, w) || c < 0) continue;
         const int ix = c & 1023, iy = (c >> 10) & 1023, iz = c >> 20;
         const bool x0 = ix > 0, x1 = ix + 1 < gx - 1;
