@@ -310,11 +310,16 @@ sb2_status sb2_propagator_read_losses(sb2_propagator* p, int32_t max_records, in
  * quadrupole Yoshida use the variant without the others, with one (1) or
  * two (2, at 2 CTAs per SM) particles per thread, or not (0);
  * ctas_per_sm: grid of the particle passes (1..12 x the SM count);
- * sort_interval: re-sort before every k-th space-charge kick.  The defaults
+ * sort_interval: re-sort before every k-th space-charge kick; fft_plan: radix
+ * plan of the FFT line passes (0: radix-8 passes first, 1: the radix-2/4
+ * pass first, for lengths that are not powers of 8); deposit_chunk:
+ * particles per thread of the tile deposit (4, 8; 0: warp groups with
+ * global atomics).  The defaults
  * are the values measured best on the FODO workload of 4M macroparticles
  * (light_shape 3). */
 typedef struct sb2_tune {
     int32_t light_shape, full_occ, full_ppt, quad_variant, ctas_per_sm, sort_interval;
+    int32_t fft_plan, deposit_chunk;
 } sb2_tune;
 sb2_status sb2_propagator_get_tune(sb2_propagator* p, sb2_tune* out);
 sb2_status sb2_propagator_set_tune(sb2_propagator* p, const sb2_tune* in);

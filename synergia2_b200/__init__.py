@@ -617,7 +617,8 @@ class Propagator:
         check(lib().sb2_propagator_read_losses(self.h, cap, ctypes.byref(n), _pd(out)))
         return out[: n.value]
 
-    _TUNE_FIELDS = ("light_shape", "full_occ", "full_ppt", "quad_variant", "ctas_per_sm", "sort_interval")
+    _TUNE_FIELDS = ("light_shape", "full_occ", "full_ppt", "quad_variant", "ctas_per_sm", "sort_interval",
+                    "fft_plan", "deposit_chunk")
 
     def get_tune(self):
         """Launch shape of the particle passes and the re-sort interval
@@ -639,12 +640,13 @@ class Propagator:
         configuration and the list of trials (fields + milliseconds)."""
         best = _lib.sb2_tune()
         cap = 64
-        trials = np.zeros(7 * cap)
+        nf = len(self._TUNE_FIELDS)
+        trials = np.zeros((nf + 1) * cap)
         nt = ctypes.c_int32()
         check(lib().sb2_propagator_autotune(self.h, bunch.h, int(steps), ctypes.byref(best), _pd(trials), cap,
                                             ctypes.byref(nt)))
-        rows = trials[: 7 * min(nt.value, cap)].reshape(-1, 7)
-        log = [dict(zip(self._TUNE_FIELDS + ("ms",), [int(v) for v in r[:6]] + [float(r[6])])) for r in rows]
+        rows = trials[: (nf + 1) * min(nt.value, cap)].reshape(-1, nf + 1)
+        log = [dict(zip(self._TUNE_FIELDS + ("ms",), [int(v) for v in r[:nf]] + [float(r[nf])])) for r in rows]
         return {k: getattr(best, k) for k in self._TUNE_FIELDS}, log
 
     def set_step_counts(self, capacity):

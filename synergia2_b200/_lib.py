@@ -50,7 +50,8 @@ _pstate = _c.POINTER(sb2_bunch_state)
 
 class sb2_tune(ctypes.Structure):
     _fields_ = [("light_shape", _c.c_int32), ("full_occ", _c.c_int32), ("full_ppt", _c.c_int32),
-                ("quad_variant", _c.c_int32), ("ctas_per_sm", _c.c_int32), ("sort_interval", _c.c_int32)]
+                ("quad_variant", _c.c_int32), ("ctas_per_sm", _c.c_int32), ("sort_interval", _c.c_int32),
+                ("fft_plan", _c.c_int32), ("deposit_chunk", _c.c_int32)]
 
 
 class sb2_step_counts(ctypes.Structure):

@@ -99,7 +99,10 @@ struct Dft<8> {
     }
 };
 
-// Radix plan: 8 while at least 8 remains, then 4 or 2; REV runs it backwards.
+// Radix plans.  A length L = 8^k * rem (rem 1, 2 or 4) takes k radix-8
+// passes and, if rem > 1, one pass of radix rem: plan 0 runs the 8s first,
+// plan 1 the radix-rem pass first (the autotuner picks one per propagator);
+// REV runs a plan backwards.  Lengths that are powers of 8 have one plan.
 __host__ __device__ constexpr int npasses(int L)
 {
     int n = 0;
@@ -109,27 +112,39 @@ __host__ __device__ constexpr int npasses(int L)
     }
     return n;
 }
-__host__ __device__ constexpr int radix_fwd(int L, int p)
+__host__ __device__ constexpr int rem_radix(int L)
 {
-    for (int i = 0; i < p; ++i) L /= (L >= 8 ? 8 : L);
-    return L >= 8 ? 8 : L;
+    while (L >= 8) L /= 8;
+    return L;
 }
-template <int L, bool REV>
+__host__ __device__ constexpr int radix_fwd(int L, int p, int plan)
+{
+    const int rem = rem_radix(L), n = npasses(L);
+    if (rem == 1) return 8;
+    return plan == 0 ? (p < n - 1 ? 8 : rem) : (p == 0 ? rem : 8);
+}
+// the plan a length actually has (1 only where the two plans differ)
+template <int L>
+__host__ __device__ constexpr int plan_of(int plan)
+{
+    return rem_radix(L) > 1 ? plan : 0;
+}
+template <int L, bool REV, int PLAN = 0>
 __host__ __device__ constexpr int radix_at(int p)
 {
-    return REV ? radix_fwd(L, npasses(L) - 1 - p) : radix_fwd(L, p);
+    return REV ? radix_fwd(L, npasses(L) - 1 - p, PLAN) : radix_fwd(L, p, PLAN);
 }
-template <int L, bool REV>
+template <int L, bool REV, int PLAN = 0>
 __host__ __device__ constexpr int span_at(int p)
 {
     int ns = 1;
-    for (int i = 0; i < p; ++i) ns *= radix_at<L, REV>(i);
+    for (int i = 0; i < p; ++i) ns *= radix_at<L, REV, PLAN>(i);
     return ns;
 }
-template <int L, bool REV>
-__host__ __device__ constexpr int first_radix() { return radix_at<L, REV>(0); }
-template <int L, bool REV>
-__host__ __device__ constexpr int last_radix() { return radix_at<L, REV>(npasses(L) - 1); }
+template <int L, bool REV, int PLAN = 0>
+__host__ __device__ constexpr int first_radix() { return radix_at<L, REV, PLAN>(0); }
+template <int L, bool REV, int PLAN = 0>
+__host__ __device__ constexpr int last_radix() { return radix_at<L, REV, PLAN>(npasses(L) - 1); }
 
 // CTA shape for length L: 256 threads up to L = 512 (two CTAs per SM at the
 // pass kernels' ~110 registers, so one CTA's loads overlap another's
@@ -224,20 +239,20 @@ __device__ __forceinline__ int io_pos(int t, int e)
 // The passes of one transform.  On entry v holds the first pass's inputs,
 // on return the last pass's outputs.  Every thread of the CTA calls it (it
 // synchronises the CTA).
-template <int L, bool REV, class LAY, int P = 0, typename C>
+template <int L, bool REV, class LAY, int PLAN = 0, int P = 0, typename C>
 __device__ __forceinline__ void run_passes(C* v, int li, int t, C* sm, const C* __restrict__ tw, bool inv)
 {
     if constexpr (P < npasses(L)) {
-        constexpr int R = radix_at<L, REV>(P);
-        constexpr int Ns = span_at<L, REV>(P);
+        constexpr int R = radix_at<L, REV, PLAN>(P);
+        constexpr int Ns = span_at<L, REV, PLAN>(P);
         pass_math<L, R, C>(v, t, Ns, tw, inv);
         if constexpr (P + 1 < npasses(L)) {
-            constexpr int R2 = radix_at<L, REV>(P + 1);
+            constexpr int R2 = radix_at<L, REV, PLAN>(P + 1);
             pass_store<L, R, LAY, C>(v, li, t, Ns, sm);
             __syncthreads();
             pass_load<L, R2, LAY, C>(v, li, t, sm);
             __syncthreads();
-            run_passes<L, REV, LAY, P + 1, C>(v, li, t, sm, tw, inv);
+            run_passes<L, REV, LAY, PLAN, P + 1, C>(v, li, t, sm, tw, inv);
         }
     }
 }

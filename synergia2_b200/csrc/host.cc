@@ -1891,6 +1891,7 @@ struct SpaceCharge {
     float2 *tw32_x = nullptr, *tw32_y = nullptr, *tw32_z = nullptr;
     int fp32_butterflies = 0;
     bool last_rho32 = false; // the last solve's charge is in rho32
+    int deposit_chunk = deposit_default_chunk(); // particles per thread of the tile deposit (0: warp groups)
     ScState* state = nullptr;
     double* mom_partials = nullptr;
     int n_partials = 0;
@@ -2056,12 +2057,14 @@ struct SpaceCharge {
             ProfScope ps(PROF_DEPOSIT, s);
             if (last_rho32) {
                 cuda_check(cudaMemsetAsync(rho32, 0, sizeof(float) * G, s), "memset rho");
-                cuda_check(launch_deposit_f32(b.parts, b.stride, b.masks, b.n, state, rho32, d.gx, d.gy, d.gz, s),
+                cuda_check(launch_deposit_f32_k(deposit_chunk, b.parts, b.stride, b.masks, b.n, state, rho32, d.gx,
+                                                d.gy, d.gz, s),
                            "deposit");
             } else {
                 if (!rho) rho = dalloc<double>(G, "rho"); // mixed precision with an exchange: FP64 charge
                 cuda_check(cudaMemsetAsync(rho, 0, sizeof(double) * G, s), "memset rho");
-                cuda_check(launch_deposit(b.parts, b.stride, b.masks, b.n, state, rho, d.gx, d.gy, d.gz, s),
+                cuda_check(launch_deposit_k(deposit_chunk, b.parts, b.stride, b.masks, b.n, state, rho, d.gx, d.gy,
+                                            d.gz, s),
                            "deposit");
             }
         }
@@ -2450,6 +2453,13 @@ struct Propagator {
     bool cell_sort = true;
     int sort_interval = 4; // re-sort before every k-th space-charge kick (measured best of 1, 2, 4, 8 at 4M particles)
     TrackTune tune = track_tune_defaults(); // launch shape of the particle passes
+    // space-charge launch shapes: FFT radix plan of the line passes, particles
+    // per thread of the tile deposit
+    struct SolveTune {
+        int fft_plan = 0;
+        int deposit_chunk = deposit_default_chunk();
+        bool operator==(const SolveTune& o) const { return fft_plan == o.fft_plan && deposit_chunk == o.deposit_chunk; }
+    } solve_tune;
     int32_t* sort_scratch = nullptr; // histogram, offsets, cursors and block sums of the counting sort
 
     Propagator(const Lattice& l, int stepper_kind, int n, const sb2_sc3d_options* opts)
@@ -2557,7 +2567,11 @@ struct Propagator {
     void ensure_device()
     {
         if (!engine_) engine_.reset(new Engine());
-        if (has_sc && !sc) sc.reset(new SpaceCharge(sc_opts));
+        if (has_sc && !sc) {
+            sc.reset(new SpaceCharge(sc_opts));
+            sc->d.plan = solve_tune.fft_plan;
+            sc->deposit_chunk = solve_tune.deposit_chunk;
+        }
         engine_->hook = &hook;
         engine_->tune = tune;
         if (sc) sc->hook = &hook;
@@ -2687,21 +2701,27 @@ struct Propagator {
     std::vector<std::array<double, 3>> loss_tags;
 
     // ----- autotuning -------------------------------------------------------
-    // Coordinate descent over the particle-pass launch shapes and the re-sort
-    // interval: every candidate propagates `steps` untimed steps of a scratch
-    // copy of the bunch and then `steps` more timed with CUDA events, and the
-    // fastest is kept.  The
-    // bunch, the diagnostics, the loss and step records and the per-element
-    // lost charge are left as they were.  Each trial appends (light_shape,
-    // full_occ, full_ppt, quad_variant, ctas_per_sm, sort_interval, ms).
-    void apply_tune(const TrackTune& t, int si)
+    // Coordinate descent over the particle-pass launch shapes, the re-sort
+    // interval, the FFT radix plan and the deposit tile chunk: every
+    // candidate propagates `steps` untimed steps of a scratch copy of the
+    // bunch and then `steps` more timed with CUDA events, and the fastest is
+    // kept.  The bunch, the diagnostics, the loss and step records and the
+    // per-element lost charge are left as they were.  Each trial appends (light_shape,
+    // full_occ, full_ppt, quad_variant, ctas_per_sm, sort_interval, fft_plan,
+    // deposit_chunk, ms).
+    void apply_tune(const TrackTune& t, int si, const SolveTune& st)
     {
         tune = t;
         sort_interval = si;
+        solve_tune = st;
         if (engine_) engine_->tune = t;
+        if (sc) {
+            sc->d.plan = st.fft_plan;
+            sc->deposit_chunk = st.deposit_chunk;
+        }
         drop_graphs();
     }
-    void autotune(Bunch& b, int steps, std::vector<std::array<double, 7>>& log)
+    void autotune(Bunch& b, int steps, std::vector<std::array<double, 9>>& log)
     {
         if (hook) throw Error(SB2_ERR_UNSUPPORTED, "autotuning is not available on a sharded propagator");
         if (steps < 1) throw Error(SB2_ERR_INVALID, "autotune: steps must be >= 1");
@@ -2724,6 +2744,7 @@ struct Propagator {
         const bool keep_graphs = use_graphs;
         const TrackTune t0 = tune;
         const int si0 = sort_interval;
+        const SolveTune st0 = solve_tune;
         diag_cap = 0;
         loss_cap = 0;
         step_rec_cap = 0;
@@ -2746,8 +2767,8 @@ struct Propagator {
         try {
             cuda_check(cudaEventCreate(&e0), "event");
             cuda_check(cudaEventCreate(&e1), "event");
-            auto trial = [&](const TrackTune& tt, int si) -> double {
-                apply_tune(tt, si);
+            auto trial = [&](const TrackTune& tt, int si, const SolveTune& st) -> double {
+                apply_tune(tt, si, st);
                 t.drop_work();
                 t.kicks_since_sort = 0;
                 if (b.n) {
@@ -2778,50 +2799,65 @@ struct Propagator {
                 float ms = 0.f;
                 cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event");
                 log.push_back({(double)tt.light_shape, (double)tt.full_occ, (double)tt.full_ppt,
-                               (double)tt.quad_variant, (double)tt.ctas_per_sm, (double)si, (double)ms});
+                               (double)tt.quad_variant, (double)tt.ctas_per_sm, (double)si, (double)st.fft_plan,
+                               (double)st.deposit_chunk, (double)ms});
                 return ms;
             };
-            trial(t0, si0); // warm-up: allocations of the scratch working copy
+            trial(t0, si0, st0); // warm-up: allocations of the scratch working copy
             log.clear();
             TrackTune best = t0;
             int best_si = si0;
-            double best_ms = trial(best, best_si);
-            auto consider = [&](TrackTune c, int si) {
-                if (!std::memcmp(&c, &best, sizeof(c)) && si == best_si) return;
-                const double ms = trial(c, si);
+            SolveTune best_st = st0;
+            double best_ms = trial(best, best_si, best_st);
+            auto consider = [&](TrackTune c, int si, SolveTune st) {
+                if (!std::memcmp(&c, &best, sizeof(c)) && si == best_si && st == best_st) return;
+                const double ms = trial(c, si, st);
                 if (ms < best_ms) {
                     best_ms = ms;
                     best = c;
                     best_si = si;
+                    best_st = st;
                 }
             };
             for (int v : {1, 3, 2, 0}) {
                 TrackTune c = best;
                 c.light_shape = v;
-                consider(c, best_si);
+                consider(c, best_si, best_st);
             }
             const int fulls[3][2] = {{2, 1}, {2, 2}, {3, 1}};
             for (auto& f : fulls) {
                 TrackTune c = best;
                 c.full_occ = f[0];
                 c.full_ppt = f[1];
-                consider(c, best_si);
+                consider(c, best_si, best_st);
             }
             for (int v : {1, 2, 0}) {
                 TrackTune c = best;
                 c.quad_variant = v;
-                consider(c, best_si);
+                consider(c, best_si, best_st);
             }
             for (int v : {4, 8, 12}) {
                 TrackTune c = best;
                 c.ctas_per_sm = v;
-                consider(c, best_si);
+                consider(c, best_si, best_st);
             }
             if (has_sc && cell_sort)
-                for (int v : {2, 4, 8}) consider(best, v);
-            apply_tune(best, best_si);
+                for (int v : {2, 4, 8}) consider(best, v, best_st);
+            if (has_sc) {
+                for (int v : {0, 1}) { // FFT radix plans
+                    SolveTune st = best_st;
+                    st.fft_plan = v;
+                    consider(best, best_si, st);
+                }
+                for (int v : {4, 8}) { // deposit tile: particles per thread
+                    SolveTune st = best_st;
+                    st.deposit_chunk = v;
+                    consider(best, best_si, st);
+                }
+            }
+            apply_tune(best, best_si, best_st);
         } catch (...) {
-            apply_tune(t0, si0);
+            apply_tune(t0, si0, st0);
             restore();
             throw;
         }
@@ -3241,7 +3277,7 @@ struct Batch {
             std::vector<std::vector<size_t>> groups;
             auto key_of = [&](const LaunchRec& r) {
                 std::vector<int> key = {r.kind, r.choice, r.fast ? 1 : 0, r.f32 ? 1 : 0, r.d.gx, r.d.gy, r.d.gz,
-                                        r.linear, r.mode};
+                                        r.d.plan, r.linear, r.mode};
                 return key;
             };
             {
@@ -4299,6 +4335,9 @@ static void check_tune(const sb2_tune& t)
     SB2_REQUIRE(t.quad_variant >= 0 && t.quad_variant <= 2, "tune: quad_variant is 0, 1 or 2");
     SB2_REQUIRE(t.ctas_per_sm >= 1 && t.ctas_per_sm <= kMaxCtasPerSm, "tune: ctas_per_sm is 1..12");
     SB2_REQUIRE(t.sort_interval >= 1, "tune: sort_interval >= 1");
+    SB2_REQUIRE(t.fft_plan == 0 || t.fft_plan == 1, "tune: fft_plan is 0 or 1");
+    SB2_REQUIRE(t.deposit_chunk == 0 || t.deposit_chunk == 4 || t.deposit_chunk == 8,
+                "tune: deposit_chunk is 0, 4 or 8");
 }
 
 static sb2_tune export_tune(const Propagator& P)
@@ -4310,6 +4349,8 @@ static sb2_tune export_tune(const Propagator& P)
     t.quad_variant = P.tune.quad_variant;
     t.ctas_per_sm = P.tune.ctas_per_sm;
     t.sort_interval = P.sort_interval;
+    t.fft_plan = P.solve_tune.fft_plan;
+    t.deposit_chunk = P.solve_tune.deposit_chunk;
     return t;
 }
 
@@ -4327,7 +4368,10 @@ sb2_status sb2_propagator_set_tune(sb2_propagator* p, const sb2_tune* in)
     SB2_REQUIRE(p && in, "null argument");
     check_tune(*in);
     TrackTune t{in->light_shape, in->full_occ, in->full_ppt, in->quad_variant, in->ctas_per_sm};
-    p->p->apply_tune(t, in->sort_interval);
+    Propagator::SolveTune st;
+    st.fft_plan = in->fft_plan;
+    st.deposit_chunk = in->deposit_chunk;
+    p->p->apply_tune(t, in->sort_interval, st);
     SB2_CATCH
 }
 
@@ -4336,14 +4380,14 @@ sb2_status sb2_propagator_autotune(sb2_propagator* p, sb2_bunch* b, int32_t step
 {
     SB2_TRY
     SB2_REQUIRE(p && b, "null argument");
-    std::vector<std::array<double, 7>> log;
+    std::vector<std::array<double, 9>> log;
     p->p->autotune(b->b, steps, log);
     if (best) *best = export_tune(*p->p);
     const int n = (int)log.size();
     if (ntrials) *ntrials = n;
     if (trials)
         for (int i = 0; i < std::min(n, (int)max_trials); ++i)
-            for (int j = 0; j < 7; ++j) trials[7 * i + j] = log[i][j];
+            for (int j = 0; j < 9; ++j) trials[9 * i + j] = log[i][j];
     SB2_CATCH
 }
 

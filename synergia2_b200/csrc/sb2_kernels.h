@@ -64,6 +64,7 @@ struct Dims {
     int nx, ny, nz;    // doubled grid
     int nkx, nkxp;     // nx/2+1, padded row pitch of S
     int lx, ly, lz;    // log2 of nx, ny, nz
+    int plan;          // FFT radix plan of the line passes (fft.cuh): 0 radix 8 first, 1 the remainder first
 };
 
 // Working copy of a bunch ordered by deposit cell (sort.cu), double-buffered.
@@ -160,6 +161,14 @@ cudaError_t launch_shard_count(const BunchCounters* c, double* xchg, cudaStream_
 cudaError_t launch_shard_total(BunchCounters* c, const double* xchg, cudaStream_t s);
 cudaError_t launch_deposit(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
                            const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s);
+// with an explicit chunk: 4 or 8 particles per thread of the tile deposit,
+// 0 the warp-group deposit (FP64 grid only); the default chunk comes from
+// SB2_DEPOSIT / SB2_DEPOSIT_K (4 unless set)
+int deposit_default_chunk();
+cudaError_t launch_deposit_k(int chunk, const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
+                             const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s);
+cudaError_t launch_deposit_f32_k(int chunk, const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
+                                 const ScState* sc, float* rho, int gx, int gy, int gz, cudaStream_t s);
 // the same deposit into an FP32 charge grid (the tiles' sums are exact; only
 // the merge of neighbouring tiles rounds to FP32)
 cudaError_t launch_deposit_f32(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,

@@ -775,7 +775,7 @@ template <typename W> __device__ __forceinline__ W czero() { return cvt_c<W>(mak
 // XF: pairs of real rows (y, y+1) of rho -> S rows (r2c, first gx inputs).
 // Lines l = (pair, z); the last pass goes through shared memory so that
 // each output k can combine Z[k] and Z[L-k].
-template <int L, typename RI, typename C, typename W>
+template <int L, int PLAN, typename RI, typename C, typename W>
 __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xf_kernel(const RI* __restrict__ rho, C* S,
                                                                         const W* __restrict__ tw, Dims d,
                                                                         const ScState* __restrict__ scp,
@@ -789,7 +789,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xf_kernel(const RI
     typedef fft::XMajor<L> LAY;
     typedef typename CxT<W>::R R;
     constexpr int NW = fft::Shape<L>::W, TPL = fft::Shape<L>::TPL;
-    constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
+    constexpr int R0 = fft::first_radix<L, false, PLAN>(), RL = fft::last_radix<L, false, PLAN>();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     W* sm = (W*)sm_raw;
     if (!scp->valid) return;
@@ -812,7 +812,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xf_kernel(const RI
             if (yb < d.gy) v[e].y = (R)rb[pos];
         }
     }
-    fft::run_passes<L, false, LAY>(v, li, t, sm, tw, false);
+    fft::run_passes<L, false, LAY, PLAN>(v, li, t, sm, tw, false);
 #pragma unroll
     for (int e = 0; e < fft::kE; ++e) sm[LAY::at(li, fft::io_pos<L, RL>(t, e))] = v[e];
     __syncthreads();
@@ -829,7 +829,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xf_kernel(const RI
 
 // Y passes: lines (kx, z < gz) along y, NW consecutive kx per CTA.  forward:
 // first gy inputs, all ny outputs; inverse: all inputs, first gy outputs.
-template <int L, typename C, typename W, bool INV>
+template <int L, int PLAN, typename C, typename W, bool INV>
 __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_y_kernel(C* S, const W* __restrict__ tw, Dims d,
                                                                        const ScState* __restrict__ scp,
                                                                        const ConvItem* __restrict__ list)
@@ -840,7 +840,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_y_kernel(C* S, con
     }
     typedef fft::LMajor<L> LAY;
     constexpr int NW = fft::Shape<L>::W;
-    constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
+    constexpr int R0 = fft::first_radix<L, false, PLAN>(), RL = fft::last_radix<L, false, PLAN>();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     W* sm = (W*)sm_raw;
     if (!scp->valid) return;
@@ -855,7 +855,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_y_kernel(C* S, con
         const int pos = fft::io_pos<L, R0>(t, e);
         v[e] = (ok && pos < nin) ? cvt_c<W>(col[(int64_t)pos * d.nkxp]) : czero<W>();
     }
-    fft::run_passes<L, false, LAY>(v, li, t, sm, tw, INV);
+    fft::run_passes<L, false, LAY, PLAN>(v, li, t, sm, tw, INV);
     if (!ok) return;
     const int nout = INV ? d.gy : L;
 #pragma unroll
@@ -870,7 +870,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_y_kernel(C* S, con
 // (radices reversed, so it starts from the registers), first gz outputs.
 // (alg_cplx_multiplier space_charge_3d_open_hockney.cc:350-372 fused between
 // the transforms.)
-template <int L, typename C, typename W>
+template <int L, int PLAN, typename C, typename W>
 __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_z_conv_kernel(C* S, const double* __restrict__ Ghat,
                                                                             const W* __restrict__ tw, Dims d,
                                                                             const ScState* __restrict__ scp,
@@ -884,8 +884,8 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_z_conv_kernel(C* S
     typedef fft::LMajor<L> LAY;
     typedef typename CxT<W>::R R;
     constexpr int NW = fft::Shape<L>::W;
-    constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
-    constexpr int RI = fft::last_radix<L, true>();
+    constexpr int R0 = fft::first_radix<L, false, PLAN>(), RL = fft::last_radix<L, false, PLAN>();
+    constexpr int RI = fft::last_radix<L, true, PLAN>();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     W* sm = (W*)sm_raw;
     if (!scp->valid) return;
@@ -900,7 +900,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_z_conv_kernel(C* S
         const int pos = fft::io_pos<L, R0>(t, e);
         v[e] = (ok && pos < d.gz) ? cvt_c<W>(col[pos * zs]) : czero<W>();
     }
-    fft::run_passes<L, false, LAY>(v, li, t, sm, tw, false);
+    fft::run_passes<L, false, LAY, PLAN>(v, li, t, sm, tw, false);
     const int ogx = d.nx / 2 + 1, ogy = d.ny / 2 + 1;
     const int my = ky <= d.ny / 2 ? ky : d.ny - ky;
     const double* gcol = Ghat + (int64_t)my * ogx + (ok ? kx : 0);
@@ -911,7 +911,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_z_conv_kernel(C* S
         const R g = ok ? (R)__ldg(&gcol[(int64_t)mz * ogy * ogx]) : (R)0;
         v[e] = fft::mk(v[e], v[e].x * g, v[e].y * g);
     }
-    fft::run_passes<L, true, LAY>(v, li, t, sm, tw, true);
+    fft::run_passes<L, true, LAY, PLAN>(v, li, t, sm, tw, true);
     if (!ok) return;
 #pragma unroll
     for (int e = 0; e < fft::kE; ++e) {
@@ -923,7 +923,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_z_conv_kernel(C* S
 // XI: Hermitian pairs of spectrum rows -> real rows (y, y+1) of phi (c2r,
 // first gx outputs); imaginary parts of the k = 0 and k = nx/2 terms are
 // ignored as a c2r transform does.
-template <int L, typename C, typename W, typename RO>
+template <int L, int PLAN, typename C, typename W, typename RO>
 __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xi_kernel(const C* __restrict__ S, RO* phi,
                                                                         const W* __restrict__ tw, Dims d,
                                                                         const ScState* __restrict__ scp,
@@ -936,7 +936,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xi_kernel(const C*
     }
     typedef fft::XMajor<L> LAY;
     constexpr int NW = fft::Shape<L>::W;
-    constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
+    constexpr int R0 = fft::first_radix<L, false, PLAN>(), RL = fft::last_radix<L, false, PLAN>();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     W* sm = (W*)sm_raw;
     if (!scp->valid) return;
@@ -970,7 +970,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xi_kernel(const C*
         }
         v[e] = fft::mk(A, A.x - B.y, A.y + B.x);
     }
-    fft::run_passes<L, false, LAY>(v, li, t, sm, tw, true);
+    fft::run_passes<L, false, LAY, PLAN>(v, li, t, sm, tw, true);
     if (!ok) return;
     RO* pa = phi + ((int64_t)z * d.gy + ya) * d.gx;
     RO* pb = phi + ((int64_t)z * d.gy + yb) * d.gx;
@@ -991,7 +991,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xi_kernel(const C*
 // one complex transform (lines 2c and 2c+1 as its real and imaginary parts)
 // and come out as its real and imaginary parts.  Axis 0 (x rows, contiguous)
 // uses the x-major tile; axes 1 and 2 take W consecutive line pairs.
-template <int L, int AXIS>
+template <int L, int AXIS, int PLAN>
 __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_green_kernel(double* G,
                                                                            const double2* __restrict__ tw, int ox,
                                                                            int oy, int oz,
@@ -1004,7 +1004,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_green_kernel(doubl
     }
     typedef typename std::conditional<AXIS == 0, fft::XMajor<L>, fft::LMajor<L>>::type LAY;
     constexpr int W = fft::Shape<L>::W;
-    constexpr int R0 = fft::first_radix<L, false>(), RL = fft::last_radix<L, false>();
+    constexpr int R0 = fft::first_radix<L, false, PLAN>(), RL = fft::last_radix<L, false, PLAN>();
     constexpr int half = L / 2;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     double2* sm = (double2*)sm_raw;
@@ -1031,7 +1031,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_green_kernel(doubl
         const int m = j <= half ? j : L - j;
         v[e] = make_double2(oka ? ga[m * sj] : 0.0, okb ? gb[m * sj] : 0.0);
     }
-    fft::run_passes<L, false, LAY>(v, li, t, sm, tw, false);
+    fft::run_passes<L, false, LAY, PLAN>(v, li, t, sm, tw, false);
     double* wa = G + (oka ? line_base(la) : 0);
     double* wb = G + (okb ? line_base(lb) : 0);
 #pragma unroll
@@ -1191,6 +1191,27 @@ static int deposit_variant()
     return v;
 }
 
+int deposit_default_chunk() { return deposit_variant(); }
+
+cudaError_t launch_deposit_k(int chunk, const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
+                             const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s)
+{
+    switch (chunk) {
+    case 4: return deposit_tile<4, double>(parts, stride, masks, n, sc, rho, gx, gy, gz, s);
+    case 8: return deposit_tile<8, double>(parts, stride, masks, n, sc, rho, gx, gy, gz, s);
+    default:
+        deposit_kernel<<<sm_count() * SB2_DEPOSIT_CTAS, 256, 0, s>>>(parts, stride, masks, n, sc, rho, gx, gy, gz);
+        return cudaGetLastError();
+    }
+}
+
+cudaError_t launch_deposit_f32_k(int chunk, const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
+                                 const ScState* sc, float* rho, int gx, int gy, int gz, cudaStream_t s)
+{
+    return chunk == 8 ? deposit_tile<8, float>(parts, stride, masks, n, sc, rho, gx, gy, gz, s)
+                      : deposit_tile<4, float>(parts, stride, masks, n, sc, rho, gx, gy, gz, s);
+}
+
 cudaError_t launch_deposit(const double* parts, int64_t stride, const uint8_t* masks, int64_t n,
                            const ScState* sc, double* rho, int gx, int gy, int gz, cudaStream_t s)
 {
@@ -1247,30 +1268,30 @@ static cudaError_t fft_smem(KERN* k, int bytes)
 // in lockstep, nitems bunches of the same grid shape whose pointers are in
 // the device array `list` (the kernels take item blockIdx.z, or blockIdx.y
 // for the field and the octant).
-template <int L>
+template <int L, int PLAN>
 static cudaError_t green_passes_axis0(double* G, const double2* tw, int ox, int oy, int oz, const ScState* sc,
                                       const ConvItem* list, int nitems, cudaStream_t s)
 {
     typedef fft::XMajor<L> LAY;
     const int bytes = LAY::kSmemElems * 16;
-    static cudaError_t once = fft_smem(fft_green_kernel<L, 0>, bytes);
+    static cudaError_t once = fft_smem(fft_green_kernel<L, 0, PLAN>, bytes);
     if (once) return once;
     const int64_t pairs = ((int64_t)oy * oz + 1) / 2;
     dim3 grid(ceil_div64(pairs, fft::Shape<L>::W), 1, nitems);
-    fft_green_kernel<L, 0><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(G, tw, ox, oy, oz, sc, list);
+    fft_green_kernel<L, 0, PLAN><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(G, tw, ox, oy, oz, sc, list);
     return cudaSuccess;
 }
-template <int L, int AXIS>
+template <int L, int AXIS, int PLAN>
 static cudaError_t green_passes_lmajor(double* G, const double2* tw, int ox, int oy, int oz, const ScState* sc,
                                        const ConvItem* list, int nitems, cudaStream_t s)
 {
     typedef fft::LMajor<L> LAY;
     const int bytes = LAY::kSmemElems * 16;
-    static cudaError_t once = fft_smem(fft_green_kernel<L, AXIS>, bytes);
+    static cudaError_t once = fft_smem(fft_green_kernel<L, AXIS, PLAN>, bytes);
     if (once) return once;
     const int64_t nlines = AXIS == 1 ? (int64_t)ox * oz : (int64_t)ox * oy;
     dim3 grid(ceil_div64((nlines + 1) / 2, fft::Shape<L>::W), 1, nitems);
-    fft_green_kernel<L, AXIS><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(G, tw, ox, oy, oz, sc, list);
+    fft_green_kernel<L, AXIS, PLAN><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(G, tw, ox, oy, oz, sc, list);
     return cudaSuccess;
 }
 
@@ -1281,9 +1302,12 @@ static cudaError_t green_t(const ScState* sc, double* G, const Dims& d, int line
     const int nb = list ? std::max(1, sm_count() * 4 / nitems) : sm_count() * 4;
     green_octant_kernel<<<dim3(nb, nitems), 256, 0, s>>>(sc, G, d.gx, d.gy, d.gz, linear, list);
     cudaError_t e = cudaSuccess;
-#define SB2_G0(LL) case LL: e = green_passes_axis0<LL>(G, tw_x, ox, oy, oz, sc, list, nitems, s); break;
-#define SB2_G1(LL) case LL: e = green_passes_lmajor<LL, 1>(G, tw_y, ox, oy, oz, sc, list, nitems, s); break;
-#define SB2_G2(LL) case LL: e = green_passes_lmajor<LL, 2>(G, tw_z, ox, oy, oz, sc, list, nitems, s); break;
+#define SB2_G0(LL) case LL: e = d.plan ? green_passes_axis0<LL, fft::plan_of<LL>(1)>(G, tw_x, ox, oy, oz, sc, list, nitems, s) \
+                                   : green_passes_axis0<LL, 0>(G, tw_x, ox, oy, oz, sc, list, nitems, s); break;
+#define SB2_G1(LL) case LL: e = d.plan ? green_passes_lmajor<LL, 1, fft::plan_of<LL>(1)>(G, tw_y, ox, oy, oz, sc, list, nitems, s) \
+                                   : green_passes_lmajor<LL, 1, 0>(G, tw_y, ox, oy, oz, sc, list, nitems, s); break;
+#define SB2_G2(LL) case LL: e = d.plan ? green_passes_lmajor<LL, 2, fft::plan_of<LL>(1)>(G, tw_z, ox, oy, oz, sc, list, nitems, s) \
+                                   : green_passes_lmajor<LL, 2, 0>(G, tw_z, ox, oy, oz, sc, list, nitems, s); break;
     switch (d.nx) { SB2_FFT_LENGTHS(SB2_G0) default: return cudaErrorInvalidValue; }
     if (e) return e;
     switch (d.ny) { SB2_FFT_LENGTHS(SB2_G1) default: return cudaErrorInvalidValue; }
@@ -1309,51 +1333,51 @@ cudaError_t launch_green_list(const ConvItem* items, int nitems, const Dims& d, 
     return green_t(nullptr, nullptr, d, linear, tw_x, tw_y, tw_z, items, nitems, s);
 }
 
-template <int L, typename RI, typename C, typename W>
+template <int L, int PLAN, typename RI, typename C, typename W>
 static cudaError_t pass_xf(const RI* rho, C* S, const W* tw, const Dims& d, const ScState* sc, const ConvItem* list,
                            int nitems, cudaStream_t s)
 {
     const int bytes = fft::XMajor<L>::kSmemElems * (int)sizeof(W);
-    static cudaError_t once = fft_smem(fft_xf_kernel<L, RI, C, W>, bytes);
+    static cudaError_t once = fft_smem(fft_xf_kernel<L, PLAN, RI, C, W>, bytes);
     if (once) return once;
     const int64_t nlines = (int64_t)((d.gy + 1) / 2) * d.gz;
     dim3 grid(ceil_div64(nlines, fft::Shape<L>::W), 1, nitems);
-    fft_xf_kernel<L, RI, C, W><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(rho, S, tw, d, sc, list);
+    fft_xf_kernel<L, PLAN, RI, C, W><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(rho, S, tw, d, sc, list);
     return cudaSuccess;
 }
-template <int L, typename C, typename W, bool INV>
+template <int L, int PLAN, typename C, typename W, bool INV>
 static cudaError_t pass_y(C* S, const W* tw, const Dims& d, const ScState* sc, const ConvItem* list, int nitems,
                           cudaStream_t s)
 {
     const int bytes = fft::LMajor<L>::kSmemElems * (int)sizeof(W);
-    static cudaError_t once = fft_smem(fft_y_kernel<L, C, W, INV>, bytes);
+    static cudaError_t once = fft_smem(fft_y_kernel<L, PLAN, C, W, INV>, bytes);
     if (once) return once;
     dim3 grid(ceil_div64(d.nkx, fft::Shape<L>::W), d.gz, nitems);
-    fft_y_kernel<L, C, W, INV><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, tw, d, sc, list);
+    fft_y_kernel<L, PLAN, C, W, INV><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, tw, d, sc, list);
     return cudaSuccess;
 }
-template <int L, typename C, typename W>
+template <int L, int PLAN, typename C, typename W>
 static cudaError_t pass_z(C* S, const double* Ghat, const W* tw, const Dims& d, const ScState* sc, const ConvItem* list,
                           int nitems, cudaStream_t s)
 {
     const int bytes = fft::LMajor<L>::kSmemElems * (int)sizeof(W);
-    static cudaError_t once = fft_smem(fft_z_conv_kernel<L, C, W>, bytes);
+    static cudaError_t once = fft_smem(fft_z_conv_kernel<L, PLAN, C, W>, bytes);
     if (once) return once;
     dim3 grid(ceil_div64(d.nkx, fft::Shape<L>::W), d.ny, nitems);
-    fft_z_conv_kernel<L, C, W><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, Ghat, tw, d, sc, list);
+    fft_z_conv_kernel<L, PLAN, C, W><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, Ghat, tw, d, sc, list);
     return cudaSuccess;
 }
-template <int L, typename C, typename W>
+template <int L, int PLAN, typename C, typename W>
 static cudaError_t pass_xi(const C* S, typename CxT<C>::R* phi, const W* tw, const Dims& d, const ScState* sc,
                            const ConvItem* list, int nitems, cudaStream_t s)
 {
     typedef typename CxT<C>::R RO;
     const int bytes = fft::XMajor<L>::kSmemElems * (int)sizeof(W);
-    static cudaError_t once = fft_smem(fft_xi_kernel<L, C, W, RO>, bytes);
+    static cudaError_t once = fft_smem(fft_xi_kernel<L, PLAN, C, W, RO>, bytes);
     if (once) return once;
     const int64_t nlines = (int64_t)((d.gy + 1) / 2) * d.gz;
     dim3 grid(ceil_div64(nlines, fft::Shape<L>::W), 1, nitems);
-    fft_xi_kernel<L, C, W, RO><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, phi, tw, d, sc, list);
+    fft_xi_kernel<L, PLAN, C, W, RO><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, phi, tw, d, sc, list);
     return cudaSuccess;
 }
 
@@ -1363,11 +1387,16 @@ static cudaError_t convolve_t(const RI* rho, C* S, const double* Ghat, typename 
                               const ConvItem* list = nullptr, int nitems = 1)
 {
     cudaError_t e = cudaSuccess;
-#define SB2_XF(LL) case LL: e = pass_xf<LL, RI, C, W>(rho, S, tw_x, d, sc, list, nitems, s); break;
-#define SB2_YF(LL) case LL: e = pass_y<LL, C, W, false>(S, tw_y, d, sc, list, nitems, s); break;
-#define SB2_ZC(LL) case LL: e = pass_z<LL, C, W>(S, Ghat, tw_z, d, sc, list, nitems, s); break;
-#define SB2_YI(LL) case LL: e = pass_y<LL, C, W, true>(S, tw_y, d, sc, list, nitems, s); break;
-#define SB2_XI(LL) case LL: e = pass_xi<LL, C, W>(S, phi, tw_x, d, sc, list, nitems, s); break;
+#define SB2_XF(LL) case LL: e = d.plan ? pass_xf<LL, fft::plan_of<LL>(1), RI, C, W>(rho, S, tw_x, d, sc, list, nitems, s) \
+                                   : pass_xf<LL, 0, RI, C, W>(rho, S, tw_x, d, sc, list, nitems, s); break;
+#define SB2_YF(LL) case LL: e = d.plan ? pass_y<LL, fft::plan_of<LL>(1), C, W, false>(S, tw_y, d, sc, list, nitems, s) \
+                                   : pass_y<LL, 0, C, W, false>(S, tw_y, d, sc, list, nitems, s); break;
+#define SB2_ZC(LL) case LL: e = d.plan ? pass_z<LL, fft::plan_of<LL>(1), C, W>(S, Ghat, tw_z, d, sc, list, nitems, s) \
+                                   : pass_z<LL, 0, C, W>(S, Ghat, tw_z, d, sc, list, nitems, s); break;
+#define SB2_YI(LL) case LL: e = d.plan ? pass_y<LL, fft::plan_of<LL>(1), C, W, true>(S, tw_y, d, sc, list, nitems, s) \
+                                   : pass_y<LL, 0, C, W, true>(S, tw_y, d, sc, list, nitems, s); break;
+#define SB2_XI(LL) case LL: e = d.plan ? pass_xi<LL, fft::plan_of<LL>(1), C, W>(S, phi, tw_x, d, sc, list, nitems, s) \
+                                   : pass_xi<LL, 0, C, W>(S, phi, tw_x, d, sc, list, nitems, s); break;
     switch (d.nx) { SB2_FFT_LENGTHS(SB2_XF) default: return cudaErrorInvalidValue; }
     if (e) return e;
     switch (d.ny) { SB2_FFT_LENGTHS(SB2_YF) default: return cudaErrorInvalidValue; }

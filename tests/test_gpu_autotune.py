@@ -1,7 +1,8 @@
-"""The project's autotuner over the particle-pass launch shapes and the
-re-sort interval (sb2_propagator_autotune): it leaves the bunch and the
-propagator's records untouched, applies the fastest configuration, and
-every configuration computes the same results."""
+"""The project's autotuner over the particle-pass launch shapes, the
+re-sort interval, the FFT radix plan and the deposit tile chunk
+(sb2_propagator_autotune): it leaves the bunch and the propagator's records
+untouched, applies the fastest configuration, and every configuration
+computes the same results."""
 import numpy as np
 import pytest
 
@@ -55,6 +56,29 @@ def test_gpu_launch_shapes_with_space_charge(syn):
             assert rel_l2(parts[:, j], out[0][:, j]) <= 1e-12, j
 
 
+@pytest.mark.parametrize("grid", [(16, 16, 32), (8, 32, 64)])
+def test_gpu_fft_plans_and_deposit_chunks_agree(syn, grid):
+    """Both FFT radix plans (the doubled lengths 16, 32 and 128 are not powers
+    of 8, so the plans differ there) and every deposit chunk give the same
+    particles to the FFT's and the deposit's rounding."""
+    n = 40000
+    p = gaussian_bunch(n, SIG_C0, 54)
+    lat, ref = product_lattice(fodo_cell())
+    out = []
+    for plan, chunk in ((0, 4), (1, 4), (0, 8), (1, 8), (0, 0)):
+        prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(*grid), 8))
+        prop.set_tune(fft_plan=plan, deposit_chunk=chunk)
+        assert prop.get_tune()["fft_plan"] == plan and prop.get_tune()["deposit_chunk"] == chunk
+        b = syn.Bunch(ref, n, 1e11)
+        b.set_particles(p)
+        prop.propagate(b, 2)
+        out.append(b.get_particles()[0])
+    for parts in out[1:]:
+        assert np.array_equal(parts[:, 6], out[0][:, 6])
+        for j in range(6):
+            assert rel_l2(parts[:, j], out[0][:, j]) <= 1e-12, j
+
+
 def test_gpu_autotune_leaves_state_and_applies_best(syn):
     """autotune: trials cover every knob, the fastest is applied, the bunch
     (particles, state), per-turn diagnostics and step records are unchanged,
@@ -78,6 +102,7 @@ def test_gpu_autotune_leaves_state_and_applies_best(syn):
     assert len(log) >= 10
     assert {r["light_shape"] for r in log} == {0, 1, 2, 3} and {r["ctas_per_sm"] for r in log} == {4, 8, 12}
     assert {r["sort_interval"] for r in log} == {2, 4, 8}
+    assert {r["fft_plan"] for r in log} == {0, 1} and {r["deposit_chunk"] for r in log} == {4, 8}
     fastest = min(log, key=lambda r: r["ms"])
     assert best == {k: fastest[k] for k in best} == prop.get_tune()
     after = b.get_particles()
@@ -101,3 +126,7 @@ def test_gpu_tune_validation(syn):
         prop.set_tune(ctas_per_sm=13)
     with pytest.raises(syn.SB2Error, match="full_occ"):
         prop.set_tune(full_occ=1)
+    with pytest.raises(syn.SB2Error, match="fft_plan"):
+        prop.set_tune(fft_plan=2)
+    with pytest.raises(syn.SB2Error, match="deposit_chunk"):
+        prop.set_tune(deposit_chunk=6)
