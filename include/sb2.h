@@ -269,6 +269,15 @@ sb2_status sb2_propagator_sc_last(sb2_propagator* p, double left[3], double h[3]
  * returns to a whole bunch. */
 typedef int32_t (*sb2_allreduce_fn)(void* ctx, double* data, int64_t count, int32_t on_host);
 sb2_status sb2_propagator_set_allreduce(sb2_propagator* p, sb2_allreduce_fn fn, void* ctx, int32_t on_host);
+/* Typed sum-allreduce, the MPI_Allreduce(MPI_SUM) of the reference with its
+ * datatype: dtype 0 = double, 1 = float; on_host as above.  With a typed
+ * callback a mixed-precision propagator exchanges its FP32 charge grid as
+ * float (half the bytes of the FP64 grid); the domain moments and valid
+ * counts stay double.  Replaces the untyped callback (and is replaced by
+ * it); fn = NULL returns to a whole bunch. */
+typedef int32_t (*sb2_allreduce_typed_fn)(void* ctx, void* data, int64_t count, int32_t dtype, int32_t on_host);
+sb2_status sb2_propagator_set_allreduce_typed(sb2_propagator* p, sb2_allreduce_typed_fn fn, void* ctx,
+                                              int32_t on_host);
 /* Inside a sum-allreduce callback: the cudaStream_t of the exchange (the
  * stream of the propagate call); NULL outside a callback. */
 void* sb2_allreduce_stream(void);

@@ -578,15 +578,35 @@ class Propagator:
         check(lib().sb2_propagator_graph_stats(self.h, ctypes.byref(c), ctypes.byref(r)))
         return c.value, r.value
 
-    def set_allreduce(self, fn, on_host=True):
+    def set_allreduce(self, fn, on_host=True, typed=False):
         """Run this propagator on one shard of a bunch split over ranks
         (sb2_propagator_set_allreduce).  on_host: fn(array) receives a numpy
         view of pinned host memory and sums it in place over the ranks;
-        otherwise fn(pointer, count) gets the device pointer.  None returns
-        to a whole bunch."""
+        otherwise fn(pointer, count) gets the device pointer.  typed
+        (sb2_propagator_set_allreduce_typed): the buffers are float64 or
+        float32 -- the array's dtype on the host, fn(pointer, count, dtype)
+        on the device, dtype a numpy dtype -- so a mixed-precision
+        propagator exchanges its FP32 charge grid as float.  None returns to
+        a whole bunch."""
         if fn is None:
             self._allreduce = None
             check(lib().sb2_propagator_set_allreduce(self.h, None, None, 0))
+            return
+        if typed:
+            def tcb(ctx, data, count, dtype, host):
+                try:
+                    dt = np.dtype(np.float32 if dtype == 1 else np.float64)
+                    if host:
+                        buf = (ctypes.c_char * (int(count) * dt.itemsize)).from_address(data)
+                        fn(np.frombuffer(buf, dtype=dt))
+                    else:
+                        fn(int(data), int(count), dt)
+                    return 0
+                except Exception:  # reported as a failed collective
+                    return 1
+
+            self._allreduce = _lib.ALLREDUCE_TYPED_FN(tcb)  # kept alive with the propagator
+            check(lib().sb2_propagator_set_allreduce_typed(self.h, self._allreduce, None, 1 if on_host else 0))
             return
 
         def cb(ctx, data, count, host):

@@ -125,6 +125,7 @@ SIGNATURES = {
     "sb2_sc3d_last": (_i32, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd]),
     "sb2_sc3d_apply_noalloc": (_i32, [_popts, _vp, _i64, _vp, _i64, _i32, _d, _i32, _d, _d, _i32, _d, _vp]),
     "sb2_allreduce_stream": (_vp, []),
+    "sb2_propagator_set_allreduce_typed": (_i32, [_vp, _vp, _vp, _i32]),
     "sb2_batch_run_lockstep": (_i32, [_vp, _pi32, _i32, _i32]),
     "sb2_libff_apply": (_i32, [_vp, _pd, _i32, _vp, _vp]),
     "sb2_aperture_apply": (_i32, [_vp, _i32, _cp, _vp, _pi32, _vp]),
@@ -156,6 +157,8 @@ def lib():
 
 # sb2_allreduce_fn: int32_t (*)(void* ctx, double* data, int64_t count, int32_t on_host)
 ALLREDUCE_FN = _c.CFUNCTYPE(_c.c_int32, _c.c_void_p, _c.POINTER(_c.c_double), _c.c_int64, _c.c_int32)
+# sb2_allreduce_typed_fn: int32_t (*)(void* ctx, void* data, int64_t count, int32_t dtype, int32_t on_host)
+ALLREDUCE_TYPED_FN = _c.CFUNCTYPE(_c.c_int32, _c.c_void_p, _c.c_void_p, _c.c_int64, _c.c_int32, _c.c_int32)
 
 
 def check(rc):

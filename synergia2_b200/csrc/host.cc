@@ -1826,41 +1826,57 @@ static thread_local cudaStream_t g_hook_stream = nullptr;
 
 struct AllreduceHook {
     sb2_allreduce_fn fn = nullptr;
+    sb2_allreduce_typed_fn tfn = nullptr; // typed: FP32 buffers too
     void* ctx = nullptr;
     int on_host = 0;
-    double* pinned = nullptr;
-    size_t pinned_n = 0;
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
     ~AllreduceHook()
     {
         if (pinned) cudaFreeHost(pinned);
     }
-    explicit operator bool() const { return fn != nullptr; }
+    explicit operator bool() const { return fn != nullptr || tfn != nullptr; }
+    bool typed() const { return tfn != nullptr; }
     // Host buffers: the stream is drained, the data staged through pinned
-    // memory, summed by fn and copied back.  Device buffers: fn is called at
-    // once with the device pointer and must order its collective on the
-    // library's stream (sb2_allreduce_stream() inside the callback), so
-    // nothing waits on the host.
-    void run(double* dev, int64_t n, cudaStream_t s)
+    // memory, summed by the callback and copied back.  Device buffers: the
+    // callback is called at once with the device pointer and must order its
+    // collective on the library's stream (sb2_allreduce_stream() inside the
+    // callback), so nothing waits on the host.
+    void run(double* dev, int64_t n, cudaStream_t s) { run_bytes(dev, n, 0, s); }
+    void run(float* dev, int64_t n, cudaStream_t s)
+    {
+        if (!tfn) throw Error(SB2_ERR_RUNTIME, "FP32 exchange without a typed allreduce");
+        run_bytes(dev, n, 1, s);
+    }
+
+  private:
+    int32_t call(void* data, int64_t n, int dtype, int host)
+    {
+        return tfn ? tfn(ctx, data, n, dtype, host) : fn(ctx, (double*)data, n, host);
+    }
+    void run_bytes(void* dev, int64_t n, int dtype, cudaStream_t s)
     {
         struct StreamScope {
             cudaStream_t prev;
             explicit StreamScope(cudaStream_t st) : prev(g_hook_stream) { g_hook_stream = st; }
             ~StreamScope() { g_hook_stream = prev; }
         } scope(s);
+        const size_t bytes = (size_t)n * (dtype ? sizeof(float) : sizeof(double));
         int32_t rc;
         if (on_host) {
             cuda_check(cudaStreamSynchronize(s), "allreduce");
-            if (pinned_n < (size_t)n) {
+            if (pinned_bytes < bytes) {
                 if (pinned) cudaFreeHost(pinned);
                 pinned = nullptr;
-                cuda_check(cudaMallocHost((void**)&pinned, sizeof(double) * n), "allreduce staging");
-                pinned_n = n;
+                pinned_bytes = 0;
+                cuda_check(cudaMallocHost(&pinned, bytes), "allreduce staging");
+                pinned_bytes = bytes;
             }
-            cuda_check(cudaMemcpy(pinned, dev, sizeof(double) * n, cudaMemcpyDeviceToHost), "allreduce staging");
-            rc = fn(ctx, pinned, n, 1);
-            cuda_check(cudaMemcpy(dev, pinned, sizeof(double) * n, cudaMemcpyHostToDevice), "allreduce staging");
+            cuda_check(cudaMemcpy(pinned, dev, bytes, cudaMemcpyDeviceToHost), "allreduce staging");
+            rc = call(pinned, n, dtype, 1);
+            cuda_check(cudaMemcpy(dev, pinned, bytes, cudaMemcpyHostToDevice), "allreduce staging");
         } else {
-            rc = fn(ctx, dev, n, 0);
+            rc = call(dev, n, dtype, 0);
         }
         if (rc != 0) throw Error(SB2_ERR_RUNTIME, "allreduce callback failed");
     }
@@ -2048,7 +2064,8 @@ struct SpaceCharge {
             return;
         }
         const bool exchange = hook && *hook;
-        last_rho32 = mixed && !exchange;
+        // an FP32 charge grid is exchanged as float through a typed callback
+        last_rho32 = mixed && (!exchange || hook->typed());
         if (g_rec) {
             record_solve(b);
             return;
@@ -2068,7 +2085,12 @@ struct SpaceCharge {
                            "deposit");
             }
         }
-        if (exchange) hook->run(rho, G, s); // charge of all ranks
+        if (exchange) { // charge of all ranks
+            if (last_rho32)
+                hook->run(rho32, G, s);
+            else
+                hook->run(rho, G, s);
+        }
         if (!o.domain_fixed || !ghat_valid) {
             ProfScope ps(PROF_GREEN, s);
             cuda_check(launch_green(state, ghat, d, o.green_fn == SB2_GREEN_LINEAR, tw_x, tw_y, tw_z, s), "green");
@@ -4288,6 +4310,21 @@ sb2_status sb2_propagator_set_allreduce(sb2_propagator* p, sb2_allreduce_fn fn, 
     if (fn && (p->p->use_graphs || p->p->diag_cap))
         throw Error(SB2_ERR_UNSUPPORTED, "a sharded propagator runs without CUDA-graph turns and per-turn diagnostics");
     p->p->hook.fn = fn;
+    p->p->hook.tfn = nullptr;
+    p->p->hook.ctx = ctx;
+    p->p->hook.on_host = on_host != 0;
+    SB2_CATCH
+}
+
+sb2_status sb2_propagator_set_allreduce_typed(sb2_propagator* p, sb2_allreduce_typed_fn fn, void* ctx,
+                                              int32_t on_host)
+{
+    SB2_TRY
+    SB2_REQUIRE(p, "null propagator");
+    if (fn && (p->p->use_graphs || p->p->diag_cap))
+        throw Error(SB2_ERR_UNSUPPORTED, "a sharded propagator runs without CUDA-graph turns and per-turn diagnostics");
+    p->p->hook.fn = nullptr;
+    p->p->hook.tfn = fn;
     p->p->hook.ctx = ctx;
     p->p->hook.on_host = on_host != 0;
     SB2_CATCH

@@ -20,7 +20,8 @@ def shard_range(n, rank, world):
 def attach(propagator, group=None, on_host=None):
     """Give `propagator` a torch.distributed sum-allreduce over `group`.
     on_host (default: True for the gloo backend, False for NCCL) selects host
-    staging or device buffers."""
+    staging or device buffers.  The callback is typed, so a mixed-precision
+    propagator sums its FP32 charge grid as float32."""
     import torch
     import torch.distributed as dist
     if on_host is None:
@@ -33,20 +34,20 @@ def attach(propagator, group=None, on_host=None):
             dist.all_reduce(torch.from_numpy(arr), op=dist.ReduceOp.SUM, group=group)
     else:
         class _Dev:  # a device buffer seen through __cuda_array_interface__
-            def __init__(self, ptr, n):
-                self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False),
+            def __init__(self, ptr, n, dtype):
+                self.__cuda_array_interface__ = {"shape": (n,), "typestr": dtype.str, "data": (ptr, False),
                                                  "version": 3, "strides": None}
 
         from . import _lib
 
-        def fn(ptr, n):
+        def fn(ptr, n, dtype):
             # the collective is ordered on the library's stream: NCCL waits
             # for the deposit queued there, and the library's next kernels
             # wait for NCCL; the host does not wait
             ptr_s = _lib.lib().sb2_allreduce_stream()
             st = torch.cuda.ExternalStream(ptr_s) if ptr_s else torch.cuda.default_stream()
             with torch.cuda.stream(st):
-                t = torch.as_tensor(_Dev(ptr, n), device="cuda")
+                t = torch.as_tensor(_Dev(ptr, n, dtype), device="cuda")
                 dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
-    propagator.set_allreduce(fn, on_host=on_host)
+    propagator.set_allreduce(fn, on_host=on_host, typed=True)
     return propagator
