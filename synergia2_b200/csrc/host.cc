@@ -511,7 +511,10 @@ struct Bunch {
     {
         if (permuted) return;
         if (!wc.parts) {
-            const int64_t cap = std::max<int64_t>(n, 1);
+            // a multiple of 32 particles: every column starts 256-byte
+            // aligned, and the sort's 16-byte staging copies of the last
+            // tile stay inside the arrays
+            const int64_t cap = (std::max<int64_t>(n, 1) + 31) / 32 * 32;
             wc.n = n;
             wc.stride = cap;
             wc.parts = dalloc<double>((size_t)7 * cap, "working copy");

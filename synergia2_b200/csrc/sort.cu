@@ -163,23 +163,51 @@ __device__ __forceinline__ int table_insert_n(int* t_key, int* t_cnt, int key, i
     return -1; // unreachable: the table has more slots than a tile has keys
 }
 
-__global__ void __launch_bounds__(kTileThreads) sort_scatter_tiled_kernel(
+// The tile's arrays come into shared memory by asynchronous 16-byte copies
+// (cp.async), each while the previous one is stored (two buffers); the
+// first array's copy is in flight during the grouping.  After its
+// reservation a table slot's key is replaced by the run's first
+// destination.  The copies of the last tile are rounded up to 16 bytes: the
+// working copy's arrays hold a multiple of 32 particles.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(kTileThreads) sort_scatter_piped_kernel(
     const double* __restrict__ src, const uint8_t* __restrict__ m_src, const uint8_t* __restrict__ d_src,
     const int32_t* __restrict__ p_src, double* dst, uint8_t* m_dst, uint8_t* d_dst, int32_t* p_dst, int64_t n,
     int64_t stride, const ScState* __restrict__ scp, int gx, int gy, int gz, const int32_t* __restrict__ offsets,
     int32_t* cursor)
 {
-    __shared__ int t_key[kTable];
+    __shared__ int t_key[kTable]; // key; after the reservation, the run's first destination
     __shared__ int t_cnt[kTable];
-    __shared__ int t_off[kTable];   // local exclusive offsets
-    __shared__ int t_gpos[kTable];  // first global destination of the key's run
-    __shared__ short s_src[kTile];  // tile index of the particle in local slot j
-    __shared__ int s_dst[kTile];    // its global destination
-    __shared__ double s_buf[kTile]; // one array of the tile
+    __shared__ int t_off[kTable]; // local exclusive offsets
+    __shared__ short s_src[kTile];
+    __shared__ int s_dst[kTile];
+    __shared__ __align__(16) double s_buf[2][kTile];
     __shared__ int s_wsum[kTileThreads / 32];
     const ScState& sc = *scp;
     const int G = gx * gy * gz;
     constexpr int PPT = kTile / kTileThreads;
+    // copies of array a of the tile at `base` (tn particles; the lengths
+    // rounded up to 16 bytes: the arrays hold a multiple of 32 particles)
+    auto issue = [&](int a, int64_t base, int tn) {
+        unsigned char* b = (unsigned char*)s_buf[a & 1];
+        if (a < 7) {
+            const double* c = src + a * stride + base;
+            for (int k = threadIdx.x; k < (tn + 1) / 2; k += kTileThreads) cp_async16(b + 16 * k, c + 2 * k);
+        } else if (a < 9) {
+            const uint8_t* c = (a == 7 ? m_src : d_src) + base;
+            for (int k = threadIdx.x; k < (tn + 15) / 16; k += kTileThreads) cp_async16(b + 16 * k, c + 16 * k);
+        } else {
+            const int32_t* c = p_src + base;
+            for (int k = threadIdx.x; k < (tn + 3) / 4; k += kTileThreads) cp_async16(b + 16 * k, c + 4 * k);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
     for (int e = threadIdx.x; e < kTable; e += kTileThreads) {
         t_key[e] = kEmpty;
         t_cnt[e] = 0;
@@ -187,6 +215,7 @@ __global__ void __launch_bounds__(kTileThreads) sort_scatter_tiled_kernel(
     __syncthreads();
     for (int64_t base = (int64_t)blockIdx.x * kTile; base < n; base += (int64_t)gridDim.x * kTile) {
         const int tn = (int)min((int64_t)kTile, n - base);
+        issue(0, base, tn);
         int ent[PPT], rnk[PPT];
 #pragma unroll
         for (int q = 0; q < PPT; ++q) {
@@ -198,8 +227,6 @@ __global__ void __launch_bounds__(kTileThreads) sort_scatter_tiled_kernel(
                 key = (!m_src[i] || !sc.valid) ? G + 1
                                                : cell_key(src[i], src[i + 2 * stride], src[i + 4 * stride], sc, gx, gy, gz);
             }
-            // lanes with the same key insert once: the lowest one reserves
-            // the group's ranks, the others take theirs by lane order
             const unsigned peers = __match_any_sync(0xffffffffu, key);
             const int lead = __ffs(peers) - 1;
             unsigned below;
@@ -214,8 +241,6 @@ __global__ void __launch_bounds__(kTileThreads) sort_scatter_tiled_kernel(
             }
         }
         __syncthreads();
-        // local exclusive scan of the counts (table order) and one global
-        // reservation per distinct key
         constexpr int EPT = kTable / kTileThreads;
         int c[EPT], tot = 0;
 #pragma unroll
@@ -230,6 +255,13 @@ __global__ void __launch_bounds__(kTileThreads) sort_scatter_tiled_kernel(
             if (lane >= o) inc += u;
         }
         if (lane == 31) s_wsum[w] = inc;
+        // one global reservation per distinct key, a thread's atomics all in flight
+        int g[EPT];
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            const int e = threadIdx.x * EPT + k;
+            g[k] = c[k] ? offsets[t_key[e]] + atomicAdd(&cursor[t_key[e]], c[k]) : 0;
+        }
         __syncthreads();
         int run = inc - tot;
         for (int k = 0; k < w; ++k) run += s_wsum[k];
@@ -237,7 +269,7 @@ __global__ void __launch_bounds__(kTileThreads) sort_scatter_tiled_kernel(
         for (int k = 0; k < EPT; ++k) {
             const int e = threadIdx.x * EPT + k;
             t_off[e] = run;
-            if (c[k]) t_gpos[e] = offsets[t_key[e]] + atomicAdd(&cursor[t_key[e]], c[k]);
+            if (c[k]) t_key[e] = g[k];
             run += c[k];
         }
         __syncthreads();
@@ -246,37 +278,32 @@ __global__ void __launch_bounds__(kTileThreads) sort_scatter_tiled_kernel(
             if (ent[q] < 0) continue;
             const int slot = t_off[ent[q]] + rnk[q];
             s_src[slot] = (short)(q * kTileThreads + threadIdx.x);
-            s_dst[slot] = t_gpos[ent[q]] + rnk[q];
+            s_dst[slot] = t_key[ent[q]] + rnk[q];
         }
-        __syncthreads();
-        // move the tile array by array: coalesced loads into shared memory,
-        // stores in slot order (runs of consecutive destinations)
+        // array by array, the next one's copies in flight during the stores
         for (int a = 0; a < 10; ++a) {
-            if (a < 7) {
-                for (int l = threadIdx.x; l < tn; l += kTileThreads) s_buf[l] = src[base + l + a * stride];
-            } else if (a == 7) {
-                for (int l = threadIdx.x; l < tn; l += kTileThreads) s_buf[l] = (double)m_src[base + l];
-            } else if (a == 8) {
-                for (int l = threadIdx.x; l < tn; l += kTileThreads) s_buf[l] = (double)d_src[base + l];
+            if (a + 1 < 10) {
+                issue(a + 1, base, tn);
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
             } else {
-                for (int l = threadIdx.x; l < tn; l += kTileThreads) s_buf[l] = (double)p_src[base + l];
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
             }
             __syncthreads();
+            const unsigned char* b = (const unsigned char*)s_buf[a & 1];
             for (int j = threadIdx.x; j < tn; j += kTileThreads) {
-                const double v = s_buf[s_src[j]];
+                const int l = s_src[j];
                 const int64_t d = s_dst[j];
                 if (a < 7)
-                    dst[d + a * stride] = v;
+                    dst[d + a * stride] = ((const double*)b)[l];
                 else if (a == 7)
-                    m_dst[d] = (uint8_t)v;
+                    m_dst[d] = b[l];
                 else if (a == 8)
-                    d_dst[d] = (uint8_t)v;
+                    d_dst[d] = b[l];
                 else
-                    p_dst[d] = (int32_t)v;
+                    p_dst[d] = ((const int32_t*)b)[l];
             }
             __syncthreads();
         }
-        // clear the table for the next tile
         for (int e = threadIdx.x; e < kTable; e += kTileThreads) {
             t_key[e] = kEmpty;
             t_cnt[e] = 0;
@@ -355,8 +382,9 @@ cudaError_t launch_cell_sort(const SortBuffers& sb, int32_t* scratch, const ScSt
     scan_block_kernel<<<nb, 256, 0, s>>>(counts, offsets, m, bsums);
     scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nb);
     scan_add_kernel<<<(m + 255) / 256, 256, 0, s>>>(offsets, m, bsums);
-    sort_scatter_tiled_kernel<<<grid, kTileThreads, 0, s>>>(sb.parts, sb.masks, sb.discards, sb.perm, sb.parts2, sb.masks2,
-                                             sb.discards2, sb.perm2, sb.n, sb.stride, sc, gx, gy, gz, offsets, cursor);
+    sort_scatter_piped_kernel<<<grid, kTileThreads, 0, s>>>(sb.parts, sb.masks, sb.discards, sb.perm, sb.parts2,
+                                                            sb.masks2, sb.discards2, sb.perm2, sb.n, sb.stride, sc, gx,
+                                                            gy, gz, offsets, cursor);
     return cudaGetLastError();
 }
 
