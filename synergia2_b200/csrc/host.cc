@@ -471,6 +471,7 @@ struct Bunch {
     Refpart design;
     bool design_set = false;
     int turns_done = 0;
+    int next_step = 0; // step of the stepper the bunch is at (0 after whole turns)
 
     // Home arrays: the ones the caller handed over or reads back, in the
     // caller's particle order.
@@ -2815,10 +2816,14 @@ struct Propagator {
                 t.turns_done = b.turns_done;
                 // an untimed lead-in of the same length brings the scratch
                 // copy to the state the timed steps see in a long run (its
-                // cell order aged as the re-sort interval lets it)
-                propagate_steps(t, 0, steps, 0);
+                // cell order aged as the re-sort interval lets it).  Both
+                // continue from the bunch's own step: started elsewhere in
+                // the lattice the beam is mismatched to the optics, its size
+                // and density change, and so do the costs being compared.
+                const int first = b.next_step;
+                propagate_steps(t, first, steps, 0);
                 cuda_check(cudaEventRecord(e0, 0), "event");
-                propagate_steps(t, steps, steps, 0);
+                propagate_steps(t, first + steps, steps, 0);
                 cuda_check(cudaEventRecord(e1, 0), "event");
                 cuda_check(cudaEventSynchronize(e1), "event");
                 float ms = 0.f;
@@ -3050,6 +3055,7 @@ struct Propagator {
             else
                 run_turn(b, s);
         }
+        if (turns > 0) b.next_step = 0;
         engine_->flush(b, sc.get(), elem_charge, false, 0.0, s);
         leave_sorted(b, s);
     }
@@ -3076,6 +3082,7 @@ struct Propagator {
                 record_diagnostics(b, s);
             }
         }
+        if (count > 0 && ns > 0) b.next_step = (((first + count) % ns) + ns) % ns;
         engine_->flush(b, sc.get(), elem_charge, false, 0.0, s);
         leave_sorted(b, s);
         finish(b, s);
@@ -3520,7 +3527,10 @@ struct Batch {
                 record([&](Job& j, cudaStream_t s) {
                     if (si == 0) j.b->ref.start_repetition();
                     j.p->run_step(*j.b, j.p->steps[si], s);
-                    if (si == ns - 1) j.b->turns_done += 1;
+                    if (si == ns - 1) {
+                        j.b->turns_done += 1;
+                        j.b->next_step = 0;
+                    }
                 });
         record([&](Job& j, cudaStream_t s) {
             j.p->engine_->flush(*j.b, j.p->sc.get(), j.p->elem_charge, false, 0.0, s);
