@@ -388,7 +388,8 @@ sb2_status sb2_batch_launch(sb2_batch* q, int32_t slot, int32_t turns);
  * of steps per turn and the same launch sequence per step (one lattice with
  * different strengths; bunch sizes and grids may differ), otherwise
  * SB2_ERR_UNSUPPORTED; per-turn diagnostics, step-count records and
- * sharded propagators are not available.  Returns when the turns are done. */
+ * sharded propagators are not available, and every job needs its own
+ * propagator and bunch.  Returns when the turns are done. */
 sb2_status sb2_batch_run_lockstep(sb2_batch* q, const int32_t* slots, int32_t n, int32_t turns);
 sb2_status sb2_batch_query(sb2_batch* q, int32_t slot, int32_t* done);
 

@@ -1802,7 +1802,7 @@ struct LaunchRec {
     int linear = 0, mode = 0;
     const double2* tw64[3] = {nullptr, nullptr, nullptr};
     const float2* tw32[3] = {nullptr, nullptr, nullptr};
-    std::function<void(cudaStream_t)> run; // SORT: the bunch's own launches
+    SortItem sort{}; // SORT
 };
 static thread_local std::vector<LaunchRec>* g_rec = nullptr;
 
@@ -2572,14 +2572,12 @@ struct Propagator {
         if (g_rec) {
             LaunchRec r;
             r.kind = LaunchRec::SORT;
-            const SortBuffers wc = b.wc;
-            int32_t* scr = sort_scratch;
-            const ScState* st = sc->state;
-            const int gx = sc->d.gx, gy = sc->d.gy, gz = sc->d.gz;
-            r.run = [wc, scr, st, gx, gy, gz](cudaStream_t ss) {
-                ProfScope ps(PROF_SORT, ss);
-                cuda_check(launch_cell_sort(wc, scr, st, gx, gy, gz, ss), "cell sort");
-            };
+            r.sort.sb = b.wc;
+            r.sort.sc = sc->state;
+            r.sort.scratch = sort_scratch;
+            r.sort.gx = sc->d.gx;
+            r.sort.gy = sc->d.gy;
+            r.sort.gz = sc->d.gz;
             g_rec->push_back(std::move(r));
         } else if (!g_sig.dry) {
             ProfScope ps(PROF_SORT, s);
@@ -3264,20 +3262,27 @@ struct Batch {
             int linear, mode;
             const double2* tw64[3];
             const float2* tw32[3];
-            size_t sort_job;
+            int sort_blocks[4], sort_max_m;
         };
         std::vector<Op> ops;
         std::vector<int> mom_blocks(nj, 0);
         for (size_t k = 0; k < npos; ++k) {
             const int kind = recs[0][k].kind;
-            if (kind == LaunchRec::SORT) {
+            if (kind == LaunchRec::SORT) { // every bunch's counting sort in one set of list launches
+                std::vector<SortItem> items(nj);
+                std::vector<int> first(4 * (nj + 1));
+                Op o{};
+                o.kind = kind;
+                o.nitems = (int)nj;
                 for (size_t j = 0; j < nj; ++j) {
-                    Op o{};
-                    o.kind = kind;
-                    o.sort_job = j;
-                    o.variant = (int)k;
-                    ops.push_back(o);
+                    items[j] = recs[j][k].sort;
+                    const SortItem& it = items[j];
+                    o.sort_max_m = std::max(o.sort_max_m, it.gx * it.gy * it.gz + 2);
                 }
+                sort_list_plan(items.data(), (int)nj, first.data(), o.sort_blocks);
+                o.items = m.add(items.data(), sizeof(SortItem) * nj);
+                o.first = m.add(first.data(), sizeof(int) * first.size());
+                ops.push_back(o);
                 continue;
             }
             if (kind == LaunchRec::DOMAIN) {
@@ -3448,9 +3453,13 @@ struct Batch {
                            "efield list");
                 break;
             }
-            case LaunchRec::SORT:
-                recs[o.sort_job][o.variant].run(s);
+            case LaunchRec::SORT: {
+                ProfScope ps(PROF_SORT, s);
+                cuda_check(launch_cell_sort_list((const SortItem*)items, first, o.nitems, o.sort_blocks, o.sort_max_m,
+                                                 s),
+                           "cell sort list");
                 break;
+            }
             }
         }
     }
@@ -3462,8 +3471,13 @@ struct Batch {
         for (int k = 0; k < n; ++k) {
             Job& j = job(slots[k]);
             if (j.pending) throw Error(SB2_ERR_INVALID, "batch slot already has turns in flight");
-            for (Job* o : js)
+            for (Job* o : js) {
                 if (o == &j) throw Error(SB2_ERR_INVALID, "run_lockstep: a slot is listed twice");
+                // the list launches run all jobs at once: one job's grids,
+                // scratch and working copy must not be another's
+                if (o->p == j.p || o->b == j.b)
+                    throw Error(SB2_ERR_UNSUPPORTED, "run_lockstep: jobs must have their own propagator and bunch");
+            }
             Propagator& P = *j.p;
             if (P.hook) throw Error(SB2_ERR_UNSUPPORTED, "run_lockstep: sharded propagators are not supported");
             if (P.diag_cap || P.step_rec_cap)

@@ -80,6 +80,15 @@ struct SortBuffers {
     int64_t n, stride;
 };
 
+// One bunch of a counting sort over many bunches (sort.cu, batch in
+// lockstep): its working copy, domain, grid and scratch (sort_scratch_ints).
+struct SortItem {
+    SortBuffers sb;
+    const ScState* sc;
+    int32_t* scratch;
+    int gx, gy, gz;
+};
+
 // Launch shape of the particle passes: the autotuner's search space
 // (host.cc, Propagator::autotune).
 struct TrackTune {
@@ -194,6 +203,9 @@ cudaError_t launch_convolve_mixed(const MixedConv& m, float2* S, const double* G
 cudaError_t launch_efield_f32(const float* phi, float4* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s);
 // sort.cu
 size_t sort_scratch_ints(int64_t G);
+void sort_list_plan(const SortItem* items, int nitems, int* first, int* nblocks);
+cudaError_t launch_cell_sort_list(const SortItem* items, const int* first, int nitems, const int* nblocks,
+                                  int max_m, cudaStream_t s);
 cudaError_t launch_cell_sort(const SortBuffers& sb, int32_t* scratch, const ScState* sc, int gx, int gy, int gz,
                              cudaStream_t s);
 cudaError_t launch_sort_gather_in(const double* ups, int64_t ustride, const uint8_t* um, const uint8_t* ud,

@@ -19,6 +19,7 @@
 // of it.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "sb2_kernels.h"
@@ -36,16 +37,17 @@ __device__ __forceinline__ int cell_key(double x, double y, double z, const ScSt
     return (iz * gy + iy) * gx + ix;
 }
 
-__global__ void __launch_bounds__(256) sort_hist_kernel(const double* __restrict__ parts, int64_t stride,
-                                                        const uint8_t* __restrict__ masks, int64_t n,
-                                                        const ScState* __restrict__ scp, int gx, int gy, int gz,
-                                                        int32_t* counts)
+// block vb of vg blocks of one bunch's histogram
+__device__ __forceinline__ void sort_hist_body(const double* __restrict__ parts, int64_t stride,
+                                               const uint8_t* __restrict__ masks, int64_t n,
+                                               const ScState* __restrict__ scp, int gx, int gy, int gz,
+                                               int32_t* counts, int vb, int vg)
 {
     const ScState& sc = *scp;
     const int G = gx * gy * gz;
     const int lane = threadIdx.x & 31;
-    const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t wb = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane; wb < n; wb += wstride) {
+    const int64_t wstride = (int64_t)vg * blockDim.x;
+    for (int64_t wb = (vb * (int64_t)blockDim.x + threadIdx.x) - lane; wb < n; wb += wstride) {
         const int64_t i = wb + lane;
         int key = -1;
         if (i < n) {
@@ -59,15 +61,23 @@ __global__ void __launch_bounds__(256) sort_hist_kernel(const double* __restrict
     }
 }
 
+__global__ void __launch_bounds__(256) sort_hist_kernel(const double* __restrict__ parts, int64_t stride,
+                                                        const uint8_t* __restrict__ masks, int64_t n,
+                                                        const ScState* __restrict__ scp, int gx, int gy, int gz,
+                                                        int32_t* counts)
+{
+    sort_hist_body(parts, stride, masks, n, scp, gx, gy, gz, counts, blockIdx.x, gridDim.x);
+}
+
 // exclusive scan: per-block (1024 values), then block sums, then add
 constexpr int kScanBlock = 1024;
 
-__global__ void __launch_bounds__(256) scan_block_kernel(const int32_t* __restrict__ in, int32_t* out, int n,
-                                                         int32_t* block_sums)
+__device__ __forceinline__ void scan_block_body(const int32_t* __restrict__ in, int32_t* out, int n,
+                                                int32_t* block_sums, int blk)
 {
     __shared__ int32_t s[kScanBlock];
     __shared__ int32_t warp_tot[8];
-    const int base = blockIdx.x * kScanBlock;
+    const int base = blk * kScanBlock;
     for (int k = threadIdx.x; k < kScanBlock; k += blockDim.x) s[k] = (base + k < n) ? in[base + k] : 0;
     __syncthreads();
     // each thread owns 4 consecutive values
@@ -95,11 +105,17 @@ __global__ void __launch_bounds__(256) scan_block_kernel(const int32_t* __restri
     if (threadIdx.x == blockDim.x - 1) {
         int32_t all = 0;
         for (int k = 0; k < 8; ++k) all += warp_tot[k];
-        block_sums[blockIdx.x] = all;
+        block_sums[blk] = all;
     }
 }
 
-__global__ void __launch_bounds__(1024) scan_sums_kernel(int32_t* sums, int nb)
+__global__ void __launch_bounds__(256) scan_block_kernel(const int32_t* __restrict__ in, int32_t* out, int n,
+                                                         int32_t* block_sums)
+{
+    scan_block_body(in, out, n, block_sums, blockIdx.x);
+}
+
+__device__ __forceinline__ void scan_sums_body(int32_t* sums, int nb)
 {
     // single block: sequential per-thread chunks, then a block scan of the
     // chunk totals
@@ -123,6 +139,8 @@ __global__ void __launch_bounds__(1024) scan_sums_kernel(int32_t* sums, int nb)
         run += v;
     }
 }
+
+__global__ void __launch_bounds__(1024) scan_sums_kernel(int32_t* sums, int nb) { scan_sums_body(sums, nb); }
 
 __global__ void scan_add_kernel(int32_t* out, int n, const int32_t* __restrict__ sums)
 {
@@ -176,11 +194,12 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src)
                  : "memory");
 }
 
-__global__ void __launch_bounds__(kTileThreads) sort_scatter_piped_kernel(
+// block vb of vg blocks of one bunch's scatter
+__device__ __forceinline__ void sort_scatter_piped_body(
     const double* __restrict__ src, const uint8_t* __restrict__ m_src, const uint8_t* __restrict__ d_src,
     const int32_t* __restrict__ p_src, double* dst, uint8_t* m_dst, uint8_t* d_dst, int32_t* p_dst, int64_t n,
     int64_t stride, const ScState* __restrict__ scp, int gx, int gy, int gz, const int32_t* __restrict__ offsets,
-    int32_t* cursor)
+    int32_t* cursor, int vb, int vg)
 {
     __shared__ int t_key[kTable]; // key; after the reservation, the run's first destination
     __shared__ int t_cnt[kTable];
@@ -213,7 +232,7 @@ __global__ void __launch_bounds__(kTileThreads) sort_scatter_piped_kernel(
         t_cnt[e] = 0;
     }
     __syncthreads();
-    for (int64_t base = (int64_t)blockIdx.x * kTile; base < n; base += (int64_t)gridDim.x * kTile) {
+    for (int64_t base = (int64_t)vb * kTile; base < n; base += (int64_t)vg * kTile) {
         const int tn = (int)min((int64_t)kTile, n - base);
         issue(0, base, tn);
         int ent[PPT], rnk[PPT];
@@ -310,6 +329,137 @@ __global__ void __launch_bounds__(kTileThreads) sort_scatter_piped_kernel(
         }
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(kTileThreads) sort_scatter_piped_kernel(
+    const double* __restrict__ src, const uint8_t* __restrict__ m_src, const uint8_t* __restrict__ d_src,
+    const int32_t* __restrict__ p_src, double* dst, uint8_t* m_dst, uint8_t* d_dst, int32_t* p_dst, int64_t n,
+    int64_t stride, const ScState* __restrict__ scp, int gx, int gy, int gz, const int32_t* __restrict__ offsets,
+    int32_t* cursor)
+{
+    sort_scatter_piped_body(src, m_src, d_src, p_src, dst, m_dst, d_dst, p_dst, n, stride, scp, gx, gy, gz, offsets,
+                            cursor, blockIdx.x, gridDim.x);
+}
+
+// ---------------------------------------------------------------------------
+// The counting sort of many bunches at once (a batch in lockstep): every
+// kernel of the sort takes a list of SortItem, and the blocks of one launch
+// are split among the items in proportion to their work (item i owns blocks
+// [first[i], first[i+1]) of each kernel).
+// ---------------------------------------------------------------------------
+struct SortView {
+    int G, m, nb;
+    int32_t *counts, *offsets, *cursor, *bsums;
+};
+__host__ __device__ __forceinline__ SortView sort_view(const SortItem& it)
+{
+    SortView v;
+    v.G = it.gx * it.gy * it.gz;
+    v.m = v.G + 2;
+    v.nb = (v.m + kScanBlock - 1) / kScanBlock;
+    v.counts = it.scratch;
+    v.offsets = v.counts + v.m;
+    v.cursor = v.offsets + v.m;
+    v.bsums = v.cursor + v.m;
+    return v;
+}
+
+__device__ __forceinline__ int sort_item_of(const int* __restrict__ first, int nitems)
+{
+    int lo = 0, hi = nitems;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (first[mid] <= (int)blockIdx.x)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// grid (x, nitems): item blockIdx.y clears its counts and cursors
+__global__ void sort_zero_list_kernel(const SortItem* __restrict__ items)
+{
+    const SortView v = sort_view(items[blockIdx.y]);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.m; i += gridDim.x * blockDim.x) {
+        v.counts[i] = 0;
+        v.cursor[i] = 0;
+    }
+}
+
+__global__ void __launch_bounds__(256) sort_hist_list_kernel(const SortItem* __restrict__ items,
+                                                             const int* __restrict__ first, int nitems)
+{
+    const int k = sort_item_of(first, nitems);
+    const SortItem& it = items[k];
+    sort_hist_body(it.sb.parts, it.sb.stride, it.sb.masks, it.sb.n, it.sc, it.gx, it.gy, it.gz, sort_view(it).counts,
+                   (int)blockIdx.x - first[k], first[k + 1] - first[k]);
+}
+
+__global__ void __launch_bounds__(256) scan_block_list_kernel(const SortItem* __restrict__ items,
+                                                              const int* __restrict__ first, int nitems)
+{
+    const int k = sort_item_of(first, nitems);
+    const SortView v = sort_view(items[k]);
+    scan_block_body(v.counts, v.offsets, v.m, v.bsums, (int)blockIdx.x - first[k]);
+}
+
+// one block per item
+__global__ void __launch_bounds__(1024) scan_sums_list_kernel(const SortItem* __restrict__ items)
+{
+    const SortView v = sort_view(items[blockIdx.x]);
+    scan_sums_body(v.bsums, v.nb);
+}
+
+__global__ void scan_add_list_kernel(const SortItem* __restrict__ items, const int* __restrict__ first, int nitems)
+{
+    const int k = sort_item_of(first, nitems);
+    const SortView v = sort_view(items[k]);
+    const int i = ((int)blockIdx.x - first[k]) * blockDim.x + threadIdx.x;
+    if (i < v.m) v.offsets[i] += v.bsums[i / kScanBlock];
+}
+
+__global__ void __launch_bounds__(kTileThreads, 4) sort_scatter_list_kernel(const SortItem* __restrict__ items,
+                                                                        const int* __restrict__ first, int nitems)
+{
+    const int k = sort_item_of(first, nitems);
+    const SortItem& it = items[k];
+    const SortView v = sort_view(it);
+    const SortBuffers& sb = it.sb;
+    sort_scatter_piped_body(sb.parts, sb.masks, sb.discards, sb.perm, sb.parts2, sb.masks2, sb.discards2, sb.perm2,
+                            sb.n, sb.stride, it.sc, it.gx, it.gy, it.gz, v.offsets, v.cursor,
+                            (int)blockIdx.x - first[k], first[k + 1] - first[k]);
+}
+
+// the block partitions of the list launches: first holds 4 arrays of
+// nitems + 1 entries (histogram, block scan, scan add, scatter)
+void sort_list_plan(const SortItem* items, int nitems, int* first, int* nblocks)
+{
+    const int stride = nitems + 1;
+    for (int a = 0; a < 4; ++a) first[a * stride] = 0;
+    for (int i = 0; i < nitems; ++i) {
+        const SortView v = sort_view(items[i]);
+        const int64_t n = items[i].sb.n;
+        const int64_t tiles = (n + kTile - 1) / kTile;
+        const int b[4] = {(int)std::max<int64_t>(1, (n + 4095) / 4096), v.nb, (v.m + 255) / 256,
+                          (int)std::max<int64_t>(1, (tiles + 1) / 2)};
+        for (int a = 0; a < 4; ++a) first[a * stride + i + 1] = first[a * stride + i] + b[a];
+    }
+    for (int a = 0; a < 4; ++a) nblocks[a] = first[a * stride + nitems];
+}
+
+cudaError_t launch_cell_sort_list(const SortItem* items, const int* first, int nitems, const int* nblocks,
+                                  int max_m, cudaStream_t s)
+{
+    const int stride = nitems + 1;
+    const int zb = std::max(1, std::min(64, (max_m + 255) / 256));
+    sort_zero_list_kernel<<<dim3(zb, nitems), 256, 0, s>>>(items);
+    sort_hist_list_kernel<<<nblocks[0], 256, 0, s>>>(items, first, nitems);
+    scan_block_list_kernel<<<nblocks[1], 256, 0, s>>>(items, first + stride, nitems);
+    scan_sums_list_kernel<<<nitems, 1024, 0, s>>>(items);
+    scan_add_list_kernel<<<nblocks[2], 256, 0, s>>>(items, first + 2 * stride, nitems);
+    sort_scatter_list_kernel<<<nblocks[3], kTileThreads, 0, s>>>(items, first + 3 * stride, nitems);
+    return cudaGetLastError();
 }
 
 // working copy <- caller arrays (identity order)

@@ -228,3 +228,16 @@ def test_lockstep_rejects_jobs_out_of_step(syn):
     s1, s2 = batch.add(*a), batch.add(p2, b2)
     with pytest.raises(syn.SB2Error, match="lockstep"):
         batch.run_lockstep([s1, s2], 1)
+
+
+def test_lockstep_rejects_shared_propagator_or_bunch(syn):
+    """The list launches advance all jobs at once, so two jobs of one
+    lockstep call cannot share a propagator (its grids and sort scratch) or
+    a bunch."""
+    p1, b1 = _job(syn, 0.6, 10000, (16, 16, 32), 1, syn.precision_t.fp64, False)
+    p2, b2 = _job(syn, 0.7, 10000, (16, 16, 32), 2, syn.precision_t.fp64, False)
+    for pair in (((p1, b1), (p1, b2)), ((p1, b1), (p2, b1))):
+        batch = syn.Batch()
+        s1, s2 = batch.add(*pair[0]), batch.add(*pair[1])
+        with pytest.raises(syn.SB2Error, match="own propagator and bunch"):
+            batch.run_lockstep([s1, s2], 1)
