@@ -2486,7 +2486,7 @@ struct Propagator {
         int deposit_chunk = deposit_default_chunk();
         bool operator==(const SolveTune& o) const { return fft_plan == o.fft_plan && deposit_chunk == o.deposit_chunk; }
     } solve_tune;
-    int32_t* sort_scratch = nullptr; // histogram, offsets, cursors and block sums of the counting sort
+    int32_t* sort_scratch = nullptr; // histogram, offsets (the scatter's cursors) and block sums of the counting sort
 
     Propagator(const Lattice& l, int stepper_kind, int n, const sb2_sc3d_options* opts)
         : lat(l), stepper(stepper_kind), num(n)

@@ -37,7 +37,8 @@ __device__ __forceinline__ int cell_key(double x, double y, double z, const ScSt
     return (iz * gy + iy) * gx + ix;
 }
 
-// block vb of vg blocks of one bunch's histogram
+// block vb of vg blocks of one bunch's histogram; a warp takes 64
+// consecutive particles per iteration, both loads of a lane in flight
 __device__ __forceinline__ void sort_hist_body(const double* __restrict__ parts, int64_t stride,
                                                const uint8_t* __restrict__ masks, int64_t n,
                                                const ScState* __restrict__ scp, int gx, int gy, int gz,
@@ -46,22 +47,32 @@ __device__ __forceinline__ void sort_hist_body(const double* __restrict__ parts,
     const ScState& sc = *scp;
     const int G = gx * gy * gz;
     const int lane = threadIdx.x & 31;
-    const int64_t wstride = (int64_t)vg * blockDim.x;
-    for (int64_t wb = (vb * (int64_t)blockDim.x + threadIdx.x) - lane; wb < n; wb += wstride) {
-        const int64_t i = wb + lane;
-        int key = -1;
-        if (i < n) {
-            if (!masks[i] || !sc.valid)
-                key = G + 1;
-            else
-                key = cell_key(parts[i], parts[i + 2 * stride], parts[i + 4 * stride], sc, gx, gy, gz);
+    const int64_t wstride = (int64_t)vg * blockDim.x * 2;
+    for (int64_t wb = (vb * (int64_t)blockDim.x + threadIdx.x - lane) * 2; wb < n; wb += wstride) {
+        double x[2], y[2], z[2];
+        int m[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int64_t i = wb + u * 32 + lane;
+            m[u] = -1;
+            if (i < n) {
+                m[u] = masks[i];
+                x[u] = parts[i];
+                y[u] = parts[i + 2 * stride];
+                z[u] = parts[i + 4 * stride];
+            }
         }
-        const unsigned grp = __match_any_sync(0xffffffffu, key);
-        if (key >= 0 && lane == __ffs(grp) - 1) atomicAdd(&counts[key], __popc(grp));
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            int key = -1;
+            if (m[u] >= 0) key = (!m[u] || !sc.valid) ? G + 1 : cell_key(x[u], y[u], z[u], sc, gx, gy, gz);
+            const unsigned grp = __match_any_sync(0xffffffffu, key);
+            if (key >= 0 && lane == __ffs(grp) - 1) atomicAdd(&counts[key], __popc(grp));
+        }
     }
 }
 
-__global__ void __launch_bounds__(256) sort_hist_kernel(const double* __restrict__ parts, int64_t stride,
+__global__ void __launch_bounds__(256, 6) sort_hist_kernel(const double* __restrict__ parts, int64_t stride,
                                                         const uint8_t* __restrict__ masks, int64_t n,
                                                         const ScState* __restrict__ scp, int gx, int gy, int gz,
                                                         int32_t* counts)
@@ -194,12 +205,13 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src)
                  : "memory");
 }
 
-// block vb of vg blocks of one bunch's scatter
+// block vb of vg blocks of one bunch's scatter.  cursor holds the exclusive
+// scan of the key counts; each distinct key of a tile reserves its run of
+// destinations by advancing cursor[key] atomically.
 __device__ __forceinline__ void sort_scatter_piped_body(
     const double* __restrict__ src, const uint8_t* __restrict__ m_src, const uint8_t* __restrict__ d_src,
     const int32_t* __restrict__ p_src, double* dst, uint8_t* m_dst, uint8_t* d_dst, int32_t* p_dst, int64_t n,
-    int64_t stride, const ScState* __restrict__ scp, int gx, int gy, int gz, const int32_t* __restrict__ offsets,
-    int32_t* cursor, int vb, int vg)
+    int64_t stride, const ScState* __restrict__ scp, int gx, int gy, int gz, int32_t* cursor, int vb, int vg)
 {
     __shared__ int t_key[kTable]; // key; after the reservation, the run's first destination
     __shared__ int t_cnt[kTable];
@@ -279,7 +291,7 @@ __device__ __forceinline__ void sort_scatter_piped_body(
 #pragma unroll
         for (int k = 0; k < EPT; ++k) {
             const int e = threadIdx.x * EPT + k;
-            g[k] = c[k] ? offsets[t_key[e]] + atomicAdd(&cursor[t_key[e]], c[k]) : 0;
+            g[k] = c[k] ? atomicAdd(&cursor[t_key[e]], c[k]) : 0;
         }
         __syncthreads();
         int run = inc - tot;
@@ -334,11 +346,10 @@ __device__ __forceinline__ void sort_scatter_piped_body(
 __global__ void __launch_bounds__(kTileThreads) sort_scatter_piped_kernel(
     const double* __restrict__ src, const uint8_t* __restrict__ m_src, const uint8_t* __restrict__ d_src,
     const int32_t* __restrict__ p_src, double* dst, uint8_t* m_dst, uint8_t* d_dst, int32_t* p_dst, int64_t n,
-    int64_t stride, const ScState* __restrict__ scp, int gx, int gy, int gz, const int32_t* __restrict__ offsets,
-    int32_t* cursor)
+    int64_t stride, const ScState* __restrict__ scp, int gx, int gy, int gz, int32_t* cursor)
 {
-    sort_scatter_piped_body(src, m_src, d_src, p_src, dst, m_dst, d_dst, p_dst, n, stride, scp, gx, gy, gz, offsets,
-                            cursor, blockIdx.x, gridDim.x);
+    sort_scatter_piped_body(src, m_src, d_src, p_src, dst, m_dst, d_dst, p_dst, n, stride, scp, gx, gy, gz, cursor,
+                            blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -349,7 +360,7 @@ __global__ void __launch_bounds__(kTileThreads) sort_scatter_piped_kernel(
 // ---------------------------------------------------------------------------
 struct SortView {
     int G, m, nb;
-    int32_t *counts, *offsets, *cursor, *bsums;
+    int32_t *counts, *offsets, *bsums;
 };
 __host__ __device__ __forceinline__ SortView sort_view(const SortItem& it)
 {
@@ -359,8 +370,7 @@ __host__ __device__ __forceinline__ SortView sort_view(const SortItem& it)
     v.nb = (v.m + kScanBlock - 1) / kScanBlock;
     v.counts = it.scratch;
     v.offsets = v.counts + v.m;
-    v.cursor = v.offsets + v.m;
-    v.bsums = v.cursor + v.m;
+    v.bsums = v.offsets + v.m;
     return v;
 }
 
@@ -377,17 +387,14 @@ __device__ __forceinline__ int sort_item_of(const int* __restrict__ first, int n
     return lo;
 }
 
-// grid (x, nitems): item blockIdx.y clears its counts and cursors
+// grid (x, nitems): item blockIdx.y clears its counts
 __global__ void sort_zero_list_kernel(const SortItem* __restrict__ items)
 {
     const SortView v = sort_view(items[blockIdx.y]);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.m; i += gridDim.x * blockDim.x) {
-        v.counts[i] = 0;
-        v.cursor[i] = 0;
-    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v.m; i += gridDim.x * blockDim.x) v.counts[i] = 0;
 }
 
-__global__ void __launch_bounds__(256) sort_hist_list_kernel(const SortItem* __restrict__ items,
+__global__ void __launch_bounds__(256, 6) sort_hist_list_kernel(const SortItem* __restrict__ items,
                                                              const int* __restrict__ first, int nitems)
 {
     const int k = sort_item_of(first, nitems);
@@ -427,7 +434,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) sort_scatter_list_kernel(cons
     const SortView v = sort_view(it);
     const SortBuffers& sb = it.sb;
     sort_scatter_piped_body(sb.parts, sb.masks, sb.discards, sb.perm, sb.parts2, sb.masks2, sb.discards2, sb.perm2,
-                            sb.n, sb.stride, it.sc, it.gx, it.gy, it.gz, v.offsets, v.cursor,
+                            sb.n, sb.stride, it.sc, it.gx, it.gy, it.gz, v.offsets,
                             (int)blockIdx.x - first[k], first[k + 1] - first[k]);
 }
 
@@ -509,9 +516,9 @@ static int sm_count_s()
 }
 
 size_t sort_scratch_ints(int64_t G)
-{ // counts, offsets (=cursor base), cursor, block sums
+{ // counts, offsets (advanced in place by the scatter's reservations), block sums
     const int64_t m = G + 2;
-    return (size_t)(3 * m + (m + kScanBlock - 1) / kScanBlock + 8);
+    return (size_t)(2 * m + (m + kScanBlock - 1) / kScanBlock + 8);
 }
 
 cudaError_t launch_cell_sort(const SortBuffers& sb, int32_t* scratch, const ScState* sc, int gx, int gy, int gz,
@@ -521,20 +528,19 @@ cudaError_t launch_cell_sort(const SortBuffers& sb, int32_t* scratch, const ScSt
     const int m = (int)(G + 2);
     int32_t* counts = scratch;
     int32_t* offsets = counts + m;
-    int32_t* cursor = offsets + m;
-    int32_t* bsums = cursor + m;
+    int32_t* bsums = offsets + m;
     const int nb = (m + kScanBlock - 1) / kScanBlock;
     cudaError_t e;
     if ((e = cudaMemsetAsync(counts, 0, sizeof(int32_t) * m, s))) return e;
-    if ((e = cudaMemsetAsync(cursor, 0, sizeof(int32_t) * m, s))) return e;
     const int grid = sm_count_s() * 8;
-    sort_hist_kernel<<<grid, 256, 0, s>>>(sb.parts, sb.stride, sb.masks, sb.n, sc, gx, gy, gz, counts);
+    sort_hist_kernel<<<sm_count_s() * 6, 256, 0, s>>>(sb.parts, sb.stride, sb.masks, sb.n, sc, gx, gy, gz, counts);
     scan_block_kernel<<<nb, 256, 0, s>>>(counts, offsets, m, bsums);
     scan_sums_kernel<<<1, 1024, 0, s>>>(bsums, nb);
     scan_add_kernel<<<(m + 255) / 256, 256, 0, s>>>(offsets, m, bsums);
+    // each distinct key of a tile reserves its run by advancing offsets[key]
     sort_scatter_piped_kernel<<<grid, kTileThreads, 0, s>>>(sb.parts, sb.masks, sb.discards, sb.perm, sb.parts2,
                                                             sb.masks2, sb.discards2, sb.perm2, sb.n, sb.stride, sc, gx,
-                                                            gy, gz, offsets, cursor);
+                                                            gy, gz, offsets);
     return cudaGetLastError();
 }
 
