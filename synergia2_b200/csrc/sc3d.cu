@@ -601,11 +601,16 @@ __device__ __forceinline__ void deposit_tile_body(const double* __restrict__ par
         __syncthreads();
         // 4. the tile's interior points to rho
         const double back = w0 / scale;
+        // v / BX and r / BY through float reciprocals: (v + 0.5) / BX lies at
+        // least 0.5 / BX from an integer, and with v < 2^22 / BX the float
+        // rounding stays below that, so the truncation is the integer quotient
+        const float ibx = 1.0f / (float)BX, iby = 1.0f / (float)BY;
         for (int v = t; v < V; v += kDepT) {
             const uint32_t a0 = sm.d0[v], a1 = sm.d1[v], a2 = sm.d2[v];
             if ((a0 | a1 | a2) == 0u) continue;
-            const int r = v / BX;
-            const int X = bmin[0] + (v - r * BX), Y = bmin[1] + (r % BY), Z = bmin[2] + r / BY;
+            const int r = (int)(((float)v + 0.5f) * ibx);
+            const int rz = (int)(((float)r + 0.5f) * iby);
+            const int X = bmin[0] + (v - r * BX), Y = bmin[1] + (r - rz * BY), Z = bmin[2] + rz;
             if (X > 0 && X < gx - 1 && Y > 0 && Y < gy - 1 && Z > 0 && Z < gz - 1) {
                 const double sum = ((double)a2 * 4398046511104.0 + (double)a1 * 2097152.0) + (double)a0;
                 atomicAdd(&rho[((int64_t)Z * gy + Y) * gx + X], (RT)(sum * back));
