@@ -709,9 +709,10 @@ __global__ void green_octant_kernel(const ScState* __restrict__ scp, double* G, 
         const double G000 = 2.8 / fmin(hx, fmin(hy, hz));
         for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
              t += (int64_t)gridDim.x * blockDim.x) {
-            const int ix = (int)(t % ox);
-            const int iy = (int)((t / ox) % oy);
-            const int iz = (int)(t / ((int64_t)ox * oy));
+            const unsigned tt = (unsigned)t, r = tt / (unsigned)ox; // total < 2^31
+            const int ix = (int)(tt - r * (unsigned)ox);
+            const int iy = (int)(r % (unsigned)oy);
+            const int iz = (int)(r / (unsigned)oy);
             const double dx = ix * hx, dy = iy * hy, dz = iz * hz;
             G[t] = (ix == 0 && iy == 0 && iz == 0) ? G000 : 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
         }
@@ -726,9 +727,10 @@ __global__ void green_octant_kernel(const ScState* __restrict__ scp, double* G, 
     const int64_t plane = (int64_t)ox * oy;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
          t += (int64_t)gridDim.x * blockDim.x) {
-        const int ix = (int)(t % ox);
-        const int iy = (int)((t / ox) % oy);
-        const int c = (int)(t / plane);
+        const unsigned tt = (unsigned)t, r = tt / (unsigned)ox; // total < 2^31
+        const int ix = (int)(tt - r * (unsigned)ox);
+        const int iy = (int)(r % (unsigned)oy);
+        const int c = (int)(r / (unsigned)oy);
         const int k0 = c * kGreenChunk, k1 = min(oz, k0 + kGreenChunk);
         const double x = ix * hx, y = iy * hy;
         const double rr = x * x + y * y;
@@ -805,7 +807,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xf_kernel(const RI
     const int64_t nlines = (int64_t)npy * d.gz;
     const int64_t l = (int64_t)blockIdx.x * NW + li;
     const bool ok = l < nlines;
-    const int pr = ok ? (int)(l % npy) : 0, z = ok ? (int)(l / npy) : 0;
+    const int z = ok ? (int)((unsigned)l / (unsigned)npy) : 0, pr = ok ? (int)l - z * npy : 0; // nlines < 2^31
     const int ya = 2 * pr, yb = ya + 1;
     const RI* ra = rho + ((int64_t)z * d.gy + ya) * d.gx;
     const RI* rb = rho + ((int64_t)z * d.gy + yb) * d.gx;
@@ -952,7 +954,7 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_xi_kernel(const C*
     const int64_t nlines = (int64_t)npy * d.gz;
     const int64_t l = (int64_t)blockIdx.x * NW + li;
     const bool ok = l < nlines;
-    const int pr = ok ? (int)(l % npy) : 0, z = ok ? (int)(l / npy) : 0;
+    const int z = ok ? (int)((unsigned)l / (unsigned)npy) : 0, pr = ok ? (int)l - z * npy : 0; // nlines < 2^31
     const int ya = 2 * pr, yb = ya + 1;
     const C* sa = S + ((int64_t)z * d.ny + ya) * d.nkxp;
     const C* sb = S + ((int64_t)z * d.ny + yb) * d.nkxp;
@@ -1023,7 +1025,10 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_green_kernel(doubl
     else { nlines = (int64_t)ox * oy; sj = (int64_t)ox * oy; }
     auto line_base = [&](int64_t l) -> int64_t {
         if (AXIS == 0) return l * ox;                                  // (y, z) rows
-        if (AXIS == 1) return (l % ox) + (l / ox) * (int64_t)ox * oy;  // (kx, z)
+        if (AXIS == 1) { // (kx, z); nlines < 2^31
+            const int zz = (int)((unsigned)l / (unsigned)ox);
+            return (l - (int64_t)zz * ox) + zz * (int64_t)ox * oy;
+        }
         return l;                                                      // (kx, ky)
     };
     const int64_t c = (int64_t)blockIdx.x * W + li;
@@ -1054,16 +1059,20 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_green_kernel(doubl
 // E = -grad phi by central differences on interior cells of the original
 // grid, zero on the boundary: alg_force_extractor_doubled_domain
 // space_charge_3d_kernels.h:217-307 (h of the doubled domain).
+// one 32-byte store per FP64 cell {ex, ey, ez, 0} (the field is 32-byte
+// aligned: the kick reads each cell with one 32-byte load)
 __device__ __forceinline__ void store_e(double2* E, int64_t i, double ex, double ey, double ez)
 {
-    E[2 * i] = make_double2(ex, ey);
-    E[2 * i + 1] = make_double2(ez, 0.0);
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(E + 2 * i), "d"(ex), "d"(ey), "d"(ez), "d"(0.0)
+                 : "memory");
 }
 __device__ __forceinline__ void store_e(float4* E, int64_t i, float ex, float ey, float ez)
 {
     E[i] = make_float4(ex, ey, ez, 0.0f);
 }
 
+// One warp per x row (iy, iz): the row's indices come from one 32-bit
+// division instead of three 64-bit ones per point.
 template <typename R, typename EV>
 __global__ void efield_kernel(const R* __restrict__ phi, EV* E, int gx, int gy, int gz,
                               const ScState* __restrict__ scp, const ConvItem* __restrict__ list)
@@ -1076,19 +1085,23 @@ __global__ void efield_kernel(const R* __restrict__ phi, EV* E, int gx, int gy, 
     const ScState& sc = *scp;
     if (!sc.valid) return;
     const R ihx = (R)(0.5 / sc.dh[0]), ihy = (R)(0.5 / sc.dh[1]), ihz = (R)(0.5 / sc.dh[2]);
-    const int64_t total = (int64_t)gx * gy * gz;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        int ix = (int)(i % gx);
-        int iy = (int)((i / gx) % gy);
-        int iz = (int)(i / ((int64_t)gx * gy));
-        R ex = 0, ey = 0, ez = 0;
-        if (!(ix == 0 || ix == gx - 1 || iy == 0 || iy == gy - 1 || iz == 0 || iz == gz - 1)) {
-            ex = -(phi[i + 1] - phi[i - 1]) * ihx;
-            ey = -(phi[i + gx] - phi[i - gx]) * ihy;
-            ez = -(phi[i + (int64_t)gx * gy] - phi[i - (int64_t)gx * gy]) * ihz;
+    const int rows = gy * gz, lane = threadIdx.x & 31;
+    const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+    const int64_t plane = (int64_t)gx * gy;
+    for (int r = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); r < rows; r += nw) {
+        const int iz = r / gy, iy = r - iz * gy;
+        const bool yz_in = iy > 0 && iy < gy - 1 && iz > 0 && iz < gz - 1;
+        const int64_t row = (int64_t)r * gx;
+        for (int ix = lane; ix < gx; ix += 32) {
+            const int64_t i = row + ix;
+            R ex = 0, ey = 0, ez = 0;
+            if (yz_in && ix > 0 && ix < gx - 1) {
+                ex = -(phi[i + 1] - phi[i - 1]) * ihx;
+                ey = -(phi[i + gx] - phi[i - gx]) * ihy;
+                ez = -(phi[i + plane] - phi[i - plane]) * ihz;
+            }
+            store_e(E, i, ex, ey, ez);
         }
-        store_e(E, i, ex, ey, ez);
     }
 }
 
@@ -1470,7 +1483,7 @@ cudaError_t launch_convolve_list(int mode, const ConvItem* items, int nitems, co
 
 cudaError_t launch_efield(const double* phi, double2* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s)
 {
-    int64_t total = (int64_t)gx * gy * gz;
+    int64_t total = (int64_t)gy * gz * 32; // one warp per x row
     int nb = (int)std::min<int64_t>((total + 255) / 256, (int64_t)sm_count() * 16);
     efield_kernel<double, double2><<<nb, 256, 0, s>>>(phi, E, gx, gy, gz, sc, nullptr);
     return cudaGetLastError();
@@ -1478,7 +1491,7 @@ cudaError_t launch_efield(const double* phi, double2* E, int gx, int gy, int gz,
 
 cudaError_t launch_efield_f32(const float* phi, float4* E, int gx, int gy, int gz, const ScState* sc, cudaStream_t s)
 {
-    int64_t total = (int64_t)gx * gy * gz;
+    int64_t total = (int64_t)gy * gz * 32; // one warp per x row
     int nb = (int)std::min<int64_t>((total + 255) / 256, (int64_t)sm_count() * 16);
     efield_kernel<float, float4><<<nb, 256, 0, s>>>(phi, E, gx, gy, gz, sc, nullptr);
     return cudaGetLastError();
@@ -1486,7 +1499,7 @@ cudaError_t launch_efield_f32(const float* phi, float4* E, int gx, int gy, int g
 
 cudaError_t launch_efield_list(bool f32, const ConvItem* items, int nitems, int gx, int gy, int gz, cudaStream_t s)
 {
-    int64_t total = (int64_t)gx * gy * gz;
+    int64_t total = (int64_t)gy * gz * 32; // one warp per x row
     int nb = (int)std::min<int64_t>((total + 255) / 256, std::max<int64_t>(1, (int64_t)sm_count() * 16 / nitems));
     if (f32)
         efield_kernel<float, float4><<<dim3(nb, nitems), 256, 0, s>>>(nullptr, nullptr, gx, gy, gz, nullptr, items);
