@@ -854,9 +854,12 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_y_kernel(C* S, con
     W* sm = (W*)sm_raw;
     if (!scp->valid) return;
     const int li = LAY::line(), t = LAY::thr();
-    const int kx = blockIdx.x * NW + li, z = blockIdx.y;
-    const bool ok = kx < d.nkx;
-    C* col = S + (int64_t)z * d.ny * d.nkxp + kx;
+    // lines (kx, z) numbered z * nkxp + kx over the padded row pitch, so no
+    // CTA idles on a row's last column (nkx = nx / 2 + 1 is odd)
+    const int l = blockIdx.x * NW + li;
+    const int z = (int)((unsigned)l / (unsigned)d.nkxp), kx = l - z * d.nkxp;
+    const bool ok = kx < d.nkx && z < d.gz;
+    C* col = S + (int64_t)(ok ? z : 0) * d.ny * d.nkxp + (ok ? kx : 0);
     const int nin = INV ? L : d.gy;
     W v[fft::kE];
 #pragma unroll
@@ -899,8 +902,11 @@ __global__ void __launch_bounds__(fft::Shape<L>::THREADS) fft_z_conv_kernel(C* S
     W* sm = (W*)sm_raw;
     if (!scp->valid) return;
     const int li = LAY::line(), t = LAY::thr();
-    const int kx = blockIdx.x * NW + li, ky = blockIdx.y;
-    const bool ok = kx < d.nkx;
+    // lines (kx, ky) numbered ky * nkxp + kx (see the y pass)
+    const int l = blockIdx.x * NW + li;
+    const int ky0 = (int)((unsigned)l / (unsigned)d.nkxp), kx0 = l - ky0 * d.nkxp;
+    const bool ok = kx0 < d.nkx && ky0 < d.ny;
+    const int kx = ok ? kx0 : 0, ky = ok ? ky0 : 0;
     C* col = S + (int64_t)ky * d.nkxp + kx;
     const int64_t zs = (int64_t)d.ny * d.nkxp;
     W v[fft::kE];
@@ -1372,7 +1378,7 @@ static cudaError_t pass_y(C* S, const W* tw, const Dims& d, const ScState* sc, c
     const int bytes = fft::LMajor<L>::kSmemElems * (int)sizeof(W);
     static cudaError_t once = fft_smem(fft_y_kernel<L, PLAN, C, W, INV>, bytes);
     if (once) return once;
-    dim3 grid(ceil_div64(d.nkx, fft::Shape<L>::W), d.gz, nitems);
+    dim3 grid(ceil_div64((int64_t)d.gz * d.nkxp, fft::Shape<L>::W), 1, nitems);
     fft_y_kernel<L, PLAN, C, W, INV><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, tw, d, sc, list);
     return cudaSuccess;
 }
@@ -1383,7 +1389,7 @@ static cudaError_t pass_z(C* S, const double* Ghat, const W* tw, const Dims& d, 
     const int bytes = fft::LMajor<L>::kSmemElems * (int)sizeof(W);
     static cudaError_t once = fft_smem(fft_z_conv_kernel<L, PLAN, C, W>, bytes);
     if (once) return once;
-    dim3 grid(ceil_div64(d.nkx, fft::Shape<L>::W), d.ny, nitems);
+    dim3 grid(ceil_div64((int64_t)d.ny * d.nkxp, fft::Shape<L>::W), 1, nitems);
     fft_z_conv_kernel<L, PLAN, C, W><<<grid, fft::Shape<L>::THREADS, bytes, s>>>(S, Ghat, tw, d, sc, list);
     return cudaSuccess;
 }
