@@ -516,6 +516,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="time the default launch shapes")
+    ap.add_argument("--no-graphs", action="store_true", help="time direct launches instead of CUDA-graph turns")
     ap.add_argument("--particles", type=int, default=N_PART, help="bunch size (profiling cases only)")
     ap.add_argument("--config", default="c1", choices=["c1", "c2", "c3", "c4"],
                     help="c1: FODO 4M FP64 + mixed (default); c2: 64-bunch quad scan; c3: 24-cell ring, 2^24 "
@@ -605,6 +606,14 @@ def main():
                  "default_ms": round(trials[0]["ms"], 3), "best_ms": round(min(r["ms"] for r in trials), 3)}
     barrier()
 
+    # CUDA-graph turns: every whole turn inside the K steps is one graph
+    # launch (the steps before and after run as direct launches); the graphs
+    # are captured ahead, untimed, without running anything
+    if not args.no_graphs:
+        prop.set_graphs(True)
+        prop.prepare_steps(bunch, args.warmup, args.steps, stream=sp)
+    barrier()
+
     # timed region: device time with CUDA events on the launching stream
     # (the library's per-category profiler is off: its event pairs around
     # every launch would be timed too)
@@ -619,6 +628,8 @@ def main():
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
     n_alive = bunch.get_total_num()
+    graph_stats = prop.graph_stats()
+    prop.set_graphs(False)  # the breakdown and the e2e leg launch directly
 
     # the same K steps once more with the per-category profiler (CUDA events
     # around every launch on the launching stream): the step breakdown and
@@ -698,9 +709,13 @@ def main():
                        "global_batch": npart * world, "grid": list(GRID),
                        "precision": "fp64 (drop-in)", "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (bunch 235 MB per GPU)",
+                       "launch": ("CUDA-graph turns for the whole turns inside the K steps (%d captured ahead, "
+                                  "%d replayed), direct launches for the rest" % graph_stats)
+                       if not args.no_graphs else "direct launches",
                        "step_breakdown_ms": {k: round(v[0] / args.steps, 4) for k, v in prof.items()},
-                       "step_breakdown_how": "a second run of the same K steps with CUDA events around every "
-                                             "launch (%.4f ms/step with those events)" % (prof_ms / args.steps)},
+                       "step_breakdown_how": "a second run of the same K steps, direct launches with CUDA events "
+                                             "around every launch (%.4f ms/step with those events)"
+                                             % (prof_ms / args.steps)},
             "roofline": {"kernel": "track_kernel light variant (fused particle pass)", "bound": "hbm",
                          "achieved": achieved, "peak": pk["hbm_gbs"], "peak_source": src, "unit": "GB/s",
                          "frac": achieved / pk["hbm_gbs"], "traffic": traffic,

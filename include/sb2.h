@@ -234,9 +234,20 @@ sb2_status sb2_propagator_propagate_steps(sb2_propagator* p, sb2_bunch* b, int32
                                           int32_t count, void* stream);
 /* Replay each turn from a CUDA graph: the first turn with a given launch
  * signature is captured, later turns whose host-side re-derivation (op
- * lists, time steps) gives the same signature are replayed with one graph
- * launch.  The cell-ordered working copy is not used in this mode. */
+ * lists, time steps, working-copy buffers) gives the same signature are
+ * replayed with one graph launch.  propagate replays every turn;
+ * propagate_steps replays every whole turn inside its range of steps and
+ * launches the steps before and after them directly.  Off (0) drops the
+ * cached graphs. */
 sb2_status sb2_propagator_set_graphs(sb2_propagator* p, int32_t on);
+/* With CUDA-graph turns on: capture, without running anything on the GPU,
+ * the graphs that sb2_propagator_propagate_steps(p, b, first, count, ...)
+ * will replay, so that call starts no capture.  The bunch is left as it was
+ * (the steps are re-derived on the host only).  Does nothing with graphs
+ * off, or for a bunch that has not been propagated yet (its first call
+ * captures). */
+sb2_status sb2_propagator_prepare_steps(sb2_propagator* p, sb2_bunch* b, int32_t first, int32_t count,
+                                        void* stream);
 sb2_status sb2_propagator_graph_stats(sb2_propagator* p, int64_t* captures, int64_t* replays);
 /* Charge lost on lattice element `index` through the aperture operations
  * (Lattice_element::deposit_charge, aperture_operation.h:14-24), summed over

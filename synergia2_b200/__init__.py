@@ -570,8 +570,16 @@ class Propagator:
         check(lib().sb2_propagator_propagate_steps(self.h, bunch.h, int(first), int(count), stream))
 
     def set_graphs(self, on=True):
-        """Replay each turn from a CUDA graph (captured on first use)."""
+        """Replay each turn from a CUDA graph (captured on first use):
+        every turn of propagate, every whole turn inside the range of
+        propagate_steps."""
         check(lib().sb2_propagator_set_graphs(self.h, 1 if on else 0))
+
+    def prepare_steps(self, bunch, first, count, stream=None):
+        """Capture ahead, without running them, the graphs that
+        propagate_steps(bunch, first, count) will replay
+        (sb2_propagator_prepare_steps); the bunch is left as it was."""
+        check(lib().sb2_propagator_prepare_steps(self.h, bunch.h, int(first), int(count), stream))
 
     def graph_stats(self):
         c, r = ctypes.c_int64(), ctypes.c_int64()

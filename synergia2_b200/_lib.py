@@ -125,6 +125,7 @@ SIGNATURES = {
     "sb2_sc3d_last": (_i32, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd]),
     "sb2_sc3d_apply_noalloc": (_i32, [_popts, _vp, _i64, _vp, _i64, _i32, _d, _i32, _d, _d, _i32, _d, _vp]),
     "sb2_allreduce_stream": (_vp, []),
+    "sb2_propagator_prepare_steps": (_i32, [_vp, _vp, _i32, _i32, _vp]),
     "sb2_propagator_set_allreduce_typed": (_i32, [_vp, _vp, _vp, _i32]),
     "sb2_batch_run_lockstep": (_i32, [_vp, _pi32, _i32, _i32]),
     "sb2_libff_apply": (_i32, [_vp, _pd, _i32, _vp, _vp]),

@@ -511,6 +511,13 @@ struct Bunch {
     void enter_work(cudaStream_t s)
     {
         if (permuted) return;
+        enter_work_host();
+        cuda_check(launch_sort_gather_in(home_parts, home_stride, home_masks, home_discards, wc, s), "sort gather");
+    }
+    // enter_work's host side: the working copy's buffers and the switch to
+    // them (without the gather, which enter_work launches)
+    void enter_work_host()
+    {
         if (!wc.parts) {
             // a multiple of 32 particles: every column starts 256-byte
             // aligned, and the sort's 16-byte staging copies of the last
@@ -527,7 +534,6 @@ struct Bunch {
             wc.perm = dalloc<int32_t>(cap, "working copy");
             wc.perm2 = dalloc<int32_t>(cap, "working copy");
         }
-        cuda_check(launch_sort_gather_in(home_parts, home_stride, home_masks, home_discards, wc, s), "sort gather");
         parts = wc.parts;
         stride = wc.stride;
         masks = wc.masks;
@@ -3009,6 +3015,13 @@ struct Propagator {
             }
         // capture this turn
         restore(b, s0);
+        cuda_check(cudaGraphLaunch(capture_turn(b, s), s), "graph launch");
+    }
+
+    // Capture run_turn into a new cached graph (the host state advances as
+    // if the turn ran; nothing runs on the GPU) and return it.
+    cudaGraphExec_t capture_turn(Bunch& b, cudaStream_t s)
+    {
         std::vector<unsigned char> sig2;
         cudaGraph_t graph = nullptr;
         cuda_check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -3034,9 +3047,84 @@ struct Propagator {
             cudaGraphExecDestroy(graphs[lru].exec);
             graphs.erase(graphs.begin() + lru);
         }
-        graphs.push_back(CachedGraph{sig2, exec, graph_clock});
+        graphs.push_back(CachedGraph{sig2, exec, ++graph_clock});
         ++graph_captures;
-        cuda_check(cudaGraphLaunch(exec, s), "graph launch");
+        return exec;
+    }
+
+    // Capture, without running them, the graphs that propagate_steps(b,
+    // first, count) will replay: the steps are re-derived on the host only
+    // (as the signature check of a graph turn does), each whole turn whose
+    // signature is not cached yet is captured, and the bunch's host state is
+    // put back.  Nothing runs on the GPU (a bunch not yet in its cell-ordered
+    // working copy gets the copy's buffers, not its gather).
+    void prepare_steps(Bunch& b, int first, int count, cudaStream_t s)
+    {
+        if (!use_graphs || count <= 0 || steps.empty()) return;
+        s = graph_stream(s);
+        ensure_device();
+        const int ns = (int)steps.size();
+        const HostSnap s0 = snap(b);
+        const bool keep_sort = sort_active, keep_permuted = b.permuted;
+        const int64_t keep_stride = b.stride;
+        sort_active = sorting(b);
+        if (sort_active && !b.permuted) { // as the call's enter_sorted will (its gather is not launched here)
+            if (!sort_scratch) {
+                const int64_t G = (int64_t)sc_opts.shape[0] * sc_opts.shape[1] * sc_opts.shape[2];
+                sort_scratch = dalloc<int32_t>(sort_scratch_ints(G), "sort scratch");
+            }
+            b.enter_work_host();
+        }
+        auto put_back = [&]() {
+            g_sig = LaunchSig{};
+            const SortBuffers wc = b.wc;
+            restore(b, s0);
+            // buffers allocated here stay: the call enters the same ones,
+            // which the captured graphs name
+            if (!keep_permuted && !s0.wc.parts) b.wc = wc;
+            b.permuted = keep_permuted;
+            b.stride = keep_stride;
+            sort_active = keep_sort;
+        };
+        const bool design_set = b.design_set;
+        if (b.turns_done == 0 && !b.design_set) { // as begin() does
+            b.design = lat.ref;
+            b.design_set = true;
+        }
+        std::vector<unsigned char> scratch_sig;
+        try {
+            for (int k = first; k < first + count;) {
+                if (((k % ns) + ns) % ns == 0 && first + count - k >= ns) {
+                    const HostSnap t0 = snap(b);
+                    std::vector<unsigned char> sig;
+                    g_sig.dry = true;
+                    g_sig.sig = &sig;
+                    run_turn(b, s);
+                    g_sig = LaunchSig{};
+                    bool cached = false;
+                    for (auto& g : graphs)
+                        if (g.sig == sig) cached = true;
+                    if (!cached) {
+                        restore(b, t0);
+                        capture_turn(b, s);
+                    }
+                    k += ns;
+                } else {
+                    g_sig.dry = true;
+                    g_sig.sig = &scratch_sig;
+                    plain_step(b, k, s);
+                    g_sig = LaunchSig{};
+                    scratch_sig.clear();
+                    ++k;
+                }
+            }
+        } catch (...) {
+            put_back();
+            b.design_set = design_set;
+            throw;
+        }
+        put_back();
+        b.design_set = design_set;
     }
 
     // Turns without the end-of-call synchronisation (batched jobs): the
@@ -3065,19 +3153,36 @@ struct Propagator {
         finish(b, s);
     }
 
+    // one step of propagate_steps outside a graph turn
+    void plain_step(Bunch& b, int k, cudaStream_t s)
+    {
+        const int ns = (int)steps.size();
+        const int si = ((k % ns) + ns) % ns;
+        if (si == 0) b.ref.start_repetition();
+        run_step(b, steps[si], s);
+        if (si == ns - 1) {
+            b.turns_done += 1;
+            record_diagnostics(b, s);
+        }
+    }
+    // With CUDA-graph turns on, every whole turn inside [first, first +
+    // count) is one graph launch (run_turn is the same start of repetition,
+    // steps, turn count and diagnostics as the plain steps); the steps before
+    // the first and after the last whole turn run as plain launches.
     void propagate_steps(Bunch& b, int first, int count, cudaStream_t s)
     {
+        if (use_graphs) s = graph_stream(s);
         begin(b, s);
         enter_sorted(b, s);
         if (diag_cap && diag_s.empty()) record_diagnostics(b, s); // initial state
         const int ns = (int)steps.size();
-        for (int k = first; k < first + count; ++k) {
-            int si = ((k % ns) + ns) % ns;
-            if (si == 0) b.ref.start_repetition();
-            run_step(b, steps[si], s);
-            if (si == ns - 1) {
-                b.turns_done += 1;
-                record_diagnostics(b, s);
+        for (int k = first; k < first + count;) {
+            if (use_graphs && ns > 0 && ((k % ns) + ns) % ns == 0 && first + count - k >= ns) {
+                propagate_graph_turn(b, s);
+                k += ns;
+            } else {
+                plain_step(b, k, s);
+                ++k;
             }
         }
         if (count > 0 && ns > 0) b.next_step = (((first + count) % ns) + ns) % ns;
@@ -4254,6 +4359,13 @@ sb2_status sb2_propagator_propagate_steps(sb2_propagator* p, sb2_bunch* b, int32
     SB2_TRY
     SB2_REQUIRE(p && b && count >= 0, "bad argument");
     p->p->propagate_steps(b->b, first, count, as_stream(stream));
+    SB2_CATCH
+}
+sb2_status sb2_propagator_prepare_steps(sb2_propagator* p, sb2_bunch* b, int32_t first, int32_t count, void* stream)
+{
+    SB2_TRY
+    SB2_REQUIRE(p && b && count >= 0, "bad argument");
+    p->p->prepare_steps(b->b, first, count, as_stream(stream));
     SB2_CATCH
 }
 sb2_status sb2_propagator_set_graphs(sb2_propagator* p, int32_t on)

@@ -241,3 +241,39 @@ def test_lockstep_rejects_shared_propagator_or_bunch(syn):
         s1, s2 = batch.add(*pair[0]), batch.add(*pair[1])
         with pytest.raises(syn.SB2Error, match="own propagator and bunch"):
             batch.run_lockstep([s1, s2], 1)
+
+
+def test_graph_turns_inside_propagate_steps(syn):
+    """propagate_steps with CUDA-graph turns (the working copy cell-sorted):
+    the whole turns inside the range replay graphs, the steps before and after
+    them launch directly, and the result equals the same steps without graphs
+    (ids and masks exact, coordinates to the deposit-order tolerance 1e-10).
+    prepare_steps captures those graphs ahead and leaves the bunch as it was,
+    so the call itself only replays."""
+    n = 60000
+    p = gaussian_bunch(n, SIG_C0, 83)
+    lat, ref = product_lattice(fodo_cell())
+    out = []
+    for graphs in (False, True):
+        prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(16, 16, 32), 8))
+        b = syn.Bunch(ref, n, 1e11)
+        b.set_particles(p)
+        prop.propagate_steps(b, 0, 5)
+        if graphs:
+            prop.set_graphs(True)
+            before = b.get_particles()
+            state = bytes(b.get_state())
+            prop.prepare_steps(b, 5, 21)
+            for x, y in zip(before, b.get_particles()):
+                assert np.array_equal(x, y)
+            assert bytes(b.get_state()) == state
+            c0, r0 = prop.graph_stats()
+            assert c0 >= 1 and r0 == 0
+        prop.propagate_steps(b, 5, 21)  # steps 5-7 direct, turns 8-15 and 16-23 graphs, 24-25 direct
+        if graphs:
+            assert prop.graph_stats() == (c0, r0 + 2)
+        out.append((b.get_particles(), b.counts()))
+    ((a, am, ad), ac), ((g, gm, gd), gc) = out
+    assert np.array_equal(am, gm) and np.array_equal(ad, gd) and np.array_equal(a[:, 6], g[:, 6]) and ac == gc
+    for j in range(6):
+        assert rel_l2(g[:, j], a[:, j]) <= 1e-10, j
