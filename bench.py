@@ -606,9 +606,9 @@ def main():
                  "default_ms": round(trials[0]["ms"], 3), "best_ms": round(min(r["ms"] for r in trials), 3)}
     barrier()
 
-    # CUDA-graph turns: every whole turn inside the K steps is one graph
-    # launch (the steps before and after run as direct launches); the graphs
-    # are captured ahead, untimed, without running anything
+    # CUDA-graph turns: the steps of the K that fall in one turn are one
+    # graph launch; the graphs are captured ahead, untimed, without running
+    # anything
     if not args.no_graphs:
         prop.set_graphs(True)
         prop.prepare_steps(bunch, args.warmup, args.steps, stream=sp)
@@ -709,8 +709,8 @@ def main():
                        "global_batch": npart * world, "grid": list(GRID),
                        "precision": "fp64 (drop-in)", "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (bunch 235 MB per GPU)",
-                       "launch": ("CUDA-graph turns for the whole turns inside the K steps (%d captured ahead, "
-                                  "%d replayed), direct launches for the rest" % graph_stats)
+                       "launch": ("CUDA graphs, one per turn or part of a turn inside the K steps (%d captured "
+                                  "ahead, untimed; %d replayed)" % graph_stats)
                        if not args.no_graphs else "direct launches",
                        "step_breakdown_ms": {k: round(v[0] / args.steps, 4) for k, v in prof.items()},
                        "step_breakdown_how": "a second run of the same K steps, direct launches with CUDA events "

@@ -236,9 +236,9 @@ sb2_status sb2_propagator_propagate_steps(sb2_propagator* p, sb2_bunch* b, int32
  * signature is captured, later turns whose host-side re-derivation (op
  * lists, time steps, working-copy buffers) gives the same signature are
  * replayed with one graph launch.  propagate replays every turn;
- * propagate_steps replays every whole turn inside its range of steps and
- * launches the steps before and after them directly.  Off (0) drops the
- * cached graphs. */
+ * propagate_steps launches the steps of its range that fall in one turn as
+ * one graph (whole turns, and the partial turns at either end).  Off (0)
+ * drops the cached graphs. */
 sb2_status sb2_propagator_set_graphs(sb2_propagator* p, int32_t on);
 /* With CUDA-graph turns on: capture, without running anything on the GPU,
  * the graphs that sb2_propagator_propagate_steps(p, b, first, count, ...)

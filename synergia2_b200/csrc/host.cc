@@ -2994,12 +2994,26 @@ struct Propagator {
 
     void propagate_graph_turn(Bunch& b, cudaStream_t s)
     {
+        graph_run(b, s, [&] { run_turn(b, s); });
+    }
+    // Steps [k0, k1) of one turn as one graph (propagate_steps).
+    void graph_segment(Bunch& b, int k0, int k1, cudaStream_t s)
+    {
+        graph_run(b, s, [&] {
+            for (int k = k0; k < k1; ++k) plain_step(b, k, s);
+        });
+    }
+    // The launches of run() from a cached graph with the same signature, or
+    // captured into a new one.
+    template <class F>
+    void graph_run(Bunch& b, cudaStream_t s, F&& run)
+    {
         HostSnap s0 = snap(b);
         std::vector<unsigned char> sig;
         g_sig.dry = true;
         g_sig.sig = &sig;
         try {
-            run_turn(b, s);
+            run();
         } catch (...) {
             g_sig = LaunchSig{};
             throw;
@@ -3013,21 +3027,21 @@ struct Propagator {
                 cuda_check(cudaGraphLaunch(g.exec, s), "graph launch");
                 return;
             }
-        // capture this turn
         restore(b, s0);
-        cuda_check(cudaGraphLaunch(capture_turn(b, s), s), "graph launch");
+        cuda_check(cudaGraphLaunch(capture(b, s, run), s), "graph launch");
     }
 
-    // Capture run_turn into a new cached graph (the host state advances as
-    // if the turn ran; nothing runs on the GPU) and return it.
-    cudaGraphExec_t capture_turn(Bunch& b, cudaStream_t s)
+    // Capture run() into a new cached graph (the host state advances as if
+    // it ran; nothing runs on the GPU) and return it.
+    template <class F>
+    cudaGraphExec_t capture(Bunch& b, cudaStream_t s, F&& run)
     {
         std::vector<unsigned char> sig2;
         cudaGraph_t graph = nullptr;
         cuda_check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
         g_sig.sig = &sig2;
         try {
-            run_turn(b, s);
+            run();
         } catch (...) {
             g_sig = LaunchSig{};
             cudaStreamEndCapture(s, &graph);
@@ -3054,7 +3068,7 @@ struct Propagator {
 
     // Capture, without running them, the graphs that propagate_steps(b,
     // first, count) will replay: the steps are re-derived on the host only
-    // (as the signature check of a graph turn does), each whole turn whose
+    // (as the signature check of a graph does), each segment whose
     // signature is not cached yet is captured, and the bunch's host state is
     // put back.  Nothing runs on the GPU (a bunch not yet in its cell-ordered
     // working copy gets the copy's buffers, not its gather).
@@ -3091,32 +3105,26 @@ struct Propagator {
             b.design = lat.ref;
             b.design_set = true;
         }
-        std::vector<unsigned char> scratch_sig;
         try {
             for (int k = first; k < first + count;) {
-                if (((k % ns) + ns) % ns == 0 && first + count - k >= ns) {
-                    const HostSnap t0 = snap(b);
-                    std::vector<unsigned char> sig;
-                    g_sig.dry = true;
-                    g_sig.sig = &sig;
-                    run_turn(b, s);
-                    g_sig = LaunchSig{};
-                    bool cached = false;
-                    for (auto& g : graphs)
-                        if (g.sig == sig) cached = true;
-                    if (!cached) {
-                        restore(b, t0);
-                        capture_turn(b, s);
-                    }
-                    k += ns;
-                } else {
-                    g_sig.dry = true;
-                    g_sig.sig = &scratch_sig;
-                    plain_step(b, k, s);
-                    g_sig = LaunchSig{};
-                    scratch_sig.clear();
-                    ++k;
+                const int k1 = std::min(first + count, k + ns - ((k % ns) + ns) % ns);
+                auto run = [&] {
+                    for (int j = k; j < k1; ++j) plain_step(b, j, s);
+                };
+                const HostSnap t0 = snap(b);
+                std::vector<unsigned char> sig;
+                g_sig.dry = true;
+                g_sig.sig = &sig;
+                run();
+                g_sig = LaunchSig{};
+                bool cached = false;
+                for (auto& g : graphs)
+                    if (g.sig == sig) cached = true;
+                if (!cached) {
+                    restore(b, t0);
+                    capture(b, s, run);
                 }
+                k = k1;
             }
         } catch (...) {
             put_back();
@@ -3165,10 +3173,10 @@ struct Propagator {
             record_diagnostics(b, s);
         }
     }
-    // With CUDA-graph turns on, every whole turn inside [first, first +
-    // count) is one graph launch (run_turn is the same start of repetition,
-    // steps, turn count and diagnostics as the plain steps); the steps before
-    // the first and after the last whole turn run as plain launches.
+    // With CUDA-graph turns on, the steps of [first, first + count) that
+    // fall in one turn are one graph launch: whole turns (the same start of
+    // repetition, steps, turn count and diagnostics as run_turn, so they share
+    // graphs with propagate) and the partial turns at either end.
     void propagate_steps(Bunch& b, int first, int count, cudaStream_t s)
     {
         if (use_graphs) s = graph_stream(s);
@@ -3177,9 +3185,10 @@ struct Propagator {
         if (diag_cap && diag_s.empty()) record_diagnostics(b, s); // initial state
         const int ns = (int)steps.size();
         for (int k = first; k < first + count;) {
-            if (use_graphs && ns > 0 && ((k % ns) + ns) % ns == 0 && first + count - k >= ns) {
-                propagate_graph_turn(b, s);
-                k += ns;
+            if (use_graphs && ns > 0) {
+                const int k1 = std::min(first + count, k + ns - ((k % ns) + ns) % ns);
+                graph_segment(b, k, k1, s);
+                k = k1;
             } else {
                 plain_step(b, k, s);
                 ++k;

@@ -245,11 +245,11 @@ def test_lockstep_rejects_shared_propagator_or_bunch(syn):
 
 def test_graph_turns_inside_propagate_steps(syn):
     """propagate_steps with CUDA-graph turns (the working copy cell-sorted):
-    the whole turns inside the range replay graphs, the steps before and after
-    them launch directly, and the result equals the same steps without graphs
-    (ids and masks exact, coordinates to the deposit-order tolerance 1e-10).
-    prepare_steps captures those graphs ahead and leaves the bunch as it was,
-    so the call itself only replays."""
+    the steps that fall in one turn are one graph (the partial turns at either
+    end and the whole turns between), and the result equals the same steps
+    without graphs (ids and masks exact, coordinates to the deposit-order
+    tolerance 1e-10).  prepare_steps captures those graphs ahead and leaves the
+    bunch as it was, so the call itself only replays."""
     n = 60000
     p = gaussian_bunch(n, SIG_C0, 83)
     lat, ref = product_lattice(fodo_cell())
@@ -268,10 +268,10 @@ def test_graph_turns_inside_propagate_steps(syn):
                 assert np.array_equal(x, y)
             assert bytes(b.get_state()) == state
             c0, r0 = prop.graph_stats()
-            assert c0 >= 1 and r0 == 0
-        prop.propagate_steps(b, 5, 21)  # steps 5-7 direct, turns 8-15 and 16-23 graphs, 24-25 direct
+            assert c0 >= 3 and r0 == 0  # steps 5-7, a whole turn, steps 24-25
+        prop.propagate_steps(b, 5, 21)  # graphs: steps 5-7, turns 8-15 and 16-23, steps 24-25
         if graphs:
-            assert prop.graph_stats() == (c0, r0 + 2)
+            assert prop.graph_stats() == (c0, r0 + 4)
         out.append((b.get_particles(), b.counts()))
     ((a, am, ad), ac), ((g, gm, gd), gc) = out
     assert np.array_equal(am, gm) and np.array_equal(ad, gd) and np.array_equal(a[:, 6], g[:, 6]) and ac == gc
