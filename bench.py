@@ -291,6 +291,8 @@ def mixed_vs_fp64(syn, torch, steps, warmup, passes, seed=1):
     b = syn.Bunch(ref, N_PART, REAL_NUM)
     b.populate_gaussian(SIGMAS, seed=seed)
     prop.propagate_steps(b, 0, warmup, stream=sp)
+    prop.set_graphs(True)  # as the FP64 headline: graphs per turn segment, captured ahead
+    prop.prepare_steps(b, warmup, steps, stream=sp)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
