@@ -3089,13 +3089,13 @@ struct Propagator {
             }
             b.enter_work_host();
         }
+        const SortBuffers entered_wc = b.wc; // before the sorts of the derivation swap its buffers
         auto put_back = [&]() {
             g_sig = LaunchSig{};
-            const SortBuffers wc = b.wc;
             restore(b, s0);
-            // buffers allocated here stay: the call enters the same ones,
-            // which the captured graphs name
-            if (!keep_permuted && !s0.wc.parts) b.wc = wc;
+            // buffers allocated here stay, in the order the call will enter
+            // them: the captured graphs name them
+            if (!keep_permuted && !s0.wc.parts) b.wc = entered_wc;
             b.permuted = keep_permuted;
             b.stride = keep_stride;
             sort_active = keep_sort;
@@ -3106,6 +3106,13 @@ struct Propagator {
             b.design_set = true;
         }
         try {
+            if (diag_cap && diag_s.empty()) { // the call's record of the initial state
+                std::vector<unsigned char> sig;
+                g_sig.dry = true;
+                g_sig.sig = &sig;
+                record_diagnostics(b, s);
+                g_sig = LaunchSig{};
+            }
             for (int k = first; k < first + count;) {
                 const int k1 = std::min(first + count, k + ns - ((k % ns) + ns) % ns);
                 auto run = [&] {

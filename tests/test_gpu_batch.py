@@ -277,3 +277,34 @@ def test_graph_turns_inside_propagate_steps(syn):
     assert np.array_equal(am, gm) and np.array_equal(ad, gd) and np.array_equal(a[:, 6], g[:, 6]) and ac == gc
     for j in range(6):
         assert rel_l2(g[:, j], a[:, j]) <= 1e-10, j
+
+
+def test_prepare_steps_with_diagnostics_from_the_first_call(syn):
+    """prepare_steps on a bunch never propagated, with per-turn diagnostics
+    on: the first propagate_steps call (which also records the initial state)
+    only replays, and its particles and diagnostics equal the same call
+    without graphs."""
+    n = 40000
+    p = gaussian_bunch(n, SIG_C0, 84)
+    lat, ref = product_lattice(fodo_cell())
+    out = []
+    for graphs in (False, True):
+        prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(16, 16, 32), 8))
+        prop.set_diagnostics(8)
+        b = syn.Bunch(ref, n, 1e11)
+        b.set_particles(p)
+        if graphs:
+            prop.set_graphs(True)
+            prop.prepare_steps(b, 0, 19)
+            c0, r0 = prop.graph_stats()
+        prop.propagate_steps(b, 0, 19)  # graphs: two whole turns, then steps 16-18
+        if graphs:
+            assert prop.graph_stats() == (c0, r0 + 3)
+        out.append((b.get_particles()[0], prop.diagnostics()))
+    (a, da), (g, dg) = out
+    assert np.array_equal(a[:, 6], g[:, 6])
+    for j in range(6):
+        assert rel_l2(g[:, j], a[:, j]) <= 1e-10, j
+    assert list(da["s"]) == list(dg["s"]) and len(da["s"]) == 3  # the initial state and two turn ends
+    for key in ("mean", "std"):
+        assert np.allclose(np.asarray(dg[key]), np.asarray(da[key]), rtol=1e-8, atol=1e-13), key
