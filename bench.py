@@ -218,6 +218,9 @@ def ring_c3(syn, torch, turns=1, warmup_steps=16):
         bunch.populate_gaussian([2e-3, 1e-4, 2e-3, 1e-4, 0.3, 1e-4], 3)
         prop.propagate_steps(bunch, 0, warmup_steps)
         best, trials = prop.autotune(bunch, steps=16)
+        # graphs per turn segment, captured ahead (untimed)
+        prop.set_graphs(True)
+        prop.prepare_steps(bunch, warmup_steps, 384 * turns)
         torch.cuda.synchronize()
         L = syn.lib()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -226,6 +229,8 @@ def ring_c3(syn, torch, turns=1, warmup_steps=16):
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
+        graph_stats = prop.graph_stats()
+        prop.set_graphs(False)  # the breakdown launches directly
         alive = bunch.get_total_num()
         emit = [float(x) for x in bunch.moments()[2]]
         # breakdown: the first 96 steps of the next turn with CUDA events
@@ -248,7 +253,8 @@ def ring_c3(syn, torch, turns=1, warmup_steps=16):
                      "roofline_fp64": fp64_roofline(syn, "ring_c3", alive, raw.get("track", (0.0, 0)),
                                                     raw.get("track_full", (0.0, 0))),
                      "autotune": {"best": best, "trials": len(trials), "default_ms": round(trials[0]["ms"], 3),
-                                  "best_ms": round(min(r["ms"] for r in trials), 3)}}
+                                  "best_ms": round(min(r["ms"] for r in trials), 3)},
+                     "graphs": {"captured_ahead": graph_stats[0], "replayed": graph_stats[1]}}
         del prop, bunch
         torch.cuda.empty_cache()
     out["value"] = out["mixed"]["value"]
