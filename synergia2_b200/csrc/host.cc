@@ -2273,6 +2273,7 @@ struct Engine {
     // the caller's host buffer in stream order.
     BunchCounters* rec_dev = nullptr;
     BunchCounters* rec_host = nullptr;
+    int32_t* rec_cursor = nullptr; // device cursor when rec_host is pinned (written by the device directly)
     TrackTune tune = track_tune_defaults(); // launch shape of the particle passes
     int32_t rec_cap = 0, rec_next = 0;
     int32_t rec_first = -1, rec_count = 0; // records completed by the pending book
@@ -2306,7 +2307,7 @@ struct Engine {
         if (book.n_operators == kMaxOperatorsPerPass) flush(b, sc, elem_charge, false, 0.0, s);
         const int o = book.n_operators++;
         book.slot_begin[o] = book.slot_end[o] = nslots;
-        book.op_record[o] = rec_next;
+        book.op_record[o] = rec_cursor ? 0 : rec_next; // with the device cursor a flag, so turns stay alike
         if (rec_first < 0) rec_first = rec_next;
         ++rec_count;
         ++rec_next;
@@ -2443,7 +2444,9 @@ struct Engine {
             dp.elem_charge = elem_charge;
             dp.book = book;
             dp.xchg = nullptr;
-            dp.step_records = rec_count ? rec_dev : nullptr;
+            dp.step_records = rec_count ? (rec_cursor ? rec_host : rec_dev) : nullptr;
+            dp.rec_cursor = rec_count ? rec_cursor : nullptr;
+            dp.rec_cap = rec_cap;
             if (hook && *hook) {
                 if (!xchg) xchg = dalloc<double>(6 + kMaxSlotsPerPass, "exchange");
                 cuda_check(launch_shard_pack(dp, nslots, xchg, s), "shard pack");
@@ -2459,7 +2462,7 @@ struct Engine {
                 ProfScope ps(PROF_DOMAIN, s);
                 cuda_check(launch_book_domain(dp, s), "domain kernel");
             }
-            if (rec_count)
+            if (rec_count && !rec_cursor) // pageable buffer: copied in stream order
                 cuda_check(cudaMemcpyAsync(rec_host + rec_first, rec_dev + rec_first, sizeof(BunchCounters) * rec_count,
                                            cudaMemcpyDeviceToHost, s),
                            "step records");
@@ -2538,6 +2541,7 @@ struct Propagator {
         dfree(diag_tmp);
         dfree(loss_buf);
         dfree(step_rec_dev);
+        dfree(step_rec_cursor);
         dfree(loss_count);
     }
 
@@ -2689,12 +2693,13 @@ struct Propagator {
         SortBuffers wc;
         int kicks_since_sort;
         size_t ndiag; // host-side diagnostic entries
+        int32_t rec_next, rec_first, rec_count; // per-step count records
     };
     HostSnap snap(const Bunch& b) const
     {
         HostSnap h{b.ref, b.design, b.design_set, b.turns_done, engine_->ops, engine_->book, engine_->nslots,
                    sc ? sc->ghat_valid : false, b.parts, b.masks, b.discards, b.wc, b.kicks_since_sort,
-                   diag_s.size()};
+                   diag_s.size(), engine_->rec_next, engine_->rec_first, engine_->rec_count};
         return h;
     }
     void restore(Bunch& b, const HostSnap& h)
@@ -2713,6 +2718,9 @@ struct Propagator {
         engine_->ops = h.ops;
         engine_->book = h.book;
         engine_->nslots = h.nslots;
+        engine_->rec_next = h.rec_next;
+        engine_->rec_first = h.rec_first;
+        engine_->rec_count = h.rec_count;
         if (sc) sc->ghat_valid = h.ghat_valid;
     }
     // ----- per-turn diagnostics (Diagnostics_full2 at turn ends) ----------
@@ -2899,16 +2907,36 @@ struct Propagator {
     }
 
     // ----- per-step count records -----------------------------------------
+    // A pinned (page-locked, device-addressable) caller buffer is written by
+    // the pass bookkeeping directly, at a device-side cursor: the launches of
+    // a turn are then the same every turn, and CUDA-graph turns can replay
+    // them.  A pageable buffer gets the records by stream-ordered copies of a
+    // device array, and CUDA-graph turns are refused.
     int step_rec_cap = 0;
     BunchCounters* step_rec_dev = nullptr;
     BunchCounters* step_rec_host = nullptr;
+    int32_t* step_rec_cursor = nullptr; // pinned buffer: the device-side record cursor
+    bool step_rec_pinned() const { return step_rec_cursor != nullptr; }
     void set_step_counts(BunchCounters* host, int capacity)
     {
         dfree(step_rec_dev);
         step_rec_dev = nullptr;
+        dfree(step_rec_cursor);
+        step_rec_cursor = nullptr;
         step_rec_host = capacity > 0 ? host : nullptr;
         step_rec_cap = capacity > 0 ? capacity : 0;
-        if (step_rec_cap) step_rec_dev = dalloc<BunchCounters>((size_t)step_rec_cap, "step records");
+        if (step_rec_cap) {
+            cudaPointerAttributes a{};
+            const bool pinned = cudaPointerGetAttributes(&a, host) == cudaSuccess &&
+                                a.type == cudaMemoryTypeHost && a.devicePointer == (void*)host;
+            cudaGetLastError(); // a pageable pointer may leave an error behind
+            if (pinned) {
+                step_rec_cursor = dalloc<int32_t>(1, "step record cursor");
+                cuda_check(cudaMemset(step_rec_cursor, 0, sizeof(int32_t)), "step record cursor");
+            } else {
+                step_rec_dev = dalloc<BunchCounters>((size_t)step_rec_cap, "step records");
+            }
+        }
         wire_step_counts(true);
     }
     void wire_step_counts(bool restart)
@@ -2917,6 +2945,7 @@ struct Propagator {
         engine_->rec_dev = step_rec_dev;
         engine_->rec_host = step_rec_host;
         engine_->rec_cap = step_rec_cap;
+        engine_->rec_cursor = step_rec_cursor;
         if (restart) engine_->rec_next = 0;
     }
 
@@ -4391,8 +4420,9 @@ sb2_status sb2_propagator_set_graphs(sb2_propagator* p, int32_t on)
     if (on && p->p->hook) throw Error(SB2_ERR_UNSUPPORTED, "CUDA-graph turns are not available on a sharded propagator");
     if (on && p->p->loss_cap)
         throw Error(SB2_ERR_UNSUPPORTED, "loss diagnostics are not available with CUDA-graph turns");
-    if (on && p->p->step_rec_cap)
-        throw Error(SB2_ERR_UNSUPPORTED, "per-step count records are not available with CUDA-graph turns");
+    if (on && p->p->step_rec_cap && !p->p->step_rec_pinned())
+        throw Error(SB2_ERR_UNSUPPORTED, "per-step count records into a pageable buffer are not available with "
+                                         "CUDA-graph turns (pass pinned memory)");
     p->p->use_graphs = on != 0;
     if (!on) p->p->drop_graphs();
     SB2_CATCH
@@ -4588,9 +4618,13 @@ sb2_status sb2_propagator_set_step_counts(sb2_propagator* p, sb2_step_counts* ho
     SB2_TRY
     SB2_REQUIRE(p && capacity >= 0 && (host || capacity == 0), "bad argument");
     static_assert(sizeof(sb2_step_counts) == sizeof(BunchCounters), "step record layout");
-    if (capacity > 0 && p->p->use_graphs)
-        throw Error(SB2_ERR_UNSUPPORTED, "per-step count records are not available with CUDA-graph turns");
     p->p->set_step_counts(reinterpret_cast<BunchCounters*>(host), capacity);
+    if (capacity > 0 && p->p->use_graphs && !p->p->step_rec_pinned()) {
+        p->p->set_step_counts(nullptr, 0);
+        throw Error(SB2_ERR_UNSUPPORTED, "per-step count records into a pageable buffer are not available with "
+                                         "CUDA-graph turns (pass pinned memory)");
+    }
+    p->p->drop_graphs(); // captured launches name the record arrays
     SB2_CATCH
 }
 

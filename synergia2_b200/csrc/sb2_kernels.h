@@ -55,8 +55,13 @@ struct DomainParams {
     // the ranks (null for a whole bunch); counters then hold the local
     // n_valid and the global n_total / real_num
     const double* xchg;
-    // per-step count records (PassBook::op_record), may be null
+    // per-step count records (PassBook::op_record), may be null.  With
+    // rec_cursor the records go to step_records[*rec_cursor] (pinned host
+    // memory written by the device; op_record only flags the operators that
+    // end a step), and the cursor advances; up to rec_cap records.
     BunchCounters* step_records;
+    int32_t* rec_cursor;
+    int32_t rec_cap;
 };
 
 struct Dims {

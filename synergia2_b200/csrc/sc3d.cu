@@ -86,7 +86,15 @@ __device__ __forceinline__ void book_domain_body(const DomainParams& p)
         // update_total_num: total = sum over ranks of the valid counts
         c.n_total = p.xchg ? old_total - nd_all : c.n_valid;
         c.real_num = old_total ? c.n_total * c.real_num / old_total : 0.0;
-        if (p.step_records && p.book.op_record[o] >= 0) p.step_records[p.book.op_record[o]] = c;
+        if (p.step_records && p.book.op_record[o] >= 0) {
+            if (p.rec_cursor) {
+                const int r = *p.rec_cursor;
+                if (r < p.rec_cap) p.step_records[r] = c;
+                *p.rec_cursor = r + 1;
+            } else {
+                p.step_records[p.book.op_record[o]] = c;
+            }
+        }
     }
     *p.counters = c;
     if (!p.compute_domain) return;

@@ -146,7 +146,8 @@ def test_gpu_step_counts_match_per_step_calls(syn):
 
 def test_gpu_step_counts_with_space_charge_and_graph_refusal(syn):
     """One record per step with space charge; records continue across calls;
-    CUDA-graph turns and per-step records exclude each other."""
+    CUDA-graph turns refuse records into a pageable host buffer (the records
+    then come by copies that a graph would replay to the same addresses)."""
     from helpers import SIG_C0, fodo_cell, gaussian_bunch, product_lattice
     n = 20000
     lat, ref = product_lattice(fodo_cell())
@@ -158,12 +159,47 @@ def test_gpu_step_counts_with_space_charge_and_graph_refusal(syn):
     prop.propagate_steps(bunch, 5, 7)
     recs = prop.step_counts()
     assert len(recs) == 12 and all(r == (n, n, 1e11) for r in recs)
-    with pytest.raises(syn.SB2Error, match="graph"):
-        prop.set_graphs(True)
     prop.set_step_counts(0)
+    import ctypes
+    pageable = np.zeros(4 * ctypes.sizeof(syn._lib.sb2_step_counts), np.uint8)
+    L = syn.lib()
+    syn.check(L.sb2_propagator_set_step_counts(prop.h, ctypes.c_void_p(pageable.ctypes.data), 4))
+    with pytest.raises(syn.SB2Error, match="pageable"):
+        prop.set_graphs(True)
+    syn.check(L.sb2_propagator_set_step_counts(prop.h, None, 0))
     prop.set_graphs(True)
-    with pytest.raises(syn.SB2Error, match="graph"):
-        prop.set_step_counts(4)
+    with pytest.raises(syn.SB2Error, match="pageable"):
+        syn.check(L.sb2_propagator_set_step_counts(prop.h, ctypes.c_void_p(pageable.ctypes.data), 4))
+
+
+def test_gpu_step_counts_with_graph_turns(syn):
+    """Per-step records into pinned memory with CUDA-graph turns (ring cell
+    with losses, space charge): the records equal the same steps launched
+    directly, the turns replay graphs (the records go to a device-side
+    cursor, so turns stay alike), and the bunches agree."""
+    from helpers import gaussian_bunch, product_lattice, ring_cell
+    n = 30000
+    p = gaussian_bunch(n, [2e-3, 1e-4, 2e-3, 1e-4, 0.3, 1e-4], 43)
+    lat, ref = product_lattice(ring_cell(radius=0.004))
+    out = []
+    for graphs in (False, True):
+        prop = syn.Propagator(lat, syn.Split_operator_stepper(syn.Space_charge_3d_open_hockney_options(16, 16, 32),
+                                                               16))
+        ns = prop.num_steps()
+        b = syn.Bunch(ref, n, 1e11)
+        b.set_particles(p)
+        prop.set_step_counts(4 * ns)
+        if graphs:
+            prop.set_graphs(True)
+        prop.propagate_steps(b, 0, 3 * ns + 5)
+        if graphs:
+            captures, replays = prop.graph_stats()
+            assert replays >= 1 and captures <= 3, (captures, replays)
+        out.append((prop.step_counts(), b.get_particles()))
+    (ra, (pa, ma, _)), (rg, (pg, mg, _)) = out
+    assert len(ra) == len(rg) == 3 * ns + 5 and ra == rg
+    assert ra[-1][0] < n  # particles were lost along the way
+    assert np.array_equal(ma, mg) and np.array_equal(pa[:, 6], pg[:, 6])
 
 
 def test_gpu_fp64_peak_probe(syn):
