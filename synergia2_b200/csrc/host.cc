@@ -506,14 +506,24 @@ struct Bunch {
         dfree(wc.discards2);
         dfree(wc.perm2);
         wc = SortBuffers{};
+        perm_valid = false;
     }
-    // home -> working copy in the caller's order (identity permutation)
+    // home -> working copy: the first time in the caller's order (identity
+    // permutation), later in the order the bunch last left its working copy
     void enter_work(cudaStream_t s)
     {
         if (permuted) return;
+        const bool again = perm_valid;
         enter_work_host();
-        cuda_check(launch_sort_gather_in(home_parts, home_stride, home_masks, home_discards, wc, s), "sort gather");
+        if (again) // the order the bunch last left: nearly cell-ordered
+            cuda_check(launch_sort_gather_perm(home_parts, home_stride, home_masks, home_discards, wc, s),
+                       "sort gather");
+        else
+            cuda_check(launch_sort_gather_in(home_parts, home_stride, home_masks, home_discards, wc, s),
+                       "sort gather");
+        perm_valid = true;
     }
+    bool perm_valid = false; // wc.perm holds the last working copy's order
     // enter_work's host side: the working copy's buffers and the switch to
     // them (without the gather, which enter_work launches)
     void enter_work_host()

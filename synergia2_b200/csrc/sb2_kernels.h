@@ -213,6 +213,8 @@ cudaError_t launch_cell_sort_list(const SortItem* items, const int* first, int n
                                   int max_m, cudaStream_t s);
 cudaError_t launch_cell_sort(const SortBuffers& sb, int32_t* scratch, const ScState* sc, int gx, int gy, int gz,
                              cudaStream_t s);
+cudaError_t launch_sort_gather_perm(const double* ups, int64_t ustride, const uint8_t* um, const uint8_t* ud,
+                                    const SortBuffers& sb, cudaStream_t s);
 cudaError_t launch_sort_gather_in(const double* ups, int64_t ustride, const uint8_t* um, const uint8_t* ud,
                                   const SortBuffers& sb, cudaStream_t s);
 cudaError_t launch_sort_scatter_out(const SortBuffers& sb, double* ups, int64_t ustride, uint8_t* um, uint8_t* ud,

@@ -482,6 +482,22 @@ __global__ void sort_gather_in_kernel(const double* __restrict__ ups, int64_t us
     }
 }
 
+// working copy <- caller arrays in the order of the working copy the bunch
+// last left (perm: slot -> caller index, kept): nearly cell-ordered for the
+// last domain, so the first sort after it is a cheap re-sort
+__global__ void sort_gather_perm_kernel(const double* __restrict__ ups, int64_t ustride,
+                                        const uint8_t* __restrict__ um, const uint8_t* __restrict__ ud, double* w,
+                                        uint8_t* wm, uint8_t* wd, const int32_t* __restrict__ wp, int64_t n,
+                                        int64_t wstride)
+{
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = wp[j];
+        for (int c = 0; c < 7; ++c) w[j + c * wstride] = ups[i + c * ustride];
+        wm[j] = um[i];
+        wd[j] = ud ? ud[i] : 0;
+    }
+}
+
 // caller arrays <- working copy, back in the original order: invert the
 // permutation (4-byte scattered writes), then gather so that the wide
 // writes to the caller's columns are coalesced
@@ -541,6 +557,14 @@ cudaError_t launch_cell_sort(const SortBuffers& sb, int32_t* scratch, const ScSt
     sort_scatter_piped_kernel<<<grid, kTileThreads, 0, s>>>(sb.parts, sb.masks, sb.discards, sb.perm, sb.parts2,
                                                             sb.masks2, sb.discards2, sb.perm2, sb.n, sb.stride, sc, gx,
                                                             gy, gz, offsets);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort_gather_perm(const double* ups, int64_t ustride, const uint8_t* um, const uint8_t* ud,
+                                    const SortBuffers& sb, cudaStream_t s)
+{
+    sort_gather_perm_kernel<<<sm_count_s() * 8, 256, 0, s>>>(ups, ustride, um, ud, sb.parts, sb.masks, sb.discards,
+                                                               sb.perm, sb.n, sb.stride);
     return cudaGetLastError();
 }
 
