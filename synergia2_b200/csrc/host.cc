@@ -565,6 +565,49 @@ struct Bunch {
         cuda_check(launch_sort_scatter_out(wc, home_parts, home_stride, home_masks, home_discards, s), "sort scatter");
         drop_work();
     }
+    // settle() with the caller's copy made at the same time: each array is
+    // put back in the caller's order and copied to the host while the next
+    // one is being put back (host arrays as sb2_bunch_get_particles takes
+    // them; null ones are skipped).  Returns when the copies are done.
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t col_done[9] = {};
+    void settle_to_host(double* host_parts, uint8_t* host_masks, uint8_t* host_discards)
+    {
+        if (!copy_stream) {
+            cuda_check(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking), "stream");
+            for (auto& e : col_done) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        }
+        cudaStream_t s = 0;
+        cuda_check(launch_sort_invert(wc, s), "sort invert");
+        for (int c = 0; c < 9; ++c) {
+            void* host = nullptr;
+            const void* dev = nullptr;
+            size_t bytes = 0;
+            if (c < 7) {
+                cuda_check(launch_sort_scatter_out_col(wc, c, home_parts + c * home_stride, s), "sort scatter");
+                host = host_parts ? host_parts + c * n : nullptr;
+                dev = home_parts + c * home_stride;
+                bytes = sizeof(double) * n;
+            } else if (c == 7) {
+                cuda_check(launch_sort_scatter_out_bytes(wc.masks, wc, home_masks, s), "sort scatter");
+                host = host_masks;
+                dev = home_masks;
+                bytes = n;
+            } else if (home_discards) {
+                cuda_check(launch_sort_scatter_out_bytes(wc.discards, wc, home_discards, s), "sort scatter");
+                host = host_discards;
+                dev = home_discards;
+                bytes = n;
+            }
+            if (!host || !bytes) continue;
+            cuda_check(cudaEventRecord(col_done[c], s), "event");
+            cuda_check(cudaStreamWaitEvent(copy_stream, col_done[c], 0), "event");
+            cuda_check(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, copy_stream), "checkout");
+        }
+        cuda_check(cudaStreamSynchronize(copy_stream), "checkout");
+        cuda_check(cudaStreamSynchronize(s), "checkout");
+        drop_work();
+    }
     // forget the working copy (the home arrays are about to be overwritten)
     void drop_work()
     {
@@ -596,6 +639,9 @@ struct Bunch {
         free_work();
         dfree(counters);
         if (snap_counters) cudaFreeHost(snap_counters);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+        for (auto e : col_done)
+            if (e) cudaEventDestroy(e);
     }
     void sync_counters(cudaStream_t s)
     {
@@ -4051,6 +4097,11 @@ sb2_status sb2_bunch_get_particles(sb2_bunch* h, double* host_parts, uint8_t* ho
     SB2_TRY
     SB2_REQUIRE(h, "null bunch");
     Bunch& b = h->b;
+    if (b.permuted && b.n > 0) { // put back in the caller's order and copied out, array by array
+        b.settle_to_host(host_parts, host_masks, host_discards);
+        if (host_discards && !b.discards) std::memset(host_discards, 0, b.n);
+        return SB2_OK;
+    }
     b.settle(0);
     if (b.n == 0) return SB2_OK;
     if (host_parts)

@@ -213,6 +213,11 @@ cudaError_t launch_cell_sort_list(const SortItem* items, const int* first, int n
                                   int max_m, cudaStream_t s);
 cudaError_t launch_cell_sort(const SortBuffers& sb, int32_t* scratch, const ScState* sc, int gx, int gy, int gz,
                              cudaStream_t s);
+// the inverse permutation into perm2, then one array at a time back in the
+// caller's order (pipelined check-out)
+cudaError_t launch_sort_invert(const SortBuffers& sb, cudaStream_t s);
+cudaError_t launch_sort_scatter_out_col(const SortBuffers& sb, int col, double* out, cudaStream_t s);
+cudaError_t launch_sort_scatter_out_bytes(const uint8_t* w, const SortBuffers& sb, uint8_t* out, cudaStream_t s);
 cudaError_t launch_sort_gather_perm(const double* ups, int64_t ustride, const uint8_t* um, const uint8_t* ud,
                                     const SortBuffers& sb, cudaStream_t s);
 cudaError_t launch_sort_gather_in(const double* ups, int64_t ustride, const uint8_t* um, const uint8_t* ud,

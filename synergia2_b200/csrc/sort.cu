@@ -576,6 +576,33 @@ cudaError_t launch_sort_gather_in(const double* ups, int64_t ustride, const uint
     return cudaGetLastError();
 }
 
+// one array back in the caller's order: out[o] = w[inv[o]]
+template <typename T>
+__global__ void sort_scatter_out_col_kernel(const T* __restrict__ w, const int32_t* __restrict__ inv, T* out, int64_t n)
+{
+    for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < n; o += (int64_t)gridDim.x * blockDim.x)
+        out[o] = w[inv[o]];
+}
+
+cudaError_t launch_sort_invert(const SortBuffers& sb, cudaStream_t s)
+{
+    sort_invert_kernel<<<sm_count_s() * 8, 256, 0, s>>>(sb.perm, sb.perm2, sb.n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort_scatter_out_col(const SortBuffers& sb, int col, double* out, cudaStream_t s)
+{
+    sort_scatter_out_col_kernel<double><<<sm_count_s() * 8, 256, 0, s>>>(sb.parts + col * sb.stride, sb.perm2, out,
+                                                                          sb.n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort_scatter_out_bytes(const uint8_t* w, const SortBuffers& sb, uint8_t* out, cudaStream_t s)
+{
+    sort_scatter_out_col_kernel<uint8_t><<<sm_count_s() * 8, 256, 0, s>>>(w, sb.perm2, out, sb.n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_sort_scatter_out(const SortBuffers& sb, double* ups, int64_t ustride, uint8_t* um, uint8_t* ud,
                                     cudaStream_t s)
 {
